@@ -1,0 +1,306 @@
+"""Throughput benchmark of the B200 channel-flow RK3 step.
+
+Default workload: the 2nd-order, partially implicit (y Crank-Nicolson) FP64
+channel at 768 x 384 x 576 cells (~170M), Re_b 21900, dt 3e-4: the large
+throughput configuration.  Metric: grid-point-steps per second (Gpt-steps/s
+= cells * steps / s / 1e9), whole job over all ranks.
+
+One process per GPU (torchrun for N > 1).  The path has no data-path
+exchange on one GPU per field, so N GPUs run N independent replicas ("replicas
+only", weak scaling); the only collectives are the timing barrier and the
+max-over-ranks reduction.
+
+--impl reference times the reference algorithm's CPU implementation (the C++
+restatement in oracle/, all host threads) on a bounded sample of the same
+workload and prints the same JSON line with "impl": "reference".
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic HBM bytes per cell per step, 2nd-order partially implicit path
+# (full-field arrays that must cross HBM once per substep x 3 substeps x word size)
+ALG_ARRAYS_PER_SUBSTEP = 32
+# per-launch algorithmic arrays of each kernel group (reads + writes), see DESIGN.md
+GROUP_ARRAYS = {0: 13, 1: 9, 2: 4, 3: 6, 4: 2, 5: 9}
+GROUP_NAMES = {0: "rhs_pimp", 1: "uhat_pimp", 2: "prsrc_xfft", 3: "zfft_ysolve_izfft", 4: "xifft", 5: "proj",
+               6: "scalar"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="channel768x384x576_re21900")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl"
+        try:
+            import torch
+            if not torch.cuda.is_available():
+                backend = "gloo"
+            else:
+                torch.cuda.set_device(local)
+        except Exception:
+            backend = "gloo"
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, v):
+    if ws <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference(cfg, args, ws, rank, steps=1):
+    """Times the CPU restatement (oracle/) on `steps` full steps of the workload."""
+    from oracle import oracle as O
+    from channel3d_b200 import initfield
+    if args.cpu_threads:
+        O.set_threads(args.cpu_threads)
+    threads = O.num_threads()
+    o = O.Oracle(cfg)
+    yp = o.mesh()[0]
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp)
+    o.set_state(ux, uy, uz, p)
+    del ux, uy, uz, p
+    o.step(1)  # untimed warm-up step (page-in, first-touch)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    return cfg.npoints * steps / dt / 1e9, threads, dt
+
+
+def run_reference(args, ws, rank):
+    from channel3d_b200 import workloads
+    cfg, _ = workloads.get(args.workload, precision=args.precision)
+    if rank != 0:
+        return
+    steps = max(1, args.steps // max(1, args.steps))  # one full step per timed sample
+    vals = []
+    for _ in range(max(1, min(args.steps, 2))):
+        v, thr, dt = cpu_reference(cfg, args, ws, rank, steps=steps)
+        vals.append(v)
+    v = float(np.median(vals))
+    line = {
+        "impl": "reference", "metric": "Gpt-steps/s", "value": v, "unit": "Gpt-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cfg.npoints / (v * 1e9) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": "2nd-order PIMP RK3"},
+        "cpu_baseline": {"value": v, "unit": "Gpt-steps/s", "cores": thr, "kind": "port",
+                         "sample": "%d full RK3 step(s) of the %s workload per timed sample, after one untimed step; "
+                                   "C++ restatement of the reference (oracle/), OpenMP" % (steps, args.workload)},
+        "e2e": {"value": v, "unit": "Gpt-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from channel3d_b200 import ChannelSolver, initfield, workloads
+    cfg, _ = workloads.get(args.workload, precision=args.precision)
+    cfg = cfg.copy(device=local)
+    torch.cuda.set_device(local)
+    s = ChannelSolver(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=s.yp)
+    s.upload(ux, uy, uz, p)
+    s.project()
+    s.step(max(args.warmup, 3) if args.warmup >= 3 else 3)
+
+    clk = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clk.start()
+    t0 = time.perf_counter()
+    info = s.step(args.steps)
+    ms_dev = s.last_step_ms()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(ws)
+    clocks = clk.stop()
+    ms_max = allmax(ws, ms_dev)
+    ms_per_step = ms_max / args.steps
+    value = ws * cfg.npoints * args.steps / (ms_max * 1e-3) / 1e9
+
+    # per-kernel-group device times (one more instrumented step)
+    kt = s.kernel_times(2)
+    word = 4 if args.precision == "mixed" else 8
+    per_group = {}
+    for g, arrs in GROUP_ARRAYS.items():
+        b = arrs * cfg.npoints * word
+        per_group[GROUP_NAMES[g]] = {"ms": kt[g], "alg_bytes": b, "GBps": b / (kt[g] * 1e-3) / 1e9 if kt[g] > 0 else None}
+    dom = max(GROUP_ARRAYS, key=lambda g: kt[g])
+    peak, peak_kind = load_peaks()
+    dom_b = GROUP_ARRAYS[dom] * cfg.npoints * word
+    achieved = dom_b / (kt[dom] * 1e-3) / 1e9
+    step_alg = ALG_ARRAYS_PER_SUBSTEP * 3 * word * cfg.npoints
+    step_achieved = step_alg / (ms_per_step * 1e-3) / 1e9
+
+    # end-to-end through the public API: pinned host arrays -> upload -> K steps -> download
+    e2e = None
+    if not args.no_e2e:
+        pin = [torch.empty(cfg.npoints, dtype=torch.float64).pin_memory().numpy().reshape(cfg.shape)
+               for _ in range(4)]
+        for dst, src in zip(pin, (ux, uy, uz, p)):
+            dst[...] = src
+        outs = [torch.empty(cfg.npoints, dtype=torch.float64).pin_memory().numpy().reshape(cfg.shape)
+                for _ in range(4)]
+        barrier(ws)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.upload(*pin)
+        inf2 = s.step(args.steps)
+        from channel3d_b200 import _lib
+        _lib.check(s.lib.ch3d_download_state(s.ctx, _lib.LAYOUT_INTERIOR, *(_lib.dptr(o) for o in outs), None))
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        te = allmax(ws, te)
+        bytes_io = 4 * cfg.npoints * 8
+        e2e = {"value": ws * cfg.npoints * args.steps / te / 1e9, "unit": "Gpt-steps/s",
+               "h2d_bytes_per_step": bytes_io / args.steps, "d2h_bytes_per_step": bytes_io / args.steps,
+               "what": "ch3d_upload_state (4 FP64 arrays from pinned host memory) + ch3d_step(K) + "
+                       "ch3d_download_state (4 arrays), wall clock, max over ranks"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            v, thr, dt = cpu_reference(cfg.copy(precision="fp64"), args, ws, rank, steps=1)
+            cpu = {"value": v, "unit": "Gpt-steps/s", "cores": thr, "kind": "port",
+                   "sample": "1 full RK3 step of %s (%.1f s) after one untimed step; C++ restatement "
+                             "(oracle/), OpenMP" % (args.workload, dt)}
+        except Exception as ex:  # keep the GPU line even if host memory is short
+            cpu = {"value": None, "unit": "Gpt-steps/s", "cores": None, "kind": "port", "sample": "failed: %s" % ex}
+
+    if rank == 0:
+        line = {
+            "metric": "Gpt-steps/s", "value": value, "unit": "Gpt-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded laminar + 10% uniform noise, projected divergence-free)",
+            "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": "2nd-order PIMP RK3",
+                       "precision": args.precision, "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (%.1f GB of fields)" % (s.memory_bytes() / 1e9)},
+            "steps_per_s": 1e3 / ms_per_step,
+            "gpu_launches": int(args.steps * 35),
+            "roofline": {"bound": "hbm", "kernel": GROUP_NAMES[dom], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
+            "step_roofline": {"alg_bytes_per_cell_step": ALG_ARRAYS_PER_SUBSTEP * 3 * word,
+                              "achieved": step_achieved, "peak": peak, "frac": step_achieved / peak},
+            "kernels": per_group,
+            "memory_bytes": s.memory_bytes(),
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "last_info": info,
+            "wall_s": wall,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,760 @@
+// ch3d_api.cu -- host side of the C ABI declared in include/ch3d.h.
+//
+// Replaces, for one GPU, the start-up and time-step call sites of the
+// reference (src/CFD_2nd/m_ChannelSystem.f90:28-154): metric vectors are built
+// on the host exactly as InitMeshAndMetries does, uploaded once, and the whole
+// RK3 step runs on the device as one captured CUDA graph.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "ch3d_ctx.h"
+
+using namespace ch3d;
+
+namespace {
+
+thread_local std::string g_err = "";
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CU(x)                                                                                  \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) return fail(CH3D_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_));   \
+  } while (0)
+
+const double PI = 3.141592653589793238462643383279502884;
+
+// src/CFD_2nd/m_MeshAndMetries.f90:292-360 (clcCoord), 1-based yp
+void mesh_section(double* yp1, int id1, int id2, double c1, double c2, int StretType, double cStret, int StretOption) {
+  double* yp = yp1 - 1;  // yp[j] with Fortran j
+  int m = id2 - id1;
+  double secLen = c2 - c1;
+  yp[id1] = c1; yp[id2] = c2;
+  switch (StretType) {
+    case 0:
+      for (int j = 0; j <= m; ++j) yp[id1 + j] = c1 + (double)j / (double)m * secLen;
+      break;
+    case 1: {
+      double tstr = std::tanh(cStret);
+      for (int j = 0; j <= m; ++j) {
+        double xi = (double)j / (double)(float)m;  // real(m) is default (single) kind
+        double setCrd = std::tanh(cStret * (xi - 1.0)) / tstr + 1.0;
+        if (StretOption == 0) yp[id1 + j] = c1 + setCrd * secLen;
+        else yp[id2 - j] = c2 - setCrd * secLen;
+      }
+      break;
+    }
+    case 2: {
+      double tstr = std::sin(0.5 * cStret * PI);
+      for (int j = 0; j <= m; ++j) {
+        double xi = (double)j / (double)m - 1.0;
+        double setCrd = std::sin(cStret * xi * PI * 0.5) / tstr + 1.0;
+        if (StretOption == 0) yp[id1 + j] = c1 + setCrd * secLen;
+        else yp[id2 - j] = c2 - setCrd * secLen;
+      }
+      break;
+    }
+    case 3: {
+      if (cStret == 1.0) {
+        for (int j = 0; j <= m; ++j) yp[j + id1] = c1 + (double)j / (double)m * secLen;
+      } else {
+        double tstr = (std::pow(cStret, m) - 1.0) / (cStret - 1.0);
+        for (int j = 0; j <= m - 1; ++j) {
+          double setCrd = std::pow(cStret, j) / tstr;
+          if (StretOption == 0) yp[id1 + j + 1] = yp[id1 + j] + setCrd * secLen;
+          else yp[id2 - j - 1] = yp[id2 - j] - setCrd * secLen;
+        }
+      }
+      break;
+    }
+  }
+  yp[id1] = c1; yp[id2] = c2;
+}
+
+bool factor23(int n, FFTPlanDev& pl) {
+  pl.n = n; pl.npass = 0;
+  int m = n;
+  while (m % 4 == 0) { pl.radix[pl.npass++] = 4; m /= 4; }
+  while (m % 2 == 0) { pl.radix[pl.npass++] = 2; m /= 2; }
+  while (m % 3 == 0) { pl.radix[pl.npass++] = 3; m /= 3; }
+  return m == 1 && pl.npass <= CH3D_MAX_PASSES;
+}
+
+template <class CT>
+std::vector<CT> twiddles(int n, int count) {
+  std::vector<CT> w(count);
+  for (int q = 0; q < count; ++q) {
+    long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)q / (long double)n;
+    w[q].x = (decltype(w[q].x))cosl(ang);
+    w[q].y = (decltype(w[q].y))sinl(ang);
+  }
+  return w;
+}
+
+enum { NMET = 17 };
+
+// Host-side restatement of src/CFD_2nd/m_MeshAndMetries.f90:171-286 and the
+// CN metrics of src/CFD_2nd/m_TScheme.f90:73-85.
+void build_metrics(ch3d_ctx* c) {
+  const ch3d_config& g = c->cfg;
+  const int nyc = c->ny, nyp = nyc + 1, L = nyc + 3;
+  auto vec = [&](std::vector<double>& v) { v.assign(L, 0.0); };
+  vec(c->yc); vec(c->dyp); vec(c->dyc); vec(c->rdyp); vec(c->rdyc); vec(c->yinterp);
+  vec(c->ap2c); vec(c->ac2c); vec(c->am2c); vec(c->ap2p); vec(c->ac2p); vec(c->am2p);
+  vec(c->ap2Pr); vec(c->ac2Pr); vec(c->am2Pr); vec(c->am2cForCN); vec(c->ap2cForCN); vec(c->s1coe);
+  std::vector<double>& yp = c->yp;
+  for (int j = 1; j <= nyc; ++j) c->yc[j] = 0.5 * (yp[j] + yp[j + 1]);
+  c->yc[0] = 2.0 * yp[1] - c->yc[1];
+  c->yc[nyp] = 2.0 * yp[nyp] - c->yc[nyc];
+  for (int j = 1; j <= nyc; ++j) c->dyp[j] = yp[j + 1] - yp[j];
+  c->dyp[0] = c->dyp[1]; c->dyp[nyp] = c->dyp[nyc];
+  for (int j = 2; j <= nyc; ++j) c->dyc[j] = c->yc[j] - c->yc[j - 1];
+  c->dyc[1] = c->dyp[1]; c->dyc[nyp] = c->dyp[nyc];
+  for (int j = 0; j <= nyp; ++j) c->rdyp[j] = 1.0 / c->dyp[j];
+  for (int j = 1; j <= nyp; ++j) c->rdyc[j] = 1.0 / c->dyc[j];
+  for (int j = 1; j <= nyp; ++j) c->yinterp[j] = c->dyp[j] / (c->dyp[j] + c->dyp[j - 1]);
+  const int* Bc = g.BcOption;
+  for (int j = 1; j <= nyc; ++j) { c->am2Pr[j] = c->rdyp[j] * c->rdyc[j]; c->ap2Pr[j] = c->rdyp[j] * c->rdyc[j + 1]; }
+  if (Bc[2] != 0) { c->am2Pr[1] = 0.0; c->ap2Pr[1] = c->rdyp[1] * c->rdyc[2]; }
+  if (Bc[3] != 0) { c->am2Pr[nyc] = c->rdyp[nyc] * c->rdyc[nyc]; c->ap2Pr[nyc] = 0.0; }
+  for (int j = 1; j <= nyc; ++j) c->ac2Pr[j] = -(c->am2Pr[j] + c->ap2Pr[j]);
+  for (int j = 1; j <= nyc; ++j) { c->am2c[j] = c->rdyp[j] * c->rdyc[j]; c->ap2c[j] = c->rdyp[j] * c->rdyc[j + 1]; }
+  if (Bc[2] == -1) {
+    c->am2c[1] = 4.0 * c->rdyc[1] / (c->dyc[1] + 2.0 * c->dyc[2]);
+    c->ap2c[1] = 4.0 * c->rdyc[2] / (c->dyc[1] + 2.0 * c->dyc[2]);
+  }
+  if (Bc[3] == -1) {
+    c->am2c[nyc] = 4.0 * c->rdyc[nyc] / (c->dyc[nyp] + 2.0 * c->dyc[nyc]);
+    c->ap2c[nyc] = 4.0 * c->rdyc[nyp] / (c->dyc[nyp] + 2.0 * c->dyc[nyc]);
+  }
+  for (int j = 1; j <= nyc; ++j) c->ac2c[j] = -(c->am2c[j] + c->ap2c[j]);
+  for (int j = 1; j <= nyc; ++j) { c->am2p[j] = c->rdyc[j] * c->rdyp[j - 1]; c->ap2p[j] = c->rdyc[j] * c->rdyp[j]; }
+  for (int j = 1; j <= nyc; ++j) c->ac2p[j] = -(c->am2p[j] + c->ap2p[j]);
+  for (int j = 1; j <= nyc; ++j) { c->ap2cForCN[j] = c->ap2c[j]; c->am2cForCN[j] = c->am2c[j]; }
+  if (Bc[2] == -1) c->am2cForCN[1] = 2.0 * c->am2c[1]; else if (Bc[2] == -2) c->am2cForCN[1] = 0.0;
+  if (Bc[3] == -1) c->ap2cForCN[nyc] = 2.0 * c->ap2c[nyc]; else if (Bc[3] == -2) c->ap2cForCN[nyc] = 0.0;
+  // bulk-velocity weights (clcRhsX_PIMP, src/CFD_2nd/m_TSchemePIMP_inc.f90:25-27)
+  for (int j = 1; j <= nyc; ++j) {
+    double w = c->dyp[j];
+    if (c->yc[j] < g.ybulk1 || c->yc[j] >= g.ybulk2) w = 0.0;
+    c->s1coe[j] = w;
+  }
+  // x, z (uniform, periodic)
+  c->dx = g.xlx / (double)c->nx; c->dz = g.zlz / (double)c->nz;
+  c->rdx = (double)c->nx / g.xlx; c->rdz = (double)c->nz / g.zlz;
+  c->rdx2 = c->rdx * c->rdx; c->rdz2 = c->rdz * c->rdz;
+  double rdy = (double)nyc / g.yly;
+  c->rdy2 = rdy * rdy;
+  // modified wavenumbers, src/CFD_2nd/m_Poisson.f90:38-66
+  c->WaveNumX.assign(c->nx, 0.0);
+  c->WaveNumZ.assign(c->nz, 0.0);
+  for (int i = 1; i <= c->nx; ++i) c->WaveNumX[i - 1] = 2.0 * c->rdx2 * (std::cos(2.0 * PI * (double)(i - 1) / (double)c->nx) - 1.0);
+  for (int k = 1; k <= c->nz; ++k) c->WaveNumZ[k - 1] = 2.0 * c->rdz2 * (std::cos(2.0 * PI * (double)(k - 1) / (double)c->nz) - 1.0);
+  c->normfft = 1.0 / ((double)c->nx * (double)c->nz);
+}
+
+template <class T>
+void pack_metrics(const ch3d_ctx* c, std::vector<T>& out) {
+  const int L = c->ny + 3;
+  out.assign((size_t)NMET * L, (T)0);
+  const std::vector<double>* v[NMET] = {&c->dyp,   &c->rdyp,  &c->rdyc,  &c->yinterp,   &c->ap2c,      &c->ac2c,
+                                        &c->am2c,  &c->ap2p,  &c->ac2p,  &c->am2p,      &c->ap2Pr,     &c->ac2Pr,
+                                        &c->am2Pr, &c->s1coe, &c->ap2cForCN, &c->am2cForCN, &c->yc};
+  for (int q = 0; q < NMET; ++q)
+    for (int j = 0; j < L; ++j) out[(size_t)q * L + j] = (T)(*v[q])[j];
+}
+
+template <class T>
+Metrics<T> metrics_ptrs(const T* base, int ny) {
+  const int L = ny + 3;
+  Metrics<T> m;
+  m.dyp = base + 0 * L; m.rdyp = base + 1 * L; m.rdyc = base + 2 * L; m.yinterp = base + 3 * L;
+  m.ap2c = base + 4 * L; m.ac2c = base + 5 * L; m.am2c = base + 6 * L;
+  m.ap2p = base + 7 * L; m.ac2p = base + 8 * L; m.am2p = base + 9 * L;
+  m.ap2Pr = base + 10 * L; m.ac2Pr = base + 11 * L; m.am2Pr = base + 12 * L;
+  m.s1coe = base + 13 * L;
+  return m;
+}
+
+int check_config(const ch3d_config* g) {
+  if (!g) return fail(CH3D_ERR_INVALID, "config is NULL");
+  if (g->order != 2 && g->order != 4) return fail(CH3D_ERR_INVALID, "order must be 2 or 4");
+  if (g->order != 2) return fail(CH3D_ERR_UNSUPPORTED, "order %d is not built in this library version", g->order);
+  if (g->nxc < 4 || g->nyc < 4 || g->nzc < 2) return fail(CH3D_ERR_INVALID, "grid too small: %d %d %d", g->nxc, g->nyc, g->nzc);
+  if (g->nxc % 2) return fail(CH3D_ERR_INVALID, "nxc must be even (real-to-complex x transform)");
+  if (g->ischeme != 3) return fail(CH3D_ERR_UNSUPPORTED, "only RK3 (ischeme=3) is built");
+  if (g->IsImplicit != 1) return fail(CH3D_ERR_UNSUPPORTED, "IsImplicit=%d not built (PIMP=1 is)", g->IsImplicit);
+  if (g->BcOption[0] != 0 || g->BcOption[1] != 0 || g->BcOption[4] != 0 || g->BcOption[5] != 0)
+    return fail(CH3D_ERR_UNSUPPORTED, "x and z must be periodic (BcOption 1,2,5,6 = 0)");
+  for (int s = 2; s < 4; ++s)
+    if (g->BcOption[s] != -1 && g->BcOption[s] != -2)
+      return fail(CH3D_ERR_UNSUPPORTED, "y boundaries must be no-slip (-1) or free-slip (-2)");
+  if (g->LES_type != 0) return fail(CH3D_ERR_UNSUPPORTED, "LES_type=%d not built", g->LES_type);
+  if (g->precision != CH3D_PREC_FP64 && g->precision != CH3D_PREC_MIXED) return fail(CH3D_ERR_INVALID, "bad precision");
+  if (g->IsUxConst && !(g->ybulk2 > g->ybulk1)) return fail(CH3D_ERR_INVALID, "ybulk1 OR ybulk2 wrong");
+  if (!(g->dtMax > 0)) return fail(CH3D_ERR_INVALID, "dtMax must be positive");
+  return CH3D_OK;
+}
+
+template <class T>
+int alloc_fields(ch3d_ctx* c) {
+  typedef typename CplxOf<T>::type CT;
+  for (int q = 0; q < 11; ++q) {
+    CU(cudaMalloc(&c->f[q], (size_t)c->N * sizeof(T)));
+    CU(cudaMemsetAsync(c->f[q], 0, (size_t)c->N * sizeof(T), c->stream));
+    c->bytes += (long long)c->N * sizeof(T);
+  }
+  CU(cudaMalloc(&c->spec, (size_t)c->NS * sizeof(CT)));
+  c->bytes += (long long)c->NS * sizeof(CT);
+  std::vector<T> met;
+  pack_metrics<T>(c, met);
+  CU(cudaMalloc(&c->met, met.size() * sizeof(T)));
+  CU(cudaMemcpy(c->met, met.data(), met.size() * sizeof(T), cudaMemcpyHostToDevice));
+  std::vector<CT> tx = twiddles<CT>(c->nx / 2, c->nx / 2), tr = twiddles<CT>(c->nx, c->nx / 2 + 1),
+                  tz = twiddles<CT>(c->nz, c->nz);
+  CU(cudaMalloc(&c->twx, tx.size() * sizeof(CT)));
+  CU(cudaMalloc(&c->twr, tr.size() * sizeof(CT)));
+  CU(cudaMalloc(&c->twz, tz.size() * sizeof(CT)));
+  CU(cudaMemcpy(c->twx, tx.data(), tx.size() * sizeof(CT), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c->twr, tr.data(), tr.size() * sizeof(CT), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c->twz, tz.data(), tz.size() * sizeof(CT), cudaMemcpyHostToDevice));
+  return CH3D_OK;
+}
+
+size_t gidx2(const ch3d_ctx* c, int i, int j, int k) {
+  // (0:nxc+2, 0:nyc+2, 0:nzc+2)
+  return (size_t)i + (size_t)(c->nx + 3) * ((size_t)j + (size_t)(c->ny + 3) * (size_t)k);
+}
+size_t gidx4(const ch3d_ctx* c, int i, int j, int k) {
+  // (-1:nxc+2, 0:nyc+1, -1:nzc+2)
+  return (size_t)(i + 1) + (size_t)(c->nx + 4) * ((size_t)j + (size_t)(c->ny + 2) * (size_t)(k + 1));
+}
+
+// interior (1-based Fortran i,j,k) value from a host array of the given layout
+double host_get(const ch3d_ctx* c, int layout, const double* a, int i, int j, int k) {
+  if (layout == CH3D_LAYOUT_INTERIOR) return a[(size_t)(i - 1) + (size_t)c->nx * ((size_t)(j - 1) + (size_t)c->ny * (k - 1))];
+  if (layout == CH3D_LAYOUT_GHOST2) return a[gidx2(c, i, j, k)];
+  return a[gidx4(c, i, j, k)];
+}
+
+// Host-side ghost fill of a downloaded field, per SetBC_and_UpdateHalo /
+// SetBC_and_UpdateHalo_pr (src/CFD_2nd/m_BC_and_Halo.f90:232-344,410-456)
+// for periodic x,z.  comp: 0 ux, 1 uy, 2 uz, 3 p.
+void host_fill_ghosts(const ch3d_ctx* c, int layout, double* a, int comp) {
+  const int nxc = c->nx, nyc = c->ny, nzc = c->nz, nyp = nyc + 1;
+  const ch3d_config& g = c->cfg;
+  auto at = [&](int i, int j, int k) -> double& {
+    return layout == CH3D_LAYOUT_GHOST2 ? a[gidx2(c, i, j, k)] : a[gidx4(c, i, j, k)];
+  };
+  const int jtop = layout == CH3D_LAYOUT_GHOST2 ? nyc + 2 : nyc + 1;
+  for (int k = 1; k <= nzc; ++k)
+    for (int i = 1; i <= nxc; ++i) {
+      if (comp == 3) { at(i, nyp, k) = at(i, nyc, k); at(i, 0, k) = at(i, 1, k); continue; }
+      if (comp == 1) {
+        at(i, nyp, k) = g.uyBcValue[3];
+        if (jtop >= nyp + 1) at(i, nyp + 1, k) = g.uyBcValue[3] * 2.0 - at(i, nyc, k);
+        at(i, 0, k) = g.uyBcValue[2] * 2.0 - at(i, 2, k);
+        continue;
+      }
+      double wl = comp == 0 ? g.uxBcValue[2] : g.uzBcValue[2];
+      double wh = comp == 0 ? g.uxBcValue[3] : g.uzBcValue[3];
+      if (g.BcOption[3] == -1) at(i, nyp, k) = wh * 2.0 - at(i, nyc, k);
+      else at(i, nyp, k) = wh * c->dyp[nyp] + at(i, nyc, k);
+      if (g.BcOption[2] == -1) at(i, 0, k) = wl * 2.0 - at(i, 1, k);
+      else at(i, 0, k) = at(i, 1, k) - wl * c->dyp[1];
+    }
+  const int hx = layout == CH3D_LAYOUT_GHOST2 ? 1 : 2;  // halo depth kept by the layout
+  const int jlo = 0, jhi = jtop;
+  for (int k = 1; k <= nzc; ++k)
+    for (int j = jlo; j <= jhi; ++j)
+      for (int h = 1; h <= hx; ++h) {
+        at(1 - h, j, k) = at(nxc - h + 1, j, k);
+        at(nxc + h, j, k) = at(h, j, k);
+      }
+  const int ilo = 1 - hx, ihi = nxc + hx;
+  for (int h = 1; h <= hx; ++h)
+    for (int j = jlo; j <= jhi; ++j)
+      for (int i = ilo; i <= ihi; ++i) {
+        at(i, j, 1 - h) = at(i, j, nzc - h + 1);
+        at(i, j, nzc + h) = at(i, j, h);
+      }
+}
+
+template <class T>
+int upload_field(ch3d_ctx* c, int q, int layout, const double* a, int comp) {
+  std::vector<T> h((size_t)c->N);
+  size_t n = 0;
+  for (int k = 1; k <= c->nz; ++k)
+    for (int j = 1; j <= c->ny; ++j)
+      for (int i = 1; i <= c->nx; ++i, ++n) {
+        double v = a ? host_get(c, layout, a, i, j, k) : 0.0;
+        if (comp == 1 && j == 1) v = c->cfg.uyBcValue[2];  // uy(ic,1,kc) = uy_ym
+        h[n] = (T)v;
+      }
+  CU(cudaMemcpyAsync(c->f[q], h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return CH3D_OK;
+}
+
+template <class T>
+int download_field(ch3d_ctx* c, int q, int layout, double* a, int comp) {
+  std::vector<T> h((size_t)c->N);
+  CU(cudaMemcpyAsync(h.data(), c->f[q], h.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  size_t n = 0;
+  for (int k = 1; k <= c->nz; ++k)
+    for (int j = 1; j <= c->ny; ++j)
+      for (int i = 1; i <= c->nx; ++i, ++n) {
+        size_t o = layout == CH3D_LAYOUT_INTERIOR ? n : (layout == CH3D_LAYOUT_GHOST2 ? gidx2(c, i, j, k) : gidx4(c, i, j, k));
+        a[o] = (double)h[n];
+      }
+  if (layout != CH3D_LAYOUT_INTERIOR && comp >= 0) host_fill_ghosts(c, layout, a, comp);
+  return CH3D_OK;
+}
+
+int init_scalars(ch3d_ctx* c) {
+  DevScalars s;
+  std::memset(&s, 0, sizeof(s));
+  s.dt = c->cfg.dtMax;
+  CU(cudaMemcpyAsync(c->sc, &s, sizeof(s), cudaMemcpyHostToDevice, c->stream));
+  CU(launch_bulk_partials(c));
+  CU(launch_diag(c));
+  CU(cudaStreamSynchronize(c->stream));
+  c->scalars_ready = true;
+  return CH3D_OK;
+}
+
+int record_step(ch3d_ctx* c) {
+  CU(launch_step_begin(c));
+  for (int ns = 1; ns <= c->iadvance; ++ns) {
+    CU(launch_substep_setup(c, ns));
+    CU(launch_rhs(c));
+    CU(launch_uhat(c));
+    CU(launch_prsrc_xfft(c, 0));
+    CU(launch_poisson_spectral(c));
+    CU(launch_xifft(c));
+    CU(launch_proj(c, 0));
+  }
+  CU(launch_diag(c));
+  CU(launch_step_end(c));
+  return CH3D_OK;
+}
+
+int build_graph(ch3d_ctx* c) {
+  if (c->graph_exec) return CH3D_OK;
+  // the first launch of each kernel sets its shared-memory attribute outside capture
+  CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = record_step(c);
+  cudaGraph_t gph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
+  if (rc != CH3D_OK) { if (gph) cudaGraphDestroy(gph); return rc; }
+  if (e != cudaSuccess) return fail(CH3D_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  c->graph = gph;
+  CU(cudaGraphInstantiate(&c->graph_exec, c->graph, 0));
+  return CH3D_OK;
+}
+
+int fetch_info(ch3d_ctx* c, ch3d_step_info* info) {
+  DevScalars s;
+  CU(cudaMemcpyAsync(&s, c->sc, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  if (info) {
+    info->SimTime = s.SimTime; info->dt = s.dt; info->cflmp = s.cflmp;
+    info->divmax1 = __builtin_bit_cast(double, s.divmax1);
+    info->divmax2 = __builtin_bit_cast(double, s.divmax2);
+    for (int q = 0; q < 3; ++q) info->vmax[q] = __builtin_bit_cast(double, s.vmax[q]);
+    info->uxm = s.uxm; info->PrGradAver = s.PrGradAver; info->itime = s.itime; info->status = s.status;
+  }
+  return s.status ? CH3D_ERR_DIVERGED : CH3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ch3d_version(void) { return "ch3d-b200 0.1 (sm_100a)"; }
+
+const char* ch3d_last_error(void) { return g_err.c_str(); }
+
+int ch3d_mesh_section(double* yp, int id1, int id2, double c1, double c2, int StretType, double cStret, int StretOption) {
+  if (!yp || id2 <= id1 || id1 < 1) return fail(CH3D_ERR_INVALID, "bad mesh section");
+  if (StretType < 0 || StretType > 3) return fail(CH3D_ERR_INVALID, "StretType Wrong !!!");
+  mesh_section(yp, id1, id2, c1, c2, StretType, cStret, StretOption);
+  return CH3D_OK;
+}
+
+// src/CFD_2nd/m_MeshAndMetries.f90:122-160
+int ch3d_mesh_y(int nyc, double yly, int nSection, const double* SectionLength, const int* nycSection,
+                const int* StretType, const int* StretOption, const double* SectioncStret, double* yp) {
+  if (nSection < 1 || !yp) return fail(CH3D_ERR_INVALID, "nSection Wrong !!!");
+  int tot = 0;
+  for (int j = 0; j < nSection; ++j) {
+    if (SectionLength[j] < 0) return fail(CH3D_ERR_INVALID, "SectionLength Wrong !!!");
+    if (SectioncStret[j] < 0) return fail(CH3D_ERR_INVALID, "SectioncStret Wrong !!!");
+    if (nycSection[j] < 1) return fail(CH3D_ERR_INVALID, "nycSection Wrong 1 !!!");
+    if (StretType[j] < 0 || StretType[j] > 3) return fail(CH3D_ERR_INVALID, "StretType Wrong !!!");
+    if (StretOption[j] < 0 || StretOption[j] > 1) return fail(CH3D_ERR_INVALID, "StretOption Wrong !!!");
+    tot += nycSection[j];
+  }
+  if (tot != nyc) return fail(CH3D_ERR_INVALID, "nycSection Wrong 2 !!!");
+  std::vector<int> nid(nSection + 1, 1);
+  std::vector<double> ysc(nSection + 1, 0.0);
+  double SumLength = 0;
+  for (int j = 0; j < nSection; ++j) SumLength += SectionLength[j];
+  for (int j = 0; j < nSection; ++j) {
+    nid[j + 1] = nid[j] + nycSection[j];
+    ysc[j + 1] = ysc[j] + SectionLength[j] / SumLength * yly;
+  }
+  ysc[nSection] = yly;
+  for (int j = 0; j < nSection; ++j)
+    mesh_section(yp, nid[j], nid[j + 1], ysc[j], ysc[j + 1], StretType[j], SectioncStret[j], StretOption[j]);
+  return CH3D_OK;
+}
+
+int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
+  if (!out) return fail(CH3D_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  if (!yp) return fail(CH3D_ERR_INVALID, "yp is NULL");
+  for (int j = 1; j <= cfg->nyc; ++j)
+    if (!(yp[j] > yp[j - 1])) return fail(CH3D_ERR_INVALID, "yp must increase (yp(%d) <= yp(%d))", j + 1, j);
+  ch3d_ctx* c = new ch3d_ctx();
+  c->cfg = *cfg;
+  c->nx = cfg->nxc; c->ny = cfg->nyc; c->nz = cfg->nzc; c->nxh = cfg->nxc / 2 + 1;
+  c->N = (long long)c->nx * c->ny * c->nz;
+  c->NS = (long long)c->nxh * c->ny * c->nz;
+  c->fp32 = cfg->precision == CH3D_PREC_MIXED;
+  c->device = cfg->device;
+  if (!factor23(c->nx / 2, c->planx) || !factor23(c->nz, c->planz)) {
+    delete c;
+    return fail(CH3D_ERR_UNSUPPORTED, "nxc/2 and nzc must be products of 2 and 3 (got %d, %d)", cfg->nxc / 2, cfg->nzc);
+  }
+  // RK3 constants (src/CFD_2nd/m_Parameters.f90:299-306)
+  c->iadvance = 3;
+  c->gam[0] = 8.0 / 15.0; c->gam[1] = 5.0 / 12.0; c->gam[2] = 3.0 / 4.0;
+  c->the[0] = 0.0; c->the[1] = -17.0 / 60.0; c->the[2] = -5.0 / 12.0;
+  for (int s = 0; s < 3; ++s) c->alp[s] = c->gam[s] + c->the[s];
+  c->yp.assign(c->ny + 3, 0.0);
+  for (int j = 1; j <= c->ny + 1; ++j) c->yp[j] = yp[j - 1];
+  build_metrics(c);
+  auto cleanup = [&](int code) { ch3d_destroy(c); return code; };
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) { int r = fail(CH3D_ERR_CUDA, "cudaSetDevice(%d): %s", c->device, cudaGetErrorString(e)); delete c; return r; }
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { int r = fail(CH3D_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); delete c; return r; }
+  if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+    return cleanup(fail(CH3D_ERR_CUDA, "event create failed"));
+  rc = c->fp32 ? alloc_fields<float>(c) : alloc_fields<double>(c);
+  if (rc) return cleanup(rc);
+  {
+    std::vector<double> met;
+    pack_metrics<double>(c, met);
+    if (cudaMalloc(&c->met64, met.size() * sizeof(double)) != cudaSuccess) return cleanup(fail(CH3D_ERR_NOMEM, "metrics"));
+    cudaMemcpy(c->met64, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice);
+    std::vector<double> w(c->nx + c->nz);
+    for (int i = 0; i < c->nx; ++i) w[i] = c->WaveNumX[i];
+    for (int k = 0; k < c->nz; ++k) w[c->nx + k] = c->WaveNumZ[k];
+    if (cudaMalloc(&c->wave, w.size() * sizeof(double)) != cudaSuccess) return cleanup(fail(CH3D_ERR_NOMEM, "wave"));
+    cudaMemcpy(c->wave, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  c->m64 = metrics_ptrs<double>(c->met64, c->ny);
+  if (c->fp32) c->m32 = metrics_ptrs<float>((const float*)c->met, c->ny);
+  else c->m32 = Metrics<float>();
+  if (!c->fp32) c->m64 = metrics_ptrs<double>((const double*)c->met, c->ny);
+  {
+    dim3 g((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz);
+    c->npart = (int)(g.x * g.y * g.z);
+    if (cudaMalloc(&c->part, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->part2, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->red1, CH3D_NRED * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->red2, CH3D_NRED * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->sc, sizeof(DevScalars)) != cudaSuccess)
+      return cleanup(fail(CH3D_ERR_NOMEM, "partials"));
+    cudaMemsetAsync(c->part, 0, (size_t)c->npart * sizeof(double), c->stream);
+    cudaMemsetAsync(c->part2, 0, (size_t)c->npart * sizeof(double), c->stream);
+    cudaMemsetAsync(c->sc, 0, sizeof(DevScalars), c->stream);
+    c->bytes += 2LL * c->npart * sizeof(double);
+  }
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "create: %s", cudaGetErrorString(e)));
+  *out = c;
+  return CH3D_OK;
+}
+
+int ch3d_destroy(ch3d_ctx* c) {
+  if (!c) return CH3D_OK;
+  cudaSetDevice(c->device);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  for (int q = 0; q < 12; ++q) if (c->f[q]) cudaFree(c->f[q]);
+  void* bufs[] = {c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+                  c->red1, c->red2, c->stat, c->statpart};
+  for (void* b : bufs) if (b) cudaFree(b);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return CH3D_OK;
+}
+
+int ch3d_upload_state(ch3d_ctx* c, int layout, const double* ux, const double* uy, const double* uz, const double* p,
+                      const double* hist) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (layout < 0 || layout > 2) return fail(CH3D_ERR_INVALID, "bad layout %d", layout);
+  if (!ux || !uy || !uz || !p) return fail(CH3D_ERR_INVALID, "state arrays must not be NULL");
+  CU(cudaSetDevice(c->device));
+  int rc;
+  const double* arrs[4] = {ux, uy, uz, p};
+  for (int q = 0; q < 4; ++q) {
+    rc = c->fp32 ? upload_field<float>(c, q, layout, arrs[q], q) : upload_field<double>(c, q, layout, arrs[q], q);
+    if (rc) return rc;
+  }
+  for (int q = 0; q < 3; ++q) {
+    const double* h = hist ? hist + (size_t)q * c->N : nullptr;
+    rc = c->fp32 ? upload_field<float>(c, 4 + q, CH3D_LAYOUT_INTERIOR, h, -1)
+                 : upload_field<double>(c, 4 + q, CH3D_LAYOUT_INTERIOR, h, -1);
+    if (rc) return rc;
+  }
+  return init_scalars(c);
+}
+
+int ch3d_download_state(ch3d_ctx* c, int layout, double* ux, double* uy, double* uz, double* p, double* hist) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (layout < 0 || layout > 2) return fail(CH3D_ERR_INVALID, "bad layout %d", layout);
+  CU(cudaSetDevice(c->device));
+  double* arrs[4] = {ux, uy, uz, p};
+  for (int q = 0; q < 4; ++q) {
+    if (!arrs[q]) continue;
+    int rc = c->fp32 ? download_field<float>(c, q, layout, arrs[q], q) : download_field<double>(c, q, layout, arrs[q], q);
+    if (rc) return rc;
+  }
+  if (hist)
+    for (int q = 0; q < 3; ++q) {
+      int rc = c->fp32 ? download_field<float>(c, 4 + q, CH3D_LAYOUT_INTERIOR, hist + (size_t)q * c->N, -1)
+                       : download_field<double>(c, 4 + q, CH3D_LAYOUT_INTERIOR, hist + (size_t)q * c->N, -1);
+      if (rc) return rc;
+    }
+  return CH3D_OK;
+}
+
+int ch3d_step(ch3d_ctx* c, int nsteps, ch3d_step_info* info) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (nsteps < 0) return fail(CH3D_ERR_INVALID, "nsteps < 0");
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) {
+    int rc = init_scalars(c);
+    if (rc) return rc;
+  }
+  if (!c->graph_exec) {
+    // run one uncaptured step first so that kernel attributes are set outside capture
+    CU(cudaEventRecord(c->ev0, c->stream));
+    int rc = record_step(c);
+    if (rc) return rc;
+    CU(cudaEventRecord(c->ev1, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    rc = build_graph(c);
+    if (rc) return rc;
+    nsteps -= 1;
+    if (nsteps <= 0) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+      c->last_ms = ms;
+      return fetch_info(c, info);
+    }
+  }
+  CU(cudaEventRecord(c->ev0, c->stream));
+  for (int s = 0; s < nsteps; ++s) CU(cudaGraphLaunch(c->graph_exec, c->stream));
+  CU(cudaEventRecord(c->ev1, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  return fetch_info(c, info);
+}
+
+int ch3d_stage(ch3d_ctx* c, int stage, int ns) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (ns < 1 || ns > c->iadvance) return fail(CH3D_ERR_INVALID, "ns out of range");
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) {
+    int rc = init_scalars(c);
+    if (rc) return rc;
+  }
+  switch (stage) {
+    case 0: CU(launch_substep_setup(c, ns)); break;
+    case 1: CU(launch_rhs(c)); break;
+    case 2: CU(launch_uhat(c)); break;
+    case 3: break;  // clcPrSrc is fused into the forward x transform of stage 4
+    case 4:
+      CU(launch_prsrc_xfft(c, 0));
+      CU(launch_poisson_spectral(c));
+      CU(launch_xifft(c));
+      break;
+    case 5: CU(launch_proj(c, 0)); break;  // FluidVelUpdate fused with PressureUpdate
+    case 6: break;
+    default: return fail(CH3D_ERR_INVALID, "bad stage %d", stage);
+  }
+  CU(cudaStreamSynchronize(c->stream));
+  return CH3D_OK;
+}
+
+static int array_slot(int which) {
+  // 0 ux, 1 uy, 2 uz, 3 p, 4..6 Hist, 7 RhsX, 8 RhsY, 9 RhsZ / prphi, 10 nut
+  switch (which) {
+    case 0: case 1: case 2: case 3: case 4: case 5: case 6: case 7: case 8: return which;
+    case 9: return 10;   // prphi (the reference keeps RhsZ and prphiHalo in RealHalo)
+    case 11: return 9;   // RhsZ
+    default: return -1;
+  }
+}
+
+int ch3d_get_array(ch3d_ctx* c, int which, double* host) {
+  if (!c || !host) return fail(CH3D_ERR_INVALID, "NULL argument");
+  int q = array_slot(which);
+  if (q < 0) return fail(CH3D_ERR_INVALID, "bad array id %d", which);
+  CU(cudaSetDevice(c->device));
+  return c->fp32 ? download_field<float>(c, q, CH3D_LAYOUT_INTERIOR, host, -1)
+                 : download_field<double>(c, q, CH3D_LAYOUT_INTERIOR, host, -1);
+}
+
+int ch3d_set_array(ch3d_ctx* c, int which, const double* host) {
+  if (!c || !host) return fail(CH3D_ERR_INVALID, "NULL argument");
+  int q = array_slot(which);
+  if (q < 0) return fail(CH3D_ERR_INVALID, "bad array id %d", which);
+  CU(cudaSetDevice(c->device));
+  int rc = c->fp32 ? upload_field<float>(c, q, CH3D_LAYOUT_INTERIOR, host, q == 1 ? 1 : -1)
+                   : upload_field<double>(c, q, CH3D_LAYOUT_INTERIOR, host, q == 1 ? 1 : -1);
+  if (rc) return rc;
+  c->scalars_ready = false;
+  return CH3D_OK;
+}
+
+int ch3d_poisson(ch3d_ctx* c, const double* src, double* phi) {
+  if (!c || !src || !phi) return fail(CH3D_ERR_INVALID, "NULL argument");
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
+  // src goes through slot 10 (phi) and mode 2 of the x transform
+  int rc = c->fp32 ? upload_field<float>(c, 10, CH3D_LAYOUT_INTERIOR, src, -1)
+                   : upload_field<double>(c, 10, CH3D_LAYOUT_INTERIOR, src, -1);
+  if (rc) return rc;
+  CU(launch_prsrc_xfft(c, 2));
+  CU(launch_poisson_spectral(c));
+  CU(launch_xifft(c));
+  return c->fp32 ? download_field<float>(c, 10, CH3D_LAYOUT_INTERIOR, phi, -1)
+                 : download_field<double>(c, 10, CH3D_LAYOUT_INTERIOR, phi, -1);
+}
+
+int ch3d_project(ch3d_ctx* c, double* divmax_before, double* divmax_after) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
+  unsigned long long* slots = nullptr;
+  CU(cudaMalloc(&slots, 2 * sizeof(unsigned long long)));
+  CU(cudaMemsetAsync(slots, 0, 2 * sizeof(unsigned long long), c->stream));
+  CU(launch_divmax(c, slots));
+  CU(launch_prsrc_xfft(c, 1));
+  CU(launch_poisson_spectral(c));
+  CU(launch_xifft(c));
+  CU(launch_proj(c, 1));
+  CU(launch_divmax(c, slots + 1));
+  unsigned long long h[2];
+  CU(cudaMemcpyAsync(h, slots, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  cudaFree(slots);
+  if (divmax_before) *divmax_before = __builtin_bit_cast(double, h[0]);
+  if (divmax_after) *divmax_after = __builtin_bit_cast(double, h[1]);
+  c->scalars_ready = false;
+  return CH3D_OK;
+}
+
+int ch3d_set_dt(ch3d_ctx* c, double dt) {
+  if (!c || !(dt > 0)) return fail(CH3D_ERR_INVALID, "bad dt");
+  c->cfg.dtMax = dt;
+  if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+  CU(cudaMemcpyAsync(&c->sc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return CH3D_OK;
+}
+
+int ch3d_stats_accumulate(ch3d_ctx* c) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  return fail(CH3D_ERR_UNSUPPORTED, "statistics not built yet");
+}
+
+int ch3d_stats_fetch(ch3d_ctx* c, double* sumstat, int* nfstime, double* prgradsum, int reset) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  (void)sumstat; (void)nfstime; (void)prgradsum; (void)reset;
+  return fail(CH3D_ERR_UNSUPPORTED, "statistics not built yet");
+}
+
+int ch3d_memory_bytes(ch3d_ctx* c, long long* bytes) {
+  if (!c || !bytes) return fail(CH3D_ERR_INVALID, "NULL argument");
+  *bytes = c->bytes;
+  return CH3D_OK;
+}
+
+// Runs `nsteps` steps kernel group by kernel group with CUDA events between
+// the groups on the context's stream; out[q] = mean milliseconds per launch of
+// group q: 0 rhs, 1 uhat, 2 prsrc+x FFT, 3 z FFT + y solve + z iFFT,
+// 4 x iFFT, 5 projection, 6 scalar/reduction kernels.
+int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
+  if (!c || !out || nout < 7 || nsteps < 1) return fail(CH3D_ERR_INVALID, "bad argument");
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
+  const int G = 7;
+  const int per_step = 1 + 7 * c->iadvance + 1;  // timed groups per step
+  std::vector<cudaEvent_t> ev((size_t)2 * per_step * nsteps, nullptr);
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  std::vector<int> grp;
+  size_t q = 0;
+  auto mark = [&](int g) { grp.push_back(g); return cudaEventRecord(ev[q++], c->stream); };
+  auto done = [&]() { return cudaEventRecord(ev[q++], c->stream); };
+  for (int s = 0; s < nsteps; ++s) {
+    CU(mark(6)); CU(launch_step_begin(c)); CU(done());
+    for (int ns = 1; ns <= c->iadvance; ++ns) {
+      CU(mark(6)); CU(launch_substep_setup(c, ns)); CU(done());
+      CU(mark(0)); CU(launch_rhs(c)); CU(done());
+      CU(mark(1)); CU(launch_uhat(c)); CU(done());
+      CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());
+      CU(mark(3)); CU(launch_poisson_spectral(c)); CU(done());
+      CU(mark(4)); CU(launch_xifft(c)); CU(done());
+      CU(mark(5)); CU(launch_proj(c, 0)); CU(done());
+    }
+    CU(mark(6)); CU(launch_diag(c)); CU(launch_step_end(c)); CU(done());
+  }
+  if (q != ev.size()) return fail(CH3D_ERR_INVALID, "kernel_times event count mismatch");
+  CU(cudaStreamSynchronize(c->stream));
+  std::vector<double> sum(G, 0.0);
+  std::vector<int> cnt(G, 0);
+  for (size_t m = 0; m < grp.size(); ++m) {
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, ev[2 * m], ev[2 * m + 1]));
+    sum[grp[m]] += ms;
+    cnt[grp[m]] += 1;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int g = 0; g < G; ++g) out[g] = cnt[g] ? sum[g] / cnt[g] : 0.0;
+  return fetch_info(c, nullptr);
+}
+
+int ch3d_last_step_ms(ch3d_ctx* c, double* ms) {
+  if (!c || !ms) return fail(CH3D_ERR_INVALID, "NULL argument");
+  *ms = c->last_ms;
+  return CH3D_OK;
+}
+
+}  // extern "C"

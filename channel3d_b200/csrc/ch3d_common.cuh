@@ -1,0 +1,102 @@
+// ch3d_common.cuh -- shared device types for the B200 channel-flow step.
+//
+// Device layout (all fields): interior cells only, Fortran order with i
+// fastest, 0-based index idx = i + nx*(j + ny*k), i in [0,nx), j in [0,ny),
+// k in [0,nz); j = jc-1 of the reference.  Periodic x and z neighbours wrap;
+// y ghost values are produced inline from the boundary rules of
+// SetBC_and_UpdateHalo (src/CFD_2nd/m_BC_and_Halo.f90:232-344) instead of
+// being stored, so no halo planes are kept or exchanged.
+// Metric vectors keep the reference's Fortran index (jc = 0..nyp+1).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ch3d {
+
+template <class T> struct CplxOf;
+template <> struct CplxOf<double> { typedef double2 type; };
+template <> struct CplxOf<float> { typedef float2 type; };
+
+__host__ __device__ inline double2 mk(double a, double b) { return make_double2(a, b); }
+__host__ __device__ inline float2 mk(float a, float b) { return make_float2(a, b); }
+template <class CT> __device__ __forceinline__ CT cadd(CT a, CT b) { return mk(a.x + b.x, a.y + b.y); }
+template <class CT> __device__ __forceinline__ CT csub(CT a, CT b) { return mk(a.x - b.x, a.y - b.y); }
+template <class CT> __device__ __forceinline__ CT cmul(CT a, CT b) {
+  return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <class CT> __device__ __forceinline__ CT cconj(CT a) { return mk(a.x, -a.y); }
+
+// Scalars that change during a run live on the device so that a whole time
+// step can be replayed as one CUDA graph without host round trips.
+struct DevScalars {
+  double dt, SimTime;
+  double pmGamma, pmTheta, pmAlpha, pmBeta, pmAlphaC, pmBetaT;
+  double dpmdxns, PrGradNow, PrGradAver;
+  double cflmp, uxm, s1tot1;
+  unsigned long long divmax1, divmax2, vmax[3], uddx;  // bit patterns of non-negative doubles
+  int itime, status, ns, pad;
+};
+
+// Metric vectors (FP64 master copies; FP32 copies for the mixed path).
+// Indexed with the reference's Fortran index.
+template <class T> struct Metrics {
+  const T* dyp;        // 0..nyp
+  const T* rdyp;       // 0..nyp
+  const T* rdyc;       // 0..nyp (1..nyp valid)
+  const T* yinterp;    // YinterpCoe 1..nyp (0 unused)
+  const T* ap2c; const T* ac2c; const T* am2c;    // 1..nyc
+  const T* ap2p; const T* ac2p; const T* am2p;    // 1..nyc
+  const T* ap2Pr; const T* ac2Pr; const T* am2Pr; // 1..nyc
+  const T* s1coe;      // bulk-sum weight dyp(jc) or 0 (clcRhsX_PIMP :25-27), 1..nyc
+};
+
+// Boundary description for y (x and z are periodic).
+struct YBc {
+  int lo, hi;                     // BcOption(3), BcOption(4): -1 no-slip, -2 free-slip
+  double ux_lo, ux_hi, uz_lo, uz_hi, uy_lo, uy_hi;
+  double dyp1, dypN;              // dyp(1), dyp(nyp)
+};
+
+template <class T> struct Geo {
+  int nx, ny, nz, nxh;
+  long long N;
+  T rdx, rdz, rdx2, rdz2;
+  T ap1c, ac1c, am1c, ap3c, ac3c, am3c;  // constant for periodic x and z
+  T xnu, g1, g2, g3;
+  YBc bc;
+};
+
+__device__ __forceinline__ int wrapm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
+__device__ __forceinline__ int wrapp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
+
+// Field value with y ghost cells from the boundary rules
+// (SetBC_and_UpdateHalo, src/CFD_2nd/m_BC_and_Halo.f90:241-282).
+// comp: 0 ux, 1 uy, 2 uz, 3 pressure.  j may be -1 .. ny.
+template <class T>
+__device__ __forceinline__ T fld(const T* __restrict__ a, const Geo<T>& g, int comp, int i, int j, int k) {
+  const int nx = g.nx, ny = g.ny;
+  if (j >= 0 && j < ny) return __ldg(a + i + (long long)nx * (j + (long long)ny * k));
+  if (j < 0) {
+    if (comp == 1) {  // uy(ic,0,kc) = uy_ym*2 - uy(ic,2,kc)
+      return (T)(g.bc.uy_lo * 2.0) - __ldg(a + i + (long long)nx * (1 + (long long)ny * k));
+    }
+    T v = __ldg(a + i + (long long)nx * (0 + (long long)ny * k));
+    if (comp == 3) return v;  // pressure(ic,0,kc) = pressure(ic,1,kc)
+    double w = comp == 0 ? g.bc.ux_lo : g.bc.uz_lo;
+    if (g.bc.lo == -1) return (T)(w * 2.0) - v;
+    return v - (T)(w * g.bc.dyp1);
+  }
+  // j == ny  (reference index nyp)
+  if (comp == 1) return (T)g.bc.uy_hi;  // uy(ic,nyp,kc) = uyBcValue(yp)
+  T v = __ldg(a + i + (long long)nx * ((ny - 1) + (long long)ny * k));
+  if (comp == 3) return v;
+  double w = comp == 0 ? g.bc.ux_hi : g.bc.uz_hi;
+  if (g.bc.hi == -1) return (T)(w * 2.0) - v;
+  return (T)(w * g.bc.dypN) + v;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+}  // namespace ch3d

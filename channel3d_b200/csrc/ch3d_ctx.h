@@ -1,0 +1,78 @@
+// ch3d_ctx.h -- host-side context of the C ABI (no device code).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "../../include/ch3d.h"
+#include "ch3d_common.cuh"
+#include "fft.cuh"
+
+#define CH3D_NRED 256
+
+struct ch3d_ctx {
+  ch3d_config cfg;
+  int nx = 0, ny = 0, nz = 0, nxh = 0;
+  long long N = 0, NS = 0;  // real points, complex spectral points
+  bool fp32 = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+
+  // Runge-Kutta constants (src/CFD_2nd/m_Parameters.f90:291-306)
+  int iadvance = 3;
+  double gam[3] = {0, 0, 0}, the[3] = {0, 0, 0}, alp[3] = {0, 0, 0};
+
+  // host metrics, Fortran-indexed (m_MeshAndMetries)
+  double dx = 0, dz = 0, rdx = 0, rdz = 0, rdx2 = 0, rdz2 = 0, rdy2 = 0;
+  double normfft = 1.0;
+  std::vector<double> yp, yc, dyp, dyc, rdyp, rdyc, yinterp;
+  std::vector<double> ap2c, ac2c, am2c, ap2p, ac2p, am2p, ap2Pr, ac2Pr, am2Pr;
+  std::vector<double> am2cForCN, ap2cForCN, s1coe, WaveNumX, WaveNumZ;
+
+  // device buffers
+  void* f[12] = {nullptr};   // ux uy uz p hx hy hz rx ry rz phi nut (precision T)
+  void* spec = nullptr;      // complex spectrum (kx,j,kz)
+  void* met = nullptr;       // packed metric vectors (precision T)
+  double* met64 = nullptr;   // FP64 copy (always)
+  double* wave = nullptr;    // WaveNumX (nx) | WaveNumZ (nz), FP64
+  void* twx = nullptr;       // W_{nx/2} table
+  void* twr = nullptr;       // W_{nx} table, 0..nx/2
+  void* twz = nullptr;       // W_{nz} table
+  ch3d::DevScalars* sc = nullptr;
+  double* part = nullptr;    // block partial sums of ux*s1coe (bulk constraint)
+  double* part2 = nullptr;   // block partial sums of ux*dyp (CalcUxAver)
+  double* red1 = nullptr;    // CH3D_NRED second-level sums of part
+  double* red2 = nullptr;    // CH3D_NRED second-level sums of part2
+  int npart = 0;
+  double* stat = nullptr;    // SumStat(35, nyp) accumulator (FP64)
+  double* statpart = nullptr;
+  int nfstime = 0;
+  double prgradsum = 0;
+  long long bytes = 0;
+
+  ch3d::FFTPlanDev planx, planz;
+  ch3d::Metrics<double> m64;
+  ch3d::Metrics<float> m32;
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool scalars_ready = false;
+};
+
+namespace ch3d {
+// launchers (ch3d_step.cu)
+cudaError_t launch_substep_setup(ch3d_ctx* c, int ns);
+cudaError_t launch_step_begin(ch3d_ctx* c);
+cudaError_t launch_step_end(ch3d_ctx* c);
+cudaError_t launch_rhs(ch3d_ctx* c);
+cudaError_t launch_uhat(ch3d_ctx* c);
+cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: step (1/pmAlpha), 1: projection (1)
+cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv
+cudaError_t launch_xifft(ch3d_ctx* c);
+cudaError_t launch_proj(ch3d_ctx* c, int mode);        // mode 0: step, 1: projection only
+cudaError_t launch_bulk_partials(ch3d_ctx* c);
+cudaError_t launch_diag(ch3d_ctx* c);
+cudaError_t launch_stats(ch3d_ctx* c);
+cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot);
+}  // namespace ch3d

@@ -1,0 +1,1009 @@
+// ch3d_step.cu -- sm_100a kernels of the 2nd-order partially implicit RK3
+// step (src/CFD_2nd/m_ChannelSystem.f90:73-154 with the PIMP procedures of
+// src/CFD_2nd/m_TSchemePIMP_inc.f90) and the pressure Poisson pipeline
+// (src/CFD_2nd/m_Poisson.f90:1078-1201).  FP64 and FP32 (mixed) instances.
+//
+// Per substep the device runs:
+//   substep_setup  PMcoeUpdate + bulk-velocity reduction (clcRhsX_PIMP :60-74)
+//   rhs            clcRhsX/Y/Z_PIMP (stencils, Hist update)
+//   uhat           clcU1/2/3Hat_PIMP (y Crank-Nicolson, partitioned tridiagonal)
+//   prsrc_xfft     clcPrSrcOther fused with the forward x R2C FFT
+//   spectral       z FFT, y tridiagonal per (kx,kz) with the (0,0) pin, z iFFT
+//   xifft          x C2R FFT * normfft -> phi
+//   proj           FluidVelUpdate + PressureUpdate_PIMP + next bulk partial sums
+// and per step: step_begin (CalcMaxCFL/dt), diag (CheckDivergence, CalcVmax,
+// CalcUxAver, next CFL), step_end (limit checks).
+#include <cstdio>
+#include "ch3d_ctx.h"
+
+namespace ch3d {
+
+// ---------------------------------------------------------------------------
+// scalar kernels
+// ---------------------------------------------------------------------------
+
+// src/CFD_2nd/m_ChannelSystem.f90:81-88 (CalcMaxCFL result -> cflmp, dt)
+__global__ void k_step_begin(DevScalars* sc, int iCFL, double CFLc, double dtMax) {
+  if (sc->status) return;
+  double uddx = __longlong_as_double((long long)sc->uddx);
+  sc->itime += 1;
+  sc->cflmp = uddx * sc->dt;
+  if (iCFL == 1) {
+    double d = CFLc / uddx;
+    sc->dt = d < dtMax ? d : dtMax;
+  } else {
+    sc->dt = dtMax;
+  }
+}
+
+// src/CFD_2nd/m_Parameters.f90:329-342 (PMcoeUpdate) and the bulk constraint of
+// src/CFD_2nd/m_TSchemePIMP_inc.f90:60-74 from the partial sums of the current ux.
+__global__ void k_substep_setup(DevScalars* sc, const double* __restrict__ part, int npart, int ns, double gam,
+                                double the, double alp, double xnu, int IsUxConst, double ubulk, double norm_bulk) {
+  __shared__ double red[256];
+  if (sc->status) return;
+  double s = 0;
+  for (int q = threadIdx.x; q < npart; q += blockDim.x) s += part[q];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double dt = sc->dt;
+    sc->pmGamma = gam * dt;
+    sc->pmTheta = the * dt;
+    sc->pmAlpha = alp * dt;
+    sc->pmBeta = 0.5 * alp * xnu * dt;
+    sc->SimTime = sc->SimTime + dt * alp;
+    sc->pmAlphaC = alp;
+    sc->pmBetaT = 0.5 * alp * dt;
+    if (ns == 1) sc->PrGradAver = 0.0;
+    sc->ns = ns;
+    sc->divmax1 = 0ull;
+    if (IsUxConst) {
+      double s1tot1 = red[0] * norm_bulk;
+      sc->s1tot1 = s1tot1;
+      sc->dpmdxns = alp * (ubulk - s1tot1);
+      sc->PrGradNow = (ubulk - s1tot1) / dt;
+      sc->PrGradAver = sc->PrGradAver + alp * sc->PrGradNow;
+    } else {
+      sc->dpmdxns = 0.0;
+    }
+  }
+}
+
+// src/CFD_2nd/m_ChannelSystem.f90:127-130 (limit checks after the step) and
+// CalcUxAver (src/CFD_2nd/m_Tools.f90:250-270) from partial sums.
+__global__ void k_step_end(DevScalars* sc, const double* __restrict__ part, int npart, double norm_uxm, double div_limit,
+                           double vel_limit) {
+  __shared__ double red[256];
+  if (sc->status) return;
+  double s = 0;
+  for (int q = threadIdx.x; q < npart; q += blockDim.x) s += part[q];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sc->uxm = red[0] * norm_uxm;
+    double d2 = __longlong_as_double((long long)sc->divmax2);
+    double v0 = __longlong_as_double((long long)sc->vmax[0]);
+    double v1 = __longlong_as_double((long long)sc->vmax[1]);
+    double v2 = __longlong_as_double((long long)sc->vmax[2]);
+    double vmin = fmin(v0, fmin(v1, v2));
+    if (!(d2 <= div_limit)) sc->status = 1;        // NaN trips too
+    else if (!(vmin <= vel_limit)) sc->status = 2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// clcRhsX/Y/Z_PIMP  (src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75, 161-209, 277-325)
+// One thread per cell; all three components share the loads.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                  const T* __restrict__ uy, const T* __restrict__ uz,
+                                                  const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
+                                                  T* __restrict__ hz, T* __restrict__ rx, T* __restrict__ ry,
+                                                  T* __restrict__ rz, const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j >= ny) return;
+  const int im = wrapm(i, nx), ip = wrapp(i, nx), km = wrapm(k, nz), kp = wrapp(k, nz);
+  const int jc = j + 1;
+  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
+  const T two = (T)2, half = (T)0.5, quarter = (T)0.25, one = (T)1;
+  const long long idx = i + (long long)nx * (j + (long long)ny * k);
+
+  // ux samples
+  const T ux_c = ux[idx];
+  const T ux_ip = fld(ux, g, 0, ip, j, k), ux_im = fld(ux, g, 0, im, j, k);
+  const T ux_jp = fld(ux, g, 0, i, j + 1, k), ux_jm = fld(ux, g, 0, i, j - 1, k);
+  const T ux_kp = fld(ux, g, 0, i, j, kp), ux_km = fld(ux, g, 0, i, j, km);
+  const T ux_ip_jm = fld(ux, g, 0, ip, j - 1, k), ux_ip_km = fld(ux, g, 0, ip, j, km);
+  // uy samples
+  const T uy_c = uy[idx];
+  const T uy_ip = fld(uy, g, 1, ip, j, k), uy_im = fld(uy, g, 1, im, j, k);
+  const T uy_jp = fld(uy, g, 1, i, j + 1, k), uy_jm = fld(uy, g, 1, i, j - 1, k);
+  const T uy_im_jp = fld(uy, g, 1, im, j + 1, k);
+  const T uy_kp = fld(uy, g, 1, i, j, kp), uy_km = fld(uy, g, 1, i, j, km);
+  const T uy_jp_km = fld(uy, g, 1, i, j + 1, km);
+  // uz samples
+  const T uz_c = uz[idx];
+  const T uz_ip = fld(uz, g, 2, ip, j, k), uz_im = fld(uz, g, 2, im, j, k);
+  const T uz_jp = fld(uz, g, 2, i, j + 1, k), uz_jm = fld(uz, g, 2, i, j - 1, k);
+  const T uz_kp = fld(uz, g, 2, i, j, kp), uz_km = fld(uz, g, 2, i, j, km);
+  const T uz_im_kp = fld(uz, g, 2, im, j, kp), uz_jm_kp = fld(uz, g, 2, i, j - 1, kp);
+  // pressure samples
+  const T p_c = pr[idx];
+  const T p_im = fld(pr, g, 3, im, j, k), p_jm = fld(pr, g, 3, i, j - 1, k), p_km = fld(pr, g, 3, i, j, km);
+
+  const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
+  const T IY1 = m.yinterp[jc], IY2 = one - IY1;
+  const T IY3 = m.yinterp[jc + 1], IY4 = one - IY3;
+
+  // ---- RhsX ----
+  {
+    const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+    const T sucaj = half * m.rdyp[jc];
+    T h11 = ((ux_ip + ux_c) * (ux_ip + ux_c) - (ux_c + ux_im) * (ux_c + ux_im)) * qdx1;
+    T h12 = ((uy_jp + uy_im_jp) * (IY3 * ux_c + IY4 * ux_jp) - (uy_c + uy_im) * (IY1 * ux_jm + IY2 * ux_c)) * sucaj;
+    T h13 = ((uz_kp + uz_im_kp) * (ux_kp + ux_c) - (uz_c + uz_im) * (ux_c + ux_km)) * qdx3;
+    T d11q1 = (ux_ip - two * ux_c + ux_im) * rdx2;
+    T d22q1 = m.ap2c[jc] * ux_jp + m.ac2c[jc] * ux_c + m.am2c[jc] * ux_jm;
+    T d33q1 = g.ap3c * ux_kp + g.ac3c * ux_c + g.am3c * ux_km;
+    T dcq13 = d11q1 + d33q1;
+    T gradp1 = (p_c - p_im) * rdx;
+    T convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g.g1;
+    rx[idx] = pmGamma * convEd1 + pmTheta * hx[idx] - pmAlpha * gradp1 + two * pmBeta * d22q1;
+    hx[idx] = convEd1;
+  }
+  // ---- RhsY ----
+  {
+    const T hdx1 = half * rdx, hdx3 = half * rdz;
+    const T sucac = m.rdyc[jc], qsucac = quarter * sucac;
+    T h21 = ((IY1 * ux_ip_jm + IY2 * ux_ip) * (uy_ip + uy_c) - (IY1 * ux_jm + IY2 * ux_c) * (uy_c + uy_im)) * hdx1;
+    T h22 = ((uy_jp + uy_c) * (uy_jp + uy_c) - (uy_c + uy_jm) * (uy_c + uy_jm)) * qsucac;
+    T h23 = ((IY1 * uz_jm_kp + IY2 * uz_kp) * (uy_kp + uy_c) - (IY1 * uz_jm + IY2 * uz_c) * (uy_c + uy_km)) * hdx3;
+    T d11q2 = g.ap1c * uy_ip + g.ac1c * uy_c + g.am1c * uy_im;
+    T d22q2 = m.ap2p[jc] * uy_jp + m.ac2p[jc] * uy_c + m.am2p[jc] * uy_jm;
+    T d33q2 = g.ap3c * uy_kp + g.ac3c * uy_c + g.am3c * uy_km;
+    T dcq13 = d11q2 + d33q2;
+    T gradp2 = (p_c - p_jm) * sucac;
+    T convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g.g2;
+    ry[idx] = pmGamma * convEd2 + pmTheta * hy[idx] - pmAlpha * gradp2 + two * pmBeta * d22q2;
+    hy[idx] = convEd2;
+  }
+  // ---- RhsZ ----
+  {
+    const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+    const T sucaj = half * m.rdyp[jc];
+    T h31 = ((ux_ip + ux_ip_km) * (uz_ip + uz_c) - (ux_c + ux_km) * (uz_c + uz_im)) * qdx1;
+    T h32 = ((uy_jp + uy_jp_km) * (IY3 * uz_c + IY4 * uz_jp) - (uy_c + uy_km) * (IY1 * uz_jm + IY2 * uz_c)) * sucaj;
+    T h33 = ((uz_kp + uz_c) * (uz_kp + uz_c) - (uz_c + uz_km) * (uz_c + uz_km)) * qdx3;
+    T d11q3 = g.ap1c * uz_ip + g.ac1c * uz_c + g.am1c * uz_im;
+    T d22q3 = m.ap2c[jc] * uz_jp + m.ac2c[jc] * uz_c + m.am2c[jc] * uz_jm;
+    T d33q3 = (uz_kp - two * uz_c + uz_km) * rdz2;
+    T dcq13 = d11q3 + d33q3;
+    T gradp3 = (p_c - p_km) * rdz;
+    T convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g.g3;
+    rz[idx] = pmGamma * convEd3 + pmTheta * hz[idx] - pmAlpha * gradp3 + two * pmBeta * d22q3;
+    hz[idx] = convEd3;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Partitioned tridiagonal solve (used by clcU*Hat and the Poisson y solve).
+// A system of n rows is cut into P chunks.  Each chunk is solved locally
+// (Thomas) for the data and for two "spikes" (its response to the unknown
+// just left of and just right of it); the 2(P-1) interface unknowns then
+// satisfy a 2x2-block tridiagonal system solved by one thread.  This is the
+// same decomposition as the reference's InverseTridiagonal_reduce
+// (src/CFD_2nd/m_Poisson.f90:1462) applied inside one thread block.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int chunk_lo(int p, int n, int P) { return (p * n) / P; }
+__device__ __forceinline__ int chunk_hi(int p, int n, int P) { return ((p + 1) * n) / P - 1; }
+
+// Coefficients of the velocity Helmholtz systems (identical for all columns).
+// comp 0/2: clcU1Hat_PIMP / clcU3Hat_PIMP (m_TSchemePIMP_inc.f90:410-416, 720-726)
+// comp 1:   clcU2Hat_PIMP (:561-572), row 1 is the identity.
+struct HelmCoef {
+  const double* ap2cForCN; const double* am2cForCN;
+  const double* ap2p; const double* ac2p; const double* am2p;
+};
+
+__device__ __forceinline__ void helm_abc(const HelmCoef& hc, int comp, double pmBeta, int j, double& a, double& b,
+                                         double& c) {
+  const int jc = j + 1;
+  if (comp == 1) {
+    if (j == 0) { a = 0.0; b = 1.0; c = 0.0; return; }
+    c = -pmBeta * hc.ap2p[jc];
+    b = -pmBeta * hc.ac2p[jc] + 1.0;
+    a = -pmBeta * hc.am2p[jc];
+  } else {
+    c = -pmBeta * hc.ap2cForCN[jc];
+    a = -pmBeta * hc.am2cForCN[jc];
+    b = -c - a + 1.0;
+  }
+}
+
+// clcU1Hat/U2Hat/U3Hat_PIMP: (I - pmBeta L_y) du = Rhs ; u += du.
+// Block: TI consecutive i at one k, all j; threads = TI * P.
+template <class T, int TI>
+__global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, HelmCoef hc, T* __restrict__ ux, T* __restrict__ uy,
+                                                   T* __restrict__ uz, const T* __restrict__ rx,
+                                                   const T* __restrict__ ry, const T* __restrict__ rz, int P,
+                                                   const DevScalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int comp = blockIdx.z;
+  T* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
+  const T* rhs = comp == 0 ? rx : (comp == 1 ? ry : rz);
+  const int nx = g.nx, ny = g.ny;
+  const int k = blockIdx.y;
+  const int i0 = blockIdx.x * TI;
+  const int Q = P - 1;
+  double* RM = (double*)smem_raw;
+  double* CP = RM + ny;
+  double* AL = CP + ny;
+  double* BE = AL + ny;
+  double* AA = BE + ny;
+  double* RED = AA + ny;                 // Q * 6 : Minv(4), l, v
+  T* F = (T*)(RED + 6 * (Q > 0 ? Q : 1)); // ny * TI
+  T* IF = F + (size_t)ny * TI;           // TI * Q * 2
+  const double pmBeta = sc->pmBeta;
+  const T add = comp == 0 ? (T)sc->dpmdxns : (T)0;
+  const int tid = threadIdx.x;
+
+  // load the right-hand side tile (RhsX gets the mean pressure gradient, :65-71)
+  for (int t = tid; t < ny * TI; t += blockDim.x) {
+    const int j = t / TI, ii = t % TI;
+    const int i = i0 + ii;
+    T v = (T)0;
+    if (i < nx) {
+      v = rhs[i + (long long)nx * (j + (long long)ny * k)] + add;
+      if (comp == 1 && j == 0) v = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
+    }
+    F[t] = v;
+  }
+  // chunk factors (shared by all columns)
+  if (tid < P) {
+    const int p = tid, s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
+    double cpp = 0.0, dal = 0.0;
+    for (int j = s; j <= e; ++j) {
+      double a, b, c;
+      helm_abc(hc, comp, pmBeta, j, a, b, c);
+      const double mm = (j == s) ? b : b - a * cpp;
+      const double rm = 1.0 / mm;
+      const double cp = c * rm;
+      dal = (j == s) ? -a * rm : -a * dal * rm;
+      RM[j] = rm; CP[j] = cp; AL[j] = (p == 0) ? 0.0 : dal; AA[j] = a;
+      cpp = cp;
+    }
+    BE[e] = (p == P - 1) ? 0.0 : -CP[e];
+    for (int j = e - 1; j >= s; --j) {
+      AL[j] = AL[j] - CP[j] * AL[j + 1];
+      BE[j] = -CP[j] * BE[j + 1];
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double m01p = 0.0, vprev = 0.0;
+    for (int q = 0; q < Q; ++q) {
+      const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
+      const double l = -AL[eq], v = -BE[sq1];
+      double d00 = 1.0, d01 = -BE[eq], d10 = -AL[sq1], d11 = 1.0;
+      if (q > 0) d01 -= l * m01p * vprev;  // (L_q Minv_{q-1} U_{q-1}) has only a (0,1) entry
+      const double det = d00 * d11 - d01 * d10;
+      const double r = 1.0 / det;
+      double* R = RED + 6 * q;
+      R[0] = d11 * r; R[1] = -d01 * r; R[2] = -d10 * r; R[3] = d00 * r; R[4] = l; R[5] = v;
+      m01p = R[1]; vprev = v;
+    }
+  }
+  // local chunk solves for every column
+  for (int t = tid; t < TI * P; t += blockDim.x) {
+    const int ii = t % TI, p = t / TI;
+    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
+    T d = F[s * TI + ii] * (T)RM[s];
+    F[s * TI + ii] = d;
+    for (int j = s + 1; j <= e; ++j) {
+      d = (F[j * TI + ii] - (T)AA[j] * d) * (T)RM[j];
+      F[j * TI + ii] = d;
+    }
+    for (int j = e - 1; j >= s; --j) {
+      d = F[j * TI + ii] - (T)CP[j] * d;
+      F[j * TI + ii] = d;
+    }
+  }
+  __syncthreads();
+  // interface system per column
+  if (tid < TI && Q > 0) {
+    const int ii = tid;
+    T gu = 0, gw = 0;
+    for (int q = 0; q < Q; ++q) {
+      const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
+      const double* R = RED + 6 * q;
+      T ru = F[eq * TI + ii] - (q > 0 ? (T)R[4] * gu : (T)0);
+      T rw = F[sq1 * TI + ii];
+      gu = (T)R[0] * ru + (T)R[1] * rw;
+      gw = (T)R[2] * ru + (T)R[3] * rw;
+      IF[(ii * Q + q) * 2 + 0] = gu;
+      IF[(ii * Q + q) * 2 + 1] = gw;
+    }
+    T zw = IF[(ii * Q + Q - 1) * 2 + 1];
+    for (int q = Q - 2; q >= 0; --q) {
+      const double* R = RED + 6 * q;
+      const T f = (T)R[5] * zw;
+      T zu = IF[(ii * Q + q) * 2 + 0] - (T)R[1] * f;
+      T zwn = IF[(ii * Q + q) * 2 + 1] - (T)R[3] * f;
+      IF[(ii * Q + q) * 2 + 0] = zu;
+      IF[(ii * Q + q) * 2 + 1] = zwn;
+      zw = zwn;
+    }
+  }
+  __syncthreads();
+  // reconstruct and update u
+  for (int t = tid; t < ny * TI; t += blockDim.x) {
+    const int j = t / TI, ii = t % TI;
+    const int i = i0 + ii;
+    if (i >= nx) continue;
+    int p = (j * P) / ny;  // chunk of row j (balanced partition)
+    while (chunk_lo(p, ny, P) > j) --p;
+    while (chunk_hi(p, ny, P) < j) ++p;
+    T x = F[t];
+    if (p > 0) x += (T)AL[j] * IF[(ii * Q + (p - 1)) * 2 + 0];
+    if (p < P - 1) x += (T)BE[j] * IF[(ii * Q + p) * 2 + 1];
+    const long long idx = i + (long long)nx * (j + (long long)ny * k);
+    u[idx] = u[idx] + x;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// clcPrSrcOther (src/CFD_2nd/m_TScheme.f90:213-241) fused with the forward
+// x transform: src = div(u)/pmAlpha, packed as z_n = src_2n + i src_2n+1,
+// complex FFT of length nx/2, then the real-to-complex split
+// X_k = (Z_k + conj Z_{M-k})/2 - i W_nx^k (Z_k - conj Z_{M-k})/2, k = 0..M.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_prsrc_xfft(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                    const T* __restrict__ uy, const T* __restrict__ uz,
+                                                    typename CplxOf<T>::type* __restrict__ spec, FFTPlanDev pl,
+                                                    const typename CplxOf<T>::type* __restrict__ tw,
+                                                    const typename CplxOf<T>::type* __restrict__ twr, int LPB, int mode,
+                                                    DevScalars* __restrict__ sc) {
+  typedef typename CplxOf<T>::type CT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, M = nx / 2, nxh = g.nxh;
+  const int nlines = ny * nz;
+  const int line0 = blockIdx.x * LPB;
+  const int nl = min(LPB, nlines - line0);
+  CT* A = (CT*)smem_raw;
+  CT* B = A + (size_t)LPB * M;
+  const T sudtal = mode == 0 ? (T)(1.0 / sc->pmAlpha) : (T)1;
+  const T rdx = g.rdx, rdz = g.rdz;
+  double dmax = 0.0;
+  for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
+    const int l = t / M, n = t % M;
+    const int line = line0 + l;
+    const int j = line % ny, k = line / ny;
+    const int kp = wrapp(k, nz);
+    const int i0 = 2 * n, i1 = 2 * n + 1, i2 = wrapp(i1, nx);
+    const long long base = (long long)nx * (j + (long long)ny * k);
+    const T sucaj = m.rdyp[j + 1];
+    const T u0 = ux[base + i0], u1 = ux[base + i1], u2 = ux[base + i2];
+    const T v0 = uy[base + i0], v1 = uy[base + i1];
+    const T v0p = fld(uy, g, 1, i0, j + 1, k), v1p = fld(uy, g, 1, i1, j + 1, k);
+    const long long basep = (long long)nx * (j + (long long)ny * kp);
+    const T w0 = uz[base + i0], w1 = uz[base + i1];
+    const T w0p = uz[basep + i0], w1p = uz[basep + i1];
+    T r0 = (u1 - u0) * rdx + (v0p - v0) * sucaj + (w0p - w0) * rdz;
+    T r1 = (u2 - u1) * rdx + (v1p - v1) * sucaj + (w1p - w1) * rdz;
+    if (mode == 2) { r0 = u0; r1 = u1; }  // standalone Poisson: ux carries the source
+    dmax = fmax(dmax, fmax(fabs((double)r0), fabs((double)r1)));
+    A[l * M + n] = mk(sudtal * r0, sudtal * r1);
+  }
+  // block max of |div|
+  {
+    __shared__ double red[256];
+    red[threadIdx.x] = dmax;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) atomic_max_nonneg(&sc->divmax1, red[0]);
+  }
+  CT* Z = fft_lines<CT, false>(A, B, pl, nl, M, 1, tw);
+  const T hf = (T)0.5;
+  for (int t = threadIdx.x; t < nl * (M + 1); t += blockDim.x) {
+    const int l = t / (M + 1), kk = t % (M + 1);
+    const CT a = Z[l * M + (kk == M ? 0 : kk)];
+    const CT b = cconj(Z[l * M + (kk == 0 ? 0 : M - kk)]);
+    const CT e = mk(hf * (a.x + b.x), hf * (a.y + b.y));
+    const CT dd = csub(a, b);
+    const CT o = mk(hf * dd.y, -hf * dd.x);  // (a-b)/(2i)
+    const CT w = __ldg(twr + kk);
+    spec[(long long)nxh * (line0 + l) + kk] = cadd(e, cmul(w, o));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z transform of the spectrum, in place: layout (kx, j, kz), lines over kz.
+// Block = TKX consecutive kx at one j; lines interleaved in shared memory.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_zfft(Geo<T> g, typename CplxOf<T>::type* __restrict__ spec, FFTPlanDev pl,
+                                              const typename CplxOf<T>::type* __restrict__ tw, int TKX, int inverse,
+                                              const DevScalars* __restrict__ sc) {
+  typedef typename CplxOf<T>::type CT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int nz = g.nz, ny = g.ny, nxh = g.nxh;
+  const int kx0 = blockIdx.x * TKX, j = blockIdx.y;
+  CT* A = (CT*)smem_raw;
+  CT* B = A + (size_t)TKX * nz;
+  const long long zs = (long long)nxh * ny;
+  for (int t = threadIdx.x; t < TKX * nz; t += blockDim.x) {
+    const int l = t % TKX, kz = t / TKX;
+    const int kx = kx0 + l;
+    CT v = mk((T)0, (T)0);
+    if (kx < nxh) v = spec[kx + (long long)nxh * j + zs * kz];
+    if (inverse) v = cconj(v);
+    A[kz * TKX + l] = v;
+  }
+  __syncthreads();
+  CT* Z = fft_lines<CT, true>(A, B, pl, TKX, 1, TKX, tw);
+  for (int t = threadIdx.x; t < TKX * nz; t += blockDim.x) {
+    const int l = t % TKX, kz = t / TKX;
+    const int kx = kx0 + l;
+    if (kx >= nxh) continue;
+    CT v = Z[kz * TKX + l];
+    if (inverse) v = cconj(v);
+    spec[kx + (long long)nxh * j + zs * kz] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// y tridiagonal per (kx,kz) (src/CFD_2nd/m_Poisson.f90:1114-1156):
+// [am2Pr, ac2Pr + WaveNumX + WaveNumZ, ap2Pr], with the (kx,kz)=(0,0) system's
+// first row replaced by the identity and zero right-hand side.  Solved in FP64
+// in shared memory (also in the mixed path), partitioned as in k_uhat_pimp
+// but with per-system factors.  Block = TS consecutive kx at one kz.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) k_ysolve(Geo<T> g, Metrics<double> m, const double* __restrict__ wave,
+                                                typename CplxOf<T>::type* __restrict__ spec, int TS, int P,
+                                                const DevScalars* __restrict__ sc) {
+  typedef typename CplxOf<T>::type CT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int nx = g.nx, ny = g.ny, nxh = g.nxh;
+  const int kx0 = blockIdx.x * TS, kz = blockIdx.y;
+  const int Q = P - 1;
+  double2* F = (double2*)smem_raw;               // ny * TS
+  double* CP = (double*)(F + (size_t)ny * TS);   // ny * TS  (cp, later beta)
+  double* AL = CP + (size_t)ny * TS;             // ny * TS
+  double2* IFc = (double2*)(AL + (size_t)ny * TS); // TS * Q * 2
+  double* RED = (double*)(IFc + (size_t)TS * (Q > 0 ? Q : 1) * 2);  // TS * Q * 5 : Minv(4), v
+  const long long zs = (long long)nxh * ny;
+  for (int t = threadIdx.x; t < ny * TS; t += blockDim.x) {
+    const int s = t % TS, j = t / TS;
+    const int kx = kx0 + s;
+    double2 v = make_double2(0.0, 0.0);
+    if (kx < nxh) {
+      CT c = spec[kx + (long long)nxh * j + zs * kz];
+      v = make_double2((double)c.x, (double)c.y);
+    }
+    F[t] = v;
+  }
+  __syncthreads();
+  const double wz = wave[nx + kz];
+  for (int t = threadIdx.x; t < TS * P; t += blockDim.x) {
+    const int s = t % TS, p = t / TS;
+    const int kx = kx0 + s;
+    const double lam = wave[kx < nxh ? kx : 0] + wz;
+    const bool pin = (kx == 0 && kz == 0);
+    const int jlo = chunk_lo(p, ny, P), jhi = chunk_hi(p, ny, P);
+    double cpp = 0.0, dal = 0.0;
+    double2 d = make_double2(0.0, 0.0);
+    for (int j = jlo; j <= jhi; ++j) {
+      const int jc = j + 1;
+      double a = m.am2Pr[jc], c = m.ap2Pr[jc], b = m.ac2Pr[jc] + lam;
+      double2 f = F[j * TS + s];
+      if (pin && j == 0) { a = 0.0; b = 1.0; c = 0.0; f = make_double2(0.0, 0.0); }
+      const double mm = (j == jlo) ? b : b - a * cpp;
+      const double rm = 1.0 / mm;
+      const double cp = c * rm;
+      if (j == jlo) { d.x = f.x * rm; d.y = f.y * rm; dal = -a * rm; }
+      else { d.x = (f.x - a * d.x) * rm; d.y = (f.y - a * d.y) * rm; dal = -a * dal * rm; }
+      F[j * TS + s] = d;
+      CP[j * TS + s] = cp;
+      AL[j * TS + s] = (p == 0) ? 0.0 : dal;
+      cpp = cp;
+    }
+    double be = (p == P - 1) ? 0.0 : -CP[jhi * TS + s];
+    double al = AL[jhi * TS + s];
+    double2 y = F[jhi * TS + s];
+    CP[jhi * TS + s] = be;
+    for (int j = jhi - 1; j >= jlo; --j) {
+      const double cp = CP[j * TS + s];
+      const double2 dj = F[j * TS + s];
+      y.x = dj.x - cp * y.x; y.y = dj.y - cp * y.y;
+      al = AL[j * TS + s] - cp * al;
+      be = -cp * be;
+      F[j * TS + s] = y;
+      AL[j * TS + s] = al;
+      CP[j * TS + s] = be;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < TS && Q > 0) {
+    const int s = threadIdx.x;
+    double* R = RED + (size_t)s * Q * 5;
+    double2* G = IFc + (size_t)s * Q * 2;
+    double m01p = 0.0, vprev = 0.0;
+    double2 gu = make_double2(0.0, 0.0), gw;
+    for (int q = 0; q < Q; ++q) {
+      const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
+      const double l = -AL[eq * TS + s], v = -CP[sq1 * TS + s];
+      double d00 = 1.0, d01 = -CP[eq * TS + s], d10 = -AL[sq1 * TS + s], d11 = 1.0;
+      if (q > 0) d01 -= l * m01p * vprev;  // (L_q Minv_{q-1} U_{q-1}) has only a (0,1) entry
+      const double r = 1.0 / (d00 * d11 - d01 * d10);
+      const double M00 = d11 * r, M01 = -d01 * r, M10 = -d10 * r, M11 = d00 * r;
+      double2 ru = F[eq * TS + s];
+      if (q > 0) { ru.x -= l * gu.x; ru.y -= l * gu.y; }
+      const double2 rw = F[sq1 * TS + s];
+      gu = make_double2(M00 * ru.x + M01 * rw.x, M00 * ru.y + M01 * rw.y);
+      gw = make_double2(M10 * ru.x + M11 * rw.x, M10 * ru.y + M11 * rw.y);
+      G[2 * q] = gu; G[2 * q + 1] = gw;
+      R[5 * q + 0] = M00; R[5 * q + 1] = M01; R[5 * q + 2] = M10; R[5 * q + 3] = M11; R[5 * q + 4] = v;
+      m01p = M01; vprev = v;
+    }
+    double2 zw = G[2 * (Q - 1) + 1];
+    for (int q = Q - 2; q >= 0; --q) {
+      const double* Rq = R + 5 * q;
+      const double fx = Rq[4] * zw.x, fy = Rq[4] * zw.y;
+      double2 zu = G[2 * q], zwn = G[2 * q + 1];
+      zu.x -= Rq[1] * fx; zu.y -= Rq[1] * fy;
+      zwn.x -= Rq[3] * fx; zwn.y -= Rq[3] * fy;
+      G[2 * q] = zu; G[2 * q + 1] = zwn;
+      zw = zwn;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < ny * TS; t += blockDim.x) {
+    const int s = t % TS, j = t / TS;
+    const int kx = kx0 + s;
+    if (kx >= nxh) continue;
+    int p = (j * P) / ny;
+    while (chunk_lo(p, ny, P) > j) --p;
+    while (chunk_hi(p, ny, P) < j) ++p;
+    double2 x = F[t];
+    const double2* G = IFc + (size_t)s * Q * 2;
+    if (p > 0) { const double al = AL[t]; x.x += al * G[2 * (p - 1)].x; x.y += al * G[2 * (p - 1)].y; }
+    if (p < P - 1) { const double be = CP[t]; x.x += be * G[2 * p + 1].x; x.y += be * G[2 * p + 1].y; }
+    spec[kx + (long long)nxh * j + zs * kz] = mk((T)x.x, (T)x.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// inverse x transform (complex-to-real, unnormalised as FFTW's HC2R) * normfft
+// (src/CFD_2nd/m_Poisson.f90:1194-1200) -> phi.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_xifft(Geo<T> g, const typename CplxOf<T>::type* __restrict__ spec,
+                                               T* __restrict__ phi, FFTPlanDev pl,
+                                               const typename CplxOf<T>::type* __restrict__ tw,
+                                               const typename CplxOf<T>::type* __restrict__ twr, int LPB, T normfft,
+                                               const DevScalars* __restrict__ sc) {
+  typedef typename CplxOf<T>::type CT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, M = nx / 2, nxh = g.nxh;
+  const int nlines = ny * nz;
+  const int line0 = blockIdx.x * LPB;
+  const int nl = min(LPB, nlines - line0);
+  CT* A = (CT*)smem_raw;
+  CT* B = A + (size_t)LPB * M;
+  for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
+    const int l = t / M, kk = t % M;
+    const CT* X = spec + (long long)nxh * (line0 + l);
+    const CT a = X[kk];
+    const CT b = cconj(X[M - kk]);
+    const CT e = cadd(a, b);
+    const CT o = cmul(csub(a, b), cconj(__ldg(twr + kk)));
+    // Z_k = e + i o ; stored conjugated for the forward-transform-based inverse
+    const CT z = mk(e.x - o.y, e.y + o.x);
+    A[l * M + kk] = cconj(z);
+  }
+  __syncthreads();
+  CT* Z = fft_lines<CT, false>(A, B, pl, nl, M, 1, tw);
+  for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
+    const int l = t / M, n = t % M;
+    const CT z = cconj(Z[l * M + n]);
+    const long long base = (long long)nx * (line0 + l);
+    phi[base + 2 * n] = z.x * normfft;
+    phi[base + 2 * n + 1] = z.y * normfft;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FluidVelUpdate (src/CFD_2nd/m_TScheme.f90:281-306) + PressureUpdate_PIMP
+// (src/CFD_2nd/m_TSchemePIMP_inc.f90:852-873), phi ghosts from
+// SetBC_and_UpdateHalo_pr (Neumann in y, periodic x,z), plus the block partial
+// sums of ux*dyp used by the next substep's bulk constraint.
+// mode 1: projection only (pmAlpha = 1, no pressure update).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, T* __restrict__ ux, T* __restrict__ uy,
+                                              T* __restrict__ uz, T* __restrict__ pr, const T* __restrict__ phi,
+                                              double* __restrict__ part, int mode, const DevScalars* __restrict__ sc) {
+  __shared__ double red[256];
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+  double s = 0.0;
+  if (i < nx && j < ny) {
+    const int jc = j + 1;
+    const int im = wrapm(i, nx), km = wrapm(k, nz);
+    const long long idx = i + (long long)nx * (j + (long long)ny * k);
+    const T pmAlpha = mode == 0 ? (T)sc->pmAlpha : (T)1;
+    const T phic = phi[idx];
+    const T phim_x = phi[im + (long long)nx * (j + (long long)ny * k)];
+    const T phim_y = phi[i + (long long)nx * ((j > 0 ? j - 1 : 0) + (long long)ny * k)];
+    const T phim_z = phi[i + (long long)nx * (j + (long long)ny * km)];
+    const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha, sucacEta2 = m.rdyc[jc] * pmAlpha;
+    const T uxn = ux[idx] - (phic - phim_x) * rdxEta2;
+    ux[idx] = uxn;
+    uy[idx] = uy[idx] - (phic - phim_y) * sucacEta2;
+    uz[idx] = uz[idx] - (phic - phim_z) * rdzEta2;
+    if (mode == 0) {
+      const T phip_y = phi[i + (long long)nx * ((j < ny - 1 ? j + 1 : ny - 1) + (long long)ny * k)];
+      const T pmBeta = (T)sc->pmBeta;
+      const T pmBetap = -pmBeta * m.ap2Pr[jc];
+      const T pmBetac = -pmBeta * m.ac2Pr[jc] + (T)1;
+      const T pmBetam = -pmBeta * m.am2Pr[jc];
+      pr[idx] = pr[idx] + pmBetap * phip_y + pmBetac * phic + pmBetam * phim_y;
+    }
+    s = (double)uxn * (double)m.s1coe[jc];
+  }
+  red[tl] = s;
+  __syncthreads();
+  for (int w = blockDim.x * blockDim.y / 2; w > 0; w >>= 1) {
+    if (tl < w) red[tl] += red[tl + w];
+    __syncthreads();
+  }
+  if (tl == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = red[0];
+}
+
+// bulk partial sums of ux*s1coe for a freshly uploaded field
+template <class T>
+__global__ void __launch_bounds__(256) k_bulk_partial(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                      double* __restrict__ part) {
+  __shared__ double red[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+  double s = 0.0;
+  if (i < g.nx && j < g.ny) s = (double)ux[i + (long long)g.nx * (j + (long long)g.ny * k)] * (double)m.s1coe[j + 1];
+  red[tl] = s;
+  __syncthreads();
+  for (int w = blockDim.x * blockDim.y / 2; w > 0; w >>= 1) {
+    if (tl < w) red[tl] += red[tl + w];
+    __syncthreads();
+  }
+  if (tl == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = red[0];
+}
+
+// CheckDivergence, CalcVmax, CalcMaxCFL of the next step, CalcUxAver partials
+// (src/CFD_2nd/m_Tools.f90:21-104,250-270).
+template <class T>
+__global__ void __launch_bounds__(256) k_diag(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                              const T* __restrict__ uy, const T* __restrict__ uz,
+                                              double* __restrict__ part, DevScalars* __restrict__ sc, int only_cfl) {
+  __shared__ double red[4][256];
+  __shared__ double rsum[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+  double dv = 0, v0 = 0, v1 = 0, v2 = 0, cf = 0, s = 0;
+  if (i < nx && j < ny) {
+    const int jc = j + 1;
+    const int ip = wrapp(i, nx), kp = wrapp(k, nz);
+    const long long idx = i + (long long)nx * (j + (long long)ny * k);
+    const double a = ux[idx], b = uy[idx], c = uz[idx];
+    const double aip = ux[ip + (long long)nx * (j + (long long)ny * k)];
+    const double bjp = fld(uy, g, 1, i, j + 1, k);
+    const double ckp = uz[i + (long long)nx * (j + (long long)ny * kp)];
+    const double rdx = g.rdx, rdz = g.rdz, rdyp = m.rdyp[jc];
+    dv = fabs((aip - a) * rdx + (bjp - b) * rdyp + (ckp - c) * rdz);
+    v0 = fabs(a); v1 = fabs(b); v2 = fabs(c);
+    cf = fabs(a + aip) * rdx + fabs(b + bjp) * rdyp + fabs(c + ckp) * rdz;
+    s = a * (double)m.dyp[jc];
+  }
+  red[0][tl] = dv; red[1][tl] = v0; red[2][tl] = v1; red[3][tl] = fmax(v2, 0.0);
+  rsum[tl] = s;
+  __shared__ double rcf[256];
+  rcf[tl] = cf;
+  __syncthreads();
+  for (int w = blockDim.x * blockDim.y / 2; w > 0; w >>= 1) {
+    if (tl < w) {
+      for (int q = 0; q < 4; ++q) red[q][tl] = fmax(red[q][tl], red[q][tl + w]);
+      rcf[tl] = fmax(rcf[tl], rcf[tl + w]);
+      rsum[tl] += rsum[tl + w];
+    }
+    __syncthreads();
+  }
+  if (tl == 0) {
+    atomic_max_nonneg(&sc->uddx, rcf[0] * 0.5);
+    if (!only_cfl) {
+      atomic_max_nonneg(&sc->divmax2, red[0][0]);
+      atomic_max_nonneg(&sc->vmax[0], red[1][0]);
+      atomic_max_nonneg(&sc->vmax[1], red[2][0]);
+      atomic_max_nonneg(&sc->vmax[2], red[3][0]);
+      part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = rsum[0];
+    }
+  }
+}
+
+__global__ void k_diag_reset(DevScalars* sc) {
+  if (sc->status) return;
+  sc->divmax2 = 0ull; sc->vmax[0] = 0ull; sc->vmax[1] = 0ull; sc->vmax[2] = 0ull; sc->uddx = 0ull;
+}
+
+// max |div u| of the current field into *slot (for ch3d_project)
+template <class T>
+__global__ void __launch_bounds__(256) k_divmax(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                const T* __restrict__ uy, const T* __restrict__ uz,
+                                                unsigned long long* slot) {
+  __shared__ double red[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+  double dv = 0;
+  if (i < g.nx && j < g.ny) {
+    const int ip = wrapp(i, g.nx), kp = wrapp(k, g.nz);
+    const long long idx = i + (long long)g.nx * (j + (long long)g.ny * k);
+    dv = fabs(((double)ux[ip + (long long)g.nx * (j + (long long)g.ny * k)] - ux[idx]) * g.rdx +
+              ((double)fld(uy, g, 1, i, j + 1, k) - uy[idx]) * m.rdyp[j + 1] +
+              ((double)uz[i + (long long)g.nx * (j + (long long)g.ny * kp)] - uz[idx]) * g.rdz);
+  }
+  red[tl] = dv;
+  __syncthreads();
+  for (int w = blockDim.x * blockDim.y / 2; w > 0; w >>= 1) {
+    if (tl < w) red[tl] = fmax(red[tl], red[tl + w]);
+    __syncthreads();
+  }
+  if (tl == 0) atomic_max_nonneg(slot, red[0]);
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+template <class T> Geo<T> make_geo(const ch3d_ctx* c) {
+  Geo<T> g;
+  g.nx = c->nx; g.ny = c->ny; g.nz = c->nz; g.nxh = c->nxh; g.N = c->N;
+  g.rdx = (T)c->rdx; g.rdz = (T)c->rdz; g.rdx2 = (T)c->rdx2; g.rdz2 = (T)c->rdz2;
+  // periodic x and z: am1c = ap1c = rdx2, ac1c = -(am1c+ap1c) (m_MeshAndMetries.f90:243-252)
+  g.ap1c = (T)c->rdx2; g.am1c = (T)c->rdx2; g.ac1c = (T)(-(c->rdx2 + c->rdx2));
+  g.ap3c = (T)c->rdz2; g.am3c = (T)c->rdz2; g.ac3c = (T)(-(c->rdz2 + c->rdz2));
+  g.xnu = (T)c->cfg.xnu;
+  g.g1 = (T)c->cfg.gravity[0]; g.g2 = (T)c->cfg.gravity[1]; g.g3 = (T)c->cfg.gravity[2];
+  g.bc.lo = c->cfg.BcOption[2]; g.bc.hi = c->cfg.BcOption[3];
+  g.bc.ux_lo = c->cfg.uxBcValue[2]; g.bc.ux_hi = c->cfg.uxBcValue[3];
+  g.bc.uy_lo = c->cfg.uyBcValue[2]; g.bc.uy_hi = c->cfg.uyBcValue[3];
+  g.bc.uz_lo = c->cfg.uzBcValue[2]; g.bc.uz_hi = c->cfg.uzBcValue[3];
+  g.bc.dyp1 = c->dyp[1]; g.bc.dypN = c->dyp[c->ny + 1];
+  return g;
+}
+
+template <class T> const Metrics<T>& metrics_of(const ch3d_ctx* c);
+template <> const Metrics<double>& metrics_of<double>(const ch3d_ctx* c) { return c->m64; }
+template <> const Metrics<float>& metrics_of<float>(const ch3d_ctx* c) { return c->m32; }
+
+static dim3 cell_grid(const ch3d_ctx* c) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz); }
+static dim3 cell_block() { return dim3(32, 8, 1); }
+
+static int pick_P(int ny) {
+  int P = 16;
+  while (P > 1 && ny < 2 * P) P >>= 1;
+  return P;
+}
+
+cudaError_t launch_step_begin(ch3d_ctx* c) {
+  k_step_begin<<<1, 1, 0, c->stream>>>(c->sc, c->cfg.iCFL, c->cfg.CFLc, c->cfg.dtMax);
+  return cudaGetLastError();
+}
+
+// first level of the deterministic two-level sum of block partials
+__global__ void __launch_bounds__(256) k_reduce_partials(const double* __restrict__ in, int n, double* __restrict__ out) {
+  __shared__ double red[256];
+  const int nb = gridDim.x;
+  const int chunk = (n + nb - 1) / nb;
+  const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+  double s = 0.0;
+  for (int q = lo + threadIdx.x; q < hi; q += blockDim.x) s += in[q];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+cudaError_t launch_substep_setup(ch3d_ctx* c, int ns) {
+  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part, c->npart, c->red1);
+  const double norm_bulk = 1.0 / ((double)c->nx * (double)c->nz) / (c->cfg.ybulk2 - c->cfg.ybulk1);
+  k_substep_setup<<<1, 256, 0, c->stream>>>(c->sc, c->red1, CH3D_NRED, ns, c->gam[ns - 1], c->the[ns - 1],
+                                            c->alp[ns - 1], c->cfg.xnu, c->cfg.IsUxConst, c->cfg.ubulk, norm_bulk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_end(ch3d_ctx* c) {
+  const double norm = 1.0 / ((double)c->nx * (double)c->nz) / c->cfg.yly;
+  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part2, c->npart, c->red2);
+  k_step_end<<<1, 256, 0, c->stream>>>(c->sc, c->red2, CH3D_NRED, norm, c->cfg.div_limit, c->cfg.vel_limit);
+  return cudaGetLastError();
+}
+
+template <class T> static cudaError_t rhs_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  k_rhs_pimp<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], f[3],
+                                                              f[4], f[5], f[6], f[7], f[8], f[9], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_rhs(ch3d_ctx* c) { return c->fp32 ? rhs_t<float>(c) : rhs_t<double>(c); }
+
+template <class T> static cudaError_t uhat_t(ch3d_ctx* c) {
+  constexpr int TI = 16;
+  T** f = (T**)c->f;
+  const int P = pick_P(c->ny), Q = P - 1;
+  HelmCoef hc;
+  const double* M = c->met64;
+  const int L = c->ny + 3;
+  // packed metric offsets, see ch3d_api.cu (pack order)
+  hc.ap2p = M + 7 * L; hc.ac2p = M + 8 * L; hc.am2p = M + 9 * L;
+  hc.ap2cForCN = M + 14 * L; hc.am2cForCN = M + 15 * L;
+  size_t smem = (size_t)5 * c->ny * sizeof(double) + (size_t)6 * (Q > 0 ? Q : 1) * sizeof(double) +
+                (size_t)c->ny * TI * sizeof(T) + (size_t)TI * (Q > 0 ? Q : 1) * 2 * sizeof(T) + 16;
+  static bool attr_set[2] = {false, false};
+  auto kern = k_uhat_pimp<T, TI>;
+  if (!attr_set[sizeof(T) == 4]) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set[sizeof(T) == 4] = true;
+  }
+  dim3 grid((c->nx + TI - 1) / TI, c->nz, 3);
+  kern<<<grid, TI * P < 64 ? 64 : TI * P, smem, c->stream>>>(make_geo<T>(c), hc, f[0], f[1], f[2], f[7], f[8], f[9], P,
+                                                             c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_uhat(ch3d_ctx* c) { return c->fp32 ? uhat_t<float>(c) : uhat_t<double>(c); }
+
+template <class T> static int lines_per_block(int M) {
+  // two ping-pong buffers of M complex per line within ~96 KB
+  int lpb = (96 * 1024) / (2 * M * (int)sizeof(typename CplxOf<T>::type));
+  if (lpb > 16) lpb = 16;
+  if (lpb < 1) lpb = 1;
+  return lpb;
+}
+
+template <class T> static cudaError_t prsrc_t(ch3d_ctx* c, int mode) {
+  typedef typename CplxOf<T>::type CT;
+  T** f = (T**)c->f;
+  const int M = c->nx / 2;
+  const int LPB = lines_per_block<T>(M);
+  const int nlines = c->ny * c->nz;
+  size_t smem = (size_t)2 * LPB * M * sizeof(CT);
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[sizeof(T) == 4]) {
+    cudaFuncSetAttribute(k_prsrc_xfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set[sizeof(T) == 4] = true;
+  }
+  T* src = mode == 2 ? f[10] : f[0];
+  k_prsrc_xfft<T><<<(nlines + LPB - 1) / LPB, 256, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), src, f[1], f[2],
+                                                                      (CT*)c->spec, c->planx, (const CT*)c->twx,
+                                                                      (const CT*)c->twr, LPB, mode, c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode) { return c->fp32 ? prsrc_t<float>(c, mode) : prsrc_t<double>(c, mode); }
+
+template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
+  typedef typename CplxOf<T>::type CT;
+  const int nz = c->nz;
+  int TKX = (96 * 1024) / (2 * nz * (int)sizeof(CT));
+  int t = 1;
+  while (t * 2 <= TKX && t * 2 <= 16) t *= 2;
+  TKX = t;
+  size_t smemz = (size_t)2 * TKX * nz * sizeof(CT);
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[sizeof(T) == 4]) {
+    cudaFuncSetAttribute(k_zfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_ysolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set[sizeof(T) == 4] = true;
+  }
+  dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
+  k_zfft<T><<<gz, 256, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int TS = 8, P = pick_P(c->ny), Q = P - 1;
+  size_t smemy = (size_t)c->ny * TS * (sizeof(double2) + 2 * sizeof(double)) +
+                 (size_t)TS * (Q > 0 ? Q : 1) * (2 * sizeof(double2) + 5 * sizeof(double)) + 16;
+  dim3 gy((c->nxh + TS - 1) / TS, c->nz);
+  k_ysolve<T><<<gy, 128, smemy, c->stream>>>(make_geo<T>(c), c->m64, c->wave, (CT*)c->spec, TS, P, c->sc);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_zfft<T><<<gz, 256, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_poisson_spectral(ch3d_ctx* c) { return c->fp32 ? spectral_t<float>(c) : spectral_t<double>(c); }
+
+template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {
+  typedef typename CplxOf<T>::type CT;
+  T** f = (T**)c->f;
+  const int M = c->nx / 2;
+  const int LPB = lines_per_block<T>(M);
+  const int nlines = c->ny * c->nz;
+  size_t smem = (size_t)2 * LPB * M * sizeof(CT);
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[sizeof(T) == 4]) {
+    cudaFuncSetAttribute(k_xifft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set[sizeof(T) == 4] = true;
+  }
+  k_xifft<T><<<(nlines + LPB - 1) / LPB, 256, smem, c->stream>>>(make_geo<T>(c), (const CT*)c->spec, f[10], c->planx,
+                                                                 (const CT*)c->twx, (const CT*)c->twr, LPB,
+                                                                 (T)c->normfft, c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_xifft(ch3d_ctx* c) { return c->fp32 ? xifft_t<float>(c) : xifft_t<double>(c); }
+
+template <class T> static cudaError_t proj_t(ch3d_ctx* c, int mode) {
+  T** f = (T**)c->f;
+  k_proj<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], f[3], f[10],
+                                                          c->part, mode, c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_proj(ch3d_ctx* c, int mode) { return c->fp32 ? proj_t<float>(c, mode) : proj_t<double>(c, mode); }
+
+template <class T> static cudaError_t bulk_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  k_bulk_partial<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], c->part);
+  return cudaGetLastError();
+}
+cudaError_t launch_bulk_partials(ch3d_ctx* c) { return c->fp32 ? bulk_t<float>(c) : bulk_t<double>(c); }
+
+template <class T> static cudaError_t diag_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  k_diag_reset<<<1, 1, 0, c->stream>>>(c->sc);
+  k_diag<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], c->part2,
+                                                          c->sc, 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_diag(ch3d_ctx* c) { return c->fp32 ? diag_t<float>(c) : diag_t<double>(c); }
+
+template <class T> static cudaError_t divmax_t(ch3d_ctx* c, unsigned long long* slot) {
+  T** f = (T**)c->f;
+  k_divmax<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], slot);
+  return cudaGetLastError();
+}
+cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot) {
+  return c->fp32 ? divmax_t<float>(c, slot) : divmax_t<double>(c, slot);
+}
+
+}  // namespace ch3d

@@ -1,0 +1,113 @@
+"""Host-side mirror of the reference's ChannelInitialize / ChannelIterate
+(src/CFD_2nd/m_ChannelSystem.f90:28-154) over the C ABI of libch3d.so.
+
+Arrays are numpy float64, C-order shape (nzc, nyc, nxc), which is the
+memory order of the reference's Fortran (nxc, nyc, nzc) arrays.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .config import mesh_y
+
+
+class ChannelSolver:
+    # ch3d_get_array ids (include/ch3d.h)
+    UX, UY, UZ, P, HISTX, HISTY, HISTZ, RHSX, RHSY, PRPHI, RHSZ = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 11
+
+    def __init__(self, cfg, yp=None):
+        self.lib = _lib.load_library()
+        self.cfg = cfg
+        self.yp = np.ascontiguousarray(mesh_y(cfg, self.lib) if yp is None else yp, dtype=np.float64)
+        self._c = cfg.to_c()
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.ch3d_create(ctypes.byref(self._c), _lib.dptr(self.yp), ctypes.byref(h)), self.lib)
+        self.ctx = h
+
+    def close(self):
+        if self.ctx:
+            self.lib.ch3d_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _arr(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.size == self.cfg.npoints, "array size does not match the grid"
+        return a
+
+    def upload(self, ux, uy, uz, p, hist=None):
+        ux, uy, uz, p = (self._arr(a) for a in (ux, uy, uz, p))
+        h = None
+        if hist is not None:
+            h = np.ascontiguousarray(np.stack([self._arr(a) for a in hist]))
+        _lib.check(self.lib.ch3d_upload_state(self.ctx, _lib.LAYOUT_INTERIOR, _lib.dptr(ux), _lib.dptr(uy),
+                                              _lib.dptr(uz), _lib.dptr(p), _lib.dptr(h)), self.lib)
+
+    def download(self, hist=False):
+        shp = self.cfg.shape
+        ux, uy, uz, p = (np.empty(shp) for _ in range(4))
+        h = np.empty((3,) + shp) if hist else None
+        _lib.check(self.lib.ch3d_download_state(self.ctx, _lib.LAYOUT_INTERIOR, _lib.dptr(ux), _lib.dptr(uy),
+                                                _lib.dptr(uz), _lib.dptr(p), _lib.dptr(h)), self.lib)
+        out = {"ux": ux, "uy": uy, "uz": uz, "p": p}
+        if hist:
+            out["hist"] = h
+        return out
+
+    def step(self, n=1, raise_on_diverge=True):
+        info = _lib.Ch3dStepInfo()
+        rc = self.lib.ch3d_step(self.ctx, int(n), ctypes.byref(info))
+        if rc == _lib.CH3D_ERR_DIVERGED and not raise_on_diverge:
+            return info.as_dict()
+        _lib.check(rc, self.lib)
+        return info.as_dict()
+
+    def stage(self, st, ns):
+        _lib.check(self.lib.ch3d_stage(self.ctx, int(st), int(ns)), self.lib)
+
+    def get_array(self, which):
+        out = np.empty(self.cfg.shape)
+        _lib.check(self.lib.ch3d_get_array(self.ctx, int(which), _lib.dptr(out)), self.lib)
+        return out
+
+    def set_array(self, which, a):
+        a = self._arr(a)
+        _lib.check(self.lib.ch3d_set_array(self.ctx, int(which), _lib.dptr(a)), self.lib)
+
+    def poisson(self, src):
+        src = self._arr(src)
+        phi = np.empty(self.cfg.shape)
+        _lib.check(self.lib.ch3d_poisson(self.ctx, _lib.dptr(src), _lib.dptr(phi)), self.lib)
+        return phi
+
+    def project(self):
+        b, a = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.lib.ch3d_project(self.ctx, ctypes.byref(b), ctypes.byref(a)), self.lib)
+        return b.value, a.value
+
+    def memory_bytes(self):
+        v = ctypes.c_longlong()
+        _lib.check(self.lib.ch3d_memory_bytes(self.ctx, ctypes.byref(v)), self.lib)
+        return v.value
+
+    def kernel_times(self, nsteps=1):
+        out = np.zeros(7)
+        _lib.check(self.lib.ch3d_kernel_times(self.ctx, int(nsteps), _lib.dptr(out), 7), self.lib)
+        return out
+
+    def last_step_ms(self):
+        v = ctypes.c_double()
+        _lib.check(self.lib.ch3d_last_step_ms(self.ctx, ctypes.byref(v)), self.lib)
+        return v.value

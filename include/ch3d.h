@@ -1,0 +1,200 @@
+/*
+ * ch3d.h -- C ABI of the B200 implementation of Channel3d's RK3 time step.
+ *
+ * The Fortran host of the reference keeps its .prm input, its module call
+ * sites and its restart/statistics layout, and binds these entry points
+ * through ISO_C_BINDING.  Every function returns an int
+ * status (CH3D_OK = 0); the message of the last failure of a thread is
+ * available from ch3d_last_error().  Arrays crossing this boundary are plain
+ * host pointers to real(8) data in Fortran (column-major) order.
+ *
+ * Array layouts (argument `layout`):
+ *   CH3D_LAYOUT_INTERIOR   (1:nxc,1:nyc,1:nzc), the restart-file layout of
+ *                          write_restart/read_restart
+ *                          (src/CFD_2nd/m_IOAndVisu.f90:352-558).
+ *   CH3D_LAYOUT_GHOST2     (0:nxc+2,0:nyc+2,0:nzc+2), the `mb1` bounds of the
+ *                          2nd-order solver (src/CFD_2nd/m_Variables.f90:59-61).
+ *   CH3D_LAYOUT_GHOST4     (-1:nxc+2,0:nyc+1,-1:nzc+2), the `mb1` bounds of the
+ *                          4th-order solver (src/CFD_4th/m_Variables.f90:47-49).
+ * On download, ghost cells are filled by the boundary/halo rules of
+ * SetBC_and_UpdateHalo (src/CFD_2nd/m_BC_and_Halo.f90:232-344).
+ *
+ * Threading: one context = one CUDA stream on one device; a context is not
+ * thread-safe, distinct contexts are independent.  Device memory is owned by
+ * the context; host arrays are only borrowed during the call.
+ */
+#ifndef CH3D_H_
+#define CH3D_H_
+
+#if defined(__GNUC__)
+#define CH3D_API __attribute__((visibility("default")))
+#else
+#define CH3D_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CH3D_OK 0
+#define CH3D_ERR_INVALID 1      /* bad argument or configuration */
+#define CH3D_ERR_UNSUPPORTED 2  /* valid for the reference, not built here */
+#define CH3D_ERR_CUDA 3         /* CUDA runtime failure */
+#define CH3D_ERR_DIVERGED 4     /* div_limit or vel_limit exceeded (the
+                                   reference's ErrT_Abort in ChannelIterate,
+                                   src/CFD_2nd/m_ChannelSystem.f90:127-130) */
+#define CH3D_ERR_NOMEM 5
+
+#define CH3D_LAYOUT_INTERIOR 0
+#define CH3D_LAYOUT_GHOST2 1
+#define CH3D_LAYOUT_GHOST4 2
+
+#define CH3D_PREC_FP64 0
+#define CH3D_PREC_MIXED 1       /* FP32 fields, FP64 low-mode Poisson, bulk
+                                   constraint and statistics */
+
+/* LES closures; the reference's LES_type values (src/CFD_2nd/m_Parameters.f90:256-259)
+   plus the closures added on top (no counterpart in the reference). */
+#define CH3D_LES_NONE 0
+#define CH3D_LES_WALE 2
+#define CH3D_LES_MTS 3
+#define CH3D_LES_SMAG_VD 10     /* Smagorinsky + van Driest damping */
+#define CH3D_LES_MLP 11         /* learned closure, Smagorinsky fallback */
+
+/* Configuration: the namelist variables of &BasicParam, &ubulk_Param and
+   &LesOptions (src/CFD_2nd/m_Parameters.f90:273-277,
+   src/CFD_2nd/m_TScheme.f90:47) that the time step reads, plus the
+   precision mode. */
+typedef struct ch3d_config {
+  int order;              /* 2: src/CFD_2nd, 4: src/CFD_4th */
+  int nxc, nyc, nzc;
+  double xlx, yly, zlz;
+  double xnu;
+  double dtMax;
+  int iCFL;               /* 1: dt from CFLc, 2: dt = dtMax */
+  double CFLc;
+  int ischeme;            /* 1 AB2, 2 RK2, 3 RK3 */
+  int IsImplicit;         /* 1 PIMP (y Crank-Nicolson), 2 FIMP (x,z,y ADI) */
+  int FlowType;           /* 1 channel, 2 half channel */
+  int BcOption[6];        /* x-,x+,y-,y+,z-,z+ : 0 periodic, -1 no-slip, -2 free-slip */
+  double uxBcValue[6], uyBcValue[6], uzBcValue[6];
+  double gravity[3];
+  int IsUxConst;
+  double ubulk, ybulk1, ybulk2;
+  int LES_type;
+  int FilterType;
+  double Cs;              /* Smagorinsky constant for CH3D_LES_SMAG_VD */
+  double vel_limit, div_limit;
+  int precision;          /* CH3D_PREC_* */
+  int device;             /* CUDA device ordinal */
+} ch3d_config;
+
+/* Per-step diagnostics: what ChannelIterate logs
+   (src/CFD_2nd/m_ChannelSystem.f90:138-153). */
+typedef struct ch3d_step_info {
+  double SimTime, dt, cflmp, divmax1, divmax2, vmax[3], uxm, PrGradAver;
+  int itime;
+  int status;             /* 0, or 1 div_limit / 2 vel_limit tripped */
+} ch3d_step_info;
+
+typedef struct ch3d_ctx ch3d_ctx;
+
+/* Version string of the library. */
+CH3D_API const char* ch3d_version(void);
+
+/* Message of the last failed call on this thread (never NULL). */
+CH3D_API const char* ch3d_last_error(void);
+
+/* y grid of one mesh section, as clcCoord computes it
+   (src/CFD_2nd/m_MeshAndMetries.f90:292-360): fills coordinate[id1..id2]
+   (1-based Fortran indices into yp). */
+CH3D_API int ch3d_mesh_section(double* yp, int id1, int id2, double c1, double c2,
+                      int StretType, double cStret, int StretOption);
+
+/* Whole y grid yp(1:nyp) from &MeshSection/&MeshOptions
+   (src/CFD_2nd/m_MeshAndMetries.f90:122-160). */
+CH3D_API int ch3d_mesh_y(int nyc, double yly, int nSection, const double* SectionLength,
+                const int* nycSection, const int* StretType,
+                const int* StretOption, const double* SectioncStret,
+                double* yp);
+
+/* Replaces InitMeshAndMetries + AllocateVariables + InitPoissonSolver +
+   InitTimeScheme (src/CFD_2nd/m_ChannelSystem.f90:39-45): builds the metric
+   vectors from yp(1:nyp) exactly as InitMeshAndMetries does
+   (src/CFD_2nd/m_MeshAndMetries.f90:171-286) and allocates the device state. */
+CH3D_API int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out);
+
+/* Frees the device state. */
+CH3D_API int ch3d_destroy(ch3d_ctx* ctx);
+
+/* Replaces read_restart + the ghost rebuild of ChannelInitialize
+   (src/CFD_2nd/m_ChannelSystem.f90:54-63).  hist (3 arrays, interior layout,
+   HistX|HistY|HistZ) may be NULL (zeros, as RK3 restarts use). */
+CH3D_API int ch3d_upload_state(ch3d_ctx* ctx, int layout, const double* ux,
+                      const double* uy, const double* uz, const double* p,
+                      const double* hist);
+
+/* Copies the state back to host arrays (write_restart's data). Any pointer may be NULL. */
+CH3D_API int ch3d_download_state(ch3d_ctx* ctx, int layout, double* ux, double* uy,
+                        double* uz, double* p, double* hist);
+
+/* Replaces `nsteps` calls of ChannelIterate (src/CFD_2nd/m_ChannelSystem.f90:73-154;
+   src/CFD_4th/m_ChannelSystem.f90:83-190) without statistics/IO.
+   Returns CH3D_ERR_DIVERGED if a limit tripped (info->itime tells when). */
+CH3D_API int ch3d_step(ch3d_ctx* ctx, int nsteps, ch3d_step_info* info);
+
+/* Stage-level entry points, one per procedure pointer of the reference's
+   substep (src/CFD_2nd/m_ChannelSystem.f90:91-124), for parity tests and for
+   hosts that keep their own loop:
+     0 PMcoeUpdate(ns) + Update_uy_ym   (m_Parameters.f90:329-342)
+     1 clcRhsX/Y/Z                      (m_TSchemePIMP_inc.f90:7-325)
+     2 clcU1Hat/U2Hat/U3Hat             (m_TSchemePIMP_inc.f90:392-740)
+     3 clcPrSrc                         (m_TScheme.f90:213-241)
+     4 clcPPE                           (m_Poisson.f90:1078-1201)
+     5 FluidVelUpdate                   (m_TScheme.f90:281-306)
+     6 PressureUpdate                   (m_TSchemePIMP_inc.f90:852-873)  */
+CH3D_API int ch3d_stage(ch3d_ctx* ctx, int stage, int ns);
+
+/* Internal arrays for inspection, interior layout: 0 ux, 1 uy, 2 uz,
+   3 pressure, 4 HistXOld, 5 HistYOld, 6 HistZOld, 7 RhsX, 8 RhsY,
+   9 prphi (the pressure correction of the last clcPPE), 11 RhsZ. */
+CH3D_API int ch3d_get_array(ch3d_ctx* ctx, int which, double* host);
+CH3D_API int ch3d_set_array(ch3d_ctx* ctx, int which, const double* host);
+
+/* Standalone pressure Poisson solve of clcPPE (src/CFD_2nd/m_Poisson.f90:1078-1201),
+   src and phi in the interior layout. */
+CH3D_API int ch3d_poisson(ch3d_ctx* ctx, const double* src, double* phi);
+
+/* Projects the current velocity onto the discrete divergence-free space
+   (Poisson solve of div(u) + FluidVelUpdate with pmAlpha = 1). */
+CH3D_API int ch3d_project(ch3d_ctx* ctx, double* divmax_before, double* divmax_after);
+
+/* Sets dt (iCFL = 2 runs only use dtMax). */
+CH3D_API int ch3d_set_dt(ch3d_ctx* ctx, double dt);
+
+/* Statistics: clcStat_CH moment sums (src/CFD_2nd/m_FlowType_Channel.f90:175-330),
+   accumulated on the device in FP64; fetch returns SumStat(35,nyp) in
+   Fortran order, nfstime and PrGradsum, and optionally resets them. */
+CH3D_API int ch3d_stats_accumulate(ch3d_ctx* ctx);
+CH3D_API int ch3d_stats_fetch(ch3d_ctx* ctx, double* sumstat, int* nfstime,
+                     double* prgradsum, int reset);
+
+/* Device bytes held by the context. */
+CH3D_API int ch3d_memory_bytes(ch3d_ctx* ctx, long long* bytes);
+
+/* Runs `nsteps` steps launching kernel groups one by one, with CUDA events
+   between them on the context's stream, and returns the mean time per launch
+   (ms) of each group in out[0..6]: 0 RHS stencils, 1 y Helmholtz solves,
+   2 divergence + forward x FFT, 3 z FFT + y Poisson solve + inverse z FFT,
+   4 inverse x FFT, 5 projection + pressure update, 6 scalar/reduction kernels.
+   The steps advance the state like ch3d_step. */
+CH3D_API int ch3d_kernel_times(ch3d_ctx* ctx, int nsteps, double* out, int nout);
+
+/* Time of the last ch3d_step call's kernels, measured with CUDA events on the
+   context's stream (milliseconds). */
+CH3D_API int ch3d_last_step_ms(ch3d_ctx* ctx, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CH3D_H_ */

@@ -1,0 +1,1189 @@
+// ch3d_oracle.cpp -- CPU oracle for the Channel3d RK3 channel-flow step.
+//
+// TEST INFRASTRUCTURE ONLY.  This file restates, in plain C++ (FP64,
+// -ffp-contract=off), the reference's Fortran algorithm for the time step of
+// the channel solvers.  Only tests/, the smoke check and the CPU-baseline leg
+// of bench.py load it, and only as a checker or as the timed CPU baseline;
+// the product library never links or calls it.
+//
+// Parity status: UNPINNED against reference runs.  The reference is Fortran
+// 2003 + MPI and no Fortran compiler exists on any machine of this build, and
+// the reference ships no tests, golden vectors or fixtures.  The restatement
+// is pinned instead by known-answer tests (naive DFT, discrete-Laplacian
+// residual of the Poisson solve, Taylor-Green and Poiseuille states,
+// divergence after projection) that live in tests/.
+//
+// Every routine cites the reference routine it follows (paths relative to the
+// reference project).  Array conventions follow the reference: Fortran order
+// (i fastest), ghosted arrays with the bounds of `myallocate`
+// (src/CFD_2nd/m_Decomp2d.f90:1517-1583) for a single rank (y1start=1,
+// y1end=n).  Only periodic x and z are supported (the channel configuration);
+// y may be no-slip or free-slip.
+//
+// The FFT that the reference takes from FFTW 3.3.9 (r2r kinds R2HC/HC2R,
+// src/CFD_2nd/m_Poisson.f90:267-307) is restated from its definition
+// (unnormalised DFT, halfcomplex storage r0..r_{n/2}, i_{(n+1)/2-1}..i_1).
+
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+typedef std::complex<double> cplx;
+
+// ---------------------------------------------------------------------------
+// Field with arbitrary Fortran lower/upper bounds (column-major).
+// ---------------------------------------------------------------------------
+struct F3 {
+  int xl = 0, yl = 0, zl = 0, sx = 0, sy = 0, sz = 0;
+  std::vector<double> a;
+  void init(int xl_, int xh, int yl_, int yh, int zl_, int zh) {
+    xl = xl_; yl = yl_; zl = zl_;
+    sx = xh - xl_ + 1; sy = yh - yl_ + 1; sz = zh - zl_ + 1;
+    a.assign((size_t)sx * sy * sz, 0.0);
+  }
+  inline double& operator()(int i, int j, int k) {
+    return a[(size_t)(i - xl) + (size_t)sx * ((size_t)(j - yl) + (size_t)sy * (size_t)(k - zl))];
+  }
+  inline double operator()(int i, int j, int k) const {
+    return a[(size_t)(i - xl) + (size_t)sx * ((size_t)(j - yl) + (size_t)sy * (size_t)(k - zl))];
+  }
+};
+
+// 1-D array addressed with Fortran indices lo..hi.
+struct V1 {
+  int lo = 0;
+  std::vector<double> a;
+  void init(int lo_, int hi) { lo = lo_; a.assign((size_t)(hi - lo_ + 1), 0.0); }
+  inline double& operator()(int j) { return a[(size_t)(j - lo)]; }
+  inline double operator()(int j) const { return a[(size_t)(j - lo)]; }
+};
+
+const double zero = 0.0, quarter = 0.25, half = 0.5, one = 1.0, two = 2.0,
+             three = 3.0, four = 4.0;
+const double PI = 3.141592653589793238462643383279502884;
+
+// ---------------------------------------------------------------------------
+// FFT: unnormalised complex DFT by recursive mixed-radix decimation in time,
+// with twiddles from an exact table.  Used to restate FFTW's R2HC/HC2R.
+// ---------------------------------------------------------------------------
+struct FFTPlan {
+  int n = 0;
+  std::vector<cplx> w;  // w[q] = exp(-2 pi i q / n)
+  std::vector<int> factors;
+  void init(int n_) {
+    n = n_;
+    w.resize(n);
+    for (int q = 0; q < n; ++q) {
+      long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)q / (long double)n;
+      w[q] = cplx((double)cosl(ang), (double)sinl(ang));
+    }
+    factors.clear();
+    int m = n;
+    const int pref[] = {4, 2, 3, 5};
+    for (int f : pref) while (m % f == 0) { factors.push_back(f); m /= f; }
+    for (int f = 7; m > 1; f += 2) while (m % f == 0) { factors.push_back(f); m /= f; }
+  }
+  // out[k] = sum_j in[j*stride] * exp(sign * 2 pi i j k / len); len = n / step
+  void rec(const cplx* in, cplx* out, int len, int stride, int step, size_t fi, bool inv) const {
+    if (len == 1) { out[0] = in[0]; return; }
+    int p = factors[fi];
+    int m = len / p;
+    for (int r = 0; r < p; ++r) rec(in + (size_t)r * stride, out + (size_t)r * m, m, stride * p, step * p, fi + 1, inv);
+    cplx tmpa[16], resa[16];
+    std::vector<cplx> tmpv, resv;
+    cplx* tmp = tmpa; cplx* res = resa;
+    if (p > 16) { tmpv.resize(p); resv.resize(p); tmp = tmpv.data(); res = resv.data(); }
+    for (int k = 0; k < m; ++k) {
+      for (int r = 0; r < p; ++r) {
+        int q = (int)(((long long)r * k * step) % n);
+        cplx tw = inv ? std::conj(w[q]) : w[q];
+        tmp[r] = out[(size_t)r * m + k] * tw;
+      }
+      for (int s = 0; s < p; ++s) {
+        cplx acc = 0.0;
+        for (int r = 0; r < p; ++r) {
+          int q = (int)(((long long)r * s * m * step) % n);
+          acc += tmp[r] * (inv ? std::conj(w[q]) : w[q]);
+        }
+        res[s] = acc;
+      }
+      for (int s = 0; s < p; ++s) out[(size_t)s * m + k] = res[s];
+    }
+  }
+  void exec(const cplx* in, cplx* out, bool inv) const { rec(in, out, n, 1, 1, 0, inv); }
+};
+
+// FFTW_R2HC on a contiguous line (in place).  Halfcomplex output layout:
+// hc[k] = Re X_k (k = 0..n/2), hc[n-k] = Im X_k (k = 1..(n+1)/2-1).
+void r2hc(const FFTPlan& pl, double* x, std::vector<cplx>& bufa, std::vector<cplx>& bufb) {
+  int n = pl.n;
+  bufa.resize(n); bufb.resize(n);
+  for (int j = 0; j < n; ++j) bufa[j] = cplx(x[j], 0.0);
+  pl.exec(bufa.data(), bufb.data(), false);
+  for (int k = 0; k <= n / 2; ++k) x[k] = bufb[k].real();
+  for (int k = 1; k < (n + 1) / 2; ++k) x[n - k] = bufb[k].imag();
+}
+
+// FFTW_HC2R on a contiguous line (in place), unnormalised:
+// x_j = sum_{k=0}^{n-1} X_k exp(+2 pi i j k / n) with Hermitian X.
+void hc2r(const FFTPlan& pl, double* x, std::vector<cplx>& bufa, std::vector<cplx>& bufb) {
+  int n = pl.n;
+  bufa.resize(n); bufb.resize(n);
+  bufa[0] = cplx(x[0], 0.0);
+  for (int k = 1; k < (n + 1) / 2; ++k) {
+    bufa[k] = cplx(x[k], x[n - k]);
+    bufa[n - k] = std::conj(bufa[k]);
+  }
+  if (n % 2 == 0) bufa[n / 2] = cplx(x[n / 2], 0.0);
+  pl.exec(bufa.data(), bufb.data(), true);
+  for (int j = 0; j < n; ++j) x[j] = bufb[j].real();
+}
+
+}  // namespace
+
+// ===========================================================================
+// Public C interface
+// ===========================================================================
+extern "C" {
+
+typedef struct orc_params {
+  int order;          // 2 = src/CFD_2nd, 4 = src/CFD_4th
+  int nxc, nyc, nzc;
+  double xlx, yly, zlz;
+  double xnu;
+  double dtMax;
+  int iCFL;
+  double CFLc;
+  int ischeme;        // 1 AB2, 2 RK2, 3 RK3
+  int IsImplicit;     // 0 FEXP, 1 PIMP, 2 FIMP
+  int FlowType;       // 1 channel, 2 half channel
+  int BcOption[6];
+  double uxBcValue[6], uyBcValue[6], uzBcValue[6];
+  double gravity[3];
+  int IsUxConst;
+  double ubulk, ybulk1, ybulk2;
+  int LES_type;       // 0 none, 2 WALE, 3 MTS, 10 Smagorinsky + van Driest
+  int FilterType;
+  double Cs;          // Smagorinsky constant (LES_type 10)
+  double vel_limit, div_limit;
+  // mesh sections (&MeshSection / &MeshOptions), at most 8
+  int nSection;
+  double SectionLength[8];
+  double SectioncStret[8];
+  int nycSection[8];
+  int StretType[8];
+  int StretOption[8];
+} orc_params;
+
+typedef struct orc_info {
+  double SimTime, dt, cflmp, divmax1, divmax2, vmax[3], uxm, PrGradAver;
+  int itime;
+  int status;         // 0 ok, 1 divergence limit, 2 velocity limit
+} orc_info;
+
+}  // extern "C"
+
+namespace {
+
+struct Oracle {
+  orc_params P;
+  int nxc, nyc, nzc, nxp, nyp, nzp;
+  int iadvance = 3;
+  double pmGammaConst[3], pmThetaConst[3], pmAlphaConst[3];
+  double pmGamma = 0, pmTheta = 0, pmAlpha = 0, pmBeta = 0, pmAlphaC = 0, pmBetaT = 0;
+  double dt = 0, SimTime = 0, PrGradAver = 0, PrGradNow = 0;
+  int itime = 0;
+  double ybulk1 = 0, ybulk2 = 0;
+
+  // metrics (m_MeshAndMetries)
+  double dx, dy, dz, dx2, dy2, dz2, rdx, rdy, rdz, rdx2, rdy2, rdz2;
+  V1 yp, yc, dyp, dyc, rdyp, rdyc, YinterpCoe, VolCell, DeltaCell;
+  V1 ap2Pr, ac2Pr, am2Pr, am1c, ac1c, ap1c, am2c, ac2c, ap2c, am2p, ac2p, ap2p, am3c, ac3c, ap3c;
+  V1 am2cForCN, ap2cForCN, am1cForCN, ap1cForCN, am3cForCN, ap3cForCN;
+
+  // Poisson
+  V1 WaveNumX, WaveNumZ;
+  double normfft = 1.0;
+  FFTPlan planx, planz;
+
+  // state (m_Variables)
+  F3 ux, uy, uz, pressure, RealHalo, nut;
+  F3 HistX, HistY, HistZ, RealArr1, RealArr2;  // interior (1:nxc,1:nyc,1:nzc)
+  std::vector<double> uy_ym, duy_ym;           // (nxc,nzc)
+
+  // statistics (m_FlowType_Channel)
+  std::vector<double> SumStat;  // (35, nyp)
+  int nfstime = 0;
+  double PrGradsum = 0;
+
+  double divmax1_last = 0;
+
+  int nthreads() const {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+  }
+
+  // ---- src/CFD_2nd/m_MeshAndMetries.f90:292-360 (clcCoord) ----
+  void clcCoord(int id1, int id2, double c1, double c2, int StretType, double cStret, int StretOption) {
+    int m = id2 - id1;
+    double secLen = c2 - c1;
+    yp(id1) = c1; yp(id2) = c2;
+    switch (StretType) {
+      case 0:
+        for (int j = 0; j <= m; ++j) yp(id1 + j) = c1 + (double)j / (double)m * secLen;
+        break;
+      case 1: {
+        double tstr = std::tanh(cStret);
+        for (int j = 0; j <= m; ++j) {
+          double xi = (double)j / (double)(float)m;
+          double setCrd = std::tanh(cStret * (xi - one)) / tstr + one;
+          if (StretOption == 0) yp(id1 + j) = c1 + setCrd * secLen;
+          else yp(id2 - j) = c2 - setCrd * secLen;
+        }
+        break;
+      }
+      case 2: {
+        double tstr = std::sin(half * cStret * PI);
+        for (int j = 0; j <= m; ++j) {
+          double xi = (double)j / (double)m - one;
+          double setCrd = std::sin(cStret * xi * PI * half) / tstr + one;
+          if (StretOption == 0) yp(id1 + j) = c1 + setCrd * secLen;
+          else yp(id2 - j) = c2 - setCrd * secLen;
+        }
+        break;
+      }
+      case 3: {
+        if (cStret == one) {
+          for (int j = 0; j <= m; ++j) yp(j + id1) = c1 + (double)j / (double)m * secLen;
+        } else {
+          double tstr = (std::pow(cStret, m) - one) / (cStret - one);
+          for (int j = 0; j <= m - 1; ++j) {
+            double setCrd = std::pow(cStret, j) / tstr;
+            if (StretOption == 0) yp(id1 + j + 1) = yp(id1 + j) + setCrd * secLen;
+            else yp(id2 - j - 1) = yp(id2 - j) - setCrd * secLen;
+          }
+        }
+        break;
+      }
+    }
+    yp(id1) = c1; yp(id2) = c2;
+  }
+
+  // ---- src/CFD_2nd/m_MeshAndMetries.f90:64-287 (InitMeshAndMetries) ----
+  void InitMeshAndMetries() {
+    dx = P.xlx / (double)nxc; dy = P.yly / (double)nyc; dz = P.zlz / (double)nzc;
+    rdx = (double)nxc / P.xlx; rdy = (double)nyc / P.yly; rdz = (double)nzc / P.zlz;
+    dx2 = dx * dx; rdx2 = rdx * rdx; dy2 = dy * dy; rdy2 = rdy * rdy; dz2 = dz * dz; rdz2 = rdz * rdz;
+    yp.init(0, nyp); yc.init(0, nyp); dyp.init(0, nyp); rdyp.init(0, nyp); dyc.init(0, nyp); rdyc.init(0, nyp);
+    ap2Pr.init(1, nyc); ac2Pr.init(1, nyc); am2Pr.init(1, nyc);
+    ap1c.init(1, nxc); ac1c.init(1, nxc); am1c.init(1, nxc);
+    ap2c.init(1, nyc); ac2c.init(1, nyc); am2c.init(1, nyc);
+    ap2p.init(1, nyc); ac2p.init(1, nyc); am2p.init(1, nyc);
+    ap3c.init(1, nzc); ac3c.init(1, nzc); am3c.init(1, nzc);
+    VolCell.init(0, nyp); DeltaCell.init(0, nyp); YinterpCoe.init(1, nyp);
+
+    int ns = P.nSection;
+    std::vector<int> nid(ns + 1, 1);
+    std::vector<double> ysc(ns + 1, 0.0);
+    double SumLength = 0;
+    for (int j = 0; j < ns; ++j) SumLength += P.SectionLength[j];
+    for (int j = 0; j < ns; ++j) {
+      nid[j + 1] = nid[j] + P.nycSection[j];
+      ysc[j + 1] = ysc[j] + P.SectionLength[j] / SumLength * P.yly;
+    }
+    ysc[ns] = P.yly;
+    for (int j = 0; j < ns; ++j)
+      clcCoord(nid[j], nid[j + 1], ysc[j], ysc[j + 1], P.StretType[j], P.SectioncStret[j], P.StretOption[j]);
+
+    for (int j = 1; j <= nyc; ++j) yc(j) = half * (yp(j) + yp(j + 1));
+    yc(0) = two * yp(1) - yc(1);
+    yc(nyp) = two * yp(nyp) - yc(nyc);
+    for (int j = 1; j <= nyc; ++j) dyp(j) = yp(j + 1) - yp(j);
+    dyp(0) = dyp(1); dyp(nyp) = dyp(nyc);
+    for (int j = 0; j <= nyp; ++j) VolCell(j) = dyp(j) * dx * dz;
+    for (int j = 0; j <= nyp; ++j) DeltaCell(j) = std::pow(dyp(j) * dx * dz, one / three);
+    for (int j = 2; j <= nyc; ++j) dyc(j) = yc(j) - yc(j - 1);
+    dyc(1) = dyp(1); dyc(nyp) = dyp(nyc);
+    for (int j = 0; j <= nyp; ++j) rdyp(j) = one / dyp(j);
+    for (int j = 1; j <= nyp; ++j) rdyc(j) = one / dyc(j);
+    for (int j = 1; j <= nyp; ++j) YinterpCoe(j) = dyp(j) / (dyp(j) + dyp(j - 1));
+
+    const int* Bc = P.BcOption;
+    for (int j = 1; j <= nyc; ++j) { am2Pr(j) = rdyp(j) * rdyc(j); ap2Pr(j) = rdyp(j) * rdyc(j + 1); }
+    if (Bc[2] != 0) { am2Pr(1) = zero; ap2Pr(1) = rdyp(1) * rdyc(2); }
+    if (Bc[3] != 0) { am2Pr(nyc) = rdyp(nyc) * rdyc(nyc); ap2Pr(nyc) = zero; }
+    for (int j = 1; j <= nyc; ++j) ac2Pr(j) = -(am2Pr(j) + ap2Pr(j));
+
+    for (int i = 1; i <= nxc; ++i) { am1c(i) = rdx2; ap1c(i) = rdx2; }
+    if (Bc[0] == -1) { am1c(1) = four / three * rdx2; ap1c(1) = four / three * rdx2; }
+    if (Bc[1] == -1) { am1c(nxc) = four / three * rdx2; ap1c(nxc) = four / three * rdx2; }
+    for (int i = 1; i <= nxc; ++i) ac1c(i) = -(am1c(i) + ap1c(i));
+
+    for (int j = 1; j <= nyc; ++j) { am2c(j) = rdyp(j) * rdyc(j); ap2c(j) = rdyp(j) * rdyc(j + 1); }
+    if (Bc[2] == -1) {
+      am2c(1) = four * rdyc(1) / (dyc(1) + two * dyc(2));
+      ap2c(1) = four * rdyc(2) / (dyc(1) + two * dyc(2));
+    }
+    if (Bc[3] == -1) {
+      am2c(nyc) = four * rdyc(nyc) / (dyc(nyp) + two * dyc(nyc));
+      ap2c(nyc) = four * rdyc(nyp) / (dyc(nyp) + two * dyc(nyc));
+    }
+    for (int j = 1; j <= nyc; ++j) ac2c(j) = -(am2c(j) + ap2c(j));
+
+    for (int k = 1; k <= nzc; ++k) { am3c(k) = rdz2; ap3c(k) = rdz2; }
+    if (Bc[4] == -1) { am3c(1) = four / three * rdz2; ap3c(1) = four / three * rdz2; }
+    if (Bc[5] == -1) { am3c(nzc) = four / three * rdz2; ap3c(nzc) = four / three * rdz2; }
+    for (int k = 1; k <= nzc; ++k) ac3c(k) = -(am3c(k) + ap3c(k));
+
+    for (int j = 1; j <= nyc; ++j) { am2p(j) = rdyc(j) * rdyp(j - 1); ap2p(j) = rdyc(j) * rdyp(j); }
+    for (int j = 1; j <= nyc; ++j) ac2p(j) = -(am2p(j) + ap2p(j));
+  }
+
+  // ---- src/CFD_2nd/m_TScheme.f90:40-100 (CN metrics of InitTimeScheme) ----
+  void InitTimeScheme() {
+    ybulk1 = P.ybulk1; ybulk2 = P.ybulk2;
+    const int* Bc = P.BcOption;
+    am1cForCN.init(1, nxc); ap1cForCN.init(1, nxc);
+    for (int i = 1; i <= nxc; ++i) { ap1cForCN(i) = ap1c(i); am1cForCN(i) = am1c(i); }
+    if (Bc[0] == -1) am1cForCN(1) = two * am1c(1); else if (Bc[0] == -2) am1cForCN(1) = zero;
+    if (Bc[1] == -1) ap1cForCN(nxc) = two * ap1c(nxc); else if (Bc[1] == -2) ap1cForCN(nxc) = zero;
+    am2cForCN.init(1, nyc); ap2cForCN.init(1, nyc);
+    for (int j = 1; j <= nyc; ++j) { ap2cForCN(j) = ap2c(j); am2cForCN(j) = am2c(j); }
+    if (Bc[2] == -1) am2cForCN(1) = two * am2c(1); else if (Bc[2] == -2) am2cForCN(1) = zero;
+    if (Bc[3] == -1) ap2cForCN(nyc) = two * ap2c(nyc); else if (Bc[3] == -2) ap2cForCN(nyc) = zero;
+    am3cForCN.init(1, nzc); ap3cForCN.init(1, nzc);
+    for (int k = 1; k <= nzc; ++k) { ap3cForCN(k) = ap3c(k); am3cForCN(k) = am3c(k); }
+    if (Bc[4] == -1) am3cForCN(1) = two * am3c(1); else if (Bc[4] == -2) am3cForCN(1) = zero;
+    if (Bc[5] == -1) ap3cForCN(nzc) = two * ap3c(nzc); else if (Bc[5] == -2) ap3cForCN(nzc) = zero;
+  }
+
+  // ---- src/CFD_2nd/m_Poisson.f90:28-66 (modified wavenumbers, normfft) ----
+  void InitPoissonSolver() {
+    WaveNumX.init(1, nxc); WaveNumZ.init(1, nzc);
+    normfft = one;
+    for (int i = 1; i <= nxc; ++i) {
+      double wa1 = 2.0 * PI * (double)(i - 1) / (double)nxc;
+      WaveNumX(i) = two * rdx2 * (std::cos(wa1) - one);
+    }
+    normfft = normfft * one * (double)nxc;
+    for (int k = 1; k <= nzc; ++k) {
+      double wa3 = 2.0 * PI * (double)(k - 1) / (double)nzc;
+      WaveNumZ(k) = two * rdz2 * (std::cos(wa3) - one);
+    }
+    normfft = normfft * one * (double)nzc;
+    normfft = one / normfft;
+    planx.init(nxc);
+    planz.init(nzc);
+  }
+
+  void init(const orc_params* p) {
+    P = *p;
+    nxc = P.nxc; nyc = P.nyc; nzc = P.nzc; nxp = nxc + 1; nyp = nyc + 1; nzp = nzc + 1;
+    // src/CFD_2nd/m_Parameters.f90:288-306
+    if (P.ischeme == 1) {
+      iadvance = 1;
+      pmGammaConst[0] = 1.5; pmGammaConst[1] = 0; pmGammaConst[2] = 0;
+      pmThetaConst[0] = -0.5; pmThetaConst[1] = 0; pmThetaConst[2] = 0;
+    } else if (P.ischeme == 2) {
+      iadvance = 2;
+      pmGammaConst[0] = 0.5; pmGammaConst[1] = 1.0; pmGammaConst[2] = 0;
+      pmThetaConst[0] = 0; pmThetaConst[1] = -0.5; pmThetaConst[2] = 0;
+    } else {
+      iadvance = 3;
+      pmGammaConst[0] = 8.0 / 15.0; pmGammaConst[1] = 5.0 / 12.0; pmGammaConst[2] = 3.0 / 4.0;
+      pmThetaConst[0] = 0.0; pmThetaConst[1] = -17.0 / 60.0; pmThetaConst[2] = -5.0 / 12.0;
+    }
+    for (int s = 0; s < 3; ++s) pmAlphaConst[s] = pmGammaConst[s] + pmThetaConst[s];
+    InitMeshAndMetries();
+    InitTimeScheme();
+    InitPoissonSolver();
+    // src/CFD_2nd/m_Variables.f90:59-61 (ghosts xme=1,xpe=2,...)
+    ux.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
+    uy.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
+    uz.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
+    pressure.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
+    RealHalo.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
+    nut.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
+    HistX.init(1, nxc, 1, nyc, 1, nzc); HistY.init(1, nxc, 1, nyc, 1, nzc); HistZ.init(1, nxc, 1, nyc, 1, nzc);
+    RealArr1.init(1, nxc, 1, nyc, 1, nzc); RealArr2.init(1, nxc, 1, nyc, 1, nzc);
+    uy_ym.assign((size_t)nxc * nzc, 0.0); duy_ym.assign((size_t)nxc * nzc, 0.0);
+    SumStat.assign((size_t)35 * nyp, 0.0);
+    dt = P.dtMax; SimTime = 0;
+  }
+
+  // ---- src/CFD_2nd/m_Parameters.f90:329-342 (PMcoeUpdate) ----
+  void PMcoeUpdate(int ns) {
+    pmGamma = pmGammaConst[ns - 1] * dt;
+    pmTheta = pmThetaConst[ns - 1] * dt;
+    pmAlpha = pmAlphaConst[ns - 1] * dt;
+    pmBeta = half * pmAlphaConst[ns - 1] * P.xnu * dt;
+    SimTime = SimTime + dt * pmAlphaConst[ns - 1];
+    pmAlphaC = pmAlphaConst[ns - 1];
+    pmBetaT = half * pmAlphaConst[ns - 1] * dt;
+    if (ns == 1) PrGradAver = zero;
+  }
+
+  // ---- src/CFD_2nd/m_FlowType_Channel.f90:157-168 (Update_uy_ym_CH) ----
+  void Update_uy_ym() {
+    for (size_t q = 0; q < uy_ym.size(); ++q) {
+      double old = uy_ym[q];
+      uy_ym[q] = P.uyBcValue[2];
+      duy_ym[q] = uy_ym[q] - old;
+    }
+  }
+
+  // ---- src/CFD_2nd/m_Decomp2d.f90:1588-1743 (myupdate_halo, y-pencil, one rank,
+  //      periodic x and z: self copies over the full extent of the other dims) ----
+  void halo(F3& m, int xmh, int xph, int ymh, int yph, int zmh, int zph) {
+    int xmm = m.xl, xpm = m.xl + m.sx - 1, ymm = m.yl, ypm = m.yl + m.sy - 1, zmm = m.zl, zpm = m.zl + m.sz - 1;
+    // step1/2: y (only when y periodic)
+    if (ymh > 0)
+      for (int k = 1; k <= nzc; ++k) for (int h = 1; h <= ymh; ++h) for (int i = 1; i <= nxc; ++i)
+        m(i, 1 - h, k) = m(i, nyc - h + 1, k);
+    if (yph > 0)
+      for (int k = 1; k <= nzc; ++k) for (int h = 1; h <= yph; ++h) for (int i = 1; i <= nxc; ++i)
+        m(i, nyc + h, k) = m(i, h, k);
+    // step3: receive from xm (i = 1-xmh..0  <- nxc-xmh+1..nxc)
+    if (xmh > 0)
+      for (int k = zmm; k <= zpm; ++k) for (int j = ymm; j <= ypm; ++j) for (int h = 1; h <= xmh; ++h)
+        m(1 - h, j, k) = m(nxc - h + 1, j, k);
+    if (xph > 0)
+      for (int k = zmm; k <= zpm; ++k) for (int j = ymm; j <= ypm; ++j) for (int h = 1; h <= xph; ++h)
+        m(nxc + h, j, k) = m(h, j, k);
+    if (zmh > 0)
+      for (int h = 1; h <= zmh; ++h) for (int j = ymm; j <= ypm; ++j) for (int i = xmm; i <= xpm; ++i)
+        m(i, j, 1 - h) = m(i, j, nzc - h + 1);
+    if (zph > 0)
+      for (int h = 1; h <= zph; ++h) for (int j = ymm; j <= ypm; ++j) for (int i = xmm; i <= xpm; ++i)
+        m(i, j, nzc + h) = m(i, j, h);
+  }
+  bool yper() const { return P.BcOption[2] == 0; }
+
+  // ---- src/CFD_2nd/m_BC_and_Halo.f90:232-344 (SetBC_and_UpdateHalo), x/z periodic ----
+  void SetBC_and_UpdateHalo() {
+    const int* Bc = P.BcOption;
+    if (Bc[3] == -1) {
+      for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+        ux(i, nyp, k) = P.uxBcValue[3] * two - ux(i, nyc, k);
+        uy(i, nyp, k) = P.uyBcValue[3];
+        uy(i, nyp + 1, k) = P.uyBcValue[3] * two - uy(i, nyc, k);
+        uz(i, nyp, k) = P.uzBcValue[3] * two - uz(i, nyc, k);
+      }
+    } else if (Bc[3] == -2) {
+      for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+        ux(i, nyp, k) = P.uxBcValue[3] * dyp(nyp) + ux(i, nyc, k);
+        uy(i, nyp, k) = P.uyBcValue[3];
+        uy(i, nyp + 1, k) = P.uyBcValue[3] * two - uy(i, nyc, k);
+        uz(i, nyp, k) = P.uzBcValue[3] * dyp(nyp) + uz(i, nyc, k);
+      }
+    }
+    if (Bc[2] == -1) {
+      for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+        double w = uy_ym[(size_t)(i - 1) + (size_t)nxc * (k - 1)];
+        ux(i, 0, k) = P.uxBcValue[2] * two - ux(i, 1, k);
+        uy(i, 1, k) = w;
+        uy(i, 0, k) = w * two - uy(i, 2, k);
+        uz(i, 0, k) = P.uzBcValue[2] * two - uz(i, 1, k);
+      }
+    } else if (Bc[2] == -2) {
+      for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+        double w = uy_ym[(size_t)(i - 1) + (size_t)nxc * (k - 1)];
+        ux(i, 0, k) = ux(i, 1, k) - P.uxBcValue[2] * dyp(1);
+        uy(i, 1, k) = w;
+        uy(i, 0, k) = w * two - uy(i, 2, k);
+        uz(i, 0, k) = uz(i, 1, k) - P.uzBcValue[2] * dyp(1);
+      }
+    }
+    int yh = yper() ? 1 : 0;
+    halo(ux, 1, 1, yh, yh, 1, 1);
+    halo(uy, 1, 1, yh, yh, 1, 1);
+    halo(uz, 1, 1, yh, yh, 1, 1);
+  }
+
+  // ---- src/CFD_2nd/m_BC_and_Halo.f90:349-405 (SetBC_and_UpdateHaloForPrSrc) ----
+  void SetBC_and_UpdateHaloForPrSrc() {
+    const int* Bc = P.BcOption;
+    if (Bc[3] == -1 || Bc[3] == -2)
+      for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) uy(i, nyp, k) = P.uyBcValue[3];
+    if (Bc[2] == -1 || Bc[2] == -2)
+      for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i)
+        uy(i, 1, k) = uy_ym[(size_t)(i - 1) + (size_t)nxc * (k - 1)];
+    halo(ux, 0, 1, 0, 0, 0, 0);
+    halo(uy, 0, 0, 0, yper() ? 1 : 0, 0, 0);
+    halo(uz, 0, 0, 0, 0, 0, 1);
+  }
+
+  // ---- src/CFD_2nd/m_BC_and_Halo.f90:410-456 (SetBC_and_UpdateHalo_pr) ----
+  void SetBC_and_UpdateHalo_pr(F3& pr) {
+    const int* Bc = P.BcOption;
+    if (Bc[3] < 0) for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) pr(i, nyp, k) = pr(i, nyc, k);
+    if (Bc[2] < 0) for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) pr(i, 0, k) = pr(i, 1, k);
+    int yh = yper() ? 1 : 0;
+    halo(pr, 1, 1, yh, yh, 1, 1);
+  }
+
+  // ---- src/CFD_2nd/m_Tools.f90:21-46 (CalcMaxCFL) ----
+  double CalcMaxCFL() {
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      double m = 0;
+      for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) {
+        double vcf = std::fabs(ux(ic, jc, kc) + ux(ic + 1, jc, kc)) * rdx +
+                     std::fabs(uy(ic, jc, kc) + uy(ic, jc + 1, kc)) * rdyp(jc) +
+                     std::fabs(uz(ic, jc, kc) + uz(ic, jc, kc + 1)) * rdz;
+        if (vcf > m) m = vcf;
+      }
+      part[kc] = m;
+    }
+    double m = 0;
+    for (int kc = 1; kc <= nzc; ++kc) m = std::max(m, part[kc]);
+    return m * half;
+  }
+
+  // ---- src/CFD_2nd/m_Tools.f90:51-75 (CheckDivergence) ----
+  double CheckDivergence() {
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      double m = 0;
+      for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) {
+        double udiv = std::fabs((ux(ic + 1, jc, kc) - ux(ic, jc, kc)) * rdx + (uy(ic, jc + 1, kc) - uy(ic, jc, kc)) * rdyp(jc) +
+                                (uz(ic, jc, kc + 1) - uz(ic, jc, kc)) * rdz);
+        if (udiv > m) m = udiv;
+      }
+      part[kc] = m;
+    }
+    double m = 0;
+    for (int kc = 1; kc <= nzc; ++kc) m = std::max(m, part[kc]);
+    return m;
+  }
+
+  // ---- src/CFD_2nd/m_Tools.f90:80-104 (CalcVmax) ----
+  void CalcVmax(double v[3]) {
+    v[0] = v[1] = v[2] = 0;
+    for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) {
+      v[0] = std::max(v[0], std::fabs(ux(ic, jc, kc)));
+      v[1] = std::max(v[1], std::fabs(uy(ic, jc, kc)));
+      v[2] = std::max(v[2], std::fabs(uz(ic, jc, kc)));
+    }
+  }
+
+  // ---- src/CFD_2nd/m_Tools.f90:250-270 (CalcUxAver) ----
+  double CalcUxAver() {
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      double s = 0;
+      for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) s += ux(ic, jc, kc) * dyp(jc);
+      part[kc] = s;
+    }
+    double s = 0;
+    for (int kc = 1; kc <= nzc; ++kc) s += part[kc];
+    return s / ((double)nxc * (double)nzc) / P.yly;
+  }
+
+  // ---- src/CFD_2nd/m_Tools.f90:218-245 (InverseTridiagonal), one system ----
+  static void InverseTridiagonal1(const double* aj, const double* bj, const double* cj, double* fj, int n, double* arr) {
+    double vecm = bj[0];
+    fj[0] = fj[0] / vecm;
+    for (int j = 1; j < n; ++j) {
+      arr[j] = cj[j - 1] / vecm;
+      vecm = bj[j] - aj[j] * arr[j];
+      fj[j] = (fj[j] - aj[j] * fj[j - 1]) / vecm;
+    }
+    for (int j = n - 2; j >= 0; --j) fj[j] = fj[j] - arr[j + 1] * fj[j + 1];
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75 (clcRhsX_PIMP) ----
+  void clcRhsX_PIMP(F3& RhsX, F3& Hist) {
+    double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+    std::vector<double> part(nzc + 1, 0.0);
+    const double g1 = P.gravity[0], xnu = P.xnu;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1;
+      double s1tot = 0;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double s1totCoe = dyp(jc);
+        double sucaj = half * rdyp(jc);
+        if (yc(jc) < ybulk1 || yc(jc) >= ybulk2) s1totCoe = zero;
+        double InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+        double InterpY3 = YinterpCoe(jp), InterpY4 = one - InterpY3;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double h11 = ((ux(ip, jc, kc) + ux(ic, jc, kc)) * (ux(ip, jc, kc) + ux(ic, jc, kc)) -
+                        (ux(ic, jc, kc) + ux(im, jc, kc)) * (ux(ic, jc, kc) + ux(im, jc, kc))) * qdx1;
+          double h12 = ((uy(ic, jp, kc) + uy(im, jp, kc)) * (InterpY3 * ux(ic, jc, kc) + InterpY4 * ux(ic, jp, kc)) -
+                        (uy(ic, jc, kc) + uy(im, jc, kc)) * (InterpY1 * ux(ic, jm, kc) + InterpY2 * ux(ic, jc, kc))) * sucaj;
+          double h13 = ((uz(ic, jc, kp) + uz(im, jc, kp)) * (ux(ic, jc, kp) + ux(ic, jc, kc)) -
+                        (uz(ic, jc, kc) + uz(im, jc, kc)) * (ux(ic, jc, kc) + ux(ic, jc, km))) * qdx3;
+          double d11q1 = (ux(ip, jc, kc) - two * ux(ic, jc, kc) + ux(im, jc, kc)) * rdx2;
+          double d22q1 = ap2c(jc) * ux(ic, jp, kc) + ac2c(jc) * ux(ic, jc, kc) + am2c(jc) * ux(ic, jm, kc);
+          double d33q1 = ap3c(kc) * ux(ic, jc, kp) + ac3c(kc) * ux(ic, jc, kc) + am3c(kc) * ux(ic, jc, km);
+          double dcq13 = d11q1 + d33q1;
+          double gradp1 = (pressure(ic, jc, kc) - pressure(im, jc, kc)) * rdx;
+          s1tot = s1tot + ux(ic, jc, kc) * s1totCoe;
+          double convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g1;
+          RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1 + two * pmBeta * d22q1;
+          Hist(ic, jc, kc) = convEd1;
+        }
+      }
+      part[kc] = s1tot;
+    }
+    if (P.IsUxConst) {
+      double s1tot1 = 0;
+      for (int kc = 1; kc <= nzc; ++kc) s1tot1 += part[kc];
+      s1tot1 = s1tot1 / ((double)nxc * (double)nzc) / (ybulk2 - ybulk1);
+      double dpmdxns = pmAlphaC * (P.ubulk - s1tot1);
+#pragma omp parallel for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) RhsX(ic, jc, kc) = RhsX(ic, jc, kc) + dpmdxns;
+      PrGradNow = (P.ubulk - s1tot1) / dt;
+      PrGradAver = PrGradAver + pmAlphaC * PrGradNow;
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:161-209 (clcRhsY_PIMP) ----
+  void clcRhsY_PIMP(F3& RhsY, F3& Hist) {
+    double hdx1 = half * rdx, hdx3 = half * rdz;
+    const double g2 = P.gravity[1], xnu = P.xnu;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double sucac = rdyc(jc), qsucac = quarter * sucac;
+        double InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double h21 = ((InterpY1 * ux(ip, jm, kc) + InterpY2 * ux(ip, jc, kc)) * (uy(ip, jc, kc) + uy(ic, jc, kc)) -
+                        (InterpY1 * ux(ic, jm, kc) + InterpY2 * ux(ic, jc, kc)) * (uy(ic, jc, kc) + uy(im, jc, kc))) * hdx1;
+          double h22 = ((uy(ic, jp, kc) + uy(ic, jc, kc)) * (uy(ic, jp, kc) + uy(ic, jc, kc)) -
+                        (uy(ic, jc, kc) + uy(ic, jm, kc)) * (uy(ic, jc, kc) + uy(ic, jm, kc))) * qsucac;
+          double h23 = ((InterpY1 * uz(ic, jm, kp) + InterpY2 * uz(ic, jc, kp)) * (uy(ic, jc, kp) + uy(ic, jc, kc)) -
+                        (InterpY1 * uz(ic, jm, kc) + InterpY2 * uz(ic, jc, kc)) * (uy(ic, jc, kc) + uy(ic, jc, km))) * hdx3;
+          double d11q2 = ap1c(ic) * uy(ip, jc, kc) + ac1c(ic) * uy(ic, jc, kc) + am1c(ic) * uy(im, jc, kc);
+          double d22q2 = ap2p(jc) * uy(ic, jp, kc) + ac2p(jc) * uy(ic, jc, kc) + am2p(jc) * uy(ic, jm, kc);
+          double d33q2 = ap3c(kc) * uy(ic, jc, kp) + ac3c(kc) * uy(ic, jc, kc) + am3c(kc) * uy(ic, jc, km);
+          double dcq13 = d11q2 + d33q2;
+          double gradp2 = (pressure(ic, jc, kc) - pressure(ic, jm, kc)) * sucac;
+          double convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g2;
+          RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2 + two * pmBeta * d22q2;
+          Hist(ic, jc, kc) = convEd2;
+        }
+      }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:277-325 (clcRhsZ_PIMP); RhsZ is the
+  //      ghosted RealHalo in the reference, only its interior is written ----
+  void clcRhsZ_PIMP(F3& RhsZ, F3& Hist) {
+    double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+    const double g3 = P.gravity[2], xnu = P.xnu;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double sucaj = half * rdyp(jc);
+        double InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+        double InterpY3 = YinterpCoe(jp), InterpY4 = one - InterpY3;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double h31 = ((ux(ip, jc, kc) + ux(ip, jc, km)) * (uz(ip, jc, kc) + uz(ic, jc, kc)) -
+                        (ux(ic, jc, kc) + ux(ic, jc, km)) * (uz(ic, jc, kc) + uz(im, jc, kc))) * qdx1;
+          double h32 = ((uy(ic, jp, kc) + uy(ic, jp, km)) * (InterpY3 * uz(ic, jc, kc) + InterpY4 * uz(ic, jp, kc)) -
+                        (uy(ic, jc, kc) + uy(ic, jc, km)) * (InterpY1 * uz(ic, jm, kc) + InterpY2 * uz(ic, jc, kc))) * sucaj;
+          double h33 = ((uz(ic, jc, kp) + uz(ic, jc, kc)) * (uz(ic, jc, kp) + uz(ic, jc, kc)) -
+                        (uz(ic, jc, kc) + uz(ic, jc, km)) * (uz(ic, jc, kc) + uz(ic, jc, km))) * qdx3;
+          double d11q3 = ap1c(ic) * uz(ip, jc, kc) + ac1c(ic) * uz(ic, jc, kc) + am1c(ic) * uz(im, jc, kc);
+          double d22q3 = ap2c(jc) * uz(ic, jp, kc) + ac2c(jc) * uz(ic, jc, kc) + am2c(jc) * uz(ic, jm, kc);
+          double d33q3 = (uz(ic, jc, kp) - two * uz(ic, jc, kc) + uz(ic, jc, km)) * rdz2;
+          double dcq13 = d11q3 + d33q3;
+          double gradp3 = (pressure(ic, jc, kc) - pressure(ic, jc, km)) * rdz;
+          double convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g3;
+          RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3 + two * pmBeta * d22q3;
+          Hist(ic, jc, kc) = convEd3;
+        }
+      }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:392-430 (clcU1Hat_PIMP) and :702-740
+  //      (clcU3Hat_PIMP): (I - pmBeta*L_y) du = Rhs, u += du, per k-slab ----
+  void clcUHat_PIMP_c(F3& u, F3& Rhs) {
+    std::vector<double> tp(nyc), tm(nyc), tc(nyc);
+    for (int jc = 1; jc <= nyc; ++jc) {
+      tp[jc - 1] = -pmBeta * ap2cForCN(jc);
+      tm[jc - 1] = -pmBeta * am2cForCN(jc);
+      tc[jc - 1] = -tp[jc - 1] - tm[jc - 1] + one;
+    }
+#pragma omp parallel
+    {
+      std::vector<double> f(nyc), arr(nyc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int jc = 1; jc <= nyc; ++jc) f[jc - 1] = Rhs(ic, jc, kc);
+          InverseTridiagonal1(tm.data(), tc.data(), tp.data(), f.data(), nyc, arr.data());
+          for (int jc = 1; jc <= nyc; ++jc) u(ic, jc, kc) = u(ic, jc, kc) + f[jc - 1];
+        }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:542-589 (clcU2Hat_PIMP) ----
+  void clcU2Hat_PIMP(F3& Rhs) {
+    std::vector<double> tp(nyc), tm(nyc), tc(nyc);
+    tp[0] = zero; tc[0] = one; tm[0] = zero;
+    for (int jc = 2; jc <= nyc; ++jc) {
+      tp[jc - 1] = -pmBeta * ap2p(jc);
+      tc[jc - 1] = -pmBeta * ac2p(jc) + one;
+      tm[jc - 1] = -pmBeta * am2p(jc);
+    }
+#pragma omp parallel
+    {
+      std::vector<double> f(nyc), arr(nyc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          f[0] = duy_ym[(size_t)(ic - 1) + (size_t)nxc * (kc - 1)];
+          for (int jc = 2; jc <= nyc; ++jc) f[jc - 1] = Rhs(ic, jc, kc);
+          InverseTridiagonal1(tm.data(), tc.data(), tp.data(), f.data(), nyc, arr.data());
+          for (int jc = 1; jc <= nyc; ++jc) uy(ic, jc, kc) = uy(ic, jc, kc) + f[jc - 1];
+        }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TScheme.f90:213-241 (clcPrSrcOther) ----
+  double clcPrSrcOther(F3& prsrc) {
+    double sudtal = one / pmAlpha;
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int kp = kc + 1;
+      double m = 0;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jp = jc + 1;
+        double sucaj = rdyp(jc);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int ip = ic + 1;
+          double rdiv = (ux(ip, jc, kc) - ux(ic, jc, kc)) * rdx + (uy(ic, jp, kc) - uy(ic, jc, kc)) * sucaj +
+                        (uz(ic, jc, kp) - uz(ic, jc, kc)) * rdz;
+          m = std::max(std::fabs(rdiv), m);
+          prsrc(ic, jc, kc) = sudtal * rdiv;
+        }
+      }
+      part[kc] = m;
+    }
+    double m = 0;
+    for (int kc = 1; kc <= nzc; ++kc) m = std::max(m, part[kc]);
+    return m;
+  }
+
+  // ---- src/CFD_2nd/m_Poisson.f90:1078-1201 (clcPPE_z1: z R2HC, x R2HC, per-slot
+  //      y tridiagonal with the (1,1,1) pin, x HC2R, z HC2R, * normfft) ----
+  void clcPPE(F3& prsrc, F3& prphiHalo) {
+    // forward z transform of every (i,j) line
+#pragma omp parallel
+    {
+      std::vector<double> line(nzc);
+      std::vector<cplx> ba, bb;
+#pragma omp for schedule(static)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int kc = 1; kc <= nzc; ++kc) line[kc - 1] = prsrc(ic, jc, kc);
+          r2hc(planz, line.data(), ba, bb);
+          for (int kc = 1; kc <= nzc; ++kc) prsrc(ic, jc, kc) = line[kc - 1];
+        }
+    }
+    // forward x transform of every (j,k) line
+#pragma omp parallel
+    {
+      std::vector<cplx> ba, bb;
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) r2hc(planx, &prsrc(1, jc, kc), ba, bb);
+    }
+    // y tridiagonal per (ic,kc) slot
+#pragma omp parallel
+    {
+      std::vector<double> a(nyc), b(nyc), c(nyc), f(nyc), arr(nyc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int jc = 1; jc <= nyc; ++jc) {
+            a[jc - 1] = am2Pr(jc);
+            c[jc - 1] = ap2Pr(jc);
+            b[jc - 1] = ac2Pr(jc) + WaveNumX(ic) + WaveNumZ(kc);
+            f[jc - 1] = prsrc(ic, jc, kc);
+          }
+          if (ic == 1 && kc == 1) { c[0] = zero; b[0] = one; a[0] = zero; f[0] = zero; }
+          InverseTridiagonal1(a.data(), b.data(), c.data(), f.data(), nyc, arr.data());
+          for (int jc = 1; jc <= nyc; ++jc) prsrc(ic, jc, kc) = f[jc - 1];
+        }
+    }
+    // inverse x then inverse z
+#pragma omp parallel
+    {
+      std::vector<cplx> ba, bb;
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) hc2r(planx, &prsrc(1, jc, kc), ba, bb);
+    }
+#pragma omp parallel
+    {
+      std::vector<double> line(nzc);
+      std::vector<cplx> ba, bb;
+#pragma omp for schedule(static)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int kc = 1; kc <= nzc; ++kc) line[kc - 1] = prsrc(ic, jc, kc);
+          hc2r(planz, line.data(), ba, bb);
+          for (int kc = 1; kc <= nzc; ++kc) prsrc(ic, jc, kc) = line[kc - 1];
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) prphiHalo(ic, jc, kc) = prsrc(ic, jc, kc) * normfft;
+  }
+
+  // ---- src/CFD_2nd/m_TScheme.f90:281-306 (FluidVelUpdate) ----
+  void FluidVelUpdate(const F3& phi) {
+    double rdxEta2 = rdx * pmAlpha, rdzEta2 = rdz * pmAlpha;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1;
+        double sucacEta2 = rdyc(jc) * pmAlpha;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1;
+          double locphi = phi(ic, jc, kc);
+          ux(ic, jc, kc) = ux(ic, jc, kc) - (locphi - phi(im, jc, kc)) * rdxEta2;
+          uy(ic, jc, kc) = uy(ic, jc, kc) - (locphi - phi(ic, jm, kc)) * sucacEta2;
+          uz(ic, jc, kc) = uz(ic, jc, kc) - (locphi - phi(ic, jc, km)) * rdzEta2;
+        }
+      }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:852-873 (PressureUpdate_PIMP) ----
+  void PressureUpdate_PIMP(const F3& phi) {
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jp = jc + 1, jm = jc - 1;
+        double pmBetap = -pmBeta * ap2Pr(jc);
+        double pmBetac = -pmBeta * ac2Pr(jc) + one;
+        double pmBetam = -pmBeta * am2Pr(jc);
+        for (int ic = 1; ic <= nxc; ++ic)
+          pressure(ic, jc, kc) = pressure(ic, jc, kc) + pmBetap * phi(ic, jp, kc) + pmBetac * phi(ic, jc, kc) + pmBetam * phi(ic, jm, kc);
+      }
+  }
+
+  // ---- src/CFD_2nd/m_ChannelSystem.f90:91-124, one substep split in stages ----
+  // stage 0: PMcoeUpdate + Update_uy_ym; 1: clcRhsX/Y/Z; 2: clcU1/2/3Hat;
+  // 3: SetBC_and_UpdateHaloForPrSrc + clcPrSrc; 4: clcPPE + SetBC_and_UpdateHalo_pr;
+  // 5: FluidVelUpdate; 6: PressureUpdate + SetBC_and_UpdateHalo(u) + ..._pr(p)
+  void stage(int st, int ns) {
+    switch (st) {
+      case 0: PMcoeUpdate(ns); Update_uy_ym(); break;
+      case 1:
+        clcRhsX_PIMP(RealArr1, HistX);
+        clcRhsY_PIMP(RealArr2, HistY);
+        clcRhsZ_PIMP(RealHalo, HistZ);
+        break;
+      case 2:
+        clcUHat_PIMP_c(ux, RealArr1);
+        clcU2Hat_PIMP(RealArr2);
+        clcUHat_PIMP_c(uz, RealHalo);
+        break;
+      case 3:
+        SetBC_and_UpdateHaloForPrSrc();
+        divmax1_last = clcPrSrcOther(RealArr1);
+        break;
+      case 4:
+        clcPPE(RealArr1, RealHalo);
+        SetBC_and_UpdateHalo_pr(RealHalo);
+        break;
+      case 5: FluidVelUpdate(RealHalo); break;
+      case 6:
+        PressureUpdate_PIMP(RealHalo);
+        SetBC_and_UpdateHalo();
+        SetBC_and_UpdateHalo_pr(pressure);
+        break;
+    }
+  }
+
+  // ---- src/CFD_2nd/m_ChannelSystem.f90:73-154 (ChannelIterate) ----
+  int ChannelIterate(orc_info* info) {
+    itime += 1;
+    double uddxmax = CalcMaxCFL();
+    double cflmp = uddxmax * dt;
+    if (P.iCFL == 1) { dt = P.CFLc / uddxmax; dt = std::min(dt, P.dtMax); }
+    else dt = P.dtMax;
+    for (int ns = 1; ns <= iadvance; ++ns)
+      for (int st = 0; st <= 6; ++st) stage(st, ns);
+    double divmax2 = CheckDivergence();
+    double vmax[3];
+    CalcVmax(vmax);
+    int status = 0;
+    if (divmax2 > P.div_limit) status = 1;
+    else if (std::min(vmax[0], std::min(vmax[1], vmax[2])) > P.vel_limit) status = 2;
+    if (info) {
+      info->SimTime = SimTime; info->dt = dt; info->cflmp = cflmp; info->divmax1 = divmax1_last;
+      info->divmax2 = divmax2; info->vmax[0] = vmax[0]; info->vmax[1] = vmax[1]; info->vmax[2] = vmax[2];
+      info->uxm = CalcUxAver(); info->PrGradAver = PrGradAver; info->itime = itime; info->status = status;
+    }
+    return status;
+  }
+
+  // ---- src/CFD_2nd/m_FlowType_Channel.f90:175-330 (clcStat_CH moment sums) ----
+  void clcStat_CH() {
+    double rdxh = rdx * half;
+    double inxz = one / ((double)nxc * (double)nzc);
+    for (int jc = 1; jc <= nyc; ++jc) {
+      int jp = jc + 1, jm = jc - 1;
+      double InterpY1 = half * YinterpCoe(jc), InterpY2 = half - InterpY1;
+      double cac = rdyc(jc), cacU = rdyc(jp), caj = rdyp(jc);
+      double S[35] = {0};
+      for (int kc = 1; kc <= nzc; ++kc) {
+        int km = kc - 1, kp = kc + 1;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double uxloc = ux(ic, jc, kc), uyloc = uy(ic, jc, kc), uzloc = uz(ic, jc, kc), prloc = pressure(ic, jc, kc);
+          double uxCell = half * (ux(ic, jc, kc) + ux(ip, jc, kc));
+          double uyCell = half * (uy(ic, jc, kc) + uy(ic, jp, kc));
+          double uzCell = half * (uz(ic, jc, kc) + uz(ic, jc, kp));
+          double prloc2 = InterpY1 * (pressure(im, jm, kc) + pressure(ic, jm, kc)) + InterpY2 * (pressure(im, jc, kc) + pressure(ic, jc, kc));
+          double dudx = (ux(ip, jc, kc) - ux(ic, jc, kc)) * rdx;
+          double dudy = (ux(ic, jc, kc) - ux(ic, jm, kc)) * cac;
+          double dudz = (ux(ic, jc, kc) - ux(ic, jc, km)) * rdz;
+          double dvdx = (uy(ic, jc, kc) - uy(im, jc, kc)) * rdx;
+          double dvdy = (uy(ic, jp, kc) - uy(ic, jc, kc)) * caj;
+          double dvdz = (uy(ic, jc, kc) - uy(ic, jc, km)) * rdz;
+          double dwdx = (uz(ic, jc, kc) - uz(im, jc, kc)) * rdx;
+          double dwdy = (uz(ic, jc, kc) - uz(ic, jm, kc)) * cac;
+          double dwdz = (uz(ic, jc, kp) - uz(ic, jc, kc)) * rdz;
+          double dudxx = (ux(ip, jc, kc) - two * ux(ic, jc, kc) + ux(im, jc, kc)) * rdx2;
+          double dudyy = ap2c(jc) * ux(ic, jp, kc) + ac2c(jc) * ux(ic, jc, kc) + am2c(jc) * ux(ic, jm, kc);
+          double dudzz = (ux(ic, jc, kp) - two * ux(ic, jc, kc) + ux(ic, jc, km)) * rdz2;
+          double dvdxx = (uy(ip, jc, kc) - two * uy(ic, jc, kc) + uy(im, jc, kc)) * rdx2;
+          double dvdyy = ap2p(jc) * uy(ic, jp, kc) + ac2p(jc) * uy(ic, jc, kc) + am2p(jc) * uy(ic, jm, kc);
+          double dvdzz = (uy(ic, jc, kp) - two * uy(ic, jc, kc) + uy(ic, jc, km)) * rdz2;
+          double dwdxx = (uz(ip, jc, kc) - two * uz(ic, jc, kc) + uz(im, jc, kc)) * rdx2;
+          double dwdyy = ap2c(jc) * uz(ic, jp, kc) + ac2c(jc) * uz(ic, jc, kc) + am2c(jc) * uz(ic, jm, kc);
+          double dwdzz = (uz(ic, jc, kp) - two * uz(ic, jc, kc) + uz(ic, jc, km)) * rdz2;
+          double vor_x = dwdy - dvdz, vor_y = dudz - dwdx, vor_z = dvdx - dudy;
+          double dudxC = (ux(ip, jc, kc) - ux(im, jc, kc)) * rdxh;
+          double dvdxU = (uy(ic, jp, kc) - uy(im, jp, kc)) * rdx;
+          double dudyU = (ux(ic, jp, kc) - ux(ic, jc, kc)) * cacU;
+          double dvdyM = (uy(im, jp, kc) - uy(im, jc, kc)) * caj;
+          double dudzC = (InterpY1 * (ux(ic, jm, kp) - ux(ic, jm, km)) + InterpY2 * (ux(ic, jc, kp) - ux(ic, jc, km))) * rdz;
+          double dvdzC = (uy(im, jc, kp) - uy(im, jc, km) + uy(ic, jc, kp) - uy(ic, jc, km)) * rdz * quarter;
+          S[0] += uxloc; S[1] += uyloc; S[2] += uzloc; S[3] += prloc;
+          S[4] += uxloc * uxloc; S[5] += uyloc * uyloc; S[6] += uzloc * uzloc; S[7] += prloc * prloc;
+          S[8] += uxCell * uyCell; S[9] += uyCell * uzCell; S[10] += uxCell * uzCell;
+          S[11] += uxCell * prloc; S[12] += uyCell * prloc; S[13] += uzCell * prloc;
+          S[14] += uxCell * uxCell * uyCell; S[15] += uyloc * uyloc * uyloc; S[16] += uzCell * uzCell * uyCell;
+          S[17] += uxCell * uyCell * uyCell; S[18] += uxloc * uxloc * uxloc; S[19] += uzloc * uzloc * uzloc;
+          S[20] += uxloc * uxloc * uxloc * uxloc; S[21] += uyloc * uyloc * uyloc * uyloc; S[22] += uzloc * uzloc * uzloc * uzloc;
+          S[23] += prloc * dudx; S[24] += prloc * dvdy; S[25] += prloc * dwdz;
+          S[26] += prloc2 * (dudy + dvdx);
+          S[27] += uxloc * (dudxx + dudyy + dudzz); S[28] += uyloc * (dvdxx + dvdyy + dvdzz); S[29] += uzloc * (dwdxx + dwdyy + dwdzz);
+          S[30] += dudxC * (dvdxU + dvdx) * half + (dudyU + dudy) * (dvdyM + dvdy) * quarter;
+          S[31] += dudzC * dvdzC;
+          S[32] += vor_x * vor_x; S[33] += vor_y * vor_y; S[34] += vor_z * vor_z;
+        }
+      }
+      for (int q = 0; q < 35; ++q) SumStat[(size_t)q + 35 * (size_t)(jc - 1)] += S[q] * inxz;
+    }
+    {
+      int jc = nyp, jm = jc - 1;
+      double cac = rdyc(jc);
+      double InterpY1 = half * YinterpCoe(jc), InterpY2 = half - InterpY1;
+      double S26 = 0, S32 = 0, S34 = 0;
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1;
+          double prloc2 = InterpY1 * (pressure(im, jm, kc) + pressure(ic, jm, kc)) + InterpY2 * (pressure(im, jc, kc) + pressure(ic, jc, kc));
+          double dudy = (ux(ic, jc, kc) - ux(ic, jm, kc)) * cac;
+          double dwdy = (uz(ic, jc, kc) - uz(ic, jm, kc)) * cac;
+          double vor_x = dwdy, vor_z = -dudy;
+          S26 += prloc2 * (dudy + zero);
+          S32 += vor_x * vor_x;
+          S34 += vor_z * vor_z;
+        }
+      SumStat[26 + 35 * (size_t)(jc - 1)] += S26 * inxz;
+      SumStat[32 + 35 * (size_t)(jc - 1)] += S32 * inxz;
+      SumStat[34 + 35 * (size_t)(jc - 1)] += S34 * inxz;
+    }
+    PrGradsum = PrGradsum + PrGradAver;
+    nfstime += 1;
+  }
+
+  F3* field(int id) {
+    switch (id) {
+      case 0: return &ux; case 1: return &uy; case 2: return &uz; case 3: return &pressure;
+      case 4: return &HistX; case 5: return &HistY; case 6: return &HistZ;
+      case 7: return &RealArr1; case 8: return &RealArr2; case 9: return &RealHalo; case 10: return &nut;
+    }
+    return nullptr;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void* orc_create(const orc_params* p) {
+  if (!p || p->nxc < 2 || p->nyc < 2 || p->nzc < 2) return nullptr;
+  Oracle* o = new Oracle();
+  o->init(p);
+  return o;
+}
+
+void orc_destroy(void* h) { delete (Oracle*)h; }
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+// y grid yp(1..nyp) and the metric vectors, for cross-checking the product's own mesh code.
+void orc_get_mesh(void* h, double* yp_out, double* yc_out, double* dyp_out, double* dyc_out) {
+  Oracle* o = (Oracle*)h;
+  for (int j = 1; j <= o->nyp; ++j) {
+    if (yp_out) yp_out[j - 1] = o->yp(j);
+    if (yc_out) yc_out[j - 1] = o->yc(j);
+    if (dyp_out) dyp_out[j - 1] = o->dyp(j);
+    if (dyc_out) dyc_out[j - 1] = o->dyc(j);
+  }
+}
+
+// Interior (nxc,nyc,nzc) Fortran-order state, as in the restart file
+// (src/CFD_2nd/m_IOAndVisu.f90:352-438).  hist may be NULL.  Afterwards the
+// ghost cells are rebuilt like ChannelInitialize (m_ChannelSystem.f90:57-63).
+void orc_set_state(void* h, const double* ux, const double* uy, const double* uz, const double* p, const double* hist) {
+  Oracle* o = (Oracle*)h;
+  size_t N = (size_t)o->nxc * o->nyc * o->nzc;
+  size_t q = 0;
+  for (int k = 1; k <= o->nzc; ++k) for (int j = 1; j <= o->nyc; ++j) for (int i = 1; i <= o->nxc; ++i, ++q) {
+    o->ux(i, j, k) = ux[q]; o->uy(i, j, k) = uy[q]; o->uz(i, j, k) = uz[q]; o->pressure(i, j, k) = p[q];
+    if (hist) { o->HistX(i, j, k) = hist[q]; o->HistY(i, j, k) = hist[N + q]; o->HistZ(i, j, k) = hist[2 * N + q]; }
+    else { o->HistX(i, j, k) = 0; o->HistY(i, j, k) = 0; o->HistZ(i, j, k) = 0; }
+  }
+  o->Update_uy_ym();
+  o->SetBC_and_UpdateHalo();
+  o->SetBC_and_UpdateHalo_pr(o->pressure);
+  std::fill(o->RealArr1.a.begin(), o->RealArr1.a.end(), 0.0);
+  std::fill(o->RealArr2.a.begin(), o->RealArr2.a.end(), 0.0);
+  o->SimTime = 0; o->dt = o->P.dtMax; o->itime = 0;
+}
+
+void orc_get_state(void* h, double* ux, double* uy, double* uz, double* p, double* hist) {
+  Oracle* o = (Oracle*)h;
+  size_t N = (size_t)o->nxc * o->nyc * o->nzc;
+  size_t q = 0;
+  for (int k = 1; k <= o->nzc; ++k) for (int j = 1; j <= o->nyc; ++j) for (int i = 1; i <= o->nxc; ++i, ++q) {
+    if (ux) ux[q] = o->ux(i, j, k);
+    if (uy) uy[q] = o->uy(i, j, k);
+    if (uz) uz[q] = o->uz(i, j, k);
+    if (p) p[q] = o->pressure(i, j, k);
+    if (hist) { hist[q] = o->HistX(i, j, k); hist[N + q] = o->HistY(i, j, k); hist[2 * N + q] = o->HistZ(i, j, k); }
+  }
+}
+
+// Full array with its ghost cells (Fortran order over the allocated bounds).
+// Returns the number of doubles written, or the needed size when out is NULL.
+long long orc_get_array(void* h, int id, double* out) {
+  Oracle* o = (Oracle*)h;
+  F3* f = o->field(id);
+  if (!f) return -1;
+  if (out) std::memcpy(out, f->a.data(), f->a.size() * sizeof(double));
+  return (long long)f->a.size();
+}
+
+long long orc_set_array(void* h, int id, const double* in) {
+  Oracle* o = (Oracle*)h;
+  F3* f = o->field(id);
+  if (!f) return -1;
+  std::memcpy(f->a.data(), in, f->a.size() * sizeof(double));
+  return (long long)f->a.size();
+}
+
+void orc_set_dt(void* h, double dt) { ((Oracle*)h)->dt = dt; }
+
+void orc_stage(void* h, int st, int ns) { ((Oracle*)h)->stage(st, ns); }
+
+int orc_step(void* h, int nsteps, orc_info* info) {
+  Oracle* o = (Oracle*)h;
+  int st = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    st = o->ChannelIterate(info);
+    if (st) break;
+  }
+  return st;
+}
+
+// Standalone Poisson solve: src and phi interior (nxc,nyc,nzc) arrays.
+void orc_poisson(void* h, const double* src, double* phi) {
+  Oracle* o = (Oracle*)h;
+  size_t q = 0;
+  for (int k = 1; k <= o->nzc; ++k) for (int j = 1; j <= o->nyc; ++j) for (int i = 1; i <= o->nxc; ++i, ++q)
+    o->RealArr1(i, j, k) = src[q];
+  o->clcPPE(o->RealArr1, o->RealHalo);
+  q = 0;
+  for (int k = 1; k <= o->nzc; ++k) for (int j = 1; j <= o->nyc; ++j) for (int i = 1; i <= o->nxc; ++i, ++q)
+    phi[q] = o->RealHalo(i, j, k);
+}
+
+// FFTW-convention r2r transforms of one line, for known-answer tests.
+void orc_r2hc(int n, double* x) {
+  FFTPlan pl; pl.init(n);
+  std::vector<cplx> a, b;
+  r2hc(pl, x, a, b);
+}
+void orc_hc2r(int n, double* x) {
+  FFTPlan pl; pl.init(n);
+  std::vector<cplx> a, b;
+  hc2r(pl, x, a, b);
+}
+
+void orc_stats_accumulate(void* h) { ((Oracle*)h)->clcStat_CH(); }
+
+// SumStat (35 x nyp, Fortran order), nfstime and PrGradsum.
+int orc_stats_get(void* h, double* sumstat, double* prgradsum) {
+  Oracle* o = (Oracle*)h;
+  if (sumstat) std::memcpy(sumstat, o->SumStat.data(), o->SumStat.size() * sizeof(double));
+  if (prgradsum) *prgradsum = o->PrGradsum;
+  return o->nfstime;
+}
+
+}  // extern "C"

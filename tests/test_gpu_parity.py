@@ -1,0 +1,79 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle, FP64.
+
+Tolerances: per-stage results within 1e-12 relative (L2 and max norms);
+whole steps within the 1e-10 relative bound of the specification."""
+import numpy as np
+import pytest
+
+from helpers import rel_l2, rel_max, small_channel
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(cfg, seed=0x5EED):
+    from channel3d_b200 import ChannelSolver, initfield, mesh_y
+    from oracle import oracle as O
+    yp = mesh_y(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp, seed=seed)
+    p = 0.01 * np.random.default_rng(seed).standard_normal(cfg.shape)
+    o = O.Oracle(cfg)
+    o.set_state(ux, uy, uz, p)
+    s = ChannelSolver(cfg, yp=yp)
+    s.upload(ux, uy, uz, p)
+    return o, s
+
+
+@pytest.mark.parametrize("shape", [(32, 24, 16), (48, 32, 36), (64, 64, 64)])
+def test_stage_parity(built, shape):
+    cfg = small_channel(*shape)
+    o, s = _pair(cfg)
+    for ns in (1, 2, 3):
+        o.stage(0, ns); s.stage(0, ns)
+        o.stage(1, ns); s.stage(1, ns)
+        for wo, wg in ((o.ARR2, s.RHSY), (o.HALO, s.RHSZ), (o.HISTX, s.HISTX),
+                       (o.HISTY, s.HISTY), (o.HISTZ, s.HISTZ)):
+            a, b = s.get_array(wg), o.get_interior(wo)
+            assert rel_max(a, b) < 1e-12, (ns, wg, rel_max(a, b))
+        # the device adds the mean pressure gradient dpmdxns (clcRhsX_PIMP :65-71)
+        # when it loads RhsX into the Helmholtz solve, so RhsX differs by a constant
+        d = s.get_array(s.RHSX) - o.get_interior(o.ARR1)
+        assert np.abs(d - d.mean()).max() < 1e-12 * np.abs(o.get_interior(o.ARR1)).max(), ns
+        o.stage(2, ns); s.stage(2, ns)
+        go, gs = o.get_state(), s.download()
+        for k in ("ux", "uy", "uz"):
+            assert rel_max(gs[k], go[k]) < 1e-12, (ns, "uhat", k, rel_max(gs[k], go[k]))
+        o.stage(3, ns); s.stage(3, ns)
+        o.stage(4, ns); s.stage(4, ns)
+        phi_o, phi_g = o.get_interior(o.HALO), s.get_array(s.PRPHI)
+        assert rel_l2(phi_g, phi_o) < 1e-11, (ns, "phi", rel_l2(phi_g, phi_o))
+        o.stage(5, ns); s.stage(5, ns)
+        o.stage(6, ns); s.stage(6, ns)
+        go, gs = o.get_state(), s.download()
+        for k in ("ux", "uy", "uz", "p"):
+            assert rel_max(gs[k], go[k]) < 1e-11, (ns, "final", k, rel_max(gs[k], go[k]))
+
+
+def test_poisson_parity(built):
+    cfg = small_channel(48, 40, 24)
+    from channel3d_b200 import ChannelSolver, mesh_y
+    from oracle import oracle as O
+    src = np.random.default_rng(1).standard_normal(cfg.shape)
+    o = O.Oracle(cfg)
+    s = ChannelSolver(cfg, yp=mesh_y(cfg))
+    a, b = s.poisson(src), o.poisson(src)
+    assert rel_l2(a, b) < 1e-12, rel_l2(a, b)
+
+
+def test_step_parity_64cubed_200_steps(built):
+    from channel3d_b200 import workloads
+    cfg, nsteps = workloads.get("channel64_re5600")
+    o, s = _pair(cfg)
+    di = s.step(nsteps)
+    do = o.step(nsteps)
+    go, gs = o.get_state(), s.download()
+    for k in ("ux", "uy", "uz", "p"):
+        e = rel_l2(gs[k], go[k])
+        assert e < 1e-10, (k, e)
+    assert di["divmax2"] < 1e-12 and do["divmax2"] < 1e-12
+    assert abs(di["PrGradAver"] - do["PrGradAver"]) <= 1e-10 * max(1.0, abs(do["PrGradAver"]))
+    assert di["itime"] == nsteps

@@ -185,6 +185,8 @@ def parse_namelists(text):
             elif ch == "!" and q is None:
                 s = s[:idx]
                 break
+        if s.strip().startswith("/"):
+            s = "/"  # namelist terminator; the rest of the line is free text
         lines.append(s)
     text = "\n".join(lines)
     for m in re.finditer(r"&(\w+)(.*?)(?:^|\s)/", text, flags=re.S | re.M):

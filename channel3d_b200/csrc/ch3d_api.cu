@@ -89,7 +89,13 @@ bool factor23(int n, FFTPlanDev& pl) {
   while (m % 4 == 0) { pl.radix[pl.npass++] = 4; m /= 4; }
   while (m % 2 == 0) { pl.radix[pl.npass++] = 2; m /= 2; }
   while (m % 3 == 0) { pl.radix[pl.npass++] = 3; m /= 3; }
-  return m == 1 && pl.npass <= CH3D_MAX_PASSES;
+  int Ns = 1;
+  for (int p = 0; p < pl.npass; ++p) {
+    pl.mNB[p] = fdiv_magic((unsigned)(n / pl.radix[p]));
+    pl.mNs[p] = fdiv_magic((unsigned)Ns);
+    Ns *= pl.radix[p];
+  }
+  return m == 1 && pl.npass <= CH3D_MAX_PASSES && n < (1 << 16);
 }
 
 template <class CT>
@@ -211,7 +217,8 @@ int check_config(const ch3d_config* g) {
 template <class T>
 int alloc_fields(ch3d_ctx* c) {
   typedef typename CplxOf<T>::type CT;
-  for (int q = 0; q < 11; ++q) {
+  for (int q = 0; q < 15; ++q) {
+    if (q == 11) continue;  // nut: LES only
     CU(cudaMalloc(&c->f[q], (size_t)c->N * sizeof(T)));
     CU(cudaMemsetAsync(c->f[q], 0, (size_t)c->N * sizeof(T), c->stream));
     c->bytes += (long long)c->N * sizeof(T);
@@ -340,8 +347,8 @@ int record_step(ch3d_ctx* c) {
   CU(launch_step_begin(c));
   for (int ns = 1; ns <= c->iadvance; ++ns) {
     CU(launch_substep_setup(c, ns));
-    CU(launch_rhs(c));
-    CU(launch_uhat(c));
+    CU(launch_helm_factors(c));
+    CU(launch_rhs_uhat(c));
     CU(launch_prsrc_xfft(c, 0));
     CU(launch_poisson_spectral(c));
     CU(launch_xifft(c));
@@ -474,6 +481,14 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
   if (c->fp32) c->m32 = metrics_ptrs<float>((const float*)c->met, c->ny);
   else c->m32 = Metrics<float>();
   if (!c->fp32) c->m64 = metrics_ptrs<double>((const double*)c->met, c->ny);
+  c->P = 32;
+  while (c->P > 1 && c->ny < 2 * c->P) c->P >>= 1;
+  c->Pv = 32;
+  while (c->Pv > 1 && c->ny < 2 * c->Pv) c->Pv >>= 1;
+  {
+    size_t nf = (size_t)2 * (5 * c->ny + 6 * (c->Pv > 1 ? c->Pv - 1 : 1));
+    if (cudaMalloc(&c->hfac, nf * sizeof(double)) != cudaSuccess) return cleanup(fail(CH3D_ERR_NOMEM, "hfac"));
+  }
   {
     dim3 g((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz);
     c->npart = (int)(g.x * g.y * g.z);
@@ -499,8 +514,8 @@ int ch3d_destroy(ch3d_ctx* c) {
   cudaSetDevice(c->device);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
-  for (int q = 0; q < 12; ++q) if (c->f[q]) cudaFree(c->f[q]);
-  void* bufs[] = {c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  for (int q = 0; q < 15; ++q) if (c->f[q]) cudaFree(c->f[q]);
+  void* bufs[] = {c->hfac, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -596,7 +611,7 @@ int ch3d_stage(ch3d_ctx* c, int stage, int ns) {
   switch (stage) {
     case 0: CU(launch_substep_setup(c, ns)); break;
     case 1: CU(launch_rhs(c)); break;
-    case 2: CU(launch_uhat(c)); break;
+    case 2: CU(launch_helm_factors(c)); CU(launch_uhat(c)); break;
     case 3: break;  // clcPrSrc is fused into the forward x transform of stage 4
     case 4:
       CU(launch_prsrc_xfft(c, 0));
@@ -617,6 +632,7 @@ static int array_slot(int which) {
     case 0: case 1: case 2: case 3: case 4: case 5: case 6: case 7: case 8: return which;
     case 9: return 10;   // prphi (the reference keeps RhsZ and prphiHalo in RealHalo)
     case 11: return 9;   // RhsZ
+    case 12: case 13: case 14: return which;  // u* (velocity after the Helmholtz solves)
     default: return -1;
   }
 }
@@ -726,9 +742,9 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
   for (int s = 0; s < nsteps; ++s) {
     CU(mark(6)); CU(launch_step_begin(c)); CU(done());
     for (int ns = 1; ns <= c->iadvance; ++ns) {
-      CU(mark(6)); CU(launch_substep_setup(c, ns)); CU(done());
-      CU(mark(0)); CU(launch_rhs(c)); CU(done());
-      CU(mark(1)); CU(launch_uhat(c)); CU(done());
+      CU(mark(6)); CU(launch_substep_setup(c, ns)); CU(launch_helm_factors(c)); CU(done());
+      CU(mark(0)); CU(launch_rhs_uhat(c)); CU(done());
+      CU(mark(1)); CU(done());
       CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());
       CU(mark(3)); CU(launch_poisson_spectral(c)); CU(done());
       CU(mark(4)); CU(launch_xifft(c)); CU(done());

@@ -31,7 +31,10 @@ struct ch3d_ctx {
   std::vector<double> am2cForCN, ap2cForCN, s1coe, WaveNumX, WaveNumZ;
 
   // device buffers
-  void* f[12] = {nullptr};   // ux uy uz p hx hy hz rx ry rz phi nut (precision T)
+  void* f[15] = {nullptr};   // ux uy uz p hx hy hz rx ry rz phi nut u*x u*y u*z (precision T)
+  double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
+  int P = 16;                // chunks of the partitioned Poisson y solves
+  int Pv = 32;               // chunks of the partitioned velocity Helmholtz solves
   void* spec = nullptr;      // complex spectrum (kx,j,kz)
   void* met = nullptr;       // packed metric vectors (precision T)
   double* met64 = nullptr;   // FP64 copy (always)
@@ -66,11 +69,13 @@ cudaError_t launch_substep_setup(ch3d_ctx* c, int ns);
 cudaError_t launch_step_begin(ch3d_ctx* c);
 cudaError_t launch_step_end(ch3d_ctx* c);
 cudaError_t launch_rhs(ch3d_ctx* c);
-cudaError_t launch_uhat(ch3d_ctx* c);
-cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: step (1/pmAlpha), 1: projection (1)
+cudaError_t launch_uhat(ch3d_ctx* c);                  // stage path: Rhs arrays -> u*
+cudaError_t launch_rhs_uhat(ch3d_ctx* c);              // fused step path: u -> u*
+cudaError_t launch_helm_factors(ch3d_ctx* c);
+cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlpha, 1: div(u), 2: source in phi
 cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv
 cudaError_t launch_xifft(ch3d_ctx* c);
-cudaError_t launch_proj(ch3d_ctx* c, int mode);        // mode 0: step, 1: projection only
+cudaError_t launch_proj(ch3d_ctx* c, int mode);        // mode 0: u = u* - a grad phi, p update; 1: u -= grad phi
 cudaError_t launch_bulk_partials(ch3d_ctx* c);
 cudaError_t launch_diag(ch3d_ctx* c);
 cudaError_t launch_stats(ch3d_ctx* c);

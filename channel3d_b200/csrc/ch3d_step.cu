@@ -102,55 +102,45 @@ __global__ void k_step_end(DevScalars* sc, const double* __restrict__ part, int 
 
 // ---------------------------------------------------------------------------
 // clcRhsX/Y/Z_PIMP  (src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75, 161-209, 277-325)
-// One thread per cell; all three components share the loads.
+// at one cell: returns the three right-hand sides and updates HistX/Y/Z.
+// The mean pressure gradient dpmdxns (:61-74) is added by the callers.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
-                                                  const T* __restrict__ uy, const T* __restrict__ uz,
-                                                  const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
-                                                  T* __restrict__ hz, T* __restrict__ rx, T* __restrict__ ry,
-                                                  T* __restrict__ rz, const DevScalars* __restrict__ sc) {
-  if (sc->status) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+__device__ __forceinline__ void rhs_point(const Geo<T>& g, const Metrics<T>& m, const T* __restrict__ ux,
+                                          const T* __restrict__ uy, const T* __restrict__ uz,
+                                          const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
+                                          T* __restrict__ hz, int i, int j, int k, T pmGamma, T pmTheta, T pmAlpha,
+                                          T pmBeta, T& rxo, T& ryo, T& rzo) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  if (i >= nx || j >= ny) return;
   const int im = wrapm(i, nx), ip = wrapp(i, nx), km = wrapm(k, nz), kp = wrapp(k, nz);
   const int jc = j + 1;
-  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
   const T two = (T)2, half = (T)0.5, quarter = (T)0.25, one = (T)1;
   const long long idx = i + (long long)nx * (j + (long long)ny * k);
 
-  // ux samples
-  const T ux_c = ux[idx];
+  const T ux_c = __ldg(ux + idx);
   const T ux_ip = fld(ux, g, 0, ip, j, k), ux_im = fld(ux, g, 0, im, j, k);
   const T ux_jp = fld(ux, g, 0, i, j + 1, k), ux_jm = fld(ux, g, 0, i, j - 1, k);
   const T ux_kp = fld(ux, g, 0, i, j, kp), ux_km = fld(ux, g, 0, i, j, km);
   const T ux_ip_jm = fld(ux, g, 0, ip, j - 1, k), ux_ip_km = fld(ux, g, 0, ip, j, km);
-  // uy samples
-  const T uy_c = uy[idx];
+  const T uy_c = __ldg(uy + idx);
   const T uy_ip = fld(uy, g, 1, ip, j, k), uy_im = fld(uy, g, 1, im, j, k);
   const T uy_jp = fld(uy, g, 1, i, j + 1, k), uy_jm = fld(uy, g, 1, i, j - 1, k);
   const T uy_im_jp = fld(uy, g, 1, im, j + 1, k);
   const T uy_kp = fld(uy, g, 1, i, j, kp), uy_km = fld(uy, g, 1, i, j, km);
   const T uy_jp_km = fld(uy, g, 1, i, j + 1, km);
-  // uz samples
-  const T uz_c = uz[idx];
+  const T uz_c = __ldg(uz + idx);
   const T uz_ip = fld(uz, g, 2, ip, j, k), uz_im = fld(uz, g, 2, im, j, k);
   const T uz_jp = fld(uz, g, 2, i, j + 1, k), uz_jm = fld(uz, g, 2, i, j - 1, k);
   const T uz_kp = fld(uz, g, 2, i, j, kp), uz_km = fld(uz, g, 2, i, j, km);
   const T uz_im_kp = fld(uz, g, 2, im, j, kp), uz_jm_kp = fld(uz, g, 2, i, j - 1, kp);
-  // pressure samples
-  const T p_c = pr[idx];
+  const T p_c = __ldg(pr + idx);
   const T p_im = fld(pr, g, 3, im, j, k), p_jm = fld(pr, g, 3, i, j - 1, k), p_km = fld(pr, g, 3, i, j, km);
+  const T hx_o = hx[idx], hy_o = hy[idx], hz_o = hz[idx];
 
   const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
   const T IY1 = m.yinterp[jc], IY2 = one - IY1;
   const T IY3 = m.yinterp[jc + 1], IY4 = one - IY3;
-
-  // ---- RhsX ----
-  {
+  {  // RhsX
     const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
     const T sucaj = half * m.rdyp[jc];
     T h11 = ((ux_ip + ux_c) * (ux_ip + ux_c) - (ux_c + ux_im) * (ux_c + ux_im)) * qdx1;
@@ -162,11 +152,10 @@ __global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const 
     T dcq13 = d11q1 + d33q1;
     T gradp1 = (p_c - p_im) * rdx;
     T convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g.g1;
-    rx[idx] = pmGamma * convEd1 + pmTheta * hx[idx] - pmAlpha * gradp1 + two * pmBeta * d22q1;
+    rxo = pmGamma * convEd1 + pmTheta * hx_o - pmAlpha * gradp1 + two * pmBeta * d22q1;
     hx[idx] = convEd1;
   }
-  // ---- RhsY ----
-  {
+  {  // RhsY
     const T hdx1 = half * rdx, hdx3 = half * rdz;
     const T sucac = m.rdyc[jc], qsucac = quarter * sucac;
     T h21 = ((IY1 * ux_ip_jm + IY2 * ux_ip) * (uy_ip + uy_c) - (IY1 * ux_jm + IY2 * ux_c) * (uy_c + uy_im)) * hdx1;
@@ -178,11 +167,10 @@ __global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const 
     T dcq13 = d11q2 + d33q2;
     T gradp2 = (p_c - p_jm) * sucac;
     T convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g.g2;
-    ry[idx] = pmGamma * convEd2 + pmTheta * hy[idx] - pmAlpha * gradp2 + two * pmBeta * d22q2;
+    ryo = pmGamma * convEd2 + pmTheta * hy_o - pmAlpha * gradp2 + two * pmBeta * d22q2;
     hy[idx] = convEd2;
   }
-  // ---- RhsZ ----
-  {
+  {  // RhsZ
     const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
     const T sucaj = half * m.rdyp[jc];
     T h31 = ((ux_ip + ux_ip_km) * (uz_ip + uz_c) - (ux_c + ux_km) * (uz_c + uz_im)) * qdx1;
@@ -194,9 +182,165 @@ __global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const 
     T dcq13 = d11q3 + d33q3;
     T gradp3 = (p_c - p_km) * rdz;
     T convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g.g3;
-    rz[idx] = pmGamma * convEd3 + pmTheta * hz[idx] - pmAlpha * gradp3 + two * pmBeta * d22q3;
+    rzo = pmGamma * convEd3 + pmTheta * hz_o - pmAlpha * gradp3 + two * pmBeta * d22q3;
     hz[idx] = convEd3;
   }
+}
+
+// Neighbour addressing of one cell: a base index plus signed offsets that
+// already contain the periodic wrap in x and z; y neighbours past the walls
+// are replaced by the ghost rules of SetBC_and_UpdateHalo
+// (src/CFD_2nd/m_BC_and_Halo.f90:241-282).
+struct Nbr {
+  long long c;        // cell index
+  int xp, xm;         // offsets to i+1, i-1
+  long long zp, zm;   // offsets to k+1, k-1
+  int yp;             // +nx (offset to j+1)
+  bool jlo, jhi;      // j == 0, j == ny-1
+};
+
+template <class T>
+__device__ __forceinline__ Nbr make_nbr(const Geo<T>& g, int i, int j, int k) {
+  Nbr n;
+  const long long plane = (long long)g.nx * g.ny;
+  n.c = i + (long long)g.nx * j + plane * k;
+  n.xp = (i + 1 == g.nx) ? 1 - g.nx : 1;
+  n.xm = (i == 0) ? g.nx - 1 : -1;
+  n.zp = (k + 1 == g.nz) ? -(long long)(g.nz - 1) * plane : plane;
+  n.zm = (k == 0) ? (long long)(g.nz - 1) * plane : -plane;
+  n.yp = g.nx;
+  n.jlo = (j == 0);
+  n.jhi = (j == g.ny - 1);
+  return n;
+}
+
+// value at offset o (same j) and at j-1 / j+1 of the same offset column
+template <class T> __device__ __forceinline__ T at(const T* __restrict__ a, const Nbr& n, long long o) {
+  return __ldg(a + n.c + o);
+}
+// ux / uz (comp 0 / 2): wall ghosts 2 w - u (no-slip) or u -/+ w dyp (free-slip)
+template <class T>
+__device__ __forceinline__ T at_jm(const T* __restrict__ a, const Geo<T>& g, int comp, const Nbr& n, long long o) {
+  if (!n.jlo) return __ldg(a + n.c + o - n.yp);
+  if (comp == 1) return (T)(g.bc.uy_lo * 2.0) - __ldg(a + n.c + o + n.yp);  // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc)
+  const T v = __ldg(a + n.c + o);
+  if (comp == 3) return v;
+  const double w = comp == 0 ? g.bc.ux_lo : g.bc.uz_lo;
+  return g.bc.lo == -1 ? (T)(w * 2.0) - v : v - (T)(w * g.bc.dyp1);
+}
+template <class T>
+__device__ __forceinline__ T at_jp(const T* __restrict__ a, const Geo<T>& g, int comp, const Nbr& n, long long o) {
+  if (!n.jhi) return __ldg(a + n.c + o + n.yp);
+  if (comp == 1) return (T)g.bc.uy_hi;  // uy(ic,nyp,kc) = uyBcValue(yp)
+  const T v = __ldg(a + n.c + o);
+  if (comp == 3) return v;
+  const double w = comp == 0 ? g.bc.ux_hi : g.bc.uz_hi;
+  return g.bc.hi == -1 ? (T)(w * 2.0) - v : (T)(w * g.bc.dypN) + v;
+}
+
+// One component of clcRhsX/Y/Z_PIMP at one cell (C = 0, 1, 2), with its Hist
+// update; used by the fused solve kernel, where one block handles one component.
+template <class T, int C>
+__device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, const T* __restrict__ ux,
+                                      const T* __restrict__ uy, const T* __restrict__ uz, const T* __restrict__ pr,
+                                      T* __restrict__ h, int i, int j, int k, T pmGamma, T pmTheta, T pmAlpha,
+                                      T pmBeta) {
+  const Nbr n = make_nbr(g, i, j, k);
+  const int jc = j + 1;
+  const T two = (T)2, half = (T)0.5, quarter = (T)0.25, one = (T)1;
+  const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
+  const T IY1 = m.yinterp[jc], IY2 = one - IY1;
+  if (C == 0) {
+    const T ux_c = at(ux, n, 0), ux_ip = at(ux, n, n.xp), ux_im = at(ux, n, n.xm);
+    const T ux_jp = at_jp(ux, g, 0, n, 0), ux_jm = at_jm(ux, g, 0, n, 0);
+    const T ux_kp = at(ux, n, n.zp), ux_km = at(ux, n, n.zm);
+    const T uy_c = at(uy, n, 0), uy_im = at(uy, n, n.xm);
+    const T uy_jp = at_jp(uy, g, 1, n, 0), uy_im_jp = at_jp(uy, g, 1, n, n.xm);
+    const T uz_c = at(uz, n, 0), uz_im = at(uz, n, n.xm);
+    const T uz_kp = at(uz, n, n.zp), uz_im_kp = at(uz, n, n.zp + n.xm);
+    const T p_c = at(pr, n, 0), p_im = at(pr, n, n.xm);
+    const T h_o = h[n.c];
+    const T IY3 = m.yinterp[jc + 1], IY4 = one - IY3;
+    const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+    const T sucaj = half * m.rdyp[jc];
+    T h11 = ((ux_ip + ux_c) * (ux_ip + ux_c) - (ux_c + ux_im) * (ux_c + ux_im)) * qdx1;
+    T h12 = ((uy_jp + uy_im_jp) * (IY3 * ux_c + IY4 * ux_jp) - (uy_c + uy_im) * (IY1 * ux_jm + IY2 * ux_c)) * sucaj;
+    T h13 = ((uz_kp + uz_im_kp) * (ux_kp + ux_c) - (uz_c + uz_im) * (ux_c + ux_km)) * qdx3;
+    T d11q1 = (ux_ip - two * ux_c + ux_im) * rdx2;
+    T d22q1 = m.ap2c[jc] * ux_jp + m.ac2c[jc] * ux_c + m.am2c[jc] * ux_jm;
+    T d33q1 = g.ap3c * ux_kp + g.ac3c * ux_c + g.am3c * ux_km;
+    T dcq13 = d11q1 + d33q1;
+    T gradp1 = (p_c - p_im) * rdx;
+    T convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g.g1;
+    h[n.c] = convEd1;
+    return pmGamma * convEd1 + pmTheta * h_o - pmAlpha * gradp1 + two * pmBeta * d22q1;
+  } else if (C == 1) {
+    const T ux_c = at(ux, n, 0), ux_ip = at(ux, n, n.xp);
+    const T ux_jm = at_jm(ux, g, 0, n, 0), ux_ip_jm = at_jm(ux, g, 0, n, n.xp);
+    const T uy_c = at(uy, n, 0), uy_ip = at(uy, n, n.xp), uy_im = at(uy, n, n.xm);
+    const T uy_jp = at_jp(uy, g, 1, n, 0), uy_jm = at_jm(uy, g, 1, n, 0);
+    const T uy_kp = at(uy, n, n.zp), uy_km = at(uy, n, n.zm);
+    const T uz_c = at(uz, n, 0), uz_jm = at_jm(uz, g, 2, n, 0);
+    const T uz_kp = at(uz, n, n.zp), uz_jm_kp = at_jm(uz, g, 2, n, n.zp);
+    const T p_c = at(pr, n, 0), p_jm = at_jm(pr, g, 3, n, 0);
+    const T h_o = h[n.c];
+    const T hdx1 = half * rdx, hdx3 = half * rdz;
+    const T sucac = m.rdyc[jc], qsucac = quarter * sucac;
+    T h21 = ((IY1 * ux_ip_jm + IY2 * ux_ip) * (uy_ip + uy_c) - (IY1 * ux_jm + IY2 * ux_c) * (uy_c + uy_im)) * hdx1;
+    T h22 = ((uy_jp + uy_c) * (uy_jp + uy_c) - (uy_c + uy_jm) * (uy_c + uy_jm)) * qsucac;
+    T h23 = ((IY1 * uz_jm_kp + IY2 * uz_kp) * (uy_kp + uy_c) - (IY1 * uz_jm + IY2 * uz_c) * (uy_c + uy_km)) * hdx3;
+    T d11q2 = g.ap1c * uy_ip + g.ac1c * uy_c + g.am1c * uy_im;
+    T d22q2 = m.ap2p[jc] * uy_jp + m.ac2p[jc] * uy_c + m.am2p[jc] * uy_jm;
+    T d33q2 = g.ap3c * uy_kp + g.ac3c * uy_c + g.am3c * uy_km;
+    T dcq13 = d11q2 + d33q2;
+    T gradp2 = (p_c - p_jm) * sucac;
+    T convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g.g2;
+    h[n.c] = convEd2;
+    return pmGamma * convEd2 + pmTheta * h_o - pmAlpha * gradp2 + two * pmBeta * d22q2;
+  } else {
+    const T ux_c = at(ux, n, 0), ux_ip = at(ux, n, n.xp);
+    const T ux_km = at(ux, n, n.zm), ux_ip_km = at(ux, n, n.zm + n.xp);
+    const T uy_c = at(uy, n, 0), uy_jp = at_jp(uy, g, 1, n, 0);
+    const T uy_km = at(uy, n, n.zm), uy_jp_km = at_jp(uy, g, 1, n, n.zm);
+    const T uz_c = at(uz, n, 0), uz_ip = at(uz, n, n.xp), uz_im = at(uz, n, n.xm);
+    const T uz_jp = at_jp(uz, g, 2, n, 0), uz_jm = at_jm(uz, g, 2, n, 0);
+    const T uz_kp = at(uz, n, n.zp), uz_km = at(uz, n, n.zm);
+    const T p_c = at(pr, n, 0), p_km = at(pr, n, n.zm);
+    const T h_o = h[n.c];
+    const T IY3 = m.yinterp[jc + 1], IY4 = one - IY3;
+    const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+    const T sucaj = half * m.rdyp[jc];
+    T h31 = ((ux_ip + ux_ip_km) * (uz_ip + uz_c) - (ux_c + ux_km) * (uz_c + uz_im)) * qdx1;
+    T h32 = ((uy_jp + uy_jp_km) * (IY3 * uz_c + IY4 * uz_jp) - (uy_c + uy_km) * (IY1 * uz_jm + IY2 * uz_c)) * sucaj;
+    T h33 = ((uz_kp + uz_c) * (uz_kp + uz_c) - (uz_c + uz_km) * (uz_c + uz_km)) * qdx3;
+    T d11q3 = g.ap1c * uz_ip + g.ac1c * uz_c + g.am1c * uz_im;
+    T d22q3 = m.ap2c[jc] * uz_jp + m.ac2c[jc] * uz_c + m.am2c[jc] * uz_jm;
+    T d33q3 = (uz_kp - two * uz_c + uz_km) * rdz2;
+    T dcq13 = d11q3 + d33q3;
+    T gradp3 = (p_c - p_km) * rdz;
+    T convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g.g3;
+    h[n.c] = convEd3;
+    return pmGamma * convEd3 + pmTheta * h_o - pmAlpha * gradp3 + two * pmBeta * d22q3;
+  }
+}
+
+// Stand-alone clcRhsX/Y/Z (one thread per cell); the stage-level entry point.
+template <class T>
+__global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                  const T* __restrict__ uy, const T* __restrict__ uz,
+                                                  const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
+                                                  T* __restrict__ hz, T* __restrict__ rx, T* __restrict__ ry,
+                                                  T* __restrict__ rz, const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  T a, b, c;
+  rhs_point(g, m, ux, uy, uz, pr, hx, hy, hz, i, j, k, (T)sc->pmGamma, (T)sc->pmTheta, (T)sc->pmAlpha,
+            (T)sc->pmBeta, a, b, c);
+  const long long idx = i + (long long)g.nx * (j + (long long)g.ny * k);
+  rx[idx] = a; ry[idx] = b; rz[idx] = c;
 }
 
 // ---------------------------------------------------------------------------
@@ -210,19 +354,21 @@ __global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int chunk_lo(int p, int n, int P) { return (p * n) / P; }
 __device__ __forceinline__ int chunk_hi(int p, int n, int P) { return ((p + 1) * n) / P - 1; }
+// the chunk p with chunk_lo(p) <= j <= chunk_hi(p): the largest p with p*n/P <= j
+__device__ __forceinline__ int chunk_of(int j, int n, int P) { return ((j + 1) * P - 1) / n; }
 
 // Coefficients of the velocity Helmholtz systems (identical for all columns).
-// comp 0/2: clcU1Hat_PIMP / clcU3Hat_PIMP (m_TSchemePIMP_inc.f90:410-416, 720-726)
-// comp 1:   clcU2Hat_PIMP (:561-572), row 1 is the identity.
+// set 0: clcU1Hat_PIMP / clcU3Hat_PIMP (m_TSchemePIMP_inc.f90:410-416, 720-726)
+// set 1: clcU2Hat_PIMP (:561-572), row 1 is the identity.
 struct HelmCoef {
   const double* ap2cForCN; const double* am2cForCN;
   const double* ap2p; const double* ac2p; const double* am2p;
 };
 
-__device__ __forceinline__ void helm_abc(const HelmCoef& hc, int comp, double pmBeta, int j, double& a, double& b,
+__device__ __forceinline__ void helm_abc(const HelmCoef& hc, int set, double pmBeta, int j, double& a, double& b,
                                          double& c) {
   const int jc = j + 1;
-  if (comp == 1) {
+  if (set == 1) {
     if (j == 0) { a = 0.0; b = 1.0; c = 0.0; return; }
     c = -pmBeta * hc.ap2p[jc];
     b = -pmBeta * hc.ac2p[jc] + 1.0;
@@ -234,52 +380,26 @@ __device__ __forceinline__ void helm_abc(const HelmCoef& hc, int comp, double pm
   }
 }
 
-// clcU1Hat/U2Hat/U3Hat_PIMP: (I - pmBeta L_y) du = Rhs ; u += du.
-// Block: TI consecutive i at one k, all j; threads = TI * P.
-template <class T, int TI>
-__global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, HelmCoef hc, T* __restrict__ ux, T* __restrict__ uy,
-                                                   T* __restrict__ uz, const T* __restrict__ rx,
-                                                   const T* __restrict__ ry, const T* __restrict__ rz, int P,
-                                                   const DevScalars* __restrict__ sc) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  if (sc->status) return;
-  const int comp = blockIdx.z;
-  T* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
-  const T* rhs = comp == 0 ? rx : (comp == 1 ? ry : rz);
-  const int nx = g.nx, ny = g.ny;
-  const int k = blockIdx.y;
-  const int i0 = blockIdx.x * TI;
-  const int Q = P - 1;
-  double* RM = (double*)smem_raw;
-  double* CP = RM + ny;
-  double* AL = CP + ny;
-  double* BE = AL + ny;
-  double* AA = BE + ny;
-  double* RED = AA + ny;                 // Q * 6 : Minv(4), l, v
-  T* F = (T*)(RED + 6 * (Q > 0 ? Q : 1)); // ny * TI
-  T* IF = F + (size_t)ny * TI;           // TI * Q * 2
-  const double pmBeta = sc->pmBeta;
-  const T add = comp == 0 ? (T)sc->dpmdxns : (T)0;
-  const int tid = threadIdx.x;
+// Factor layout of one set: RM | AA | CP | AL | BE (ny each), then per
+// interface q: M00 M01 M10 M11 l v (6 each).
+__host__ __device__ inline int helm_set_stride(int ny, int P) { return 5 * ny + 6 * (P > 1 ? P - 1 : 1); }
 
-  // load the right-hand side tile (RhsX gets the mean pressure gradient, :65-71)
-  for (int t = tid; t < ny * TI; t += blockDim.x) {
-    const int j = t / TI, ii = t % TI;
-    const int i = i0 + ii;
-    T v = (T)0;
-    if (i < nx) {
-      v = rhs[i + (long long)nx * (j + (long long)ny * k)] + add;
-      if (comp == 1 && j == 0) v = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
-    }
-    F[t] = v;
-  }
-  // chunk factors (shared by all columns)
-  if (tid < P) {
-    const int p = tid, s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
+// Precomputes the chunk factors, spikes and interface block-Thomas factors of
+// both Helmholtz sets for the current pmBeta (once per substep; block = set).
+__global__ void k_helm_factors(HelmCoef hc, int ny, int P, double* __restrict__ fac,
+                               const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int set = blockIdx.x;
+  double* F = fac + (size_t)set * helm_set_stride(ny, P);
+  double *RM = F, *AA = F + ny, *CP = F + 2 * ny, *AL = F + 3 * ny, *BE = F + 4 * ny, *IFD = F + 5 * ny;
+  const double pmBeta = sc->pmBeta;
+  const int Q = P - 1;
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
     double cpp = 0.0, dal = 0.0;
     for (int j = s; j <= e; ++j) {
       double a, b, c;
-      helm_abc(hc, comp, pmBeta, j, a, b, c);
+      helm_abc(hc, set, pmBeta, j, a, b, c);
       const double mm = (j == s) ? b : b - a * cpp;
       const double rm = 1.0 / mm;
       const double cp = c * rm;
@@ -294,28 +414,84 @@ __global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, HelmCoef hc, T* __r
     }
   }
   __syncthreads();
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     double m01p = 0.0, vprev = 0.0;
     for (int q = 0; q < Q; ++q) {
       const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
       const double l = -AL[eq], v = -BE[sq1];
       double d00 = 1.0, d01 = -BE[eq], d10 = -AL[sq1], d11 = 1.0;
       if (q > 0) d01 -= l * m01p * vprev;  // (L_q Minv_{q-1} U_{q-1}) has only a (0,1) entry
-      const double det = d00 * d11 - d01 * d10;
-      const double r = 1.0 / det;
-      double* R = RED + 6 * q;
+      const double r = 1.0 / (d00 * d11 - d01 * d10);
+      double* R = IFD + 6 * q;
       R[0] = d11 * r; R[1] = -d01 * r; R[2] = -d10 * r; R[3] = d00 * r; R[4] = l; R[5] = v;
       m01p = R[1]; vprev = v;
     }
   }
-  // local chunk solves for every column
+}
+
+// Interface (reduced) block-tridiagonal solve of one column, with the
+// precomputed factors; F: chunk-local solutions of the column (stride fs).
+template <class T>
+__device__ __forceinline__ void helm_interfaces(const double* __restrict__ IFD, const T* F, int fs, int ny, int P,
+                                                T* G /* 2*(P-1) */) {
+  const int Q = P - 1;
+  T gu = (T)0, gw = (T)0;
+  for (int q = 0; q < Q; ++q) {
+    const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
+    const double* R = IFD + 6 * q;
+    const T ru = F[eq * fs] - (q > 0 ? (T)R[4] * gu : (T)0);
+    const T rw = F[sq1 * fs];
+    gu = (T)R[0] * ru + (T)R[1] * rw;
+    gw = (T)R[2] * ru + (T)R[3] * rw;
+    G[2 * q] = gu;
+    G[2 * q + 1] = gw;
+  }
+  if (Q < 1) return;
+  T zw = G[2 * (Q - 1) + 1];
+  for (int q = Q - 2; q >= 0; --q) {
+    const double* R = IFD + 6 * q;
+    const T f = (T)R[5] * zw;
+    const T zu = G[2 * q] - (T)R[1] * f;
+    const T zwn = G[2 * q + 1] - (T)R[3] * f;
+    G[2 * q] = zu;
+    G[2 * q + 1] = zwn;
+    zw = zwn;
+  }
+}
+
+// clcU1Hat/U2Hat/U3Hat_PIMP from RhsX/Y/Z in memory (stage-level entry point):
+// (I - pmBeta L_y) du = Rhs ; u* = u + du written to the u* buffers.
+// Block: TI consecutive i at one k, all j; threads = TI * P; blockIdx.z = component.
+template <class T, int TI>
+__global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, const double* __restrict__ fac, int P,
+                                                   const T* __restrict__ ux, const T* __restrict__ uy,
+                                                   const T* __restrict__ uz, const T* __restrict__ rx,
+                                                   const T* __restrict__ ry, const T* __restrict__ rz,
+                                                   T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
+                                                   const DevScalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int comp = blockIdx.z;
+  const T* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
+  T* us = comp == 0 ? uxs : (comp == 1 ? uys : uzs);
+  const T* rhs = comp == 0 ? rx : (comp == 1 ? ry : rz);
+  const int nx = g.nx, ny = g.ny, k = blockIdx.y, i0 = blockIdx.x * TI, Q = P - 1;
+  const double* F64 = fac + (size_t)(comp == 1 ? 1 : 0) * helm_set_stride(ny, P);
+  const double *RM = F64, *AA = F64 + ny, *CP = F64 + 2 * ny, *AL = F64 + 3 * ny, *BE = F64 + 4 * ny,
+               *IFD = F64 + 5 * ny;
+  T* F = (T*)smem_raw;                    // ny * TI
+  T* IF = F + (size_t)ny * TI;            // TI * 2Q
+  const T add = comp == 0 ? (T)sc->dpmdxns : (T)0;
+  const int tid = threadIdx.x;
   for (int t = tid; t < TI * P; t += blockDim.x) {
-    const int ii = t % TI, p = t / TI;
+    const int ii = t % TI, p = t / TI, i = i0 + ii;
     const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
-    T d = F[s * TI + ii] * (T)RM[s];
-    F[s * TI + ii] = d;
-    for (int j = s + 1; j <= e; ++j) {
-      d = (F[j * TI + ii] - (T)AA[j] * d) * (T)RM[j];
+    T d = (T)0;
+    for (int j = s; j <= e; ++j) {
+      T f = (T)0;
+      if (i < nx) f = rhs[i + (long long)nx * (j + (long long)ny * k)] + add;
+      if (comp == 1 && j == 0) f = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
+      d = (j == s) ? f * (T)RM[j] : (f - (T)AA[j] * d) * (T)RM[j];
       F[j * TI + ii] = d;
     }
     for (int j = e - 1; j >= s; --j) {
@@ -324,46 +500,95 @@ __global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, HelmCoef hc, T* __r
     }
   }
   __syncthreads();
-  // interface system per column
-  if (tid < TI && Q > 0) {
-    const int ii = tid;
-    T gu = 0, gw = 0;
-    for (int q = 0; q < Q; ++q) {
-      const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
-      const double* R = RED + 6 * q;
-      T ru = F[eq * TI + ii] - (q > 0 ? (T)R[4] * gu : (T)0);
-      T rw = F[sq1 * TI + ii];
-      gu = (T)R[0] * ru + (T)R[1] * rw;
-      gw = (T)R[2] * ru + (T)R[3] * rw;
-      IF[(ii * Q + q) * 2 + 0] = gu;
-      IF[(ii * Q + q) * 2 + 1] = gw;
+  for (int t = tid; t < TI; t += blockDim.x) helm_interfaces<T>(IFD, F + t, TI, ny, P, IF + (size_t)t * 2 * (Q > 0 ? Q : 1));
+  __syncthreads();
+  for (int t = tid; t < ny * TI; t += blockDim.x) {
+    const int j = t / TI, ii = t % TI, i = i0 + ii;
+    if (i >= nx) continue;
+    const int p = chunk_of(j, ny, P);
+    const T* G = IF + (size_t)ii * 2 * (Q > 0 ? Q : 1);
+    T x = F[t];
+    if (p > 0) x += (T)AL[j] * G[2 * (p - 1)];
+    if (p < P - 1) x += (T)BE[j] * G[2 * p + 1];
+    const long long idx = i + (long long)nx * (j + (long long)ny * k);
+    us[idx] = u[idx] + x;
+  }
+}
+
+// clcRhsX/Y/Z fused with clcU1/2/3Hat: the right-hand sides never leave the
+// SM.  Block: one velocity component (blockIdx.x % 3, so the three blocks of
+// a column tile run back to back and share their neighbour reads in L2), TI
+// consecutive i at one k, all j.  (a) every thread evaluates RHS cells of the
+// tile into shared memory; (b) thread (ii, p) eliminates chunk p of column
+// ii; (c) per column the interface system; (d) u* = u + du.
+template <class T, int C, int TI>
+__device__ __forceinline__ void rhs_uhat_body(const Geo<T>& g, const Metrics<T>& m, const double* __restrict__ fac,
+                                              int P, const T* __restrict__ ux, const T* __restrict__ uy,
+                                              const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ h,
+                                              T* __restrict__ us, int i0, int k, const DevScalars* __restrict__ sc,
+                                              T* F, T* IF) {
+  const int nx = g.nx, ny = g.ny, Q = P - 1;
+  const int QQ = 2 * (Q > 0 ? Q : 1);
+  const double* FS = fac + (C == 1 ? helm_set_stride(ny, P) : 0);
+  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
+  const T add = C == 0 ? (T)sc->dpmdxns : (T)0;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < ny * TI; t += blockDim.x) {
+    const int j = t / TI, ii = t % TI, i = i0 + ii;
+    T r = (T)0;
+    if (i < nx) r = rhs_comp<T, C>(g, m, ux, uy, uz, pr, h, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
+    if (C == 0) r += add;
+    if (C == 1 && j == 0) r = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
+    F[t] = r;
+  }
+  __syncthreads();
+  for (int t = tid; t < TI * P; t += blockDim.x) {
+    const int ii = t % TI, p = t / TI;
+    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
+    T d = F[s * TI + ii] * (T)FS[s];
+    F[s * TI + ii] = d;
+    for (int j = s + 1; j <= e; ++j) {
+      d = (F[j * TI + ii] - (T)FS[ny + j] * d) * (T)FS[j];
+      F[j * TI + ii] = d;
     }
-    T zw = IF[(ii * Q + Q - 1) * 2 + 1];
-    for (int q = Q - 2; q >= 0; --q) {
-      const double* R = RED + 6 * q;
-      const T f = (T)R[5] * zw;
-      T zu = IF[(ii * Q + q) * 2 + 0] - (T)R[1] * f;
-      T zwn = IF[(ii * Q + q) * 2 + 1] - (T)R[3] * f;
-      IF[(ii * Q + q) * 2 + 0] = zu;
-      IF[(ii * Q + q) * 2 + 1] = zwn;
-      zw = zwn;
+    for (int j = e - 1; j >= s; --j) {
+      d = F[j * TI + ii] - (T)FS[2 * ny + j] * d;
+      F[j * TI + ii] = d;
     }
   }
   __syncthreads();
-  // reconstruct and update u
+  for (int t = tid; t < TI; t += blockDim.x) helm_interfaces<T>(FS + 5 * ny, F + t, TI, ny, P, IF + (size_t)t * QQ);
+  __syncthreads();
   for (int t = tid; t < ny * TI; t += blockDim.x) {
-    const int j = t / TI, ii = t % TI;
-    const int i = i0 + ii;
+    const int j = t / TI, ii = t % TI, i = i0 + ii;
     if (i >= nx) continue;
-    int p = (j * P) / ny;  // chunk of row j (balanced partition)
-    while (chunk_lo(p, ny, P) > j) --p;
-    while (chunk_hi(p, ny, P) < j) ++p;
+    const int p = chunk_of(j, ny, P);
+    const T* G = IF + (size_t)ii * QQ;
     T x = F[t];
-    if (p > 0) x += (T)AL[j] * IF[(ii * Q + (p - 1)) * 2 + 0];
-    if (p < P - 1) x += (T)BE[j] * IF[(ii * Q + p) * 2 + 1];
+    if (p > 0) x += (T)FS[3 * ny + j] * G[2 * (p - 1)];
+    if (p < P - 1) x += (T)FS[4 * ny + j] * G[2 * p + 1];
     const long long idx = i + (long long)nx * (j + (long long)ny * k);
-    u[idx] = u[idx] + x;
+    const T* u = C == 0 ? ux : (C == 1 ? uy : uz);
+    us[idx] = __ldg(u + idx) + x;
   }
+}
+
+template <class T, int TI>
+__global__ void __launch_bounds__(256, 4) k_rhs_uhat(Geo<T> g, Metrics<T> m, const double* __restrict__ fac, int P,
+                                                     const T* __restrict__ ux, const T* __restrict__ uy,
+                                                     const T* __restrict__ uz, const T* __restrict__ pr,
+                                                     T* __restrict__ hx, T* __restrict__ hy, T* __restrict__ hz,
+                                                     T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
+                                                     const DevScalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int comp = blockIdx.x % 3;
+  const int i0 = (blockIdx.x / 3) * TI, k = blockIdx.y;
+  T* F = (T*)smem_raw;
+  T* IF = F + (size_t)g.ny * TI;
+  if (comp == 0) rhs_uhat_body<T, 0, TI>(g, m, fac, P, ux, uy, uz, pr, hx, uxs, i0, k, sc, F, IF);
+  else if (comp == 1) rhs_uhat_body<T, 1, TI>(g, m, fac, P, ux, uy, uz, pr, hy, uys, i0, k, sc, F, IF);
+  else rhs_uhat_body<T, 2, TI>(g, m, fac, P, ux, uy, uz, pr, hz, uzs, i0, k, sc, F, IF);
 }
 
 // ---------------------------------------------------------------------------
@@ -411,18 +636,20 @@ __global__ void __launch_bounds__(256) k_prsrc_xfft(Geo<T> g, Metrics<T> m, cons
     dmax = fmax(dmax, fmax(fabs((double)r0), fabs((double)r1)));
     A[l * M + n] = mk(sudtal * r0, sudtal * r1);
   }
-  // block max of |div|
+  // block max of |div| (any block size up to 1024)
   {
-    __shared__ double red[256];
-    red[threadIdx.x] = dmax;
+    __shared__ double wred[32];
+    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    if ((threadIdx.x & 31) == 0) wred[threadIdx.x >> 5] = dmax;
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
-      __syncthreads();
+    if (threadIdx.x < 32) {
+      double v = threadIdx.x < (blockDim.x + 31) / 32 ? wred[threadIdx.x] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (threadIdx.x == 0) atomic_max_nonneg(&sc->divmax1, v);
     }
-    if (threadIdx.x == 0) atomic_max_nonneg(&sc->divmax1, red[0]);
+    __syncthreads();
   }
-  CT* Z = fft_lines<CT, false>(A, B, pl, nl, M, 1, tw);
+  const CT* Z = fft_lines<CT, false>(A, B, pl, nl, M, 1, tw);
   const T hf = (T)0.5;
   for (int t = threadIdx.x; t < nl * (M + 1); t += blockDim.x) {
     const int l = t / (M + 1), kk = t % (M + 1);
@@ -461,7 +688,7 @@ __global__ void __launch_bounds__(256) k_zfft(Geo<T> g, typename CplxOf<T>::type
     A[kz * TKX + l] = v;
   }
   __syncthreads();
-  CT* Z = fft_lines<CT, true>(A, B, pl, TKX, 1, TKX, tw);
+  const CT* Z = fft_lines<CT, true>(A, B, pl, TKX, 1, TKX, tw);
   for (int t = threadIdx.x; t < TKX * nz; t += blockDim.x) {
     const int l = t % TKX, kz = t / TKX;
     const int kx = kx0 + l;
@@ -480,7 +707,7 @@ __global__ void __launch_bounds__(256) k_zfft(Geo<T> g, typename CplxOf<T>::type
 // but with per-system factors.  Block = TS consecutive kx at one kz.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(128) k_ysolve(Geo<T> g, Metrics<double> m, const double* __restrict__ wave,
+__global__ void __launch_bounds__(256) k_ysolve(Geo<T> g, Metrics<double> m, const double* __restrict__ wave,
                                                 typename CplxOf<T>::type* __restrict__ spec, int TS, int P,
                                                 const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
@@ -584,9 +811,7 @@ __global__ void __launch_bounds__(128) k_ysolve(Geo<T> g, Metrics<double> m, con
     const int s = t % TS, j = t / TS;
     const int kx = kx0 + s;
     if (kx >= nxh) continue;
-    int p = (j * P) / ny;
-    while (chunk_lo(p, ny, P) > j) --p;
-    while (chunk_hi(p, ny, P) < j) ++p;
+    const int p = chunk_of(j, ny, P);
     double2 x = F[t];
     const double2* G = IFc + (size_t)s * Q * 2;
     if (p > 0) { const double al = AL[t]; x.x += al * G[2 * (p - 1)].x; x.y += al * G[2 * (p - 1)].y; }
@@ -626,7 +851,7 @@ __global__ void __launch_bounds__(256) k_xifft(Geo<T> g, const typename CplxOf<T
     A[l * M + kk] = cconj(z);
   }
   __syncthreads();
-  CT* Z = fft_lines<CT, false>(A, B, pl, nl, M, 1, tw);
+  const CT* Z = fft_lines<CT, false>(A, B, pl, nl, M, 1, tw);
   for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
     const int l = t / M, n = t % M;
     const CT z = cconj(Z[l * M + n]);
@@ -644,8 +869,8 @@ __global__ void __launch_bounds__(256) k_xifft(Geo<T> g, const typename CplxOf<T
 // mode 1: projection only (pmAlpha = 1, no pressure update).
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, T* __restrict__ ux, T* __restrict__ uy,
-                                              T* __restrict__ uz, T* __restrict__ pr, const T* __restrict__ phi,
+__global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* uxs, const T* uys, const T* uzs,
+                                              T* ux, T* uy, T* uz, T* __restrict__ pr, const T* __restrict__ phi,
                                               double* __restrict__ part, int mode, const DevScalars* __restrict__ sc) {
   __shared__ double red[256];
   if (sc->status) return;
@@ -665,10 +890,12 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, T* __restr
     const T phim_y = phi[i + (long long)nx * ((j > 0 ? j - 1 : 0) + (long long)ny * k)];
     const T phim_z = phi[i + (long long)nx * (j + (long long)ny * km)];
     const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha, sucacEta2 = m.rdyc[jc] * pmAlpha;
-    const T uxn = ux[idx] - (phic - phim_x) * rdxEta2;
+    const T uxn = uxs[idx] - (phic - phim_x) * rdxEta2;
+    const T uyn = uys[idx] - (phic - phim_y) * sucacEta2;
+    const T uzn = uzs[idx] - (phic - phim_z) * rdzEta2;
     ux[idx] = uxn;
-    uy[idx] = uy[idx] - (phic - phim_y) * sucacEta2;
-    uz[idx] = uz[idx] - (phic - phim_z) * rdzEta2;
+    uy[idx] = uyn;
+    uz[idx] = uzn;
     if (mode == 0) {
       const T phip_y = phi[i + (long long)nx * ((j < ny - 1 ? j + 1 : ny - 1) + (long long)ny * k)];
       const T pmBeta = (T)sc->pmBeta;
@@ -820,11 +1047,6 @@ template <> const Metrics<float>& metrics_of<float>(const ch3d_ctx* c) { return 
 static dim3 cell_grid(const ch3d_ctx* c) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz); }
 static dim3 cell_block() { return dim3(32, 8, 1); }
 
-static int pick_P(int ny) {
-  int P = 16;
-  while (P > 1 && ny < 2 * P) P >>= 1;
-  return P;
-}
 
 cudaError_t launch_step_begin(ch3d_ctx* c) {
   k_step_begin<<<1, 1, 0, c->stream>>>(c->sc, c->cfg.iCFL, c->cfg.CFLc, c->cfg.dtMax);
@@ -871,18 +1093,26 @@ template <class T> static cudaError_t rhs_t(ch3d_ctx* c) {
 }
 cudaError_t launch_rhs(ch3d_ctx* c) { return c->fp32 ? rhs_t<float>(c) : rhs_t<double>(c); }
 
-template <class T> static cudaError_t uhat_t(ch3d_ctx* c) {
-  constexpr int TI = 16;
-  T** f = (T**)c->f;
-  const int P = pick_P(c->ny), Q = P - 1;
+static HelmCoef helm_coef(const ch3d_ctx* c) {
   HelmCoef hc;
   const double* M = c->met64;
   const int L = c->ny + 3;
   // packed metric offsets, see ch3d_api.cu (pack order)
   hc.ap2p = M + 7 * L; hc.ac2p = M + 8 * L; hc.am2p = M + 9 * L;
   hc.ap2cForCN = M + 14 * L; hc.am2cForCN = M + 15 * L;
-  size_t smem = (size_t)5 * c->ny * sizeof(double) + (size_t)6 * (Q > 0 ? Q : 1) * sizeof(double) +
-                (size_t)c->ny * TI * sizeof(T) + (size_t)TI * (Q > 0 ? Q : 1) * 2 * sizeof(T) + 16;
+  return hc;
+}
+
+cudaError_t launch_helm_factors(ch3d_ctx* c) {
+  k_helm_factors<<<2, 64, 0, c->stream>>>(helm_coef(c), c->ny, c->Pv, c->hfac, c->sc);
+  return cudaGetLastError();
+}
+
+template <class T> static cudaError_t uhat_t(ch3d_ctx* c) {
+  constexpr int TI = 16;
+  T** f = (T**)c->f;
+  const int P = c->Pv, Q = P - 1;
+  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) + 16;
   static bool attr_set[2] = {false, false};
   auto kern = k_uhat_pimp<T, TI>;
   if (!attr_set[sizeof(T) == 4]) {
@@ -890,15 +1120,38 @@ template <class T> static cudaError_t uhat_t(ch3d_ctx* c) {
     attr_set[sizeof(T) == 4] = true;
   }
   dim3 grid((c->nx + TI - 1) / TI, c->nz, 3);
-  kern<<<grid, TI * P < 64 ? 64 : TI * P, smem, c->stream>>>(make_geo<T>(c), hc, f[0], f[1], f[2], f[7], f[8], f[9], P,
-                                                             c->sc);
+  int nthr = TI * P < 64 ? 64 : (TI * P > 256 ? 256 : TI * P);
+  kern<<<grid, nthr, smem, c->stream>>>(make_geo<T>(c), c->hfac, P, f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13],
+                                        f[14], c->sc);
   return cudaGetLastError();
 }
 cudaError_t launch_uhat(ch3d_ctx* c) { return c->fp32 ? uhat_t<float>(c) : uhat_t<double>(c); }
 
+template <class T> static cudaError_t rhs_uhat_t(ch3d_ctx* c) {
+  constexpr int TI = 16;
+  T** f = (T**)c->f;
+  const int P = c->Pv, Q = P - 1;
+  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) + 16;
+  static bool attr_set[2] = {false, false};
+  auto kern = k_rhs_uhat<T, TI>;
+  if (!attr_set[sizeof(T) == 4]) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set[sizeof(T) == 4] = true;
+  }
+  dim3 grid(3 * ((c->nx + TI - 1) / TI), c->nz, 1);
+  int nthr = TI * P < 64 ? 64 : (TI * P > 256 ? 256 : TI * P);
+  kern<<<grid, nthr, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), c->hfac, P, f[0], f[1], f[2], f[3], f[4],
+                                        f[5], f[6], f[12], f[13], f[14], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_rhs_uhat(ch3d_ctx* c) { return c->fp32 ? rhs_uhat_t<float>(c) : rhs_uhat_t<double>(c); }
+
+// Shared-memory budget of one FFT block (two ping-pong buffers): three
+// blocks of 256 threads fit in an SM.
+static const int kFFTSmem = 74 * 1024;
+
 template <class T> static int lines_per_block(int M) {
-  // two ping-pong buffers of M complex per line within ~96 KB
-  int lpb = (96 * 1024) / (2 * M * (int)sizeof(typename CplxOf<T>::type));
+  int lpb = kFFTSmem / (2 * M * (int)sizeof(typename CplxOf<T>::type));
   if (lpb > 16) lpb = 16;
   if (lpb < 1) lpb = 1;
   return lpb;
@@ -916,8 +1169,11 @@ template <class T> static cudaError_t prsrc_t(ch3d_ctx* c, int mode) {
     cudaFuncSetAttribute(k_prsrc_xfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set[sizeof(T) == 4] = true;
   }
-  T* src = mode == 2 ? f[10] : f[0];
-  k_prsrc_xfft<T><<<(nlines + LPB - 1) / LPB, 256, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), src, f[1], f[2],
+  const int nthr = 256;
+  T* a = mode == 2 ? f[10] : (mode == 1 ? f[0] : f[12]);
+  T* b = mode == 1 ? f[1] : f[13];
+  T* cz = mode == 1 ? f[2] : f[14];
+  k_prsrc_xfft<T><<<(nlines + LPB - 1) / LPB, nthr, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), a, b, cz,
                                                                       (CT*)c->spec, c->planx, (const CT*)c->twx,
                                                                       (const CT*)c->twr, LPB, mode, c->sc);
   return cudaGetLastError();
@@ -927,11 +1183,12 @@ cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode) { return c->fp32 ? prsrc_t<
 template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   typedef typename CplxOf<T>::type CT;
   const int nz = c->nz;
-  int TKX = (96 * 1024) / (2 * nz * (int)sizeof(CT));
+  int TKX = kFFTSmem / (2 * nz * (int)sizeof(CT));
   int t = 1;
   while (t * 2 <= TKX && t * 2 <= 16) t *= 2;
   TKX = t;
   size_t smemz = (size_t)2 * TKX * nz * sizeof(CT);
+  const int nthrz = 256;
   static bool attr_set[2] = {false, false};
   if (!attr_set[sizeof(T) == 4]) {
     cudaFuncSetAttribute(k_zfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -939,17 +1196,17 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
     attr_set[sizeof(T) == 4] = true;
   }
   dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
-  k_zfft<T><<<gz, 256, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
+  k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int TS = 8, P = pick_P(c->ny), Q = P - 1;
+  const int TS = 8, P = c->P, Q = P - 1;
   size_t smemy = (size_t)c->ny * TS * (sizeof(double2) + 2 * sizeof(double)) +
                  (size_t)TS * (Q > 0 ? Q : 1) * (2 * sizeof(double2) + 5 * sizeof(double)) + 16;
   dim3 gy((c->nxh + TS - 1) / TS, c->nz);
-  k_ysolve<T><<<gy, 128, smemy, c->stream>>>(make_geo<T>(c), c->m64, c->wave, (CT*)c->spec, TS, P, c->sc);
+  k_ysolve<T><<<gy, TS * P < 64 ? 64 : TS * P, smemy, c->stream>>>(make_geo<T>(c), c->m64, c->wave, (CT*)c->spec, TS, P, c->sc);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_zfft<T><<<gz, 256, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);
+  k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);
   return cudaGetLastError();
 }
 cudaError_t launch_poisson_spectral(ch3d_ctx* c) { return c->fp32 ? spectral_t<float>(c) : spectral_t<double>(c); }
@@ -966,7 +1223,8 @@ template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {
     cudaFuncSetAttribute(k_xifft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set[sizeof(T) == 4] = true;
   }
-  k_xifft<T><<<(nlines + LPB - 1) / LPB, 256, smem, c->stream>>>(make_geo<T>(c), (const CT*)c->spec, f[10], c->planx,
+  const int nthr = 256;
+  k_xifft<T><<<(nlines + LPB - 1) / LPB, nthr, smem, c->stream>>>(make_geo<T>(c), (const CT*)c->spec, f[10], c->planx,
                                                                  (const CT*)c->twx, (const CT*)c->twr, LPB,
                                                                  (T)c->normfft, c->sc);
   return cudaGetLastError();
@@ -975,8 +1233,9 @@ cudaError_t launch_xifft(ch3d_ctx* c) { return c->fp32 ? xifft_t<float>(c) : xif
 
 template <class T> static cudaError_t proj_t(ch3d_ctx* c, int mode) {
   T** f = (T**)c->f;
-  k_proj<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], f[3], f[10],
-                                                          c->part, mode, c->sc);
+  T* in[3] = {mode == 1 ? f[0] : f[12], mode == 1 ? f[1] : f[13], mode == 1 ? f[2] : f[14]};
+  k_proj<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1], in[2], f[0],
+                                                          f[1], f[2], f[3], f[10], c->part, mode, c->sc);
   return cudaGetLastError();
 }
 cudaError_t launch_proj(ch3d_ctx* c, int mode) { return c->fp32 ? proj_t<float>(c, mode) : proj_t<double>(c, mode); }

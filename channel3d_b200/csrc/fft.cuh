@@ -15,10 +15,21 @@ namespace ch3d {
 
 #define CH3D_MAX_PASSES 16
 
+
+// Exact integer division by a runtime constant d: q = (n * m) >> 40 with
+// m = floor(2^40 / d) + 1, exact whenever n * d < 2^40 (here n < 2^24 and
+// d < 2^16).
+__host__ __device__ inline unsigned long long fdiv_magic(unsigned d) { return ((1ull << 40) / d) + 1ull; }
+__device__ __forceinline__ int fdiv(int n, unsigned long long m) {
+  return (int)(((unsigned long long)(unsigned)n * m) >> 40);
+}
+
 struct FFTPlanDev {
   int n;                          // complex length
   int npass;
   int radix[CH3D_MAX_PASSES];
+  unsigned long long mNB[CH3D_MAX_PASSES];  // division by n / radix[p]
+  unsigned long long mNs[CH3D_MAX_PASSES];  // division by radix[0] * ... * radix[p-1]
 };
 
 template <class CT, int R> struct Bfly;
@@ -59,20 +70,22 @@ template <class CT> struct Bfly<CT, 3> {
   }
 };
 
-// One Stockham pass of radix R over `nlines` lines of length N.
-// LFAST selects the thread mapping: line index fastest (lines interleaved in
-// memory) or butterfly index fastest (lines contiguous).
+// One Stockham pass of radix R over `nlines` lines of length N, from
+// buffer src to buffer dst.  LFAST selects the thread mapping: line index
+// fastest (lines interleaved in memory) or butterfly index fastest (lines
+// contiguous).
 template <class CT, int R, bool LFAST>
 __device__ __forceinline__ void fft_pass(const CT* __restrict__ src, CT* __restrict__ dst, int N, int Ns, int nlines,
-                                         int ls, int es, const CT* __restrict__ tw) {
+                                         int ls, int es, const CT* __restrict__ tw, unsigned long long mNB,
+                                         unsigned long long mNs, unsigned long long mL) {
   const int NB = N / R;
   const int total = nlines * NB;
   const int step = N / (Ns * R);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     int l, b;
-    if (LFAST) { l = t % nlines; b = t / nlines; }
-    else { b = t % NB; l = t / NB; }
-    const int kk = b % Ns;
+    if (LFAST) { b = fdiv(t, mL); l = t - b * nlines; }
+    else { l = fdiv(t, mNB); b = t - l * NB; }
+    const int kk = b - fdiv(b, mNs) * Ns;
     CT v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[l * ls + (b + r * NB) * es];
@@ -87,16 +100,18 @@ __device__ __forceinline__ void fft_pass(const CT* __restrict__ src, CT* __restr
   }
 }
 
-// Full forward FFT of the lines in buffer a (b is scratch).  Returns the
-// buffer holding the result.  Ends with a __syncthreads().
+// Full forward FFT of the lines in buffer a (b is scratch of the same size).
+// Returns the buffer holding the result.  The caller synchronises before the
+// call; the function ends with a __syncthreads().
 template <class CT, bool LFAST>
 __device__ CT* fft_lines(CT* a, CT* b, const FFTPlanDev& pl, int nlines, int ls, int es, const CT* __restrict__ tw) {
   int Ns = 1;
+  const unsigned long long mL = fdiv_magic((unsigned)nlines);
   for (int p = 0; p < pl.npass; ++p) {
     const int R = pl.radix[p];
-    if (R == 4) fft_pass<CT, 4, LFAST>(a, b, pl.n, Ns, nlines, ls, es, tw);
-    else if (R == 2) fft_pass<CT, 2, LFAST>(a, b, pl.n, Ns, nlines, ls, es, tw);
-    else fft_pass<CT, 3, LFAST>(a, b, pl.n, Ns, nlines, ls, es, tw);
+    if (R == 4) fft_pass<CT, 4, LFAST>(a, b, pl.n, Ns, nlines, ls, es, tw, pl.mNB[p], pl.mNs[p], mL);
+    else if (R == 2) fft_pass<CT, 2, LFAST>(a, b, pl.n, Ns, nlines, ls, es, tw, pl.mNB[p], pl.mNs[p], mL);
+    else fft_pass<CT, 3, LFAST>(a, b, pl.n, Ns, nlines, ls, es, tw, pl.mNB[p], pl.mNs[p], mL);
     __syncthreads();
     CT* t = a; a = b; b = t;
     Ns *= R;

@@ -1,0 +1,151 @@
+"""Host-side checks that need no GPU: the C ABI library, the mesh, the
+namelist reader, restart files and the CPU multi-rank path."""
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from helpers import small_channel
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol(built):
+    from channel3d_b200 import _lib
+    lib = _lib.load_library()
+    hdr = open(os.path.join(ROOT, "include", "ch3d.h")).read()
+    names = re.findall(r"CH3D_API\s+(?:const\s+char\*|int)\s+(ch3d_\w+)\(", hdr)
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, n
+    assert lib.ch3d_version().startswith(b"ch3d-b200")
+
+
+def test_mesh_matches_oracle(built):
+    from channel3d_b200 import mesh_y
+    from oracle import oracle as O
+    for st, opt in (([1, 1], [0, 1]), ([0, 0], [0, 0]), ([2, 2], [0, 1]), ([3, 3], [0, 1])):
+        cfg = small_channel(16, 40, 8, StretType=st, StretOption=opt, SectioncStret=[1.2, 1.2])
+        a = mesh_y(cfg)
+        b = O.Oracle(cfg).mesh()[0]
+        assert np.array_equal(a, b), st
+
+
+def test_invalid_configs_fail_cleanly(built):
+    import ctypes
+    from channel3d_b200 import _lib
+    lib = _lib.load_library()
+    yp = np.linspace(0, 2, 13)
+    for change, code in ((dict(nxc=15), _lib.CH3D_ERR_INVALID), (dict(IsImplicit=0), _lib.CH3D_ERR_UNSUPPORTED),
+                         (dict(BcOption=[-1, -1, -1, -1, 0, 0]), _lib.CH3D_ERR_UNSUPPORTED),
+                         (dict(dtMax=-1.0), _lib.CH3D_ERR_INVALID)):
+        cfg = small_channel(16, 12, 8).copy(**change)
+        c = cfg.to_c()
+        h = ctypes.c_void_p()
+        rc = lib.ch3d_create(ctypes.byref(c), _lib.dptr(yp), ctypes.byref(h))
+        assert rc == code, (change, rc, lib.ch3d_last_error())
+        assert not h.value
+    bad = np.array([0, 1, 0.5] + [2.0] * 10)
+    c = small_channel(16, 12, 8).to_c()
+    h = ctypes.c_void_p()
+    assert lib.ch3d_create(ctypes.byref(c), _lib.dptr(bad), ctypes.byref(h)) == _lib.CH3D_ERR_INVALID
+
+
+PRM = """
+&BasicParam
+  RestartFlag = T          ! Restart or not
+  FlowType = 1
+  xlx = 6.283185307, yly = 2.0
+  zlz = 3.141592654
+  nxc = 64, nyc = 48, nzc = 32
+  xnu = 3.5714E-4
+  gravity = 0.0 0.0 0.0
+  dtMax= 0.002, iCFL = 2, CFLc = 1.0
+  ifirst= 1, ilast = 200
+  ischeme = 3, IsImplicit= 1, FFTW_plan_type = 2
+  BcOption  =   0,    0,   -1,   -1,    0,    0
+  uxBcValue = 6*0.0
+  RunName   = "Cha_test"
+  vel_limit = 2.0
+  div_limit = 0.2
+/End
+&ubulk_Param
+  IsUxConst= T
+  IsUbulkGlobal =T
+  ubulk = 1.0
+/End
+&MeshSection
+  nSection = 2
+/End
+&MeshOptions
+  SectionLength =   1     1
+  nycSection    =  24    24
+  StretType     =   1     1
+  StretOption   =   0     1
+  SectioncStret =  2.0  2.0
+/End
+&LesOptions
+  LES_type = 0
+  FilterType = 1
+/End
+"""
+
+
+def test_prm_reader(tmp_path):
+    from channel3d_b200 import ChannelConfig
+    f = tmp_path / "c.prm"
+    f.write_text(PRM)
+    cfg = ChannelConfig.from_prm(str(f))
+    assert (cfg.nxc, cfg.nyc, cfg.nzc) == (64, 48, 32)
+    assert cfg.BcOption == [0, 0, -1, -1, 0, 0]
+    assert cfg.uxBcValue == [0.0] * 6
+    assert cfg.RunName == "Cha_test" and cfg.IsUxConst is True
+    assert cfg.nycSection == [24, 24] and cfg.SectioncStret == [2.0, 2.0]
+    assert abs(cfg.xnu - 3.5714e-4) < 1e-12
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/Input"), reason="reference decks not mounted")
+def test_prm_reader_reads_reference_decks():
+    from channel3d_b200 import ChannelConfig
+    cfg = ChannelConfig.from_prm("/root/reference/Input/TurbulentChannel_2nd.prm")
+    assert (cfg.nxc, cfg.nyc, cfg.nzc) == (256, 150, 256)
+    assert cfg.IsImplicit == 1 and cfg.BcOption == [0, 0, -1, -1, 0, 0]
+    assert cfg.nycSection == [75, 75] and cfg.StretType == [1, 1]
+
+
+def test_restart_roundtrip_and_size_check(tmp_path):
+    from channel3d_b200 import restart
+    cfg = small_channel(8, 6, 4)
+    rng = np.random.default_rng(0)
+    arrs = [rng.standard_normal(cfg.shape) for _ in range(4)]
+    path = restart.restart_name(str(tmp_path), cfg.RunName, 0)
+    assert path.endswith("RestartFor" + cfg.RunName + "0000000000")
+    restart.write_restart(path, *arrs)
+    back = restart.read_restart(path, cfg)
+    for a, b in zip(arrs, back[:4]):
+        assert np.array_equal(a, b)
+    assert back[4] is None
+    with open(path, "ab") as f:
+        f.write(b"\0" * 8)
+    with pytest.raises(ValueError):
+        restart.read_restart(path, cfg)
+
+
+def test_two_rank_reference_arm_on_cpu():
+    """bench.py --impl reference under torchrun with 2 gloo ranks: rank 0 prints
+    the JSON line, rank 1 exits without work."""
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", CUDA_VISIBLE_DEVICES="")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", "29533", os.path.join(ROOT, "bench.py"),
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--workload", "channel48_les"]
+    out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    import json
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"

@@ -481,13 +481,31 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
   if (c->fp32) c->m32 = metrics_ptrs<float>((const float*)c->met, c->ny);
   else c->m32 = Metrics<float>();
   if (!c->fp32) c->m64 = metrics_ptrs<double>((const double*)c->met, c->ny);
-  c->P = 32;
-  while (c->P > 1 && c->ny < 2 * c->P) c->P >>= 1;
+  // Poisson y solve: smallest power-of-two chunk count with at most CH3D_LMAX rows per chunk
+  c->P = 2;
+  while ((c->ny + c->P - 1) / c->P > CH3D_LMAX) c->P *= 2;
+  while (c->P > 2 && c->ny < 2 * c->P) c->P >>= 1;
+  c->TSy = 256 / c->P;
+  if (c->TSy > 8) c->TSy = 8;
+  if (c->TSy < 1) c->TSy = 1;
   c->Pv = 32;
   while (c->Pv > 1 && c->ny < 2 * c->Pv) c->Pv >>= 1;
   {
     size_t nf = (size_t)2 * (5 * c->ny + 6 * (c->Pv > 1 ? c->Pv - 1 : 1));
     if (cudaMalloc(&c->hfac, nf * sizeof(double)) != cudaSuccess) return cleanup(fail(CH3D_ERR_NOMEM, "hfac"));
+  }
+  {
+    // Poisson y-solve factors per (kx, |kz|), computed once
+    if ((c->ny + c->P - 1) / c->P > CH3D_LMAX) return cleanup(fail(CH3D_ERR_UNSUPPORTED, "nyc too large for the y solve"));
+    const size_t nrow = (size_t)(c->nz / 2 + 1) * c->ny * c->nxh;
+    const size_t nif = (size_t)(c->nz / 2 + 1) * (c->P > 1 ? c->P - 1 : 1) * 6 * c->nxh;
+    if (cudaMalloc(&c->yRM, nrow * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->yCP, nrow * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->yIF, nif * sizeof(double)) != cudaSuccess)
+      return cleanup(fail(CH3D_ERR_NOMEM, "Poisson factors"));
+    c->bytes += (long long)(2 * nrow + nif) * sizeof(double);
+    e = launch_ysolve_factors(c);
+    if (e != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "Poisson factors: %s", cudaGetErrorString(e)));
   }
   {
     dim3 g((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz);
@@ -515,7 +533,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   for (int q = 0; q < 15; ++q) if (c->f[q]) cudaFree(c->f[q]);
-  void* bufs[] = {c->hfac, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  void* bufs[] = {c->hfac, c->yRM, c->yCP, c->yIF, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);

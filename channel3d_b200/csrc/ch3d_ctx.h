@@ -8,6 +8,8 @@
 #include "fft.cuh"
 
 #define CH3D_NRED 256
+// maximum rows of one chunk of the partitioned Poisson y solve (register arrays)
+#define CH3D_LMAX 12
 
 struct ch3d_ctx {
   ch3d_config cfg;
@@ -33,7 +35,11 @@ struct ch3d_ctx {
   // device buffers
   void* f[15] = {nullptr};   // ux uy uz p hx hy hz rx ry rz phi nut u*x u*y u*z (precision T)
   double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
+  double* yRM = nullptr;     // Poisson y-solve chunk factors per mode (fixed for the run)
+  double* yCP = nullptr;
+  double* yIF = nullptr;     // Poisson interface factors per mode
   int P = 16;                // chunks of the partitioned Poisson y solves
+  int TSy = 8;               // Poisson y systems per block
   int Pv = 32;               // chunks of the partitioned velocity Helmholtz solves
   void* spec = nullptr;      // complex spectrum (kx,j,kz)
   void* met = nullptr;       // packed metric vectors (precision T)
@@ -75,6 +81,7 @@ cudaError_t launch_helm_factors(ch3d_ctx* c);
 cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlpha, 1: div(u), 2: source in phi
 cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv
 cudaError_t launch_xifft(ch3d_ctx* c);
+cudaError_t launch_ysolve_factors(ch3d_ctx* c);
 cudaError_t launch_proj(ch3d_ctx* c, int mode);        // mode 0: u = u* - a grad phi, p update; 1: u -= grad phi
 cudaError_t launch_bulk_partials(ch3d_ctx* c);
 cudaError_t launch_diag(ch3d_ctx* c);

@@ -533,6 +533,7 @@ __device__ __forceinline__ void rhs_uhat_body(const Geo<T>& g, const Metrics<T>&
   const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
   const T add = C == 0 ? (T)sc->dpmdxns : (T)0;
   const int tid = threadIdx.x;
+#pragma unroll 2
   for (int t = tid; t < ny * TI; t += blockDim.x) {
     const int j = t / TI, ii = t % TI, i = i0 + ii;
     T r = (T)0;
@@ -559,17 +560,19 @@ __device__ __forceinline__ void rhs_uhat_body(const Geo<T>& g, const Metrics<T>&
   __syncthreads();
   for (int t = tid; t < TI; t += blockDim.x) helm_interfaces<T>(FS + 5 * ny, F + t, TI, ny, P, IF + (size_t)t * QQ);
   __syncthreads();
-  for (int t = tid; t < ny * TI; t += blockDim.x) {
-    const int j = t / TI, ii = t % TI, i = i0 + ii;
+  const T* u = C == 0 ? ux : (C == 1 ? uy : uz);
+  for (int t = tid; t < TI * P; t += blockDim.x) {
+    const int ii = t % TI, p = t / TI, i = i0 + ii;
     if (i >= nx) continue;
-    const int p = chunk_of(j, ny, P);
+    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
     const T* G = IF + (size_t)ii * QQ;
-    T x = F[t];
-    if (p > 0) x += (T)FS[3 * ny + j] * G[2 * (p - 1)];
-    if (p < P - 1) x += (T)FS[4 * ny + j] * G[2 * p + 1];
-    const long long idx = i + (long long)nx * (j + (long long)ny * k);
-    const T* u = C == 0 ? ux : (C == 1 ? uy : uz);
-    us[idx] = __ldg(u + idx) + x;
+    const T uL = p > 0 ? G[2 * (p - 1)] : (T)0;
+    const T wR = p < P - 1 ? G[2 * p + 1] : (T)0;
+    long long idx = i + (long long)nx * (s + (long long)ny * k);
+    for (int j = s; j <= e; ++j, idx += nx) {
+      const T x = F[j * TI + ii] + (T)FS[3 * ny + j] * uL + (T)FS[4 * ny + j] * wR;
+      us[idx] = __ldg(u + idx) + x;
+    }
   }
 }
 
@@ -817,6 +820,202 @@ __global__ void __launch_bounds__(256) k_ysolve(Geo<T> g, Metrics<double> m, con
     if (p > 0) { const double al = AL[t]; x.x += al * G[2 * (p - 1)].x; x.y += al * G[2 * (p - 1)].y; }
     if (p < P - 1) { const double be = CP[t]; x.x += be * G[2 * p + 1].x; x.y += be * G[2 * p + 1].y; }
     spec[kx + (long long)nxh * j + zs * kz] = mk((T)x.x, (T)x.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// y solve with per-mode factors precomputed once per run (the Poisson matrix
+// of mode (kx,kz) does not change during a run).  Factors depend on kz only
+// through WaveNumZ, which is even in kz, so modes kz and nz-kz share them;
+// the grid visits kz and nz-kz back to back so that the second read hits L2.
+// Layout (FP64): RM[(kzh*ny + j)*nxh + kx], CP likewise (chunk-local LU),
+// IFD[((kzh*Q + q)*6 + c)*nxh + kx] (interface block factors Minv, l, v).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int kz_of_block(int y, int nz) {
+  return y == 0 ? 0 : ((y & 1) ? (y + 1) / 2 : nz - y / 2);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_ysolve_factors(Geo<T> g, Metrics<double> m, const double* __restrict__ wave,
+                                                        double* __restrict__ RMf, double* __restrict__ CPf,
+                                                        double* __restrict__ IFf, int TS, int P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* AB = (double*)smem_raw;  // TS * P * 4 : alpha_s, alpha_e, beta_s, beta_e
+  const int nx = g.nx, ny = g.ny, nxh = g.nxh;
+  const int kx0 = blockIdx.x * TS, kzh = blockIdx.y;
+  const int Q = P - 1;
+  for (int t = threadIdx.x; t < TS * P; t += blockDim.x) {
+    const int s = t % TS, p = t / TS, kx = kx0 + s;
+    if (kx >= nxh) continue;
+    const double lam = wave[kx] + wave[nx + kzh];
+    const bool pin = (kx == 0 && kzh == 0);
+    const int jlo = chunk_lo(p, ny, P), jhi = chunk_hi(p, ny, P), L = jhi - jlo + 1;
+    double cpv[CH3D_LMAX], dav[CH3D_LMAX];
+    double cpp = 0.0, dal = 0.0;
+#pragma unroll
+    for (int q = 0; q < CH3D_LMAX; ++q) {
+      if (q < L) {
+        const int j = jlo + q, jc = j + 1;
+        double a = m.am2Pr[jc], c = m.ap2Pr[jc], b = m.ac2Pr[jc] + lam;
+        if (pin && j == 0) { a = 0.0; b = 1.0; c = 0.0; }
+        const double mm = (q == 0) ? b : b - a * cpp;
+        const double rm = 1.0 / mm;
+        const double cp = c * rm;
+        dal = (q == 0) ? -a * rm : -a * dal * rm;
+        const size_t o = ((size_t)kzh * ny + j) * nxh + kx;
+        RMf[o] = rm;
+        CPf[o] = cp;
+        cpv[q] = cp;
+        dav[q] = (p == 0) ? 0.0 : dal;
+        cpp = cp;
+      }
+    }
+    // backward spikes: alpha_j = dal_j - cp_j alpha_{j+1}, beta_j = -cp_j beta_{j+1}
+    double al = dav[0], be = 0.0, al_e = 0.0, be_e = 0.0;
+#pragma unroll
+    for (int q = CH3D_LMAX - 1; q >= 0; --q) {
+      if (q < L) {
+        if (q == L - 1) { al = dav[q]; be = (p == P - 1) ? 0.0 : -cpv[q]; al_e = al; be_e = be; }
+        else { al = dav[q] - cpv[q] * al; be = -cpv[q] * be; }
+      }
+    }
+    double* A = AB + (size_t)(s * P + p) * 4;
+    A[0] = al; A[1] = al_e; A[2] = be; A[3] = be_e;
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < TS; s += blockDim.x) {
+    const int kx = kx0 + s;
+    if (kx >= nxh) continue;
+    double m01p = 0.0, vprev = 0.0;
+    for (int q = 0; q < Q; ++q) {
+      const double* Aq = AB + (size_t)(s * P + q) * 4;       // chunk q
+      const double* Aq1 = AB + (size_t)(s * P + q + 1) * 4;  // chunk q+1
+      const double l = -Aq[1], v = -Aq1[2];
+      double d00 = 1.0, d01 = -Aq[3], d10 = -Aq1[0], d11 = 1.0;
+      if (q > 0) d01 -= l * m01p * vprev;
+      const double r = 1.0 / (d00 * d11 - d01 * d10);
+      const double R[6] = {d11 * r, -d01 * r, -d10 * r, d00 * r, l, v};
+      for (int c = 0; c < 6; ++c) IFf[(((size_t)kzh * Q + q) * 6 + c) * nxh + kx] = R[c];
+      m01p = R[1]; vprev = v;
+    }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256, 2) k_ysolve2(Geo<T> g, Metrics<double> m, const double* __restrict__ RMf,
+                                                 const double* __restrict__ CPf, const double* __restrict__ IFf,
+                                                 typename CplxOf<T>::type* __restrict__ spec, int TS, int P,
+                                                 const DevScalars* __restrict__ sc) {
+  typedef typename CplxOf<T>::type CT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  const int ny = g.ny, nz = g.nz, nxh = g.nxh;
+  const int kx0 = blockIdx.x * TS, kz = kz_of_block(blockIdx.y, nz);
+  const int kzh = kz <= nz - kz ? kz : nz - kz;
+  const int Q = P - 1, QQ = 2 * (Q > 0 ? Q : 1);
+  double2* F = (double2*)smem_raw;                 // ny * TS
+  double2* G = F + (size_t)ny * TS;                // TS * QQ
+  const long long zs = (long long)nxh * ny;
+  for (int t = threadIdx.x; t < ny * TS; t += blockDim.x) {
+    const int s = t % TS, j = t / TS, kx = kx0 + s;
+    double2 v = make_double2(0.0, 0.0);
+    if (kx < nxh) {
+      const CT c = spec[kx + (long long)nxh * j + zs * kz];
+      v = make_double2((double)c.x, (double)c.y);
+    }
+    F[t] = v;
+  }
+  __syncthreads();
+  double cpv[CH3D_LMAX], alv[CH3D_LMAX];
+  const int t0 = threadIdx.x;
+  const bool act = t0 < TS * P;
+  const int s = t0 % TS, p = t0 / TS, kx = kx0 + s;
+  const int jlo = chunk_lo(p, ny, P), jhi = chunk_hi(p, ny, P), L = jhi - jlo + 1;
+  const bool pin = (kx == 0 && kz == 0);
+  if (act && kx < nxh) {
+    double2 d = make_double2(0.0, 0.0);
+    double dal = 0.0;
+#pragma unroll
+    for (int q = 0; q < CH3D_LMAX; ++q) {
+      if (q < L) {
+        const int j = jlo + q;
+        const size_t o = ((size_t)kzh * ny + j) * nxh + kx;
+        const double rm = RMf[o];
+        cpv[q] = CPf[o];
+        double a = m.am2Pr[j + 1];
+        double2 f = F[j * TS + s];
+        if (pin && j == 0) { a = 0.0; f = make_double2(0.0, 0.0); }
+        if (q == 0) { d.x = f.x * rm; d.y = f.y * rm; dal = -a * rm; }
+        else { d.x = (f.x - a * d.x) * rm; d.y = (f.y - a * d.y) * rm; dal = -a * dal * rm; }
+        F[j * TS + s] = d;
+        alv[q] = (p == 0) ? 0.0 : dal;
+      }
+    }
+    double2 y = d;
+    double al = 0.0;
+#pragma unroll
+    for (int q = CH3D_LMAX - 1; q >= 0; --q) {
+      if (q < L) {
+        const int j = jlo + q;
+        if (q == L - 1) { al = alv[q]; }
+        else {
+          const double2 dj = F[j * TS + s];
+          y.x = dj.x - cpv[q] * y.x; y.y = dj.y - cpv[q] * y.y;
+          F[j * TS + s] = y;
+          al = alv[q] - cpv[q] * al;
+          alv[q] = al;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < TS && Q > 0) {
+    const int ss = threadIdx.x, kxs = kx0 + ss;
+    if (kxs < nxh) {
+      double2* Gs = G + (size_t)ss * QQ;
+      double2 gu = make_double2(0.0, 0.0), gw = make_double2(0.0, 0.0);
+      for (int q = 0; q < Q; ++q) {
+        const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
+        const double* R = IFf + ((size_t)kzh * Q + q) * 6 * nxh + kxs;
+        const double M00 = R[0], M01 = R[nxh], M10 = R[2 * nxh], M11 = R[3 * nxh], l = R[4 * nxh];
+        double2 ru = F[eq * TS + ss];
+        if (q > 0) { ru.x -= l * gu.x; ru.y -= l * gu.y; }
+        const double2 rw = F[sq1 * TS + ss];
+        gu = make_double2(M00 * ru.x + M01 * rw.x, M00 * ru.y + M01 * rw.y);
+        gw = make_double2(M10 * ru.x + M11 * rw.x, M10 * ru.y + M11 * rw.y);
+        Gs[2 * q] = gu; Gs[2 * q + 1] = gw;
+      }
+      double2 zw = Gs[2 * (Q - 1) + 1];
+      for (int q = Q - 2; q >= 0; --q) {
+        const double* R = IFf + ((size_t)kzh * Q + q) * 6 * nxh + kxs;
+        const double M01 = R[nxh], M11 = R[3 * nxh], v = R[5 * nxh];
+        const double fx = v * zw.x, fy = v * zw.y;
+        double2 zu = Gs[2 * q], zwn = Gs[2 * q + 1];
+        zu.x -= M01 * fx; zu.y -= M01 * fy;
+        zwn.x -= M11 * fx; zwn.y -= M11 * fy;
+        Gs[2 * q] = zu; Gs[2 * q + 1] = zwn;
+        zw = zwn;
+      }
+    }
+  }
+  __syncthreads();
+  if (act && kx < nxh) {
+    const double2* Gs = G + (size_t)s * QQ;
+    const double2 uL = p > 0 ? Gs[2 * (p - 1)] : make_double2(0.0, 0.0);
+    const double2 wR = p < P - 1 ? Gs[2 * p + 1] : make_double2(0.0, 0.0);
+    double be = 0.0;
+#pragma unroll
+    for (int q = CH3D_LMAX - 1; q >= 0; --q) {
+      if (q < L) {
+        const int j = jlo + q;
+        be = (q == L - 1) ? ((p == P - 1) ? 0.0 : -cpv[q]) : -cpv[q] * be;
+        const double2 y = F[j * TS + s];
+        const double al = alv[q];
+        const double xr = y.x + al * uL.x + be * wR.x;
+        const double xi = y.y + al * uL.y + be * wR.y;
+        spec[kx + (long long)nxh * j + zs * kz] = mk((T)xr, (T)xi);
+      }
+    }
   }
 }
 
@@ -1192,23 +1391,32 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   static bool attr_set[2] = {false, false};
   if (!attr_set[sizeof(T) == 4]) {
     cudaFuncSetAttribute(k_zfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_ysolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_ysolve2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set[sizeof(T) == 4] = true;
   }
   dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int TS = 8, P = c->P, Q = P - 1;
-  size_t smemy = (size_t)c->ny * TS * (sizeof(double2) + 2 * sizeof(double)) +
-                 (size_t)TS * (Q > 0 ? Q : 1) * (2 * sizeof(double2) + 5 * sizeof(double)) + 16;
+  const int P = c->P, TS = c->TSy, Q = P - 1;
+  size_t smemy = (size_t)c->ny * TS * sizeof(double2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(double2) + 16;
   dim3 gy((c->nxh + TS - 1) / TS, c->nz);
-  k_ysolve<T><<<gy, TS * P < 64 ? 64 : TS * P, smemy, c->stream>>>(make_geo<T>(c), c->m64, c->wave, (CT*)c->spec, TS, P, c->sc);
+  k_ysolve2<T><<<gy, TS * P < 64 ? 64 : TS * P, smemy, c->stream>>>(make_geo<T>(c), c->m64, c->yRM, c->yCP, c->yIF,
+                                                                   (CT*)c->spec, TS, P, c->sc);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);
   return cudaGetLastError();
 }
+template <class T> static cudaError_t yfactors_t(ch3d_ctx* c) {
+  const int TS = c->TSy, P = c->P;
+  dim3 grid((c->nxh + TS - 1) / TS, c->nz / 2 + 1);
+  k_ysolve_factors<T><<<grid, TS * P < 64 ? 64 : TS * P, (size_t)TS * P * 4 * sizeof(double), c->stream>>>(
+      make_geo<T>(c), c->m64, c->wave, c->yRM, c->yCP, c->yIF, TS, P);
+  return cudaGetLastError();
+}
+cudaError_t launch_ysolve_factors(ch3d_ctx* c) { return c->fp32 ? yfactors_t<float>(c) : yfactors_t<double>(c); }
+
 cudaError_t launch_poisson_spectral(ch3d_ctx* c) { return c->fp32 ? spectral_t<float>(c) : spectral_t<double>(c); }
 
 template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {

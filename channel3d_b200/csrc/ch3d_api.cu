@@ -785,6 +785,27 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
   return fetch_info(c, nullptr);
 }
 
+int ch3d_poisson_noalloc(int nxc, int nyc, int nzc, double xlx, double zlz, const double* yp, int bc_ym, int bc_yp,
+                         const double* d_src, double* d_phi, void* stream) {
+  if (!yp || !d_src || !d_phi) return fail(CH3D_ERR_INVALID, "NULL argument");
+  if (nxc < 4 || nyc < 4 || nzc < 2 || (nxc % 2)) return fail(CH3D_ERR_INVALID, "bad grid %d %d %d", nxc, nyc, nzc);
+  if (!(xlx > 0) || !(zlz > 0)) return fail(CH3D_ERR_INVALID, "bad domain lengths");
+  if ((bc_ym != -1 && bc_ym != -2) || (bc_yp != -1 && bc_yp != -2))
+    return fail(CH3D_ERR_UNSUPPORTED, "y boundaries must be no-slip (-1) or free-slip (-2)");
+  for (int j = 1; j <= nyc; ++j)
+    if (!(yp[j] > yp[j - 1])) return fail(CH3D_ERR_INVALID, "yp must increase");
+  FFTPlanDev px, pz;
+  if (!factor23(nxc / 2, px) || !factor23(nzc, pz))
+    return fail(CH3D_ERR_UNSUPPORTED, "nxc/2 and nzc must be products of 2 and 3");
+  const size_t need = noalloc_bytes(nxc, nyc, nzc);
+  if (need > (size_t)CH3D_NOALLOC_SCRATCH_BYTES)
+    return fail(CH3D_ERR_INVALID, "grid %d x %d x %d needs %zu bytes of scratch, more than the %u bytes of "
+                "CH3D_NOALLOC_SCRATCH_BYTES", nxc, nyc, nzc, need, (unsigned)CH3D_NOALLOC_SCRATCH_BYTES);
+  cudaError_t e = poisson_noalloc(nxc, nyc, nzc, xlx, zlz, yp, bc_ym, bc_yp, d_src, d_phi, (cudaStream_t)stream, px, pz);
+  if (e != cudaSuccess) return fail(CH3D_ERR_CUDA, "ch3d_poisson_noalloc: %s", cudaGetErrorString(e));
+  return CH3D_OK;
+}
+
 int ch3d_last_step_ms(ch3d_ctx* c, double* ms) {
   if (!c || !ms) return fail(CH3D_ERR_INVALID, "NULL argument");
   *ms = c->last_ms;

@@ -82,6 +82,12 @@ cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlph
 cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv
 cudaError_t launch_xifft(ch3d_ctx* c);
 cudaError_t launch_ysolve_factors(ch3d_ctx* c);
+// allocation-free Poisson solve (static device scratch, ch3d_step.cu)
+size_t noalloc_bytes(int nx, int ny, int nz);
+cudaError_t noalloc_scratch_address(int dev, void** out);
+cudaError_t poisson_noalloc(int nx, int ny, int nz, double xlx, double zlz, const double* yp, int bclo, int bchi,
+                            const double* d_src, double* d_phi, cudaStream_t st, const FFTPlanDev& planx,
+                            const FFTPlanDev& planz);
 cudaError_t launch_proj(ch3d_ctx* c, int mode);        // mode 0: u = u* - a grad phi, p update; 1: u -= grad phi
 cudaError_t launch_bulk_partials(ch3d_ctx* c);
 cudaError_t launch_diag(ch3d_ctx* c);

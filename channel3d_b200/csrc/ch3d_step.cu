@@ -13,7 +13,11 @@
 //   proj           FluidVelUpdate + PressureUpdate_PIMP + next bulk partial sums
 // and per step: step_begin (CalcMaxCFL/dt), diag (CheckDivergence, CalcVmax,
 // CalcUxAver, next CFL), step_end (limit checks).
+#include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
 #include "ch3d_ctx.h"
 
 namespace ch3d {
@@ -1471,6 +1475,154 @@ template <class T> static cudaError_t divmax_t(ch3d_ctx* c, unsigned long long* 
 }
 cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot) {
   return c->fp32 ? divmax_t<float>(c, slot) : divmax_t<double>(c, slot);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free Poisson solve (ch3d_poisson_noalloc in include/ch3d.h).
+// Its working memory is this file-scope device array, present on every GPU
+// that loads the library until the process exits.  In host code the name
+// g_noalloc_scratch is only a host-side stand-in for the symbol; the device
+// address is obtained once per device with cudaGetSymbolAddress (with that
+// device current) and cached.  All calls share the array.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CH3D_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[128] = {nullptr};
+
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+}  // namespace
+
+cudaError_t noalloc_scratch_address(int dev, void** out) {
+  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return cudaSuccess;
+}
+
+// Bytes of scratch the solve of an nx x ny x nz grid needs.
+size_t noalloc_bytes(int nx, int ny, int nz) {
+  const int nxh = nx / 2 + 1, M = nx / 2;
+  size_t b = align256((size_t)nxh * ny * nz * sizeof(double2));
+  b += align256((size_t)4 * (ny + 3) * sizeof(double));     // rdyp, am2Pr, ac2Pr, ap2Pr
+  b += align256((size_t)(nx + nz) * sizeof(double));        // WaveNumX | WaveNumZ
+  b += align256((size_t)(M + M + 1 + nz) * sizeof(double2)); // twiddles
+  b += align256(sizeof(DevScalars));
+  return b;
+}
+
+cudaError_t poisson_noalloc(int nx, int ny, int nz, double xlx, double zlz, const double* yp, int bclo, int bchi,
+                            const double* d_src, double* d_phi, cudaStream_t st, const FFTPlanDev& planx,
+                            const FFTPlanDev& planz) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  void* base = nullptr;
+  e = noalloc_scratch_address(dev, &base);
+  if (e != cudaSuccess) return e;
+  const int nxh = nx / 2 + 1, M = nx / 2, L = ny + 3;
+  unsigned char* p = (unsigned char*)base;
+  double2* spec = (double2*)p;
+  p += align256((size_t)nxh * ny * nz * sizeof(double2));
+  double* met = (double*)p;
+  p += align256((size_t)4 * L * sizeof(double));
+  double* wave = (double*)p;
+  p += align256((size_t)(nx + nz) * sizeof(double));
+  double2* tw = (double2*)p;
+  p += align256((size_t)(M + M + 1 + nz) * sizeof(double2));
+  DevScalars* sc = (DevScalars*)p;
+
+  // host tables: the Poisson metrics of InitMeshAndMetries (m_MeshAndMetries.f90:186-240),
+  // the modified wavenumbers (m_Poisson.f90:38-66) and the FFT twiddles
+  std::vector<double> h(4 * (size_t)L, 0.0), dyp(L, 0.0), dyc(L, 0.0), yc(L, 0.0), rdyc(L, 0.0);
+  const int nyp = ny + 1;
+  auto Y = [&](int j) { return yp[j - 1]; };
+  for (int j = 1; j <= ny; ++j) { yc[j] = 0.5 * (Y(j) + Y(j + 1)); dyp[j] = Y(j + 1) - Y(j); }
+  dyp[0] = dyp[1]; dyp[nyp] = dyp[ny];
+  for (int j = 2; j <= ny; ++j) dyc[j] = yc[j] - yc[j - 1];
+  dyc[1] = dyp[1]; dyc[nyp] = dyp[ny];
+  double* rdyp = h.data();
+  double *am = h.data() + L, *ac = h.data() + 2 * L, *ap = h.data() + 3 * L;
+  for (int j = 0; j <= nyp; ++j) rdyp[j] = 1.0 / dyp[j];
+  for (int j = 1; j <= nyp; ++j) rdyc[j] = 1.0 / dyc[j];
+  for (int j = 1; j <= ny; ++j) { am[j] = rdyp[j] * rdyc[j]; ap[j] = rdyp[j] * rdyc[j + 1]; }
+  if (bclo != 0) { am[1] = 0.0; ap[1] = rdyp[1] * rdyc[2]; }
+  if (bchi != 0) { am[ny] = rdyp[ny] * rdyc[ny]; ap[ny] = 0.0; }
+  for (int j = 1; j <= ny; ++j) ac[j] = -(am[j] + ap[j]);
+  const double PIv = 3.141592653589793238462643383279502884;
+  const double rdx = (double)nx / xlx, rdz = (double)nz / zlz;
+  std::vector<double> w(nx + nz);
+  for (int i = 0; i < nx; ++i) w[i] = 2.0 * rdx * rdx * (std::cos(2.0 * PIv * (double)i / (double)nx) - 1.0);
+  for (int k = 0; k < nz; ++k) w[nx + k] = 2.0 * rdz * rdz * (std::cos(2.0 * PIv * (double)k / (double)nz) - 1.0);
+  std::vector<double2> t(M + M + 1 + nz);
+  auto fill = [&](double2* o, int n, int cnt) {
+    for (int q = 0; q < cnt; ++q) {
+      long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)q / (long double)n;
+      o[q] = make_double2((double)cosl(ang), (double)sinl(ang));
+    }
+  };
+  fill(t.data(), M, M);
+  fill(t.data() + M, nx, M + 1);
+  fill(t.data() + 2 * M + 1, nz, nz);
+  if ((e = cudaMemcpyAsync(met, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(wave, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(tw, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  // what must start at zero: the status word and the divergence maximum
+  if ((e = cudaMemsetAsync(sc, 0, sizeof(DevScalars), st)) != cudaSuccess) return e;
+
+  Geo<double> g;
+  std::memset(&g, 0, sizeof(g));
+  g.nx = nx; g.ny = ny; g.nz = nz; g.nxh = nxh; g.N = (long long)nx * ny * nz;
+  g.rdx = rdx; g.rdz = rdz; g.rdx2 = rdx * rdx; g.rdz2 = rdz * rdz;
+  g.bc.lo = bclo; g.bc.hi = bchi;
+  g.bc.dyp1 = dyp[1]; g.bc.dypN = dyp[nyp];
+  Metrics<double> m;
+  std::memset(&m, 0, sizeof(m));
+  m.rdyp = met; m.am2Pr = met + L; m.ac2Pr = met + 2 * L; m.ap2Pr = met + 3 * L;
+  const double2* twx = tw;
+  const double2* twr = tw + M;
+  const double2* twz = tw + 2 * M + 1;
+
+  // forward x transform of the source (mode 2: the source is read as is)
+  const int LPB = lines_per_block<double>(M);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_prsrc_xfft<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_zfft<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_ysolve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_xifft<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  const int nlines = ny * nz;
+  k_prsrc_xfft<double><<<(nlines + LPB - 1) / LPB, 256, (size_t)2 * LPB * M * sizeof(double2), st>>>(
+      g, m, d_src, d_src, d_src, spec, planx, twx, twr, LPB, 2, sc);
+  int TKX = kFFTSmem / (2 * nz * (int)sizeof(double2));
+  int tk = 1;
+  while (tk * 2 <= TKX && tk * 2 <= 16) tk *= 2;
+  TKX = tk;
+  dim3 gz((nxh + TKX - 1) / TKX, ny);
+  const size_t smz = (size_t)2 * TKX * nz * sizeof(double2);
+  k_zfft<double><<<gz, 256, smz, st>>>(g, spec, planz, twz, TKX, 0, sc);
+  int P = 16;
+  while (P > 1 && ny < 2 * P) P >>= 1;
+  const int TS = 8, Q = P - 1;
+  const size_t smy = (size_t)ny * TS * (sizeof(double2) + 2 * sizeof(double)) +
+                     (size_t)TS * (Q > 0 ? Q : 1) * (2 * sizeof(double2) + 5 * sizeof(double)) + 16;
+  k_ysolve<double><<<dim3((nxh + TS - 1) / TS, nz), TS * P < 64 ? 64 : TS * P, smy, st>>>(g, m, wave, spec, TS, P, sc);
+  k_zfft<double><<<gz, 256, smz, st>>>(g, spec, planz, twz, TKX, 1, sc);
+  k_xifft<double><<<(nlines + LPB - 1) / LPB, 256, (size_t)2 * LPB * M * sizeof(double2), st>>>(
+      g, spec, d_phi, planx, twx, twr, LPB, 1.0 / ((double)nx * (double)nz), sc);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // the host tables above are pageable and local to this call
+  return cudaStreamSynchronize(st);
 }
 
 }  // namespace ch3d

@@ -190,6 +190,30 @@ CH3D_API int ch3d_memory_bytes(ch3d_ctx* ctx, long long* bytes);
    The steps advance the state like ch3d_step. */
 CH3D_API int ch3d_kernel_times(ch3d_ctx* ctx, int nsteps, double* out, int nout);
 
+/* Allocation-free pressure Poisson solve: the solve of ch3d_poisson
+   (periodic x and z, walls in y) for callers that cannot allocate device
+   memory themselves, such as a host whose device memory is owned and fully
+   reserved by another runtime, or a process in which every device allocation
+   must go through the host application's own allocator.  It needs no context:
+   the caller passes the grid (yp = yp(1:nyc+1)), the y boundary types
+   (BcOption(3), BcOption(4): -1 no-slip, -2 free-slip) and DEVICE pointers to
+   src and phi (nxc*nyc*nzc doubles each, interior layout), and `stream`
+   (a cudaStream_t, or NULL for the legacy default stream) on the current
+   device.  The call makes no device allocation of its own: its working memory
+   is one file-scope device array of CH3D_NOALLOC_SCRATCH_BYTES in the library,
+   which every GPU that loads the library holds until the process exits.  Grids
+   whose spectrum and tables do not fit in it are rejected with
+   CH3D_ERR_INVALID.  The first call on a device looks up the array's device
+   address (cudaGetSymbolAddress) with that device current; make that first
+   call before any stream capture.  All calls share the array and each call
+   overwrites it, so calls whose work overlaps on the GPU (other streams,
+   other host threads) race; serialise them.  The call returns after its work
+   on `stream` has completed.  It has no counterpart in the reference. */
+#define CH3D_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+CH3D_API int ch3d_poisson_noalloc(int nxc, int nyc, int nzc, double xlx, double zlz,
+                                  const double* yp, int bc_ym, int bc_yp,
+                                  const double* d_src, double* d_phi, void* stream);
+
 /* Time of the last ch3d_step call's kernels, measured with CUDA events on the
    context's stream (milliseconds). */
 CH3D_API int ch3d_last_step_ms(ch3d_ctx* ctx, double* ms);

@@ -478,6 +478,7 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     cudaMemcpy(c->wave, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice);
   }
   c->m64 = metrics_ptrs<double>(c->met64, c->ny);
+  c->m64full = c->m64;
   if (c->fp32) c->m32 = metrics_ptrs<float>((const float*)c->met, c->ny);
   else c->m32 = Metrics<float>();
   if (!c->fp32) c->m64 = metrics_ptrs<double>((const double*)c->met, c->ny);
@@ -499,11 +500,23 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     if ((c->ny + c->P - 1) / c->P > CH3D_LMAX) return cleanup(fail(CH3D_ERR_UNSUPPORTED, "nyc too large for the y solve"));
     const size_t nrow = (size_t)(c->nz / 2 + 1) * c->ny * c->nxh;
     const size_t nif = (size_t)(c->nz / 2 + 1) * (c->P > 1 ? c->P - 1 : 1) * 6 * c->nxh;
-    if (cudaMalloc(&c->yRM, nrow * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&c->yCP, nrow * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&c->yIF, nif * sizeof(double)) != cudaSuccess)
+    const size_t fw = c->fp32 ? sizeof(float) : sizeof(double);
+    if (cudaMalloc(&c->yRM, nrow * fw) != cudaSuccess || cudaMalloc(&c->yCP, nrow * fw) != cudaSuccess ||
+        cudaMalloc(&c->yIF, nif * fw) != cudaSuccess)
       return cleanup(fail(CH3D_ERR_NOMEM, "Poisson factors"));
-    c->bytes += (long long)(2 * nrow + nif) * sizeof(double);
+    c->bytes += (long long)(2 * nrow + nif) * fw;
+    if (c->fp32) {
+      // low modes kept in FP64: kx < TSy, |kz| <= KL (KL < nz/2 so the two kz ranges are disjoint)
+      c->KL = 8;
+      if (c->KL > c->nz / 2 - 1) c->KL = c->nz / 2 - 1;
+      if (c->KL < 0) c->KL = 0;
+      const size_t lr = (size_t)(c->KL + 1) * c->ny * c->TSy;
+      const size_t li = (size_t)(c->KL + 1) * (c->P > 1 ? c->P - 1 : 1) * 6 * c->TSy;
+      if (cudaMalloc(&c->yRM64, lr * sizeof(double)) != cudaSuccess ||
+          cudaMalloc(&c->yCP64, lr * sizeof(double)) != cudaSuccess ||
+          cudaMalloc(&c->yIF64, li * sizeof(double)) != cudaSuccess)
+        return cleanup(fail(CH3D_ERR_NOMEM, "Poisson low-mode factors"));
+    }
     e = launch_ysolve_factors(c);
     if (e != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "Poisson factors: %s", cudaGetErrorString(e)));
   }
@@ -516,6 +529,12 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
         cudaMalloc(&c->red2, CH3D_NRED * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->sc, sizeof(DevScalars)) != cudaSuccess)
       return cleanup(fail(CH3D_ERR_NOMEM, "partials"));
+    const size_t nstat = (size_t)35 * (c->ny + 1) + 1;  // SumStat(35, nyp) | PrGradsum
+    const int kch = (c->nz + 7) / 8, nch = (c->nz + kch - 1) / kch;
+    if (cudaMalloc(&c->stat, nstat * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->statpart, (size_t)35 * (c->ny + 1) * nch * sizeof(double)) != cudaSuccess)
+      return cleanup(fail(CH3D_ERR_NOMEM, "statistics"));
+    cudaMemsetAsync(c->stat, 0, nstat * sizeof(double), c->stream);
     cudaMemsetAsync(c->part, 0, (size_t)c->npart * sizeof(double), c->stream);
     cudaMemsetAsync(c->part2, 0, (size_t)c->npart * sizeof(double), c->stream);
     cudaMemsetAsync(c->sc, 0, sizeof(DevScalars), c->stream);
@@ -533,7 +552,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   for (int q = 0; q < 15; ++q) if (c->f[q]) cudaFree(c->f[q]);
-  void* bufs[] = {c->hfac, c->yRM, c->yCP, c->yIF, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  void* bufs[] = {c->hfac, c->yRM, c->yCP, c->yIF, c->yRM64, c->yCP64, c->yIF64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -726,13 +745,30 @@ int ch3d_set_dt(ch3d_ctx* c, double dt) {
 
 int ch3d_stats_accumulate(ch3d_ctx* c) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
-  return fail(CH3D_ERR_UNSUPPORTED, "statistics not built yet");
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
+  CU(launch_stats(c));
+  CU(cudaStreamSynchronize(c->stream));
+  c->nfstime += 1;
+  return CH3D_OK;
 }
 
 int ch3d_stats_fetch(ch3d_ctx* c, double* sumstat, int* nfstime, double* prgradsum, int reset) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
-  (void)sumstat; (void)nfstime; (void)prgradsum; (void)reset;
-  return fail(CH3D_ERR_UNSUPPORTED, "statistics not built yet");
+  CU(cudaSetDevice(c->device));
+  const size_t n = (size_t)35 * (c->ny + 1);
+  std::vector<double> h(n + 1);
+  CU(cudaMemcpyAsync(h.data(), c->stat, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  if (sumstat) std::memcpy(sumstat, h.data(), n * sizeof(double));
+  if (prgradsum) *prgradsum = h[n];
+  if (nfstime) *nfstime = c->nfstime;
+  if (reset) {
+    CU(cudaMemsetAsync(c->stat, 0, (n + 1) * sizeof(double), c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    c->nfstime = 0;
+  }
+  return CH3D_OK;
 }
 
 int ch3d_memory_bytes(ch3d_ctx* c, long long* bytes) {

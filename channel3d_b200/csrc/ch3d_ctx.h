@@ -35,9 +35,13 @@ struct ch3d_ctx {
   // device buffers
   void* f[15] = {nullptr};   // ux uy uz p hx hy hz rx ry rz phi nut u*x u*y u*z (precision T)
   double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
-  double* yRM = nullptr;     // Poisson y-solve chunk factors per mode (fixed for the run)
-  double* yCP = nullptr;
-  double* yIF = nullptr;     // Poisson interface factors per mode
+  void* yRM = nullptr;       // Poisson y-solve chunk factors per mode (fixed for the run);
+  void* yCP = nullptr;       // FP64, or FP32 in the mixed path
+  void* yIF = nullptr;       // Poisson interface factors per mode
+  double* yRM64 = nullptr;   // mixed path: FP64 factors of the low modes (kx tile 0, |kz| <= KL)
+  double* yCP64 = nullptr;
+  double* yIF64 = nullptr;
+  int KL = 8;
   int P = 16;                // chunks of the partitioned Poisson y solves
   int TSy = 8;               // Poisson y systems per block
   int Pv = 32;               // chunks of the partitioned velocity Helmholtz solves
@@ -62,6 +66,7 @@ struct ch3d_ctx {
 
   ch3d::FFTPlanDev planx, planz;
   ch3d::Metrics<double> m64;
+  ch3d::Metrics<double> m64full;  // FP64 metrics (always the FP64 copy)
   ch3d::Metrics<float> m32;
 
   cudaGraph_t graph = nullptr;

@@ -839,18 +839,20 @@ __device__ __forceinline__ int kz_of_block(int y, int nz) {
   return y == 0 ? 0 : ((y & 1) ? (y + 1) / 2 : nz - y / 2);
 }
 
-template <class T>
+// Factors of the systems (kx, kzh) with kx in [0, kxn) and kzh = blockIdx.y,
+// stored in precision R with leading dimension ldx.
+template <class T, class R>
 __global__ void __launch_bounds__(256) k_ysolve_factors(Geo<T> g, Metrics<double> m, const double* __restrict__ wave,
-                                                        double* __restrict__ RMf, double* __restrict__ CPf,
-                                                        double* __restrict__ IFf, int TS, int P) {
+                                                        R* __restrict__ RMf, R* __restrict__ CPf, R* __restrict__ IFf,
+                                                        int TS, int P, int ldx, int kxn) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* AB = (double*)smem_raw;  // TS * P * 4 : alpha_s, alpha_e, beta_s, beta_e
-  const int nx = g.nx, ny = g.ny, nxh = g.nxh;
+  const int nx = g.nx, ny = g.ny;
   const int kx0 = blockIdx.x * TS, kzh = blockIdx.y;
   const int Q = P - 1;
   for (int t = threadIdx.x; t < TS * P; t += blockDim.x) {
     const int s = t % TS, p = t / TS, kx = kx0 + s;
-    if (kx >= nxh) continue;
+    if (kx >= kxn) continue;
     const double lam = wave[kx] + wave[nx + kzh];
     const bool pin = (kx == 0 && kzh == 0);
     const int jlo = chunk_lo(p, ny, P), jhi = chunk_hi(p, ny, P), L = jhi - jlo + 1;
@@ -866,15 +868,14 @@ __global__ void __launch_bounds__(256) k_ysolve_factors(Geo<T> g, Metrics<double
         const double rm = 1.0 / mm;
         const double cp = c * rm;
         dal = (q == 0) ? -a * rm : -a * dal * rm;
-        const size_t o = ((size_t)kzh * ny + j) * nxh + kx;
-        RMf[o] = rm;
-        CPf[o] = cp;
+        const size_t o = ((size_t)kzh * ny + j) * ldx + kx;
+        RMf[o] = (R)rm;
+        CPf[o] = (R)cp;
         cpv[q] = cp;
         dav[q] = (p == 0) ? 0.0 : dal;
         cpp = cp;
       }
     }
-    // backward spikes: alpha_j = dal_j - cp_j alpha_{j+1}, beta_j = -cp_j beta_{j+1}
     double al = dav[0], be = 0.0, al_e = 0.0, be_e = 0.0;
 #pragma unroll
     for (int q = CH3D_LMAX - 1; q >= 0; --q) {
@@ -889,7 +890,7 @@ __global__ void __launch_bounds__(256) k_ysolve_factors(Geo<T> g, Metrics<double
   __syncthreads();
   for (int s = threadIdx.x; s < TS; s += blockDim.x) {
     const int kx = kx0 + s;
-    if (kx >= nxh) continue;
+    if (kx >= kxn) continue;
     double m01p = 0.0, vprev = 0.0;
     for (int q = 0; q < Q; ++q) {
       const double* Aq = AB + (size_t)(s * P + q) * 4;       // chunk q
@@ -898,72 +899,85 @@ __global__ void __launch_bounds__(256) k_ysolve_factors(Geo<T> g, Metrics<double
       double d00 = 1.0, d01 = -Aq[3], d10 = -Aq1[0], d11 = 1.0;
       if (q > 0) d01 -= l * m01p * vprev;
       const double r = 1.0 / (d00 * d11 - d01 * d10);
-      const double R[6] = {d11 * r, -d01 * r, -d10 * r, d00 * r, l, v};
-      for (int c = 0; c < 6; ++c) IFf[(((size_t)kzh * Q + q) * 6 + c) * nxh + kx] = R[c];
-      m01p = R[1]; vprev = v;
+      const double Rv[6] = {d11 * r, -d01 * r, -d10 * r, d00 * r, l, v};
+      for (int c = 0; c < 6; ++c) IFf[(((size_t)kzh * Q + q) * 6 + c) * ldx + kx] = (R)Rv[c];
+      m01p = Rv[1]; vprev = v;
     }
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(256, 2) k_ysolve2(Geo<T> g, Metrics<double> m, const double* __restrict__ RMf,
-                                                 const double* __restrict__ CPf, const double* __restrict__ IFf,
-                                                 typename CplxOf<T>::type* __restrict__ spec, int TS, int P,
-                                                 const DevScalars* __restrict__ sc) {
+template <class R> struct Vec2Of;
+template <> struct Vec2Of<double> { typedef double2 type; };
+template <> struct Vec2Of<float> { typedef float2 type; };
+
+// sel: 0 every (kx tile, kz) block; 1 only the low-mode blocks (kx tile 0,
+// kz in [0,KL] or [nz-KL, nz)), grid.y enumerating them; 2 every block but those.
+template <class T, class R>
+__global__ void __launch_bounds__(256, 2) k_ysolve2(Geo<T> g, Metrics<double> m, const R* __restrict__ RMf,
+                                                    const R* __restrict__ CPf, const R* __restrict__ IFf, int ldx,
+                                                    typename CplxOf<T>::type* __restrict__ spec, int TS, int P,
+                                                    int sel, int KL, const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
+  typedef typename Vec2Of<R>::type V2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (sc->status) return;
   const int ny = g.ny, nz = g.nz, nxh = g.nxh;
-  const int kx0 = blockIdx.x * TS, kz = kz_of_block(blockIdx.y, nz);
+  int kz;
+  if (sel == 1) kz = (int)blockIdx.y <= KL ? (int)blockIdx.y : nz - ((int)blockIdx.y - KL);
+  else kz = kz_of_block(blockIdx.y, nz);
   const int kzh = kz <= nz - kz ? kz : nz - kz;
+  if (sel == 2 && blockIdx.x == 0 && kzh <= KL) return;
+  const int kx0 = blockIdx.x * TS;
   const int Q = P - 1, QQ = 2 * (Q > 0 ? Q : 1);
-  double2* F = (double2*)smem_raw;                 // ny * TS
-  double2* G = F + (size_t)ny * TS;                // TS * QQ
+  V2* F = (V2*)smem_raw;                 // ny * TS
+  V2* G = F + (size_t)ny * TS;           // TS * QQ
   const long long zs = (long long)nxh * ny;
   for (int t = threadIdx.x; t < ny * TS; t += blockDim.x) {
     const int s = t % TS, j = t / TS, kx = kx0 + s;
-    double2 v = make_double2(0.0, 0.0);
+    V2 v;
+    v.x = (R)0; v.y = (R)0;
     if (kx < nxh) {
       const CT c = spec[kx + (long long)nxh * j + zs * kz];
-      v = make_double2((double)c.x, (double)c.y);
+      v.x = (R)c.x; v.y = (R)c.y;
     }
     F[t] = v;
   }
   __syncthreads();
-  double cpv[CH3D_LMAX], alv[CH3D_LMAX];
+  R cpv[CH3D_LMAX], alv[CH3D_LMAX];
   const int t0 = threadIdx.x;
   const bool act = t0 < TS * P;
   const int s = t0 % TS, p = t0 / TS, kx = kx0 + s;
   const int jlo = chunk_lo(p, ny, P), jhi = chunk_hi(p, ny, P), L = jhi - jlo + 1;
   const bool pin = (kx == 0 && kz == 0);
   if (act && kx < nxh) {
-    double2 d = make_double2(0.0, 0.0);
-    double dal = 0.0;
+    V2 d;
+    d.x = (R)0; d.y = (R)0;
+    R dal = (R)0;
 #pragma unroll
     for (int q = 0; q < CH3D_LMAX; ++q) {
       if (q < L) {
         const int j = jlo + q;
-        const size_t o = ((size_t)kzh * ny + j) * nxh + kx;
-        const double rm = RMf[o];
+        const size_t o = ((size_t)kzh * ny + j) * ldx + kx;
+        const R rm = RMf[o];
         cpv[q] = CPf[o];
-        double a = m.am2Pr[j + 1];
-        double2 f = F[j * TS + s];
-        if (pin && j == 0) { a = 0.0; f = make_double2(0.0, 0.0); }
+        R a = (R)m.am2Pr[j + 1];
+        V2 f = F[j * TS + s];
+        if (pin && j == 0) { a = (R)0; f.x = (R)0; f.y = (R)0; }
         if (q == 0) { d.x = f.x * rm; d.y = f.y * rm; dal = -a * rm; }
         else { d.x = (f.x - a * d.x) * rm; d.y = (f.y - a * d.y) * rm; dal = -a * dal * rm; }
         F[j * TS + s] = d;
-        alv[q] = (p == 0) ? 0.0 : dal;
+        alv[q] = (p == 0) ? (R)0 : dal;
       }
     }
-    double2 y = d;
-    double al = 0.0;
+    V2 y = d;
+    R al = (R)0;
 #pragma unroll
     for (int q = CH3D_LMAX - 1; q >= 0; --q) {
       if (q < L) {
         const int j = jlo + q;
         if (q == L - 1) { al = alv[q]; }
         else {
-          const double2 dj = F[j * TS + s];
+          const V2 dj = F[j * TS + s];
           y.x = dj.x - cpv[q] * y.x; y.y = dj.y - cpv[q] * y.y;
           F[j * TS + s] = y;
           al = alv[q] - cpv[q] * al;
@@ -976,25 +990,26 @@ __global__ void __launch_bounds__(256, 2) k_ysolve2(Geo<T> g, Metrics<double> m,
   if (threadIdx.x < TS && Q > 0) {
     const int ss = threadIdx.x, kxs = kx0 + ss;
     if (kxs < nxh) {
-      double2* Gs = G + (size_t)ss * QQ;
-      double2 gu = make_double2(0.0, 0.0), gw = make_double2(0.0, 0.0);
+      V2* Gs = G + (size_t)ss * QQ;
+      V2 gu, gw;
+      gu.x = gu.y = gw.x = gw.y = (R)0;
       for (int q = 0; q < Q; ++q) {
         const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
-        const double* R = IFf + ((size_t)kzh * Q + q) * 6 * nxh + kxs;
-        const double M00 = R[0], M01 = R[nxh], M10 = R[2 * nxh], M11 = R[3 * nxh], l = R[4 * nxh];
-        double2 ru = F[eq * TS + ss];
+        const R* Rq = IFf + ((size_t)kzh * Q + q) * 6 * ldx + kxs;
+        const R M00 = Rq[0], M01 = Rq[ldx], M10 = Rq[2 * ldx], M11 = Rq[3 * ldx], l = Rq[4 * ldx];
+        V2 ru = F[eq * TS + ss];
         if (q > 0) { ru.x -= l * gu.x; ru.y -= l * gu.y; }
-        const double2 rw = F[sq1 * TS + ss];
-        gu = make_double2(M00 * ru.x + M01 * rw.x, M00 * ru.y + M01 * rw.y);
-        gw = make_double2(M10 * ru.x + M11 * rw.x, M10 * ru.y + M11 * rw.y);
+        const V2 rw = F[sq1 * TS + ss];
+        gu.x = M00 * ru.x + M01 * rw.x; gu.y = M00 * ru.y + M01 * rw.y;
+        gw.x = M10 * ru.x + M11 * rw.x; gw.y = M10 * ru.y + M11 * rw.y;
         Gs[2 * q] = gu; Gs[2 * q + 1] = gw;
       }
-      double2 zw = Gs[2 * (Q - 1) + 1];
+      V2 zw = Gs[2 * (Q - 1) + 1];
       for (int q = Q - 2; q >= 0; --q) {
-        const double* R = IFf + ((size_t)kzh * Q + q) * 6 * nxh + kxs;
-        const double M01 = R[nxh], M11 = R[3 * nxh], v = R[5 * nxh];
-        const double fx = v * zw.x, fy = v * zw.y;
-        double2 zu = Gs[2 * q], zwn = Gs[2 * q + 1];
+        const R* Rq = IFf + ((size_t)kzh * Q + q) * 6 * ldx + kxs;
+        const R M01 = Rq[ldx], M11 = Rq[3 * ldx], v = Rq[5 * ldx];
+        const R fx = v * zw.x, fy = v * zw.y;
+        V2 zu = Gs[2 * q], zwn = Gs[2 * q + 1];
         zu.x -= M01 * fx; zu.y -= M01 * fy;
         zwn.x -= M11 * fx; zwn.y -= M11 * fy;
         Gs[2 * q] = zu; Gs[2 * q + 1] = zwn;
@@ -1004,19 +1019,21 @@ __global__ void __launch_bounds__(256, 2) k_ysolve2(Geo<T> g, Metrics<double> m,
   }
   __syncthreads();
   if (act && kx < nxh) {
-    const double2* Gs = G + (size_t)s * QQ;
-    const double2 uL = p > 0 ? Gs[2 * (p - 1)] : make_double2(0.0, 0.0);
-    const double2 wR = p < P - 1 ? Gs[2 * p + 1] : make_double2(0.0, 0.0);
-    double be = 0.0;
+    const V2* Gs = G + (size_t)s * QQ;
+    V2 uL, wR;
+    uL.x = uL.y = wR.x = wR.y = (R)0;
+    if (p > 0) uL = Gs[2 * (p - 1)];
+    if (p < P - 1) wR = Gs[2 * p + 1];
+    R be = (R)0;
 #pragma unroll
     for (int q = CH3D_LMAX - 1; q >= 0; --q) {
       if (q < L) {
         const int j = jlo + q;
-        be = (q == L - 1) ? ((p == P - 1) ? 0.0 : -cpv[q]) : -cpv[q] * be;
-        const double2 y = F[j * TS + s];
-        const double al = alv[q];
-        const double xr = y.x + al * uL.x + be * wR.x;
-        const double xi = y.y + al * uL.y + be * wR.y;
+        be = (q == L - 1) ? ((p == P - 1) ? (R)0 : -cpv[q]) : -cpv[q] * be;
+        const V2 y = F[j * TS + s];
+        const R al = alv[q];
+        const R xr = y.x + al * uL.x + be * wR.x;
+        const R xi = y.y + al * uL.y + be * wR.y;
         spec[kx + (long long)nxh * j + zs * kz] = mk((T)xr, (T)xi);
       }
     }
@@ -1395,7 +1412,8 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   static bool attr_set[2] = {false, false};
   if (!attr_set[sizeof(T) == 4]) {
     cudaFuncSetAttribute(k_zfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_ysolve2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_ysolve2<T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_ysolve2<T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set[sizeof(T) == 4] = true;
   }
   dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
@@ -1403,10 +1421,26 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int P = c->P, TS = c->TSy, Q = P - 1;
-  size_t smemy = (size_t)c->ny * TS * sizeof(double2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(double2) + 16;
-  dim3 gy((c->nxh + TS - 1) / TS, c->nz);
-  k_ysolve2<T><<<gy, TS * P < 64 ? 64 : TS * P, smemy, c->stream>>>(make_geo<T>(c), c->m64, c->yRM, c->yCP, c->yIF,
-                                                                   (CT*)c->spec, TS, P, c->sc);
+  if (!c->fp32) {
+    const size_t smemy = (size_t)c->ny * TS * sizeof(double2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(double2) + 16;
+    dim3 gy((c->nxh + TS - 1) / TS, c->nz);
+    k_ysolve2<T, double><<<gy, TS * P < 64 ? 64 : TS * P, smemy, c->stream>>>(
+        make_geo<T>(c), c->m64full, (const double*)c->yRM, (const double*)c->yCP, (const double*)c->yIF, c->nxh,
+        (CT*)c->spec, TS, P, 0, 0, c->sc);
+  } else {
+    // mixed: FP32 systems and factors, except the low modes near kx = kz = 0 in FP64
+    const size_t smem32 = (size_t)c->ny * TS * sizeof(float2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(float2) + 16;
+    const size_t smem64 = (size_t)c->ny * TS * sizeof(double2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(double2) + 16;
+    dim3 gy((c->nxh + TS - 1) / TS, c->nz);
+    k_ysolve2<T, float><<<gy, TS * P < 64 ? 64 : TS * P, smem32, c->stream>>>(
+        make_geo<T>(c), c->m64full, (const float*)c->yRM, (const float*)c->yCP, (const float*)c->yIF, c->nxh,
+        (CT*)c->spec, TS, P, 2, c->KL, c->sc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dim3 gl(1, 2 * c->KL + 1);
+    k_ysolve2<T, double><<<gl, TS * P < 64 ? 64 : TS * P, smem64, c->stream>>>(
+        make_geo<T>(c), c->m64full, c->yRM64, c->yCP64, c->yIF64, TS, (CT*)c->spec, TS, P, 1, c->KL, c->sc);
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);
@@ -1414,9 +1448,21 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
 }
 template <class T> static cudaError_t yfactors_t(ch3d_ctx* c) {
   const int TS = c->TSy, P = c->P;
+  const size_t sm = (size_t)TS * P * 4 * sizeof(double);
+  const int nthr = TS * P < 64 ? 64 : TS * P;
   dim3 grid((c->nxh + TS - 1) / TS, c->nz / 2 + 1);
-  k_ysolve_factors<T><<<grid, TS * P < 64 ? 64 : TS * P, (size_t)TS * P * 4 * sizeof(double), c->stream>>>(
-      make_geo<T>(c), c->m64, c->wave, c->yRM, c->yCP, c->yIF, TS, P);
+  if (!c->fp32) {
+    k_ysolve_factors<T, double><<<grid, nthr, sm, c->stream>>>(make_geo<T>(c), c->m64full, c->wave, (double*)c->yRM,
+                                                               (double*)c->yCP, (double*)c->yIF, TS, P, c->nxh,
+                                                               c->nxh);
+  } else {
+    k_ysolve_factors<T, float><<<grid, nthr, sm, c->stream>>>(make_geo<T>(c), c->m64full, c->wave, (float*)c->yRM,
+                                                              (float*)c->yCP, (float*)c->yIF, TS, P, c->nxh, c->nxh);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_ysolve_factors<T, double><<<dim3(1, c->KL + 1), nthr, sm, c->stream>>>(
+        make_geo<T>(c), c->m64full, c->wave, c->yRM64, c->yCP64, c->yIF64, TS, P, TS, c->nxh < TS ? c->nxh : TS);
+  }
   return cudaGetLastError();
 }
 cudaError_t launch_ysolve_factors(ch3d_ctx* c) { return c->fp32 ? yfactors_t<float>(c) : yfactors_t<double>(c); }
@@ -1476,6 +1522,151 @@ template <class T> static cudaError_t divmax_t(ch3d_ctx* c, unsigned long long* 
 cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot) {
   return c->fp32 ? divmax_t<float>(c, slot) : divmax_t<double>(c, slot);
 }
+
+// ---------------------------------------------------------------------------
+// clcStat_CH moment sums (src/CFD_2nd/m_FlowType_Channel.f90:175-330), FP64
+// accumulation in both precision modes.  Block (j, k-chunk); blockIdx.x == ny
+// is the nyp row (:296-316).  Partials are summed in a fixed order by
+// k_stats_finalize, so the statistics are deterministic.
+// ---------------------------------------------------------------------------
+#define CH3D_NSTAT 35
+
+template <class T>
+__device__ __forceinline__ double fd(const T* a, const Geo<T>& g, int comp, int i, int j, int k) {
+  return (double)fld(a, g, comp, i, j, k);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_stats(Geo<T> g, Metrics<double> m, const T* __restrict__ ux,
+                                               const T* __restrict__ uy, const T* __restrict__ uz,
+                                               const T* __restrict__ pr, double* __restrict__ part, int kch) {
+  __shared__ double wred[CH3D_NSTAT][8];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int j = blockIdx.x;  // 0..ny-1 interior rows (jc = j+1); ny: the nyp row
+  const int k0 = blockIdx.y * kch, k1 = min(nz, k0 + kch);
+  double S[CH3D_NSTAT];
+#pragma unroll
+  for (int q = 0; q < CH3D_NSTAT; ++q) S[q] = 0.0;
+  const double rdx = (double)g.rdx, rdz = (double)g.rdz, rdx2 = (double)g.rdx2, rdz2 = (double)g.rdz2;
+  const double rdxh = rdx * 0.5;
+  if (j < ny) {
+    const int jc = j + 1;
+    const double InterpY1 = 0.5 * m.yinterp[jc], InterpY2 = 0.5 - InterpY1;
+    const double cac = m.rdyc[jc], cacU = m.rdyc[jc + 1], caj = m.rdyp[jc];
+    for (int k = k0; k < k1; ++k) {
+      const int km = wrapm(k, nz), kp = wrapp(k, nz);
+      for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const int im = wrapm(i, nx), ip = wrapp(i, nx);
+        const double uxloc = fd(ux, g, 0, i, j, k), uyloc = fd(uy, g, 1, i, j, k), uzloc = fd(uz, g, 2, i, j, k);
+        const double prloc = fd(pr, g, 3, i, j, k);
+        const double ux_ip = fd(ux, g, 0, ip, j, k), ux_im = fd(ux, g, 0, im, j, k);
+        const double ux_jm = fd(ux, g, 0, i, j - 1, k), ux_jp = fd(ux, g, 0, i, j + 1, k);
+        const double ux_km = fd(ux, g, 0, i, j, km), ux_kp = fd(ux, g, 0, i, j, kp);
+        const double uy_jp = fd(uy, g, 1, i, j + 1, k), uy_im = fd(uy, g, 1, im, j, k), uy_ip = fd(uy, g, 1, ip, j, k);
+        const double uy_jm = fd(uy, g, 1, i, j - 1, k), uy_km = fd(uy, g, 1, i, j, km), uy_kp = fd(uy, g, 1, i, j, kp);
+        const double uy_im_jp = fd(uy, g, 1, im, j + 1, k);
+        const double uz_kp = fd(uz, g, 2, i, j, kp), uz_km = fd(uz, g, 2, i, j, km);
+        const double uz_im = fd(uz, g, 2, im, j, k), uz_ip = fd(uz, g, 2, ip, j, k);
+        const double uz_jm = fd(uz, g, 2, i, j - 1, k), uz_jp = fd(uz, g, 2, i, j + 1, k);
+        const double uxCell = 0.5 * (uxloc + ux_ip);
+        const double uyCell = 0.5 * (uyloc + uy_jp);
+        const double uzCell = 0.5 * (uzloc + uz_kp);
+        const double prloc2 = InterpY1 * (fd(pr, g, 3, im, j - 1, k) + fd(pr, g, 3, i, j - 1, k)) +
+                              InterpY2 * (fd(pr, g, 3, im, j, k) + prloc);
+        const double dudx = (ux_ip - uxloc) * rdx, dudy = (uxloc - ux_jm) * cac, dudz = (uxloc - ux_km) * rdz;
+        const double dvdx = (uyloc - uy_im) * rdx, dvdy = (uy_jp - uyloc) * caj, dvdz = (uyloc - uy_km) * rdz;
+        const double dwdx = (uzloc - uz_im) * rdx, dwdy = (uzloc - uz_jm) * cac, dwdz = (uz_kp - uzloc) * rdz;
+        const double dudxx = (ux_ip - 2.0 * uxloc + ux_im) * rdx2;
+        const double dudyy = m.ap2c[jc] * ux_jp + m.ac2c[jc] * uxloc + m.am2c[jc] * ux_jm;
+        const double dudzz = (ux_kp - 2.0 * uxloc + ux_km) * rdz2;
+        const double dvdxx = (uy_ip - 2.0 * uyloc + uy_im) * rdx2;
+        const double dvdyy = m.ap2p[jc] * uy_jp + m.ac2p[jc] * uyloc + m.am2p[jc] * uy_jm;
+        const double dvdzz = (uy_kp - 2.0 * uyloc + uy_km) * rdz2;
+        const double dwdxx = (uz_ip - 2.0 * uzloc + uz_im) * rdx2;
+        const double dwdyy = m.ap2c[jc] * uz_jp + m.ac2c[jc] * uzloc + m.am2c[jc] * uz_jm;
+        const double dwdzz = (uz_kp - 2.0 * uzloc + uz_km) * rdz2;
+        const double vor_x = dwdy - dvdz, vor_y = dudz - dwdx, vor_z = dvdx - dudy;
+        const double dudxC = (ux_ip - ux_im) * rdxh;
+        const double dvdxU = (uy_jp - uy_im_jp) * rdx;
+        const double dudyU = (ux_jp - uxloc) * cacU;
+        const double dvdyM = (uy_im_jp - uy_im) * caj;
+        const double dudzC = (InterpY1 * (fd(ux, g, 0, i, j - 1, kp) - fd(ux, g, 0, i, j - 1, km)) +
+                              InterpY2 * (ux_kp - ux_km)) * rdz;
+        const double dvdzC = (fd(uy, g, 1, im, j, kp) - fd(uy, g, 1, im, j, km) + uy_kp - uy_km) * rdz * 0.25;
+        S[0] += uxloc; S[1] += uyloc; S[2] += uzloc; S[3] += prloc;
+        S[4] += uxloc * uxloc; S[5] += uyloc * uyloc; S[6] += uzloc * uzloc; S[7] += prloc * prloc;
+        S[8] += uxCell * uyCell; S[9] += uyCell * uzCell; S[10] += uxCell * uzCell;
+        S[11] += uxCell * prloc; S[12] += uyCell * prloc; S[13] += uzCell * prloc;
+        S[14] += uxCell * uxCell * uyCell; S[15] += uyloc * uyloc * uyloc; S[16] += uzCell * uzCell * uyCell;
+        S[17] += uxCell * uyCell * uyCell; S[18] += uxloc * uxloc * uxloc; S[19] += uzloc * uzloc * uzloc;
+        S[20] += uxloc * uxloc * uxloc * uxloc; S[21] += uyloc * uyloc * uyloc * uyloc;
+        S[22] += uzloc * uzloc * uzloc * uzloc;
+        S[23] += prloc * dudx; S[24] += prloc * dvdy; S[25] += prloc * dwdz;
+        S[26] += prloc2 * (dudy + dvdx);
+        S[27] += uxloc * (dudxx + dudyy + dudzz); S[28] += uyloc * (dvdxx + dvdyy + dvdzz);
+        S[29] += uzloc * (dwdxx + dwdyy + dwdzz);
+        S[30] += dudxC * (dvdxU + dvdx) * 0.5 + (dudyU + dudy) * (dvdyM + dvdy) * 0.25;
+        S[31] += dudzC * dvdzC;
+        S[32] += vor_x * vor_x; S[33] += vor_y * vor_y; S[34] += vor_z * vor_z;
+      }
+    }
+  } else {
+    // jc = nyp: ghost row above the last cell (SetBC_and_UpdateHalo values)
+    const int jc = ny + 1, jm = ny - 1;
+    const double cac = m.rdyc[jc];
+    const double InterpY1 = 0.5 * m.yinterp[jc], InterpY2 = 0.5 - InterpY1;
+    for (int k = k0; k < k1; ++k)
+      for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const int im = wrapm(i, nx);
+        const double prloc2 = InterpY1 * (fd(pr, g, 3, im, jm, k) + fd(pr, g, 3, i, jm, k)) +
+                              InterpY2 * (fd(pr, g, 3, im, ny, k) + fd(pr, g, 3, i, ny, k));
+        const double dudy = (fd(ux, g, 0, i, ny, k) - fd(ux, g, 0, i, jm, k)) * cac;
+        const double dwdy = (fd(uz, g, 2, i, ny, k) - fd(uz, g, 2, i, jm, k)) * cac;
+        const double vor_x = dwdy, vor_z = -dudy;
+        S[26] += prloc2 * (dudy + 0.0);
+        S[32] += vor_x * vor_x;
+        S[34] += vor_z * vor_z;
+      }
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < CH3D_NSTAT; ++q) {
+    double v = S[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) wred[q][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < CH3D_NSTAT) {
+    double v = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) v += wred[threadIdx.x][q];
+    part[((size_t)j * gridDim.y + blockIdx.y) * CH3D_NSTAT + threadIdx.x] = v;
+  }
+}
+
+// SumStat(:,jc) += sum of the partials * inxz (m_FlowType_Channel.f90:290-293);
+// PrGradsum += PrGradAver (:318).
+__global__ void k_stats_finalize(const double* __restrict__ part, int nch, double inxz, double* __restrict__ sumstat,
+                                 DevScalars* sc, double* prgradsum) {
+  const int j = blockIdx.x, q = threadIdx.x;
+  if (q < CH3D_NSTAT) {
+    double v = 0.0;
+    for (int c = 0; c < nch; ++c) v += part[((size_t)j * nch + c) * CH3D_NSTAT + q];
+    sumstat[(size_t)j * CH3D_NSTAT + q] += v * inxz;
+  }
+  if (j == 0 && q == 0) *prgradsum += sc->PrGradAver;
+}
+
+template <class T> static cudaError_t stats_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  const int kch = (c->nz + 7) / 8;
+  const int nch = (c->nz + kch - 1) / kch;
+  k_stats<T><<<dim3(c->ny + 1, nch), 256, 0, c->stream>>>(make_geo<T>(c), c->m64full, f[0], f[1], f[2], f[3],
+                                                           c->statpart, kch);
+  k_stats_finalize<<<c->ny + 1, 64, 0, c->stream>>>(c->statpart, nch, 1.0 / ((double)c->nx * (double)c->nz), c->stat,
+                                                   c->sc, c->stat + (size_t)CH3D_NSTAT * (c->ny + 1));
+  return cudaGetLastError();
+}
+cudaError_t launch_stats(ch3d_ctx* c) { return c->fp32 ? stats_t<float>(c) : stats_t<double>(c); }
 
 // ---------------------------------------------------------------------------
 // Allocation-free Poisson solve (ch3d_poisson_noalloc in include/ch3d.h).

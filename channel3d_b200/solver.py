@@ -102,6 +102,18 @@ class ChannelSolver:
         _lib.check(self.lib.ch3d_memory_bytes(self.ctx, ctypes.byref(v)), self.lib)
         return v.value
 
+    def stats_accumulate(self):
+        _lib.check(self.lib.ch3d_stats_accumulate(self.ctx), self.lib)
+
+    def stats_fetch(self, reset=False):
+        """(SumStat as (nyp, 35), nfstime, PrGradsum)."""
+        s = np.empty((self.cfg.nyc + 1) * 35)
+        n = ctypes.c_int()
+        pg = ctypes.c_double()
+        _lib.check(self.lib.ch3d_stats_fetch(self.ctx, _lib.dptr(s), ctypes.byref(n), ctypes.byref(pg), int(reset)),
+                   self.lib)
+        return s.reshape(self.cfg.nyc + 1, 35), n.value, pg.value
+
     def kernel_times(self, nsteps=1):
         out = np.zeros(7)
         _lib.check(self.lib.ch3d_kernel_times(self.ctx, int(nsteps), _lib.dptr(out), 7), self.lib)

@@ -96,3 +96,34 @@ def test_fused_rhs_uhat_matches_stages(built):
     ga, gb = a.download(hist=True), b.download(hist=True)
     for k in ("ux", "uy", "uz", "p", "hist"):
         assert rel_max(ga[k], gb[k]) < 1e-11, (k, rel_max(ga[k], gb[k]))
+
+
+def test_statistics_parity(built):
+    """clcStat_CH moment sums accumulated on the device (FP64) against the oracle."""
+    cfg = small_channel(32, 24, 16)
+    o, s = _pair(cfg)
+    for _ in range(3):
+        s.step(2); o.step(2)
+        s.stats_accumulate(); o.stats_accumulate()
+    a, na, pa = s.stats_fetch()
+    b, nb, pb = o.stats_get()
+    assert na == nb == 3
+    assert rel_max(a, b) < 1e-11, rel_max(a, b)
+    assert abs(pa - pb) <= 1e-10 * max(1.0, abs(pb))
+
+
+def test_mixed_precision_error_bound(built):
+    """Mixed FP32/FP64 path (FP32 fields, stencils, FFTs and high-mode y
+    solves; FP64 low-mode y solves, bulk constraint, reductions) stays within
+    1e-4 relative (L2) of the FP64 oracle on velocity after 50 steps of the
+    64^3 channel, with divergence at FP32 round-off."""
+    from channel3d_b200 import workloads
+    cfg, _ = workloads.get("channel64_re5600")
+    o, s = _pair(cfg.copy(precision="mixed"))
+    info = s.step(50)
+    o.step(50)
+    go, gs = o.get_state(), s.download()
+    for k in ("ux", "uy", "uz"):
+        assert rel_l2(gs[k], go[k]) < 1e-4, (k, rel_l2(gs[k], go[k]))
+    assert rel_l2(gs["p"], go["p"]) < 1e-3
+    assert info["divmax2"] < 1e-4

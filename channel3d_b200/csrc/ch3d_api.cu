@@ -168,6 +168,17 @@ void build_metrics(ch3d_ctx* c) {
   c->WaveNumZ.assign(c->nz, 0.0);
   for (int i = 1; i <= c->nx; ++i) c->WaveNumX[i - 1] = 2.0 * c->rdx2 * (std::cos(2.0 * PI * (double)(i - 1) / (double)c->nx) - 1.0);
   for (int k = 1; k <= c->nz; ++k) c->WaveNumZ[k - 1] = 2.0 * c->rdz2 * (std::cos(2.0 * PI * (double)(k - 1) / (double)c->nz) - 1.0);
+  if (g.order == 4) {
+    // 4th-order modified wavenumbers, src/CFD_4th/m_Poisson.f90:40-47
+    for (int i = 1; i <= c->nx; ++i) {
+      const double wa = 2.0 * PI * (double)(i - 1) / (double)c->nx;
+      c->WaveNumX[i - 1] = c->rdx2 / 288.0 * (std::cos(3.0 * wa) - 54.0 * std::cos(2.0 * wa) + 783.0 * std::cos(wa) - 730.0);
+    }
+    for (int k = 1; k <= c->nz; ++k) {
+      const double wa = 2.0 * PI * (double)(k - 1) / (double)c->nz;
+      c->WaveNumZ[k - 1] = c->rdz2 / 288.0 * (std::cos(3.0 * wa) - 54.0 * std::cos(2.0 * wa) + 783.0 * std::cos(wa) - 730.0);
+    }
+  }
   c->normfft = 1.0 / ((double)c->nx * (double)c->nz);
 }
 
@@ -197,11 +208,13 @@ Metrics<T> metrics_ptrs(const T* base, int ny) {
 int check_config(const ch3d_config* g) {
   if (!g) return fail(CH3D_ERR_INVALID, "config is NULL");
   if (g->order != 2 && g->order != 4) return fail(CH3D_ERR_INVALID, "order must be 2 or 4");
-  if (g->order != 2) return fail(CH3D_ERR_UNSUPPORTED, "order %d is not built in this library version", g->order);
+  if (g->order == 4 && (g->FlowType != 1 || g->BcOption[2] != -1 || g->BcOption[3] != -1))
+    return fail(CH3D_ERR_UNSUPPORTED, "the 4th-order solver is built for the channel (FlowType=1, no-slip walls)");
   if (g->nxc < 4 || g->nyc < 4 || g->nzc < 2) return fail(CH3D_ERR_INVALID, "grid too small: %d %d %d", g->nxc, g->nyc, g->nzc);
   if (g->nxc % 2) return fail(CH3D_ERR_INVALID, "nxc must be even (real-to-complex x transform)");
   if (g->ischeme != 3) return fail(CH3D_ERR_UNSUPPORTED, "only RK3 (ischeme=3) is built");
-  if (g->IsImplicit != 1) return fail(CH3D_ERR_UNSUPPORTED, "IsImplicit=%d not built (PIMP=1 is)", g->IsImplicit);
+  if (g->IsImplicit != 1 && !(g->order == 2 && g->IsImplicit == 2))
+    return fail(CH3D_ERR_UNSUPPORTED, "IsImplicit=%d not built (PIMP=1, and FIMP=2 for order 2, are)", g->IsImplicit);
   if (g->BcOption[0] != 0 || g->BcOption[1] != 0 || g->BcOption[4] != 0 || g->BcOption[5] != 0)
     return fail(CH3D_ERR_UNSUPPORTED, "x and z must be periodic (BcOption 1,2,5,6 = 0)");
   for (int s = 2; s < 4; ++s)
@@ -223,6 +236,18 @@ int alloc_fields(ch3d_ctx* c) {
     CU(cudaMemsetAsync(c->f[q], 0, (size_t)c->N * sizeof(T), c->stream));
     c->bytes += (long long)c->N * sizeof(T);
   }
+  if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
+    const size_t nb = ptri_factor_doubles(c->nx, c->nz) * sizeof(double);
+    CU(cudaMalloc(&c->pfac, nb));
+    CU(cudaMemsetAsync(c->pfac, 0, nb, c->stream));
+    c->bytes += (long long)nb;
+  }
+  if (c->cfg.order == 4)
+    for (int q = 0; q < 6; ++q) {
+      CU(cudaMalloc(&c->ih[q], (size_t)c->N * sizeof(T)));
+      CU(cudaMemsetAsync(c->ih[q], 0, (size_t)c->N * sizeof(T), c->stream));
+      c->bytes += (long long)c->N * sizeof(T);
+    }
   CU(cudaMalloc(&c->spec, (size_t)c->NS * sizeof(CT)));
   c->bytes += (long long)c->NS * sizeof(CT);
   std::vector<T> met;
@@ -272,7 +297,8 @@ void host_fill_ghosts(const ch3d_ctx* c, int layout, double* a, int comp) {
       if (comp == 1) {
         at(i, nyp, k) = g.uyBcValue[3];
         if (jtop >= nyp + 1) at(i, nyp + 1, k) = g.uyBcValue[3] * 2.0 - at(i, nyc, k);
-        at(i, 0, k) = g.uyBcValue[2] * 2.0 - at(i, 2, k);
+        // uy(ic,0,kc) is never set by the 4th-order solver (zero)
+        at(i, 0, k) = g.order == 4 ? 0.0 : g.uyBcValue[2] * 2.0 - at(i, 2, k);
         continue;
       }
       double wl = comp == 0 ? g.uxBcValue[2] : g.uzBcValue[2];
@@ -345,10 +371,18 @@ int init_scalars(ch3d_ctx* c) {
 
 int record_step(ch3d_ctx* c) {
   CU(launch_step_begin(c));
+  const bool o4 = c->cfg.order == 4, fimp = c->cfg.order == 2 && c->cfg.IsImplicit == 2;
   for (int ns = 1; ns <= c->iadvance; ++ns) {
+    if (o4) CU(launch_visc4_partials(c));
     CU(launch_substep_setup(c, ns));
     CU(launch_helm_factors(c));
-    CU(launch_rhs_uhat(c));
+    if (fimp) {
+      CU(launch_rhs_fimp(c));
+      CU(launch_ptri_xz(c));
+      CU(launch_uhat(c));
+    } else {
+      CU(o4 ? launch_rhs4_uhat(c) : launch_rhs_uhat(c));
+    }
     CU(launch_prsrc_xfft(c, 0));
     CU(launch_poisson_spectral(c));
     CU(launch_xifft(c));
@@ -552,6 +586,8 @@ int ch3d_destroy(ch3d_ctx* c) {
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   for (int q = 0; q < 15; ++q) if (c->f[q]) cudaFree(c->f[q]);
+  for (int q = 0; q < 6; ++q) if (c->ih[q]) cudaFree(c->ih[q]);
+  if (c->pfac) cudaFree(c->pfac);
   void* bufs[] = {c->hfac, c->yRM, c->yCP, c->yIF, c->yRM64, c->yCP64, c->yIF64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
@@ -646,9 +682,16 @@ int ch3d_stage(ch3d_ctx* c, int stage, int ns) {
     if (rc) return rc;
   }
   switch (stage) {
-    case 0: CU(launch_substep_setup(c, ns)); break;
-    case 1: CU(launch_rhs(c)); break;
-    case 2: CU(launch_helm_factors(c)); CU(launch_uhat(c)); break;
+    case 0:
+      if (c->cfg.order == 4) CU(launch_visc4_partials(c));  // forcing of clcRhsXYZ from the current ux
+      CU(launch_substep_setup(c, ns));
+      break;
+    case 1: CU(c->cfg.order == 4 ? launch_rhs4(c) : (c->cfg.IsImplicit == 2 ? launch_rhs_fimp(c) : launch_rhs(c))); break;
+    case 2:
+      if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) CU(launch_ptri_xz(c));
+      CU(launch_helm_factors(c));
+      CU(launch_uhat(c));
+      break;
     case 3: break;  // clcPrSrc is fused into the forward x transform of stage 4
     case 4:
       CU(launch_prsrc_xfft(c, 0));
@@ -745,6 +788,8 @@ int ch3d_set_dt(ch3d_ctx* c, double dt) {
 
 int ch3d_stats_accumulate(ch3d_ctx* c) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (c->cfg.order != 2)
+    return fail(CH3D_ERR_UNSUPPORTED, "statistics are built for the 2nd-order solver (clcStat_CH)");
   CU(cudaSetDevice(c->device));
   if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
   CU(launch_stats(c));
@@ -796,9 +841,16 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
   for (int s = 0; s < nsteps; ++s) {
     CU(mark(6)); CU(launch_step_begin(c)); CU(done());
     for (int ns = 1; ns <= c->iadvance; ++ns) {
-      CU(mark(6)); CU(launch_substep_setup(c, ns)); CU(launch_helm_factors(c)); CU(done());
-      CU(mark(0)); CU(launch_rhs_uhat(c)); CU(done());
-      CU(mark(1)); CU(done());
+      CU(mark(6));
+      if (c->cfg.order == 4) CU(launch_visc4_partials(c));
+      CU(launch_substep_setup(c, ns)); CU(launch_helm_factors(c)); CU(done());
+      if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
+        CU(mark(0)); CU(launch_rhs_fimp(c)); CU(done());
+        CU(mark(1)); CU(launch_ptri_xz(c)); CU(launch_uhat(c)); CU(done());
+      } else {
+        CU(mark(0)); CU(c->cfg.order == 4 ? launch_rhs4_uhat(c) : launch_rhs_uhat(c)); CU(done());
+        CU(mark(1)); CU(done());
+      }
       CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());
       CU(mark(3)); CU(launch_poisson_spectral(c)); CU(done());
       CU(mark(4)); CU(launch_xifft(c)); CU(done());

@@ -59,6 +59,8 @@ struct YBc {
 
 template <class T> struct Geo {
   int nx, ny, nz, nxh;
+  int order;                            // 2: src/CFD_2nd, 4: src/CFD_4th
+  int implicit;                         // IsImplicit: 1 PIMP (CN in y), 2 FIMP (CN in x, y, z)
   long long N;
   T rdx, rdz, rdx2, rdz2;
   T ap1c, ac1c, am1c, ap3c, ac3c, am3c;  // constant for periodic x and z
@@ -77,7 +79,8 @@ __device__ __forceinline__ T fld(const T* __restrict__ a, const Geo<T>& g, int c
   const int nx = g.nx, ny = g.ny;
   if (j >= 0 && j < ny) return __ldg(a + i + (long long)nx * (j + (long long)ny * k));
   if (j < 0) {
-    if (comp == 1) {  // uy(ic,0,kc) = uy_ym*2 - uy(ic,2,kc)
+    if (comp == 1) {  // uy(ic,0,kc) = uy_ym*2 - uy(ic,2,kc); never set (zero) in the 4th-order solver
+      if (g.order == 4) return (T)0;
       return (T)(g.bc.uy_lo * 2.0) - __ldg(a + i + (long long)nx * (1 + (long long)ny * k));
     }
     T v = __ldg(a + i + (long long)nx * (0 + (long long)ny * k));

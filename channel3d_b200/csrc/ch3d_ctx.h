@@ -34,7 +34,9 @@ struct ch3d_ctx {
 
   // device buffers
   void* f[15] = {nullptr};   // ux uy uz p hx hy hz rx ry rz phi nut u*x u*y u*z (precision T)
+  void* ih[6] = {nullptr};   // 4th order: uxhx uyhx uzhx uxhz uyhz uzhz (precision T)
   double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
+  double* pfac = nullptr;    // FIMP: periodic x/z sweep factors of the current substep
   void* yRM = nullptr;       // Poisson y-solve chunk factors per mode (fixed for the run);
   void* yCP = nullptr;       // FP64, or FP32 in the mixed path
   void* yIF = nullptr;       // Poisson interface factors per mode
@@ -98,4 +100,12 @@ cudaError_t launch_bulk_partials(ch3d_ctx* c);
 cudaError_t launch_diag(ch3d_ctx* c);
 cudaError_t launch_stats(ch3d_ctx* c);
 cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot);
+// 4th-order solver (ch3d_step4.cu)
+cudaError_t launch_rhs4(ch3d_ctx* c);                  // stage path: interpolation + RhsX/Y/Z
+cudaError_t launch_rhs4_uhat(ch3d_ctx* c);             // fused step path: interpolation + RHS + y solve -> u*
+cudaError_t launch_visc4_partials(ch3d_ctx* c);        // mean viscous stress partial sums -> part
+// fully implicit 2nd-order step (ch3d_step.cu, ch3d_fimp.cu)
+cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP -> RhsX/Y/Z
+cudaError_t launch_ptri_xz(ch3d_ctx* c);               // periodic x and z sweeps of RhsX/Y/Z, in place
+size_t ptri_factor_doubles(int nx, int nz);
 }  // namespace ch3d

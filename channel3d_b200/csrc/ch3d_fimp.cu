@@ -1,0 +1,131 @@
+// ch3d_fimp.cu -- sm_100a kernels of the fully implicit (FIMP) 2nd-order
+// step for the channel: the periodic x and z Crank-Nicolson sweeps of
+// clcU1/2/3Hat_FIMP_010 (src/CFD_2nd/m_TSchemeFIMP_inc.f90:263-347, 636-729,
+// 1035-1128).  The y sweep that follows is the PIMP Helmholtz solve
+// (same coefficients), the RHS is rhs_comp with its FIMP branch.
+//
+// The periodic constant-coefficient solver is InversePTriFixedCoe
+// (src/CFD_2nd/m_Tools.f90:167-219): elimination of the first n-1 unknowns
+// with a second right-hand side for the coupling to unknown n, then the
+// closure of row n.  Its coefficient recurrences (ppj, vecn1, vecn2) are the
+// same for every line and are computed once per substep.
+#include "ch3d_ctx.h"
+#include "ch3d_dev.cuh"
+
+namespace ch3d {
+
+// Factor block of one direction: ppj | vecn1 | vecn2 (n+1 each, Fortran
+// index 1..n) then a, b, c, denominator.
+__host__ __device__ inline int ptri_stride(int n) { return 3 * (n + 1) + 4; }
+
+// blockIdx.x: 0 = x (n = nx, rdx2), 1 = z (n = nz, rdz2)
+__global__ void k_ptri_factors(int nx, int nz, double rdx2, double rdz2, double* __restrict__ pf,
+                               const DevScalars* __restrict__ sc) {
+  if (sc->status || threadIdx.x != 0) return;
+  const int d = blockIdx.x;
+  const int n = d == 0 ? nx : nz;
+  const double r2 = d == 0 ? rdx2 : rdz2;
+  double* F = pf + (d == 0 ? 0 : ptri_stride(nx));
+  double *ppj = F, *v1 = F + (n + 1), *v2 = F + 2 * (n + 1), *abc = F + 3 * (n + 1);
+  const double pmBeta = sc->pmBeta;
+  const double a = -pmBeta * r2, c = -pmBeta * r2, b = pmBeta * r2 * 2.0 + 1.0;
+  v1[1] = -c / b;
+  v2[1] = -a / b;
+  v2[n] = 1.0;
+  ppj[1] = 0.0;
+  for (int j = 2; j <= n - 1; ++j) {
+    ppj[j] = 1.0 / (b + a * v1[j - 1]);
+    v1[j] = -c * ppj[j];
+    v2[j] = -a * v2[j - 1] * ppj[j];
+  }
+  for (int j = n - 1; j >= 1; --j) v2[j] = v2[j] + v1[j] * v2[j + 1];
+  abc[0] = a; abc[1] = b; abc[2] = c;
+  abc[3] = c * v2[1] + a * v2[n - 1] + b;
+}
+
+// One periodic line f(1..n) at stride s (in place).
+template <class T>
+__device__ __forceinline__ void ptri_line(const double* __restrict__ F, int n, T* f, int s) {
+  const double *ppj = F, *v1 = F + (n + 1), *v2 = F + 2 * (n + 1), *abc = F + 3 * (n + 1);
+  const T a = (T)abc[0], b = (T)abc[1], c = (T)abc[2], den = (T)abc[3];
+  // forward elimination, rows 1..n-1
+  T prev = f[0] / b;
+  f[0] = prev;
+  for (int j = 2; j <= n - 1; ++j) {
+    prev = (f[(j - 1) * s] - a * prev) * (T)ppj[j];
+    f[(j - 1) * s] = prev;
+  }
+  // backward pass: arrmn(j) = f(j) + vecn1(j) arrmn(j+1), stored in place
+  T arr = (T)0;
+  for (int j = n - 1; j >= 1; --j) {
+    arr = f[(j - 1) * s] + (T)v1[j] * arr;
+    f[(j - 1) * s] = arr;
+  }
+  const T fn = (f[(n - 1) * s] - c * f[0] - a * f[(n - 2) * s]) / den;
+  f[(n - 1) * s] = fn;
+  for (int j = n - 1; j >= 1; --j) f[(j - 1) * s] = fn * (T)v2[j] + f[(j - 1) * s];
+}
+
+// x sweep: LB consecutive x lines (contiguous in memory) per block staged in
+// shared memory with a padded stride; one thread per line.  blockIdx.y = component.
+template <class T>
+__global__ void __launch_bounds__(128) k_ptri_x(int nx, long long nlines, int LB, const double* __restrict__ pf,
+                                                T* __restrict__ r0, T* __restrict__ r1, T* __restrict__ r2,
+                                                const DevScalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  T* S = (T*)smem_raw;
+  const int ld = nx + 1;
+  T* r = blockIdx.y == 0 ? r0 : (blockIdx.y == 1 ? r1 : r2);
+  const long long l0 = (long long)blockIdx.x * LB;
+  const int nl = (int)min((long long)LB, nlines - l0);
+  T* g = r + l0 * nx;
+  for (int t = threadIdx.x; t < nl * nx; t += blockDim.x) S[(t / nx) * ld + (t % nx)] = g[t];
+  __syncthreads();
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) ptri_line<T>(pf, nx, S + l * ld, 1);
+  __syncthreads();
+  for (int t = threadIdx.x; t < nl * nx; t += blockDim.x) g[t] = S[(t / nx) * ld + (t % nx)];
+}
+
+// z sweep: one thread per (i, j) column, in place in global memory (a warp
+// covers 32 consecutive i, so every access is coalesced).  blockIdx.z = component.
+template <class T>
+__global__ void __launch_bounds__(128) k_ptri_z(int nx, int ny, int nz, const double* __restrict__ pf,
+                                                T* __restrict__ r0, T* __restrict__ r1, T* __restrict__ r2,
+                                                const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int j = blockIdx.y * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (i >= nx || j >= ny) return;
+  T* r = blockIdx.z == 0 ? r0 : (blockIdx.z == 1 ? r1 : r2);
+  ptri_line<T>(pf + ptri_stride(nx), nz, r + i + (long long)nx * j, nx * ny);
+}
+
+template <class T> static cudaError_t ptri_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  k_ptri_factors<<<2, 32, 0, c->stream>>>(c->nx, c->nz, c->rdx2, c->rdz2, c->pfac, c->sc);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  int LB = (int)((64 * 1024) / ((size_t)(c->nx + 1) * sizeof(T)));
+  if (LB > 128) LB = 128;
+  if (LB < 1) LB = 1;
+  const long long nlines = (long long)c->ny * c->nz;
+  const size_t smem = (size_t)LB * (c->nx + 1) * sizeof(T);
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[sizeof(T) == 4]) {
+    cudaFuncSetAttribute(k_ptri_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set[sizeof(T) == 4] = true;
+  }
+  k_ptri_x<T><<<dim3((unsigned)((nlines + LB - 1) / LB), 3), 128, smem, c->stream>>>(c->nx, nlines, LB, c->pfac, f[7],
+                                                                                      f[8], f[9], c->sc);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_ptri_z<T><<<dim3((c->nx + 31) / 32, (c->ny + 3) / 4, 3), 128, 0, c->stream>>>(c->nx, c->ny, c->nz, c->pfac, f[7],
+                                                                                 f[8], f[9], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_ptri_xz(ch3d_ctx* c) { return c->fp32 ? ptri_t<float>(c) : ptri_t<double>(c); }
+
+size_t ptri_factor_doubles(int nx, int nz) { return (size_t)ptri_stride(nx) + ptri_stride(nz); }
+
+}  // namespace ch3d

@@ -19,6 +19,7 @@
 #include <mutex>
 #include <vector>
 #include "ch3d_ctx.h"
+#include "ch3d_dev.cuh"
 
 namespace ch3d {
 
@@ -42,8 +43,11 @@ __global__ void k_step_begin(DevScalars* sc, int iCFL, double CFLc, double dtMax
 
 // src/CFD_2nd/m_Parameters.f90:329-342 (PMcoeUpdate) and the bulk constraint of
 // src/CFD_2nd/m_TSchemePIMP_inc.f90:60-74 from the partial sums of the current ux.
+// 4th order (order == 4): the partial sums are those of the mean viscous stress
+// and the forcing follows src/CFD_4th/m_TScheme.f90:364-377.
 __global__ void k_substep_setup(DevScalars* sc, const double* __restrict__ part, int npart, int ns, double gam,
-                                double the, double alp, double xnu, int IsUxConst, double ubulk, double norm_bulk) {
+                                double the, double alp, double xnu, int IsUxConst, double ubulk, double norm_bulk,
+                                int order, double nxnz, double yly) {
   __shared__ double red[256];
   if (sc->status) return;
   double s = 0;
@@ -66,7 +70,12 @@ __global__ void k_substep_setup(DevScalars* sc, const double* __restrict__ part,
     if (ns == 1) sc->PrGradAver = 0.0;
     sc->ns = ns;
     sc->divmax1 = 0ull;
-    if (IsUxConst) {
+    if (IsUxConst && order == 4) {
+      const double dpm = xnu * red[0] / nxnz / yly;
+      sc->PrGradNow = dpm;
+      sc->dpmdxns = -(sc->pmAlpha * dpm);  // RhsX - pmAlpha*dpmdxns
+      sc->PrGradAver = sc->PrGradAver + dpm * alp;
+    } else if (IsUxConst) {
       double s1tot1 = red[0] * norm_bulk;
       sc->s1tot1 = s1tot1;
       sc->dpmdxns = alp * (ubulk - s1tot1);
@@ -191,57 +200,6 @@ __device__ __forceinline__ void rhs_point(const Geo<T>& g, const Metrics<T>& m, 
   }
 }
 
-// Neighbour addressing of one cell: a base index plus signed offsets that
-// already contain the periodic wrap in x and z; y neighbours past the walls
-// are replaced by the ghost rules of SetBC_and_UpdateHalo
-// (src/CFD_2nd/m_BC_and_Halo.f90:241-282).
-struct Nbr {
-  long long c;        // cell index
-  int xp, xm;         // offsets to i+1, i-1
-  long long zp, zm;   // offsets to k+1, k-1
-  int yp;             // +nx (offset to j+1)
-  bool jlo, jhi;      // j == 0, j == ny-1
-};
-
-template <class T>
-__device__ __forceinline__ Nbr make_nbr(const Geo<T>& g, int i, int j, int k) {
-  Nbr n;
-  const long long plane = (long long)g.nx * g.ny;
-  n.c = i + (long long)g.nx * j + plane * k;
-  n.xp = (i + 1 == g.nx) ? 1 - g.nx : 1;
-  n.xm = (i == 0) ? g.nx - 1 : -1;
-  n.zp = (k + 1 == g.nz) ? -(long long)(g.nz - 1) * plane : plane;
-  n.zm = (k == 0) ? (long long)(g.nz - 1) * plane : -plane;
-  n.yp = g.nx;
-  n.jlo = (j == 0);
-  n.jhi = (j == g.ny - 1);
-  return n;
-}
-
-// value at offset o (same j) and at j-1 / j+1 of the same offset column
-template <class T> __device__ __forceinline__ T at(const T* __restrict__ a, const Nbr& n, long long o) {
-  return __ldg(a + n.c + o);
-}
-// ux / uz (comp 0 / 2): wall ghosts 2 w - u (no-slip) or u -/+ w dyp (free-slip)
-template <class T>
-__device__ __forceinline__ T at_jm(const T* __restrict__ a, const Geo<T>& g, int comp, const Nbr& n, long long o) {
-  if (!n.jlo) return __ldg(a + n.c + o - n.yp);
-  if (comp == 1) return (T)(g.bc.uy_lo * 2.0) - __ldg(a + n.c + o + n.yp);  // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc)
-  const T v = __ldg(a + n.c + o);
-  if (comp == 3) return v;
-  const double w = comp == 0 ? g.bc.ux_lo : g.bc.uz_lo;
-  return g.bc.lo == -1 ? (T)(w * 2.0) - v : v - (T)(w * g.bc.dyp1);
-}
-template <class T>
-__device__ __forceinline__ T at_jp(const T* __restrict__ a, const Geo<T>& g, int comp, const Nbr& n, long long o) {
-  if (!n.jhi) return __ldg(a + n.c + o + n.yp);
-  if (comp == 1) return (T)g.bc.uy_hi;  // uy(ic,nyp,kc) = uyBcValue(yp)
-  const T v = __ldg(a + n.c + o);
-  if (comp == 3) return v;
-  const double w = comp == 0 ? g.bc.ux_hi : g.bc.uz_hi;
-  return g.bc.hi == -1 ? (T)(w * 2.0) - v : (T)(w * g.bc.dypN) + v;
-}
-
 // One component of clcRhsX/Y/Z_PIMP at one cell (C = 0, 1, 2), with its Hist
 // update; used by the fused solve kernel, where one block handles one component.
 template <class T, int C>
@@ -275,6 +233,11 @@ __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, cons
     T d33q1 = g.ap3c * ux_kp + g.ac3c * ux_c + g.am3c * ux_km;
     T dcq13 = d11q1 + d33q1;
     T gradp1 = (p_c - p_im) * rdx;
+    if (g.implicit == 2) {  // clcRhsX_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:45-55)
+      T convEd1 = -h11 - h12 - h13 + g.g1;
+      h[n.c] = convEd1;
+      return pmGamma * convEd1 + pmTheta * h_o - pmAlpha * gradp1 + two * pmBeta * (d11q1 + d22q1 + d33q1);
+    }
     T convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g.g1;
     h[n.c] = convEd1;
     return pmGamma * convEd1 + pmTheta * h_o - pmAlpha * gradp1 + two * pmBeta * d22q1;
@@ -298,6 +261,11 @@ __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, cons
     T d33q2 = g.ap3c * uy_kp + g.ac3c * uy_c + g.am3c * uy_km;
     T dcq13 = d11q2 + d33q2;
     T gradp2 = (p_c - p_jm) * sucac;
+    if (g.implicit == 2) {  // clcRhsY_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:104-115)
+      T convEd2 = -h21 - h22 - h23 + g.g2;
+      h[n.c] = convEd2;
+      return pmGamma * convEd2 + pmTheta * h_o - pmAlpha * gradp2 + two * pmBeta * (d11q2 + d22q2 + d33q2);
+    }
     T convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g.g2;
     h[n.c] = convEd2;
     return pmGamma * convEd2 + pmTheta * h_o - pmAlpha * gradp2 + two * pmBeta * d22q2;
@@ -322,6 +290,11 @@ __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, cons
     T d33q3 = (uz_kp - two * uz_c + uz_km) * rdz2;
     T dcq13 = d11q3 + d33q3;
     T gradp3 = (p_c - p_km) * rdz;
+    if (g.implicit == 2) {  // clcRhsZ_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:161-172)
+      T convEd3 = -h31 - h32 - h33 + g.g3;
+      h[n.c] = convEd3;
+      return pmGamma * convEd3 + pmTheta * h_o - pmAlpha * gradp3 + two * pmBeta * (d11q3 + d22q3 + d33q3);
+    }
     T convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g.g3;
     h[n.c] = convEd3;
     return pmGamma * convEd3 + pmTheta * h_o - pmAlpha * gradp3 + two * pmBeta * d22q3;
@@ -347,46 +320,25 @@ __global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const 
   rx[idx] = a; ry[idx] = b; rz[idx] = c;
 }
 
-// ---------------------------------------------------------------------------
-// Partitioned tridiagonal solve (used by clcU*Hat and the Poisson y solve).
-// A system of n rows is cut into P chunks.  Each chunk is solved locally
-// (Thomas) for the data and for two "spikes" (its response to the unknown
-// just left of and just right of it); the 2(P-1) interface unknowns then
-// satisfy a 2x2-block tridiagonal system solved by one thread.  This is the
-// same decomposition as the reference's InverseTridiagonal_reduce
-// (src/CFD_2nd/m_Poisson.f90:1462) applied inside one thread block.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ int chunk_lo(int p, int n, int P) { return (p * n) / P; }
-__device__ __forceinline__ int chunk_hi(int p, int n, int P) { return ((p + 1) * n) / P - 1; }
-// the chunk p with chunk_lo(p) <= j <= chunk_hi(p): the largest p with p*n/P <= j
-__device__ __forceinline__ int chunk_of(int j, int n, int P) { return ((j + 1) * P - 1) / n; }
-
-// Coefficients of the velocity Helmholtz systems (identical for all columns).
-// set 0: clcU1Hat_PIMP / clcU3Hat_PIMP (m_TSchemePIMP_inc.f90:410-416, 720-726)
-// set 1: clcU2Hat_PIMP (:561-572), row 1 is the identity.
-struct HelmCoef {
-  const double* ap2cForCN; const double* am2cForCN;
-  const double* ap2p; const double* ac2p; const double* am2p;
-};
-
-__device__ __forceinline__ void helm_abc(const HelmCoef& hc, int set, double pmBeta, int j, double& a, double& b,
-                                         double& c) {
-  const int jc = j + 1;
-  if (set == 1) {
-    if (j == 0) { a = 0.0; b = 1.0; c = 0.0; return; }
-    c = -pmBeta * hc.ap2p[jc];
-    b = -pmBeta * hc.ac2p[jc] + 1.0;
-    a = -pmBeta * hc.am2p[jc];
-  } else {
-    c = -pmBeta * hc.ap2cForCN[jc];
-    a = -pmBeta * hc.am2cForCN[jc];
-    b = -c - a + 1.0;
-  }
+// clcRhsX/Y/Z_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:6-177), one thread per
+// cell, RhsX with the mean pressure gradient (:57-66) included.
+template <class T>
+__global__ void __launch_bounds__(256) k_rhs_fimp(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                  const T* __restrict__ uy, const T* __restrict__ uz,
+                                                  const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
+                                                  T* __restrict__ hz, T* __restrict__ rx, T* __restrict__ ry,
+                                                  T* __restrict__ rz, const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
+  const long long idx = i + (long long)g.nx * (j + (long long)g.ny * k);
+  rx[idx] = rhs_comp<T, 0>(g, m, ux, uy, uz, pr, hx, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta) + (T)sc->dpmdxns;
+  ry[idx] = rhs_comp<T, 1>(g, m, ux, uy, uz, pr, hy, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
+  rz[idx] = rhs_comp<T, 2>(g, m, ux, uy, uz, pr, hz, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
 }
-
-// Factor layout of one set: RM | AA | CP | AL | BE (ny each), then per
-// interface q: M00 M01 M10 M11 l v (6 each).
-__host__ __device__ inline int helm_set_stride(int ny, int P) { return 5 * ny + 6 * (P > 1 ? P - 1 : 1); }
 
 // Precomputes the chunk factors, spikes and interface block-Thomas factors of
 // both Helmholtz sets for the current pmBeta (once per substep; block = set).
@@ -433,36 +385,6 @@ __global__ void k_helm_factors(HelmCoef hc, int ny, int P, double* __restrict__ 
   }
 }
 
-// Interface (reduced) block-tridiagonal solve of one column, with the
-// precomputed factors; F: chunk-local solutions of the column (stride fs).
-template <class T>
-__device__ __forceinline__ void helm_interfaces(const double* __restrict__ IFD, const T* F, int fs, int ny, int P,
-                                                T* G /* 2*(P-1) */) {
-  const int Q = P - 1;
-  T gu = (T)0, gw = (T)0;
-  for (int q = 0; q < Q; ++q) {
-    const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
-    const double* R = IFD + 6 * q;
-    const T ru = F[eq * fs] - (q > 0 ? (T)R[4] * gu : (T)0);
-    const T rw = F[sq1 * fs];
-    gu = (T)R[0] * ru + (T)R[1] * rw;
-    gw = (T)R[2] * ru + (T)R[3] * rw;
-    G[2 * q] = gu;
-    G[2 * q + 1] = gw;
-  }
-  if (Q < 1) return;
-  T zw = G[2 * (Q - 1) + 1];
-  for (int q = Q - 2; q >= 0; --q) {
-    const double* R = IFD + 6 * q;
-    const T f = (T)R[5] * zw;
-    const T zu = G[2 * q] - (T)R[1] * f;
-    const T zwn = G[2 * q + 1] - (T)R[3] * f;
-    G[2 * q] = zu;
-    G[2 * q + 1] = zwn;
-    zw = zwn;
-  }
-}
-
 // clcU1Hat/U2Hat/U3Hat_PIMP from RhsX/Y/Z in memory (stage-level entry point):
 // (I - pmBeta L_y) du = Rhs ; u* = u + du written to the u* buffers.
 // Block: TI consecutive i at one k, all j; threads = TI * P; blockIdx.z = component.
@@ -485,7 +407,8 @@ __global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, const double* __res
                *IFD = F64 + 5 * ny;
   T* F = (T*)smem_raw;                    // ny * TI
   T* IF = F + (size_t)ny * TI;            // TI * 2Q
-  const T add = comp == 0 ? (T)sc->dpmdxns : (T)0;
+  // the 4th-order and FIMP RhsX already carry the forcing (k_rhs4, k_rhs_fimp)
+  const T add = (comp == 0 && g.order != 4 && g.implicit != 2) ? (T)sc->dpmdxns : (T)0;
   const int tid = threadIdx.x;
   for (int t = tid; t < TI * P; t += blockDim.x) {
     const int ii = t % TI, p = t / TI, i = i0 + ii;
@@ -610,7 +533,7 @@ __global__ void __launch_bounds__(256) k_prsrc_xfft(Geo<T> g, Metrics<T> m, cons
                                                     typename CplxOf<T>::type* __restrict__ spec, FFTPlanDev pl,
                                                     const typename CplxOf<T>::type* __restrict__ tw,
                                                     const typename CplxOf<T>::type* __restrict__ twr, int LPB, int mode,
-                                                    DevScalars* __restrict__ sc) {
+                                                    DevScalars* __restrict__ sc, T* __restrict__ pr) {
   typedef typename CplxOf<T>::type CT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (sc->status) return;
@@ -639,7 +562,17 @@ __global__ void __launch_bounds__(256) k_prsrc_xfft(Geo<T> g, Metrics<T> m, cons
     const T w0p = uz[basep + i0], w1p = uz[basep + i1];
     T r0 = (u1 - u0) * rdx + (v0p - v0) * sucaj + (w0p - w0) * rdz;
     T r1 = (u2 - u1) * rdx + (v1p - v1) * sucaj + (w1p - w1) * rdz;
+    if (g.order == 4) {
+      const C4<T> c4(g);
+      r0 = div4_cell(g, c4, sucaj, ux, uy, uz, i0, j, k);
+      r1 = div4_cell(g, c4, sucaj, ux, uy, uz, i1, j, k);
+    }
     if (mode == 2) { r0 = u0; r1 = u1; }  // standalone Poisson: ux carries the source
+    if (mode == 0 && g.implicit == 2) {     // clcPrSrc_FIMP: pressure += -xnu/2 div (m_TScheme.f90:271)
+      const T xnuhm = -(T)0.5 * g.xnu;
+      pr[base + i0] = pr[base + i0] + xnuhm * r0;
+      pr[base + i1] = pr[base + i1] + xnuhm * r1;
+    }
     dmax = fmax(dmax, fmax(fabs((double)r0), fabs((double)r1)));
     A[l * M + n] = mk(sudtal * r0, sudtal * r1);
   }
@@ -1110,13 +1043,25 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
     const T phim_y = phi[i + (long long)nx * ((j > 0 ? j - 1 : 0) + (long long)ny * k)];
     const T phim_z = phi[i + (long long)nx * (j + (long long)ny * km)];
     const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha, sucacEta2 = m.rdyc[jc] * pmAlpha;
-    const T uxn = uxs[idx] - (phic - phim_x) * rdxEta2;
-    const T uyn = uys[idx] - (phic - phim_y) * sucacEta2;
-    const T uzn = uzs[idx] - (phic - phim_z) * rdzEta2;
+    T uxn = uxs[idx] - (phic - phim_x) * rdxEta2;
+    T uyn = uys[idx] - (phic - phim_y) * sucacEta2;
+    T uzn = uzs[idx] - (phic - phim_z) * rdzEta2;
+    if (g.order == 4) {  // FluidVelUpdate, src/CFD_4th/m_TScheme.f90:148-173
+      const C4<T> c4(g);
+      const Nbr n = make_nbr(g, i, j, k);
+      const T dpdx = c4.dx1 * at(phi, n, n.xm2) + c4.dx2 * phim_x + c4.dx3 * phic + c4.dx4 * at(phi, n, n.xp);
+      const T dpdy = (phic - phim_y) * m.rdyc[jc];
+      const T dpdz = c4.dz1 * at(phi, n, n.zm2) + c4.dz2 * phim_z + c4.dz3 * phic + c4.dz4 * at(phi, n, n.zp);
+      uxn = uxs[idx] - pmAlpha * dpdx;
+      uyn = uys[idx] - pmAlpha * dpdy;
+      uzn = uzs[idx] - pmAlpha * dpdz;
+    }
     ux[idx] = uxn;
     uy[idx] = uyn;
     uz[idx] = uzn;
-    if (mode == 0) {
+    if (mode == 0 && g.implicit == 2) {
+      pr[idx] = pr[idx] + phic;  // PressureUpdate_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386)
+    } else if (mode == 0) {
       const T phip_y = phi[i + (long long)nx * ((j < ny - 1 ? j + 1 : ny - 1) + (long long)ny * k)];
       const T pmBeta = (T)sc->pmBeta;
       const T pmBetap = -pmBeta * m.ap2Pr[jc];
@@ -1179,6 +1124,7 @@ __global__ void __launch_bounds__(256) k_diag(Geo<T> g, Metrics<T> m, const T* _
     const double ckp = uz[i + (long long)nx * (j + (long long)ny * kp)];
     const double rdx = g.rdx, rdz = g.rdz, rdyp = m.rdyp[jc];
     dv = fabs((aip - a) * rdx + (bjp - b) * rdyp + (ckp - c) * rdz);
+    if (g.order == 4) dv = fabs((double)div4_cell(g, C4<T>(g), m.rdyp[jc], ux, uy, uz, i, j, k));
     v0 = fabs(a); v1 = fabs(b); v2 = fabs(c);
     cf = fabs(a + aip) * rdx + fabs(b + bjp) * rdyp + fabs(c + ckp) * rdz;
     s = a * (double)m.dyp[jc];
@@ -1230,6 +1176,7 @@ __global__ void __launch_bounds__(256) k_divmax(Geo<T> g, Metrics<T> m, const T*
     dv = fabs(((double)ux[ip + (long long)g.nx * (j + (long long)g.ny * k)] - ux[idx]) * g.rdx +
               ((double)fld(uy, g, 1, i, j + 1, k) - uy[idx]) * m.rdyp[j + 1] +
               ((double)uz[i + (long long)g.nx * (j + (long long)g.ny * kp)] - uz[idx]) * g.rdz);
+    if (g.order == 4) dv = fabs((double)div4_cell(g, C4<T>(g), m.rdyp[j + 1], ux, uy, uz, i, j, k));
   }
   red[tl] = dv;
   __syncthreads();
@@ -1243,27 +1190,6 @@ __global__ void __launch_bounds__(256) k_divmax(Geo<T> g, Metrics<T> m, const T*
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-template <class T> Geo<T> make_geo(const ch3d_ctx* c) {
-  Geo<T> g;
-  g.nx = c->nx; g.ny = c->ny; g.nz = c->nz; g.nxh = c->nxh; g.N = c->N;
-  g.rdx = (T)c->rdx; g.rdz = (T)c->rdz; g.rdx2 = (T)c->rdx2; g.rdz2 = (T)c->rdz2;
-  // periodic x and z: am1c = ap1c = rdx2, ac1c = -(am1c+ap1c) (m_MeshAndMetries.f90:243-252)
-  g.ap1c = (T)c->rdx2; g.am1c = (T)c->rdx2; g.ac1c = (T)(-(c->rdx2 + c->rdx2));
-  g.ap3c = (T)c->rdz2; g.am3c = (T)c->rdz2; g.ac3c = (T)(-(c->rdz2 + c->rdz2));
-  g.xnu = (T)c->cfg.xnu;
-  g.g1 = (T)c->cfg.gravity[0]; g.g2 = (T)c->cfg.gravity[1]; g.g3 = (T)c->cfg.gravity[2];
-  g.bc.lo = c->cfg.BcOption[2]; g.bc.hi = c->cfg.BcOption[3];
-  g.bc.ux_lo = c->cfg.uxBcValue[2]; g.bc.ux_hi = c->cfg.uxBcValue[3];
-  g.bc.uy_lo = c->cfg.uyBcValue[2]; g.bc.uy_hi = c->cfg.uyBcValue[3];
-  g.bc.uz_lo = c->cfg.uzBcValue[2]; g.bc.uz_hi = c->cfg.uzBcValue[3];
-  g.bc.dyp1 = c->dyp[1]; g.bc.dypN = c->dyp[c->ny + 1];
-  return g;
-}
-
-template <class T> const Metrics<T>& metrics_of(const ch3d_ctx* c);
-template <> const Metrics<double>& metrics_of<double>(const ch3d_ctx* c) { return c->m64; }
-template <> const Metrics<float>& metrics_of<float>(const ch3d_ctx* c) { return c->m32; }
-
 static dim3 cell_grid(const ch3d_ctx* c) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz); }
 static dim3 cell_block() { return dim3(32, 8, 1); }
 
@@ -1294,7 +1220,8 @@ cudaError_t launch_substep_setup(ch3d_ctx* c, int ns) {
   k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part, c->npart, c->red1);
   const double norm_bulk = 1.0 / ((double)c->nx * (double)c->nz) / (c->cfg.ybulk2 - c->cfg.ybulk1);
   k_substep_setup<<<1, 256, 0, c->stream>>>(c->sc, c->red1, CH3D_NRED, ns, c->gam[ns - 1], c->the[ns - 1],
-                                            c->alp[ns - 1], c->cfg.xnu, c->cfg.IsUxConst, c->cfg.ubulk, norm_bulk);
+                                            c->alp[ns - 1], c->cfg.xnu, c->cfg.IsUxConst, c->cfg.ubulk, norm_bulk,
+                                            c->cfg.order, (double)(c->nx * c->nz), c->cfg.yly);
   return cudaGetLastError();
 }
 
@@ -1312,6 +1239,13 @@ template <class T> static cudaError_t rhs_t(ch3d_ctx* c) {
   return cudaGetLastError();
 }
 cudaError_t launch_rhs(ch3d_ctx* c) { return c->fp32 ? rhs_t<float>(c) : rhs_t<double>(c); }
+template <class T> static cudaError_t rhs_fimp_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  k_rhs_fimp<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], f[3],
+                                                              f[4], f[5], f[6], f[7], f[8], f[9], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_rhs_fimp(ch3d_ctx* c) { return c->fp32 ? rhs_fimp_t<float>(c) : rhs_fimp_t<double>(c); }
 
 static HelmCoef helm_coef(const ch3d_ctx* c) {
   HelmCoef hc;
@@ -1395,7 +1329,7 @@ template <class T> static cudaError_t prsrc_t(ch3d_ctx* c, int mode) {
   T* cz = mode == 1 ? f[2] : f[14];
   k_prsrc_xfft<T><<<(nlines + LPB - 1) / LPB, nthr, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), a, b, cz,
                                                                       (CT*)c->spec, c->planx, (const CT*)c->twx,
-                                                                      (const CT*)c->twr, LPB, mode, c->sc);
+                                                                      (const CT*)c->twr, LPB, mode, c->sc, f[3]);
   return cudaGetLastError();
 }
 cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode) { return c->fp32 ? prsrc_t<float>(c, mode) : prsrc_t<double>(c, mode); }
@@ -1793,7 +1727,7 @@ cudaError_t poisson_noalloc(int nx, int ny, int nz, double xlx, double zlz, cons
   }
   const int nlines = ny * nz;
   k_prsrc_xfft<double><<<(nlines + LPB - 1) / LPB, 256, (size_t)2 * LPB * M * sizeof(double2), st>>>(
-      g, m, d_src, d_src, d_src, spec, planx, twx, twr, LPB, 2, sc);
+      g, m, d_src, d_src, d_src, spec, planx, twx, twr, LPB, 2, sc, nullptr);
   int TKX = kFFTSmem / (2 * nz * (int)sizeof(double2));
   int tk = 1;
   while (tk * 2 <= TKX && tk * 2 <= 16) tk *= 2;

@@ -24,6 +24,8 @@ WORKLOADS = {
     "channel64_re5600": (lambda **kw: channel(64, 64, 64, 2 * np.pi, np.pi, 5600.0, 0.002, **kw), 200),
     # 4th-order solver, 128^3, 4pi x 2 x 4pi/3, Re_b 5600, dt 0.001, 1000 steps
     "channel128_re5600_4th": (lambda **kw: channel(128, 128, 128, 4 * np.pi, 4 * np.pi / 3, 5600.0, 0.001, order=4, **kw), 1000),
+    # 2nd-order fully implicit (ADI: periodic x, periodic z, then y Crank-Nicolson), 128^3, same box
+    "channel128_re5600_fimp": (lambda **kw: channel(128, 128, 128, 4 * np.pi, 4 * np.pi / 3, 5600.0, 0.001, implicit=2, **kw), 1000),
     # 2nd-order, 256x192x256, Re_b 13750, dt 0.0005, 2000 steps (FP64 vs mixed)
     "channel256x192x256_re13750": (lambda **kw: channel(256, 192, 256, 2 * np.pi, np.pi, 13750.0, 0.0005, **kw), 2000),
     # LES grid, 48^3, 2pi x 2 x pi, dt 0.002

@@ -210,6 +210,15 @@ struct Oracle {
   V1 ap2Pr, ac2Pr, am2Pr, am1c, ac1c, ap1c, am2c, ac2c, ap2c, am2p, ac2p, ap2p, am3c, ac3c, ap3c;
   V1 am2cForCN, ap2cForCN, am1cForCN, ap1cForCN, am3cForCN, ap3cForCN;
 
+  // 4th-order solver (src/CFD_4th): stencil constants and CN metrics
+  bool o4 = false;
+  double dxCoe1, dxCoe2, dxCoe3, dxCoe4, dzCoe1, dzCoe2, dzCoe3, dzCoe4;
+  double dxxCoe1, dxxCoe2, dxxCoe3, dxxCoe4, dxxCoe5, dzzCoe1, dzzCoe2, dzzCoe3, dzzCoe4, dzzCoe5;
+  double InterpCoe1, InterpCoe2, InterpCoe3, InterpCoe4;
+  const double uCRF = 0.0;  // IsUseCRF = F (src/CFD_4th/m_Parameters.f90:152-156)
+  V1 ac2cForCN;
+  F3 uxhx, uyhx, uzhx, uxhz, uyhz, uzhz;
+
   // Poisson
   V1 WaveNumX, WaveNumZ;
   double normfft = 1.0;
@@ -388,8 +397,32 @@ struct Oracle {
     planz.init(nzc);
   }
 
+  // ---- src/CFD_4th/m_MeshAndMetries.f90:86-91 (4th-order FD constants) ----
+  void Init4thCoefficients() {
+    dxCoe1 = rdx / 24.0; dxCoe2 = -rdx * 1.125; dxCoe3 = rdx * 1.125; dxCoe4 = -rdx / 24.0;
+    dzCoe1 = rdz / 24.0; dzCoe2 = -rdz * 1.125; dzCoe3 = rdz * 1.125; dzCoe4 = -rdz / 24.0;
+    dxxCoe1 = -rdx2 / 12.0; dxxCoe2 = 4.0 / 3.0 * rdx2; dxxCoe3 = -2.5 * rdx2; dxxCoe4 = 4.0 / 3.0 * rdx2; dxxCoe5 = -rdx2 / 12.0;
+    dzzCoe1 = -rdz2 / 12.0; dzzCoe2 = 4.0 / 3.0 * rdz2; dzzCoe3 = -2.5 * rdz2; dzzCoe4 = 4.0 / 3.0 * rdz2; dzzCoe5 = -rdz2 / 12.0;
+    InterpCoe1 = -1.0 / 16.0; InterpCoe2 = 9.0 / 16.0; InterpCoe3 = 9.0 / 16.0; InterpCoe4 = -1.0 / 16.0;
+  }
+
+  // ---- src/CFD_4th/m_TScheme.f90:35-51 (InitTimeScheme, CN metrics) ----
+  void InitTimeScheme4() {
+    am2cForCN.init(1, nyc); ac2cForCN.init(1, nyc); ap2cForCN.init(1, nyc);
+    for (int j = 1; j <= nyc; ++j) { ap2cForCN(j) = ap2c(j); ac2cForCN(j) = ac2c(j); am2cForCN(j) = am2c(j); }
+    ap2cForCN(1) = ap2c(1);
+    ac2cForCN(1) = ac2c(1) - am2c(1);
+    am2cForCN(1) = two * am2c(1);
+    if (P.FlowType == 1) {
+      am2cForCN(nyc) = am2c(nyc);
+      ac2cForCN(nyc) = ac2c(nyc) - ap2c(nyc);
+      ap2cForCN(nyc) = two * ap2c(nyc);
+    }
+  }
+
   void init(const orc_params* p) {
     P = *p;
+    o4 = (P.order == 4);
     nxc = P.nxc; nyc = P.nyc; nzc = P.nzc; nxp = nxc + 1; nyp = nyc + 1; nzp = nzc + 1;
     // src/CFD_2nd/m_Parameters.f90:288-306
     if (P.ischeme == 1) {
@@ -409,13 +442,33 @@ struct Oracle {
     InitMeshAndMetries();
     InitTimeScheme();
     InitPoissonSolver();
-    // src/CFD_2nd/m_Variables.f90:59-61 (ghosts xme=1,xpe=2,...)
-    ux.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
-    uy.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
-    uz.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
-    pressure.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
-    RealHalo.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
-    nut.init(0, nxc + 2, 0, nyc + 2, 0, nzc + 2);
+    if (o4) {
+      Init4thCoefficients();
+      InitTimeScheme4();
+      // src/CFD_4th/m_Poisson.f90:40-47 (4th-order modified wavenumbers)
+      for (int i = 1; i <= nxc; ++i) {
+        double wa1 = 2.0 * PI * (double)(i - 1) / (double)nxc;
+        WaveNumX(i) = rdx2 / 288.0 * (std::cos(three * wa1) - 54.0 * std::cos(two * wa1) + 783.0 * std::cos(wa1) - 730.0);
+      }
+      for (int k = 1; k <= nzc; ++k) {
+        double wa3 = 2.0 * PI * (double)(k - 1) / (double)nzc;
+        WaveNumZ(k) = rdz2 / 288.0 * (std::cos(three * wa3) - 54.0 * std::cos(two * wa3) + 783.0 * std::cos(wa3) - 730.0);
+      }
+      normfft = one / ((double)nxc * (double)nzc);
+    }
+    // ghosts: src/CFD_2nd/m_Variables.f90:59-61 (xme=1,xpe=2,...) or
+    // src/CFD_4th/m_Variables.f90:47-49 (xme=2,xpe=2,yme=1,ype=1,zme=2,zpe=2)
+    const int gx0 = o4 ? -1 : 0, gx1 = nxc + 2, gy1 = o4 ? nyc + 1 : nyc + 2, gz0 = o4 ? -1 : 0, gz1 = nzc + 2;
+    ux.init(gx0, gx1, 0, gy1, gz0, gz1);
+    uy.init(gx0, gx1, 0, gy1, gz0, gz1);
+    uz.init(gx0, gx1, 0, gy1, gz0, gz1);
+    pressure.init(gx0, gx1, 0, gy1, gz0, gz1);
+    RealHalo.init(gx0, gx1, 0, gy1, gz0, gz1);
+    nut.init(gx0, gx1, 0, gy1, gz0, gz1);
+    if (o4) {
+      uxhx.init(gx0, gx1, 0, gy1, gz0, gz1); uyhx.init(gx0, gx1, 0, gy1, gz0, gz1); uzhx.init(gx0, gx1, 0, gy1, gz0, gz1);
+      uxhz.init(gx0, gx1, 0, gy1, gz0, gz1); uyhz.init(gx0, gx1, 0, gy1, gz0, gz1); uzhz.init(gx0, gx1, 0, gy1, gz0, gz1);
+    }
     HistX.init(1, nxc, 1, nyc, 1, nzc); HistY.init(1, nxc, 1, nyc, 1, nzc); HistZ.init(1, nxc, 1, nyc, 1, nzc);
     RealArr1.init(1, nxc, 1, nyc, 1, nzc); RealArr2.init(1, nxc, 1, nyc, 1, nzc);
     uy_ym.assign((size_t)nxc * nzc, 0.0); duy_ym.assign((size_t)nxc * nzc, 0.0);
@@ -607,8 +660,10 @@ struct Oracle {
     for (int j = n - 2; j >= 0; --j) fj[j] = fj[j] - arr[j + 1] * fj[j + 1];
   }
 
-  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75 (clcRhsX_PIMP) ----
-  void clcRhsX_PIMP(F3& RhsX, F3& Hist) {
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75 (clcRhsX_PIMP); with fimp the
+  //      same loop is clcRhsX_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:6-67): no
+  //      explicit viscous term in convEd1, 2*pmBeta*(d11+d22+d33) instead ----
+  void clcRhsX_PIMP(F3& RhsX, F3& Hist, bool fimp = false) {
     double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
     std::vector<double> part(nzc + 1, 0.0);
     const double g1 = P.gravity[0], xnu = P.xnu;
@@ -637,8 +692,10 @@ struct Oracle {
           double dcq13 = d11q1 + d33q1;
           double gradp1 = (pressure(ic, jc, kc) - pressure(im, jc, kc)) * rdx;
           s1tot = s1tot + ux(ic, jc, kc) * s1totCoe;
-          double convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g1;
-          RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1 + two * pmBeta * d22q1;
+          double convEd1, dcn;
+          if (fimp) { convEd1 = -h11 - h12 - h13 + g1; dcn = d11q1 + d22q1 + d33q1; }
+          else { convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g1; dcn = d22q1; }
+          RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1 + two * pmBeta * dcn;
           Hist(ic, jc, kc) = convEd1;
         }
       }
@@ -657,8 +714,9 @@ struct Oracle {
     }
   }
 
-  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:161-209 (clcRhsY_PIMP) ----
-  void clcRhsY_PIMP(F3& RhsY, F3& Hist) {
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:161-209 (clcRhsY_PIMP); fimp:
+  //      clcRhsY_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:72-119) ----
+  void clcRhsY_PIMP(F3& RhsY, F3& Hist, bool fimp = false) {
     double hdx1 = half * rdx, hdx3 = half * rdz;
     const double g2 = P.gravity[1], xnu = P.xnu;
 #pragma omp parallel for schedule(static)
@@ -681,8 +739,10 @@ struct Oracle {
           double d33q2 = ap3c(kc) * uy(ic, jc, kp) + ac3c(kc) * uy(ic, jc, kc) + am3c(kc) * uy(ic, jc, km);
           double dcq13 = d11q2 + d33q2;
           double gradp2 = (pressure(ic, jc, kc) - pressure(ic, jm, kc)) * sucac;
-          double convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g2;
-          RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2 + two * pmBeta * d22q2;
+          double convEd2, dcn;
+          if (fimp) { convEd2 = -h21 - h22 - h23 + g2; dcn = d11q2 + d22q2 + d33q2; }
+          else { convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g2; dcn = d22q2; }
+          RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2 + two * pmBeta * dcn;
           Hist(ic, jc, kc) = convEd2;
         }
       }
@@ -690,8 +750,9 @@ struct Oracle {
   }
 
   // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:277-325 (clcRhsZ_PIMP); RhsZ is the
-  //      ghosted RealHalo in the reference, only its interior is written ----
-  void clcRhsZ_PIMP(F3& RhsZ, F3& Hist) {
+  //      ghosted RealHalo in the reference, only its interior is written; fimp:
+  //      clcRhsZ_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:124-177) ----
+  void clcRhsZ_PIMP(F3& RhsZ, F3& Hist, bool fimp = false) {
     double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
     const double g3 = P.gravity[2], xnu = P.xnu;
 #pragma omp parallel for schedule(static)
@@ -715,8 +776,10 @@ struct Oracle {
           double d33q3 = (uz(ic, jc, kp) - two * uz(ic, jc, kc) + uz(ic, jc, km)) * rdz2;
           double dcq13 = d11q3 + d33q3;
           double gradp3 = (pressure(ic, jc, kc) - pressure(ic, jc, km)) * rdz;
-          double convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g3;
-          RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3 + two * pmBeta * d22q3;
+          double convEd3, dcn;
+          if (fimp) { convEd3 = -h31 - h32 - h33 + g3; dcn = d11q3 + d22q3 + d33q3; }
+          else { convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g3; dcn = d22q3; }
+          RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3 + two * pmBeta * dcn;
           Hist(ic, jc, kc) = convEd3;
         }
       }
@@ -766,6 +829,441 @@ struct Oracle {
           for (int jc = 1; jc <= nyc; ++jc) uy(ic, jc, kc) = uy(ic, jc, kc) + f[jc - 1];
         }
     }
+  }
+
+  // ---- src/CFD_2nd/m_Tools.f90:167-219 (InversePTriFixedCoe), one periodic
+  //      system with constant coefficients (a: sub, b: diagonal, c: super),
+  //      values f[q*stride], q = 0..n-1 ----
+  static void InversePTriFixedCoe1(double ajf, double bjf, double cjf, double* fj, int n, long long stride,
+                                   std::vector<double>& ppj, std::vector<double>& vecn1, std::vector<double>& vecn2,
+                                   std::vector<double>& arrmn) {
+    // Fortran index j = 1..n maps to element j-1
+    ppj.assign(n + 1, 0.0); vecn1.assign(n + 1, 0.0); vecn2.assign(n + 1, 0.0); arrmn.assign(n + 1, 0.0);
+    auto F = [&](int j) -> double& { return fj[(long long)(j - 1) * stride]; };
+    vecn1[1] = -cjf / bjf;
+    vecn2[1] = -ajf / bjf;
+    vecn2[n] = one;
+    for (int j = 2; j <= n - 1; ++j) {
+      ppj[j] = one / (bjf + ajf * vecn1[j - 1]);
+      vecn1[j] = -cjf * ppj[j];
+      vecn2[j] = -ajf * vecn2[j - 1] * ppj[j];
+    }
+    for (int j = n - 1; j >= 1; --j) vecn2[j] = vecn2[j] + vecn1[j] * vecn2[j + 1];
+    F(1) = F(1) / bjf;
+    for (int j = 2; j <= n - 1; ++j) F(j) = (F(j) - ajf * F(j - 1)) * ppj[j];
+    arrmn[n] = zero;
+    for (int j = n - 1; j >= 1; --j) arrmn[j] = F(j) + vecn1[j] * arrmn[j + 1];
+    F(n) = (F(n) - cjf * arrmn[1] - ajf * arrmn[n - 1]) / (cjf * vecn2[1] + ajf * vecn2[n - 1] + bjf);
+    for (int j = n - 1; j >= 1; --j) F(j) = F(n) * vecn2[j] + arrmn[j];
+  }
+
+  // ---- src/CFD_2nd/m_TSchemeFIMP_inc.f90:263-347 (clcU1Hat_FIMP_010), :636-729
+  //      (clcU2Hat_FIMP_010), :1035-1128 (clcU3Hat_FIMP_010): periodic x sweep,
+  //      periodic z sweep (constant coefficients), then the y sweep of the PIMP
+  //      solvers.  The transposes of the reference only move data. ----
+  void clcUHat_FIMP_xz(F3& Rhs) {
+    const double mic = -pmBeta * rdx2, pic = -pmBeta * rdx2, cic = pmBeta * rdx2 * two + one;
+    const double mkc = -pmBeta * rdz2, pkc = -pmBeta * rdz2, ckc = pmBeta * rdz2 * two + one;
+#pragma omp parallel
+    {
+      std::vector<double> a, b, c, d, line(std::max(nxc, nzc));
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) {
+          for (int ic = 1; ic <= nxc; ++ic) line[ic - 1] = Rhs(ic, jc, kc);
+          InversePTriFixedCoe1(mic, cic, pic, line.data(), nxc, 1, a, b, c, d);
+          for (int ic = 1; ic <= nxc; ++ic) Rhs(ic, jc, kc) = line[ic - 1];
+        }
+    }
+#pragma omp parallel
+    {
+      std::vector<double> a, b, c, d, line(std::max(nxc, nzc));
+#pragma omp for schedule(static)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int kc = 1; kc <= nzc; ++kc) line[kc - 1] = Rhs(ic, jc, kc);
+          InversePTriFixedCoe1(mkc, ckc, pkc, line.data(), nzc, 1, a, b, c, d);
+          for (int kc = 1; kc <= nzc; ++kc) Rhs(ic, jc, kc) = line[kc - 1];
+        }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TScheme.f90:245-276 (clcPrSrc_FIMP): clcPrSrcOther plus
+  //      pressure += -xnu/2 * div ----
+  double clcPrSrc_FIMP(F3& prsrc) {
+    double sudtal = one / pmAlpha, xnuhm = -half * P.xnu;
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int kp = kc + 1;
+      double m = 0;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jp = jc + 1;
+        double sucaj = rdyp(jc);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int ip = ic + 1;
+          double rdiv = (ux(ip, jc, kc) - ux(ic, jc, kc)) * rdx + (uy(ic, jp, kc) - uy(ic, jc, kc)) * sucaj +
+                        (uz(ic, jc, kp) - uz(ic, jc, kc)) * rdz;
+          m = std::max(std::fabs(rdiv), m);
+          prsrc(ic, jc, kc) = sudtal * rdiv;
+          pressure(ic, jc, kc) = pressure(ic, jc, kc) + xnuhm * rdiv;
+        }
+      }
+      part[kc] = m;
+    }
+    double m = 0;
+    for (int kc = 1; kc <= nzc; ++kc) m = std::max(m, part[kc]);
+    return m;
+  }
+
+  // ---- src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386 (PressureUpdate_FIMP) ----
+  void PressureUpdate_FIMP(const F3& phi) {
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) pressure(ic, jc, kc) = pressure(ic, jc, kc) + phi(ic, jc, kc);
+  }
+
+
+  // =====================================================================
+  // LES (src/CFD_2nd/m_LESModels.f90 and the *_PIMP_LES procedures of
+  // src/CFD_2nd/m_TSchemePIMP_inc.f90); nut includes the molecular xnu
+  // =====================================================================
+  double utau_last = 0;
+
+  // ---- src/CFD_2nd/m_LESModels.f90:72-135 (Clc_SGS_WALE) ----
+  void Clc_SGS_WALE() {
+    const double Cw_ = 0.325, xnu = P.xnu;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jp = jc + 1, jm = jc - 1;
+        double caj = rdyp(jc), cac1 = rdyc(jc), cac2 = rdyc(jp), cac12 = cac1 - cac2;
+        double CwDelta2 = Cw_ * DeltaCell(jc);
+        CwDelta2 = CwDelta2 * CwDelta2;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double dudx = (ux(ip, jc, kc) - ux(ic, jc, kc)) * rdx;
+          double dudy = ((ux(ip, jp, kc) + ux(ic, jp, kc)) * cac2 + (ux(ip, jc, kc) + ux(ic, jc, kc)) * cac12 -
+                         (ux(ip, jm, kc) + ux(ic, jm, kc)) * cac1) * 0.25;
+          double dudz = (ux(ip, jc, kp) + ux(ic, jc, kp) - ux(ip, jc, km) - ux(ic, jc, km)) * rdz * 0.25;
+          double dvdx = (uy(ip, jp, kc) - uy(im, jp, kc) + uy(ip, jc, kc) - uy(im, jc, kc)) * rdx * 0.25;
+          double dvdy = (uy(ic, jp, kc) - uy(ic, jc, kc)) * caj;
+          double dvdz = (uy(ic, jp, kp) + uy(ic, jc, kp) - uy(ic, jp, km) - uy(ic, jc, km)) * rdz * 0.25;
+          double dwdx = (uz(ip, jc, kp) - uz(im, jc, kp) + uz(ip, jc, kc) - uz(im, jc, kc)) * rdx * 0.25;
+          double dwdy = ((uz(ic, jp, kp) + uz(ic, jp, kc)) * cac2 + (uz(ic, jc, kp) + uz(ic, jc, kc)) * cac12 -
+                         (uz(ic, jm, kp) + uz(ic, jm, kc)) * cac1) * 0.25;
+          double dwdz = (uz(ic, jc, kp) - uz(ic, jc, kc)) * rdz;
+          double S11 = dudx, S12 = (dudy + dvdx) * half, S13 = (dudz + dwdx) * half;
+          double S22 = dvdy, S23 = (dvdz + dwdy) * half, S33 = dwdz;
+          double SijSij = S11 * S11 + S22 * S22 + S33 * S33 + two * (S12 * S12 + S13 * S13 + S23 * S23);
+          double Sd11 = dudx * dudx + dudy * dvdx + dudz * dwdx;
+          double Sd12 = (dudx * dudy + dudy * dvdy + dudz * dwdy + dvdx * dudx + dvdy * dvdx + dvdz * dwdx) * half;
+          double Sd13 = (dudx * dudz + dudy * dvdz + dudz * dwdz + dwdx * dudx + dwdy * dvdx + dwdz * dwdx) * half;
+          double Sd22 = dvdx * dudy + dvdy * dvdy + dvdz * dwdy;
+          double Sd23 = (dvdx * dudz + dvdy * dvdz + dvdz * dwdz + dwdx * dudy + dwdy * dvdy + dwdz * dwdy) * half;
+          double Sd33 = dwdx * dudz + dwdy * dvdz + dwdz * dwdz;
+          double SdTrace = (Sd11 + Sd22 + Sd33) / three;
+          Sd11 = Sd11 - SdTrace; Sd22 = Sd22 - SdTrace; Sd33 = Sd33 - SdTrace;
+          double SdijSdij = Sd11 * Sd11 + Sd22 * Sd22 + Sd33 * Sd33 + two * (Sd12 * Sd12 + Sd13 * Sd13 + Sd23 * Sd23);
+          nut(ic, jc, kc) = CwDelta2 * std::pow(SdijSdij, 1.5) / (std::pow(SijSij, 2.5) + std::pow(SdijSdij, 1.25)) + xnu;
+        }
+      }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_LESModels.f90:328-370 (ClcVelStrainRate): |S| = sqrt(2 Sij Sij) ----
+  double StrainRate(int ic, int jc, int kc) {
+    int ip = ic + 1, im = ic - 1, jp = jc + 1, jm = jc - 1, kp = kc + 1, km = kc - 1;
+    double caj = rdyp(jc), cac1 = rdyc(jc), cac2 = rdyc(jp), cac12 = cac1 - cac2;
+    const double oneEighth = 0.125;
+    double st1 = (ux(ip, jc, kc) - ux(ic, jc, kc)) * rdx;
+    double st2 = (uy(ic, jp, kc) - uy(ic, jc, kc)) * caj;
+    double st3 = (uz(ic, jc, kp) - uz(ic, jc, kc)) * rdz;
+    double st4 = oneEighth * ((uy(ip, jp, kc) - uy(im, jp, kc) + uy(ip, jc, kc) - uy(im, jc, kc)) * rdx +
+                              (ux(ip, jp, kc) + ux(ic, jp, kc)) * cac2 + (ux(ip, jc, kc) + ux(ic, jc, kc)) * cac12 -
+                              (ux(ip, jm, kc) + ux(ic, jm, kc)) * cac1);
+    double st5 = oneEighth * ((ux(ip, jc, kp) + ux(ic, jc, kp) - ux(ip, jc, km) - ux(ic, jc, km)) * rdz +
+                              (uz(ip, jc, kp) - uz(im, jc, kp) + uz(ip, jc, kc) - uz(im, jc, kc)) * rdx);
+    double st6 = oneEighth * ((uy(ic, jp, kp) + uy(ic, jc, kp) - uy(ic, jp, km) - uy(ic, jc, km)) * rdz +
+                              (uz(ic, jp, kp) + uz(ic, jp, kc)) * cac2 + (uz(ic, jc, kp) + uz(ic, jc, kc)) * cac12 -
+                              (uz(ic, jm, kp) + uz(ic, jm, kc)) * cac1);
+    return std::sqrt(two * (st1 * st1 + st2 * st2 + st3 * st3) + four * (st4 * st4 + st5 * st5 + st6 * st6));
+  }
+
+  // ---- src/CFD_2nd/m_LESModels.f90:145-258 (Clc_SGS_MTS), filter from InitFilterCoe :35-41 ----
+  void Clc_SGS_MTS() {
+    double Fc[9];
+    if (P.FilterType == 1) { const double f[9] = {1, 4, 1, 4, 16, 4, 1, 4, 1}; for (int q = 0; q < 9; ++q) Fc[q] = f[q] / 36.0; }
+    else { const double f[9] = {1, 2, 1, 2, 4, 2, 1, 2, 1}; for (int q = 0; q < 9; ++q) Fc[q] = f[q] / 16.0; }
+    F3 Ktemp;
+    Ktemp.init(ux.xl, ux.xl + ux.sx - 1, ux.yl, ux.yl + ux.sy - 1, ux.zl, ux.zl + ux.sz - 1);
+    std::vector<double> Kes((size_t)nxc * nyc * nzc, 0.0);
+    auto K = [&](int i, int j, int k) -> double& { return Kes[(size_t)(i - 1) + (size_t)nxc * ((size_t)(j - 1) + (size_t)nyc * (k - 1))]; };
+    auto filt = [&](F3& u, int ic, int jc, int kc) {
+      int im = ic - 1, ip = ic + 1, km = kc - 1, kp = kc + 1;
+      return Fc[0] * u(im, jc, km) + Fc[1] * u(ic, jc, km) + Fc[2] * u(ip, jc, km) +
+             Fc[3] * u(im, jc, kc) + (Fc[4] - one) * u(ic, jc, kc) + Fc[5] * u(ip, jc, kc) +
+             Fc[6] * u(im, jc, kp) + Fc[7] * u(ic, jc, kp) + Fc[8] * u(ip, jc, kp);
+    };
+    for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) {
+      double f = filt(ux, ic, jc, kc); Ktemp(ic, jc, kc) = f * f;
+    }
+    halo(Ktemp, 0, 1, 0, 0, 0, 0);
+    for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic)
+      K(ic, jc, kc) = half * (Ktemp(ic, jc, kc) + Ktemp(ic + 1, jc, kc));
+    for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyp; ++jc) for (int ic = 1; ic <= nxc; ++ic) {
+      double f = filt(uy, ic, jc, kc); Ktemp(ic, jc, kc) = f * f;
+    }
+    for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic)
+      K(ic, jc, kc) = K(ic, jc, kc) + half * (Ktemp(ic, jc, kc) + Ktemp(ic, jc + 1, kc));
+    for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) {
+      double f = filt(uz, ic, jc, kc); Ktemp(ic, jc, kc) = f * f;
+    }
+    halo(Ktemp, 0, 0, 0, 0, 0, 1);
+    for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic)
+      K(ic, jc, kc) = K(ic, jc, kc) + half * (Ktemp(ic, jc, kc) + Ktemp(ic, jc, kc + 1));
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc) {
+        double rdelta = one / DeltaCell(jc);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          double Ksgs = K(ic, jc, kc);
+          double Ts = std::sqrt(Ksgs) * rdelta + StrainRate(ic, jc, kc) / 10.0;
+          if (Ts < 1.0e-10) Ts = zero; else Ts = one / Ts;
+          nut(ic, jc, kc) = 0.05 * Ksgs * Ts + P.xnu;
+        }
+      }
+  }
+
+  // Smagorinsky with van Driest damping (LES_type 10; not in the reference,
+  // whose LES_type 1 branch is empty): nut = xnu + (Cs D Delta)^2 |S|,
+  // D = 1 - exp(-y+/26), y+ = d_wall u_tau / xnu, u_tau from the x-z mean
+  // wall shear of the first cells of both walls, |S| from ClcVelStrainRate.
+  double WallUtau() {
+    double s1 = 0, sN = 0;
+    for (int kc = 1; kc <= nzc; ++kc) for (int ic = 1; ic <= nxc; ++ic) { s1 += ux(ic, 1, kc); sN += ux(ic, nyc, kc); }
+    const double inxz = one / ((double)nxc * (double)nzc);
+    const double d1 = yc(1) - yp(1), dN = yp(nyp) - yc(nyc);
+    const double tw = P.xnu * half * (std::fabs(s1 * inxz - P.uxBcValue[2]) / d1 + std::fabs(sN * inxz - P.uxBcValue[3]) / dN);
+    return std::sqrt(tw);
+  }
+  void Clc_SGS_SmagVD() {
+    const double utau = WallUtau();
+    utau_last = utau;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc) {
+        const double dw = std::min(yc(jc) - yp(1), yp(nyp) - yc(jc));
+        const double D = one - std::exp(-(dw * utau / P.xnu) / 26.0);
+        const double l = P.Cs * D * DeltaCell(jc);
+        for (int ic = 1; ic <= nxc; ++ic) nut(ic, jc, kc) = l * l * StrainRate(ic, jc, kc) + P.xnu;
+      }
+  }
+
+  // ---- src/CFD_2nd/m_LESModels.f90:375-428 (SetBC_and_UpdateHalo_SGS), channel ----
+  void SetBC_and_UpdateHalo_SGS() {
+    const double xnu = P.xnu;
+    for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+      if (P.BcOption[3] == -1) nut(i, nyp, k) = two * xnu - nut(i, nyc, k);
+      else if (P.BcOption[3] == -2) nut(i, nyp, k) = nut(i, nyc, k);
+      if (P.BcOption[2] == -1) nut(i, 0, k) = two * xnu - nut(i, 1, k);
+      else if (P.BcOption[2] == -2) nut(i, 0, k) = nut(i, 1, k);
+    }
+    halo(nut, 1, 1, 0, 0, 1, 1);
+  }
+
+  // ---- src/CFD_2nd/m_LESModels.f90:47-62 (Clc_SGS_Vis) ----
+  void Clc_SGS_Vis() {
+    if (P.LES_type == 2) Clc_SGS_WALE();
+    else if (P.LES_type == 3) Clc_SGS_MTS();
+    else if (P.LES_type == 10) Clc_SGS_SmagVD();
+    SetBC_and_UpdateHalo_SGS();
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:80-156 (clcRhsX_PIMP_LES) ----
+  void clcRhsX_PIMP_LES(F3& RhsX, F3& Hist) {
+    double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1;
+      double s1tot = 0;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double s1totCoe = dyp(jc), sucaj = quarter * rdyp(jc);
+        if (yc(jc) < ybulk1 || yc(jc) >= ybulk2) s1totCoe = zero;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double h11 = ((ux(ip, jc, kc) + ux(ic, jc, kc)) * (ux(ip, jc, kc) + ux(ic, jc, kc)) -
+                        (ux(ic, jc, kc) + ux(im, jc, kc)) * (ux(ic, jc, kc) + ux(im, jc, kc))) * qdx1;
+          double h12 = ((uy(ic, jp, kc) + uy(im, jp, kc)) * (ux(ic, jp, kc) + ux(ic, jc, kc)) -
+                        (uy(ic, jc, kc) + uy(im, jc, kc)) * (ux(ic, jc, kc) + ux(ic, jm, kc))) * sucaj;
+          double h13 = ((uz(ic, jc, kp) + uz(im, jc, kp)) * (ux(ic, jc, kp) + ux(ic, jc, kc)) -
+                        (uz(ic, jc, kc) + uz(im, jc, kc)) * (ux(ic, jc, kc) + ux(ic, jc, km))) * qdx3;
+          double visa = quarter * (nut(ic, jc, kc) + nut(im, jc, kc) + nut(ic, jm, kc) + nut(im, jm, kc));
+          double visb = quarter * (nut(ic, jc, kc) + nut(im, jc, kc) + nut(ic, jp, kc) + nut(im, jp, kc));
+          double visc = quarter * (nut(ic, jc, kc) + nut(im, jc, kc) + nut(ic, jc, km) + nut(im, jc, km));
+          double visd = quarter * (nut(ic, jc, kc) + nut(im, jc, kc) + nut(ic, jc, kp) + nut(im, jc, kp));
+          double sgs1 = rdx2 * (nut(ic, jc, kc) * (ux(ip, jc, kc) - ux(ic, jc, kc)) - nut(im, jc, kc) * (ux(ic, jc, kc) - ux(im, jc, kc)));
+          double sgs2 = rdx * rdyp(jc) * (visb * (uy(ic, jp, kc) - uy(im, jp, kc)) - visa * (uy(ic, jc, kc) - uy(im, jc, kc)));
+          double sgs3 = rdx * rdz * (visd * (uz(ic, jc, kp) - uz(im, jc, kp)) - visc * (uz(ic, jc, kc) - uz(im, jc, kc)));
+          double d11q1 = sgs1;
+          double d22q1 = ap2c(jc) * visb * (ux(ic, jp, kc) - ux(ic, jc, kc)) - am2c(jc) * visa * (ux(ic, jc, kc) - ux(ic, jm, kc));
+          double d33q1 = ap3c(kc) * visd * (ux(ic, jc, kp) - ux(ic, jc, kc)) - am3c(kc) * visc * (ux(ic, jc, kc) - ux(ic, jc, km));
+          double dcq13 = d11q1 + d33q1;
+          double gradp1 = (pressure(ic, jc, kc) - pressure(im, jc, kc)) * rdx;
+          s1tot = s1tot + ux(ic, jc, kc) * s1totCoe;
+          double convEd1 = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[0];
+          RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1 + two * pmBetaT * d22q1;
+          Hist(ic, jc, kc) = convEd1;
+        }
+      }
+      part[kc] = s1tot;
+    }
+    if (P.IsUxConst) {
+      double s1tot1 = 0;
+      for (int kc = 1; kc <= nzc; ++kc) s1tot1 += part[kc];
+      s1tot1 = s1tot1 / ((double)nxc * (double)nzc) / (ybulk2 - ybulk1);
+      double dpmdxns = pmAlphaC * (P.ubulk - s1tot1);
+#pragma omp parallel for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) RhsX(ic, jc, kc) = RhsX(ic, jc, kc) + dpmdxns;
+      PrGradNow = (P.ubulk - s1tot1) / dt;
+      PrGradAver = PrGradAver + pmAlphaC * PrGradNow;
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:214-272 (clcRhsY_PIMP_LES) ----
+  void clcRhsY_PIMP_LES(F3& RhsY, F3& Hist) {
+    double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double sucac = rdyc(jc), qsucac = quarter * sucac;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double h21 = ((ux(ip, jc, kc) + ux(ip, jm, kc)) * (uy(ip, jc, kc) + uy(ic, jc, kc)) -
+                        (ux(ic, jc, kc) + ux(ic, jm, kc)) * (uy(ic, jc, kc) + uy(im, jc, kc))) * qdx1;
+          double h22 = ((uy(ic, jp, kc) + uy(ic, jc, kc)) * (uy(ic, jp, kc) + uy(ic, jc, kc)) -
+                        (uy(ic, jc, kc) + uy(ic, jm, kc)) * (uy(ic, jc, kc) + uy(ic, jm, kc))) * qsucac;
+          double h23 = ((uz(ic, jc, kp) + uz(ic, jm, kp)) * (uy(ic, jc, kp) + uy(ic, jc, kc)) -
+                        (uz(ic, jc, kc) + uz(ic, jm, kc)) * (uy(ic, jc, kc) + uy(ic, jc, km))) * qdx3;
+          double visa = quarter * (nut(ic, jc, kc) + nut(im, jc, kc) + nut(ic, jm, kc) + nut(im, jm, kc));
+          double visb = quarter * (nut(ic, jc, kc) + nut(ip, jc, kc) + nut(ic, jm, kc) + nut(ip, jm, kc));
+          double visc = quarter * (nut(ic, jc, kc) + nut(ic, jm, kc) + nut(ic, jc, km) + nut(ic, jm, km));
+          double visd = quarter * (nut(ic, jc, kc) + nut(ic, jm, kc) + nut(ic, jc, kp) + nut(ic, jm, kp));
+          double sgs1 = rdx * sucac * (visb * (ux(ip, jc, kc) - ux(ip, jm, kc)) - visa * (ux(ic, jc, kc) - ux(ic, jm, kc)));
+          double sgs2 = ap2p(jc) * nut(ic, jc, kc) * (uy(ic, jp, kc) - uy(ic, jc, kc)) - am2p(jc) * nut(ic, jm, kc) * (uy(ic, jc, kc) - uy(ic, jm, kc));
+          double sgs3 = rdz * sucac * (visd * (uz(ic, jc, kp) - uz(ic, jm, kp)) - visc * (uz(ic, jc, kc) - uz(ic, jm, kc)));
+          double d11q2 = ap1c(ic) * visb * (uy(ip, jc, kc) - uy(ic, jc, kc)) - am1c(ic) * visa * (uy(ic, jc, kc) - uy(im, jc, kc));
+          double d22q2 = sgs2;
+          double d33q2 = ap3c(kc) * visd * (uy(ic, jc, kp) - uy(ic, jc, kc)) - am3c(kc) * visc * (uy(ic, jc, kc) - uy(ic, jc, km));
+          double dcq13 = d11q2 + d33q2;
+          double gradp2 = (pressure(ic, jc, kc) - pressure(ic, jm, kc)) * sucac;
+          double convEd2 = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[1];
+          RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2 + two * pmBetaT * d22q2;
+          Hist(ic, jc, kc) = convEd2;
+        }
+      }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:330-387 (clcRhsZ_PIMP_LES) ----
+  void clcRhsZ_PIMP_LES(F3& RhsZ, F3& Hist) {
+    double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double sucaj = quarter * rdyp(jc);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1;
+          double h31 = ((ux(ip, jc, kc) + ux(ip, jc, km)) * (uz(ip, jc, kc) + uz(ic, jc, kc)) -
+                        (ux(ic, jc, kc) + ux(ic, jc, km)) * (uz(ic, jc, kc) + uz(im, jc, kc))) * qdx1;
+          double h32 = ((uy(ic, jp, kc) + uy(ic, jp, km)) * (uz(ic, jp, kc) + uz(ic, jc, kc)) -
+                        (uy(ic, jc, kc) + uy(ic, jc, km)) * (uz(ic, jc, kc) + uz(ic, jm, kc))) * sucaj;
+          double h33 = ((uz(ic, jc, kp) + uz(ic, jc, kc)) * (uz(ic, jc, kp) + uz(ic, jc, kc)) -
+                        (uz(ic, jc, kc) + uz(ic, jc, km)) * (uz(ic, jc, kc) + uz(ic, jc, km))) * qdx3;
+          double visa = quarter * (nut(ic, jc, km) + nut(im, jc, km) + nut(ic, jc, kc) + nut(im, jc, kc));
+          double visb = quarter * (nut(ic, jc, km) + nut(ip, jc, km) + nut(ic, jc, kc) + nut(ip, jc, kc));
+          double visc = quarter * (nut(ic, jc, km) + nut(ic, jm, km) + nut(ic, jm, kc) + nut(ic, jc, kc));
+          double visd = quarter * (nut(ic, jc, km) + nut(ic, jp, km) + nut(ic, jp, kc) + nut(ic, jc, kc));
+          double sgs1 = rdx * rdz * (visb * (ux(ip, jc, kc) - ux(ip, jc, km)) - visa * (ux(ic, jc, kc) - ux(ic, jc, km)));
+          double sgs2 = rdz * rdyp(jc) * (visd * (uy(ic, jp, kc) - uy(ic, jp, km)) - visc * (uy(ic, jc, kc) - uy(ic, jc, km)));
+          double sgs3 = rdz2 * (nut(ic, jc, kc) * (uz(ic, jc, kp) - uz(ic, jc, kc)) - nut(ic, jc, km) * (uz(ic, jc, kc) - uz(ic, jc, km)));
+          double d11q3 = ap1c(ic) * visb * (uz(ip, jc, kc) - uz(ic, jc, kc)) - am1c(ic) * visa * (uz(ic, jc, kc) - uz(im, jc, kc));
+          double d22q3 = ap2c(jc) * visd * (uz(ic, jp, kc) - uz(ic, jc, kc)) - am2c(jc) * visc * (uz(ic, jc, kc) - uz(ic, jm, kc));
+          double d33q3 = sgs3;
+          double dcq13 = d11q3 + d33q3;
+          double gradp3 = (pressure(ic, jc, kc) - pressure(ic, jc, km)) * rdz;
+          double convEd3 = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[2];
+          RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3 + two * pmBetaT * d22q3;
+          Hist(ic, jc, kc) = convEd3;
+        }
+      }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:466-499, 626-662, 776-809
+  //      (clcU1/2/3Hat_PIMP_LES): variable-coefficient y Crank-Nicolson ----
+  void clcUHat_PIMP_LES(int comp, F3& u, F3& Rhs) {
+#pragma omp parallel
+    {
+      std::vector<double> a(nyc), b(nyc), c(nyc), f(nyc), arr(nyc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          const int im = ic - 1, km = kc - 1;
+          for (int jc = 1; jc <= nyc; ++jc) {
+            const int jm = jc - 1, jp = jc + 1;
+            double rt1, rt2;
+            if (comp == 1) {
+              if (jc == 1) { a[0] = zero; b[0] = one; c[0] = zero; f[0] = duy_ym[(size_t)(ic - 1) + (size_t)nxc * (kc - 1)]; continue; }
+              rt1 = pmBetaT * nut(ic, jm, kc) * am2p(jc);
+              rt2 = pmBetaT * nut(ic, jc, kc) * ap2p(jc);
+            } else {
+              double visc, visd;
+              if (comp == 0) {
+                visc = quarter * (nut(ic, jc, kc) + nut(im, jc, kc) + nut(ic, jm, kc) + nut(im, jm, kc));
+                visd = quarter * (nut(ic, jc, kc) + nut(im, jc, kc) + nut(ic, jp, kc) + nut(im, jp, kc));
+              } else {
+                visc = quarter * (nut(ic, jc, km) + nut(ic, jm, km) + nut(ic, jc, kc) + nut(ic, jm, kc));
+                visd = quarter * (nut(ic, jc, km) + nut(ic, jp, km) + nut(ic, jc, kc) + nut(ic, jp, kc));
+              }
+              rt1 = pmBetaT * visc * am2cForCN(jc);
+              rt2 = pmBetaT * visd * ap2cForCN(jc);
+            }
+            a[jc - 1] = -rt1;
+            b[jc - 1] = rt1 + rt2 + one;
+            c[jc - 1] = -rt2;
+            f[jc - 1] = Rhs(ic, jc, kc);
+          }
+          InverseTridiagonal1(a.data(), b.data(), c.data(), f.data(), nyc, arr.data());
+          for (int jc = 1; jc <= nyc; ++jc) u(ic, jc, kc) = u(ic, jc, kc) + f[jc - 1];
+        }
+    }
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:878-904 (PressureUpdate_PIMP_LES) ----
+  void PressureUpdate_PIMP_LES(const F3& phi) {
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jp = jc + 1, jm = jc - 1;
+        double metr1 = rdyp(jc) * rdyc(jc), metr2 = rdyp(jc) * rdyc(jp);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          double visd = half * (nut(ic, jp, kc) + nut(ic, jc, kc));
+          double visc = half * (nut(ic, jc, kc) + nut(ic, jm, kc));
+          double pmBetap = -pmBetaT * metr2 * visd;
+          double pmBetam = -pmBetaT * metr1 * visc;
+          double pmBetac = -(pmBetap + pmBetam) + one;
+          pressure(ic, jc, kc) = pressure(ic, jc, kc) + pmBetap * phi(ic, jp, kc) + pmBetac * phi(ic, jc, kc) + pmBetam * phi(ic, jm, kc);
+        }
+      }
   }
 
   // ---- src/CFD_2nd/m_TScheme.f90:213-241 (clcPrSrcOther) ----
@@ -896,26 +1394,339 @@ struct Oracle {
       }
   }
 
+  // =====================================================================
+  // 4th-order solver (src/CFD_4th)
+  // =====================================================================
+
+  // ---- src/CFD_4th/m_BC_and_Halo.f90:51-96 (SetBC_and_UpdateHalo), channel ----
+  void SetBC_and_UpdateHalo4() {
+    for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+      if (P.FlowType == 1) {
+        ux(i, nyp, k) = P.uxBcValue[3] * two - ux(i, nyc, k);
+        uy(i, nyp, k) = P.uyBcValue[3];
+        uz(i, nyp, k) = P.uzBcValue[3] * two - uz(i, nyc, k);
+      } else {
+        ux(i, nyp, k) = ux(i, nyc, k);
+        uy(i, nyp, k) = zero;
+        uz(i, nyp, k) = uz(i, nyc, k);
+      }
+      ux(i, 0, k) = P.uxBcValue[2] * two - ux(i, 1, k);
+      uy(i, 1, k) = uy_ym[(size_t)(i - 1) + (size_t)nxc * (k - 1)];
+      uz(i, 0, k) = P.uzBcValue[2] * two - uz(i, 1, k);
+    }
+    halo(ux, 2, 2, 0, 0, 2, 2);
+    halo(uy, 2, 2, 0, 0, 2, 2);
+    halo(uz, 2, 2, 0, 0, 2, 2);
+  }
+
+  // ---- src/CFD_4th/m_BC_and_Halo.f90:101-131 (SetBC_and_UpdateHaloForPrSrc) ----
+  void SetBC_and_UpdateHaloForPrSrc4() {
+    for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+      uy(i, nyp, k) = P.FlowType == 1 ? P.uyBcValue[3] : zero;
+      uy(i, 1, k) = uy_ym[(size_t)(i - 1) + (size_t)nxc * (k - 1)];
+    }
+    halo(ux, 1, 2, 0, 0, 0, 0);
+    halo(uz, 0, 0, 0, 0, 1, 2);
+  }
+
+  // ---- src/CFD_4th/m_BC_and_Halo.f90:136-150 (SetBC_and_UpdateHalo_pr) ----
+  void SetBC_and_UpdateHalo_pr4(F3& pr) {
+    for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) {
+      pr(i, 0, k) = pr(i, 1, k);
+      pr(i, nyp, k) = pr(i, nyc, k);
+    }
+    halo(pr, 2, 1, 0, 0, 2, 1);
+  }
+
+  // ---- src/CFD_4th/m_TScheme.f90:189-377 (clcRhsXYZ without scalar/particles) ----
+  void clcRhsXYZ4(F3& RhsX, F3& RhsY, F3& RhsZ) {
+    const double xnu = P.xnu;
+    // interpolated velocities (:209-227) and their halos (:228-233)
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int ks = kc - 2, km = kc - 1, kp = kc + 1, ku = kc + 2;
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int is = ic - 2, im = ic - 1, ip = ic + 1, iu = ic + 2;
+          uxhx(ic, jc, kc) = InterpCoe1 * ux(im, jc, kc) + InterpCoe2 * ux(ic, jc, kc) + InterpCoe3 * ux(ip, jc, kc) + InterpCoe4 * ux(iu, jc, kc);
+          uyhx(ic, jc, kc) = InterpCoe1 * uy(is, jc, kc) + InterpCoe2 * uy(im, jc, kc) + InterpCoe3 * uy(ic, jc, kc) + InterpCoe4 * uy(ip, jc, kc);
+          uzhx(ic, jc, kc) = InterpCoe1 * uz(is, jc, kc) + InterpCoe2 * uz(im, jc, kc) + InterpCoe3 * uz(ic, jc, kc) + InterpCoe4 * uz(ip, jc, kc);
+          uxhz(ic, jc, kc) = InterpCoe1 * ux(ic, jc, ks) + InterpCoe2 * ux(ic, jc, km) + InterpCoe3 * ux(ic, jc, kc) + InterpCoe4 * ux(ic, jc, kp);
+          uyhz(ic, jc, kc) = InterpCoe1 * uy(ic, jc, ks) + InterpCoe2 * uy(ic, jc, km) + InterpCoe3 * uy(ic, jc, kc) + InterpCoe4 * uy(ic, jc, kp);
+          uzhz(ic, jc, kc) = InterpCoe1 * uz(ic, jc, km) + InterpCoe2 * uz(ic, jc, kc) + InterpCoe3 * uz(ic, jc, kp) + InterpCoe4 * uz(ic, jc, ku);
+        }
+      for (int ic = 1; ic <= nxc; ++ic) { uyhx(ic, nyp, kc) = zero; uyhz(ic, nyp, kc) = zero; }
+    }
+    halo(uxhx, 2, 1, 0, 0, 0, 0);
+    halo(uyhx, 1, 2, 0, 0, 0, 0);
+    halo(uzhx, 1, 2, 0, 0, 1, 2);
+    halo(uxhz, 1, 2, 0, 0, 1, 2);
+    halo(uyhz, 0, 0, 0, 0, 1, 2);
+    halo(uzhz, 0, 0, 0, 0, 2, 1);
+
+    // RhsX (:235-274)
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int ks = kc - 2, km = kc - 1, kp = kc + 1, ku = kc + 2;
+      double s3tot = 0;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double sucaj = rdyp(jc);
+        double InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+        double InterpY3 = YinterpCoe(jp), InterpY4 = one - InterpY3;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int is = ic - 2, im = ic - 1, ip = ic + 1, iu = ic + 2;
+          double uxhyc = InterpY1 * ux(ic, jm, kc) + InterpY2 * ux(ic, jc, kc);
+          double uxhyp = InterpY3 * ux(ic, jc, kc) + InterpY4 * ux(ic, jp, kc);
+          double h11 = dxCoe1 * uxhx(is, jc, kc) * (uxhx(is, jc, kc) + uCRF) + dxCoe2 * uxhx(im, jc, kc) * (uxhx(im, jc, kc) + uCRF) +
+                       dxCoe3 * uxhx(ic, jc, kc) * (uxhx(ic, jc, kc) + uCRF) + dxCoe4 * uxhx(ip, jc, kc) * (uxhx(ip, jc, kc) + uCRF);
+          double h12 = (uyhx(ic, jp, kc) * uxhyp - uyhx(ic, jc, kc) * uxhyc) * sucaj;
+          double h13 = dzCoe1 * uxhz(ic, jc, km) * uzhx(ic, jc, km) + dzCoe2 * uxhz(ic, jc, kc) * uzhx(ic, jc, kc) +
+                       dzCoe3 * uxhz(ic, jc, kp) * uzhx(ic, jc, kp) + dzCoe4 * uxhz(ic, jc, ku) * uzhx(ic, jc, ku);
+          double d11q1 = dxxCoe1 * ux(is, jc, kc) + dxxCoe2 * ux(im, jc, kc) + dxxCoe3 * ux(ic, jc, kc) + dxxCoe4 * ux(ip, jc, kc) + dxxCoe5 * ux(iu, jc, kc);
+          double d22q1 = ap2c(jc) * ux(ic, jp, kc) + ac2c(jc) * ux(ic, jc, kc) + am2c(jc) * ux(ic, jm, kc);
+          double d33q1 = dzzCoe1 * ux(ic, jc, ks) + dzzCoe2 * ux(ic, jc, km) + dzzCoe3 * ux(ic, jc, kc) + dzzCoe4 * ux(ic, jc, kp) + dzzCoe5 * ux(ic, jc, ku);
+          double dcq13 = d11q1 + d33q1;
+          s3tot = s3tot + (dcq13 + d22q1) * dyp(jc);
+          double convEd1 = -h11 - h12 - h13 + xnu * dcq13 + P.gravity[0];
+          double gradp1 = dxCoe1 * pressure(is, jc, kc) + dxCoe2 * pressure(im, jc, kc) + dxCoe3 * pressure(ic, jc, kc) + dxCoe4 * pressure(ip, jc, kc);
+          RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * HistX(ic, jc, kc) - pmAlpha * gradp1 + two * pmBeta * d22q1;
+          HistX(ic, jc, kc) = convEd1;
+        }
+      }
+      part[kc] = s3tot;
+    }
+    // RhsY (:276-310)
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int ks = kc - 2, km = kc - 1, kp = kc + 1, ku = kc + 2;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double sucac = rdyc(jc), qsucac = quarter * sucac;
+        double InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int is = ic - 2, im = ic - 1, ip = ic + 1, iu = ic + 2;
+          double uxhym = InterpY1 * ux(im, jm, kc) + InterpY2 * ux(im, jc, kc) + uCRF, uzhym = InterpY1 * uz(ic, jm, km) + InterpY2 * uz(ic, jc, km);
+          double uxhyc = InterpY1 * ux(ic, jm, kc) + InterpY2 * ux(ic, jc, kc) + uCRF, uzhyc = InterpY1 * uz(ic, jm, kc) + InterpY2 * uz(ic, jc, kc);
+          double uxhyp = InterpY1 * ux(ip, jm, kc) + InterpY2 * ux(ip, jc, kc) + uCRF, uzhyp = InterpY1 * uz(ic, jm, kp) + InterpY2 * uz(ic, jc, kp);
+          double uxhyu = InterpY1 * ux(iu, jm, kc) + InterpY2 * ux(iu, jc, kc) + uCRF, uzhyu = InterpY1 * uz(ic, jm, ku) + InterpY2 * uz(ic, jc, ku);
+          double h21 = dxCoe1 * uyhx(im, jc, kc) * uxhym + dxCoe2 * uyhx(ic, jc, kc) * uxhyc + dxCoe3 * uyhx(ip, jc, kc) * uxhyp + dxCoe4 * uyhx(iu, jc, kc) * uxhyu;
+          double h22 = ((uy(ic, jp, kc) + uy(ic, jc, kc)) * (uy(ic, jp, kc) + uy(ic, jc, kc)) -
+                        (uy(ic, jc, kc) + uy(ic, jm, kc)) * (uy(ic, jc, kc) + uy(ic, jm, kc))) * qsucac;
+          double h23 = dzCoe1 * uyhz(ic, jc, km) * uzhym + dzCoe2 * uyhz(ic, jc, kc) * uzhyc + dzCoe3 * uyhz(ic, jc, kp) * uzhyp + dzCoe4 * uyhz(ic, jc, ku) * uzhyu;
+          double d11q2 = dxxCoe1 * uy(is, jc, kc) + dxxCoe2 * uy(im, jc, kc) + dxxCoe3 * uy(ic, jc, kc) + dxxCoe4 * uy(ip, jc, kc) + dxxCoe5 * uy(iu, jc, kc);
+          double d22q2 = ap2p(jc) * uy(ic, jp, kc) + ac2p(jc) * uy(ic, jc, kc) + am2p(jc) * uy(ic, jm, kc);
+          double d33q2 = dzzCoe1 * uy(ic, jc, ks) + dzzCoe2 * uy(ic, jc, km) + dzzCoe3 * uy(ic, jc, kc) + dzzCoe4 * uy(ic, jc, kp) + dzzCoe5 * uy(ic, jc, ku);
+          double dcq13 = d11q2 + d33q2;
+          double convEd2 = -h21 - h22 - h23 + xnu * dcq13 + P.gravity[1];
+          double gradp2 = (pressure(ic, jc, kc) - pressure(ic, jm, kc)) * sucac;
+          RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * HistY(ic, jc, kc) - pmAlpha * gradp2 + two * pmBeta * d22q2;
+          HistY(ic, jc, kc) = convEd2;
+        }
+      }
+    }
+    // RhsZ (:312-343)
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int ks = kc - 2, km = kc - 1, kp = kc + 1, ku = kc + 2;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1, jp = jc + 1;
+        double sucaj = rdyp(jc);
+        double InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+        double InterpY3 = YinterpCoe(jp), InterpY4 = one - InterpY3;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int is = ic - 2, im = ic - 1, ip = ic + 1, iu = ic + 2;
+          double uzhyc = InterpY1 * uz(ic, jm, kc) + InterpY2 * uz(ic, jc, kc);
+          double uzhyp = InterpY3 * uz(ic, jc, kc) + InterpY4 * uz(ic, jp, kc);
+          double h31 = dxCoe1 * uzhx(im, jc, kc) * (uxhz(im, jc, kc) + uCRF) + dxCoe2 * uzhx(ic, jc, kc) * (uxhz(ic, jc, kc) + uCRF) +
+                       dxCoe3 * uzhx(ip, jc, kc) * (uxhz(ip, jc, kc) + uCRF) + dxCoe4 * uzhx(iu, jc, kc) * (uxhz(iu, jc, kc) + uCRF);
+          double h32 = (uyhz(ic, jp, kc) * uzhyp - uyhz(ic, jc, kc) * uzhyc) * sucaj;
+          double h33 = dzCoe1 * uzhz(ic, jc, ks) * uzhz(ic, jc, ks) + dzCoe2 * uzhz(ic, jc, km) * uzhz(ic, jc, km) +
+                       dzCoe3 * uzhz(ic, jc, kc) * uzhz(ic, jc, kc) + dzCoe4 * uzhz(ic, jc, kp) * uzhz(ic, jc, kp);
+          double d11q3 = dxxCoe1 * uz(is, jc, kc) + dxxCoe2 * uz(im, jc, kc) + dxxCoe3 * uz(ic, jc, kc) + dxxCoe4 * uz(ip, jc, kc) + dxxCoe5 * uz(iu, jc, kc);
+          double d22q3 = ap2c(jc) * uz(ic, jp, kc) + ac2c(jc) * uz(ic, jc, kc) + am2c(jc) * uz(ic, jm, kc);
+          double d33q3 = dzzCoe1 * uz(ic, jc, ks) + dzzCoe2 * uz(ic, jc, km) + dzzCoe3 * uz(ic, jc, kc) + dzzCoe4 * uz(ic, jc, kp) + dzzCoe5 * uz(ic, jc, ku);
+          double dcq13 = d11q3 + d33q3;
+          double convEd3 = -h31 - h32 - h33 + xnu * dcq13 + P.gravity[2];
+          double gradp3 = dzCoe1 * pressure(ic, jc, ks) + dzCoe2 * pressure(ic, jc, km) + dzCoe3 * pressure(ic, jc, kc) + dzCoe4 * pressure(ic, jc, kp);
+          RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * HistZ(ic, jc, kc) - pmAlpha * gradp3 + two * pmBeta * d22q3;
+          HistZ(ic, jc, kc) = convEd3;
+        }
+      }
+    }
+    // constant flux from the mean viscous stress (:364-377)
+    if (P.IsUxConst) {
+      double s3tot1 = 0;
+      for (int kc = 1; kc <= nzc; ++kc) s3tot1 += part[kc];
+      double dpmdxns = xnu * s3tot1 / ((double)nxc * (double)nzc) / P.yly;
+      double dp1ns = pmAlpha * dpmdxns;
+#pragma omp parallel for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic) RhsX(ic, jc, kc) = RhsX(ic, jc, kc) - dp1ns;
+      PrGradAver = PrGradAver + dpmdxns * pmAlphaC;
+    }
+  }
+
+  // ---- src/CFD_4th/m_TScheme.f90:443-549 (clcU1Hat/clcU3Hat; clcU2Hat as PIMP) ----
+  void clcUHat4_c(F3& u, F3& Rhs) {
+    std::vector<double> tp(nyc), tm(nyc), tc(nyc);
+    for (int jc = 1; jc <= nyc; ++jc) {
+      tp[jc - 1] = -pmBeta * ap2cForCN(jc);
+      tc[jc - 1] = -pmBeta * ac2cForCN(jc) + one;
+      tm[jc - 1] = -pmBeta * am2cForCN(jc);
+    }
+#pragma omp parallel
+    {
+      std::vector<double> f(nyc), arr(nyc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int jc = 1; jc <= nyc; ++jc) f[jc - 1] = Rhs(ic, jc, kc);
+          InverseTridiagonal1(tm.data(), tc.data(), tp.data(), f.data(), nyc, arr.data());
+          for (int jc = 1; jc <= nyc; ++jc) u(ic, jc, kc) = u(ic, jc, kc) + f[jc - 1];
+        }
+    }
+  }
+
+  // ---- src/CFD_4th/m_TScheme.f90:114-143 (clcPrSrc) ----
+  double clcPrSrc4(F3& prsrc) {
+    double sudtal = one / pmAlpha;
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1, ku = kc + 2;
+      double m = 0;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jp = jc + 1;
+        double sucaj = rdyp(jc);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1, iu = ic + 2;
+          double dudx = dxCoe1 * ux(im, jc, kc) + dxCoe2 * ux(ic, jc, kc) + dxCoe3 * ux(ip, jc, kc) + dxCoe4 * ux(iu, jc, kc);
+          double dvdy = (uy(ic, jp, kc) - uy(ic, jc, kc)) * sucaj;
+          double dwdz = dzCoe1 * uz(ic, jc, km) + dzCoe2 * uz(ic, jc, kc) + dzCoe3 * uz(ic, jc, kp) + dzCoe4 * uz(ic, jc, ku);
+          double rdiv = dudx + dvdy + dwdz;
+          m = std::max(std::fabs(rdiv), m);
+          prsrc(ic, jc, kc) = sudtal * rdiv;
+        }
+      }
+      part[kc] = m;
+    }
+    double m = 0;
+    for (int kc = 1; kc <= nzc; ++kc) m = std::max(m, part[kc]);
+    return m;
+  }
+
+  // ---- src/CFD_4th/m_TScheme.f90:148-173 (FluidVelUpdate) ----
+  void FluidVelUpdate4(const F3& phi) {
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int ks = kc - 2, km = kc - 1, kp = kc + 1;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jm = jc - 1;
+        double sucac = rdyc(jc);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int is = ic - 2, im = ic - 1, ip = ic + 1;
+          double dpdx = dxCoe1 * phi(is, jc, kc) + dxCoe2 * phi(im, jc, kc) + dxCoe3 * phi(ic, jc, kc) + dxCoe4 * phi(ip, jc, kc);
+          double dpdy = (phi(ic, jc, kc) - phi(ic, jm, kc)) * sucac;
+          double dpdz = dzCoe1 * phi(ic, jc, ks) + dzCoe2 * phi(ic, jc, km) + dzCoe3 * phi(ic, jc, kc) + dzCoe4 * phi(ic, jc, kp);
+          ux(ic, jc, kc) = ux(ic, jc, kc) - pmAlpha * dpdx;
+          uy(ic, jc, kc) = uy(ic, jc, kc) - pmAlpha * dpdy;
+          uz(ic, jc, kc) = uz(ic, jc, kc) - pmAlpha * dpdz;
+        }
+      }
+    }
+  }
+
+  // ---- src/CFD_4th/m_Tools.f90:54-81 (CheckDivergence) ----
+  double CheckDivergence4() {
+    std::vector<double> part(nzc + 1, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc) {
+      int km = kc - 1, kp = kc + 1, ku = kc + 2;
+      double m = 0;
+      for (int jc = 1; jc <= nyc; ++jc) {
+        int jp = jc + 1;
+        double sucaj = rdyp(jc);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          int im = ic - 1, ip = ic + 1, iu = ic + 2;
+          double dudx = dxCoe1 * ux(im, jc, kc) + dxCoe2 * ux(ic, jc, kc) + dxCoe3 * ux(ip, jc, kc) + dxCoe4 * ux(iu, jc, kc);
+          double dvdy = (uy(ic, jp, kc) - uy(ic, jc, kc)) * sucaj;
+          double dwdz = dzCoe1 * uz(ic, jc, km) + dzCoe2 * uz(ic, jc, kc) + dzCoe3 * uz(ic, jc, kp) + dzCoe4 * uz(ic, jc, ku);
+          double udiv = std::fabs(dudx + dvdy + dwdz);
+          if (udiv > m) m = udiv;
+        }
+      }
+      part[kc] = m;
+    }
+    double m = 0;
+    for (int kc = 1; kc <= nzc; ++kc) m = std::max(m, part[kc]);
+    return m;
+  }
+
+  // ---- src/CFD_4th/m_ChannelSystem.f90:106-141, one substep in stages ----
+  void stage4(int st, int ns) {
+    switch (st) {
+      case 0: PMcoeUpdate(ns); Update_uy_ym(); break;
+      case 1: clcRhsXYZ4(RealArr1, RealArr2, RealHalo); break;
+      case 2:
+        clcUHat4_c(ux, RealArr1);
+        clcU2Hat_PIMP(RealArr2);
+        clcUHat4_c(uz, RealHalo);
+        break;
+      case 3:
+        SetBC_and_UpdateHaloForPrSrc4();
+        divmax1_last = clcPrSrc4(RealArr1);
+        break;
+      case 4:
+        clcPPE(RealArr1, RealHalo);
+        SetBC_and_UpdateHalo_pr4(RealHalo);
+        break;
+      case 5: FluidVelUpdate4(RealHalo); break;
+      case 6:
+        PressureUpdate_PIMP(RealHalo);
+        SetBC_and_UpdateHalo4();
+        SetBC_and_UpdateHalo_pr4(pressure);
+        break;
+    }
+  }
+
   // ---- src/CFD_2nd/m_ChannelSystem.f90:91-124, one substep split in stages ----
   // stage 0: PMcoeUpdate + Update_uy_ym; 1: clcRhsX/Y/Z; 2: clcU1/2/3Hat;
   // 3: SetBC_and_UpdateHaloForPrSrc + clcPrSrc; 4: clcPPE + SetBC_and_UpdateHalo_pr;
   // 5: FluidVelUpdate; 6: PressureUpdate + SetBC_and_UpdateHalo(u) + ..._pr(p)
   void stage(int st, int ns) {
+    if (o4) { stage4(st, ns); return; }
+    const bool fimp = P.IsImplicit == 2;
+    const bool les = P.LES_type > 0;
     switch (st) {
       case 0: PMcoeUpdate(ns); Update_uy_ym(); break;
       case 1:
-        clcRhsX_PIMP(RealArr1, HistX);
-        clcRhsY_PIMP(RealArr2, HistY);
-        clcRhsZ_PIMP(RealHalo, HistZ);
+        if (les) {
+          clcRhsX_PIMP_LES(RealArr1, HistX);
+          clcRhsY_PIMP_LES(RealArr2, HistY);
+          clcRhsZ_PIMP_LES(RealHalo, HistZ);
+          break;
+        }
+        clcRhsX_PIMP(RealArr1, HistX, fimp);
+        clcRhsY_PIMP(RealArr2, HistY, fimp);
+        clcRhsZ_PIMP(RealHalo, HistZ, fimp);
         break;
       case 2:
+        if (les) {
+          clcUHat_PIMP_LES(0, ux, RealArr1);
+          clcUHat_PIMP_LES(1, uy, RealArr2);
+          clcUHat_PIMP_LES(2, uz, RealHalo);
+          break;
+        }
+        if (fimp) { clcUHat_FIMP_xz(RealArr1); clcUHat_FIMP_xz(RealArr2); clcUHat_FIMP_xz(RealHalo); }
         clcUHat_PIMP_c(ux, RealArr1);
         clcU2Hat_PIMP(RealArr2);
         clcUHat_PIMP_c(uz, RealHalo);
         break;
       case 3:
         SetBC_and_UpdateHaloForPrSrc();
-        divmax1_last = clcPrSrcOther(RealArr1);
+        divmax1_last = fimp ? clcPrSrc_FIMP(RealArr1) : clcPrSrcOther(RealArr1);
         break;
       case 4:
         clcPPE(RealArr1, RealHalo);
@@ -923,7 +1734,9 @@ struct Oracle {
         break;
       case 5: FluidVelUpdate(RealHalo); break;
       case 6:
-        PressureUpdate_PIMP(RealHalo);
+        if (les) PressureUpdate_PIMP_LES(RealHalo);
+        else if (fimp) PressureUpdate_FIMP(RealHalo);
+        else PressureUpdate_PIMP(RealHalo);
         SetBC_and_UpdateHalo();
         SetBC_and_UpdateHalo_pr(pressure);
         break;
@@ -937,9 +1750,10 @@ struct Oracle {
     double cflmp = uddxmax * dt;
     if (P.iCFL == 1) { dt = P.CFLc / uddxmax; dt = std::min(dt, P.dtMax); }
     else dt = P.dtMax;
+    if (P.LES_type > 0 && !o4) Clc_SGS_Vis();
     for (int ns = 1; ns <= iadvance; ++ns)
       for (int st = 0; st <= 6; ++st) stage(st, ns);
-    double divmax2 = CheckDivergence();
+    double divmax2 = o4 ? CheckDivergence4() : CheckDivergence();
     double vmax[3];
     CalcVmax(vmax);
     int status = 0;
@@ -1100,8 +1914,13 @@ void orc_set_state(void* h, const double* ux, const double* uy, const double* uz
     else { o->HistX(i, j, k) = 0; o->HistY(i, j, k) = 0; o->HistZ(i, j, k) = 0; }
   }
   o->Update_uy_ym();
-  o->SetBC_and_UpdateHalo();
-  o->SetBC_and_UpdateHalo_pr(o->pressure);
+  if (o->o4) {
+    o->SetBC_and_UpdateHalo4();
+    o->SetBC_and_UpdateHalo_pr4(o->pressure);
+  } else {
+    o->SetBC_and_UpdateHalo();
+    o->SetBC_and_UpdateHalo_pr(o->pressure);
+  }
   std::fill(o->RealArr1.a.begin(), o->RealArr1.a.end(), 0.0);
   std::fill(o->RealArr2.a.begin(), o->RealArr2.a.end(), 0.0);
   o->SimTime = 0; o->dt = o->P.dtMax; o->itime = 0;

@@ -185,7 +185,10 @@ class Oracle:
         nx, ny, nz = self.cfg.nxc, self.cfg.nyc, self.cfg.nzc
         if a.size == nx * ny * nz:
             return a.reshape(nz, ny, nx)
-        g = a.reshape(nz + 3, ny + 3, nx + 3)
+        if self.cfg.order == 4:  # (-1:nxc+2, 0:nyc+1, -1:nzc+2)
+            g = a.reshape(nz + 4, ny + 2, nx + 4)
+            return np.ascontiguousarray(g[2:nz + 2, 1:ny + 1, 2:nx + 2])
+        g = a.reshape(nz + 3, ny + 3, nx + 3)   # (0:nxc+2, 0:nyc+2, 0:nzc+2)
         return np.ascontiguousarray(g[1:nz + 1, 1:ny + 1, 1:nx + 1])
 
     def stage(self, st, ns):

@@ -134,3 +134,148 @@ def test_golden_fixtures_reproduce(built):
     for k in ("ux", "uy", "uz", "p"):
         assert rel_l2(s[k], g[k + "1"]) < 1e-14, k
     assert abs(d["divmax2"] - meta["info"]["1"]["divmax2"]) < 1e-14
+
+
+def _cfg4(nx, ny, nz):
+    from channel3d_b200 import workloads
+    cfg, _ = workloads.get("channel128_re5600_4th")
+    return cfg.copy(nxc=nx, nyc=ny, nzc=nz, nycSection=[ny // 2, ny - ny // 2])
+
+
+def _d4(a, axis, rd, shift):
+    """Staggered 4th-order first difference (1/24, -9/8, 9/8, -1/24) * rd over
+    the points shift-1 .. shift+2 relative to each cell (periodic axis)."""
+    c = (1.0 / 24.0, -1.125, 1.125, -1.0 / 24.0)
+    return sum(cq * np.roll(a, -(shift + q - 1), axis) for q, cq in enumerate(c)) * rd
+
+
+def test_poisson_residual_4th(built):
+    """The 4th-order pressure operator is div4(grad4 phi) in x and z: the
+    modified wavenumber rdx2/288 (cos 3t - 54 cos 2t + 783 cos t - 730)
+    (src/CFD_4th/m_Poisson.f90:40-47) is the symbol of the composition of the
+    staggered 4th-order difference with itself."""
+    from oracle import oracle as O
+    cfg = _cfg4(24, 20, 12)
+    o = O.Oracle(cfg)
+    src = np.random.default_rng(5).standard_normal(cfg.shape)
+    phi = o.poisson(src)
+    rdx, rdz = cfg.nxc / cfg.xlx, cfg.nzc / cfg.zlz
+    # gradient at the face below the cell (shift -1: points i-2..i+1), divergence
+    # over the faces i..i+1 with the wide neighbours (points i-1..i+2)
+    L = _d4(_d4(phi, 2, rdx, -1), 2, rdx, 0) + _d4(_d4(phi, 0, rdz, -1), 0, rdz, 0)
+    yL = _laplacian(cfg, o, phi) - (
+        (np.roll(phi, 1, 2) - 2 * phi + np.roll(phi, -1, 2)) * rdx ** 2
+        + (np.roll(phi, 1, 0) - 2 * phi + np.roll(phi, -1, 0)) * rdz ** 2)
+    r = L + yL - src
+    rm = r.mean(axis=(0, 2))
+    assert np.abs(r - rm[None, :, None]).max() < 1e-9 * np.abs(src).max()
+    assert np.abs(rm[1:]).max() < 1e-9 * np.abs(src).max()
+
+
+def test_step_4th_is_divergence_free_and_deterministic(built):
+    from channel3d_b200 import initfield
+    from oracle import oracle as O
+    cfg = _cfg4(32, 24, 16)
+    o = O.Oracle(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0])
+    O.set_threads(1)
+    o.set_state(ux, uy, uz, p)
+    d = o.step(3)
+    a = o.get_state()
+    assert d["divmax2"] < 1e-13 and d["rc"] == 0
+    O.set_threads(4)
+    o.set_state(ux, uy, uz, p)
+    o.step(3)
+    b = o.get_state()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_laminar_4th_keeps_flux_balance(built):
+    """Without noise the 4th-order step keeps v = w = 0 and an x,z-uniform
+    ux; the forcing (mean viscous stress, src/CFD_4th/m_TScheme.f90:364-377)
+    balances the wall friction, so the bulk velocity is unchanged."""
+    from channel3d_b200 import initfield
+    from oracle import oracle as O
+    cfg = _cfg4(16, 24, 8)
+    o = O.Oracle(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0], amplitude=0.0)
+    o.set_state(ux, uy, uz, p)
+    d0 = o.step(1)
+    d = o.step(9)
+    s = o.get_state()
+    assert np.abs(s["uy"]).max() < 1e-14 and np.abs(s["uz"]).max() < 1e-14
+    assert np.abs(s["ux"] - s["ux"][:1, :, :1]).max() < 1e-13
+    assert abs(d["uxm"] - d0["uxm"]) < 1e-12
+
+
+def _cfg_fimp(nx, ny, nz):
+    from channel3d_b200 import workloads
+    cfg, _ = workloads.get("channel128_re5600_fimp")
+    return cfg.copy(nxc=nx, nyc=ny, nzc=nz, nycSection=[ny // 2, ny - ny // 2])
+
+
+def test_fimp_adi_factorisation(built):
+    """clcU1Hat_FIMP_010 (src/CFD_2nd/m_TSchemeFIMP_inc.f90:263-347): the
+    increment du = u* - u satisfies (I - b Lx)(I - b Lz)(I - b Ly) du = RhsX
+    with the periodic 3-point Lx, Lz and the Crank-Nicolson Ly whose wall
+    coefficient is doubled (am2cForCN(1), ap2cForCN(nyc))."""
+    from oracle import oracle as O
+    cfg = _cfg_fimp(16, 12, 10)
+    o = O.Oracle(cfg)
+    from channel3d_b200 import initfield
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0])
+    o.set_state(ux, uy, uz, p)
+    o.stage(0, 1)
+    o.stage(1, 1)
+    rhs = o.get_interior(o.ARR1)
+    u0 = o.get_state()["ux"]
+    o.stage(2, 1)
+    du = o.get_state()["ux"] - u0
+    beta = 0.5 * (8.0 / 15.0) * cfg.xnu * cfg.dtMax
+    rdx2, rdz2 = (cfg.nxc / cfg.xlx) ** 2, (cfg.nzc / cfg.zlz) ** 2
+    yp = o.mesh()[0]
+    ny = cfg.nyc
+    dyp = yp[1:] - yp[:-1]
+    yc = 0.5 * (yp[1:] + yp[:-1])
+    dyc = np.ones(ny + 2)
+    dyc[2:ny + 1] = yc[1:] - yc[:-1]
+    dyc[1] = dyp[0]
+    dyc[ny + 1] = dyp[-1]
+    rdyc = 1.0 / dyc
+    am = np.array([rdyc[j] / dyp[j - 1] for j in range(1, ny + 1)])
+    ap = np.array([rdyc[j + 1] / dyp[j - 1] for j in range(1, ny + 1)])
+    am[0] = 4 * rdyc[1] / (dyc[1] + 2 * dyc[2])
+    ap[0] = 4 * rdyc[2] / (dyc[1] + 2 * dyc[2])
+    am[-1] = 4 * rdyc[ny] / (dyc[ny + 1] + 2 * dyc[ny])
+    ap[-1] = 4 * rdyc[ny + 1] / (dyc[ny + 1] + 2 * dyc[ny])
+    am[0] *= 2.0
+    ap[-1] *= 2.0
+    tp, tm = -beta * ap, -beta * am
+    tc = 1.0 - tp - tm
+    w = tc[None, :, None] * du
+    w[:, :-1, :] += tp[None, :-1, None] * du[:, 1:, :]
+    w[:, 1:, :] += tm[None, 1:, None] * du[:, :-1, :]
+    w = (1 + 2 * beta * rdz2) * w - beta * rdz2 * (np.roll(w, 1, 0) + np.roll(w, -1, 0))
+    w = (1 + 2 * beta * rdx2) * w - beta * rdx2 * (np.roll(w, 1, 2) + np.roll(w, -1, 2))
+    assert np.abs(w - rhs).max() < 1e-12 * np.abs(rhs).max()
+
+
+def test_fimp_step_is_divergence_free_and_laminar_steady(built):
+    from channel3d_b200 import initfield
+    from oracle import oracle as O
+    cfg = _cfg_fimp(32, 24, 16)
+    o = O.Oracle(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0])
+    o.set_state(ux, uy, uz, p)
+    d = o.step(3)
+    assert d["divmax2"] < 1e-13 and d["rc"] == 0
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0], amplitude=0.0)
+    o.set_state(ux, uy, uz, p)
+    d0 = o.step(1)
+    d = o.step(5)
+    s = o.get_state()
+    assert np.abs(s["uy"]).max() < 1e-14 and np.abs(s["uz"]).max() < 1e-14
+    assert np.abs(s["ux"] - s["ux"][:1, :, :1]).max() < 1e-13
+    # the bulk controller drives <u> to ubulk = 1 from the discretised profile
+    assert abs(d["uxm"] - 1.0) < 0.01 * abs(d0["uxm"] - 1.0)

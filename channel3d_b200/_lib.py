@@ -91,6 +91,7 @@ SIGNATURES = {
     "ch3d_project": (ctypes.c_int, [_VP, _DP, _DP]),
     "ch3d_set_dt": (ctypes.c_int, [_VP, ctypes.c_double]),
     "ch3d_stats_accumulate": (ctypes.c_int, [_VP]),
+    "ch3d_sgs_viscosity": (ctypes.c_int, [_VP]),
     "ch3d_stats_fetch": (ctypes.c_int, [_VP, _DP, _IP, _DP, ctypes.c_int]),
     "ch3d_memory_bytes": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong)]),
     "ch3d_last_step_ms": (ctypes.c_int, [_VP, _DP]),

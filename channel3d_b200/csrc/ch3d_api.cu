@@ -220,7 +220,15 @@ int check_config(const ch3d_config* g) {
   for (int s = 2; s < 4; ++s)
     if (g->BcOption[s] != -1 && g->BcOption[s] != -2)
       return fail(CH3D_ERR_UNSUPPORTED, "y boundaries must be no-slip (-1) or free-slip (-2)");
-  if (g->LES_type != 0) return fail(CH3D_ERR_UNSUPPORTED, "LES_type=%d not built", g->LES_type);
+  if (g->LES_type != 0) {
+    if (g->LES_type != CH3D_LES_WALE && g->LES_type != CH3D_LES_MTS && g->LES_type != CH3D_LES_SMAG_VD)
+      return fail(CH3D_ERR_UNSUPPORTED, "LES_type=%d not built", g->LES_type);
+    if (g->order != 2 || g->IsImplicit != 1 || g->precision != CH3D_PREC_FP64)
+      return fail(CH3D_ERR_UNSUPPORTED, "LES is built for the 2nd-order partially implicit FP64 step (the reference "
+                  "has no FIMP+LES either)");
+    if (g->LES_type == CH3D_LES_MTS && g->FilterType != 0 && g->FilterType != 1)
+      return fail(CH3D_ERR_INVALID, "unrecognized FilterType");
+  }
   if (g->precision != CH3D_PREC_FP64 && g->precision != CH3D_PREC_MIXED) return fail(CH3D_ERR_INVALID, "bad precision");
   if (g->IsUxConst && !(g->ybulk2 > g->ybulk1)) return fail(CH3D_ERR_INVALID, "ybulk1 OR ybulk2 wrong");
   if (!(g->dtMax > 0)) return fail(CH3D_ERR_INVALID, "dtMax must be positive");
@@ -231,10 +239,19 @@ template <class T>
 int alloc_fields(ch3d_ctx* c) {
   typedef typename CplxOf<T>::type CT;
   for (int q = 0; q < 15; ++q) {
-    if (q == 11) continue;  // nut: LES only
+    if (q == 11 && c->cfg.LES_type == 0) continue;  // nut: LES only
     CU(cudaMalloc(&c->f[q], (size_t)c->N * sizeof(T)));
     CU(cudaMemsetAsync(c->f[q], 0, (size_t)c->N * sizeof(T), c->stream));
     c->bytes += (long long)c->N * sizeof(T);
+  }
+  if (c->cfg.LES_type > 0) {
+    // DeltaCell(jc) = (dyp dx dz)^(1/3) (src/CFD_2nd/m_MeshAndMetries.f90:204) and the
+    // wall distance of the cell centres for the van Driest damping
+    std::vector<double> h((size_t)2 * (c->ny + 2), 0.0);
+    for (int j = 0; j <= c->ny + 1; ++j) h[j] = std::pow(c->dyp[j] * c->dx * c->dz, 1.0 / 3.0);
+    for (int j = 1; j <= c->ny; ++j) h[c->ny + 2 + j] = std::min(c->yc[j] - c->yp[1], c->yp[c->ny + 1] - c->yc[j]);
+    CU(cudaMalloc(&c->les_delta, h.size() * sizeof(double)));
+    CU(cudaMemcpy(c->les_delta, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
   if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
     const size_t nb = ptri_factor_doubles(c->nx, c->nz) * sizeof(double);
@@ -371,12 +388,16 @@ int init_scalars(ch3d_ctx* c) {
 
 int record_step(ch3d_ctx* c) {
   CU(launch_step_begin(c));
+  if (c->cfg.LES_type > 0) CU(launch_sgs_nut(c));  // once per step, after the CFL (m_ChannelSystem.f90:89)
   const bool o4 = c->cfg.order == 4, fimp = c->cfg.order == 2 && c->cfg.IsImplicit == 2;
   for (int ns = 1; ns <= c->iadvance; ++ns) {
     if (o4) CU(launch_visc4_partials(c));
     CU(launch_substep_setup(c, ns));
     CU(launch_helm_factors(c));
-    if (fimp) {
+    if (c->cfg.LES_type > 0) {
+      CU(launch_rhs_les(c));
+      CU(launch_uhat_les(c));
+    } else if (fimp) {
       CU(launch_rhs_fimp(c));
       CU(launch_ptri_xz(c));
       CU(launch_uhat(c));
@@ -588,6 +609,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   for (int q = 0; q < 15; ++q) if (c->f[q]) cudaFree(c->f[q]);
   for (int q = 0; q < 6; ++q) if (c->ih[q]) cudaFree(c->ih[q]);
   if (c->pfac) cudaFree(c->pfac);
+  if (c->les_delta) cudaFree(c->les_delta);
   void* bufs[] = {c->hfac, c->yRM, c->yCP, c->yIF, c->yRM64, c->yCP64, c->yIF64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
@@ -686,8 +708,12 @@ int ch3d_stage(ch3d_ctx* c, int stage, int ns) {
       if (c->cfg.order == 4) CU(launch_visc4_partials(c));  // forcing of clcRhsXYZ from the current ux
       CU(launch_substep_setup(c, ns));
       break;
-    case 1: CU(c->cfg.order == 4 ? launch_rhs4(c) : (c->cfg.IsImplicit == 2 ? launch_rhs_fimp(c) : launch_rhs(c))); break;
+    case 1:
+      if (c->cfg.LES_type > 0) CU(launch_rhs_les(c));
+      else CU(c->cfg.order == 4 ? launch_rhs4(c) : (c->cfg.IsImplicit == 2 ? launch_rhs_fimp(c) : launch_rhs(c)));
+      break;
     case 2:
+      if (c->cfg.LES_type > 0) { CU(launch_uhat_les(c)); break; }
       if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) CU(launch_ptri_xz(c));
       CU(launch_helm_factors(c));
       CU(launch_uhat(c));
@@ -711,6 +737,7 @@ static int array_slot(int which) {
   switch (which) {
     case 0: case 1: case 2: case 3: case 4: case 5: case 6: case 7: case 8: return which;
     case 9: return 10;   // prphi (the reference keeps RhsZ and prphiHalo in RealHalo)
+    case 10: return 11;  // nut (LES), total viscosity
     case 11: return 9;   // RhsZ
     case 12: case 13: case 14: return which;  // u* (velocity after the Helmholtz solves)
     default: return -1;
@@ -816,6 +843,16 @@ int ch3d_stats_fetch(ch3d_ctx* c, double* sumstat, int* nfstime, double* prgrads
   return CH3D_OK;
 }
 
+int ch3d_sgs_viscosity(ch3d_ctx* c) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (c->cfg.LES_type == 0) return fail(CH3D_ERR_INVALID, "LES_type is 0");
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
+  CU(launch_sgs_nut(c));
+  CU(cudaStreamSynchronize(c->stream));
+  return CH3D_OK;
+}
+
 int ch3d_memory_bytes(ch3d_ctx* c, long long* bytes) {
   if (!c || !bytes) return fail(CH3D_ERR_INVALID, "NULL argument");
   *bytes = c->bytes;
@@ -839,12 +876,15 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
   auto mark = [&](int g) { grp.push_back(g); return cudaEventRecord(ev[q++], c->stream); };
   auto done = [&]() { return cudaEventRecord(ev[q++], c->stream); };
   for (int s = 0; s < nsteps; ++s) {
-    CU(mark(6)); CU(launch_step_begin(c)); CU(done());
+    CU(mark(6)); CU(launch_step_begin(c)); if (c->cfg.LES_type > 0) CU(launch_sgs_nut(c)); CU(done());
     for (int ns = 1; ns <= c->iadvance; ++ns) {
       CU(mark(6));
       if (c->cfg.order == 4) CU(launch_visc4_partials(c));
       CU(launch_substep_setup(c, ns)); CU(launch_helm_factors(c)); CU(done());
-      if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
+      if (c->cfg.LES_type > 0) {
+        CU(mark(0)); CU(launch_rhs_les(c)); CU(done());
+        CU(mark(1)); CU(launch_uhat_les(c)); CU(done());
+      } else if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
         CU(mark(0)); CU(launch_rhs_fimp(c)); CU(done());
         CU(mark(1)); CU(launch_ptri_xz(c)); CU(launch_uhat(c)); CU(done());
       } else {

@@ -33,6 +33,7 @@ struct DevScalars {
   double pmGamma, pmTheta, pmAlpha, pmBeta, pmAlphaC, pmBetaT;
   double dpmdxns, PrGradNow, PrGradAver;
   double cflmp, uxm, s1tot1;
+  double utau;                                          // LES: wall friction velocity of the step
   unsigned long long divmax1, divmax2, vmax[3], uddx;  // bit patterns of non-negative doubles
   int itime, status, ns, pad;
 };
@@ -61,6 +62,7 @@ template <class T> struct Geo {
   int nx, ny, nz, nxh;
   int order;                            // 2: src/CFD_2nd, 4: src/CFD_4th
   int implicit;                         // IsImplicit: 1 PIMP (CN in y), 2 FIMP (CN in x, y, z)
+  int les;                              // LES_type > 0: variable viscosity nut
   long long N;
   T rdx, rdz, rdx2, rdz2;
   T ap1c, ac1c, am1c, ap3c, ac3c, am3c;  // constant for periodic x and z

@@ -37,6 +37,7 @@ struct ch3d_ctx {
   void* ih[6] = {nullptr};   // 4th order: uxhx uyhx uzhx uxhz uyhz uzhz (precision T)
   double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
   double* pfac = nullptr;    // FIMP: periodic x/z sweep factors of the current substep
+  double* les_delta = nullptr;  // LES: DeltaCell (ny+2) | wall distance of the cell centres (ny+2)
   void* yRM = nullptr;       // Poisson y-solve chunk factors per mode (fixed for the run);
   void* yCP = nullptr;       // FP64, or FP32 in the mixed path
   void* yIF = nullptr;       // Poisson interface factors per mode
@@ -108,4 +109,8 @@ cudaError_t launch_visc4_partials(ch3d_ctx* c);        // mean viscous stress pa
 cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP -> RhsX/Y/Z
 cudaError_t launch_ptri_xz(ch3d_ctx* c);               // periodic x and z sweeps of RhsX/Y/Z, in place
 size_t ptri_factor_doubles(int nx, int nz);
+// LES (ch3d_les.cu), FP64
+cudaError_t launch_sgs_nut(ch3d_ctx* c);               // Clc_SGS_Vis -> nut
+cudaError_t launch_rhs_les(ch3d_ctx* c);               // clcRhsX/Y/Z_PIMP_LES -> RhsX/Y/Z
+cudaError_t launch_uhat_les(ch3d_ctx* c);              // clcU1/2/3Hat_PIMP_LES -> u*
 }  // namespace ch3d

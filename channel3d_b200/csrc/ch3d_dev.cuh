@@ -170,6 +170,7 @@ template <class T> Geo<T> make_geo(const ch3d_ctx* c) {
   g.nx = c->nx; g.ny = c->ny; g.nz = c->nz; g.nxh = c->nxh; g.N = c->N;
   g.order = c->cfg.order;
   g.implicit = c->cfg.IsImplicit;
+  g.les = c->cfg.LES_type > 0 ? 1 : 0;
   g.rdx = (T)c->rdx; g.rdz = (T)c->rdz; g.rdx2 = (T)c->rdx2; g.rdz2 = (T)c->rdz2;
   // periodic x and z: am1c = ap1c = rdx2, ac1c = -(am1c+ap1c) (m_MeshAndMetries.f90:243-252)
   g.ap1c = (T)c->rdx2; g.am1c = (T)c->rdx2; g.ac1c = (T)(-(c->rdx2 + c->rdx2));

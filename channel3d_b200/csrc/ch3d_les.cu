@@ -1,0 +1,393 @@
+// ch3d_les.cu -- sm_100a kernels of the LES step (2nd order, y Crank-Nicolson):
+// the eddy viscosity of Clc_SGS_Vis (src/CFD_2nd/m_LESModels.f90:47-428)
+// for the WALE and mixed-time-scale models and the Smagorinsky model with
+// van Driest damping, the variable-viscosity right-hand sides
+// clcRhsX/Y/Z_PIMP_LES and the variable-coefficient y solves
+// clcU1/2/3Hat_PIMP_LES (src/CFD_2nd/m_TSchemePIMP_inc.f90:80-387, 466-809).
+// FP64.  nut holds the total viscosity (xnu included), interior cells; its
+// wall ghosts follow SetBC_and_UpdateHalo_SGS (2 xnu - nut for no-slip walls,
+// nut for free-slip), x and z wrap.
+#include "ch3d_ctx.h"
+#include "ch3d_dev.cuh"
+
+namespace ch3d {
+
+// nut at a y row that may be the wall ghost (j = -1 or ny)
+__device__ __forceinline__ double nut_at(const double* __restrict__ nut, const Geo<double>& g, const Nbr& n,
+                                         long long o, int dj) {
+  if (dj < 0 && n.jlo) {
+    const double v = __ldg(nut + n.c + o);
+    return g.bc.lo == -1 ? 2.0 * (double)g.xnu - v : v;
+  }
+  if (dj > 0 && n.jhi) {
+    const double v = __ldg(nut + n.c + o);
+    return g.bc.hi == -1 ? 2.0 * (double)g.xnu - v : v;
+  }
+  return __ldg(nut + n.c + o + (long long)dj * n.yp);
+}
+
+// |S| = sqrt(2 Sij Sij) of ClcVelStrainRate (src/CFD_2nd/m_LESModels.f90:328-370)
+__device__ __forceinline__ double strain_rate(const Geo<double>& g, const Metrics<double>& m, const double* ux,
+                                              const double* uy, const double* uz, const Nbr& n, int jc) {
+  const double rdx = g.rdx, rdz = g.rdz;
+  const double caj = m.rdyp[jc], cac1 = m.rdyc[jc], cac2 = m.rdyc[jc + 1], cac12 = cac1 - cac2;
+  const double e = 0.125;
+  const double st1 = (at(ux, n, n.xp) - at(ux, n, 0)) * rdx;
+  const double st2 = (at_jp(uy, g, 1, n, 0) - at(uy, n, 0)) * caj;
+  const double st3 = (at(uz, n, n.zp) - at(uz, n, 0)) * rdz;
+  const double st4 = e * ((at_jp(uy, g, 1, n, n.xp) - at_jp(uy, g, 1, n, n.xm) + at(uy, n, n.xp) - at(uy, n, n.xm)) * rdx +
+                          (at_jp(ux, g, 0, n, n.xp) + at_jp(ux, g, 0, n, 0)) * cac2 +
+                          (at(ux, n, n.xp) + at(ux, n, 0)) * cac12 -
+                          (at_jm(ux, g, 0, n, n.xp) + at_jm(ux, g, 0, n, 0)) * cac1);
+  const double st5 = e * ((at(ux, n, n.xp + n.zp) + at(ux, n, n.zp) - at(ux, n, n.xp + n.zm) - at(ux, n, n.zm)) * rdz +
+                          (at(uz, n, n.xp + n.zp) - at(uz, n, n.xm + n.zp) + at(uz, n, n.xp) - at(uz, n, n.xm)) * rdx);
+  const double st6 = e * ((at_jp(uy, g, 1, n, n.zp) + at(uy, n, n.zp) - at_jp(uy, g, 1, n, n.zm) - at(uy, n, n.zm)) * rdz +
+                          (at_jp(uz, g, 2, n, n.zp) + at_jp(uz, g, 2, n, 0)) * cac2 +
+                          (at(uz, n, n.zp) + at(uz, n, 0)) * cac12 -
+                          (at_jm(uz, g, 2, n, n.zp) + at_jm(uz, g, 2, n, 0)) * cac1);
+  return sqrt(2.0 * (st1 * st1 + st2 * st2 + st3 * st3) + 4.0 * (st4 * st4 + st5 * st5 + st6 * st6));
+}
+
+struct LesPar {
+  const double* delta;  // DeltaCell(jc), jc = 0..nyp
+  const double* dwall;  // wall distance of the cell centre, jc = 1..nyc
+  double Fc[9];         // MTS test filter (InitFilterCoe)
+  double Cs;
+  int model;            // CH3D_LES_*
+};
+
+// x-z mean wall shear -> u_tau (Smagorinsky / van Driest); one block
+__global__ void __launch_bounds__(1024) k_wall_utau(Geo<double> g, const double* __restrict__ ux, double d1, double dN,
+                                                    DevScalars* __restrict__ sc) {
+  __shared__ double r1[1024], r2[1024];
+  if (sc->status) return;
+  const long long plane = (long long)g.nx * g.ny;
+  double s1 = 0, s2 = 0;
+  for (int q = threadIdx.x; q < g.nx * g.nz; q += blockDim.x) {
+    const int i = q % g.nx, k = q / g.nx;
+    s1 += ux[i + plane * k];
+    s2 += ux[i + (long long)g.nx * (g.ny - 1) + plane * k];
+  }
+  r1[threadIdx.x] = s1; r2[threadIdx.x] = s2;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { r1[threadIdx.x] += r1[threadIdx.x + w]; r2[threadIdx.x] += r2[threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double inxz = 1.0 / ((double)g.nx * (double)g.nz);
+    const double tw = (double)g.xnu * 0.5 * (fabs(r1[0] * inxz - g.bc.ux_lo) / d1 + fabs(r2[0] * inxz - g.bc.ux_hi) / dN);
+    sc->utau = sqrt(tw);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_sgs_nut(Geo<double> g, Metrics<double> m, LesPar lp,
+                                                 const double* __restrict__ ux, const double* __restrict__ uy,
+                                                 const double* __restrict__ uz, double* __restrict__ nut,
+                                                 const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const Nbr n = make_nbr(g, i, j, k);
+  const int jc = j + 1;
+  const double xnu = g.xnu, rdx = g.rdx, rdz = g.rdz;
+  double v;
+  if (lp.model == CH3D_LES_WALE) {  // Clc_SGS_WALE (m_LESModels.f90:72-135)
+    const double caj = m.rdyp[jc], cac1 = m.rdyc[jc], cac2 = m.rdyc[jc + 1], cac12 = cac1 - cac2;
+    double CwDelta2 = 0.325 * lp.delta[jc];
+    CwDelta2 = CwDelta2 * CwDelta2;
+    const double dudx = (at(ux, n, n.xp) - at(ux, n, 0)) * rdx;
+    const double dudy = ((at_jp(ux, g, 0, n, n.xp) + at_jp(ux, g, 0, n, 0)) * cac2 + (at(ux, n, n.xp) + at(ux, n, 0)) * cac12 -
+                         (at_jm(ux, g, 0, n, n.xp) + at_jm(ux, g, 0, n, 0)) * cac1) * 0.25;
+    const double dudz = (at(ux, n, n.xp + n.zp) + at(ux, n, n.zp) - at(ux, n, n.xp + n.zm) - at(ux, n, n.zm)) * rdz * 0.25;
+    const double dvdx = (at_jp(uy, g, 1, n, n.xp) - at_jp(uy, g, 1, n, n.xm) + at(uy, n, n.xp) - at(uy, n, n.xm)) * rdx * 0.25;
+    const double dvdy = (at_jp(uy, g, 1, n, 0) - at(uy, n, 0)) * caj;
+    const double dvdz = (at_jp(uy, g, 1, n, n.zp) + at(uy, n, n.zp) - at_jp(uy, g, 1, n, n.zm) - at(uy, n, n.zm)) * rdz * 0.25;
+    const double dwdx = (at(uz, n, n.xp + n.zp) - at(uz, n, n.xm + n.zp) + at(uz, n, n.xp) - at(uz, n, n.xm)) * rdx * 0.25;
+    const double dwdy = ((at_jp(uz, g, 2, n, n.zp) + at_jp(uz, g, 2, n, 0)) * cac2 + (at(uz, n, n.zp) + at(uz, n, 0)) * cac12 -
+                         (at_jm(uz, g, 2, n, n.zp) + at_jm(uz, g, 2, n, 0)) * cac1) * 0.25;
+    const double dwdz = (at(uz, n, n.zp) - at(uz, n, 0)) * rdz;
+    const double S11 = dudx, S12 = (dudy + dvdx) * 0.5, S13 = (dudz + dwdx) * 0.5;
+    const double S22 = dvdy, S23 = (dvdz + dwdy) * 0.5, S33 = dwdz;
+    const double SijSij = S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23);
+    double Sd11 = dudx * dudx + dudy * dvdx + dudz * dwdx;
+    const double Sd12 = (dudx * dudy + dudy * dvdy + dudz * dwdy + dvdx * dudx + dvdy * dvdx + dvdz * dwdx) * 0.5;
+    const double Sd13 = (dudx * dudz + dudy * dvdz + dudz * dwdz + dwdx * dudx + dwdy * dvdx + dwdz * dwdx) * 0.5;
+    double Sd22 = dvdx * dudy + dvdy * dvdy + dvdz * dwdy;
+    const double Sd23 = (dvdx * dudz + dvdy * dvdz + dvdz * dwdz + dwdx * dudy + dwdy * dvdy + dwdz * dwdy) * 0.5;
+    double Sd33 = dwdx * dudz + dwdy * dvdz + dwdz * dwdz;
+    const double SdTrace = (Sd11 + Sd22 + Sd33) / 3.0;
+    Sd11 -= SdTrace; Sd22 -= SdTrace; Sd33 -= SdTrace;
+    const double Sd2 = Sd11 * Sd11 + Sd22 * Sd22 + Sd33 * Sd33 + 2.0 * (Sd12 * Sd12 + Sd13 * Sd13 + Sd23 * Sd23);
+    v = CwDelta2 * pow(Sd2, 1.5) / (pow(SijSij, 2.5) + pow(Sd2, 1.25)) + xnu;
+  } else if (lp.model == CH3D_LES_MTS) {  // Clc_SGS_MTS (m_LESModels.f90:145-258)
+    const double* F = lp.Fc;
+    // test-filtered fluctuation u - F(u) of a staggered component at offset o of row dj
+    auto filt = [&](const double* u, int comp, long long o, int dj) {
+      auto val = [&](long long oo) { return dj > 0 ? at_jp(u, g, comp, n, o + oo) : at(u, n, o + oo); };
+      return F[0] * val(n.xm + n.zm) + F[1] * val(n.zm) + F[2] * val(n.xp + n.zm) +
+             F[3] * val(n.xm) + (F[4] - 1.0) * val(0) + F[5] * val(n.xp) +
+             F[6] * val(n.xm + n.zp) + F[7] * val(n.zp) + F[8] * val(n.xp + n.zp);
+    };
+    // ux at i and i+1 (the i+1 stencil wraps through the offsets of cell i+1)
+    const Nbr nx1 = make_nbr(g, (i + 1 == g.nx) ? 0 : i + 1, j, k);
+    const double fa = filt(ux, 0, 0, 0);
+    double fb;
+    {
+      const Nbr& q = nx1;
+      auto valb = [&](long long oo) { return at(ux, q, oo); };
+      fb = F[0] * valb(q.xm + q.zm) + F[1] * valb(q.zm) + F[2] * valb(q.xp + q.zm) + F[3] * valb(q.xm) +
+           (F[4] - 1.0) * valb(0) + F[5] * valb(q.xp) + F[6] * valb(q.xm + q.zp) + F[7] * valb(q.zp) +
+           F[8] * valb(q.xp + q.zp);
+    }
+    double Kes = 0.5 * (fa * fa + fb * fb);
+    const double ga = filt(uy, 1, 0, 0), gb = filt(uy, 1, 0, 1);  // uy at jc and jc+1 (jc+1 = nyp: wall value)
+    Kes = Kes + 0.5 * (ga * ga + gb * gb);
+    const Nbr nz1 = make_nbr(g, i, j, (k + 1 == g.nz) ? 0 : k + 1);
+    const double ha = filt(uz, 2, 0, 0);
+    double hb;
+    {
+      const Nbr& q = nz1;
+      auto valb = [&](long long oo) { return at(uz, q, oo); };
+      hb = F[0] * valb(q.xm + q.zm) + F[1] * valb(q.zm) + F[2] * valb(q.xp + q.zm) + F[3] * valb(q.xm) +
+           (F[4] - 1.0) * valb(0) + F[5] * valb(q.xp) + F[6] * valb(q.xm + q.zp) + F[7] * valb(q.zp) +
+           F[8] * valb(q.xp + q.zp);
+    }
+    Kes = Kes + 0.5 * (ha * ha + hb * hb);
+    const double rdelta = 1.0 / lp.delta[jc];
+    double Ts = sqrt(Kes) * rdelta + strain_rate(g, m, ux, uy, uz, n, jc) / 10.0;
+    Ts = Ts < 1.0e-10 ? 0.0 : 1.0 / Ts;
+    v = 0.05 * Kes * Ts + xnu;
+  } else {  // Smagorinsky + van Driest damping
+    const double D = 1.0 - exp(-(lp.dwall[jc] * sc->utau / xnu) / 26.0);
+    const double l = lp.Cs * D * lp.delta[jc];
+    v = l * l * strain_rate(g, m, ux, uy, uz, n, jc) + xnu;
+  }
+  nut[n.c] = v;
+}
+
+// clcRhsX/Y/Z_PIMP_LES at one cell; RhsX includes dpmdxns (:140-153).
+__global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> m, const double* __restrict__ ux,
+                                                 const double* __restrict__ uy, const double* __restrict__ uz,
+                                                 const double* __restrict__ pr, const double* __restrict__ nut,
+                                                 double* __restrict__ hx, double* __restrict__ hy,
+                                                 double* __restrict__ hz, double* __restrict__ rx,
+                                                 double* __restrict__ ry, double* __restrict__ rz,
+                                                 const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const Nbr n = make_nbr(g, i, j, k);
+  const int jc = j + 1;
+  const double pmGamma = sc->pmGamma, pmTheta = sc->pmTheta, pmAlpha = sc->pmAlpha, pmBetaT = sc->pmBetaT;
+  const double rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2;
+  const double qdx1 = 0.25 * rdx, qdx3 = 0.25 * rdz;
+  auto N = [&](long long o, int dj) { return nut_at(nut, g, n, o, dj); };
+  {  // RhsX (m_TSchemePIMP_inc.f90:80-156)
+    const double sucaj = 0.25 * m.rdyp[jc];
+    const double u_c = at(ux, n, 0), u_ip = at(ux, n, n.xp), u_im = at(ux, n, n.xm);
+    const double u_jp = at_jp(ux, g, 0, n, 0), u_jm = at_jm(ux, g, 0, n, 0);
+    const double u_kp = at(ux, n, n.zp), u_km = at(ux, n, n.zm);
+    const double h11 = ((u_ip + u_c) * (u_ip + u_c) - (u_c + u_im) * (u_c + u_im)) * qdx1;
+    const double h12 = ((at_jp(uy, g, 1, n, 0) + at_jp(uy, g, 1, n, n.xm)) * (u_jp + u_c) -
+                        (at(uy, n, 0) + at(uy, n, n.xm)) * (u_c + u_jm)) * sucaj;
+    const double h13 = ((at(uz, n, n.zp) + at(uz, n, n.xm + n.zp)) * (u_kp + u_c) -
+                        (at(uz, n, 0) + at(uz, n, n.xm)) * (u_c + u_km)) * qdx3;
+    const double n_c = N(0, 0), n_im = N(n.xm, 0);
+    const double visa = 0.25 * (n_c + n_im + N(0, -1) + N(n.xm, -1));
+    const double visb = 0.25 * (n_c + n_im + N(0, 1) + N(n.xm, 1));
+    const double visc = 0.25 * (n_c + n_im + N(n.zm, 0) + N(n.xm + n.zm, 0));
+    const double visd = 0.25 * (n_c + n_im + N(n.zp, 0) + N(n.xm + n.zp, 0));
+    const double sgs1 = rdx2 * (n_c * (u_ip - u_c) - n_im * (u_c - u_im));
+    const double sgs2 = rdx * m.rdyp[jc] * (visb * (at_jp(uy, g, 1, n, 0) - at_jp(uy, g, 1, n, n.xm)) -
+                                            visa * (at(uy, n, 0) - at(uy, n, n.xm)));
+    const double sgs3 = rdx * rdz * (visd * (at(uz, n, n.zp) - at(uz, n, n.xm + n.zp)) - visc * (at(uz, n, 0) - at(uz, n, n.xm)));
+    const double d22q1 = m.ap2c[jc] * visb * (u_jp - u_c) - m.am2c[jc] * visa * (u_c - u_jm);
+    const double d33q1 = g.ap3c * visd * (u_kp - u_c) - g.am3c * visc * (u_c - u_km);
+    const double dcq13 = sgs1 + d33q1;
+    const double gradp1 = (at(pr, n, 0) - at(pr, n, n.xm)) * rdx;
+    const double conv = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + g.g1;
+    const double ho = hx[n.c];
+    hx[n.c] = conv;
+    rx[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp1 + 2.0 * pmBetaT * d22q1 + sc->dpmdxns;
+  }
+  {  // RhsY (:214-272)
+    const double sucac = m.rdyc[jc], qsucac = 0.25 * sucac;
+    const double v_c = at(uy, n, 0), v_ip = at(uy, n, n.xp), v_im = at(uy, n, n.xm);
+    const double v_jp = at_jp(uy, g, 1, n, 0), v_jm = at_jm(uy, g, 1, n, 0);
+    const double v_kp = at(uy, n, n.zp), v_km = at(uy, n, n.zm);
+    const double h21 = ((at(ux, n, n.xp) + at_jm(ux, g, 0, n, n.xp)) * (v_ip + v_c) -
+                        (at(ux, n, 0) + at_jm(ux, g, 0, n, 0)) * (v_c + v_im)) * qdx1;
+    const double h22 = ((v_jp + v_c) * (v_jp + v_c) - (v_c + v_jm) * (v_c + v_jm)) * qsucac;
+    const double h23 = ((at(uz, n, n.zp) + at_jm(uz, g, 2, n, n.zp)) * (v_kp + v_c) -
+                        (at(uz, n, 0) + at_jm(uz, g, 2, n, 0)) * (v_c + v_km)) * qdx3;
+    const double n_c = N(0, 0), n_jm = N(0, -1);
+    const double visa = 0.25 * (n_c + N(n.xm, 0) + n_jm + N(n.xm, -1));
+    const double visb = 0.25 * (n_c + N(n.xp, 0) + n_jm + N(n.xp, -1));
+    const double visc = 0.25 * (n_c + n_jm + N(n.zm, 0) + N(n.zm, -1));
+    const double visd = 0.25 * (n_c + n_jm + N(n.zp, 0) + N(n.zp, -1));
+    const double sgs1 = rdx * sucac * (visb * (at(ux, n, n.xp) - at_jm(ux, g, 0, n, n.xp)) - visa * (at(ux, n, 0) - at_jm(ux, g, 0, n, 0)));
+    const double sgs2 = m.ap2p[jc] * n_c * (v_jp - v_c) - m.am2p[jc] * n_jm * (v_c - v_jm);
+    const double sgs3 = rdz * sucac * (visd * (at(uz, n, n.zp) - at_jm(uz, g, 2, n, n.zp)) - visc * (at(uz, n, 0) - at_jm(uz, g, 2, n, 0)));
+    const double d11q2 = g.ap1c * visb * (v_ip - v_c) - g.am1c * visa * (v_c - v_im);
+    const double d33q2 = g.ap3c * visd * (v_kp - v_c) - g.am3c * visc * (v_c - v_km);
+    const double dcq13 = d11q2 + d33q2;
+    const double gradp2 = (at(pr, n, 0) - at_jm(pr, g, 3, n, 0)) * sucac;
+    const double conv = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + g.g2;
+    const double ho = hy[n.c];
+    hy[n.c] = conv;
+    ry[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp2 + 2.0 * pmBetaT * sgs2;
+  }
+  {  // RhsZ (:330-387)
+    const double sucaj = 0.25 * m.rdyp[jc];
+    const double w_c = at(uz, n, 0), w_ip = at(uz, n, n.xp), w_im = at(uz, n, n.xm);
+    const double w_jp = at_jp(uz, g, 2, n, 0), w_jm = at_jm(uz, g, 2, n, 0);
+    const double w_kp = at(uz, n, n.zp), w_km = at(uz, n, n.zm);
+    const double h31 = ((at(ux, n, n.xp) + at(ux, n, n.xp + n.zm)) * (w_ip + w_c) -
+                        (at(ux, n, 0) + at(ux, n, n.zm)) * (w_c + w_im)) * qdx1;
+    const double h32 = ((at_jp(uy, g, 1, n, 0) + at_jp(uy, g, 1, n, n.zm)) * (w_jp + w_c) -
+                        (at(uy, n, 0) + at(uy, n, n.zm)) * (w_c + w_jm)) * sucaj;
+    const double h33 = ((w_kp + w_c) * (w_kp + w_c) - (w_c + w_km) * (w_c + w_km)) * qdx3;
+    const double n_c = N(0, 0), n_km = N(n.zm, 0);
+    const double visa = 0.25 * (n_km + N(n.xm + n.zm, 0) + n_c + N(n.xm, 0));
+    const double visb = 0.25 * (n_km + N(n.xp + n.zm, 0) + n_c + N(n.xp, 0));
+    const double visc = 0.25 * (n_km + N(n.zm, -1) + N(0, -1) + n_c);
+    const double visd = 0.25 * (n_km + N(n.zm, 1) + N(0, 1) + n_c);
+    const double sgs1 = rdx * rdz * (visb * (at(ux, n, n.xp) - at(ux, n, n.xp + n.zm)) - visa * (at(ux, n, 0) - at(ux, n, n.zm)));
+    const double sgs2 = rdz * m.rdyp[jc] * (visd * (at_jp(uy, g, 1, n, 0) - at_jp(uy, g, 1, n, n.zm)) -
+                                            visc * (at(uy, n, 0) - at(uy, n, n.zm)));
+    const double sgs3 = rdz2 * (n_c * (w_kp - w_c) - n_km * (w_c - w_km));
+    const double d11q3 = g.ap1c * visb * (w_ip - w_c) - g.am1c * visa * (w_c - w_im);
+    const double d22q3 = m.ap2c[jc] * visd * (w_jp - w_c) - m.am2c[jc] * visc * (w_c - w_jm);
+    const double dcq13 = d11q3 + sgs3;
+    const double gradp3 = (at(pr, n, 0) - at(pr, n, n.zm)) * rdz;
+    const double conv = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + g.g3;
+    const double ho = hz[n.c];
+    hz[n.c] = conv;
+    rz[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp3 + 2.0 * pmBetaT * d22q3;
+  }
+}
+
+// clcU1/2/3Hat_PIMP_LES: one thread per (i, k) column, Thomas along y
+// (InverseTridiagonal, src/CFD_2nd/m_Tools.f90:224-251) with the column's own
+// coefficients; the u* buffer holds the elimination factors until the back
+// substitution overwrites them.  blockIdx.y = component.
+__global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, const double* __restrict__ nut,
+                                                  const double* __restrict__ ux, const double* __restrict__ uy,
+                                                  const double* __restrict__ uz, double* __restrict__ rx,
+                                                  double* __restrict__ ry, double* __restrict__ rz,
+                                                  double* __restrict__ uxs, double* __restrict__ uys,
+                                                  double* __restrict__ uzs, const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= g.nx * g.nz) return;
+  const int comp = blockIdx.y;
+  const int i = col % g.nx, k = col / g.nx;
+  const double* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
+  double* r = comp == 0 ? rx : (comp == 1 ? ry : rz);  // the RHS column is consumed in place
+  double* us = comp == 0 ? uxs : (comp == 1 ? uys : uzs);
+  const double pmBetaT = sc->pmBetaT;
+  const int ny = g.ny;
+  const long long nxl = g.nx;
+  auto coef = [&](int j, double& a, double& b, double& c) {
+    const Nbr n = make_nbr(g, i, j, k);
+    const int jc = j + 1;
+    double rt1, rt2;
+    if (comp == 1) {
+      if (j == 0) { a = 0.0; b = 1.0; c = 0.0; return; }
+      rt1 = pmBetaT * nut_at(nut, g, n, 0, -1) * hc.am2p[jc];
+      rt2 = pmBetaT * nut_at(nut, g, n, 0, 0) * hc.ap2p[jc];
+    } else {
+      const long long o = comp == 0 ? n.xm : n.zm;
+      const double visc = comp == 0 ? 0.25 * (nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, 0, -1) + nut_at(nut, g, n, o, -1))
+                                    : 0.25 * (nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, o, -1) + nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, 0, -1));
+      const double visd = comp == 0 ? 0.25 * (nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, 0, 1) + nut_at(nut, g, n, o, 1))
+                                    : 0.25 * (nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, o, 1) + nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, 0, 1));
+      rt1 = pmBetaT * visc * hc.am2cForCN[jc];
+      rt2 = pmBetaT * visd * hc.ap2cForCN[jc];
+    }
+    a = -rt1; b = rt1 + rt2 + 1.0; c = -rt2;
+  };
+  const long long base = i + nxl * ny * k;
+  double a, b, c;
+  coef(0, a, b, c);
+  double vecm = b;
+  // row 1 of the uy system is the wall condition duy_ym = 0 (constant wall velocity)
+  double f = (comp == 1 ? 0.0 : r[base]) / vecm;
+  r[base] = f;
+  double cprev = c;
+  // forward sweep; arr(j) = c(j-1)/vecm(j-1) is parked in the u* column
+  for (int j = 1; j < ny; ++j) {
+    coef(j, a, b, c);
+    const double arr = cprev / vecm;
+    us[base + nxl * j] = arr;
+    vecm = b - a * arr;
+    f = (r[base + nxl * j] - a * f) / vecm;
+    r[base + nxl * j] = f;
+    cprev = c;
+  }
+  // back substitution f(j) -= arr(j+1) f(j+1), then u* = u + f
+  double fn = f;
+  for (int j = ny - 2; j >= 0; --j) {
+    const double arr = us[base + nxl * (j + 1)];
+    us[base + nxl * (j + 1)] = u[base + nxl * (j + 1)] + fn;
+    fn = r[base + nxl * j] - arr * fn;
+  }
+  us[base] = u[base] + fn;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static LesPar les_par(const ch3d_ctx* c) {
+  LesPar lp;
+  lp.delta = c->les_delta;
+  lp.dwall = c->les_delta + (c->ny + 2);
+  const double tr[9] = {1, 2, 1, 2, 4, 2, 1, 2, 1}, si[9] = {1, 4, 1, 4, 16, 4, 1, 4, 1};
+  for (int q = 0; q < 9; ++q) lp.Fc[q] = c->cfg.FilterType == 1 ? si[q] / 36.0 : tr[q] / 16.0;
+  lp.Cs = c->cfg.Cs;
+  lp.model = c->cfg.LES_type == CH3D_LES_MLP ? CH3D_LES_SMAG_VD : c->cfg.LES_type;
+  return lp;
+}
+
+static dim3 les_grid(const ch3d_ctx* c) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz); }
+
+cudaError_t launch_sgs_nut(ch3d_ctx* c) {
+  double** f = (double**)c->f;
+  const Geo<double> g = make_geo<double>(c);
+  const LesPar lp = les_par(c);
+  if (lp.model == CH3D_LES_SMAG_VD) {
+    const double d1 = c->yc[1] - c->yp[1], dN = c->yp[c->ny + 1] - c->yc[c->ny];
+    k_wall_utau<<<1, 1024, 0, c->stream>>>(g, f[0], d1, dN, c->sc);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  k_sgs_nut<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, f[0], f[1], f[2], f[11], c->sc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rhs_les(ch3d_ctx* c) {
+  double** f = (double**)c->f;
+  k_rhs_les<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(make_geo<double>(c), c->m64, f[0], f[1], f[2], f[3], f[11],
+                                                         f[4], f[5], f[6], f[7], f[8], f[9], c->sc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uhat_les(ch3d_ctx* c) {
+  double** f = (double**)c->f;
+  HelmCoef hc;
+  const double* M = c->met64;
+  const int L = c->ny + 3;
+  hc.ap2p = M + 7 * L; hc.ac2p = M + 8 * L; hc.am2p = M + 9 * L;
+  hc.ap2cForCN = M + 14 * L; hc.am2cForCN = M + 15 * L;
+  const int ncol = c->nx * c->nz;
+  k_uhat_les<<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(make_geo<double>(c), hc, f[11], f[0], f[1], f[2], f[7],
+                                                                 f[8], f[9], f[12], f[13], f[14], c->sc);
+  return cudaGetLastError();
+}
+
+}  // namespace ch3d

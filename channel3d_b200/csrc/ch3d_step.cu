@@ -1024,7 +1024,8 @@ __global__ void __launch_bounds__(256) k_xifft(Geo<T> g, const typename CplxOf<T
 template <class T>
 __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* uxs, const T* uys, const T* uzs,
                                               T* ux, T* uy, T* uz, T* __restrict__ pr, const T* __restrict__ phi,
-                                              double* __restrict__ part, int mode, const DevScalars* __restrict__ sc) {
+                                              double* __restrict__ part, int mode, const DevScalars* __restrict__ sc,
+                                              const T* __restrict__ nut) {
   __shared__ double red[256];
   if (sc->status) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1059,7 +1060,19 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
     ux[idx] = uxn;
     uy[idx] = uyn;
     uz[idx] = uzn;
-    if (mode == 0 && g.implicit == 2) {
+    if (mode == 0 && g.les) {  // PressureUpdate_PIMP_LES (src/CFD_2nd/m_TSchemePIMP_inc.f90:878-904)
+      const T phip_y = phi[i + (long long)nx * ((j < ny - 1 ? j + 1 : ny - 1) + (long long)ny * k)];
+      const T nc = nut[idx];
+      const T njp = j < ny - 1 ? nut[idx + nx] : (g.bc.hi == -1 ? (T)2 * g.xnu - nc : nc);
+      const T njm = j > 0 ? nut[idx - nx] : (g.bc.lo == -1 ? (T)2 * g.xnu - nc : nc);
+      const T pmBetaT = (T)sc->pmBetaT;
+      const T metr1 = m.rdyp[jc] * m.rdyc[jc], metr2 = m.rdyp[jc] * m.rdyc[jc + 1];
+      const T visd = (T)0.5 * (njp + nc), visc = (T)0.5 * (nc + njm);
+      const T pmBetap = -pmBetaT * metr2 * visd;
+      const T pmBetam = -pmBetaT * metr1 * visc;
+      const T pmBetac = -(pmBetap + pmBetam) + (T)1;
+      pr[idx] = pr[idx] + pmBetap * phip_y + pmBetac * phic + pmBetam * phim_y;
+    } else if (mode == 0 && g.implicit == 2) {
       pr[idx] = pr[idx] + phic;  // PressureUpdate_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386)
     } else if (mode == 0) {
       const T phip_y = phi[i + (long long)nx * ((j < ny - 1 ? j + 1 : ny - 1) + (long long)ny * k)];
@@ -1427,7 +1440,7 @@ template <class T> static cudaError_t proj_t(ch3d_ctx* c, int mode) {
   T** f = (T**)c->f;
   T* in[3] = {mode == 1 ? f[0] : f[12], mode == 1 ? f[1] : f[13], mode == 1 ? f[2] : f[14]};
   k_proj<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1], in[2], f[0],
-                                                          f[1], f[2], f[3], f[10], c->part, mode, c->sc);
+                                                          f[1], f[2], f[3], f[10], c->part, mode, c->sc, f[11]);
   return cudaGetLastError();
 }
 cudaError_t launch_proj(ch3d_ctx* c, int mode) { return c->fp32 ? proj_t<float>(c, mode) : proj_t<double>(c, mode); }

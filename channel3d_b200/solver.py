@@ -14,7 +14,7 @@ from .config import mesh_y
 
 class ChannelSolver:
     # ch3d_get_array ids (include/ch3d.h)
-    UX, UY, UZ, P, HISTX, HISTY, HISTZ, RHSX, RHSY, PRPHI, RHSZ = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 11
+    UX, UY, UZ, P, HISTX, HISTY, HISTZ, RHSX, RHSY, PRPHI, NUT, RHSZ = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
 
     def __init__(self, cfg, yp=None):
         self.lib = _lib.load_library()
@@ -101,6 +101,11 @@ class ChannelSolver:
         v = ctypes.c_longlong()
         _lib.check(self.lib.ch3d_memory_bytes(self.ctx, ctypes.byref(v)), self.lib)
         return v.value
+
+    def sgs_viscosity(self):
+        """LES: nut from the current velocity (Clc_SGS_Vis); returns it (interior)."""
+        _lib.check(self.lib.ch3d_sgs_viscosity(self.ctx))
+        return self.get_array(self.NUT)
 
     def stats_accumulate(self):
         _lib.check(self.lib.ch3d_stats_accumulate(self.ctx), self.lib)

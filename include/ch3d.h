@@ -157,7 +157,9 @@ CH3D_API int ch3d_stage(ch3d_ctx* ctx, int stage, int ns);
 
 /* Internal arrays for inspection, interior layout: 0 ux, 1 uy, 2 uz,
    3 pressure, 4 HistXOld, 5 HistYOld, 6 HistZOld, 7 RhsX, 8 RhsY,
-   9 prphi (the pressure correction of the last clcPPE), 11 RhsZ. */
+   9 prphi (the pressure correction of the last clcPPE), 10 nut (LES: the
+   total viscosity of Clc_SGS_Vis, xnu included), 11 RhsZ, 12..14 the
+   velocity after the Helmholtz solves (u*). */
 CH3D_API int ch3d_get_array(ch3d_ctx* ctx, int which, double* host);
 CH3D_API int ch3d_set_array(ch3d_ctx* ctx, int which, const double* host);
 
@@ -178,6 +180,16 @@ CH3D_API int ch3d_set_dt(ch3d_ctx* ctx, double dt);
 CH3D_API int ch3d_stats_accumulate(ch3d_ctx* ctx);
 CH3D_API int ch3d_stats_fetch(ch3d_ctx* ctx, double* sumstat, int* nfstime,
                      double* prgradsum, int reset);
+
+/* LES: computes nut from the current velocity as the step does once per
+   step, Clc_SGS_Vis (src/CFD_2nd/m_LESModels.f90:47-62) followed by the wall
+   and periodic ghost rules of SetBC_and_UpdateHalo_SGS (:375-428).
+   CH3D_LES_WALE and CH3D_LES_MTS follow Clc_SGS_WALE / Clc_SGS_MTS;
+   CH3D_LES_SMAG_VD (no counterpart in the reference, whose Smagorinsky
+   branch is empty) is nut = xnu + (Cs D Delta)^2 |S| with the van Driest
+   damping D = 1 - exp(-y+/26), y+ from the x-z mean wall shear of the first
+   cells. */
+CH3D_API int ch3d_sgs_viscosity(ch3d_ctx* ctx);
 
 /* Device bytes held by the context. */
 CH3D_API int ch3d_memory_bytes(ch3d_ctx* ctx, long long* bytes);

@@ -1874,6 +1874,15 @@ void* orc_create(const orc_params* p) {
 
 void orc_destroy(void* h) { delete (Oracle*)h; }
 
+// LES eddy viscosity of the current state (Clc_SGS_Vis); returns u_tau of the
+// Smagorinsky / van Driest model (0 for the others)
+double orc_sgs(void* h) {
+  Oracle* o = (Oracle*)h;
+  o->utau_last = 0;
+  o->Clc_SGS_Vis();
+  return o->utau_last;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -86,6 +86,8 @@ def lib():
         L.orc_stats_get.restype = ctypes.c_int
         L.orc_stats_get.argtypes = [ctypes.c_void_p, _DP, _DP]
         L.orc_num_threads.restype = ctypes.c_int
+        L.orc_sgs.restype = ctypes.c_double
+        L.orc_sgs.argtypes = [ctypes.c_void_p]
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
@@ -206,6 +208,11 @@ class Oracle:
         phi = np.empty(self.shape)
         self.L.orc_poisson(self.h, _p(src), _p(phi))
         return phi
+
+    def sgs(self):
+        """Clc_SGS_Vis on the current state: nut (interior) and u_tau."""
+        ut = self.L.orc_sgs(self.h)
+        return self.get_interior(self.NUT), ut
 
     def stats_accumulate(self):
         self.L.orc_stats_accumulate(self.h)

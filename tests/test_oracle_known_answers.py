@@ -279,3 +279,63 @@ def test_fimp_step_is_divergence_free_and_laminar_steady(built):
     assert np.abs(s["ux"] - s["ux"][:1, :, :1]).max() < 1e-13
     # the bulk controller drives <u> to ubulk = 1 from the discretised profile
     assert abs(d["uxm"] - 1.0) < 0.01 * abs(d0["uxm"] - 1.0)
+
+
+def _cfg_les(model, nx=24, ny=16, nz=12):
+    from channel3d_b200 import workloads
+    cfg, _ = workloads.get("channel48_les")
+    return cfg.copy(nxc=nx, nyc=ny, nzc=nz, nycSection=[ny // 2, ny - ny // 2], LES_type=model, Cs=0.1)
+
+
+def test_sgs_models_on_laminar_shear(built):
+    """Properties of the eddy-viscosity models on a laminar profile u(y):
+    WALE (Nicoud & Ducros 1999) vanishes in pure shear, the mixed-time-scale
+    model's test-filtered energy is zero for an x,z-uniform field, and the
+    Smagorinsky / van Driest model equals xnu + (Cs D Delta)^2 |du/dy| with
+    the staggered |S| of ClcVelStrainRate."""
+    from channel3d_b200 import initfield
+    from oracle import oracle as O
+    for model in (2, 3):
+        cfg = _cfg_les(model)
+        o = O.Oracle(cfg)
+        ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0], amplitude=0.0)
+        o.set_state(ux, uy, uz, p)
+        nut, _ = o.sgs()
+        assert np.abs(nut - cfg.xnu).max() < 1e-15, model
+    cfg = _cfg_les(10)
+    o = O.Oracle(cfg)
+    yp = o.mesh()[0]
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp, amplitude=0.0)
+    o.set_state(ux, uy, uz, p)
+    nut, utau = o.sgs()
+    ny = cfg.nyc
+    u = ux[0, :, 0]
+    yc = 0.5 * (yp[1:] + yp[:-1])
+    dyp = yp[1:] - yp[:-1]
+    ug = np.concatenate([[-u[0]], u, [-u[-1]]])          # no-slip ghosts 2*0 - u
+    ycg = np.concatenate([[2 * yp[0] - yc[0]], yc, [2 * yp[-1] - yc[-1]]])
+    rdyc = 1.0 / np.diff(ycg)                               # rdyc(jc), jc = 1..nyp
+    rdyc[0] = 1.0 / dyp[0]
+    rdyc[-1] = 1.0 / dyp[-1]
+    st4 = 0.125 * (2 * ug[2:] * rdyc[1:] + 2 * ug[1:-1] * (rdyc[:-1] - rdyc[1:]) - 2 * ug[:-2] * rdyc[:-1])
+    S = np.abs(2 * st4)
+    tw = cfg.xnu * 0.5 * (abs(u[0]) / (yc[0] - yp[0]) + abs(u[-1]) / (yp[-1] - yc[-1]))
+    assert abs(utau - np.sqrt(tw)) < 1e-14
+    dw = np.minimum(yc - yp[0], yp[-1] - yc)
+    D = 1 - np.exp(-(dw * utau / cfg.xnu) / 26.0)
+    delta = (dyp * (cfg.xlx / cfg.nxc) * (cfg.zlz / cfg.nzc)) ** (1.0 / 3.0)
+    ref = cfg.xnu + (cfg.Cs * D * delta) ** 2 * S
+    assert np.abs(nut[0, :, 0] - ref).max() < 1e-12 * ref.max()
+    assert np.abs(nut - nut[:1, :, :1]).max() < 1e-18
+
+
+def test_les_step_is_divergence_free(built):
+    from channel3d_b200 import initfield
+    from oracle import oracle as O
+    for model in (2, 3, 10):
+        cfg = _cfg_les(model)
+        o = O.Oracle(cfg)
+        ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0])
+        o.set_state(ux, uy, uz, p)
+        d = o.step(3)
+        assert d["divmax2"] < 1e-13 and d["rc"] == 0, model

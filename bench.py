@@ -27,13 +27,25 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# algorithmic HBM bytes per cell per step, 2nd-order partially implicit path
-# (full-field arrays that must cross HBM once per substep x 3 substeps x word size)
-ALG_ARRAYS_PER_SUBSTEP = 32
-# per-launch algorithmic arrays of each kernel group (reads + writes), see DESIGN.md
-GROUP_ARRAYS = {0: 13, 1: 9, 2: 4, 3: 6, 4: 2, 5: 9}
-GROUP_NAMES = {0: "rhs_pimp", 1: "uhat_pimp", 2: "prsrc_xfft", 3: "zfft_ysolve_izfft", 4: "xifft", 5: "proj",
-               6: "scalar"}
+# Algorithmic HBM traffic: full-field arrays that must cross HBM once per
+# substep (reads + writes) under the minimal-fusion plan of the data
+# dependencies, x 3 substeps x word size.  2nd-order partially implicit and
+# 4th order: 32 arrays per substep; fully implicit (ADI): 47.
+ALG_ARRAYS_PER_SUBSTEP = {"pimp": 32, "order4": 32, "fimp": 47, "les": 32}
+# per-launch algorithmic arrays of each kernel group of ch3d_kernel_times
+# (0: RHS + y Helmholtz solve, fused: read u v w p Hist x3, write Hist x3 u* x3;
+#  2: divergence + forward x FFT: read u* x3, write the half spectrum;
+#  3: z FFT, y Poisson solve, inverse z FFT: 3 x (read + write) of the spectrum;
+#  4: inverse x FFT: read spectrum, write phi;
+#  5: projection + pressure update: read phi u* x3 p, write u x3 p)
+GROUP_ARRAYS = {0: 13, 2: 4, 3: 6, 4: 2, 5: 9}
+GROUP_NAMES = {0: "k_rhs_uhat", 1: "y_solves", 2: "k_prsrc_xfft", 3: "k_zfft+k_ysolve2+k_zfft", 4: "k_xifft",
+               5: "k_proj", 6: "scalar"}
+# CUDA kernels launched per step by the step graph (ch3d_api.cu record_step):
+# step_begin 1 + per substep (reduce_partials + substep_setup 2, helm_factors 1,
+# rhs+uhat 1, prsrc_xfft 1, zfft + ysolve2 (+ FP64 low modes in mixed) + zfft 3|4,
+# xifft 1, proj 1) + diag_reset + diag 2 + reduce_partials + step_end 2
+LAUNCHES_PER_SUBSTEP = {"fp64": 10, "mixed": 11}
 
 
 def parse():
@@ -47,6 +59,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--cpu-nz", type=int, default=48, help="z planes of the CPU-baseline sample")
+    ap.add_argument("--cpu-nz-ref", type=int, default=12, help="z planes of the --impl reference sample")
     return ap.parse_args()
 
 
@@ -141,8 +155,17 @@ def allmax(ws, v):
     return float(t.item())
 
 
+def cpu_sample_cfg(cfg, nz_sample):
+    """A bounded sample of a workload for the CPU timing: the same x-y grid,
+    metrics and parameters on a z-slab of nz_sample planes (the step's cost
+    per grid point does not depend on nz beyond the z FFT's log factor)."""
+    if nz_sample >= cfg.nzc:
+        return cfg
+    return cfg.copy(nzc=nz_sample, zlz=cfg.zlz * nz_sample / cfg.nzc)
+
+
 def cpu_reference(cfg, args, ws, rank, steps=1):
-    """Times the CPU restatement (oracle/) on `steps` full steps of the workload."""
+    """Times the CPU restatement (oracle/) on `steps` full steps of cfg."""
     from oracle import oracle as O
     from channel3d_b200 import initfield
     if args.cpu_threads:
@@ -161,28 +184,77 @@ def cpu_reference(cfg, args, ws, rank, steps=1):
     return cfg.npoints * steps / dt / 1e9, threads, dt
 
 
+def solver_name(cfg):
+    if cfg.LES_type:
+        return "2nd-order PIMP RK3 LES (LES_type %d)" % cfg.LES_type
+    if cfg.order == 4:
+        return "4th-order RK3 (y Crank-Nicolson)"
+    return "2nd-order %s RK3" % ("FIMP (ADI)" if cfg.IsImplicit == 2 else "PIMP")
+
+
+def scheme_key(cfg):
+    if cfg.LES_type:
+        return "les"
+    if cfg.order == 4:
+        return "order4"
+    return "fimp" if cfg.IsImplicit == 2 else "pimp"
+
+
 def run_reference(args, ws, rank):
+    """The reference's algorithm on the host cores: the C++ restatement of the
+    step (oracle/, OpenMP over all host threads), each timed step one RK3 step
+    of a z-slab sample of the workload."""
     from channel3d_b200 import workloads
-    cfg, _ = workloads.get(args.workload, precision=args.precision)
+    cfg, _ = workloads.get(args.workload, precision="fp64")
     if rank != 0:
         return
-    steps = max(1, args.steps // max(1, args.steps))  # one full step per timed sample
-    vals = []
-    for _ in range(max(1, min(args.steps, 2))):
-        v, thr, dt = cpu_reference(cfg, args, ws, rank, steps=steps)
-        vals.append(v)
-    v = float(np.median(vals))
+    sample = cpu_sample_cfg(cfg, args.cpu_nz_ref)
+    from oracle import oracle as O
+    from channel3d_b200 import initfield
+    if args.cpu_threads:
+        O.set_threads(args.cpu_threads)
+    thr = O.num_threads()
+    o = O.Oracle(sample)
+    ux, uy, uz, p = initfield.laminar_noise(sample, yp=o.mesh()[0])
+    o.set_state(ux, uy, uz, p)
+    del ux, uy, uz, p
+    o.step(max(1, args.warmup))
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    v = sample.npoints * args.steps / dt / 1e9
     line = {
         "impl": "reference", "metric": "Gpt-steps/s", "value": v, "unit": "Gpt-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": cfg.npoints / (v * 1e9) * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": "2nd-order PIMP RK3"},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded laminar + 10% uniform noise)",
+        "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": solver_name(cfg),
+                   "precision": "fp64"},
         "cpu_baseline": {"value": v, "unit": "Gpt-steps/s", "cores": thr, "kind": "port",
-                         "sample": "%d full RK3 step(s) of the %s workload per timed sample, after one untimed step; "
-                                   "C++ restatement of the reference (oracle/), OpenMP" % (steps, args.workload)},
+                         "sample": "%d RK3 steps (after %d untimed) of a %dx%dx%d z-slab of the %s workload "
+                                   "(%.1f s); C++ restatement of the reference step (oracle/), OpenMP, %d threads"
+                                   % (args.steps, max(1, args.warmup), sample.nxc, sample.nyc, sample.nzc,
+                                      args.workload, dt, thr)},
         "e2e": {"value": v, "unit": "Gpt-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def profile_traffic(kernel, precision):
+    """DRAM bytes per grid point per launch of `kernel`, from the committed ncu
+    summaries (a line 'bench-traffic: <kernel> <precision> <bytes per point>')."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None, None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(d, fn)):
+            t = line.strip().split()
+            if len(t) == 4 and t[0] == "bench-traffic:" and t[1] == kernel and t[2] == precision:
+                return float(t[3]), fn
+    return None, None
 
 
 def run_ours(args, ws, rank, local):
@@ -212,19 +284,33 @@ def run_ours(args, ws, rank, local):
     ms_per_step = ms_max / args.steps
     value = ws * cfg.npoints * args.steps / (ms_max * 1e-3) / 1e9
 
-    # per-kernel-group device times (one more instrumented step)
+    # per-kernel-group device times: CUDA events around each group on the
+    # context's stream over two more (ungraphed) steps
     kt = s.kernel_times(2)
     word = 4 if args.precision == "mixed" else 8
+    key = scheme_key(cfg)
     per_group = {}
     for g, arrs in GROUP_ARRAYS.items():
         b = arrs * cfg.npoints * word
         per_group[GROUP_NAMES[g]] = {"ms": kt[g], "alg_bytes": b, "GBps": b / (kt[g] * 1e-3) / 1e9 if kt[g] > 0 else None}
+    if kt[1] > 0:
+        per_group[GROUP_NAMES[1]] = {"ms": kt[1]}
+    per_group[GROUP_NAMES[6]] = {"ms": kt[6]}
     dom = max(GROUP_ARRAYS, key=lambda g: kt[g])
     peak, peak_kind = load_peaks()
     dom_b = GROUP_ARRAYS[dom] * cfg.npoints * word
     achieved = dom_b / (kt[dom] * 1e-3) / 1e9
-    step_alg = ALG_ARRAYS_PER_SUBSTEP * 3 * word * cfg.npoints
+    tpp, tsrc = profile_traffic(GROUP_NAMES[dom], args.precision)
+    traffic = tpp * cfg.npoints if tpp is not None else None
+    step_alg = ALG_ARRAYS_PER_SUBSTEP[key] * 3 * word * cfg.npoints
     step_achieved = step_alg / (ms_per_step * 1e-3) / 1e9
+    launches = 1 + 3 * LAUNCHES_PER_SUBSTEP[args.precision] + 4
+    if key == "order4":
+        launches += 3 * 2        # mean viscous stress partials, interpolated velocities
+    elif key == "fimp":
+        launches += 3 * 4        # RHS and y solve unfused, x/z periodic sweeps + their factors
+    elif key == "les":
+        launches += 3 * 1 + 1 + (1 if cfg.LES_type == 10 else 0)  # RHS/y solve unfused, eddy viscosity (+ wall shear)
 
     # end-to-end through the public API: pinned host arrays -> upload -> K steps -> download
     e2e = None
@@ -254,10 +340,12 @@ def run_ours(args, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
-            v, thr, dt = cpu_reference(cfg.copy(precision="fp64"), args, ws, rank, steps=1)
+            sample = cpu_sample_cfg(cfg.copy(precision="fp64", device=0), args.cpu_nz)
+            v, thr, dt = cpu_reference(sample, args, ws, rank, steps=1)
             cpu = {"value": v, "unit": "Gpt-steps/s", "cores": thr, "kind": "port",
-                   "sample": "1 full RK3 step of %s (%.1f s) after one untimed step; C++ restatement "
-                             "(oracle/), OpenMP" % (args.workload, dt)}
+                   "sample": "1 RK3 step (after 1 untimed) of a %dx%dx%d z-slab of %s (%.1f s); C++ restatement "
+                             "of the reference step (oracle/), OpenMP, %d threads"
+                             % (sample.nxc, sample.nyc, sample.nzc, args.workload, dt, thr)}
         except Exception as ex:  # keep the GPU line even if host memory is short
             cpu = {"value": None, "unit": "Gpt-steps/s", "cores": None, "kind": "port", "sample": "failed: %s" % ex}
 
@@ -267,14 +355,18 @@ def run_ours(args, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded laminar + 10% uniform noise, projected divergence-free)",
-            "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": "2nd-order PIMP RK3",
+            "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": solver_name(cfg),
                        "precision": args.precision, "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (%.1f GB of fields)" % (s.memory_bytes() / 1e9)},
             "steps_per_s": 1e3 / ms_per_step,
-            "gpu_launches": int(args.steps * 35),
+            "gpu_launches": int(args.steps * launches),
             "roofline": {"bound": "hbm", "kernel": GROUP_NAMES[dom], "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
-            "step_roofline": {"alg_bytes_per_cell_step": ALG_ARRAYS_PER_SUBSTEP * 3 * word,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind + " (hbm_gbs, burst copy)",
+                         "alg_bytes_per_launch": dom_b,
+                         "traffic_source": ("profiles/%s: ncu dram__bytes_read.sum + dram__bytes_write.sum per grid "
+                                            "point of a smaller capture, scaled to this launch" % tsrc) if tsrc else None},
+            "step_roofline": {"alg_bytes_per_cell_step": ALG_ARRAYS_PER_SUBSTEP[key] * 3 * word,
                               "achieved": step_achieved, "peak": peak, "frac": step_achieved / peak},
             "kernels": per_group,
             "memory_bytes": s.memory_bytes(),

@@ -96,6 +96,15 @@ SIGNATURES = {
     "ch3d_memory_bytes": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong)]),
     "ch3d_last_step_ms": (ctypes.c_int, [_VP, _DP]),
     "ch3d_kernel_times": (ctypes.c_int, [_VP, ctypes.c_int, _DP, ctypes.c_int]),
+    "ch3d_mlp_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p]),
+    "ch3d_mlp_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int]),
+    "ch3d_mlp_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "ch3d_mlp_adam": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                     ctypes.c_void_p]),
     "ch3d_poisson_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, _DP, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.c_void_p]),

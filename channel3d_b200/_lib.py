@@ -92,6 +92,9 @@ SIGNATURES = {
     "ch3d_set_dt": (ctypes.c_int, [_VP, ctypes.c_double]),
     "ch3d_stats_accumulate": (ctypes.c_int, [_VP]),
     "ch3d_sgs_viscosity": (ctypes.c_int, [_VP]),
+    "ch3d_sgs_mlp_set": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "ch3d_sgs_training_samples": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     "ch3d_stats_fetch": (ctypes.c_int, [_VP, _DP, _IP, _DP, ctypes.c_int]),
     "ch3d_memory_bytes": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong)]),
     "ch3d_last_step_ms": (ctypes.c_int, [_VP, _DP]),

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include "../../include/ch3d_mlp.h"
 #include "ch3d_ctx.h"
 
 using namespace ch3d;
@@ -221,7 +222,8 @@ int check_config(const ch3d_config* g) {
     if (g->BcOption[s] != -1 && g->BcOption[s] != -2)
       return fail(CH3D_ERR_UNSUPPORTED, "y boundaries must be no-slip (-1) or free-slip (-2)");
   if (g->LES_type != 0) {
-    if (g->LES_type != CH3D_LES_WALE && g->LES_type != CH3D_LES_MTS && g->LES_type != CH3D_LES_SMAG_VD)
+    if (g->LES_type != CH3D_LES_WALE && g->LES_type != CH3D_LES_MTS && g->LES_type != CH3D_LES_SMAG_VD &&
+        g->LES_type != CH3D_LES_MLP)
       return fail(CH3D_ERR_UNSUPPORTED, "LES_type=%d not built", g->LES_type);
     if (g->order != 2 || g->IsImplicit != 1 || g->precision != CH3D_PREC_FP64)
       return fail(CH3D_ERR_UNSUPPORTED, "LES is built for the 2nd-order partially implicit FP64 step (the reference "
@@ -252,6 +254,18 @@ int alloc_fields(ch3d_ctx* c) {
     for (int j = 1; j <= c->ny; ++j) h[c->ny + 2 + j] = std::min(c->yc[j] - c->yp[1], c->yp[c->ny + 1] - c->yc[j]);
     CU(cudaMalloc(&c->les_delta, h.size() * sizeof(double)));
     CU(cudaMemcpy(c->les_delta, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (c->cfg.LES_type == CH3D_LES_MLP) {
+    CU(cudaMalloc(&c->mlp_params, CH3D_MLP_NPARAM * sizeof(float)));
+    CU(cudaMalloc(&c->mlp_x, (size_t)c->N * 10 * sizeof(float)));
+    CU(cudaMalloc(&c->mlp_y, (size_t)c->N * 6 * sizeof(float)));
+    CU(cudaMalloc(&c->mlp_fb, (size_t)c->N));
+    CU(cudaMalloc(&c->mlp_status, sizeof(int)));
+    CU(cudaMemsetAsync(c->mlp_status, 0, sizeof(int), c->stream));
+    CU(cudaMalloc(&c->sgs_tau, (size_t)c->N * 6 * sizeof(double)));
+    CU(cudaMalloc(&c->sgs_f, (size_t)c->N * 3 * sizeof(double)));
+    CU(cudaMemsetAsync(c->sgs_f, 0, (size_t)c->N * 3 * sizeof(double), c->stream));
+    c->bytes += (long long)c->N * (16 * 4 + 1 + 9 * 8);
   }
   if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
     const size_t nb = ptri_factor_doubles(c->nx, c->nz) * sizeof(double);
@@ -537,13 +551,7 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
   if (c->fp32) c->m32 = metrics_ptrs<float>((const float*)c->met, c->ny);
   else c->m32 = Metrics<float>();
   if (!c->fp32) c->m64 = metrics_ptrs<double>((const double*)c->met, c->ny);
-  // Poisson y solve: smallest power-of-two chunk count with at most CH3D_LMAX rows per chunk
-  c->P = 2;
-  while ((c->ny + c->P - 1) / c->P > CH3D_LMAX) c->P *= 2;
-  while (c->P > 2 && c->ny < 2 * c->P) c->P >>= 1;
-  c->TSy = 256 / c->P;
-  if (c->TSy > 8) c->TSy = 8;
-  if (c->TSy < 1) c->TSy = 1;
+  c->TSy = 8;  // kx extent of the FP64 low modes of the mixed path
   c->Pv = 32;
   while (c->Pv > 1 && c->ny < 2 * c->Pv) c->Pv >>= 1;
   {
@@ -551,25 +559,22 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     if (cudaMalloc(&c->hfac, nf * sizeof(double)) != cudaSuccess) return cleanup(fail(CH3D_ERR_NOMEM, "hfac"));
   }
   {
-    // Poisson y-solve factors per (kx, |kz|), computed once
-    if ((c->ny + c->P - 1) / c->P > CH3D_LMAX) return cleanup(fail(CH3D_ERR_UNSUPPORTED, "nyc too large for the y solve"));
+    // Poisson y-solve (Thomas) factors per (kx, |kz|), computed once
     const size_t nrow = (size_t)(c->nz / 2 + 1) * c->ny * c->nxh;
-    const size_t nif = (size_t)(c->nz / 2 + 1) * (c->P > 1 ? c->P - 1 : 1) * 6 * c->nxh;
     const size_t fw = c->fp32 ? sizeof(float) : sizeof(double);
-    if (cudaMalloc(&c->yRM, nrow * fw) != cudaSuccess || cudaMalloc(&c->yCP, nrow * fw) != cudaSuccess ||
-        cudaMalloc(&c->yIF, nif * fw) != cudaSuccess)
+    if (cudaMalloc(&c->yRM, nrow * fw) != cudaSuccess || cudaMalloc(&c->yCP, nrow * fw) != cudaSuccess)
       return cleanup(fail(CH3D_ERR_NOMEM, "Poisson factors"));
-    c->bytes += (long long)(2 * nrow + nif) * fw;
+    c->bytes += (long long)(2 * nrow) * fw;
     if (c->fp32) {
       // low modes kept in FP64: kx < TSy, |kz| <= KL (KL < nz/2 so the two kz ranges are disjoint)
       c->KL = 8;
       if (c->KL > c->nz / 2 - 1) c->KL = c->nz / 2 - 1;
       if (c->KL < 0) c->KL = 0;
       const size_t lr = (size_t)(c->KL + 1) * c->ny * c->TSy;
-      const size_t li = (size_t)(c->KL + 1) * (c->P > 1 ? c->P - 1 : 1) * 6 * c->TSy;
+      const size_t ls = (size_t)(2 * c->KL + 1) * c->TSy * c->ny * 2;  // FP64 complex sweep scratch
       if (cudaMalloc(&c->yRM64, lr * sizeof(double)) != cudaSuccess ||
           cudaMalloc(&c->yCP64, lr * sizeof(double)) != cudaSuccess ||
-          cudaMalloc(&c->yIF64, li * sizeof(double)) != cudaSuccess)
+          cudaMalloc(&c->ylow, ls * sizeof(double)) != cudaSuccess)
         return cleanup(fail(CH3D_ERR_NOMEM, "Poisson low-mode factors"));
     }
     e = launch_ysolve_factors(c);
@@ -610,7 +615,9 @@ int ch3d_destroy(ch3d_ctx* c) {
   for (int q = 0; q < 6; ++q) if (c->ih[q]) cudaFree(c->ih[q]);
   if (c->pfac) cudaFree(c->pfac);
   if (c->les_delta) cudaFree(c->les_delta);
-  void* bufs[] = {c->hfac, c->yRM, c->yCP, c->yIF, c->yRM64, c->yCP64, c->yIF64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  void* mbufs[] = {c->mlp_params, c->mlp_x, c->mlp_y, c->mlp_fb, c->mlp_status, c->sgs_tau, c->sgs_f};
+  for (void* b : mbufs) if (b) cudaFree(b);
+  void* bufs[] = {c->hfac, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -660,9 +667,19 @@ int ch3d_download_state(ch3d_ctx* c, int layout, double* ux, double* uy, double*
   return CH3D_OK;
 }
 
+static int mlp_check(ch3d_ctx* c) {
+  if (c->cfg.LES_type != CH3D_LES_MLP) return CH3D_OK;
+  if (!c->mlp_ready) return fail(CH3D_ERR_INVALID, "learned closure: call ch3d_sgs_mlp_set before stepping");
+  int st = 0;
+  CU(cudaMemcpy(&st, c->mlp_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) return fail(CH3D_ERR_CUDA, "learned closure: tensor-core kernel timed out waiting for its MMAs");
+  return CH3D_OK;
+}
+
 int ch3d_step(ch3d_ctx* c, int nsteps, ch3d_step_info* info) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
   if (nsteps < 0) return fail(CH3D_ERR_INVALID, "nsteps < 0");
+  if (int rc = mlp_check(c)) return rc;
   CU(cudaSetDevice(c->device));
   if (!c->scalars_ready) {
     int rc = init_scalars(c);
@@ -692,11 +709,13 @@ int ch3d_step(ch3d_ctx* c, int nsteps, ch3d_step_info* info) {
   float ms = 0;
   CU(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
+  if (int rc = mlp_check(c)) return rc;
   return fetch_info(c, info);
 }
 
 int ch3d_stage(ch3d_ctx* c, int stage, int ns) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (int rc = mlp_check(c)) return rc;
   if (ns < 1 || ns > c->iadvance) return fail(CH3D_ERR_INVALID, "ns out of range");
   CU(cudaSetDevice(c->device));
   if (!c->scalars_ready) {
@@ -746,6 +765,13 @@ static int array_slot(int which) {
 
 int ch3d_get_array(ch3d_ctx* c, int which, double* host) {
   if (!c || !host) return fail(CH3D_ERR_INVALID, "NULL argument");
+  if (which >= 15 && which <= 20) {  // learned closure: SGS stress components at the cell centres
+    if (!c->sgs_tau) return fail(CH3D_ERR_INVALID, "array %d exists for LES_type CH3D_LES_MLP only", which);
+    CU(cudaSetDevice(c->device));
+    CU(cudaMemcpy(host, c->sgs_tau + (size_t)(which - 15) * c->N, (size_t)c->N * sizeof(double),
+                  cudaMemcpyDeviceToHost));
+    return CH3D_OK;
+  }
   int q = array_slot(which);
   if (q < 0) return fail(CH3D_ERR_INVALID, "bad array id %d", which);
   CU(cudaSetDevice(c->device));
@@ -843,9 +869,39 @@ int ch3d_stats_fetch(ch3d_ctx* c, double* sumstat, int* nfstime, double* prgrads
   return CH3D_OK;
 }
 
+int ch3d_sgs_mlp_set(ch3d_ctx* c, const float* params, const float* norm) {
+  if (!c || !params || !norm) return fail(CH3D_ERR_INVALID, "NULL argument");
+  if (c->cfg.LES_type != CH3D_LES_MLP) return fail(CH3D_ERR_INVALID, "LES_type is not CH3D_LES_MLP");
+  for (int q = 0; q < 10; ++q)
+    if (!(norm[10 + q] > 0)) return fail(CH3D_ERR_INVALID, "input standard deviation %d not positive", q);
+  for (int q = 0; q < 6; ++q)
+    if (!(norm[46 + q] > 0)) return fail(CH3D_ERR_INVALID, "output standard deviation %d not positive", q);
+  CU(cudaSetDevice(c->device));
+  CU(cudaMemcpy(c->mlp_params, params, CH3D_MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  std::memcpy(c->mlp_norm, norm, sizeof(c->mlp_norm));
+  c->mlp_ready = true;
+  if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }  // the norm is a kernel argument
+  if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+  return CH3D_OK;
+}
+
+int ch3d_sgs_training_samples(ch3d_ctx* c, int fx, int fy, int fz, float* X, float* T, long long* nbox) {
+  if (!c || !X || !T || !nbox) return fail(CH3D_ERR_INVALID, "NULL argument");
+  if (c->fp32) return fail(CH3D_ERR_UNSUPPORTED, "training samples are taken from an FP64 field");
+  if (fx < 1 || fy < 1 || fz < 1 || c->nx % fx || c->ny % fy || c->nz % fz)
+    return fail(CH3D_ERR_INVALID, "box %d x %d x %d does not tile the grid", fx, fy, fz);
+  CU(cudaSetDevice(c->device));
+  if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
+  CU(launch_sgs_samples(c, fx, fy, fz, X, T));
+  CU(cudaStreamSynchronize(c->stream));
+  *nbox = (long long)(c->nx / fx) * (c->ny / fy) * (c->nz / fz);
+  return CH3D_OK;
+}
+
 int ch3d_sgs_viscosity(ch3d_ctx* c) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
   if (c->cfg.LES_type == 0) return fail(CH3D_ERR_INVALID, "LES_type is 0");
+  if (int rc = mlp_check(c)) return rc;
   CU(cudaSetDevice(c->device));
   if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
   CU(launch_sgs_nut(c));

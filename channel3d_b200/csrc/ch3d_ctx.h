@@ -8,8 +8,6 @@
 #include "fft.cuh"
 
 #define CH3D_NRED 256
-// maximum rows of one chunk of the partitioned Poisson y solve (register arrays)
-#define CH3D_LMAX 12
 
 struct ch3d_ctx {
   ch3d_config cfg;
@@ -38,15 +36,23 @@ struct ch3d_ctx {
   double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
   double* pfac = nullptr;    // FIMP: periodic x/z sweep factors of the current substep
   double* les_delta = nullptr;  // LES: DeltaCell (ny+2) | wall distance of the cell centres (ny+2)
-  void* yRM = nullptr;       // Poisson y-solve chunk factors per mode (fixed for the run);
+  // learned closure (LES_type CH3D_LES_MLP)
+  float* mlp_params = nullptr;   // CH3D_MLP_NPARAM FP32
+  float mlp_norm[CH3D_SGS_NORM_FLOATS] = {0};
+  bool mlp_ready = false;
+  float* mlp_x = nullptr;        // N x 10 inputs
+  float* mlp_y = nullptr;        // N x 6 outputs
+  unsigned char* mlp_fb = nullptr;  // N fallback flags
+  int* mlp_status = nullptr;
+  double* sgs_tau = nullptr;     // 6 N stresses at the cell centres
+  double* sgs_f = nullptr;       // 3 N stress-divergence forces at the velocity points
+  void* yRM = nullptr;       // Poisson y-solve Thomas factors per mode (fixed for the run);
   void* yCP = nullptr;       // FP64, or FP32 in the mixed path
-  void* yIF = nullptr;       // Poisson interface factors per mode
-  double* yRM64 = nullptr;   // mixed path: FP64 factors of the low modes (kx tile 0, |kz| <= KL)
+  double* yRM64 = nullptr;   // mixed path: FP64 factors of the low modes (kx < TSy, |kz| <= KL)
   double* yCP64 = nullptr;
-  double* yIF64 = nullptr;
+  double* ylow = nullptr;    // mixed path: FP64 forward-sweep scratch of the low modes
   int KL = 8;
-  int P = 16;                // chunks of the partitioned Poisson y solves
-  int TSy = 8;               // Poisson y systems per block
+  int TSy = 8;               // kx extent of the FP64 low modes
   int Pv = 32;               // chunks of the partitioned velocity Helmholtz solves
   void* spec = nullptr;      // complex spectrum (kx,j,kz)
   void* met = nullptr;       // packed metric vectors (precision T)
@@ -113,4 +119,5 @@ size_t ptri_factor_doubles(int nx, int nz);
 cudaError_t launch_sgs_nut(ch3d_ctx* c);               // Clc_SGS_Vis -> nut
 cudaError_t launch_rhs_les(ch3d_ctx* c);               // clcRhsX/Y/Z_PIMP_LES -> RhsX/Y/Z
 cudaError_t launch_uhat_les(ch3d_ctx* c);              // clcU1/2/3Hat_PIMP_LES -> u*
+cudaError_t launch_sgs_samples(ch3d_ctx* c, int fx, int fy, int fz, float* X, float* T);
 }  // namespace ch3d

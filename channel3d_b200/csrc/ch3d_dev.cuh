@@ -137,14 +137,14 @@ __host__ __device__ inline int helm_set_stride(int ny, int P) { return 5 * ny + 
 
 // Interface (reduced) block-tridiagonal solve of one column, with the
 // precomputed factors; F: chunk-local solutions of the column (stride fs).
-template <class T>
-__device__ __forceinline__ void helm_interfaces(const double* __restrict__ IFD, const T* F, int fs, int ny, int P,
+template <class T, class FT>
+__device__ __forceinline__ void helm_interfaces(const FT* __restrict__ IFD, const T* F, int fs, int ny, int P,
                                                 T* G /* 2*(P-1) */) {
   const int Q = P - 1;
   T gu = (T)0, gw = (T)0;
   for (int q = 0; q < Q; ++q) {
     const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
-    const double* R = IFD + 6 * q;
+    const FT* R = IFD + 6 * q;
     const T ru = F[eq * fs] - (q > 0 ? (T)R[4] * gu : (T)0);
     const T rw = F[sq1 * fs];
     gu = (T)R[0] * ru + (T)R[1] * rw;
@@ -155,7 +155,7 @@ __device__ __forceinline__ void helm_interfaces(const double* __restrict__ IFD, 
   if (Q < 1) return;
   T zw = G[2 * (Q - 1) + 1];
   for (int q = Q - 2; q >= 0; --q) {
-    const double* R = IFD + 6 * q;
+    const FT* R = IFD + 6 * q;
     const T f = (T)R[5] * zw;
     const T zu = G[2 * q] - (T)R[1] * f;
     const T zwn = G[2 * q + 1] - (T)R[3] * f;

@@ -7,6 +7,8 @@
 // FP64.  nut holds the total viscosity (xnu included), interior cells; its
 // wall ghosts follow SetBC_and_UpdateHalo_SGS (2 xnu - nut for no-slip walls,
 // nut for free-slip), x and z wrap.
+#include <cstring>
+#include "../../include/ch3d_mlp.h"
 #include "ch3d_ctx.h"
 #include "ch3d_dev.cuh"
 
@@ -160,6 +162,8 @@ __global__ void __launch_bounds__(256) k_sgs_nut(Geo<double> g, Metrics<double> 
     double Ts = sqrt(Kes) * rdelta + strain_rate(g, m, ux, uy, uz, n, jc) / 10.0;
     Ts = Ts < 1.0e-10 ? 0.0 : 1.0 / Ts;
     v = 0.05 * Kes * Ts + xnu;
+  } else if (lp.model == CH3D_LES_MLP) {  // learned closure: explicit stress force, molecular viscosity
+    v = xnu;
   } else {  // Smagorinsky + van Driest damping
     const double D = 1.0 - exp(-(lp.dwall[jc] * sc->utau / xnu) / 26.0);
     const double l = lp.Cs * D * lp.delta[jc];
@@ -175,7 +179,7 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
                                                  double* __restrict__ hx, double* __restrict__ hy,
                                                  double* __restrict__ hz, double* __restrict__ rx,
                                                  double* __restrict__ ry, double* __restrict__ rz,
-                                                 const DevScalars* __restrict__ sc) {
+                                                 const double* __restrict__ fsgs, const DevScalars* __restrict__ sc) {
   if (sc->status) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -183,6 +187,8 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
   if (i >= g.nx || j >= g.ny) return;
   const Nbr n = make_nbr(g, i, j, k);
   const int jc = j + 1;
+  // explicit SGS force of the learned closure (zero for the eddy-viscosity models)
+  const double f1 = fsgs ? fsgs[n.c] : 0.0, f2 = fsgs ? fsgs[g.N + n.c] : 0.0, f3 = fsgs ? fsgs[2 * g.N + n.c] : 0.0;
   const double pmGamma = sc->pmGamma, pmTheta = sc->pmTheta, pmAlpha = sc->pmAlpha, pmBetaT = sc->pmBetaT;
   const double rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2;
   const double qdx1 = 0.25 * rdx, qdx3 = 0.25 * rdz;
@@ -210,7 +216,7 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
     const double d33q1 = g.ap3c * visd * (u_kp - u_c) - g.am3c * visc * (u_c - u_km);
     const double dcq13 = sgs1 + d33q1;
     const double gradp1 = (at(pr, n, 0) - at(pr, n, n.xm)) * rdx;
-    const double conv = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + g.g1;
+    const double conv = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + g.g1 + f1;
     const double ho = hx[n.c];
     hx[n.c] = conv;
     rx[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp1 + 2.0 * pmBetaT * d22q1 + sc->dpmdxns;
@@ -237,7 +243,7 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
     const double d33q2 = g.ap3c * visd * (v_kp - v_c) - g.am3c * visc * (v_c - v_km);
     const double dcq13 = d11q2 + d33q2;
     const double gradp2 = (at(pr, n, 0) - at_jm(pr, g, 3, n, 0)) * sucac;
-    const double conv = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + g.g2;
+    const double conv = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + g.g2 + f2;
     const double ho = hy[n.c];
     hy[n.c] = conv;
     ry[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp2 + 2.0 * pmBetaT * sgs2;
@@ -265,7 +271,7 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
     const double d22q3 = m.ap2c[jc] * visd * (w_jp - w_c) - m.am2c[jc] * visc * (w_c - w_jm);
     const double dcq13 = d11q3 + sgs3;
     const double gradp3 = (at(pr, n, 0) - at(pr, n, n.zm)) * rdz;
-    const double conv = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + g.g3;
+    const double conv = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + g.g3 + f3;
     const double ho = hz[n.c];
     hz[n.c] = conv;
     rz[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp3 + 2.0 * pmBetaT * d22q3;
@@ -341,6 +347,195 @@ __global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, co
 }
 
 // ---------------------------------------------------------------------------
+// Learned closure (LES_type = CH3D_LES_MLP; no counterpart in the reference).
+// Per step: cell-centre velocity gradients g_ij = du_i/dx_j and y+ form the
+// network input (standardised with the training statistics); the network
+// predicts the six SGS stresses tau_ij / u_tau^2 (standardised); points whose
+// input leaves the training range use the Smagorinsky / van Driest stress
+// tau_ij = -2 nu_t S_ij instead.  The explicit force -d tau_ij / dx_j at the
+// staggered velocity points enters the convective part of the RHS.
+// ---------------------------------------------------------------------------
+struct MlpNorm {
+  float in_mean[10], in_std[10], in_lo[10], in_hi[10];  // lo/hi: training range of the standardised inputs
+  float out_mean[6], out_std[6];
+};
+
+// cell-centre gradients (the WALE stencils, m_LESModels.f90:98-111)
+__device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metrics<double>& m, const double* ux,
+                                               const double* uy, const double* uz, const Nbr& n, int jc,
+                                               double* G /* 9: dudx dudy dudz dvdx dvdy dvdz dwdx dwdy dwdz */) {
+  const double rdx = g.rdx, rdz = g.rdz;
+  const double caj = m.rdyp[jc], cac1 = m.rdyc[jc], cac2 = m.rdyc[jc + 1], cac12 = cac1 - cac2;
+  G[0] = (at(ux, n, n.xp) - at(ux, n, 0)) * rdx;
+  G[1] = ((at_jp(ux, g, 0, n, n.xp) + at_jp(ux, g, 0, n, 0)) * cac2 + (at(ux, n, n.xp) + at(ux, n, 0)) * cac12 -
+          (at_jm(ux, g, 0, n, n.xp) + at_jm(ux, g, 0, n, 0)) * cac1) * 0.25;
+  G[2] = (at(ux, n, n.xp + n.zp) + at(ux, n, n.zp) - at(ux, n, n.xp + n.zm) - at(ux, n, n.zm)) * rdz * 0.25;
+  G[3] = (at_jp(uy, g, 1, n, n.xp) - at_jp(uy, g, 1, n, n.xm) + at(uy, n, n.xp) - at(uy, n, n.xm)) * rdx * 0.25;
+  G[4] = (at_jp(uy, g, 1, n, 0) - at(uy, n, 0)) * caj;
+  G[5] = (at_jp(uy, g, 1, n, n.zp) + at(uy, n, n.zp) - at_jp(uy, g, 1, n, n.zm) - at(uy, n, n.zm)) * rdz * 0.25;
+  G[6] = (at(uz, n, n.xp + n.zp) - at(uz, n, n.xm + n.zp) + at(uz, n, n.xp) - at(uz, n, n.xm)) * rdx * 0.25;
+  G[7] = ((at_jp(uz, g, 2, n, n.zp) + at_jp(uz, g, 2, n, 0)) * cac2 + (at(uz, n, n.zp) + at(uz, n, 0)) * cac12 -
+          (at_jm(uz, g, 2, n, n.zp) + at_jm(uz, g, 2, n, 0)) * cac1) * 0.25;
+  G[8] = (at(uz, n, n.zp) - at(uz, n, 0)) * rdz;
+}
+
+// inputs X [N x 10] (FP32, standardised; gradients in wall units g nu / u_tau^2,
+// then y+), the fallback stress of every point into tau [6][N] and the
+// out-of-range flag
+__global__ void __launch_bounds__(256) k_sgs_features(Geo<double> g, Metrics<double> m, LesPar lp, MlpNorm nm,
+                                                      const double* __restrict__ ux, const double* __restrict__ uy,
+                                                      const double* __restrict__ uz, float* __restrict__ X,
+                                                      double* __restrict__ tau, unsigned char* __restrict__ fb,
+                                                      const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const Nbr n = make_nbr(g, i, j, k);
+  const int jc = j + 1;
+  double G[9];
+  cell_gradients(g, m, ux, uy, uz, n, jc, G);
+  const double ut = sc->utau > 1e-30 ? sc->utau : 1e-30;
+  const double gs = (double)g.xnu / (ut * ut);
+  const double yplus = lp.dwall[jc] * ut / (double)g.xnu;
+  bool out = false;
+  for (int q = 0; q < 10; ++q) {
+    const double v = q < 9 ? G[q] * gs : yplus;
+    const float xs = (float)((v - nm.in_mean[q]) / nm.in_std[q]);
+    X[n.c * 10 + q] = xs;
+    out = out || !(xs >= nm.in_lo[q] && xs <= nm.in_hi[q]);
+  }
+  fb[n.c] = out ? 1 : 0;
+  // Smagorinsky / van Driest stress: tau_ij = -2 nu_t S_ij
+  const double S11 = G[0], S22 = G[4], S33 = G[8];
+  const double S12 = 0.5 * (G[1] + G[3]), S13 = 0.5 * (G[2] + G[6]), S23 = 0.5 * (G[5] + G[7]);
+  const double Smag = sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23)));
+  const double D = 1.0 - exp(-yplus / 26.0);
+  const double l = lp.Cs * D * lp.delta[jc];
+  const double nt = l * l * Smag;
+  const long long N = g.N;
+  tau[0 * N + n.c] = -2.0 * nt * S11;
+  tau[1 * N + n.c] = -2.0 * nt * S12;
+  tau[2 * N + n.c] = -2.0 * nt * S13;
+  tau[3 * N + n.c] = -2.0 * nt * S22;
+  tau[4 * N + n.c] = -2.0 * nt * S23;
+  tau[5 * N + n.c] = -2.0 * nt * S33;
+}
+
+// network outputs -> tau (kept: the fallback stress where the input left the range)
+__global__ void __launch_bounds__(256) k_sgs_tau(long long N, MlpNorm nm, const float* __restrict__ Y,
+                                                 const unsigned char* __restrict__ fb, double* __restrict__ tau,
+                                                 const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N || fb[c]) return;
+  const double u2 = sc->utau * sc->utau;
+  for (int q = 0; q < 6; ++q) tau[q * N + c] = ((double)Y[c * 6 + q] * nm.out_std[q] + nm.out_mean[q]) * u2;
+}
+
+// f_i = -d tau_ij / dx_j at the staggered points of u_i.  Off-diagonal
+// stresses are averaged from the four surrounding cell centres onto the cell
+// edges; they vanish on the walls.
+__global__ void __launch_bounds__(256) k_sgs_force(Geo<double> g, Metrics<double> m, const double* __restrict__ tau,
+                                                   double* __restrict__ fx, double* __restrict__ fy,
+                                                   double* __restrict__ fz, const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const Nbr n = make_nbr(g, i, j, k);
+  const int jc = j + 1;
+  const long long N = g.N;
+  const double* t11 = tau;
+  const double* t12 = tau + N;
+  const double* t13 = tau + 2 * N;
+  const double* t22 = tau + 3 * N;
+  const double* t23 = tau + 4 * N;
+  const double* t33 = tau + 5 * N;
+  const double rdx = g.rdx, rdz = g.rdz;
+  // edge averages of a cell-centred field over the cells at offsets {0, o1} x {0, o2}
+  auto e4 = [&](const double* t, long long o1, long long o2) {
+    return 0.25 * (at(t, n, 0) + at(t, n, o1) + at(t, n, o2) + at(t, n, o1 + o2));
+  };
+  // y-edge averages (j -/+ 1/2); zero on the walls
+  auto ey = [&](const double* t, long long o1, int up) {
+    if (up ? n.jhi : n.jlo) return 0.0;
+    const long long oy = up ? (long long)n.yp : -(long long)n.yp;
+    return 0.25 * (at(t, n, 0) + at(t, n, o1) + at(t, n, oy) + at(t, n, o1 + oy));
+  };
+  {  // x momentum at (i-1/2, j, k)
+    const double d1 = (at(t11, n, 0) - at(t11, n, n.xm)) * rdx;
+    const double d2 = (ey(t12, n.xm, 1) - ey(t12, n.xm, 0)) * m.rdyp[jc];
+    const double d3 = (e4(t13, n.xm, n.zp) - e4(t13, n.xm, n.zm)) * rdz;
+    fx[n.c] = -(d1 + d2 + d3);
+  }
+  {  // y momentum at (i, j-1/2, k); the wall row (j = 0) is fixed by the wall condition
+    double v = 0.0;
+    if (!n.jlo) {
+      const long long ym = -(long long)n.yp;
+      const double d1 = (e4(t12, n.xp, ym) - e4(t12, n.xm, ym)) * rdx;
+      const double d2 = (at(t22, n, 0) - at(t22, n, ym)) * m.rdyc[jc];
+      const double d3 = (e4(t23, n.zp, ym) - e4(t23, n.zm, ym)) * rdz;
+      v = -(d1 + d2 + d3);
+    }
+    fy[n.c] = v;
+  }
+  {  // z momentum at (i, j, k-1/2)
+    const double d1 = (e4(t13, n.xp, n.zm) - e4(t13, n.xm, n.zm)) * rdx;
+    const double d2 = (ey(t23, n.zm, 1) - ey(t23, n.zm, 0)) * m.rdyp[jc];
+    const double d3 = (at(t33, n, 0) - at(t33, n, n.zm)) * rdz;
+    fz[n.c] = -(d1 + d2 + d3);
+  }
+}
+
+// Training samples: one thread per box of fx x fy x fz cells (anchored at
+// multiples of the box size), volume-weighted box averages in y.
+__global__ void __launch_bounds__(128) k_sgs_train_samples(Geo<double> g, Metrics<double> m, const double* __restrict__ yc,
+                                                           const double* __restrict__ ux, const double* __restrict__ uy,
+                                                           const double* __restrict__ uz, int fx, int fy, int fz,
+                                                           float* __restrict__ X, float* __restrict__ T, double ylo,
+                                                           double yhi, const DevScalars* __restrict__ sc) {
+  const int bx = g.nx / fx, by = g.ny / fy, bz = g.nz / fz;
+  const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= (long long)bx * by * bz) return;
+  const int ib = (int)(b % bx), jb = (int)((b / bx) % by), kb = (int)(b / ((long long)bx * by));
+  double W = 0, Y = 0, U[3] = {0, 0, 0}, UU[6] = {0, 0, 0, 0, 0, 0}, GG[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int kk = 0; kk < fz; ++kk)
+    for (int jj = 0; jj < fy; ++jj)
+      for (int ii = 0; ii < fx; ++ii) {
+        const int i = ib * fx + ii, j = jb * fy + jj, k = kb * fz + kk, jc = j + 1;
+        const Nbr n = make_nbr(g, i, j, k);
+        const double w = m.dyp[jc];
+        const double u = 0.5 * (at(ux, n, 0) + at(ux, n, n.xp));
+        const double v = 0.5 * (at(uy, n, 0) + at_jp(uy, g, 1, n, 0));
+        const double z = 0.5 * (at(uz, n, 0) + at(uz, n, n.zp));
+        double G[9];
+        cell_gradients(g, m, ux, uy, uz, n, jc, G);
+        W += w; Y += w * yc[jc];
+        U[0] += w * u; U[1] += w * v; U[2] += w * z;
+        UU[0] += w * u * u; UU[1] += w * u * v; UU[2] += w * u * z;
+        UU[3] += w * v * v; UU[4] += w * v * z; UU[5] += w * z * z;
+        for (int q = 0; q < 9; ++q) GG[q] += w * G[q];
+      }
+  const double iw = 1.0 / W;
+  const double ut = sc->utau > 1e-30 ? sc->utau : 1e-30;
+  const double gs = (double)g.xnu / (ut * ut), ts = 1.0 / (ut * ut);
+  const double yb = Y * iw;
+  const double dw = fmin(yb - ylo, yhi - yb);
+  for (int q = 0; q < 9; ++q) X[b * 10 + q] = (float)(GG[q] * iw * gs);
+  X[b * 10 + 9] = (float)(dw * ut / (double)g.xnu);
+  const double u0 = U[0] * iw, u1 = U[1] * iw, u2 = U[2] * iw;
+  T[b * 6 + 0] = (float)((UU[0] * iw - u0 * u0) * ts);
+  T[b * 6 + 1] = (float)((UU[1] * iw - u0 * u1) * ts);
+  T[b * 6 + 2] = (float)((UU[2] * iw - u0 * u2) * ts);
+  T[b * 6 + 3] = (float)((UU[3] * iw - u1 * u1) * ts);
+  T[b * 6 + 4] = (float)((UU[4] * iw - u1 * u2) * ts);
+  T[b * 6 + 5] = (float)((UU[5] * iw - u2 * u2) * ts);
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static LesPar les_par(const ch3d_ctx* c) {
@@ -350,7 +545,7 @@ static LesPar les_par(const ch3d_ctx* c) {
   const double tr[9] = {1, 2, 1, 2, 4, 2, 1, 2, 1}, si[9] = {1, 4, 1, 4, 16, 4, 1, 4, 1};
   for (int q = 0; q < 9; ++q) lp.Fc[q] = c->cfg.FilterType == 1 ? si[q] / 36.0 : tr[q] / 16.0;
   lp.Cs = c->cfg.Cs;
-  lp.model = c->cfg.LES_type == CH3D_LES_MLP ? CH3D_LES_SMAG_VD : c->cfg.LES_type;
+  lp.model = c->cfg.LES_type;
   return lp;
 }
 
@@ -360,20 +555,49 @@ cudaError_t launch_sgs_nut(ch3d_ctx* c) {
   double** f = (double**)c->f;
   const Geo<double> g = make_geo<double>(c);
   const LesPar lp = les_par(c);
-  if (lp.model == CH3D_LES_SMAG_VD) {
+  if (lp.model == CH3D_LES_SMAG_VD || lp.model == CH3D_LES_MLP) {
     const double d1 = c->yc[1] - c->yp[1], dN = c->yp[c->ny + 1] - c->yc[c->ny];
     k_wall_utau<<<1, 1024, 0, c->stream>>>(g, f[0], d1, dN, c->sc);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   k_sgs_nut<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, f[0], f[1], f[2], f[11], c->sc);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || lp.model != CH3D_LES_MLP) return e;
+  MlpNorm nm;
+  static_assert(sizeof(MlpNorm) == CH3D_SGS_NORM_FLOATS * sizeof(float), "norm layout");
+  memcpy(&nm, c->mlp_norm, sizeof(nm));
+  k_sgs_features<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, nm, f[0], f[1], f[2], c->mlp_x, c->sgs_tau,
+                                                             c->mlp_fb, c->sc);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (ch3d_mlp_forward(c->mlp_x, (int)c->N, c->mlp_params, c->mlp_y, c->mlp_status, c->stream) != 0)
+    return cudaErrorLaunchFailure;
+  k_sgs_tau<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>(c->N, nm, c->mlp_y, c->mlp_fb, c->sgs_tau, c->sc);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_sgs_force<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, c->sgs_tau, c->sgs_f, c->sgs_f + c->N,
+                                                          c->sgs_f + 2 * c->N, c->sc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sgs_samples(ch3d_ctx* c, int fx, int fy, int fz, float* X, float* T) {
+  double** f = (double**)c->f;
+  const Geo<double> g = make_geo<double>(c);
+  const double d1 = c->yc[1] - c->yp[1], dN = c->yp[c->ny + 1] - c->yc[c->ny];
+  k_wall_utau<<<1, 1024, 0, c->stream>>>(g, f[0], d1, dN, c->sc);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long nb = (long long)(c->nx / fx) * (c->ny / fy) * (c->nz / fz);
+  const double* yc = c->met64 + 16 * (c->ny + 3);  // packed yc (pack_metrics, vector 16)
+  k_sgs_train_samples<<<(unsigned)((nb + 127) / 128), 128, 0, c->stream>>>(g, c->m64full, yc, f[0], f[1], f[2], fx, fy,
+                                                                          fz, X, T, c->yp[1], c->yp[c->ny + 1], c->sc);
   return cudaGetLastError();
 }
 
 cudaError_t launch_rhs_les(ch3d_ctx* c) {
   double** f = (double**)c->f;
   k_rhs_les<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(make_geo<double>(c), c->m64, f[0], f[1], f[2], f[3], f[11],
-                                                         f[4], f[5], f[6], f[7], f[8], f[9], c->sc);
+                                                         f[4], f[5], f[6], f[7], f[8], f[9],
+                                                         c->cfg.LES_type == CH3D_LES_MLP ? c->sgs_f : nullptr, c->sc);
   return cudaGetLastError();
 }
 

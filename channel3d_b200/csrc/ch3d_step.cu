@@ -453,10 +453,13 @@ __device__ __forceinline__ void rhs_uhat_body(const Geo<T>& g, const Metrics<T>&
                                               int P, const T* __restrict__ ux, const T* __restrict__ uy,
                                               const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ h,
                                               T* __restrict__ us, int i0, int k, const DevScalars* __restrict__ sc,
-                                              T* F, T* IF) {
+                                              T* F, T* IF, T* FS) {
   const int nx = g.nx, ny = g.ny, Q = P - 1;
   const int QQ = 2 * (Q > 0 ? Q : 1);
-  const double* FS = fac + (C == 1 ? helm_set_stride(ny, P) : 0);
+  {  // this component's Helmholtz factors, staged in shared memory (read by the sequential sweeps)
+    const double* FG = fac + (C == 1 ? helm_set_stride(ny, P) : 0);
+    for (int t = threadIdx.x; t < helm_set_stride(ny, P); t += blockDim.x) FS[t] = (T)FG[t];
+  }
   const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
   const T add = C == 0 ? (T)sc->dpmdxns : (T)0;
   const int tid = threadIdx.x;
@@ -516,9 +519,10 @@ __global__ void __launch_bounds__(256, 4) k_rhs_uhat(Geo<T> g, Metrics<T> m, con
   const int i0 = (blockIdx.x / 3) * TI, k = blockIdx.y;
   T* F = (T*)smem_raw;
   T* IF = F + (size_t)g.ny * TI;
-  if (comp == 0) rhs_uhat_body<T, 0, TI>(g, m, fac, P, ux, uy, uz, pr, hx, uxs, i0, k, sc, F, IF);
-  else if (comp == 1) rhs_uhat_body<T, 1, TI>(g, m, fac, P, ux, uy, uz, pr, hy, uys, i0, k, sc, F, IF);
-  else rhs_uhat_body<T, 2, TI>(g, m, fac, P, ux, uy, uz, pr, hz, uzs, i0, k, sc, F, IF);
+  T* FS = IF + (size_t)TI * 2 * (P > 1 ? P - 1 : 1);
+  if (comp == 0) rhs_uhat_body<T, 0, TI>(g, m, fac, P, ux, uy, uz, pr, hx, uxs, i0, k, sc, F, IF, FS);
+  else if (comp == 1) rhs_uhat_body<T, 1, TI>(g, m, fac, P, ux, uy, uz, pr, hy, uys, i0, k, sc, F, IF, FS);
+  else rhs_uhat_body<T, 2, TI>(g, m, fac, P, ux, uy, uz, pr, hz, uzs, i0, k, sc, F, IF, FS);
 }
 
 // ---------------------------------------------------------------------------
@@ -772,70 +776,31 @@ __device__ __forceinline__ int kz_of_block(int y, int nz) {
   return y == 0 ? 0 : ((y & 1) ? (y + 1) / 2 : nz - y / 2);
 }
 
-// Factors of the systems (kx, kzh) with kx in [0, kxn) and kzh = blockIdx.y,
-// stored in precision R with leading dimension ldx.
-template <class T, class R>
-__global__ void __launch_bounds__(256) k_ysolve_factors(Geo<T> g, Metrics<double> m, const double* __restrict__ wave,
-                                                        R* __restrict__ RMf, R* __restrict__ CPf, R* __restrict__ IFf,
-                                                        int TS, int P, int ldx, int kxn) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* AB = (double*)smem_raw;  // TS * P * 4 : alpha_s, alpha_e, beta_s, beta_e
-  const int nx = g.nx, ny = g.ny;
-  const int kx0 = blockIdx.x * TS, kzh = blockIdx.y;
-  const int Q = P - 1;
-  for (int t = threadIdx.x; t < TS * P; t += blockDim.x) {
-    const int s = t % TS, p = t / TS, kx = kx0 + s;
-    if (kx >= kxn) continue;
-    const double lam = wave[kx] + wave[nx + kzh];
-    const bool pin = (kx == 0 && kzh == 0);
-    const int jlo = chunk_lo(p, ny, P), jhi = chunk_hi(p, ny, P), L = jhi - jlo + 1;
-    double cpv[CH3D_LMAX], dav[CH3D_LMAX];
-    double cpp = 0.0, dal = 0.0;
-#pragma unroll
-    for (int q = 0; q < CH3D_LMAX; ++q) {
-      if (q < L) {
-        const int j = jlo + q, jc = j + 1;
-        double a = m.am2Pr[jc], c = m.ap2Pr[jc], b = m.ac2Pr[jc] + lam;
-        if (pin && j == 0) { a = 0.0; b = 1.0; c = 0.0; }
-        const double mm = (q == 0) ? b : b - a * cpp;
-        const double rm = 1.0 / mm;
-        const double cp = c * rm;
-        dal = (q == 0) ? -a * rm : -a * dal * rm;
-        const size_t o = ((size_t)kzh * ny + j) * ldx + kx;
-        RMf[o] = (R)rm;
-        CPf[o] = (R)cp;
-        cpv[q] = cp;
-        dav[q] = (p == 0) ? 0.0 : dal;
-        cpp = cp;
-      }
-    }
-    double al = dav[0], be = 0.0, al_e = 0.0, be_e = 0.0;
-#pragma unroll
-    for (int q = CH3D_LMAX - 1; q >= 0; --q) {
-      if (q < L) {
-        if (q == L - 1) { al = dav[q]; be = (p == P - 1) ? 0.0 : -cpv[q]; al_e = al; be_e = be; }
-        else { al = dav[q] - cpv[q] * al; be = -cpv[q] * be; }
-      }
-    }
-    double* A = AB + (size_t)(s * P + p) * 4;
-    A[0] = al; A[1] = al_e; A[2] = be; A[3] = be_e;
-  }
-  __syncthreads();
-  for (int s = threadIdx.x; s < TS; s += blockDim.x) {
-    const int kx = kx0 + s;
-    if (kx >= kxn) continue;
-    double m01p = 0.0, vprev = 0.0;
-    for (int q = 0; q < Q; ++q) {
-      const double* Aq = AB + (size_t)(s * P + q) * 4;       // chunk q
-      const double* Aq1 = AB + (size_t)(s * P + q + 1) * 4;  // chunk q+1
-      const double l = -Aq[1], v = -Aq1[2];
-      double d00 = 1.0, d01 = -Aq[3], d10 = -Aq1[0], d11 = 1.0;
-      if (q > 0) d01 -= l * m01p * vprev;
-      const double r = 1.0 / (d00 * d11 - d01 * d10);
-      const double Rv[6] = {d11 * r, -d01 * r, -d10 * r, d00 * r, l, v};
-      for (int c = 0; c < 6; ++c) IFf[(((size_t)kzh * Q + q) * 6 + c) * ldx + kx] = (R)Rv[c];
-      m01p = Rv[1]; vprev = v;
-    }
+// Factors of the Thomas elimination of the Poisson y systems
+// [am2Pr, ac2Pr + wx(kx) + wz(kz), ap2Pr] (src/CFD_2nd/m_Poisson.f90:1126-1150,
+// InverseTridiagonal, m_Tools.f90:224-251), one thread per (kx, |kz|) column:
+// rm_j = 1 / (b_j - a_j cp_{j-1}), cp_j = c_j rm_j; row 1 of the (0,0) system
+// is replaced by phi = 0 (:1136-1140).  They depend on the grid only and are
+// computed once per run, in FP64 and stored in precision R, layout
+// ((kzh * ny) + j) * ldx + kx.
+template <class R>
+__global__ void __launch_bounds__(128) k_ythomas_factors(Metrics<double> m, const double* __restrict__ wave, int nx,
+                                                         int ny, R* __restrict__ RMf, R* __restrict__ CPf, int ldx,
+                                                         int kxn) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzh = blockIdx.y;
+  if (kx >= kxn) return;
+  const double lam = wave[kx] + wave[nx + kzh];
+  const bool pin = (kx == 0 && kzh == 0);
+  double cp = 0.0;
+  for (int j = 0; j < ny; ++j) {
+    const int jc = j + 1;
+    double a = m.am2Pr[jc], c = m.ap2Pr[jc], b = m.ac2Pr[jc] + lam;
+    if (pin && j == 0) { a = 0.0; b = 1.0; c = 0.0; }
+    const double rm = 1.0 / (j == 0 ? b : b - a * cp);
+    cp = c * rm;
+    const size_t o = ((size_t)kzh * ny + j) * ldx + kx;
+    RMf[o] = (R)rm;
+    CPf[o] = (R)cp;
   }
 }
 
@@ -843,133 +808,63 @@ template <class R> struct Vec2Of;
 template <> struct Vec2Of<double> { typedef double2 type; };
 template <> struct Vec2Of<float> { typedef float2 type; };
 
-// sel: 0 every (kx tile, kz) block; 1 only the low-mode blocks (kx tile 0,
-// kz in [0,KL] or [nz-KL, nz)), grid.y enumerating them; 2 every block but those.
-template <class T, class R>
-__global__ void __launch_bounds__(256, 2) k_ysolve2(Geo<T> g, Metrics<double> m, const R* __restrict__ RMf,
-                                                    const R* __restrict__ CPf, const R* __restrict__ IFf, int ldx,
-                                                    typename CplxOf<T>::type* __restrict__ spec, int TS, int P,
-                                                    int sel, int KL, const DevScalars* __restrict__ sc) {
+// Poisson y solve, Thomas across threads: one thread per (kx, kz) column,
+// a warp covers 32 consecutive kx (coalesced rows of the (kx, j, kz)
+// spectrum).  The forward sweep keeps d_j in place in the spectrum (or, for
+// the FP64 low modes of the mixed path, in an FP64 scratch column), the
+// backward sweep overwrites it with the solution.
+// sel 0: every column; 1: only the low modes kx < KX, |kz| <= KL (grid.y
+// enumerates kz = 0..KL, nz-KL..nz-1); 2: every column but those.
+template <class T, class R, bool SCR>
+__global__ void __launch_bounds__(128) k_ythomas(Geo<T> g, Metrics<double> m, const R* __restrict__ RMf,
+                                                 const R* __restrict__ CPf, int ldx,
+                                                 typename CplxOf<T>::type* __restrict__ spec,
+                                                 typename Vec2Of<R>::type* __restrict__ scr, int sel, int KL, int KX,
+                                                 const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
   typedef typename Vec2Of<R>::type V2;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   if (sc->status) return;
-  const int ny = g.ny, nz = g.nz, nxh = g.nxh;
-  int kz;
-  if (sel == 1) kz = (int)blockIdx.y <= KL ? (int)blockIdx.y : nz - ((int)blockIdx.y - KL);
-  else kz = kz_of_block(blockIdx.y, nz);
+  const int nxh = g.nxh, ny = g.ny, nz = g.nz;
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int kz = sel == 1 ? ((int)blockIdx.y <= KL ? (int)blockIdx.y : nz - ((int)blockIdx.y - KL)) : (int)blockIdx.y;
   const int kzh = kz <= nz - kz ? kz : nz - kz;
-  if (sel == 2 && blockIdx.x == 0 && kzh <= KL) return;
-  const int kx0 = blockIdx.x * TS;
-  const int Q = P - 1, QQ = 2 * (Q > 0 ? Q : 1);
-  V2* F = (V2*)smem_raw;                 // ny * TS
-  V2* G = F + (size_t)ny * TS;           // TS * QQ
-  const long long zs = (long long)nxh * ny;
-  for (int t = threadIdx.x; t < ny * TS; t += blockDim.x) {
-    const int s = t % TS, j = t / TS, kx = kx0 + s;
-    V2 v;
-    v.x = (R)0; v.y = (R)0;
-    if (kx < nxh) {
-      const CT c = spec[kx + (long long)nxh * j + zs * kz];
-      v.x = (R)c.x; v.y = (R)c.y;
-    }
-    F[t] = v;
-  }
-  __syncthreads();
-  R cpv[CH3D_LMAX], alv[CH3D_LMAX];
-  const int t0 = threadIdx.x;
-  const bool act = t0 < TS * P;
-  const int s = t0 % TS, p = t0 / TS, kx = kx0 + s;
-  const int jlo = chunk_lo(p, ny, P), jhi = chunk_hi(p, ny, P), L = jhi - jlo + 1;
+  if (kx >= nxh || (sel == 1 && kx >= KX)) return;
+  if (sel == 2 && kx < KX && kzh <= KL) return;
+  const R* rm = RMf + (size_t)kzh * ny * ldx + kx;
+  const R* cp = CPf + (size_t)kzh * ny * ldx + kx;
+  CT* col = spec + kx + (size_t)nxh * ny * kz;
+  V2* w = SCR ? scr + ((size_t)blockIdx.y * KX + kx) * ny : nullptr;
+  const size_t st = (size_t)nxh;
   const bool pin = (kx == 0 && kz == 0);
-  if (act && kx < nxh) {
-    V2 d;
-    d.x = (R)0; d.y = (R)0;
-    R dal = (R)0;
-#pragma unroll
-    for (int q = 0; q < CH3D_LMAX; ++q) {
-      if (q < L) {
-        const int j = jlo + q;
-        const size_t o = ((size_t)kzh * ny + j) * ldx + kx;
-        const R rm = RMf[o];
-        cpv[q] = CPf[o];
-        R a = (R)m.am2Pr[j + 1];
-        V2 f = F[j * TS + s];
-        if (pin && j == 0) { a = (R)0; f.x = (R)0; f.y = (R)0; }
-        if (q == 0) { d.x = f.x * rm; d.y = f.y * rm; dal = -a * rm; }
-        else { d.x = (f.x - a * d.x) * rm; d.y = (f.y - a * d.y) * rm; dal = -a * dal * rm; }
-        F[j * TS + s] = d;
-        alv[q] = (p == 0) ? (R)0 : dal;
-      }
-    }
-    V2 y = d;
-    R al = (R)0;
-#pragma unroll
-    for (int q = CH3D_LMAX - 1; q >= 0; --q) {
-      if (q < L) {
-        const int j = jlo + q;
-        if (q == L - 1) { al = alv[q]; }
-        else {
-          const V2 dj = F[j * TS + s];
-          y.x = dj.x - cpv[q] * y.x; y.y = dj.y - cpv[q] * y.y;
-          F[j * TS + s] = y;
-          al = alv[q] - cpv[q] * al;
-          alv[q] = al;
-        }
-      }
-    }
+  R dx, dy;
+  {
+    const CT f = col[0];
+    const R r = rm[0];
+    dx = pin ? (R)0 : (R)f.x * r;
+    dy = pin ? (R)0 : (R)f.y * r;
+    if (SCR) { V2 v; v.x = dx; v.y = dy; w[0] = v; }
+    else col[0] = mk((T)dx, (T)dy);
   }
-  __syncthreads();
-  if (threadIdx.x < TS && Q > 0) {
-    const int ss = threadIdx.x, kxs = kx0 + ss;
-    if (kxs < nxh) {
-      V2* Gs = G + (size_t)ss * QQ;
-      V2 gu, gw;
-      gu.x = gu.y = gw.x = gw.y = (R)0;
-      for (int q = 0; q < Q; ++q) {
-        const int eq = chunk_hi(q, ny, P), sq1 = chunk_lo(q + 1, ny, P);
-        const R* Rq = IFf + ((size_t)kzh * Q + q) * 6 * ldx + kxs;
-        const R M00 = Rq[0], M01 = Rq[ldx], M10 = Rq[2 * ldx], M11 = Rq[3 * ldx], l = Rq[4 * ldx];
-        V2 ru = F[eq * TS + ss];
-        if (q > 0) { ru.x -= l * gu.x; ru.y -= l * gu.y; }
-        const V2 rw = F[sq1 * TS + ss];
-        gu.x = M00 * ru.x + M01 * rw.x; gu.y = M00 * ru.y + M01 * rw.y;
-        gw.x = M10 * ru.x + M11 * rw.x; gw.y = M10 * ru.y + M11 * rw.y;
-        Gs[2 * q] = gu; Gs[2 * q + 1] = gw;
-      }
-      V2 zw = Gs[2 * (Q - 1) + 1];
-      for (int q = Q - 2; q >= 0; --q) {
-        const R* Rq = IFf + ((size_t)kzh * Q + q) * 6 * ldx + kxs;
-        const R M01 = Rq[ldx], M11 = Rq[3 * ldx], v = Rq[5 * ldx];
-        const R fx = v * zw.x, fy = v * zw.y;
-        V2 zu = Gs[2 * q], zwn = Gs[2 * q + 1];
-        zu.x -= M01 * fx; zu.y -= M01 * fy;
-        zwn.x -= M11 * fx; zwn.y -= M11 * fy;
-        Gs[2 * q] = zu; Gs[2 * q + 1] = zwn;
-        zw = zwn;
-      }
-    }
+#pragma unroll 4
+  for (int j = 1; j < ny; ++j) {
+    const R a = (R)m.am2Pr[j + 1];
+    const CT f = col[st * j];
+    const R r = rm[(size_t)ldx * j];
+    dx = ((R)f.x - a * dx) * r;
+    dy = ((R)f.y - a * dy) * r;
+    if (SCR) { V2 v; v.x = dx; v.y = dy; w[j] = v; }
+    else col[st * j] = mk((T)dx, (T)dy);
   }
-  __syncthreads();
-  if (act && kx < nxh) {
-    const V2* Gs = G + (size_t)s * QQ;
-    V2 uL, wR;
-    uL.x = uL.y = wR.x = wR.y = (R)0;
-    if (p > 0) uL = Gs[2 * (p - 1)];
-    if (p < P - 1) wR = Gs[2 * p + 1];
-    R be = (R)0;
-#pragma unroll
-    for (int q = CH3D_LMAX - 1; q >= 0; --q) {
-      if (q < L) {
-        const int j = jlo + q;
-        be = (q == L - 1) ? ((p == P - 1) ? (R)0 : -cpv[q]) : -cpv[q] * be;
-        const V2 y = F[j * TS + s];
-        const R al = alv[q];
-        const R xr = y.x + al * uL.x + be * wR.x;
-        const R xi = y.y + al * uL.y + be * wR.y;
-        spec[kx + (long long)nxh * j + zs * kz] = mk((T)xr, (T)xi);
-      }
-    }
+  col[st * (ny - 1)] = mk((T)dx, (T)dy);
+#pragma unroll 4
+  for (int j = ny - 2; j >= 0; --j) {
+    const R c = cp[(size_t)ldx * j];
+    R ex, ey;
+    if (SCR) { const V2 v = w[j]; ex = v.x; ey = v.y; }
+    else { const CT v = col[st * j]; ex = (R)v.x; ey = (R)v.y; }
+    dx = ex - c * dx;
+    dy = ey - c * dy;
+    col[st * j] = mk((T)dx, (T)dy);
   }
 }
 
@@ -1014,6 +909,29 @@ __global__ void __launch_bounds__(256) k_xifft(Geo<T> g, const typename CplxOf<T
   }
 }
 
+// Block reductions of a 256-thread block with warp shuffles: the result is
+// valid in thread 0 (order of the sums fixed, so results are reproducible).
+__device__ __forceinline__ double block_sum256(double v, double* sh /* 8 */) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+  if ((tl & 31) == 0) sh[tl >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (tl == 0)
+    for (int w = 0; w < 8; ++w) r += sh[w];
+  return r;
+}
+__device__ __forceinline__ double block_max256(double v, double* sh /* 8 */) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+  if ((tl & 31) == 0) sh[tl >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (tl == 0)
+    for (int w = 0; w < 8; ++w) r = fmax(r, sh[w]);
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // FluidVelUpdate (src/CFD_2nd/m_TScheme.f90:281-306) + PressureUpdate_PIMP
 // (src/CFD_2nd/m_TSchemePIMP_inc.f90:852-873), phi ghosts from
@@ -1026,7 +944,7 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
                                               T* ux, T* uy, T* uz, T* __restrict__ pr, const T* __restrict__ phi,
                                               double* __restrict__ part, int mode, const DevScalars* __restrict__ sc,
                                               const T* __restrict__ nut) {
-  __shared__ double red[256];
+  __shared__ double red[8];
   if (sc->status) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1084,13 +1002,8 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
     }
     s = (double)uxn * (double)m.s1coe[jc];
   }
-  red[tl] = s;
-  __syncthreads();
-  for (int w = blockDim.x * blockDim.y / 2; w > 0; w >>= 1) {
-    if (tl < w) red[tl] += red[tl + w];
-    __syncthreads();
-  }
-  if (tl == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = red[0];
+  const double bs = block_sum256(s, red);
+  if (tl == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
 }
 
 // bulk partial sums of ux*s1coe for a freshly uploaded field
@@ -1119,8 +1032,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_diag(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
                                               const T* __restrict__ uy, const T* __restrict__ uz,
                                               double* __restrict__ part, DevScalars* __restrict__ sc, int only_cfl) {
-  __shared__ double red[4][256];
-  __shared__ double rsum[256];
+  __shared__ double red[6][8];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -1142,27 +1054,31 @@ __global__ void __launch_bounds__(256) k_diag(Geo<T> g, Metrics<T> m, const T* _
     cf = fabs(a + aip) * rdx + fabs(b + bjp) * rdyp + fabs(c + ckp) * rdz;
     s = a * (double)m.dyp[jc];
   }
-  red[0][tl] = dv; red[1][tl] = v0; red[2][tl] = v1; red[3][tl] = fmax(v2, 0.0);
-  rsum[tl] = s;
-  __shared__ double rcf[256];
-  rcf[tl] = cf;
+  // fmax(NaN, x) = x on the device, so NaN is folded into +inf first: a NaN
+  // field still trips the limit checks of the step
+  if (!(dv == dv)) dv = INFINITY;
+  if (!(v0 == v0)) v0 = INFINITY;
+  if (!(v1 == v1)) v1 = INFINITY;
+  if (!(v2 == v2)) v2 = INFINITY;
+  const double r_cf = block_max256(cf, red[0]);
   __syncthreads();
-  for (int w = blockDim.x * blockDim.y / 2; w > 0; w >>= 1) {
-    if (tl < w) {
-      for (int q = 0; q < 4; ++q) red[q][tl] = fmax(red[q][tl], red[q][tl + w]);
-      rcf[tl] = fmax(rcf[tl], rcf[tl + w]);
-      rsum[tl] += rsum[tl + w];
-    }
-    __syncthreads();
-  }
+  const double r_dv = block_max256(dv, red[1]);
+  __syncthreads();
+  const double r_v0 = block_max256(v0, red[2]);
+  __syncthreads();
+  const double r_v1 = block_max256(v1, red[3]);
+  __syncthreads();
+  const double r_v2 = block_max256(v2, red[4]);
+  __syncthreads();
+  const double r_s = block_sum256(s, red[5]);
   if (tl == 0) {
-    atomic_max_nonneg(&sc->uddx, rcf[0] * 0.5);
+    atomic_max_nonneg(&sc->uddx, r_cf * 0.5);
     if (!only_cfl) {
-      atomic_max_nonneg(&sc->divmax2, red[0][0]);
-      atomic_max_nonneg(&sc->vmax[0], red[1][0]);
-      atomic_max_nonneg(&sc->vmax[1], red[2][0]);
-      atomic_max_nonneg(&sc->vmax[2], red[3][0]);
-      part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = rsum[0];
+      atomic_max_nonneg(&sc->divmax2, r_dv);
+      atomic_max_nonneg(&sc->vmax[0], r_v0);
+      atomic_max_nonneg(&sc->vmax[1], r_v1);
+      atomic_max_nonneg(&sc->vmax[2], r_v2);
+      part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = r_s;
     }
   }
 }
@@ -1298,7 +1214,8 @@ template <class T> static cudaError_t rhs_uhat_t(ch3d_ctx* c) {
   constexpr int TI = 16;
   T** f = (T**)c->f;
   const int P = c->Pv, Q = P - 1;
-  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) + 16;
+  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) +
+                (size_t)helm_set_stride(c->ny, P) * sizeof(T) + 16;
   static bool attr_set[2] = {false, false};
   auto kern = k_rhs_uhat<T, TI>;
   if (!attr_set[sizeof(T) == 4]) {
@@ -1359,34 +1276,27 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   static bool attr_set[2] = {false, false};
   if (!attr_set[sizeof(T) == 4]) {
     cudaFuncSetAttribute(k_zfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_ysolve2<T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_ysolve2<T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set[sizeof(T) == 4] = true;
   }
   dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int P = c->P, TS = c->TSy, Q = P - 1;
+  const dim3 gy((c->nxh + 127) / 128, c->nz);
   if (!c->fp32) {
-    const size_t smemy = (size_t)c->ny * TS * sizeof(double2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(double2) + 16;
-    dim3 gy((c->nxh + TS - 1) / TS, c->nz);
-    k_ysolve2<T, double><<<gy, TS * P < 64 ? 64 : TS * P, smemy, c->stream>>>(
-        make_geo<T>(c), c->m64full, (const double*)c->yRM, (const double*)c->yCP, (const double*)c->yIF, c->nxh,
-        (CT*)c->spec, TS, P, 0, 0, c->sc);
+    k_ythomas<T, double, false><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
+                                                           (const double*)c->yCP, c->nxh, (CT*)c->spec, nullptr, 0,
+                                                           0, 0, c->sc);
   } else {
     // mixed: FP32 systems and factors, except the low modes near kx = kz = 0 in FP64
-    const size_t smem32 = (size_t)c->ny * TS * sizeof(float2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(float2) + 16;
-    const size_t smem64 = (size_t)c->ny * TS * sizeof(double2) + (size_t)TS * 2 * (Q > 0 ? Q : 1) * sizeof(double2) + 16;
-    dim3 gy((c->nxh + TS - 1) / TS, c->nz);
-    k_ysolve2<T, float><<<gy, TS * P < 64 ? 64 : TS * P, smem32, c->stream>>>(
-        make_geo<T>(c), c->m64full, (const float*)c->yRM, (const float*)c->yCP, (const float*)c->yIF, c->nxh,
-        (CT*)c->spec, TS, P, 2, c->KL, c->sc);
+    k_ythomas<T, float, false><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const float*)c->yRM,
+                                                          (const float*)c->yCP, c->nxh, (CT*)c->spec, nullptr, 2,
+                                                          c->KL, c->TSy, c->sc);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 gl(1, 2 * c->KL + 1);
-    k_ysolve2<T, double><<<gl, TS * P < 64 ? 64 : TS * P, smem64, c->stream>>>(
-        make_geo<T>(c), c->m64full, c->yRM64, c->yCP64, c->yIF64, TS, (CT*)c->spec, TS, P, 1, c->KL, c->sc);
+    k_ythomas<T, double, true><<<dim3(1, 2 * c->KL + 1), 128, 0, c->stream>>>(
+        make_geo<T>(c), c->m64full, c->yRM64, c->yCP64, c->TSy, (CT*)c->spec, (double2*)c->ylow, 1, c->KL, c->TSy,
+        c->sc);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -1394,21 +1304,18 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   return cudaGetLastError();
 }
 template <class T> static cudaError_t yfactors_t(ch3d_ctx* c) {
-  const int TS = c->TSy, P = c->P;
-  const size_t sm = (size_t)TS * P * 4 * sizeof(double);
-  const int nthr = TS * P < 64 ? 64 : TS * P;
-  dim3 grid((c->nxh + TS - 1) / TS, c->nz / 2 + 1);
+  const dim3 g((c->nxh + 127) / 128, c->nz / 2 + 1);
   if (!c->fp32) {
-    k_ysolve_factors<T, double><<<grid, nthr, sm, c->stream>>>(make_geo<T>(c), c->m64full, c->wave, (double*)c->yRM,
-                                                               (double*)c->yCP, (double*)c->yIF, TS, P, c->nxh,
-                                                               c->nxh);
+    k_ythomas_factors<double><<<g, 128, 0, c->stream>>>(c->m64full, c->wave, c->nx, c->ny, (double*)c->yRM,
+                                                        (double*)c->yCP, c->nxh, c->nxh);
   } else {
-    k_ysolve_factors<T, float><<<grid, nthr, sm, c->stream>>>(make_geo<T>(c), c->m64full, c->wave, (float*)c->yRM,
-                                                              (float*)c->yCP, (float*)c->yIF, TS, P, c->nxh, c->nxh);
+    k_ythomas_factors<float><<<g, 128, 0, c->stream>>>(c->m64full, c->wave, c->nx, c->ny, (float*)c->yRM,
+                                                       (float*)c->yCP, c->nxh, c->nxh);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_ysolve_factors<T, double><<<dim3(1, c->KL + 1), nthr, sm, c->stream>>>(
-        make_geo<T>(c), c->m64full, c->wave, c->yRM64, c->yCP64, c->yIF64, TS, P, TS, c->nxh < TS ? c->nxh : TS);
+    k_ythomas_factors<double><<<dim3(1, c->KL + 1), 128, 0, c->stream>>>(c->m64full, c->wave, c->nx, c->ny, c->yRM64,
+                                                                        c->yCP64, c->TSy,
+                                                                        c->nxh < c->TSy ? c->nxh : c->TSy);
   }
   return cudaGetLastError();
 }

@@ -156,10 +156,14 @@ __device__ __forceinline__ void rhs4_uhat_body(const Geo<T>& g, const Metrics<T>
                                                const double* __restrict__ fac, int P, const T* __restrict__ ux,
                                                const T* __restrict__ uy, const T* __restrict__ uz,
                                                const T* __restrict__ pr, T* __restrict__ h, T* __restrict__ us,
-                                               int i0, int k, const DevScalars* __restrict__ sc, T* F, T* IF) {
+                                               int i0, int k, const DevScalars* __restrict__ sc, T* F, T* IF,
+                                               T* FS) {
   const int nx = g.nx, ny = g.ny, Q = P - 1;
   const int QQ = 2 * (Q > 0 ? Q : 1);
-  const double* FS = fac + (C == 1 ? helm_set_stride(ny, P) : 0);
+  {  // this component's Helmholtz factors, staged in shared memory
+    const double* FG = fac + (C == 1 ? helm_set_stride(ny, P) : 0);
+    for (int t = threadIdx.x; t < helm_set_stride(ny, P); t += blockDim.x) FS[t] = (T)FG[t];
+  }
   const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
   const T add = C == 0 ? (T)sc->dpmdxns : (T)0;
   const int tid = threadIdx.x;
@@ -218,9 +222,10 @@ __global__ void __launch_bounds__(256, 4) k_rhs4_uhat(Geo<T> g, Metrics<T> m, In
   const int i0 = (blockIdx.x / 3) * TI, k = blockIdx.y;
   T* F = (T*)smem_raw;
   T* IF = F + (size_t)g.ny * TI;
-  if (comp == 0) rhs4_uhat_body<T, 0, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hx, uxs, i0, k, sc, F, IF);
-  else if (comp == 1) rhs4_uhat_body<T, 1, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hy, uys, i0, k, sc, F, IF);
-  else rhs4_uhat_body<T, 2, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hz, uzs, i0, k, sc, F, IF);
+  T* FS = IF + (size_t)TI * 2 * (P > 1 ? P - 1 : 1);
+  if (comp == 0) rhs4_uhat_body<T, 0, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hx, uxs, i0, k, sc, F, IF, FS);
+  else if (comp == 1) rhs4_uhat_body<T, 1, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hy, uys, i0, k, sc, F, IF, FS);
+  else rhs4_uhat_body<T, 2, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hz, uzs, i0, k, sc, F, IF, FS);
 }
 
 // Block partial sums of (d11q1 + d33q1 + d22q1) * dyp over ux: the mean
@@ -279,7 +284,8 @@ template <class T> static cudaError_t rhs4_uhat_t(ch3d_ctx* c) {
   if (e != cudaSuccess) return e;
   T** f = (T**)c->f;
   const int P = c->Pv, Q = P - 1;
-  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) + 16;
+  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) +
+                (size_t)helm_set_stride(c->ny, P) * sizeof(T) + 16;
   static bool attr_set[2] = {false, false};
   auto kern = k_rhs4_uhat<T, TI>;
   if (!attr_set[sizeof(T) == 4]) {

@@ -107,6 +107,25 @@ class ChannelSolver:
         _lib.check(self.lib.ch3d_sgs_viscosity(self.ctx))
         return self.get_array(self.NUT)
 
+    def sgs_mlp_set(self, params, norm):
+        """Learned closure: network parameters (9414 FP32) and standardisation (52 FP32)."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        n = np.ascontiguousarray(norm, dtype=np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _lib.check(self.lib.ch3d_sgs_mlp_set(self.ctx, p.ctypes.data_as(fp), n.ctypes.data_as(fp)), self.lib)
+
+    def sgs_training_samples(self, fx, fy, fz):
+        """Box-filtered training samples of the current field: (X [n x 10], T [n x 6]) device tensors."""
+        import torch
+        nb = (self.cfg.nxc // fx) * (self.cfg.nyc // fy) * (self.cfg.nzc // fz)
+        dev = torch.device("cuda", self.cfg.device)
+        X = torch.empty((nb, 10), dtype=torch.float32, device=dev)
+        T = torch.empty((nb, 6), dtype=torch.float32, device=dev)
+        n = ctypes.c_longlong()
+        _lib.check(self.lib.ch3d_sgs_training_samples(self.ctx, fx, fy, fz, X.data_ptr(), T.data_ptr(),
+                                                      ctypes.byref(n)), self.lib)
+        return X[:n.value], T[:n.value]
+
     def stats_accumulate(self):
         _lib.check(self.lib.ch3d_stats_accumulate(self.ctx), self.lib)
 

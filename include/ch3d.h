@@ -60,6 +60,10 @@ extern "C" {
 #define CH3D_LES_MTS 3
 #define CH3D_LES_SMAG_VD 10     /* Smagorinsky + van Driest damping */
 #define CH3D_LES_MLP 11         /* learned closure, Smagorinsky fallback */
+/* standardisation of the learned closure: in_mean[10], in_std[10],
+   in_lo[10], in_hi[10] (training range of the standardised inputs),
+   out_mean[6], out_std[6] */
+#define CH3D_SGS_NORM_FLOATS 52
 
 /* Configuration: the namelist variables of &BasicParam, &ubulk_Param and
    &LesOptions (src/CFD_2nd/m_Parameters.f90:273-277,
@@ -159,7 +163,9 @@ CH3D_API int ch3d_stage(ch3d_ctx* ctx, int stage, int ns);
    3 pressure, 4 HistXOld, 5 HistYOld, 6 HistZOld, 7 RhsX, 8 RhsY,
    9 prphi (the pressure correction of the last clcPPE), 10 nut (LES: the
    total viscosity of Clc_SGS_Vis, xnu included), 11 RhsZ, 12..14 the
-   velocity after the Helmholtz solves (u*). */
+   velocity after the Helmholtz solves (u*), 15..20 (CH3D_LES_MLP, read
+   only) the SGS stresses tau_11 tau_12 tau_13 tau_22 tau_23 tau_33 at the
+   cell centres of the last ch3d_sgs_viscosity or step. */
 CH3D_API int ch3d_get_array(ch3d_ctx* ctx, int which, double* host);
 CH3D_API int ch3d_set_array(ch3d_ctx* ctx, int which, const double* host);
 
@@ -190,6 +196,26 @@ CH3D_API int ch3d_stats_fetch(ch3d_ctx* ctx, double* sumstat, int* nfstime,
    damping D = 1 - exp(-y+/26), y+ from the x-z mean wall shear of the first
    cells. */
 CH3D_API int ch3d_sgs_viscosity(ch3d_ctx* ctx);
+
+/* Learned closure (LES_type = CH3D_LES_MLP; no counterpart in the
+   reference): sets the network parameters (host FP32 array, CH3D_MLP_NPARAM
+   values in the layout of include/ch3d_mlp.h) and the standardisation (host,
+   CH3D_SGS_NORM_FLOATS values).  Network inputs per cell centre: the nine
+   velocity gradients du_i/dx_j in wall units (g xnu / u_tau^2, order dudx
+   dudy dudz dvdx dvdy dvdz dwdx dwdy dwdz) and y+; outputs: tau_11 tau_12
+   tau_13 tau_22 tau_23 tau_33 / u_tau^2.  Points whose standardised input
+   leaves [in_lo, in_hi] use the Smagorinsky / van Driest stress -2 nu_t S_ij.
+   Must be called before the first step. */
+CH3D_API int ch3d_sgs_mlp_set(ch3d_ctx* ctx, const float* params, const float* norm);
+
+/* Training samples of the learned closure from the current (DNS) field:
+   box filter over non-overlapping boxes of fx x fy x fz cells (volume
+   weighted in y); per box the nine filtered velocity gradients in wall units
+   and y+ (X, DEVICE, nbox x 10 FP32) and the subgrid stresses
+   tau_ij = <u_i u_j> - <u_i><u_j> of the cell-centre velocities divided by
+   u_tau^2 (T, DEVICE, nbox x 6 FP32), nbox = (nxc/fx) (nyc/fy) (nzc/fz).
+   *nbox receives the count; X and T must hold that many rows. */
+CH3D_API int ch3d_sgs_training_samples(ch3d_ctx* ctx, int fx, int fy, int fz, float* X, float* T, long long* nbox);
 
 /* Device bytes held by the context. */
 CH3D_API int ch3d_memory_bytes(ch3d_ctx* ctx, long long* bytes);

@@ -1078,7 +1078,58 @@ struct Oracle {
     if (P.LES_type == 2) Clc_SGS_WALE();
     else if (P.LES_type == 3) Clc_SGS_MTS();
     else if (P.LES_type == 10) Clc_SGS_SmagVD();
+    else if (P.LES_type == 11) {  // learned closure: molecular viscosity, explicit stress force
+      for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) for (int ic = 1; ic <= nxc; ++ic)
+        nut(ic, jc, kc) = P.xnu;
+    }
     SetBC_and_UpdateHalo_SGS();
+  }
+
+  // Learned closure (no counterpart in the reference; the discretisation of
+  // channel3d_b200/csrc/ch3d_les.cu k_sgs_force): the force -d tau_ij/dx_j of
+  // cell-centred stresses set by the test (sgs_tau, 6 interior arrays) at the
+  // staggered velocity points; off-diagonal stresses averaged onto the cell
+  // edges from the four neighbouring cells, zero on the walls.
+  std::vector<double> sgs_tau, sgs_f;
+  void SgsForce() {
+    const size_t N = (size_t)nxc * nyc * nzc;
+    sgs_f.assign(3 * N, 0.0);
+    if (sgs_tau.size() != 6 * N) return;
+    auto T = [&](int q, int i, int j, int k) {  // periodic i, k; 1-based
+      i = (i - 1 + nxc) % nxc; k = (k - 1 + nzc) % nzc;
+      return sgs_tau[q * N + (size_t)i + (size_t)nxc * ((size_t)(j - 1) + (size_t)nyc * k)];
+    };
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          const int im = ic - 1, ip = ic + 1, km = kc - 1, kp = kc + 1, jm = jc - 1, jp = jc + 1;
+          const size_t o = (size_t)(ic - 1) + (size_t)nxc * ((size_t)(jc - 1) + (size_t)nyc * (kc - 1));
+          // x momentum at (i-1/2, j, k)
+          double t12u = jc == nyc ? 0.0 : 0.25 * (T(1, im, jc, kc) + T(1, ic, jc, kc) + T(1, im, jp, kc) + T(1, ic, jp, kc));
+          double t12d = jc == 1 ? 0.0 : 0.25 * (T(1, im, jm, kc) + T(1, ic, jm, kc) + T(1, im, jc, kc) + T(1, ic, jc, kc));
+          double t13p = 0.25 * (T(2, im, jc, kc) + T(2, ic, jc, kc) + T(2, im, jc, kp) + T(2, ic, jc, kp));
+          double t13m = 0.25 * (T(2, im, jc, km) + T(2, ic, jc, km) + T(2, im, jc, kc) + T(2, ic, jc, kc));
+          sgs_f[o] = -((T(0, ic, jc, kc) - T(0, im, jc, kc)) * rdx + (t12u - t12d) * rdyp(jc) + (t13p - t13m) * rdz);
+          // y momentum at (i, j-1/2, k); the wall row is fixed by the wall condition
+          if (jc > 1) {
+            double t12p = 0.25 * (T(1, ic, jm, kc) + T(1, ip, jm, kc) + T(1, ic, jc, kc) + T(1, ip, jc, kc));
+            double t12m = 0.25 * (T(1, im, jm, kc) + T(1, ic, jm, kc) + T(1, im, jc, kc) + T(1, ic, jc, kc));
+            double t23p = 0.25 * (T(4, ic, jm, kc) + T(4, ic, jm, kp) + T(4, ic, jc, kc) + T(4, ic, jc, kp));
+            double t23m = 0.25 * (T(4, ic, jm, km) + T(4, ic, jm, kc) + T(4, ic, jc, km) + T(4, ic, jc, kc));
+            sgs_f[N + o] = -((t12p - t12m) * rdx + (T(3, ic, jc, kc) - T(3, ic, jm, kc)) * rdyc(jc) + (t23p - t23m) * rdz);
+          }
+          // z momentum at (i, j, k-1/2)
+          double t13p2 = 0.25 * (T(2, ic, jc, km) + T(2, ip, jc, km) + T(2, ic, jc, kc) + T(2, ip, jc, kc));
+          double t13m2 = 0.25 * (T(2, im, jc, km) + T(2, ic, jc, km) + T(2, im, jc, kc) + T(2, ic, jc, kc));
+          double t23u = jc == nyc ? 0.0 : 0.25 * (T(4, ic, jc, km) + T(4, ic, jc, kc) + T(4, ic, jp, km) + T(4, ic, jp, kc));
+          double t23d = jc == 1 ? 0.0 : 0.25 * (T(4, ic, jm, km) + T(4, ic, jm, kc) + T(4, ic, jc, km) + T(4, ic, jc, kc));
+          sgs_f[2 * N + o] = -((t13p2 - t13m2) * rdx + (t23u - t23d) * rdyp(jc) + (T(5, ic, jc, kc) - T(5, ic, jc, km)) * rdz);
+        }
+  }
+  double sgsf(int q, int ic, int jc, int kc) const {
+    if (sgs_f.empty()) return 0.0;
+    const size_t N = (size_t)nxc * nyc * nzc;
+    return sgs_f[q * N + (size_t)(ic - 1) + (size_t)nxc * ((size_t)(jc - 1) + (size_t)nyc * (kc - 1))];
   }
 
   // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:80-156 (clcRhsX_PIMP_LES) ----
@@ -1114,7 +1165,7 @@ struct Oracle {
           double dcq13 = d11q1 + d33q1;
           double gradp1 = (pressure(ic, jc, kc) - pressure(im, jc, kc)) * rdx;
           s1tot = s1tot + ux(ic, jc, kc) * s1totCoe;
-          double convEd1 = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[0];
+          double convEd1 = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[0] + sgsf(0, ic, jc, kc);
           RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1 + two * pmBetaT * d22q1;
           Hist(ic, jc, kc) = convEd1;
         }
@@ -1163,7 +1214,7 @@ struct Oracle {
           double d33q2 = ap3c(kc) * visd * (uy(ic, jc, kp) - uy(ic, jc, kc)) - am3c(kc) * visc * (uy(ic, jc, kc) - uy(ic, jc, km));
           double dcq13 = d11q2 + d33q2;
           double gradp2 = (pressure(ic, jc, kc) - pressure(ic, jm, kc)) * sucac;
-          double convEd2 = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[1];
+          double convEd2 = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[1] + sgsf(1, ic, jc, kc);
           RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2 + two * pmBetaT * d22q2;
           Hist(ic, jc, kc) = convEd2;
         }
@@ -1200,7 +1251,7 @@ struct Oracle {
           double d33q3 = sgs3;
           double dcq13 = d11q3 + d33q3;
           double gradp3 = (pressure(ic, jc, kc) - pressure(ic, jc, km)) * rdz;
-          double convEd3 = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[2];
+          double convEd3 = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[2] + sgsf(2, ic, jc, kc);
           RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3 + two * pmBetaT * d22q3;
           Hist(ic, jc, kc) = convEd3;
         }
@@ -1881,6 +1932,16 @@ double orc_sgs(void* h) {
   o->utau_last = 0;
   o->Clc_SGS_Vis();
   return o->utau_last;
+}
+
+// learned closure: cell-centred SGS stresses (6 interior arrays, or NULL to
+// clear) whose divergence the LES right-hand sides add
+void orc_set_sgs_tau(void* h, const double* tau) {
+  Oracle* o = (Oracle*)h;
+  const size_t N = (size_t)o->nxc * o->nyc * o->nzc;
+  if (!tau) { o->sgs_tau.clear(); o->sgs_f.clear(); return; }
+  o->sgs_tau.assign(tau, tau + 6 * N);
+  o->SgsForce();
 }
 
 int orc_num_threads(void) {

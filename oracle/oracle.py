@@ -88,6 +88,7 @@ def lib():
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_sgs.restype = ctypes.c_double
         L.orc_sgs.argtypes = [ctypes.c_void_p]
+        L.orc_set_sgs_tau.argtypes = [ctypes.c_void_p, _DP]
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
@@ -213,6 +214,15 @@ class Oracle:
         """Clc_SGS_Vis on the current state: nut (interior) and u_tau."""
         ut = self.L.orc_sgs(self.h)
         return self.get_interior(self.NUT), ut
+
+    def set_sgs_tau(self, tau):
+        """Learned closure: cell-centred SGS stresses (6, nzc, nyc, nxc) whose divergence the LES RHS adds."""
+        if tau is None:
+            self.L.orc_set_sgs_tau(self.h, None)
+            return
+        t = np.ascontiguousarray(tau, dtype=np.float64)
+        assert t.size == 6 * self.cfg.nxc * self.cfg.nyc * self.cfg.nzc
+        self.L.orc_set_sgs_tau(self.h, _p(t))
 
     def stats_accumulate(self):
         self.L.orc_stats_accumulate(self.h)

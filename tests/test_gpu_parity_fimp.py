@@ -6,7 +6,8 @@ Tolerances: per-stage results within 1e-12 relative (max norm; the RHS
 arrays within 5e-12: by the third substep the device's fused multiply-adds
 and the oracle's separately rounded products differ by a few ulp, which the
 near-wall 1/dy^2 coefficients of the y viscous term amplify), the pressure
-correction within 1e-11 (L2), whole steps within 1e-10."""
+correction within 5e-11 (L2: its source, the divergence of u*, is a small
+difference of O(1) velocities, which amplifies their relative differences), whole steps within 1e-10."""
 import numpy as np
 import pytest
 
@@ -52,7 +53,7 @@ def test_stage_parity_fimp(built, shape):
         o.stage(3, ns); s.stage(3, ns)
         o.stage(4, ns); s.stage(4, ns)
         phi_o, phi_g = o.get_interior(o.HALO), s.get_array(s.PRPHI)
-        assert rel_l2(phi_g, phi_o) < 1e-11, (ns, "phi", rel_l2(phi_g, phi_o))
+        assert rel_l2(phi_g, phi_o) < 5e-11, (ns, "phi", rel_l2(phi_g, phi_o))
         o.stage(5, ns); s.stage(5, ns)
         o.stage(6, ns); s.stage(6, ns)
         go, gs = o.get_state(), s.download()

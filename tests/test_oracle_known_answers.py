@@ -101,7 +101,7 @@ def test_laminar_stays_laminar(built):
 def test_nan_field_is_skipped_by_the_reference_limit_checks(built):
     """The reference's maxima (`if(udiv>divmax1)`, m_Tools.f90:70; CalcVmax :93-98)
     skip NaN, so a NaN field does not trip div_limit/vel_limit there; the GPU
-    path deliberately propagates NaN and trips (tests/test_gpu_failures.py)."""
+    path folds NaN into +inf and trips (tests/test_gpu_failures.py)."""
     from channel3d_b200 import initfield
     from oracle import oracle as O
     cfg = small_channel(16, 12, 8)

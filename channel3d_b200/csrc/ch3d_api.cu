@@ -358,6 +358,14 @@ void host_fill_ghosts(const ch3d_ctx* c, int layout, double* a, int comp) {
 
 template <class T>
 int upload_field(ch3d_ctx* c, int q, int layout, const double* a, int comp) {
+  if (sizeof(T) == sizeof(double) && layout == CH3D_LAYOUT_INTERIOR) {
+    // FP64 interior arrays are the device layout: one copy (DMA from pinned memory), then the uy wall row
+    if (a) CU(cudaMemcpyAsync(c->f[q], a, (size_t)c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    else CU(cudaMemsetAsync(c->f[q], 0, (size_t)c->N * sizeof(double), c->stream));
+    if (comp == 1) CU(launch_fill_row0(c, q, c->cfg.uyBcValue[2]));  // uy(ic,1,kc) = uy_ym
+    CU(cudaStreamSynchronize(c->stream));
+    return CH3D_OK;
+  }
   std::vector<T> h((size_t)c->N);
   size_t n = 0;
   for (int k = 1; k <= c->nz; ++k)
@@ -374,6 +382,11 @@ int upload_field(ch3d_ctx* c, int q, int layout, const double* a, int comp) {
 
 template <class T>
 int download_field(ch3d_ctx* c, int q, int layout, double* a, int comp) {
+  if (sizeof(T) == sizeof(double) && layout == CH3D_LAYOUT_INTERIOR) {
+    CU(cudaMemcpyAsync(a, c->f[q], (size_t)c->N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return CH3D_OK;
+  }
   std::vector<T> h((size_t)c->N);
   CU(cudaMemcpyAsync(h.data(), c->f[q], h.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));

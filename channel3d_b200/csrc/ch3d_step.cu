@@ -809,63 +809,128 @@ template <> struct Vec2Of<double> { typedef double2 type; };
 template <> struct Vec2Of<float> { typedef float2 type; };
 
 // Poisson y solve, Thomas across threads: one thread per (kx, kz) column,
-// a warp covers 32 consecutive kx (coalesced rows of the (kx, j, kz)
-// spectrum).  The forward sweep keeps d_j in place in the spectrum (or, for
-// the FP64 low modes of the mixed path, in an FP64 scratch column), the
-// backward sweep overwrites it with the solution.
-// sel 0: every column; 1: only the low modes kx < KX, |kz| <= KL (grid.y
-// enumerates kz = 0..KL, nz-KL..nz-1); 2: every column but those.
-template <class T, class R, bool SCR>
+// threads numbered kx fastest so that a warp reads 32 consecutive kx of one
+// row of the (kx, j, kz) spectrum.  The forward sweep keeps d_j in place in
+// the spectrum (the FP64 low modes of the mixed path in an FP64 scratch
+// array, layout [j][low column]), the backward sweep overwrites it with the
+// solution.  Rows are processed in batches of YB: the batch's loads are all
+// issued before its dependent recurrence, so YB rows of every column are in
+// flight at once.
+constexpr int YB = 8;
+
+template <class R, class CT, class LD, class ST, class STD, class LDD>
+__device__ __forceinline__ void thomas_column(int ny, bool pin, const R* __restrict__ rm, const R* __restrict__ cp,
+                                              size_t fst, const double* __restrict__ am, LD load, ST store,
+                                              STD store_d, LDD load_d) {
+  R dx = (R)0, dy = (R)0;
+  for (int j0 = 0; j0 < ny; j0 += YB) {
+    R fx[YB], fy[YB], r[YB], a[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j < ny) {
+        const CT f = load(j);
+        fx[u] = (R)f.x; fy[u] = (R)f.y;
+        r[u] = __ldg(rm + fst * j);
+        a[u] = (R)__ldg(am + j + 1);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j < ny) {
+        if (j == 0) {
+          dx = pin ? (R)0 : fx[u] * r[u];
+          dy = pin ? (R)0 : fy[u] * r[u];
+        } else {
+          dx = (fx[u] - a[u] * dx) * r[u];
+          dy = (fy[u] - a[u] * dy) * r[u];
+        }
+        store_d(j, dx, dy);
+      }
+    }
+  }
+  store(ny - 1, dx, dy);
+  for (int j1 = ny - 2; j1 >= 0; j1 -= YB) {
+    R ex[YB], ey[YB], c[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j1 - u;
+      if (j >= 0) {
+        const CT v = load_d(j);
+        ex[u] = (R)v.x; ey[u] = (R)v.y;
+        c[u] = __ldg(cp + fst * j);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j1 - u;
+      if (j >= 0) {
+        dx = ex[u] - c[u] * dx;
+        dy = ey[u] - c[u] * dy;
+        store(j, dx, dy);
+      }
+    }
+  }
+}
+
+// FP64 path: every column in FP64 (sel 0).
+template <class T, class R>
 __global__ void __launch_bounds__(128) k_ythomas(Geo<T> g, Metrics<double> m, const R* __restrict__ RMf,
-                                                 const R* __restrict__ CPf, int ldx,
-                                                 typename CplxOf<T>::type* __restrict__ spec,
-                                                 typename Vec2Of<R>::type* __restrict__ scr, int sel, int KL, int KX,
+                                                 const R* __restrict__ CPf, typename CplxOf<T>::type* __restrict__ spec,
                                                  const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
-  typedef typename Vec2Of<R>::type V2;
   if (sc->status) return;
   const int nxh = g.nxh, ny = g.ny, nz = g.nz;
-  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int kz = sel == 1 ? ((int)blockIdx.y <= KL ? (int)blockIdx.y : nz - ((int)blockIdx.y - KL)) : (int)blockIdx.y;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nxh * nz) return;
+  const int kx = (int)(t % nxh), kz = (int)(t / nxh);
   const int kzh = kz <= nz - kz ? kz : nz - kz;
-  if (kx >= nxh || (sel == 1 && kx >= KX)) return;
-  if (sel == 2 && kx < KX && kzh <= KL) return;
-  const R* rm = RMf + (size_t)kzh * ny * ldx + kx;
-  const R* cp = CPf + (size_t)kzh * ny * ldx + kx;
-  CT* col = spec + kx + (size_t)nxh * ny * kz;
-  V2* w = SCR ? scr + ((size_t)blockIdx.y * KX + kx) * ny : nullptr;
   const size_t st = (size_t)nxh;
+  CT* col = spec + kx + st * ny * kz;
+  const R* rm = RMf + (size_t)kzh * ny * st + kx;
+  const R* cp = CPf + (size_t)kzh * ny * st + kx;
+  auto load = [&](int j) { return col[st * j]; };
+  auto store = [&](int j, R x, R y) { col[st * j] = mk((T)x, (T)y); };
+  thomas_column<R, CT>(ny, kx == 0 && kz == 0, rm, cp, st, m.am2Pr, load, store, store, load);
+}
+
+// Mixed path: FP32 sweeps with FP32 factors, except the low modes kx < KX,
+// |kz| <= KL, solved in FP64 with FP64 factors and the FP64 scratch.
+template <class T>
+__global__ void __launch_bounds__(128) k_ythomas_mixed(Geo<T> g, Metrics<double> m, const float* __restrict__ RM32,
+                                                       const float* __restrict__ CP32,
+                                                       const double* __restrict__ RM64,
+                                                       const double* __restrict__ CP64,
+                                                       typename CplxOf<T>::type* __restrict__ spec,
+                                                       double2* __restrict__ scr, int KL, int KX,
+                                                       const DevScalars* __restrict__ sc) {
+  typedef typename CplxOf<T>::type CT;
+  if (sc->status) return;
+  const int nxh = g.nxh, ny = g.ny, nz = g.nz;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nxh * nz) return;
+  const int kx = (int)(t % nxh), kz = (int)(t / nxh);
+  const int kzh = kz <= nz - kz ? kz : nz - kz;
+  const size_t st = (size_t)nxh;
+  CT* col = spec + kx + st * ny * kz;
   const bool pin = (kx == 0 && kz == 0);
-  R dx, dy;
-  {
-    const CT f = col[0];
-    const R r = rm[0];
-    dx = pin ? (R)0 : (R)f.x * r;
-    dy = pin ? (R)0 : (R)f.y * r;
-    if (SCR) { V2 v; v.x = dx; v.y = dy; w[0] = v; }
-    else col[0] = mk((T)dx, (T)dy);
+  auto load = [&](int j) { return col[st * j]; };
+  if (kx < KX && kzh <= KL) {
+    const int zi = kz <= KL ? kz : KL + (nz - kz);  // 0..2KL
+    const size_t nlow = (size_t)(2 * KL + 1) * KX;
+    double2* w = scr + (size_t)zi * KX + kx;         // [j][low column]
+    auto store = [&](int j, double x, double y) { col[st * j] = mk((T)x, (T)y); };
+    auto store_d = [&](int j, double x, double y) { w[nlow * j] = make_double2(x, y); };
+    auto load_d = [&](int j) { return w[nlow * j]; };
+    thomas_column<double, double2>(ny, pin, RM64 + (size_t)kzh * ny * KX + kx, CP64 + (size_t)kzh * ny * KX + kx,
+                                   (size_t)KX, m.am2Pr, [&](int j) { const CT v = load(j); return make_double2(v.x, v.y); },
+                                   store, store_d, load_d);
+    return;
   }
-#pragma unroll 4
-  for (int j = 1; j < ny; ++j) {
-    const R a = (R)m.am2Pr[j + 1];
-    const CT f = col[st * j];
-    const R r = rm[(size_t)ldx * j];
-    dx = ((R)f.x - a * dx) * r;
-    dy = ((R)f.y - a * dy) * r;
-    if (SCR) { V2 v; v.x = dx; v.y = dy; w[j] = v; }
-    else col[st * j] = mk((T)dx, (T)dy);
-  }
-  col[st * (ny - 1)] = mk((T)dx, (T)dy);
-#pragma unroll 4
-  for (int j = ny - 2; j >= 0; --j) {
-    const R c = cp[(size_t)ldx * j];
-    R ex, ey;
-    if (SCR) { const V2 v = w[j]; ex = v.x; ey = v.y; }
-    else { const CT v = col[st * j]; ex = (R)v.x; ey = (R)v.y; }
-    dx = ex - c * dx;
-    dy = ey - c * dy;
-    col[st * j] = mk((T)dx, (T)dy);
-  }
+  auto store = [&](int j, float x, float y) { col[st * j] = mk((T)x, (T)y); };
+  thomas_column<float, CT>(ny, pin, RM32 + (size_t)kzh * ny * st + kx, CP32 + (size_t)kzh * ny * st + kx, st, m.am2Pr,
+                           load, store, store, load);
 }
 
 // ---------------------------------------------------------------------------
@@ -1282,21 +1347,15 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const dim3 gy((c->nxh + 127) / 128, c->nz);
+  const unsigned gy = (unsigned)(((long long)c->nxh * c->nz + 127) / 128);
   if (!c->fp32) {
-    k_ythomas<T, double, false><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
-                                                           (const double*)c->yCP, c->nxh, (CT*)c->spec, nullptr, 0,
-                                                           0, 0, c->sc);
+    k_ythomas<T, double><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
+                                                    (const double*)c->yCP, (CT*)c->spec, c->sc);
   } else {
     // mixed: FP32 systems and factors, except the low modes near kx = kz = 0 in FP64
-    k_ythomas<T, float, false><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const float*)c->yRM,
-                                                          (const float*)c->yCP, c->nxh, (CT*)c->spec, nullptr, 2,
-                                                          c->KL, c->TSy, c->sc);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    k_ythomas<T, double, true><<<dim3(1, 2 * c->KL + 1), 128, 0, c->stream>>>(
-        make_geo<T>(c), c->m64full, c->yRM64, c->yCP64, c->TSy, (CT*)c->spec, (double2*)c->ylow, 1, c->KL, c->TSy,
-        c->sc);
+    k_ythomas_mixed<T><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const float*)c->yRM,
+                                                  (const float*)c->yCP, c->yRM64, c->yCP64, (CT*)c->spec,
+                                                  (double2*)c->ylow, c->KL, c->TSy, c->sc);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -1373,6 +1432,19 @@ template <class T> static cudaError_t divmax_t(ch3d_ctx* c, unsigned long long* 
   k_divmax<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], slot);
   return cudaGetLastError();
 }
+template <class T> __global__ void k_fill_row0(T* __restrict__ a, int nx, int ny, int nz, T v) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * nz) return;
+  const int i = (int)(t % nx), k = (int)(t / nx);
+  a[i + (long long)nx * ny * k] = v;
+}
+cudaError_t launch_fill_row0(ch3d_ctx* c, int q, double v) {
+  const unsigned nb = (unsigned)(((long long)c->nx * c->nz + 255) / 256);
+  if (c->fp32) k_fill_row0<float><<<nb, 256, 0, c->stream>>>((float*)c->f[q], c->nx, c->ny, c->nz, (float)v);
+  else k_fill_row0<double><<<nb, 256, 0, c->stream>>>((double*)c->f[q], c->nx, c->ny, c->nz, v);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot) {
   return c->fp32 ? divmax_t<float>(c, slot) : divmax_t<double>(c, slot);
 }

@@ -154,3 +154,127 @@ def profile_errors(p, ref, yp, yref):
         r = np.interp(yc, yr, ref[k])
         out[k] = float(np.linalg.norm(p[k] - r) / max(np.linalg.norm(r), 1e-30))
     return out
+
+
+def box_filtered_profiles(fields, cfg, box):
+    """Mean and rms profiles of the box-filtered cell-centre velocities
+    (the filtered-DNS reference of the LES), on the box-row centres."""
+    fx, fy, fz = box
+    from .config import mesh_y
+    yp = mesh_y(cfg)
+    dyp = np.diff(yp)
+    ux, uy, uz = fields["ux"], fields["uy"], fields["uz"]
+    uc = 0.5 * (ux + np.roll(ux, -1, axis=2))
+    vn = np.concatenate([uy, np.zeros_like(uy[:, :1, :])], axis=1)
+    vc = 0.5 * (vn[:, :-1, :] + vn[:, 1:, :])
+    wc = 0.5 * (uz + np.roll(uz, -1, axis=0))
+    w = np.broadcast_to(dyp[None, :, None], uc.shape)
+    sh = (cfg.nzc // fz, fz, cfg.nyc // fy, fy, cfg.nxc // fx, fx)
+    ws = w.reshape(sh).sum(axis=(1, 3, 5))
+    out = {}
+    for name, a in (("u", uc), ("v", vc), ("w", wc)):
+        b = (a * w).reshape(sh).sum(axis=(1, 3, 5)) / ws       # box means
+        m = b.mean(axis=(0, 2))
+        out[name + "mean"] = m
+        out[name + "rms"] = np.sqrt(((b - m[None, :, None]) ** 2).mean(axis=(0, 2)))
+    yb = np.array([0.5 * (yp[j * fy] + yp[(j + 1) * fy]) for j in range(cfg.nyc // fy)])
+    return {"y": yb, "U": out["umean"], "urms": out["urms"], "vrms": out["vrms"], "wrms": out["wrms"]}
+
+
+def evaluate(dns_cfg, les_cfg, dns_warm, dns_steps, n_snapshots, per_snapshot, les_steps, les_avg_from,
+             box=(4, 2, 4), train_iters=3000, batch=65536, lr=1e-3, n_profile_snapshots=10, seed=0, log=print):
+    """The learned-closure experiment end to end on one GPU: DNS with
+    box-filtered snapshots, training, and LES runs with the learned closure
+    and with the Smagorinsky / van Driest model from the same seeded start.
+    Returns a report dict (profiles, errors against the filtered DNS,
+    a-priori stress errors, LES cost per step)."""
+    import time
+    import torch
+    from .config import mesh_y
+    rep = {"box": list(box)}
+    t0 = time.time()
+    s = ChannelSolver(dns_cfg)
+    s.upload(*initfield.laminar_noise(dns_cfg, yp=s.yp, seed=seed))
+    s.project()
+    s.step(dns_warm)
+    log("dns warm-up %d steps: %.1f s" % (dns_warm, time.time() - t0))
+    X, T, D, s = collect_samples(dns_cfg, dns_steps, n_snapshots, per_snapshot, box=box, seed=seed, solver=s)
+    log("dns sampling %d snapshots: %d samples, %.1f s" % (n_snapshots, X.shape[0], time.time() - t0))
+    # filtered-DNS reference profiles: a few more snapshots after the sampling window
+    prof = []
+    every = max(1, dns_steps // n_snapshots)
+    for _ in range(n_profile_snapshots):
+        s.step(every)
+        prof.append(box_filtered_profiles(s.download(), dns_cfg, box))
+    ref = {k: np.mean([p[k] for p in prof], axis=0) for k in prof[0]}
+    s.close()
+    # train / hold-out split by snapshot
+    nho = max(1, n_snapshots // 10) * per_snapshot
+    Xtr, Ttr, Xte, Tte, Dte = X[:-nho], T[:-nho], X[-nho:], T[-nho:], D[-nho:]
+    norm = fit_norm(Xtr, Ttr)
+    net, hist = train(Xtr, Ttr, norm, iters=train_iters, batch=batch, lr=lr, seed=seed, log_every=max(1, train_iters // 20))
+    rep["train_loss"] = hist
+    rep["a_priori"] = {"mlp": stress_error(predict(net, Xte, norm), Tte),
+                       "smagorinsky_vd": stress_error(smagorinsky(Xte, Dte, les_cfg.Cs), Tte)}
+    log("a priori stress errors: %s (%.1f s)" % (rep["a_priori"], time.time() - t0))
+    params = net.params().astype(np.float32)
+    del X, T, D, Xtr, Ttr
+    torch.cuda.empty_cache()
+    # LES runs from the same seeded start
+    yl = mesh_y(les_cfg)
+    rep["les"] = {}
+    for name, lt in (("mlp", 11), ("smagorinsky_vd", 10)):
+        cfg = les_cfg.copy(LES_type=lt)
+        ls = ChannelSolver(cfg)
+        ls.upload(*initfield.laminar_noise(cfg, yp=ls.yp, seed=seed))
+        ls.project()
+        if lt == 11:
+            ls.sgs_mlp_set(params, norm)
+        info = ls.step(les_avg_from, raise_on_diverge=False)
+        acc, n, ms = None, 0, 0.0
+        while info["status"] == 0 and info["itime"] < les_steps:
+            info = ls.step(min(100, les_steps - info["itime"]), raise_on_diverge=False)
+            ms += ls.last_step_ms()
+            p = profiles(ls.download(), cfg)
+            acc = p if acc is None else {k: acc[k] + p[k] for k in acc}
+            n += 1
+        r = {"status": info["status"], "steps": info["itime"], "ms_per_step": ms / max(1, info["itime"] - les_avg_from)}
+        if acc is not None:
+            pm = {k: v / n for k, v in acc.items()}
+            yc = 0.5 * (yl[1:] + yl[:-1])
+            errs = {}
+            for k in ("U", "urms", "vrms", "wrms"):
+                rr = np.interp(yc, ref["y"], ref[k])
+                errs[k] = float(np.linalg.norm(pm[k] - rr) / max(np.linalg.norm(rr), 1e-30))
+            r["profile_errors"] = errs
+            r["profiles"] = {k: v.tolist() for k, v in pm.items()}
+        rep["les"][name] = r
+        ls.close()
+        log("les %s: %s (%.1f s)" % (name, {k: v for k, v in r.items() if k != "profiles"}, time.time() - t0))
+    rep["reference_profiles"] = {k: v.tolist() for k, v in ref.items()}
+    return rep
+
+
+def main():
+    import argparse
+    import json
+    from . import workloads
+    ap = argparse.ArgumentParser(description="learned SGS closure: DNS sampling, training, LES comparison")
+    ap.add_argument("--out", default="les_closure_report.json")
+    ap.add_argument("--dns-warm", type=int, default=16000)
+    ap.add_argument("--dns-steps", type=int, default=4000)
+    ap.add_argument("--snapshots", type=int, default=400)
+    ap.add_argument("--per-snapshot", type=int, default=16384)
+    ap.add_argument("--les-steps", type=int, default=20000)
+    ap.add_argument("--les-avg-from", type=int, default=4000)
+    ap.add_argument("--train-iters", type=int, default=3000)
+    args = ap.parse_args()
+    dns, _ = workloads.get("channel256x192x256_re13750")
+    les, _ = workloads.get("channel48_les", LES_type=10, Cs=0.1)
+    rep = evaluate(dns, les, args.dns_warm, args.dns_steps, args.snapshots, args.per_snapshot, args.les_steps,
+                   args.les_avg_from, train_iters=args.train_iters)
+    json.dump(rep, open(args.out, "w"))
+
+
+if __name__ == "__main__":
+    main()

@@ -38,3 +38,40 @@ def laminar_noise(cfg, amplitude=0.1, seed=SEED, yp=None, ubulk=1.0):
     uz *= amplitude * ubulk
     p = np.zeros(shape)
     return ux, uy, uz, p
+
+
+def large_scale(cfg, amplitude=0.3, seed=SEED, yp=None, ubulk=1.0, kmax=4):
+    """Laminar profile plus large-scale perturbations that trigger transition:
+    a sum of Fourier modes |kx|, |kz| <= kmax (random phases and amplitudes
+    from the seeded generator) shaped by (1 - (y-1)^2) so that they vanish at
+    the walls, scaled to `amplitude` * U_b in max norm per component.  The
+    field is not divergence-free; ChannelSolver.project() makes it so.  (The
+    white-noise start of laminar_noise decays on fine grids.)"""
+    if yp is None:
+        yp = mesh_y(cfg)
+    yc = cell_centres(yp)
+    rng = np.random.Generator(np.random.Philox(key=seed + 1))
+    nz, ny, nx = cfg.shape
+    x = (np.arange(nx) + 0.5) * cfg.xlx / nx
+    z = (np.arange(nz) + 0.5) * cfg.zlz / nz
+    eta = yc / (0.5 * cfg.yly) - 1.0
+    env = (1.0 - eta ** 2)
+    prof = 1.5 * ubulk * env
+    out = []
+    for comp in range(3):
+        f = np.zeros((nz, ny, nx))
+        for kx in range(0, kmax + 1):
+            for kz in range(-kmax, kmax + 1):
+                if kx == 0 and kz == 0:
+                    continue
+                a, ph, ny_mode = rng.uniform(0.5, 1.0), rng.uniform(0, 2 * np.pi), rng.integers(1, 4)
+                wave = np.cos(2 * np.pi * (kx * x[None, :] / cfg.xlx + kz * z[:, None] / cfg.zlz) + ph)
+                yshape = env * np.sin(ny_mode * np.pi * (eta + 1.0) / 2.0 + rng.uniform(0, np.pi))
+                f += a * wave[:, None, :] * yshape[None, :, None]
+        f *= amplitude * ubulk / max(np.abs(f).max(), 1e-30)
+        out.append(f)
+    ux = out[0] + prof[None, :, None]
+    uy = out[1]
+    uy[:, 0, :] = 0.0
+    uz = out[2]
+    return ux, uy, uz, np.zeros((nz, ny, nx))

@@ -182,7 +182,8 @@ def box_filtered_profiles(fields, cfg, box):
 
 
 def evaluate(dns_cfg, les_cfg, dns_warm, dns_steps, n_snapshots, per_snapshot, les_steps, les_avg_from,
-             box=(4, 2, 4), train_iters=3000, batch=65536, lr=1e-3, n_profile_snapshots=10, seed=0, log=print):
+             box=(4, 2, 4), train_iters=3000, batch=65536, lr=1e-3, n_profile_snapshots=10, seed=0, log=print,
+             turbulent_start=0.0, warm_dt=None):
     """The learned-closure experiment end to end on one GPU: DNS with
     box-filtered snapshots, training, and LES runs with the learned closure
     and with the Smagorinsky / van Driest model from the same seeded start.
@@ -193,10 +194,27 @@ def evaluate(dns_cfg, les_cfg, dns_warm, dns_steps, n_snapshots, per_snapshot, l
     from .config import mesh_y
     rep = {"box": list(box)}
     t0 = time.time()
-    s = ChannelSolver(dns_cfg)
-    s.upload(*initfield.laminar_noise(dns_cfg, yp=s.yp, seed=seed))
-    s.project()
-    s.step(dns_warm)
+    if turbulent_start > 0:
+        # large-scale start, warm-up in the mixed path with a larger time step,
+        # then the state continues in FP64 with the sampling time step
+        wcfg = dns_cfg.copy(precision="mixed", dtMax=warm_dt or dns_cfg.dtMax)
+        w = ChannelSolver(wcfg)
+        w.upload(*initfield.large_scale(wcfg, amplitude=turbulent_start, yp=w.yp, seed=seed))
+        w.project()
+        for _ in range(max(1, dns_warm // 1000)):
+            info = w.step(min(1000, dns_warm))
+        st = w.download()
+        log("dns warm-up (mixed, dt %g) %d steps: u' max %.3f, %.1f s"
+            % (wcfg.dtMax, info["itime"], float(np.abs(st["uy"]).max()), time.time() - t0))
+        w.close()
+        s = ChannelSolver(dns_cfg)
+        s.upload(st["ux"], st["uy"], st["uz"], st["p"])
+        s.project()
+    else:
+        s = ChannelSolver(dns_cfg)
+        s.upload(*initfield.laminar_noise(dns_cfg, yp=s.yp, seed=seed))
+        s.project()
+        s.step(dns_warm)
     log("dns warm-up %d steps: %.1f s" % (dns_warm, time.time() - t0))
     X, T, D, s = collect_samples(dns_cfg, dns_steps, n_snapshots, per_snapshot, box=box, seed=seed, solver=s)
     log("dns sampling %d snapshots: %d samples, %.1f s" % (n_snapshots, X.shape[0], time.time() - t0))
@@ -226,7 +244,9 @@ def evaluate(dns_cfg, les_cfg, dns_warm, dns_steps, n_snapshots, per_snapshot, l
     for name, lt in (("mlp", 11), ("smagorinsky_vd", 10)):
         cfg = les_cfg.copy(LES_type=lt)
         ls = ChannelSolver(cfg)
-        ls.upload(*initfield.laminar_noise(cfg, yp=ls.yp, seed=seed))
+        start = (initfield.large_scale(cfg, amplitude=turbulent_start, yp=ls.yp, seed=seed) if turbulent_start > 0
+                 else initfield.laminar_noise(cfg, yp=ls.yp, seed=seed))
+        ls.upload(*start)
         ls.project()
         if lt == 11:
             ls.sgs_mlp_set(params, norm)
@@ -268,11 +288,15 @@ def main():
     ap.add_argument("--les-steps", type=int, default=20000)
     ap.add_argument("--les-avg-from", type=int, default=4000)
     ap.add_argument("--train-iters", type=int, default=3000)
+    ap.add_argument("--turbulent-start", type=float, default=0.0,
+                    help="amplitude of a large-scale start (0: the seeded white-noise start)")
+    ap.add_argument("--warm-dt", type=float, default=None, help="time step of the mixed-precision warm-up")
     args = ap.parse_args()
     dns, _ = workloads.get("channel256x192x256_re13750")
     les, _ = workloads.get("channel48_les", LES_type=10, Cs=0.1)
     rep = evaluate(dns, les, args.dns_warm, args.dns_steps, args.snapshots, args.per_snapshot, args.les_steps,
-                   args.les_avg_from, train_iters=args.train_iters)
+                   args.les_avg_from, train_iters=args.train_iters, turbulent_start=args.turbulent_start,
+                   warm_dt=args.warm_dt)
     json.dump(rep, open(args.out, "w"))
 
 

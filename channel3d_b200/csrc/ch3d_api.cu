@@ -413,6 +413,12 @@ int init_scalars(ch3d_ctx* c) {
   return CH3D_OK;
 }
 
+// The 2nd-order partially implicit step without LES runs its right-hand
+// sides and y solves as one column-march kernel (ch3d_march.cu).
+static bool march_path(const ch3d_ctx* c) {
+  return c->cfg.LES_type == 0 && c->cfg.order == 2 && c->cfg.IsImplicit != 2;
+}
+
 int record_step(ch3d_ctx* c) {
   CU(launch_step_begin(c));
   if (c->cfg.LES_type > 0) CU(launch_sgs_nut(c));  // once per step, after the CFL (m_ChannelSystem.f90:89)
@@ -420,16 +426,20 @@ int record_step(ch3d_ctx* c) {
   for (int ns = 1; ns <= c->iadvance; ++ns) {
     if (o4) CU(launch_visc4_partials(c));
     CU(launch_substep_setup(c, ns));
-    CU(launch_helm_factors(c));
-    if (c->cfg.LES_type > 0) {
+    if (march_path(c)) {  // RHS + y solves as one column march, its own Thomas factors
+      CU(launch_rhs_march(c));
+    } else if (c->cfg.LES_type > 0) {
+      CU(launch_helm_factors(c));
       CU(launch_rhs_les(c));
       CU(launch_uhat_les(c));
     } else if (fimp) {
+      CU(launch_helm_factors(c));
       CU(launch_rhs_fimp(c));
       CU(launch_ptri_xz(c));
       CU(launch_uhat(c));
     } else {
-      CU(o4 ? launch_rhs4_uhat(c) : launch_rhs_uhat(c));
+      CU(launch_helm_factors(c));
+      CU(launch_rhs4_uhat(c));
     }
     CU(launch_prsrc_xfft(c, 0));
     CU(launch_poisson_spectral(c));
@@ -570,6 +580,8 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
   {
     size_t nf = (size_t)2 * (5 * c->ny + 6 * (c->Pv > 1 ? c->Pv - 1 : 1));
     if (cudaMalloc(&c->hfac, nf * sizeof(double)) != cudaSuccess) return cleanup(fail(CH3D_ERR_NOMEM, "hfac"));
+    if (cudaMalloc(&c->mtab, march_table_bytes(c->ny)) != cudaSuccess)
+      return cleanup(fail(CH3D_ERR_NOMEM, "march table"));
   }
   {
     // Poisson y-solve (Thomas) factors per (kx, |kz|), computed once
@@ -630,7 +642,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   if (c->les_delta) cudaFree(c->les_delta);
   void* mbufs[] = {c->mlp_params, c->mlp_x, c->mlp_y, c->mlp_fb, c->mlp_status, c->sgs_tau, c->sgs_f};
   for (void* b : mbufs) if (b) cudaFree(b);
-  void* bufs[] = {c->hfac, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -949,15 +961,18 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
     for (int ns = 1; ns <= c->iadvance; ++ns) {
       CU(mark(6));
       if (c->cfg.order == 4) CU(launch_visc4_partials(c));
-      CU(launch_substep_setup(c, ns)); CU(launch_helm_factors(c)); CU(done());
-      if (c->cfg.LES_type > 0) {
+      CU(launch_substep_setup(c, ns)); if (!march_path(c)) CU(launch_helm_factors(c)); CU(done());
+      if (march_path(c)) {
+        CU(mark(0)); CU(launch_rhs_march(c)); CU(done());
+        CU(mark(1)); CU(done());
+      } else if (c->cfg.LES_type > 0) {
         CU(mark(0)); CU(launch_rhs_les(c)); CU(done());
         CU(mark(1)); CU(launch_uhat_les(c)); CU(done());
       } else if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
         CU(mark(0)); CU(launch_rhs_fimp(c)); CU(done());
         CU(mark(1)); CU(launch_ptri_xz(c)); CU(launch_uhat(c)); CU(done());
       } else {
-        CU(mark(0)); CU(c->cfg.order == 4 ? launch_rhs4_uhat(c) : launch_rhs_uhat(c)); CU(done());
+        CU(mark(0)); CU(launch_rhs4_uhat(c)); CU(done());
         CU(mark(1)); CU(done());
       }
       CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());

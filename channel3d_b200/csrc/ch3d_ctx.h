@@ -34,6 +34,7 @@ struct ch3d_ctx {
   void* f[15] = {nullptr};   // ux uy uz p hx hy hz rx ry rz phi nut u*x u*y u*z (precision T)
   void* ih[6] = {nullptr};   // 4th order: uxhx uyhx uzhx uxhz uyhz uzhz (precision T)
   double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
+  void* mtab = nullptr;      // column-march row table of the current substep (precision T)
   double* pfac = nullptr;    // FIMP: periodic x/z sweep factors of the current substep
   double* les_delta = nullptr;  // LES: DeltaCell (ny+2) | wall distance of the cell centres (ny+2)
   // learned closure (LES_type CH3D_LES_MLP)
@@ -91,6 +92,9 @@ cudaError_t launch_step_end(ch3d_ctx* c);
 cudaError_t launch_rhs(ch3d_ctx* c);
 cudaError_t launch_uhat(ch3d_ctx* c);                  // stage path: Rhs arrays -> u*
 cudaError_t launch_rhs_uhat(ch3d_ctx* c);              // fused step path: u -> u*
+// 2nd-order PIMP step: RHS + y solves as a column march (ch3d_march.cu)
+cudaError_t launch_rhs_march(ch3d_ctx* c);             // u -> u*, Hist, with its row table
+size_t march_table_bytes(int ny);
 cudaError_t launch_helm_factors(ch3d_ctx* c);
 cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlpha, 1: div(u), 2: source in phi
 cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv

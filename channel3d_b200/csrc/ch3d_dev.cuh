@@ -131,6 +131,17 @@ __device__ __forceinline__ void helm_abc(const HelmCoef& hc, int set, double pmB
   }
 }
 
+// The Helmholtz coefficient vectors inside the packed FP64 metric block
+// (pack order of ch3d_api.cu).
+inline HelmCoef helm_coef(const ch3d_ctx* c) {
+  HelmCoef hc;
+  const double* M = c->met64;
+  const int L = c->ny + 3;
+  hc.ap2p = M + 7 * L; hc.ac2p = M + 8 * L; hc.am2p = M + 9 * L;
+  hc.ap2cForCN = M + 14 * L; hc.am2cForCN = M + 15 * L;
+  return hc;
+}
+
 // Factor layout of one set: RM | AA | CP | AL | BE (ny each), then per
 // interface q: M00 M01 M10 M11 l v (6 each).
 __host__ __device__ inline int helm_set_stride(int ny, int P) { return 5 * ny + 6 * (P > 1 ? P - 1 : 1); }

@@ -1,0 +1,292 @@
+// ch3d_march.cu -- the 2nd-order partially implicit substep's right-hand
+// sides fused with its y Crank-Nicolson solves, as a column march:
+// clcRhsX/Y/Z_PIMP (src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75, 161-209, 277-325)
+// followed by clcU1/2/3Hat_PIMP (:392-430, 542-589, 702-740), u -> u*.
+//
+// One thread owns one (i, k) column and all three velocity components.  A
+// block of 32 x BZ columns marches j upwards through a ring of four staged
+// rows in shared memory (ux, uy, uz, p of the block's columns plus a one-cell
+// halo in x and z; rows -1 and ny are the wall ghosts of SetBC_and_UpdateHalo,
+// src/CFD_2nd/m_BC_and_Halo.f90:241-282).  At row j the thread evaluates the
+// three right-hand sides from rows j-1, j, j+1 of the ring, updates Hist, and
+// eliminates row j of the three tridiagonal systems (Thomas; the factors are
+// the same for every column and come from a per-row table).  Instead of the
+// eliminated right-hand side d_j it stores
+//     g_j = u_j + d_j + cp_j u_{j+1}
+// in the u* array; the back substitution x_j = d_j - cp_j x_{j+1} of
+// u*_j = u_j + x_j then reads only g:  u*_j = g_j - cp_j u*_{j+1}.
+// Global traffic per cell: ux uy uz p, Hist x3 read + written, g x3 written
+// and read back, u* x3 written (19 values).
+#include "ch3d_ctx.h"
+#include "ch3d_dev.cuh"
+
+namespace ch3d {
+
+// Row table of the march (precision T, MT_W values per row j = 0..ny-1):
+// the y metrics at jc = j + 1 and the Thomas factors a, 1/m, c/m of the two
+// Helmholtz sets (set 0: ux and uz, set 1: uy; m_TSchemePIMP_inc.f90:392-430,
+// 542-589, 702-740).  cp of the last row is stored as 0 (it has no upper neighbour).
+enum {
+  MT_IY1, MT_IY3, MT_RDYP, MT_RDYC, MT_AP2C, MT_AC2C, MT_AM2C, MT_AP2P, MT_AC2P, MT_AM2P,
+  MT_A0, MT_RM0, MT_CP0, MT_A1, MT_RM1, MT_CP1, MT_W
+};
+
+size_t march_table_bytes(int ny) { return (size_t)ny * MT_W * sizeof(double); }
+
+template <class T>
+__global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__ tab,
+                              const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  if (threadIdx.x == 0 || threadIdx.x == 32) {  // one thread per Helmholtz set, sequential in j
+    const int set = threadIdx.x == 0 ? 0 : 1;
+    const double pmBeta = sc->pmBeta;
+    T* col = tab + (set ? MT_A1 : MT_A0);
+    double cpp = 0.0;
+    for (int j = 0; j < ny; ++j) {
+      double a, b, c;
+      helm_abc(hc, set, pmBeta, j, a, b, c);
+      const double rm = 1.0 / (j == 0 ? b : b - a * cpp);
+      const double cp = c * rm;
+      col[(size_t)j * MT_W + 0] = (T)a;
+      col[(size_t)j * MT_W + 1] = (T)rm;
+      col[(size_t)j * MT_W + 2] = j == ny - 1 ? (T)0 : (T)cp;
+      cpp = cp;
+    }
+  }
+  for (int j = threadIdx.x; j < ny; j += blockDim.x) {
+    const int jc = j + 1;
+    T* row = tab + (size_t)j * MT_W;
+    row[MT_IY1] = m.yinterp[jc]; row[MT_IY3] = m.yinterp[jc + 1];
+    row[MT_RDYP] = m.rdyp[jc]; row[MT_RDYC] = m.rdyc[jc];
+    row[MT_AP2C] = m.ap2c[jc]; row[MT_AC2C] = m.ac2c[jc]; row[MT_AM2C] = m.am2c[jc];
+    row[MT_AP2P] = m.ap2p[jc]; row[MT_AC2P] = m.ac2p[jc]; row[MT_AM2P] = m.am2p[jc];
+  }
+}
+
+template <class T, int BZ>
+__global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
+    k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ ux, const T* __restrict__ uy,
+                const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
+                T* __restrict__ hz, T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
+                const DevScalars* __restrict__ sc) {
+  constexpr int BX = 32, NT = BX * BZ, SX = BX + 2, PL = SX * (BZ + 2), R = 4;
+  constexpr int NS = (PL + NT - 1) / NT;  // staging slots per thread and array
+  __shared__ T ring[4][R][PL];             // ux uy uz p; row r in slot r & 3
+  if (sc->status) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long plane = (long long)nx * ny;
+  const int tid = threadIdx.x, tx = tid & 31, tz = tid >> 5;
+  const int i0 = blockIdx.x * BX, k0 = blockIdx.y * BZ;
+  const int i = i0 + tx, k = k0 + tz;
+  const bool act = i < nx && k < nz;
+
+  // staging slots: s = tid + q NT -> halo-tile position (s % SX, s / SX), periodic in x and z
+  long long so[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const int s = tid + q * NT;
+    int ig = (i0 - 1 + s % SX) % nx, kg = (k0 - 1 + s / SX) % nz;
+    if (ig < 0) ig += nx;
+    if (kg < 0) kg += nz;
+    so[q] = s < PL ? ig + plane * kg : 0;
+  }
+  T st[4][NS];
+  auto load_row = [&](int r) {
+    const long long ro = (long long)r * nx;
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      if (tid + q * NT < PL) {
+        st[0][q] = __ldg(ux + so[q] + ro); st[1][q] = __ldg(uy + so[q] + ro);
+        st[2][q] = __ldg(uz + so[q] + ro); st[3][q] = __ldg(pr + so[q] + ro);
+      }
+    }
+  };
+  auto store_row = [&](int r) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const int s = tid + q * NT;
+      if (s < PL) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) ring[a][r & (R - 1)][s] = st[a][q];
+      }
+    }
+  };
+  // wall ghost rows from the staged rows next to them (at_jm / at_jp of ch3d_dev.cuh)
+  auto ghost_row = [&](int r) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const int s = tid + q * NT;
+      if (s >= PL) continue;
+      T* u0 = &ring[0][r & (R - 1)][s];
+      T* v0 = &ring[1][r & (R - 1)][s];
+      T* w0 = &ring[2][r & (R - 1)][s];
+      T* p0 = &ring[3][r & (R - 1)][s];
+      if (r < 0) {
+        const T u = ring[0][0][s], w = ring[2][0][s], v1 = ring[1][1][s];
+        *u0 = g.bc.lo == -1 ? (T)(g.bc.ux_lo * 2.0) - u : u - (T)(g.bc.ux_lo * g.bc.dyp1);
+        *v0 = (T)(g.bc.uy_lo * 2.0) - v1;  // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc)
+        *w0 = g.bc.lo == -1 ? (T)(g.bc.uz_lo * 2.0) - w : w - (T)(g.bc.uz_lo * g.bc.dyp1);
+        *p0 = ring[3][0][s];
+      } else {
+        const int sn = (ny - 1) & (R - 1);
+        const T u = ring[0][sn][s], w = ring[2][sn][s];
+        *u0 = g.bc.hi == -1 ? (T)(g.bc.ux_hi * 2.0) - u : (T)(g.bc.ux_hi * g.bc.dypN) + u;
+        *v0 = (T)g.bc.uy_hi;
+        *w0 = g.bc.hi == -1 ? (T)(g.bc.uz_hi * 2.0) - w : (T)(g.bc.uz_hi * g.bc.dypN) + w;
+        *p0 = ring[3][sn][s];
+      }
+    }
+  };
+
+  // prologue: rows 0 and 1, then the lower ghost row -1
+  load_row(0);
+  store_row(0);
+  if (ny > 1) { load_row(1); store_row(1); }
+  __syncthreads();
+  if (ny == 1) ghost_row(1);
+  __syncthreads();
+  ghost_row(-1);
+  __syncthreads();
+
+  const T two = (T)2, half = (T)0.5, quarter = (T)0.25, one = (T)1;
+  const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
+  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
+  const T dpm = (T)sc->dpmdxns;
+  const int c0 = (tz + 1) * SX + tx + 1;
+  long long idx = act ? i + plane * k : 0;
+  T d0 = (T)0, d1 = (T)0, d2 = (T)0;       // eliminated right-hand sides of the previous row
+  T g0 = (T)0, g1 = (T)0, g2 = (T)0;       // g of the last row (= u* of row ny-1)
+  T hxo = (T)0, hyo = (T)0, hzo = (T)0;
+  if (act) { hxo = hx[idx]; hyo = hy[idx]; hzo = hz[idx]; }
+
+  for (int j = 0; j < ny; ++j) {
+    const int r = j + 2;
+    if (r < ny) load_row(r);
+    T hxn = (T)0, hyn = (T)0, hzn = (T)0;
+    if (act && j + 1 < ny) { hxn = hx[idx + nx]; hyn = hy[idx + nx]; hzn = hz[idx + nx]; }
+    if (act) {
+      const T* X0 = &ring[0][(j - 1) & (R - 1)][c0];
+      const T* X1 = &ring[0][j & (R - 1)][c0];
+      const T* X2 = &ring[0][(j + 1) & (R - 1)][c0];
+      const T* Y0 = &ring[1][(j - 1) & (R - 1)][c0];
+      const T* Y1 = &ring[1][j & (R - 1)][c0];
+      const T* Y2 = &ring[1][(j + 1) & (R - 1)][c0];
+      const T* Z0 = &ring[2][(j - 1) & (R - 1)][c0];
+      const T* Z1 = &ring[2][j & (R - 1)][c0];
+      const T* Z2 = &ring[2][(j + 1) & (R - 1)][c0];
+      const T* P0 = &ring[3][(j - 1) & (R - 1)][c0];
+      const T* P1 = &ring[3][j & (R - 1)][c0];
+      const T* tr = tab + (size_t)j * MT_W;
+
+      const T ux_c = X1[0], ux_ip = X1[1], ux_im = X1[-1], ux_jp = X2[0], ux_jm = X0[0];
+      const T ux_kp = X1[SX], ux_km = X1[-SX], ux_ip_jm = X0[1], ux_ip_km = X1[1 - SX];
+      const T uy_c = Y1[0], uy_ip = Y1[1], uy_im = Y1[-1], uy_jp = Y2[0], uy_jm = Y0[0];
+      const T uy_im_jp = Y2[-1], uy_kp = Y1[SX], uy_km = Y1[-SX], uy_jp_km = Y2[-SX];
+      const T uz_c = Z1[0], uz_ip = Z1[1], uz_im = Z1[-1], uz_jp = Z2[0], uz_jm = Z0[0];
+      const T uz_kp = Z1[SX], uz_km = Z1[-SX], uz_im_kp = Z1[SX - 1], uz_jm_kp = Z0[SX];
+      const T p_c = P1[0], p_im = P1[-1], p_jm = P0[0], p_km = P1[-SX];
+
+      const T IY1 = __ldg(tr + MT_IY1), IY2 = one - IY1;
+      const T IY3 = __ldg(tr + MT_IY3), IY4 = one - IY3;
+      T rx, ry, rz;
+      {  // RhsX (clcRhsX_PIMP, m_TSchemePIMP_inc.f90:7-75)
+        const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+        const T sucaj = half * __ldg(tr + MT_RDYP);
+        T h11 = ((ux_ip + ux_c) * (ux_ip + ux_c) - (ux_c + ux_im) * (ux_c + ux_im)) * qdx1;
+        T h12 = ((uy_jp + uy_im_jp) * (IY3 * ux_c + IY4 * ux_jp) - (uy_c + uy_im) * (IY1 * ux_jm + IY2 * ux_c)) * sucaj;
+        T h13 = ((uz_kp + uz_im_kp) * (ux_kp + ux_c) - (uz_c + uz_im) * (ux_c + ux_km)) * qdx3;
+        T d11q1 = (ux_ip - two * ux_c + ux_im) * rdx2;
+        T d22q1 = __ldg(tr + MT_AP2C) * ux_jp + __ldg(tr + MT_AC2C) * ux_c + __ldg(tr + MT_AM2C) * ux_jm;
+        T d33q1 = g.ap3c * ux_kp + g.ac3c * ux_c + g.am3c * ux_km;
+        T dcq13 = d11q1 + d33q1;
+        T gradp1 = (p_c - p_im) * rdx;
+        T convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g.g1;
+        rx = pmGamma * convEd1 + pmTheta * hxo - pmAlpha * gradp1 + two * pmBeta * d22q1;
+        hx[idx] = convEd1;
+      }
+      {  // RhsY (clcRhsY_PIMP, :161-209)
+        const T hdx1 = half * rdx, hdx3 = half * rdz;
+        const T sucac = __ldg(tr + MT_RDYC), qsucac = quarter * sucac;
+        T h21 = ((IY1 * ux_ip_jm + IY2 * ux_ip) * (uy_ip + uy_c) - (IY1 * ux_jm + IY2 * ux_c) * (uy_c + uy_im)) * hdx1;
+        T h22 = ((uy_jp + uy_c) * (uy_jp + uy_c) - (uy_c + uy_jm) * (uy_c + uy_jm)) * qsucac;
+        T h23 = ((IY1 * uz_jm_kp + IY2 * uz_kp) * (uy_kp + uy_c) - (IY1 * uz_jm + IY2 * uz_c) * (uy_c + uy_km)) * hdx3;
+        T d11q2 = g.ap1c * uy_ip + g.ac1c * uy_c + g.am1c * uy_im;
+        T d22q2 = __ldg(tr + MT_AP2P) * uy_jp + __ldg(tr + MT_AC2P) * uy_c + __ldg(tr + MT_AM2P) * uy_jm;
+        T d33q2 = g.ap3c * uy_kp + g.ac3c * uy_c + g.am3c * uy_km;
+        T dcq13 = d11q2 + d33q2;
+        T gradp2 = (p_c - p_jm) * sucac;
+        T convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g.g2;
+        ry = pmGamma * convEd2 + pmTheta * hyo - pmAlpha * gradp2 + two * pmBeta * d22q2;
+        hy[idx] = convEd2;
+      }
+      {  // RhsZ (clcRhsZ_PIMP, :277-325)
+        const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
+        const T sucaj = half * __ldg(tr + MT_RDYP);
+        T h31 = ((ux_ip + ux_ip_km) * (uz_ip + uz_c) - (ux_c + ux_km) * (uz_c + uz_im)) * qdx1;
+        T h32 = ((uy_jp + uy_jp_km) * (IY3 * uz_c + IY4 * uz_jp) - (uy_c + uy_km) * (IY1 * uz_jm + IY2 * uz_c)) * sucaj;
+        T h33 = ((uz_kp + uz_c) * (uz_kp + uz_c) - (uz_c + uz_km) * (uz_c + uz_km)) * qdx3;
+        T d11q3 = g.ap1c * uz_ip + g.ac1c * uz_c + g.am1c * uz_im;
+        T d22q3 = __ldg(tr + MT_AP2C) * uz_jp + __ldg(tr + MT_AC2C) * uz_c + __ldg(tr + MT_AM2C) * uz_jm;
+        T d33q3 = (uz_kp - two * uz_c + uz_km) * rdz2;
+        T dcq13 = d11q3 + d33q3;
+        T gradp3 = (p_c - p_km) * rdz;
+        T convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g.g3;
+        rz = pmGamma * convEd3 + pmTheta * hzo - pmAlpha * gradp3 + two * pmBeta * d22q3;
+        hz[idx] = convEd3;
+      }
+      rx += dpm;                     // mean pressure gradient (clcRhsX_PIMP :61-74)
+      if (j == 0) ry = (T)0;         // duy_ym: uy_ym is constant (Update_uy_ym_CH)
+      d0 = (rx - __ldg(tr + MT_A0) * d0) * __ldg(tr + MT_RM0);
+      d1 = (ry - __ldg(tr + MT_A1) * d1) * __ldg(tr + MT_RM1);
+      d2 = (rz - __ldg(tr + MT_A0) * d2) * __ldg(tr + MT_RM0);
+      g0 = ux_c + d0 + __ldg(tr + MT_CP0) * ux_jp;
+      g1 = uy_c + d1 + __ldg(tr + MT_CP1) * uy_jp;
+      g2 = uz_c + d2 + __ldg(tr + MT_CP0) * uz_jp;
+      uxs[idx] = g0; uys[idx] = g1; uzs[idx] = g2;
+    }
+    if (r < ny) store_row(r);
+    else if (r == ny) ghost_row(ny);
+    __syncthreads();
+    idx += nx;
+    hxo = hxn; hyo = hyn; hzo = hzn;
+  }
+  if (!act) return;
+
+  // back substitution u*_j = g_j - cp_j u*_{j+1}, rows loaded in batches of 8
+  constexpr int B = 8;
+  idx -= nx;  // row ny-1 (u* = g there)
+  for (int j = ny - 2; j >= 0; j -= B) {
+    T a0[B], a1[B], a2[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      if (j - b >= 0) {
+        const long long o = idx - (long long)(b + 1) * nx;
+        a0[b] = uxs[o]; a1[b] = uys[o]; a2[b] = uzs[o];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      if (j - b >= 0) {
+        const T* tr = tab + (size_t)(j - b) * MT_W;
+        const T cp0 = __ldg(tr + MT_CP0), cp1 = __ldg(tr + MT_CP1);
+        g0 = a0[b] - cp0 * g0; g1 = a1[b] - cp1 * g1; g2 = a2[b] - cp0 * g2;
+        const long long o = idx - (long long)(b + 1) * nx;
+        uxs[o] = g0; uys[o] = g1; uzs[o] = g2;
+      }
+    }
+    idx -= (long long)B * nx;
+  }
+}
+
+template <class T> static cudaError_t rhs_march_t(ch3d_ctx* c) {
+  constexpr int BZ = 4;
+  T** f = (T**)c->f;
+  k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab, c->sc);
+  dim3 grid((c->nx + 31) / 32, (c->nz + BZ - 1) / BZ);
+  k_rhs_march<T, BZ><<<grid, 32 * BZ, 0, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3],
+                                                     f[4], f[5], f[6], f[12], f[13], f[14], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_rhs_march(ch3d_ctx* c) { return c->fp32 ? rhs_march_t<float>(c) : rhs_march_t<double>(c); }
+
+}  // namespace ch3d

@@ -1241,16 +1241,6 @@ template <class T> static cudaError_t rhs_fimp_t(ch3d_ctx* c) {
 }
 cudaError_t launch_rhs_fimp(ch3d_ctx* c) { return c->fp32 ? rhs_fimp_t<float>(c) : rhs_fimp_t<double>(c); }
 
-static HelmCoef helm_coef(const ch3d_ctx* c) {
-  HelmCoef hc;
-  const double* M = c->met64;
-  const int L = c->ny + 3;
-  // packed metric offsets, see ch3d_api.cu (pack order)
-  hc.ap2p = M + 7 * L; hc.ac2p = M + 8 * L; hc.am2p = M + 9 * L;
-  hc.ap2cForCN = M + 14 * L; hc.am2cForCN = M + 15 * L;
-  return hc;
-}
-
 cudaError_t launch_helm_factors(ch3d_ctx* c) {
   k_helm_factors<<<2, 64, 0, c->stream>>>(helm_coef(c), c->ny, c->Pv, c->hfac, c->sc);
   return cudaGetLastError();

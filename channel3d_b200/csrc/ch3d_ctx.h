@@ -99,6 +99,11 @@ cudaError_t launch_helm_factors(ch3d_ctx* c);
 cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlpha, 1: div(u), 2: source in phi
 cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv
 cudaError_t launch_xifft(ch3d_ctx* c);
+// register-resident FFT kernels for the lengths with a plan (ch3d_rfft.cu);
+// false: no plan, nothing launched
+bool launch_prsrc_xfft_r(ch3d_ctx* c, int mode, cudaError_t* err);
+bool launch_zfft_r(ch3d_ctx* c, int inverse, cudaError_t* err);
+bool launch_xifft_r(ch3d_ctx* c, cudaError_t* err);
 cudaError_t launch_ysolve_factors(ch3d_ctx* c);
 // allocation-free Poisson solve (static device scratch, ch3d_step.cu)
 size_t noalloc_bytes(int nx, int ny, int nz);

@@ -1298,6 +1298,8 @@ template <class T> static int lines_per_block(int M) {
 
 template <class T> static cudaError_t prsrc_t(ch3d_ctx* c, int mode) {
   typedef typename CplxOf<T>::type CT;
+  cudaError_t e;
+  if (launch_prsrc_xfft_r(c, mode, &e)) return e;  // register FFT when the length has a plan
   T** f = (T**)c->f;
   const int M = c->nx / 2;
   const int LPB = lines_per_block<T>(M);
@@ -1322,6 +1324,9 @@ cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode) { return c->fp32 ? prsrc_t<
 template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   typedef typename CplxOf<T>::type CT;
   const int nz = c->nz;
+  cudaError_t e;
+  const bool zr = launch_zfft_r(c, 0, &e);  // register FFT when nz has a plan
+  if (zr && e != cudaSuccess) return e;
   int TKX = kFFTSmem / (2 * nz * (int)sizeof(CT));
   int t = 1;
   while (t * 2 <= TKX && t * 2 <= 16) t *= 2;
@@ -1334,9 +1339,11 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
     attr_set[sizeof(T) == 4] = true;
   }
   dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
-  k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  if (!zr) {
+    k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   const unsigned gy = (unsigned)(((long long)c->nxh * c->nz + 127) / 128);
   if (!c->fp32) {
     k_ythomas<T, double><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
@@ -1349,6 +1356,7 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (launch_zfft_r(c, 1, &e)) return e;
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);
   return cudaGetLastError();
 }
@@ -1374,6 +1382,8 @@ cudaError_t launch_poisson_spectral(ch3d_ctx* c) { return c->fp32 ? spectral_t<f
 
 template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {
   typedef typename CplxOf<T>::type CT;
+  cudaError_t e;
+  if (launch_xifft_r(c, &e)) return e;  // register FFT when the length has a plan
   T** f = (T**)c->f;
   const int M = c->nx / 2;
   const int LPB = lines_per_block<T>(M);

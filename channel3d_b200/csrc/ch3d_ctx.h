@@ -91,7 +91,6 @@ cudaError_t launch_step_begin(ch3d_ctx* c);
 cudaError_t launch_step_end(ch3d_ctx* c);
 cudaError_t launch_rhs(ch3d_ctx* c);
 cudaError_t launch_uhat(ch3d_ctx* c);                  // stage path: Rhs arrays -> u*
-cudaError_t launch_rhs_uhat(ch3d_ctx* c);              // fused step path: u -> u*
 // 2nd-order PIMP step: RHS + y solves as a column march (ch3d_march.cu)
 cudaError_t launch_rhs_march(ch3d_ctx* c);             // u -> u*, Hist, with its row table
 size_t march_table_bytes(int ny);

@@ -5,8 +5,9 @@
 //
 // Per substep the device runs:
 //   substep_setup  PMcoeUpdate + bulk-velocity reduction (clcRhsX_PIMP :60-74)
-//   rhs            clcRhsX/Y/Z_PIMP (stencils, Hist update)
-//   uhat           clcU1/2/3Hat_PIMP (y Crank-Nicolson, partitioned tridiagonal)
+//   rhs + uhat     clcRhsX/Y/Z_PIMP and clcU1/2/3Hat_PIMP as one column march
+//                  (ch3d_march.cu); the stage entry points run them separately
+//                  (k_rhs_pimp, k_uhat_pimp: partitioned tridiagonal)
 //   prsrc_xfft     clcPrSrcOther fused with the forward x R2C FFT
 //   spectral       z FFT, y tridiagonal per (kx,kz) with the (0,0) pin, z iFFT
 //   xifft          x C2R FFT * normfft -> phi
@@ -200,8 +201,8 @@ __device__ __forceinline__ void rhs_point(const Geo<T>& g, const Metrics<T>& m, 
   }
 }
 
-// One component of clcRhsX/Y/Z_PIMP at one cell (C = 0, 1, 2), with its Hist
-// update; used by the fused solve kernel, where one block handles one component.
+// One component of clcRhsX/Y/Z_PIMP (or _FIMP) at one cell (C = 0, 1, 2),
+// with its Hist update.
 template <class T, int C>
 __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, const T* __restrict__ ux,
                                       const T* __restrict__ uy, const T* __restrict__ uz, const T* __restrict__ pr,
@@ -440,89 +441,6 @@ __global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, const double* __res
     const long long idx = i + (long long)nx * (j + (long long)ny * k);
     us[idx] = u[idx] + x;
   }
-}
-
-// clcRhsX/Y/Z fused with clcU1/2/3Hat: the right-hand sides never leave the
-// SM.  Block: one velocity component (blockIdx.x % 3, so the three blocks of
-// a column tile run back to back and share their neighbour reads in L2), TI
-// consecutive i at one k, all j.  (a) every thread evaluates RHS cells of the
-// tile into shared memory; (b) thread (ii, p) eliminates chunk p of column
-// ii; (c) per column the interface system; (d) u* = u + du.
-template <class T, int C, int TI>
-__device__ __forceinline__ void rhs_uhat_body(const Geo<T>& g, const Metrics<T>& m, const double* __restrict__ fac,
-                                              int P, const T* __restrict__ ux, const T* __restrict__ uy,
-                                              const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ h,
-                                              T* __restrict__ us, int i0, int k, const DevScalars* __restrict__ sc,
-                                              T* F, T* IF, T* FS) {
-  const int nx = g.nx, ny = g.ny, Q = P - 1;
-  const int QQ = 2 * (Q > 0 ? Q : 1);
-  {  // this component's Helmholtz factors, staged in shared memory (read by the sequential sweeps)
-    const double* FG = fac + (C == 1 ? helm_set_stride(ny, P) : 0);
-    for (int t = threadIdx.x; t < helm_set_stride(ny, P); t += blockDim.x) FS[t] = (T)FG[t];
-  }
-  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
-  const T add = C == 0 ? (T)sc->dpmdxns : (T)0;
-  const int tid = threadIdx.x;
-#pragma unroll 2
-  for (int t = tid; t < ny * TI; t += blockDim.x) {
-    const int j = t / TI, ii = t % TI, i = i0 + ii;
-    T r = (T)0;
-    if (i < nx) r = rhs_comp<T, C>(g, m, ux, uy, uz, pr, h, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
-    if (C == 0) r += add;
-    if (C == 1 && j == 0) r = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
-    F[t] = r;
-  }
-  __syncthreads();
-  for (int t = tid; t < TI * P; t += blockDim.x) {
-    const int ii = t % TI, p = t / TI;
-    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
-    T d = F[s * TI + ii] * (T)FS[s];
-    F[s * TI + ii] = d;
-    for (int j = s + 1; j <= e; ++j) {
-      d = (F[j * TI + ii] - (T)FS[ny + j] * d) * (T)FS[j];
-      F[j * TI + ii] = d;
-    }
-    for (int j = e - 1; j >= s; --j) {
-      d = F[j * TI + ii] - (T)FS[2 * ny + j] * d;
-      F[j * TI + ii] = d;
-    }
-  }
-  __syncthreads();
-  for (int t = tid; t < TI; t += blockDim.x) helm_interfaces<T>(FS + 5 * ny, F + t, TI, ny, P, IF + (size_t)t * QQ);
-  __syncthreads();
-  const T* u = C == 0 ? ux : (C == 1 ? uy : uz);
-  for (int t = tid; t < TI * P; t += blockDim.x) {
-    const int ii = t % TI, p = t / TI, i = i0 + ii;
-    if (i >= nx) continue;
-    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
-    const T* G = IF + (size_t)ii * QQ;
-    const T uL = p > 0 ? G[2 * (p - 1)] : (T)0;
-    const T wR = p < P - 1 ? G[2 * p + 1] : (T)0;
-    long long idx = i + (long long)nx * (s + (long long)ny * k);
-    for (int j = s; j <= e; ++j, idx += nx) {
-      const T x = F[j * TI + ii] + (T)FS[3 * ny + j] * uL + (T)FS[4 * ny + j] * wR;
-      us[idx] = __ldg(u + idx) + x;
-    }
-  }
-}
-
-template <class T, int TI>
-__global__ void __launch_bounds__(256, 4) k_rhs_uhat(Geo<T> g, Metrics<T> m, const double* __restrict__ fac, int P,
-                                                     const T* __restrict__ ux, const T* __restrict__ uy,
-                                                     const T* __restrict__ uz, const T* __restrict__ pr,
-                                                     T* __restrict__ hx, T* __restrict__ hy, T* __restrict__ hz,
-                                                     T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
-                                                     const DevScalars* __restrict__ sc) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  if (sc->status) return;
-  const int comp = blockIdx.x % 3;
-  const int i0 = (blockIdx.x / 3) * TI, k = blockIdx.y;
-  T* F = (T*)smem_raw;
-  T* IF = F + (size_t)g.ny * TI;
-  T* FS = IF + (size_t)TI * 2 * (P > 1 ? P - 1 : 1);
-  if (comp == 0) rhs_uhat_body<T, 0, TI>(g, m, fac, P, ux, uy, uz, pr, hx, uxs, i0, k, sc, F, IF, FS);
-  else if (comp == 1) rhs_uhat_body<T, 1, TI>(g, m, fac, P, ux, uy, uz, pr, hy, uys, i0, k, sc, F, IF, FS);
-  else rhs_uhat_body<T, 2, TI>(g, m, fac, P, ux, uy, uz, pr, hz, uzs, i0, k, sc, F, IF, FS);
 }
 
 // ---------------------------------------------------------------------------
@@ -1265,25 +1183,6 @@ template <class T> static cudaError_t uhat_t(ch3d_ctx* c) {
 }
 cudaError_t launch_uhat(ch3d_ctx* c) { return c->fp32 ? uhat_t<float>(c) : uhat_t<double>(c); }
 
-template <class T> static cudaError_t rhs_uhat_t(ch3d_ctx* c) {
-  constexpr int TI = 16;
-  T** f = (T**)c->f;
-  const int P = c->Pv, Q = P - 1;
-  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) +
-                (size_t)helm_set_stride(c->ny, P) * sizeof(T) + 16;
-  static bool attr_set[2] = {false, false};
-  auto kern = k_rhs_uhat<T, TI>;
-  if (!attr_set[sizeof(T) == 4]) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set[sizeof(T) == 4] = true;
-  }
-  dim3 grid(3 * ((c->nx + TI - 1) / TI), c->nz, 1);
-  int nthr = TI * P < 64 ? 64 : (TI * P > 256 ? 256 : TI * P);
-  kern<<<grid, nthr, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), c->hfac, P, f[0], f[1], f[2], f[3], f[4],
-                                        f[5], f[6], f[12], f[13], f[14], c->sc);
-  return cudaGetLastError();
-}
-cudaError_t launch_rhs_uhat(ch3d_ctx* c) { return c->fp32 ? rhs_uhat_t<float>(c) : rhs_uhat_t<double>(c); }
 
 // Shared-memory budget of one FFT block (two ping-pong buffers): three
 // blocks of 256 threads fit in an SM.

@@ -149,8 +149,10 @@ __global__ void __launch_bounds__(256) k_rhs4(Geo<T> g, Metrics<T> m, Interp4 ih
 }
 
 // Fused 4th-order RHS + y Crank-Nicolson solve (clcRhsXYZ + clcU1/2/3Hat,
-// src/CFD_4th/m_TScheme.f90:189-549); same block organisation as the
-// 2nd-order k_rhs_uhat.  RhsX gets -pmAlpha*dpmdxns through sc->dpmdxns.
+// src/CFD_4th/m_TScheme.f90:189-549).  Block: one velocity component, TI
+// consecutive i at one k, all j; the RHS of every row goes to shared memory,
+// then the partitioned tridiagonal solve (chunk sweeps, interface system,
+// reconstruction).  RhsX gets -pmAlpha*dpmdxns through sc->dpmdxns.
 template <class T, int C, int TI>
 __device__ __forceinline__ void rhs4_uhat_body(const Geo<T>& g, const Metrics<T>& m, const Interp4& ih,
                                                const double* __restrict__ fac, int P, const T* __restrict__ ux,

@@ -608,6 +608,9 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
   {
     dim3 g((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz);
     c->npart = (int)(g.x * g.y * g.z);
+    c->march = march_path(c);
+    c->npart_m = march_npart(c);
+    if (c->npart_m > c->npart) c->npart = c->npart_m;
     if (cudaMalloc(&c->part, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->part2, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->red1, CH3D_NRED * sizeof(double)) != cudaSuccess ||

@@ -68,6 +68,8 @@ struct ch3d_ctx {
   double* red1 = nullptr;    // CH3D_NRED second-level sums of part
   double* red2 = nullptr;    // CH3D_NRED second-level sums of part2
   int npart = 0;
+  bool march = false;        // 2nd-order PIMP without LES: march kernels, npart_m partial sums in part
+  int npart_m = 0;
   double* stat = nullptr;    // SumStat(35, nyp) accumulator (FP64)
   double* statpart = nullptr;
   int nfstime = 0;
@@ -94,6 +96,9 @@ cudaError_t launch_uhat(ch3d_ctx* c);                  // stage path: Rhs arrays
 // 2nd-order PIMP step: RHS + y solves as a column march (ch3d_march.cu)
 cudaError_t launch_rhs_march(ch3d_ctx* c);             // u -> u*, Hist, with its row table
 size_t march_table_bytes(int ny);
+cudaError_t launch_proj_march(ch3d_ctx* c, int mode);   // projection + pressure update + bulk partials
+cudaError_t launch_bulk_march(ch3d_ctx* c);            // bulk partials of an uploaded field
+int march_npart(const ch3d_ctx* c);
 cudaError_t launch_helm_factors(ch3d_ctx* c);
 cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlpha, 1: div(u), 2: source in phi
 cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv

@@ -63,15 +63,31 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
   }
 }
 
-template <class T, int BZ>
+// asynchronous 4- or 8-byte copy global -> shared (cp.async, completion by groups)
+template <class T> __device__ __forceinline__ void cp_async_el(T* smem, const T* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Ring of RS row slots (row r in slot (r + 1) % RS); rows j+2 .. j+D+1 are in
+// flight while row j is computed.  Slot (j+D+2), written after the barrier of
+// iteration j, must differ from the slots of rows j-1, j, j+1 that other
+// threads still read: RS >= D + 4.
+template <class T, int BZ, int D, int RS>
 __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
     k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ ux, const T* __restrict__ uy,
                 const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
                 T* __restrict__ hz, T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
                 const DevScalars* __restrict__ sc) {
-  constexpr int BX = 32, NT = BX * BZ, SX = BX + 2, PL = SX * (BZ + 2), R = 4;
+  constexpr int BX = 32, NT = BX * BZ, SX = BX + 2, PL = SX * (BZ + 2);
   constexpr int NS = (PL + NT - 1) / NT;  // staging slots per thread and array
-  __shared__ T ring[4][R][PL];             // ux uy uz p; row r in slot r & 3
+  static_assert(RS >= D + 4, "ring too small for the prefetch distance");
+  __shared__ __align__(16) T ring[4][RS][PL];  // ux uy uz p
   if (sc->status) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long plane = (long long)nx * ny;
@@ -79,6 +95,7 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
   const int i0 = blockIdx.x * BX, k0 = blockIdx.y * BZ;
   const int i = i0 + tx, k = k0 + tz;
   const bool act = i < nx && k < nz;
+  auto slot = [](int r) { return (r + 1) % RS; };  // r >= -1
 
   // staging slots: s = tid + q NT -> halo-tile position (s % SX, s / SX), periodic in x and z
   long long so[NS];
@@ -90,63 +107,50 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
     if (kg < 0) kg += nz;
     so[q] = s < PL ? ig + plane * kg : 0;
   }
-  T st[4][NS];
-  auto load_row = [&](int r) {
+  auto issue_row = [&](int r) {  // r < ny
     const long long ro = (long long)r * nx;
-#pragma unroll
-    for (int q = 0; q < NS; ++q) {
-      if (tid + q * NT < PL) {
-        st[0][q] = __ldg(ux + so[q] + ro); st[1][q] = __ldg(uy + so[q] + ro);
-        st[2][q] = __ldg(uz + so[q] + ro); st[3][q] = __ldg(pr + so[q] + ro);
-      }
-    }
-  };
-  auto store_row = [&](int r) {
+    const int sl = slot(r);
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
       const int s = tid + q * NT;
       if (s < PL) {
-#pragma unroll
-        for (int a = 0; a < 4; ++a) ring[a][r & (R - 1)][s] = st[a][q];
+        cp_async_el(&ring[0][sl][s], ux + so[q] + ro);
+        cp_async_el(&ring[1][sl][s], uy + so[q] + ro);
+        cp_async_el(&ring[2][sl][s], uz + so[q] + ro);
+        cp_async_el(&ring[3][sl][s], pr + so[q] + ro);
       }
     }
   };
-  // wall ghost rows from the staged rows next to them (at_jm / at_jp of ch3d_dev.cuh)
+  // wall ghost rows from the thread's own staged slots next to them (at_jm / at_jp of ch3d_dev.cuh)
   auto ghost_row = [&](int r) {
+    const int sl = slot(r);
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
       const int s = tid + q * NT;
       if (s >= PL) continue;
-      T* u0 = &ring[0][r & (R - 1)][s];
-      T* v0 = &ring[1][r & (R - 1)][s];
-      T* w0 = &ring[2][r & (R - 1)][s];
-      T* p0 = &ring[3][r & (R - 1)][s];
       if (r < 0) {
-        const T u = ring[0][0][s], w = ring[2][0][s], v1 = ring[1][1][s];
-        *u0 = g.bc.lo == -1 ? (T)(g.bc.ux_lo * 2.0) - u : u - (T)(g.bc.ux_lo * g.bc.dyp1);
-        *v0 = (T)(g.bc.uy_lo * 2.0) - v1;  // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc)
-        *w0 = g.bc.lo == -1 ? (T)(g.bc.uz_lo * 2.0) - w : w - (T)(g.bc.uz_lo * g.bc.dyp1);
-        *p0 = ring[3][0][s];
+        const T u = ring[0][slot(0)][s], w = ring[2][slot(0)][s], v1 = ring[1][slot(1)][s];
+        ring[0][sl][s] = g.bc.lo == -1 ? (T)(g.bc.ux_lo * 2.0) - u : u - (T)(g.bc.ux_lo * g.bc.dyp1);
+        ring[1][sl][s] = (T)(g.bc.uy_lo * 2.0) - v1;  // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc)
+        ring[2][sl][s] = g.bc.lo == -1 ? (T)(g.bc.uz_lo * 2.0) - w : w - (T)(g.bc.uz_lo * g.bc.dyp1);
+        ring[3][sl][s] = ring[3][slot(0)][s];
       } else {
-        const int sn = (ny - 1) & (R - 1);
+        const int sn = slot(ny - 1);
         const T u = ring[0][sn][s], w = ring[2][sn][s];
-        *u0 = g.bc.hi == -1 ? (T)(g.bc.ux_hi * 2.0) - u : (T)(g.bc.ux_hi * g.bc.dypN) + u;
-        *v0 = (T)g.bc.uy_hi;
-        *w0 = g.bc.hi == -1 ? (T)(g.bc.uz_hi * 2.0) - w : (T)(g.bc.uz_hi * g.bc.dypN) + w;
-        *p0 = ring[3][sn][s];
+        ring[0][sl][s] = g.bc.hi == -1 ? (T)(g.bc.ux_hi * 2.0) - u : (T)(g.bc.ux_hi * g.bc.dypN) + u;
+        ring[1][sl][s] = (T)g.bc.uy_hi;
+        ring[2][sl][s] = g.bc.hi == -1 ? (T)(g.bc.uz_hi * 2.0) - w : (T)(g.bc.uz_hi * g.bc.dypN) + w;
+        ring[3][sl][s] = ring[3][sn][s];
       }
     }
   };
 
-  // prologue: rows 0 and 1, then the lower ghost row -1
-  load_row(0);
-  store_row(0);
-  if (ny > 1) { load_row(1); store_row(1); }
-  __syncthreads();
-  if (ny == 1) ghost_row(1);
-  __syncthreads();
-  ghost_row(-1);
-  __syncthreads();
+  // prologue: rows 0 .. D+1 in flight, one copy group per row
+#pragma unroll
+  for (int r = 0; r <= D + 1; ++r) {
+    if (r < ny) issue_row(r);
+    cp_async_commit();
+  }
 
   const T two = (T)2, half = (T)0.5, quarter = (T)0.25, one = (T)1;
   const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
@@ -156,26 +160,34 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
   long long idx = act ? i + plane * k : 0;
   T d0 = (T)0, d1 = (T)0, d2 = (T)0;       // eliminated right-hand sides of the previous row
   T g0 = (T)0, g1 = (T)0, g2 = (T)0;       // g of the last row (= u* of row ny-1)
-  T hxo = (T)0, hyo = (T)0, hzo = (T)0;
-  if (act) { hxo = hx[idx]; hyo = hy[idx]; hzo = hz[idx]; }
+  T hxo = (T)0, hyo = (T)0, hzo = (T)0;    // Hist of row j
+  T hx1 = (T)0, hy1 = (T)0, hz1 = (T)0;    // Hist of row j+1
+  if (act) {
+    hxo = hx[idx]; hyo = hy[idx]; hzo = hz[idx];
+    if (ny > 1) { hx1 = hx[idx + nx]; hy1 = hy[idx + nx]; hz1 = hz[idx + nx]; }
+  }
 
   for (int j = 0; j < ny; ++j) {
-    const int r = j + 2;
-    if (r < ny) load_row(r);
+    cp_async_wait<D>();  // this thread's copies of rows <= j+1 are done
+    if (j + 1 == ny) ghost_row(ny);
+    if (j == 0) ghost_row(-1);
+    __syncthreads();
+    if (j + D + 2 < ny) issue_row(j + D + 2);
+    cp_async_commit();
     T hxn = (T)0, hyn = (T)0, hzn = (T)0;
-    if (act && j + 1 < ny) { hxn = hx[idx + nx]; hyn = hy[idx + nx]; hzn = hz[idx + nx]; }
+    if (act && j + 2 < ny) { hxn = hx[idx + 2 * nx]; hyn = hy[idx + 2 * nx]; hzn = hz[idx + 2 * nx]; }
     if (act) {
-      const T* X0 = &ring[0][(j - 1) & (R - 1)][c0];
-      const T* X1 = &ring[0][j & (R - 1)][c0];
-      const T* X2 = &ring[0][(j + 1) & (R - 1)][c0];
-      const T* Y0 = &ring[1][(j - 1) & (R - 1)][c0];
-      const T* Y1 = &ring[1][j & (R - 1)][c0];
-      const T* Y2 = &ring[1][(j + 1) & (R - 1)][c0];
-      const T* Z0 = &ring[2][(j - 1) & (R - 1)][c0];
-      const T* Z1 = &ring[2][j & (R - 1)][c0];
-      const T* Z2 = &ring[2][(j + 1) & (R - 1)][c0];
-      const T* P0 = &ring[3][(j - 1) & (R - 1)][c0];
-      const T* P1 = &ring[3][j & (R - 1)][c0];
+      const T* X0 = &ring[0][slot(j - 1)][c0];
+      const T* X1 = &ring[0][slot(j)][c0];
+      const T* X2 = &ring[0][slot(j + 1)][c0];
+      const T* Y0 = &ring[1][slot(j - 1)][c0];
+      const T* Y1 = &ring[1][slot(j)][c0];
+      const T* Y2 = &ring[1][slot(j + 1)][c0];
+      const T* Z0 = &ring[2][slot(j - 1)][c0];
+      const T* Z1 = &ring[2][slot(j)][c0];
+      const T* Z2 = &ring[2][slot(j + 1)][c0];
+      const T* P0 = &ring[3][slot(j - 1)][c0];
+      const T* P1 = &ring[3][slot(j)][c0];
       const T* tr = tab + (size_t)j * MT_W;
 
       const T ux_c = X1[0], ux_ip = X1[1], ux_im = X1[-1], ux_jp = X2[0], ux_jm = X0[0];
@@ -244,12 +256,11 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
       g2 = uz_c + d2 + __ldg(tr + MT_CP0) * uz_jp;
       uxs[idx] = g0; uys[idx] = g1; uzs[idx] = g2;
     }
-    if (r < ny) store_row(r);
-    else if (r == ny) ghost_row(ny);
-    __syncthreads();
     idx += nx;
-    hxo = hxn; hyo = hyn; hzo = hzn;
+    hxo = hx1; hyo = hy1; hzo = hz1;
+    hx1 = hxn; hy1 = hyn; hz1 = hzn;
   }
+  cp_async_wait<0>();
   if (!act) return;
 
   // back substitution u*_j = g_j - cp_j u*_{j+1}, rows loaded in batches of 8
@@ -278,12 +289,115 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
   }
 }
 
+// ---------------------------------------------------------------------------
+// FluidVelUpdate (src/CFD_2nd/m_TScheme.f90:281-306) + PressureUpdate_PIMP
+// (src/CFD_2nd/m_TSchemePIMP_inc.f90:852-873) as a march: a thread owns one
+// (i, k) column over a chunk of MJ rows and keeps phi at j-1, j, j+1 in
+// registers (Neumann ghosts of SetBC_and_UpdateHalo_pr at the walls).  The
+// block's sum of ux * s1coe (the next substep's bulk constraint, clcRhsX_PIMP
+// :60-74) goes to part[block].  mode 1: projection only (pmAlpha = 1, p kept).
+// ---------------------------------------------------------------------------
+constexpr int MJ = 32;  // rows per block of the march projection
+
+__device__ __forceinline__ double block_sum128(double v, double* sh /* 4 */) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  return threadIdx.x == 0 ? (sh[0] + sh[1]) + (sh[2] + sh[3]) : 0.0;
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_proj_march(Geo<T> g, Metrics<T> m, const T* uxs, const T* uys,
+                                                    const T* uzs, T* ux, T* uy, T* uz, T* __restrict__ pr,
+                                                    const T* __restrict__ phi, double* __restrict__ part, int mode,
+                                                    const DevScalars* __restrict__ sc) {
+  __shared__ double red[4];
+  if (sc->status) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long plane = (long long)nx * ny;
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31), k = blockIdx.y * 4 + (threadIdx.x >> 5);
+  const int j0 = blockIdx.z * MJ, j1 = min(j0 + MJ, ny);
+  double s = 0.0;
+  if (i < nx && k < nz) {
+    const long long col = i + plane * k;
+    const long long dxm = i == 0 ? nx - 1 : -1;                      // offset to i-1
+    const long long dzm = k == 0 ? (long long)(nz - 1) * plane : -plane;  // offset to k-1
+    const T pmAlpha = mode == 0 ? (T)sc->pmAlpha : (T)1;
+    const T pmBeta = (T)sc->pmBeta;
+    const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha;
+    T pm = __ldg(phi + col + (long long)(j0 > 0 ? j0 - 1 : 0) * nx);
+    T pc = __ldg(phi + col + (long long)j0 * nx);
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const long long idx = col + (long long)j * nx;
+      const T pp = __ldg(phi + col + (long long)(j + 1 < ny ? j + 1 : ny - 1) * nx);
+      const T phim_x = __ldg(phi + idx + dxm), phim_z = __ldg(phi + idx + dzm);
+      const int jc = j + 1;
+      const T sucacEta2 = m.rdyc[jc] * pmAlpha;
+      const T uxn = uxs[idx] - (pc - phim_x) * rdxEta2;
+      const T uyn = uys[idx] - (pc - pm) * sucacEta2;
+      const T uzn = uzs[idx] - (pc - phim_z) * rdzEta2;
+      ux[idx] = uxn; uy[idx] = uyn; uz[idx] = uzn;
+      if (mode == 0) {
+        const T pmBetap = -pmBeta * m.ap2Pr[jc];
+        const T pmBetac = -pmBeta * m.ac2Pr[jc] + (T)1;
+        const T pmBetam = -pmBeta * m.am2Pr[jc];
+        pr[idx] = pr[idx] + pmBetap * pp + pmBetac * pc + pmBetam * pm;
+      }
+      s += (double)uxn * (double)m.s1coe[jc];
+      pm = pc; pc = pp;
+    }
+  }
+  const double bs = block_sum128(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
+}
+
+// the same partial sums of ux * s1coe for a freshly uploaded field
+template <class T>
+__global__ void __launch_bounds__(128) k_bulk_march(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                    double* __restrict__ part) {
+  __shared__ double red[4];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31), k = blockIdx.y * 4 + (threadIdx.x >> 5);
+  const int j0 = blockIdx.z * MJ, j1 = min(j0 + MJ, ny);
+  double s = 0.0;
+  if (i < nx && k < nz) {
+    const long long col = i + (long long)nx * ny * k;
+    for (int j = j0; j < j1; ++j) s += (double)ux[col + (long long)j * nx] * (double)m.s1coe[j + 1];
+  }
+  const double bs = block_sum128(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
+}
+
+static dim3 march_proj_grid(const ch3d_ctx* c) { return dim3((c->nx + 31) / 32, (c->nz + 3) / 4, (c->ny + MJ - 1) / MJ); }
+int march_npart(const ch3d_ctx* c) {
+  const dim3 g = march_proj_grid(c);
+  return (int)(g.x * g.y * g.z);
+}
+
+template <class T> static cudaError_t proj_march_t(ch3d_ctx* c, int mode) {
+  T** f = (T**)c->f;
+  T* in[3] = {mode == 1 ? f[0] : f[12], mode == 1 ? f[1] : f[13], mode == 1 ? f[2] : f[14]};
+  k_proj_march<T><<<march_proj_grid(c), 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1], in[2],
+                                                              f[0], f[1], f[2], f[3], f[10], c->part, mode, c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_proj_march(ch3d_ctx* c, int mode) {
+  return c->fp32 ? proj_march_t<float>(c, mode) : proj_march_t<double>(c, mode);
+}
+template <class T> static cudaError_t bulk_march_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  k_bulk_march<T><<<march_proj_grid(c), 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], c->part);
+  return cudaGetLastError();
+}
+cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float>(c) : bulk_march_t<double>(c); }
+
 template <class T> static cudaError_t rhs_march_t(ch3d_ctx* c) {
-  constexpr int BZ = 4;
+  constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
   T** f = (T**)c->f;
   k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab, c->sc);
   dim3 grid((c->nx + 31) / 32, (c->nz + BZ - 1) / BZ);
-  k_rhs_march<T, BZ><<<grid, 32 * BZ, 0, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3],
+  k_rhs_march<T, BZ, D, RS><<<grid, 32 * BZ, 0, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3],
                                                      f[4], f[5], f[6], f[12], f[13], f[14], c->sc);
   return cudaGetLastError();
 }

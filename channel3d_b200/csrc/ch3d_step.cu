@@ -1129,7 +1129,7 @@ __global__ void __launch_bounds__(256) k_reduce_partials(const double* __restric
 }
 
 cudaError_t launch_substep_setup(ch3d_ctx* c, int ns) {
-  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part, c->npart, c->red1);
+  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part, c->march ? c->npart_m : c->npart, c->red1);
   const double norm_bulk = 1.0 / ((double)c->nx * (double)c->nz) / (c->cfg.ybulk2 - c->cfg.ybulk1);
   k_substep_setup<<<1, 256, 0, c->stream>>>(c->sc, c->red1, CH3D_NRED, ns, c->gam[ns - 1], c->the[ns - 1],
                                             c->alp[ns - 1], c->cfg.xnu, c->cfg.IsUxConst, c->cfg.ubulk, norm_bulk,
@@ -1302,6 +1302,7 @@ template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {
 cudaError_t launch_xifft(ch3d_ctx* c) { return c->fp32 ? xifft_t<float>(c) : xifft_t<double>(c); }
 
 template <class T> static cudaError_t proj_t(ch3d_ctx* c, int mode) {
+  if (c->march) return launch_proj_march(c, mode);
   T** f = (T**)c->f;
   T* in[3] = {mode == 1 ? f[0] : f[12], mode == 1 ? f[1] : f[13], mode == 1 ? f[2] : f[14]};
   k_proj<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1], in[2], f[0],
@@ -1311,6 +1312,7 @@ template <class T> static cudaError_t proj_t(ch3d_ctx* c, int mode) {
 cudaError_t launch_proj(ch3d_ctx* c, int mode) { return c->fp32 ? proj_t<float>(c, mode) : proj_t<double>(c, mode); }
 
 template <class T> static cudaError_t bulk_t(ch3d_ctx* c) {
+  if (c->march) return launch_bulk_march(c);
   T** f = (T**)c->f;
   k_bulk_partial<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], c->part);
   return cudaGetLastError();

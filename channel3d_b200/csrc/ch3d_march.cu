@@ -327,25 +327,43 @@ __global__ void __launch_bounds__(128) k_proj_march(Geo<T> g, Metrics<T> m, cons
     const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha;
     T pm = __ldg(phi + col + (long long)(j0 > 0 ? j0 - 1 : 0) * nx);
     T pc = __ldg(phi + col + (long long)j0 * nx);
-#pragma unroll 4
-    for (int j = j0; j < j1; ++j) {
-      const long long idx = col + (long long)j * nx;
-      const T pp = __ldg(phi + col + (long long)(j + 1 < ny ? j + 1 : ny - 1) * nx);
-      const T phim_x = __ldg(phi + idx + dxm), phim_z = __ldg(phi + idx + dzm);
-      const int jc = j + 1;
-      const T sucacEta2 = m.rdyc[jc] * pmAlpha;
-      const T uxn = uxs[idx] - (pc - phim_x) * rdxEta2;
-      const T uyn = uys[idx] - (pc - pm) * sucacEta2;
-      const T uzn = uzs[idx] - (pc - phim_z) * rdzEta2;
-      ux[idx] = uxn; uy[idx] = uyn; uz[idx] = uzn;
-      if (mode == 0) {
-        const T pmBetap = -pmBeta * m.ap2Pr[jc];
-        const T pmBetac = -pmBeta * m.ac2Pr[jc] + (T)1;
-        const T pmBetam = -pmBeta * m.am2Pr[jc];
-        pr[idx] = pr[idx] + pmBetap * pp + pmBetac * pc + pmBetam * pm;
+    // rows in batches of PB: all loads of a batch before its stores (u* and u may
+    // be the same arrays, mode 1, so the compiler cannot reorder them itself)
+    constexpr int PB = 4;
+    for (int jb = j0; jb < j1; jb += PB) {
+      T vpp[PB], vpx[PB], vpz[PB], vu[PB], vv[PB], vw[PB], vp[PB], mr[PB], mp[PB], mc[PB], mm[PB], ms[PB];
+#pragma unroll
+      for (int b = 0; b < PB; ++b) {
+        const int j = jb + b < j1 ? jb + b : j1 - 1;
+        const long long idx = col + (long long)j * nx;
+        vpp[b] = __ldg(phi + col + (long long)(j + 1 < ny ? j + 1 : ny - 1) * nx);
+        vpx[b] = __ldg(phi + idx + dxm);
+        vpz[b] = __ldg(phi + idx + dzm);
+        vu[b] = uxs[idx]; vv[b] = uys[idx]; vw[b] = uzs[idx];
+        vp[b] = mode == 0 ? pr[idx] : (T)0;
+        mr[b] = m.rdyc[j + 1]; mp[b] = m.ap2Pr[j + 1]; mc[b] = m.ac2Pr[j + 1]; mm[b] = m.am2Pr[j + 1];
+        ms[b] = m.s1coe[j + 1];
       }
-      s += (double)uxn * (double)m.s1coe[jc];
-      pm = pc; pc = pp;
+#pragma unroll
+      for (int b = 0; b < PB; ++b) {
+        const int j = jb + b;
+        if (j >= j1) break;
+        const long long idx = col + (long long)j * nx;
+        const T pp = vpp[b];
+        const T sucacEta2 = mr[b] * pmAlpha;
+        const T uxn = vu[b] - (pc - vpx[b]) * rdxEta2;
+        const T uyn = vv[b] - (pc - pm) * sucacEta2;
+        const T uzn = vw[b] - (pc - vpz[b]) * rdzEta2;
+        ux[idx] = uxn; uy[idx] = uyn; uz[idx] = uzn;
+        if (mode == 0) {
+          const T pmBetap = -pmBeta * mp[b];
+          const T pmBetac = -pmBeta * mc[b] + (T)1;
+          const T pmBetam = -pmBeta * mm[b];
+          pr[idx] = vp[b] + pmBetap * pp + pmBetac * pc + pmBetam * pm;
+        }
+        s += (double)uxn * (double)ms[b];
+        pm = pc; pc = pp;
+      }
     }
   }
   const double bs = block_sum128(s, red);

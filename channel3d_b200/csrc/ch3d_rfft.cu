@@ -15,6 +15,9 @@
 namespace ch3d {
 
 constexpr int kXWarps = 4;  // warps per block of the x kernels
+// padded exchange buffers for the 16-byte FP64 points (the 8-byte FP32 points
+// conflict less without the padding)
+template <class T> constexpr bool kPadX = sizeof(T) == 8;
 
 // Plans (N, P, radices): exchange radices multiply to P, in-thread ones to N / P.
 typedef RPlan<384, 32, 4, 4, 2, 12> PlanN384;
@@ -25,7 +28,7 @@ typedef RPlan<576, 48, 4, 4, 3, 12> PlanN576;
 typedef RPlan<128, 16, 8, 2, 8> PlanZ128;
 
 template <class T, class PL>
-__global__ void __launch_bounds__(32 * kXWarps, 4) k_prsrc_xfft_r(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+__global__ void __launch_bounds__(32 * kXWarps, sizeof(T) == 4 ? 6 : 4) k_prsrc_xfft_r(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
                                                               const T* __restrict__ uy, const T* __restrict__ uz,
                                                               typename CplxOf<T>::type* __restrict__ spec,
                                                               const typename CplxOf<T>::type* __restrict__ tw,
@@ -33,7 +36,7 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_prsrc_xfft_r(Geo<T> g, Metr
                                                               int mode, DevScalars* __restrict__ sc, T* __restrict__ pr) {
   typedef typename CplxOf<T>::type CT;
   constexpr int M = PL::N, P = PL::P, E = PL::E, LPW = 32 / P;
-  __shared__ CT sm[kXWarps * LPW][M];
+  __shared__ CT sm[kXWarps * LPW][PL::padded_len()];
   __shared__ double wred[kXWarps];
   if (sc->status) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz, nxh = g.nxh;
@@ -69,14 +72,16 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_prsrc_xfft_r(Geo<T> g, Metr
           r0 = div4_cell(g, c4, sucaj, ux, uy, uz, i0, j, k);
           r1 = div4_cell(g, c4, sucaj, ux, uy, uz, i0 + 1, j, k);
         } else {
-          const T u0 = __ldg(ux + base + i0), u1 = __ldg(ux + base + i0 + 1), u2 = __ldg(ux + base + i2);
-          const T v0 = __ldg(uy + base + i0), v1 = __ldg(uy + base + i0 + 1);
-          const T v0p = top ? (T)g.bc.uy_hi : __ldg(uy + base + nx + i0);
-          const T v1p = top ? (T)g.bc.uy_hi : __ldg(uy + base + nx + i0 + 1);
-          const T w0 = __ldg(uz + base + i0), w1 = __ldg(uz + base + i0 + 1);
-          const T w0p = __ldg(uz + basep + i0), w1p = __ldg(uz + basep + i0 + 1);
-          r0 = (u1 - u0) * rdx + (v0p - v0) * sucaj + (w0p - w0) * rdz;
-          r1 = (u2 - u1) * rdx + (v1p - v1) * sucaj + (w1p - w1) * rdz;
+          // pairs (i0, i0+1) as one aligned vector load (nx and i0 even)
+          typedef typename CplxOf<T>::type T2;
+          const T2 u01 = __ldg(reinterpret_cast<const T2*>(ux + base + i0));
+          const T u2 = __ldg(ux + base + i2);
+          const T2 v01 = __ldg(reinterpret_cast<const T2*>(uy + base + i0));
+          const T2 v01p = top ? mk((T)g.bc.uy_hi, (T)g.bc.uy_hi) : __ldg(reinterpret_cast<const T2*>(uy + base + nx + i0));
+          const T2 w01 = __ldg(reinterpret_cast<const T2*>(uz + base + i0));
+          const T2 w01p = __ldg(reinterpret_cast<const T2*>(uz + basep + i0));
+          r0 = (u01.y - u01.x) * rdx + (v01p.x - v01.x) * sucaj + (w01p.x - w01.x) * rdz;
+          r1 = (u2 - u01.y) * rdx + (v01p.y - v01.y) * sucaj + (w01p.y - w01.y) * rdz;
         }
         if (mode == 0 && g.implicit == 2) {  // clcPrSrc_FIMP: pressure += -xnu/2 div (m_TScheme.f90:271)
           const T xnuhm = -(T)0.5 * g.xnu;
@@ -90,10 +95,10 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_prsrc_xfft_r(Geo<T> g, Metr
 #pragma unroll
       for (int q = 0; q < E; ++q) z[q] = mk((T)0, (T)0);
     }
-    PL::run(z, L, 1, t, tw, WarpSync());
+    PL::template run<kPadX<T>>(z, L, 1, t, tw, WarpSync());
     // real-to-complex split X_k = (Z_k + conj Z_{M-k})/2 - i W_nx^k (Z_k - conj Z_{M-k})/2, k = 0..M
 #pragma unroll
-    for (int q = 0; q < E; ++q) L[t + P * q] = z[q];
+    for (int q = 0; q < E; ++q) L[xpos<kPadX<T>>(t + P * q, 1)] = z[q];
     __syncwarp();
     if (valid) {
       const T hf = (T)0.5;
@@ -102,8 +107,8 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_prsrc_xfft_r(Geo<T> g, Metr
       for (int q = 0; q <= E; ++q) {
         const int kk = q < E ? t + P * q : M;
         if (q == E && t != 0) break;
-        const CT a = L[kk == M ? 0 : kk];
-        const CT b = cconj(L[kk == 0 ? 0 : M - kk]);
+        const CT a = L[xpos<kPadX<T>>(kk == M ? 0 : kk, 1)];
+        const CT b = cconj(L[xpos<kPadX<T>>(kk == 0 ? 0 : M - kk, 1)]);
         const CT e = mk(hf * (a.x + b.x), hf * (a.y + b.y));
         const CT dd = csub(a, b);
         const CT o = mk(hf * dd.y, -hf * dd.x);  // (a-b)/(2i)
@@ -130,7 +135,7 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_xifft_r(Geo<T> g, const typ
                                                          const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
   constexpr int M = PL::N, P = PL::P, E = PL::E, LPW = 32 / P;
-  __shared__ CT sm[kXWarps * LPW][M];
+  __shared__ CT sm[kXWarps * LPW][PL::padded_len()];
   if (sc->status) return;
   const int nx = g.nx, nxh = g.nxh;
   const int nlines = g.ny * g.nz;
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_xifft_r(Geo<T> g, const typ
 #pragma unroll
       for (int q = 0; q < E; ++q) z[q] = mk((T)0, (T)0);
     }
-    PL::run(z, L, 1, t, tw, WarpSync());
+    PL::template run<kPadX<T>>(z, L, 1, t, tw, WarpSync());
     if (valid) {
       typedef typename CplxOf<T>::type T2;
       T2* out = reinterpret_cast<T2*>(phi + (long long)nx * line);
@@ -189,7 +194,7 @@ __global__ void __launch_bounds__(LZ * PL::P) k_zfft_r(Geo<T> g, typename CplxOf
     v[q] = valid ? col[zs * (t + P * q)] : mk((T)0, (T)0);
     if (inverse) v[q] = cconj(v[q]);
   }
-  PL::run(v, sm + l, LZ, t, tw, BlockSync());
+  PL::template run<false>(v, sm + l, LZ, t, tw, BlockSync());
   if (valid) {
 #pragma unroll
     for (int q = 0; q < E; ++q) col[zs * (t + P * q)] = inverse ? cconj(v[q]) : v[q];
@@ -257,7 +262,7 @@ bool launch_xifft_r(ch3d_ctx* c, cudaError_t* err) { return c->fp32 ? xifft_r_t<
 
 template <class T> static bool zfft_r_t(ch3d_ctx* c, int inverse, cudaError_t* err) {
   typedef typename CplxOf<T>::type CT;
-  constexpr int LZ = 8;
+  constexpr int LZ = sizeof(T) == 8 ? 4 : 8;  // kx lines per block (measured best per precision)
   return with_zplan(c->nz, [&](auto plan) {
     typedef decltype(plan) PL;
     auto kern = k_zfft_r<T, PL, LZ>;

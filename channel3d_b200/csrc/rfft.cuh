@@ -78,9 +78,14 @@ struct BlockSync {
   __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
 
+// Position of point p in a line's exchange buffer: p * ss, or with PAD one
+// 16-byte gap after every 8 points (p + p / 8), which spreads the stride-R
+// writes of the first pass over all shared-memory banks.
+template <bool PAD> __device__ __forceinline__ int xpos(int p, int ss) { return PAD ? p + (p >> 3) : p * ss; }
+
 // One pass (radix R, stride NS) over the thread's E points; sm: the line's
-// exchange buffer, point p at sm[p * ss].
-template <class CT, int N, int P, int E, int NS, int R, class Sync>
+// exchange buffer (point p at xpos<PAD>(p, ss)).
+template <class CT, int N, int P, int E, int NS, int R, bool PAD, class Sync>
 __device__ __forceinline__ void rs_pass(CT (&v)[E], CT* sm, int ss, int t, const CT* __restrict__ tw, Sync sync) {
   static_assert(E % R == 0, "radix must divide the points per thread");
   constexpr int Q = E / R;
@@ -102,7 +107,7 @@ __device__ __forceinline__ void rs_pass(CT (&v)[E], CT* sm, int ss, int t, const
     if (EXCH) {
       const int base = (b - kk) * R + kk;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sm[(base + r * NS) * ss] = x[r];
+      for (int r = 0; r < R; ++r) sm[xpos<PAD>(base + r * NS, ss)] = x[r];
     } else {
       constexpr int s = EXCH ? 1 : NS / P;
 #pragma unroll
@@ -112,7 +117,7 @@ __device__ __forceinline__ void rs_pass(CT (&v)[E], CT* sm, int ss, int t, const
   if (EXCH) {
     sync();
 #pragma unroll
-    for (int m = 0; m < E; ++m) v[m] = sm[(t + P * m) * ss];
+    for (int m = 0; m < E; ++m) v[m] = sm[xpos<PAD>(t + P * m, ss)];
     sync();
   } else {
 #pragma unroll
@@ -120,26 +125,29 @@ __device__ __forceinline__ void rs_pass(CT (&v)[E], CT* sm, int ss, int t, const
   }
 }
 
-template <class CT, int N, int P, int E, int NS, int... Rs> struct RRun;
-template <class CT, int N, int P, int E, int NS> struct RRun<CT, N, P, E, NS> {
+template <class CT, int N, int P, int E, bool PAD, int NS, int... Rs> struct RRun;
+template <class CT, int N, int P, int E, bool PAD, int NS> struct RRun<CT, N, P, E, PAD, NS> {
   template <class Sync> __device__ __forceinline__ static void run(CT (&)[E], CT*, int, int, const CT*, Sync) {
     static_assert(NS == N, "plan radices must multiply to N");
   }
 };
-template <class CT, int N, int P, int E, int NS, int R, int... Rs> struct RRun<CT, N, P, E, NS, R, Rs...> {
+template <class CT, int N, int P, int E, bool PAD, int NS, int R, int... Rs> struct RRun<CT, N, P, E, PAD, NS, R, Rs...> {
   template <class Sync>
   __device__ __forceinline__ static void run(CT (&v)[E], CT* sm, int ss, int t, const CT* __restrict__ tw, Sync sync) {
-    rs_pass<CT, N, P, E, NS, R>(v, sm, ss, t, tw, sync);
-    RRun<CT, N, P, E, NS * R, Rs...>::run(v, sm, ss, t, tw, sync);
+    rs_pass<CT, N, P, E, NS, R, PAD>(v, sm, ss, t, tw, sync);
+    RRun<CT, N, P, E, PAD, NS * R, Rs...>::run(v, sm, ss, t, tw, sync);
   }
 };
 
-// A plan: N points, P threads per line, radices in pass order.
+// A plan: N points, P threads per line, radices in pass order.  run<PAD>:
+// PAD for a line-contiguous buffer of padded_len() points (ss unused),
+// otherwise point p at sm[p * ss].
 template <int N_, int P_, int... Rs> struct RPlan {
   static constexpr int N = N_, P = P_, E = N_ / P_;
-  template <class CT, class Sync>
+  static constexpr int padded_len() { return N_ + N_ / 8; }
+  template <bool PAD, class CT, class Sync>
   __device__ __forceinline__ static void run(CT (&v)[E], CT* sm, int ss, int t, const CT* __restrict__ tw, Sync sync) {
-    RRun<CT, N, P, E, 1, Rs...>::run(v, sm, ss, t, tw, sync);
+    RRun<CT, N, P, E, PAD, 1, Rs...>::run(v, sm, ss, t, tw, sync);
   }
 };
 

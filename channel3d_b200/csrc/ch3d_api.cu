@@ -366,6 +366,23 @@ int upload_field(ch3d_ctx* c, int q, int layout, const double* a, int comp) {
     CU(cudaStreamSynchronize(c->stream));
     return CH3D_OK;
   }
+  if (layout == CH3D_LAYOUT_INTERIOR) {
+    // FP32 fields from FP64 interior arrays: FP64 chunks through the spectrum
+    // buffer (free between steps), converted on the device
+    if (!a) {
+      CU(cudaMemsetAsync(c->f[q], 0, (size_t)c->N * sizeof(T), c->stream));
+    } else {
+      const long long cap = (long long)((size_t)c->NS * 2 * sizeof(T) / sizeof(double));
+      for (long long off = 0; off < c->N; off += cap) {
+        const long long n = c->N - off < cap ? c->N - off : cap;
+        CU(cudaMemcpyAsync(c->spec, a + off, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CU(launch_convert(c, c->spec, (T*)c->f[q] + off, n, 1));
+      }
+    }
+    if (comp == 1) CU(launch_fill_row0(c, q, c->cfg.uyBcValue[2]));  // uy(ic,1,kc) = uy_ym
+    CU(cudaStreamSynchronize(c->stream));
+    return CH3D_OK;
+  }
   std::vector<T> h((size_t)c->N);
   size_t n = 0;
   for (int k = 1; k <= c->nz; ++k)
@@ -384,6 +401,16 @@ template <class T>
 int download_field(ch3d_ctx* c, int q, int layout, double* a, int comp) {
   if (sizeof(T) == sizeof(double) && layout == CH3D_LAYOUT_INTERIOR) {
     CU(cudaMemcpyAsync(a, c->f[q], (size_t)c->N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return CH3D_OK;
+  }
+  if (layout == CH3D_LAYOUT_INTERIOR) {  // FP32 fields: converted on the device, FP64 chunks to the host
+    const long long cap = (long long)((size_t)c->NS * 2 * sizeof(T) / sizeof(double));
+    for (long long off = 0; off < c->N; off += cap) {
+      const long long n = c->N - off < cap ? c->N - off : cap;
+      CU(launch_convert(c, (const T*)c->f[q] + off, c->spec, n, 0));
+      CU(cudaMemcpyAsync(a + off, c->spec, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
     CU(cudaStreamSynchronize(c->stream));
     return CH3D_OK;
   }

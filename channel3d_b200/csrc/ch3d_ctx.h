@@ -121,6 +121,7 @@ cudaError_t launch_diag(ch3d_ctx* c);
 cudaError_t launch_stats(ch3d_ctx* c);
 cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot);
 cudaError_t launch_fill_row0(ch3d_ctx* c, int q, double v);  // field q: every j = 0 value := v
+cudaError_t launch_convert(ch3d_ctx* c, const void* src, void* dst, long long n, int to_f32);  // FP64 <-> FP32
 // 4th-order solver (ch3d_step4.cu)
 cudaError_t launch_rhs4(ch3d_ctx* c);                  // stage path: interpolation + RhsX/Y/Z
 cudaError_t launch_rhs4_uhat(ch3d_ctx* c);             // fused step path: interpolation + RHS + y solve -> u*

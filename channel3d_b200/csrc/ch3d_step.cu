@@ -1339,6 +1339,24 @@ template <class T> __global__ void k_fill_row0(T* __restrict__ a, int nx, int ny
   const int i = (int)(t % nx), k = (int)(t / nx);
   a[i + (long long)nx * ny * k] = v;
 }
+// FP64 <-> FP32 conversion of n values (mixed-precision upload/download)
+__global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    b[t] = (float)a[t];
+}
+__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    b[t] = (double)a[t];
+}
+cudaError_t launch_convert(ch3d_ctx* c, const void* src, void* dst, long long n, int to_f32) {
+  const long long nb = (n + 255) / 256;
+  const unsigned g = (unsigned)(nb < 148LL * 32 ? nb : 148LL * 32);
+  if (n <= 0) return cudaSuccess;
+  if (to_f32) k_f64_to_f32<<<g, 256, 0, c->stream>>>((const double*)src, (float*)dst, n);
+  else k_f32_to_f64<<<g, 256, 0, c->stream>>>((const float*)src, (double*)dst, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fill_row0(ch3d_ctx* c, int q, double v) {
   const unsigned nb = (unsigned)(((long long)c->nx * c->nz + 255) / 256);
   if (c->fp32) k_fill_row0<float><<<nb, 256, 0, c->stream>>>((float*)c->f[q], c->nx, c->ny, c->nz, (float)v);

@@ -609,6 +609,7 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     if (cudaMalloc(&c->hfac, nf * sizeof(double)) != cudaSuccess) return cleanup(fail(CH3D_ERR_NOMEM, "hfac"));
     if (cudaMalloc(&c->mtab, march_table_bytes(c->ny)) != cudaSuccess)
       return cleanup(fail(CH3D_ERR_NOMEM, "march table"));
+    if (march_table_reset(c) != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "march table"));
   }
   {
     // Poisson y-solve (Thomas) factors per (kx, |kz|), computed once

@@ -96,6 +96,7 @@ cudaError_t launch_uhat(ch3d_ctx* c);                  // stage path: Rhs arrays
 // 2nd-order PIMP step: RHS + y solves as a column march (ch3d_march.cu)
 cudaError_t launch_rhs_march(ch3d_ctx* c);             // u -> u*, Hist, with its row table
 size_t march_table_bytes(int ny);
+cudaError_t march_table_reset(ch3d_ctx* c);           // forget the cached factors
 cudaError_t launch_proj_march(ch3d_ctx* c, int mode);   // projection + pressure update + bulk partials
 cudaError_t launch_bulk_march(ch3d_ctx* c);            // bulk partials of an uploaded field
 int march_npart(const ch3d_ctx* c);

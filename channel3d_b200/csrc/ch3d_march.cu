@@ -31,12 +31,31 @@ enum {
   MT_A0, MT_RM0, MT_CP0, MT_A1, MT_RM1, MT_CP1, MT_W
 };
 
-size_t march_table_bytes(int ny) { return (size_t)ny * MT_W * sizeof(double); }
+// Layout of the march table buffer: one table per RK substep (ns = 1..3,
+// ny * MT_W values of precision T each), then per substep the pmBeta its
+// factors were computed for (FP64 bit patterns; all ones = not yet computed).
+constexpr int kMarchTables = 3;
+size_t march_table_bytes(int ny) {
+  return (size_t)kMarchTables * ny * MT_W * sizeof(double) + kMarchTables * sizeof(unsigned long long);
+}
+static unsigned long long* march_beta_slots(void* mtab, int ny) {
+  return (unsigned long long*)((char*)mtab + (size_t)kMarchTables * ny * MT_W * sizeof(double));
+}
+cudaError_t march_table_reset(ch3d_ctx* c) {
+  return cudaMemsetAsync(march_beta_slots(c->mtab, c->ny), 0xff, kMarchTables * sizeof(unsigned long long),
+                         c->stream);
+}
 
+// Table of substep sc->ns; skipped when it already holds the factors of this
+// pmBeta (constant dt: computed once per substep of the run).
 template <class T>
-__global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__ tab,
-                              const DevScalars* __restrict__ sc) {
+__global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__ tabs,
+                              unsigned long long* __restrict__ beta_slot, const DevScalars* __restrict__ sc) {
   if (sc->status) return;
+  const int q = sc->ns - 1;
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(sc->pmBeta);
+  if (beta_slot[q] == bits) return;  // uniform across the block
+  T* tab = tabs + (size_t)q * ny * MT_W;
   if (threadIdx.x == 0 || threadIdx.x == 32) {  // one thread per Helmholtz set, sequential in j
     const int set = threadIdx.x == 0 ? 0 : 1;
     const double pmBeta = sc->pmBeta;
@@ -61,6 +80,8 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
     row[MT_AP2C] = m.ap2c[jc]; row[MT_AC2C] = m.ac2c[jc]; row[MT_AM2C] = m.am2c[jc];
     row[MT_AP2P] = m.ap2p[jc]; row[MT_AC2P] = m.ac2p[jc]; row[MT_AM2P] = m.am2p[jc];
   }
+  __syncthreads();
+  if (threadIdx.x == 0) beta_slot[q] = bits;
 }
 
 // asynchronous 4- or 8-byte copy global -> shared (cp.async, completion by groups)
@@ -79,7 +100,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // iteration j, must differ from the slots of rows j-1, j, j+1 that other
 // threads still read: RS >= D + 4.
 template <class T, int BZ, int D, int RS>
-__global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
+__global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * BZ))  // FP32: 5 blocks per SM
     k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ ux, const T* __restrict__ uy,
                 const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
                 T* __restrict__ hz, T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
@@ -91,6 +112,7 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
   if (sc->status) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long plane = (long long)nx * ny;
+  tab += (size_t)(sc->ns - 1) * ny * MT_W;  // this substep's table
   const int tid = threadIdx.x, tx = tid & 31, tz = tid >> 5;
   const int i0 = blockIdx.x * BX, k0 = blockIdx.y * BZ;
   const int i = i0 + tx, k = k0 + tz;
@@ -162,7 +184,9 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
   T g0 = (T)0, g1 = (T)0, g2 = (T)0;       // g of the last row (= u* of row ny-1)
   T hxo = (T)0, hyo = (T)0, hzo = (T)0;    // Hist of row j
   T hx1 = (T)0, hy1 = (T)0, hz1 = (T)0;    // Hist of row j+1
-  if (act) {
+  // pmTheta = 0 (first RK3 substep): the old Hist does not enter, so it is not read
+  const bool hread = act && pmTheta != (T)0;
+  if (hread) {
     hxo = hx[idx]; hyo = hy[idx]; hzo = hz[idx];
     if (ny > 1) { hx1 = hx[idx + nx]; hy1 = hy[idx + nx]; hz1 = hz[idx + nx]; }
   }
@@ -175,7 +199,7 @@ __global__ void __launch_bounds__(32 * BZ, 512 / (32 * BZ))
     if (j + D + 2 < ny) issue_row(j + D + 2);
     cp_async_commit();
     T hxn = (T)0, hyn = (T)0, hzn = (T)0;
-    if (act && j + 2 < ny) { hxn = hx[idx + 2 * nx]; hyn = hy[idx + 2 * nx]; hzn = hz[idx + 2 * nx]; }
+    if (hread && j + 2 < ny) { hxn = hx[idx + 2 * nx]; hyn = hy[idx + 2 * nx]; hzn = hz[idx + 2 * nx]; }
     if (act) {
       const T* X0 = &ring[0][slot(j - 1)][c0];
       const T* X1 = &ring[0][slot(j)][c0];
@@ -413,7 +437,8 @@ cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float
 template <class T> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
   T** f = (T**)c->f;
-  k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab, c->sc);
+  k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab,
+                                             march_beta_slots(c->mtab, c->ny), c->sc);
   dim3 grid((c->nx + 31) / 32, (c->nz + BZ - 1) / BZ);
   k_rhs_march<T, BZ, D, RS><<<grid, 32 * BZ, 0, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3],
                                                      f[4], f[5], f[6], f[12], f[13], f[14], c->sc);

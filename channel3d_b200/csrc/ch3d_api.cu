@@ -639,6 +639,7 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     c->march = march_path(c);
     c->npart_m = march_npart(c);
     if (c->npart_m > c->npart) c->npart = c->npart_m;
+    if (diag_npart(c) > c->npart) c->npart = diag_npart(c);
     if (cudaMalloc(&c->part, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->part2, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->red1, CH3D_NRED * sizeof(double)) != cudaSuccess ||

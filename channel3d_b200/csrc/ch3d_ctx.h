@@ -119,6 +119,7 @@ cudaError_t poisson_noalloc(int nx, int ny, int nz, double xlx, double zlz, cons
 cudaError_t launch_proj(ch3d_ctx* c, int mode);        // mode 0: u = u* - a grad phi, p update; 1: u -= grad phi
 cudaError_t launch_bulk_partials(ch3d_ctx* c);
 cudaError_t launch_diag(ch3d_ctx* c);
+int diag_npart(const ch3d_ctx* c);                     // partial sums k_diag writes to part2
 cudaError_t launch_stats(ch3d_ctx* c);
 cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot);
 cudaError_t launch_fill_row0(ch3d_ctx* c, int q, double v);  // field q: every j = 0 value := v

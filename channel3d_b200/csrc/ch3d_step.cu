@@ -1010,59 +1010,71 @@ __global__ void __launch_bounds__(256) k_bulk_partial(Geo<T> g, Metrics<T> m, co
 }
 
 // CheckDivergence, CalcVmax, CalcMaxCFL of the next step, CalcUxAver partials
-// (src/CFD_2nd/m_Tools.f90:21-104,250-270).
+// (src/CFD_2nd/m_Tools.f90:21-104,250-270).  A thread walks `rows` rows of
+// one (i, k) column (uy(j+1) carried to the next row), a block of 32 x 4
+// columns reduces its maxima and sum and issues one atomic per quantity
+// (per-cell blocks made the same-address atomics the bottleneck).
 template <class T>
-__global__ void __launch_bounds__(256) k_diag(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+__global__ void __launch_bounds__(128) k_diag(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
                                               const T* __restrict__ uy, const T* __restrict__ uz,
-                                              double* __restrict__ part, DevScalars* __restrict__ sc, int only_cfl) {
-  __shared__ double red[6][8];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+                                              double* __restrict__ part, DevScalars* __restrict__ sc, int rows) {
+  __shared__ double red[6][4];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31), k = blockIdx.y * 4 + (threadIdx.x >> 5);
+  const int j0 = blockIdx.z * rows, j1 = min(j0 + rows, ny);
   double dv = 0, v0 = 0, v1 = 0, v2 = 0, cf = 0, s = 0;
-  if (i < nx && j < ny) {
-    const int jc = j + 1;
-    const int ip = wrapp(i, nx), kp = wrapp(k, nz);
-    const long long idx = i + (long long)nx * (j + (long long)ny * k);
-    const double a = ux[idx], b = uy[idx], c = uz[idx];
-    const double aip = ux[ip + (long long)nx * (j + (long long)ny * k)];
-    const double bjp = fld(uy, g, 1, i, j + 1, k);
-    const double ckp = uz[i + (long long)nx * (j + (long long)ny * kp)];
-    const double rdx = g.rdx, rdz = g.rdz, rdyp = m.rdyp[jc];
-    dv = fabs((aip - a) * rdx + (bjp - b) * rdyp + (ckp - c) * rdz);
-    if (g.order == 4) dv = fabs((double)div4_cell(g, C4<T>(g), m.rdyp[jc], ux, uy, uz, i, j, k));
-    v0 = fabs(a); v1 = fabs(b); v2 = fabs(c);
-    cf = fabs(a + aip) * rdx + fabs(b + bjp) * rdyp + fabs(c + ckp) * rdz;
-    s = a * (double)m.dyp[jc];
-  }
-  // fmax(NaN, x) = x on the device, so NaN is folded into +inf first: a NaN
-  // field still trips the limit checks of the step
-  if (!(dv == dv)) dv = INFINITY;
-  if (!(v0 == v0)) v0 = INFINITY;
-  if (!(v1 == v1)) v1 = INFINITY;
-  if (!(v2 == v2)) v2 = INFINITY;
-  const double r_cf = block_max256(cf, red[0]);
-  __syncthreads();
-  const double r_dv = block_max256(dv, red[1]);
-  __syncthreads();
-  const double r_v0 = block_max256(v0, red[2]);
-  __syncthreads();
-  const double r_v1 = block_max256(v1, red[3]);
-  __syncthreads();
-  const double r_v2 = block_max256(v2, red[4]);
-  __syncthreads();
-  const double r_s = block_sum256(s, red[5]);
-  if (tl == 0) {
-    atomic_max_nonneg(&sc->uddx, r_cf * 0.5);
-    if (!only_cfl) {
-      atomic_max_nonneg(&sc->divmax2, r_dv);
-      atomic_max_nonneg(&sc->vmax[0], r_v0);
-      atomic_max_nonneg(&sc->vmax[1], r_v1);
-      atomic_max_nonneg(&sc->vmax[2], r_v2);
-      part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = r_s;
+  if (i < nx && k < nz) {
+    const long long plane = (long long)nx * ny;
+    const long long col = i + plane * k;
+    const long long dxp = i + 1 == nx ? 1 - nx : 1;
+    const long long dzp = k + 1 == nz ? -(long long)(nz - 1) * plane : plane;
+    const double rdx = g.rdx, rdz = g.rdz;
+    double b = uy[col + (long long)j0 * nx];
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const long long idx = col + (long long)j * nx;
+      const int jc = j + 1;
+      const double a = ux[idx], c = uz[idx];
+      const double aip = ux[idx + dxp], ckp = uz[idx + dzp];
+      const double bjp = j + 1 < ny ? (double)uy[idx + nx] : (double)(T)g.bc.uy_hi;
+      const double rdyp = m.rdyp[jc];
+      double d = fabs((aip - a) * rdx + (bjp - b) * rdyp + (ckp - c) * rdz);
+      if (g.order == 4) d = fabs((double)div4_cell(g, C4<T>(g), m.rdyp[jc], ux, uy, uz, i, j, k));
+      // fmax(NaN, x) = x on the device, so NaN is folded into +inf first: a NaN
+      // field still trips the limit checks of the step
+      if (!(d == d)) d = INFINITY;
+      dv = fmax(dv, d);
+      v0 = fmax(v0, a == a ? fabs(a) : INFINITY);
+      v1 = fmax(v1, b == b ? fabs(b) : INFINITY);
+      v2 = fmax(v2, c == c ? fabs(c) : INFINITY);
+      cf = fmax(cf, fabs(a + aip) * rdx + fabs(b + bjp) * rdyp + fabs(c + ckp) * rdz);
+      s += a * (double)m.dyp[jc];
+      b = bjp;
     }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    dv = fmax(dv, __shfl_xor_sync(0xffffffffu, dv, o));
+    v0 = fmax(v0, __shfl_xor_sync(0xffffffffu, v0, o));
+    v1 = fmax(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+    v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+    cf = fmax(cf, __shfl_xor_sync(0xffffffffu, cf, o));
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = cf; red[1][w] = dv; red[2][w] = v0; red[3][w] = v1; red[4][w] = v2; red[5][w] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r[6];
+    for (int q = 0; q < 5; ++q) r[q] = fmax(fmax(red[q][0], red[q][1]), fmax(red[q][2], red[q][3]));
+    r[5] = (red[5][0] + red[5][1]) + (red[5][2] + red[5][3]);
+    atomic_max_nonneg(&sc->uddx, r[0] * 0.5);
+    atomic_max_nonneg(&sc->divmax2, r[1]);
+    atomic_max_nonneg(&sc->vmax[0], r[2]);
+    atomic_max_nonneg(&sc->vmax[1], r[3]);
+    atomic_max_nonneg(&sc->vmax[2], r[4]);
+    part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = r[5];
   }
 }
 
@@ -1139,7 +1151,7 @@ cudaError_t launch_substep_setup(ch3d_ctx* c, int ns) {
 
 cudaError_t launch_step_end(ch3d_ctx* c) {
   const double norm = 1.0 / ((double)c->nx * (double)c->nz) / c->cfg.yly;
-  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part2, c->npart, c->red2);
+  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part2, diag_npart(c), c->red2);
   k_step_end<<<1, 256, 0, c->stream>>>(c->sc, c->red2, CH3D_NRED, norm, c->cfg.div_limit, c->cfg.vel_limit);
   return cudaGetLastError();
 }
@@ -1319,11 +1331,28 @@ template <class T> static cudaError_t bulk_t(ch3d_ctx* c) {
 }
 cudaError_t launch_bulk_partials(ch3d_ctx* c) { return c->fp32 ? bulk_t<float>(c) : bulk_t<double>(c); }
 
+// rows per k_diag block: whole columns when the x-z plane alone gives about
+// eight blocks per SM, shorter chunks on small grids
+static int diag_rows(const ch3d_ctx* c) {
+  const long long cols = (long long)((c->nx + 31) / 32) * ((c->nz + 3) / 4);
+  const long long chunks = (148LL * 8 + cols - 1) / cols;
+  const int rows = (int)((c->ny + chunks - 1) / chunks);
+  return rows < 8 ? 8 : rows;
+}
+static dim3 diag_grid(const ch3d_ctx* c) {
+  const int rows = diag_rows(c);
+  return dim3((c->nx + 31) / 32, (c->nz + 3) / 4, (c->ny + rows - 1) / rows);
+}
+int diag_npart(const ch3d_ctx* c) {
+  const dim3 g = diag_grid(c);
+  return (int)(g.x * g.y * g.z);
+}
+
 template <class T> static cudaError_t diag_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
   k_diag_reset<<<1, 1, 0, c->stream>>>(c->sc);
-  k_diag<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], c->part2,
-                                                          c->sc, 0);
+  k_diag<T><<<diag_grid(c), 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], c->part2, c->sc,
+                                                 diag_rows(c));
   return cudaGetLastError();
 }
 cudaError_t launch_diag(ch3d_ctx* c) { return c->fp32 ? diag_t<float>(c) : diag_t<double>(c); }

@@ -40,7 +40,7 @@ ALG_ARRAYS_PER_SUBSTEP = {"pimp": 32, "order4": 32, "fimp": 47, "les": 32}
 #  5: projection + pressure update: read phi u* x3 p, write u x3 p)
 GROUP_ARRAYS = {0: 13, 2: 4, 3: 6, 4: 2, 5: 9}
 GROUP_NAMES = {0: "rhs", 1: "y_solves", 2: "k_prsrc_xfft", 3: "k_zfft+k_ysolve2+k_zfft", 4: "k_xifft",
-               5: "k_proj", 6: "scalar"}
+               5: "k_proj", 6: "scalar_kernels_per_step"}
 # the group-0 kernel of each scheme (RHS, fused with the y solves for pimp and order4)
 GROUP0_KERNEL = {"pimp": "k_rhs_march", "order4": "k_rhs4_uhat", "fimp": "k_rhs_fimp", "les": "k_rhs_les"}
 # CUDA kernels launched per step by the step graph (ch3d_api.cu record_step):
@@ -287,12 +287,15 @@ def run_ours(args, ws, rank, local):
     value = ws * cfg.npoints * args.steps / (ms_max * 1e-3) / 1e9
 
     # per-kernel-group device times: CUDA events around each group on the
-    # context's stream over two more (ungraphed) steps
+    # context's stream over two more (ungraphed) steps; groups 0-5 per substep
+    # launch, the scalar kernels per step
     kt = s.kernel_times(2)
     word = 4 if args.precision == "mixed" else 8
     key = scheme_key(cfg)
     names = dict(GROUP_NAMES)
     names[0] = GROUP0_KERNEL[key]
+    if key == "pimp":
+        names[5] = "k_proj_march"
     per_group = {}
     for g, arrs in GROUP_ARRAYS.items():
         b = arrs * cfg.npoints * word

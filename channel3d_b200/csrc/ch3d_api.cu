@@ -1025,7 +1025,8 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
     cnt[grp[m]] += 1;
   }
   for (auto& e : ev) cudaEventDestroy(e);
-  for (int g = 0; g < G; ++g) out[g] = cnt[g] ? sum[g] / cnt[g] : 0.0;
+  for (int g = 0; g < G - 1; ++g) out[g] = cnt[g] ? sum[g] / cnt[g] : 0.0;  // per substep
+  out[G - 1] = sum[G - 1] / nsteps;                                          // per step
   return fetch_info(c, nullptr);
 }
 

@@ -221,11 +221,12 @@ CH3D_API int ch3d_sgs_training_samples(ch3d_ctx* ctx, int fx, int fy, int fz, fl
 CH3D_API int ch3d_memory_bytes(ch3d_ctx* ctx, long long* bytes);
 
 /* Runs `nsteps` steps launching kernel groups one by one, with CUDA events
-   between them on the context's stream, and returns the mean time per launch
-   (ms) of each group in out[0..6]: 0 RHS stencils, 1 y Helmholtz solves,
+   between them on the context's stream, and returns in out[0..5] the mean time
+   (ms) per substep of each group: 0 RHS stencils, 1 y Helmholtz solves,
    2 divergence + forward x FFT, 3 z FFT + y Poisson solve + inverse z FFT,
-   4 inverse x FFT, 5 projection + pressure update, 6 scalar/reduction kernels.
-   The steps advance the state like ch3d_step. */
+   4 inverse x FFT, 5 projection + pressure update; out[6] is the time per step
+   of the scalar and reduction kernels (CFL, substep coefficients,
+   diagnostics).  The steps advance the state like ch3d_step. */
 CH3D_API int ch3d_kernel_times(ch3d_ctx* ctx, int nsteps, double* out, int nout);
 
 /* Allocation-free pressure Poisson solve: the solve of ch3d_poisson

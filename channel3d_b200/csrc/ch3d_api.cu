@@ -471,9 +471,14 @@ int record_step(ch3d_ctx* c) {
     CU(launch_prsrc_xfft(c, 0));
     CU(launch_poisson_spectral(c));
     CU(launch_xifft(c));
-    CU(launch_proj(c, 0));
+    if (ns == c->iadvance && march_diag_fusable(c)) {  // CheckDivergence etc. ride on the last projection
+      CU(launch_diag_reset(c));
+      CU(launch_proj_diag(c));
+    } else {
+      CU(launch_proj(c, 0));
+    }
   }
-  CU(launch_diag(c));
+  if (!march_diag_fusable(c)) CU(launch_diag(c));
   CU(launch_step_end(c));
   return CH3D_OK;
 }
@@ -1010,9 +1015,13 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
       CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());
       CU(mark(3)); CU(launch_poisson_spectral(c)); CU(done());
       CU(mark(4)); CU(launch_xifft(c)); CU(done());
-      CU(mark(5)); CU(launch_proj(c, 0)); CU(done());
+      if (ns == c->iadvance && march_diag_fusable(c)) {
+        CU(mark(5)); CU(launch_diag_reset(c)); CU(launch_proj_diag(c)); CU(done());
+      } else {
+        CU(mark(5)); CU(launch_proj(c, 0)); CU(done());
+      }
     }
-    CU(mark(6)); CU(launch_diag(c)); CU(launch_step_end(c)); CU(done());
+    CU(mark(6)); if (!march_diag_fusable(c)) CU(launch_diag(c)); CU(launch_step_end(c)); CU(done());
   }
   if (q != ev.size()) return fail(CH3D_ERR_INVALID, "kernel_times event count mismatch");
   CU(cudaStreamSynchronize(c->stream));

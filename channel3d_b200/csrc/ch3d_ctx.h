@@ -97,7 +97,8 @@ cudaError_t launch_uhat(ch3d_ctx* c);                  // stage path: Rhs arrays
 cudaError_t launch_rhs_march(ch3d_ctx* c);             // u -> u*, Hist, with its row table
 size_t march_table_bytes(int ny);
 cudaError_t march_table_reset(ch3d_ctx* c);           // forget the cached factors
-cudaError_t launch_proj_march(ch3d_ctx* c, int mode);   // projection + pressure update + bulk partials
+cudaError_t launch_proj_march(ch3d_ctx* c, int mode, bool diag);  // projection + pressure update + bulk partials
+bool march_diag_fusable(const ch3d_ctx* c);            // the step diagnostics can ride on the last projection
 cudaError_t launch_bulk_march(ch3d_ctx* c);            // bulk partials of an uploaded field
 int march_npart(const ch3d_ctx* c);
 cudaError_t launch_helm_factors(ch3d_ctx* c);
@@ -117,6 +118,8 @@ cudaError_t poisson_noalloc(int nx, int ny, int nz, double xlx, double zlz, cons
                             const double* d_src, double* d_phi, cudaStream_t st, const FFTPlanDev& planx,
                             const FFTPlanDev& planz);
 cudaError_t launch_proj(ch3d_ctx* c, int mode);        // mode 0: u = u* - a grad phi, p update; 1: u -= grad phi
+cudaError_t launch_proj_diag(ch3d_ctx* c);             // last substep: projection + step diagnostics (march path)
+cudaError_t launch_diag_reset(ch3d_ctx* c);
 cudaError_t launch_bulk_partials(ch3d_ctx* c);
 cudaError_t launch_diag(ch3d_ctx* c);
 int diag_npart(const ch3d_ctx* c);                     // partial sums k_diag writes to part2

@@ -330,43 +330,60 @@ __device__ __forceinline__ double block_sum128(double v, double* sh /* 4 */) {
   return threadIdx.x == 0 ? (sh[0] + sh[1]) + (sh[2] + sh[3]) : 0.0;
 }
 
-template <class T>
+// DIAG (last substep of a step, nx % 32 == 0, nz % 4 == 0 so that no thread
+// idles): CheckDivergence, CalcVmax, the next step's CalcMaxCFL and the
+// CalcUxAver partials (src/CFD_2nd/m_Tools.f90:21-104,250-270) of the new
+// velocity, fused in.  The i+1, j+1 and k+1 neighbours of the new velocity
+// are recomputed from u* and phi with the same expressions their own threads
+// use, so they equal the stored values bit for bit.
+template <class T, bool DIAG>
 __global__ void __launch_bounds__(128) k_proj_march(Geo<T> g, Metrics<T> m, const T* uxs, const T* uys,
                                                     const T* uzs, T* ux, T* uy, T* uz, T* __restrict__ pr,
-                                                    const T* __restrict__ phi, double* __restrict__ part, int mode,
-                                                    const DevScalars* __restrict__ sc) {
-  __shared__ double red[4];
+                                                    const T* __restrict__ phi, double* __restrict__ part,
+                                                    double* __restrict__ part2, int mode, DevScalars* __restrict__ sc) {
+  __shared__ double red[7][4];
   if (sc->status) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long plane = (long long)nx * ny;
   const int i = blockIdx.x * 32 + (threadIdx.x & 31), k = blockIdx.y * 4 + (threadIdx.x >> 5);
   const int j0 = blockIdx.z * MJ, j1 = min(j0 + MJ, ny);
-  double s = 0.0;
+  double s = 0.0, s2 = 0.0, dv = 0.0, v0 = 0.0, v1 = 0.0, v2 = 0.0, cf = 0.0;
   if (i < nx && k < nz) {
     const long long col = i + plane * k;
-    const long long dxm = i == 0 ? nx - 1 : -1;                      // offset to i-1
+    const long long dxm = i == 0 ? nx - 1 : -1;                           // offset to i-1
     const long long dzm = k == 0 ? (long long)(nz - 1) * plane : -plane;  // offset to k-1
+    const long long dxp = i + 1 == nx ? 1 - nx : 1;                       // offset to i+1
+    const long long dzp = k + 1 == nz ? -(long long)(nz - 1) * plane : plane;  // offset to k+1
     const T pmAlpha = mode == 0 ? (T)sc->pmAlpha : (T)1;
     const T pmBeta = (T)sc->pmBeta;
     const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha;
+    const double rdx = g.rdx, rdz = g.rdz;
     T pm = __ldg(phi + col + (long long)(j0 > 0 ? j0 - 1 : 0) * nx);
     T pc = __ldg(phi + col + (long long)j0 * nx);
     // rows in batches of PB: all loads of a batch before its stores (u* and u may
     // be the same arrays, mode 1, so the compiler cannot reorder them itself)
-    constexpr int PB = 4;
+    constexpr int PB = DIAG ? 2 : 4;
     for (int jb = j0; jb < j1; jb += PB) {
       T vpp[PB], vpx[PB], vpz[PB], vu[PB], vv[PB], vw[PB], vp[PB], mr[PB], mp[PB], mc[PB], mm[PB], ms[PB];
+      T qux[PB], qpx[PB], quz[PB], qpz[PB], quy[PB], qr[PB], qrp[PB], qdy[PB];  // DIAG neighbours, metrics
 #pragma unroll
       for (int b = 0; b < PB; ++b) {
         const int j = jb + b < j1 ? jb + b : j1 - 1;
         const long long idx = col + (long long)j * nx;
-        vpp[b] = __ldg(phi + col + (long long)(j + 1 < ny ? j + 1 : ny - 1) * nx);
+        const int jn = j + 1 < ny ? j + 1 : ny - 1;
+        vpp[b] = __ldg(phi + col + (long long)jn * nx);
         vpx[b] = __ldg(phi + idx + dxm);
         vpz[b] = __ldg(phi + idx + dzm);
         vu[b] = uxs[idx]; vv[b] = uys[idx]; vw[b] = uzs[idx];
         vp[b] = mode == 0 ? pr[idx] : (T)0;
         mr[b] = m.rdyc[j + 1]; mp[b] = m.ap2Pr[j + 1]; mc[b] = m.ac2Pr[j + 1]; mm[b] = m.am2Pr[j + 1];
         ms[b] = m.s1coe[j + 1];
+        if (DIAG) {
+          qux[b] = uxs[idx + dxp]; qpx[b] = __ldg(phi + idx + dxp);
+          quz[b] = uzs[idx + dzp]; qpz[b] = __ldg(phi + idx + dzp);
+          quy[b] = uys[col + (long long)jn * nx];
+          qr[b] = m.rdyc[jn + 1]; qrp[b] = m.rdyp[j + 1]; qdy[b] = m.dyp[j + 1];
+        }
       }
 #pragma unroll
       for (int b = 0; b < PB; ++b) {
@@ -386,12 +403,57 @@ __global__ void __launch_bounds__(128) k_proj_march(Geo<T> g, Metrics<T> m, cons
           pr[idx] = vp[b] + pmBetap * pp + pmBetac * pc + pmBetam * pm;
         }
         s += (double)uxn * (double)ms[b];
+        if (DIAG) {
+          // the new velocity at i+1, k+1 and j+1, as the threads that own them compute it
+          const T uxp = qux[b] - (qpx[b] - pc) * rdxEta2;
+          const T uzp = quz[b] - (qpz[b] - pc) * rdzEta2;
+          const T uyp = j + 1 < ny ? quy[b] - (pp - pc) * (qr[b] * pmAlpha) : (T)g.bc.uy_hi;
+          const double a = uxn, bb = uyn, c = uzn, aip = uxp, bjp = uyp, ckp = uzp, rdyp = qrp[b];
+          double d = fabs((aip - a) * rdx + (bjp - bb) * rdyp + (ckp - c) * rdz);
+          if (!(d == d)) d = INFINITY;  // NaN folded into +inf: a NaN field trips the limits
+          dv = fmax(dv, d);
+          v0 = fmax(v0, a == a ? fabs(a) : INFINITY);
+          v1 = fmax(v1, bb == bb ? fabs(bb) : INFINITY);
+          v2 = fmax(v2, c == c ? fabs(c) : INFINITY);
+          cf = fmax(cf, fabs(a + aip) * rdx + fabs(bb + bjp) * rdyp + fabs(c + ckp) * rdz);
+          s2 += a * (double)qdy[b];
+        }
         pm = pc; pc = pp;
       }
     }
   }
-  const double bs = block_sum128(s, red);
-  if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
+  if (!DIAG) {
+    const double bs = block_sum128(s, red[0]);
+    if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
+    return;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    dv = fmax(dv, __shfl_xor_sync(0xffffffffu, dv, o));
+    v0 = fmax(v0, __shfl_xor_sync(0xffffffffu, v0, o));
+    v1 = fmax(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+    v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+    cf = fmax(cf, __shfl_xor_sync(0xffffffffu, cf, o));
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = s; red[1][w] = s2; red[2][w] = cf; red[3][w] = dv; red[4][w] = v0; red[5][w] = v1; red[6][w] = v2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r[7];
+    for (int q = 0; q < 2; ++q) r[q] = (red[q][0] + red[q][1]) + (red[q][2] + red[q][3]);
+    for (int q = 2; q < 7; ++q) r[q] = fmax(fmax(red[q][0], red[q][1]), fmax(red[q][2], red[q][3]));
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    part[bid] = r[0];
+    part2[bid] = r[1];
+    atomic_max_nonneg(&sc->uddx, r[2] * 0.5);
+    atomic_max_nonneg(&sc->divmax2, r[3]);
+    atomic_max_nonneg(&sc->vmax[0], r[4]);
+    atomic_max_nonneg(&sc->vmax[1], r[5]);
+    atomic_max_nonneg(&sc->vmax[2], r[6]);
+  }
 }
 
 // the same partial sums of ux * s1coe for a freshly uploaded field
@@ -417,15 +479,23 @@ int march_npart(const ch3d_ctx* c) {
   return (int)(g.x * g.y * g.z);
 }
 
-template <class T> static cudaError_t proj_march_t(ch3d_ctx* c, int mode) {
+bool march_diag_fusable(const ch3d_ctx* c) { return c->march && c->nx % 32 == 0 && c->nz % 4 == 0; }
+
+template <class T> static cudaError_t proj_march_t(ch3d_ctx* c, int mode, bool diag) {
   T** f = (T**)c->f;
   T* in[3] = {mode == 1 ? f[0] : f[12], mode == 1 ? f[1] : f[13], mode == 1 ? f[2] : f[14]};
-  k_proj_march<T><<<march_proj_grid(c), 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1], in[2],
-                                                              f[0], f[1], f[2], f[3], f[10], c->part, mode, c->sc);
+  if (diag)
+    k_proj_march<T, true><<<march_proj_grid(c), 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1],
+                                                                      in[2], f[0], f[1], f[2], f[3], f[10], c->part,
+                                                                      c->part2, mode, c->sc);
+  else
+    k_proj_march<T, false><<<march_proj_grid(c), 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1],
+                                                                       in[2], f[0], f[1], f[2], f[3], f[10], c->part,
+                                                                       c->part2, mode, c->sc);
   return cudaGetLastError();
 }
-cudaError_t launch_proj_march(ch3d_ctx* c, int mode) {
-  return c->fp32 ? proj_march_t<float>(c, mode) : proj_march_t<double>(c, mode);
+cudaError_t launch_proj_march(ch3d_ctx* c, int mode, bool diag) {
+  return c->fp32 ? proj_march_t<float>(c, mode, diag) : proj_march_t<double>(c, mode, diag);
 }
 template <class T> static cudaError_t bulk_march_t(ch3d_ctx* c) {
   T** f = (T**)c->f;

@@ -1151,7 +1151,9 @@ cudaError_t launch_substep_setup(ch3d_ctx* c, int ns) {
 
 cudaError_t launch_step_end(ch3d_ctx* c) {
   const double norm = 1.0 / ((double)c->nx * (double)c->nz) / c->cfg.yly;
-  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part2, diag_npart(c), c->red2);
+  // part2: written by the fused projection (march layout) or by k_diag
+  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part2, march_diag_fusable(c) ? c->npart_m : diag_npart(c),
+                                                       c->red2);
   k_step_end<<<1, 256, 0, c->stream>>>(c->sc, c->red2, CH3D_NRED, norm, c->cfg.div_limit, c->cfg.vel_limit);
   return cudaGetLastError();
 }
@@ -1314,7 +1316,7 @@ template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {
 cudaError_t launch_xifft(ch3d_ctx* c) { return c->fp32 ? xifft_t<float>(c) : xifft_t<double>(c); }
 
 template <class T> static cudaError_t proj_t(ch3d_ctx* c, int mode) {
-  if (c->march) return launch_proj_march(c, mode);
+  if (c->march) return launch_proj_march(c, mode, false);
   T** f = (T**)c->f;
   T* in[3] = {mode == 1 ? f[0] : f[12], mode == 1 ? f[1] : f[13], mode == 1 ? f[2] : f[14]};
   k_proj<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), in[0], in[1], in[2], f[0],
@@ -1322,6 +1324,11 @@ template <class T> static cudaError_t proj_t(ch3d_ctx* c, int mode) {
   return cudaGetLastError();
 }
 cudaError_t launch_proj(ch3d_ctx* c, int mode) { return c->fp32 ? proj_t<float>(c, mode) : proj_t<double>(c, mode); }
+cudaError_t launch_proj_diag(ch3d_ctx* c) { return launch_proj_march(c, 0, true); }
+cudaError_t launch_diag_reset(ch3d_ctx* c) {
+  k_diag_reset<<<1, 1, 0, c->stream>>>(c->sc);
+  return cudaGetLastError();
+}
 
 template <class T> static cudaError_t bulk_t(ch3d_ctx* c) {
   if (c->march) return launch_bulk_march(c);

@@ -114,21 +114,8 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
   const long long plane = (long long)nx * ny;
   tab += (size_t)(sc->ns - 1) * ny * MT_W;  // this substep's table
   const int tid = threadIdx.x, tx = tid & 31, tz = tid >> 5;
-  const int i0 = blockIdx.x * BX, k0 = blockIdx.y * BZ;
-  const int i = i0 + tx, k = k0 + tz;
-  const bool act = i < nx && k < nz;
   auto slot = [](int r) { return (r + 1) % RS; };  // r >= -1
-
-  // staging slots: s = tid + q NT -> halo-tile position (s % SX, s / SX), periodic in x and z
-  long long so[NS];
-#pragma unroll
-  for (int q = 0; q < NS; ++q) {
-    const int s = tid + q * NT;
-    int ig = (i0 - 1 + s % SX) % nx, kg = (k0 - 1 + s / SX) % nz;
-    if (ig < 0) ig += nx;
-    if (kg < 0) kg += nz;
-    so[q] = s < PL ? ig + plane * kg : 0;
-  }
+  long long so[NS];  // staging slot offsets of the current tile
   auto issue_row = [&](int r) {  // r < ny
     const long long ro = (long long)r * nx;
     const int sl = slot(r);
@@ -167,18 +154,38 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
     }
   };
 
+  const T two = (T)2, half = (T)0.5, quarter = (T)0.25, one = (T)1;
+  const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
+  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
+  const T dpm = (T)sc->dpmdxns;
+  const int c0 = (tz + 1) * SX + tx + 1;
+  const int ntx = (nx + BX - 1) / BX, ntiles = ntx * ((nz + BZ - 1) / BZ);
+
+  // Persistent blocks walk tiles of 32 x BZ columns.  The back substitution of
+  // a tile (HBM-bound) runs one row per forward row of the block's next tile
+  // (latency-bound), so the two overlap instead of alternating in waves.
+  bool pact = false;          // this thread's column of the previous tile is inside the grid
+  long long pidx = 0;         // its row ny-1
+  T p0 = (T)0, p1 = (T)0, p2 = (T)0;  // u* of the row above the next one to substitute
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  const int i0 = (tile % ntx) * BX, k0 = (tile / ntx) * BZ;
+  const int i = i0 + tx, k = k0 + tz;
+  const bool act = i < nx && k < nz;
+  // staging slots: s = tid + q NT -> halo-tile position (s % SX, s / SX), periodic in x and z
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const int s = tid + q * NT;
+    int ig = (i0 - 1 + s % SX) % nx, kg = (k0 - 1 + s / SX) % nz;
+    if (ig < 0) ig += nx;
+    if (kg < 0) kg += nz;
+    so[q] = s < PL ? ig + plane * kg : 0;
+  }
   // prologue: rows 0 .. D+1 in flight, one copy group per row
 #pragma unroll
   for (int r = 0; r <= D + 1; ++r) {
     if (r < ny) issue_row(r);
     cp_async_commit();
   }
-
-  const T two = (T)2, half = (T)0.5, quarter = (T)0.25, one = (T)1;
-  const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
-  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
-  const T dpm = (T)sc->dpmdxns;
-  const int c0 = (tz + 1) * SX + tx + 1;
   long long idx = act ? i + plane * k : 0;
   T d0 = (T)0, d1 = (T)0, d2 = (T)0;       // eliminated right-hand sides of the previous row
   T g0 = (T)0, g1 = (T)0, g2 = (T)0;       // g of the last row (= u* of row ny-1)
@@ -191,7 +198,16 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
     if (ny > 1) { hx1 = hx[idx + nx]; hy1 = hy[idx + nx]; hz1 = hz[idx + nx]; }
   }
 
+  // previous tile: row rb = ny-2-j of its back substitution at forward row j, its g
+  // loaded one row ahead
+  T n0 = (T)0, n1 = (T)0, n2 = (T)0;
+  if (pact && ny >= 2) { n0 = uxs[pidx - nx]; n1 = uys[pidx - nx]; n2 = uzs[pidx - nx]; }
   for (int j = 0; j < ny; ++j) {
+    const int rb = ny - 2 - j;
+    const bool bsub = pact && rb >= 0;
+    const long long ob = pidx - (long long)(j + 1) * nx;
+    const T b0 = n0, b1 = n1, b2 = n2;
+    if (pact && rb >= 1) { n0 = uxs[ob - nx]; n1 = uys[ob - nx]; n2 = uzs[ob - nx]; }
     cp_async_wait<D>();  // this thread's copies of rows <= j+1 are done
     if (j + 1 == ny) ghost_row(ny);
     if (j == 0) ghost_row(-1);
@@ -280,16 +296,26 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
       g2 = uz_c + d2 + __ldg(tr + MT_CP0) * uz_jp;
       uxs[idx] = g0; uys[idx] = g1; uzs[idx] = g2;
     }
+    if (bsub) {  // u*_rb = g_rb - cp_rb u*_{rb+1}
+      const T* tb = tab + (size_t)rb * MT_W;
+      const T cb0 = __ldg(tb + MT_CP0), cb1 = __ldg(tb + MT_CP1);
+      p0 = b0 - cb0 * p0; p1 = b1 - cb1 * p1; p2 = b2 - cb0 * p2;
+      uxs[ob] = p0; uys[ob] = p1; uzs[ob] = p2;
+    }
     idx += nx;
     hxo = hx1; hyo = hy1; hzo = hz1;
     hx1 = hxn; hy1 = hyn; hz1 = hzn;
   }
   cp_async_wait<0>();
-  if (!act) return;
+  __syncthreads();  // the ring is refilled by the next tile's prologue
+  pact = act; pidx = idx - nx; p0 = g0; p1 = g1; p2 = g2;
+  }  // tiles
+  if (!pact) return;
 
-  // back substitution u*_j = g_j - cp_j u*_{j+1}, rows loaded in batches of 8
+  // back substitution of the block's last tile, rows loaded in batches of 8
   constexpr int B = 8;
-  idx -= nx;  // row ny-1 (u* = g there)
+  long long idx = pidx;  // row ny-1 (u* = g there)
+  T g0 = p0, g1 = p1, g2 = p2;
   for (int j = ny - 2; j >= 0; j -= B) {
     T a0[B], a1[B], a2[B];
 #pragma unroll
@@ -506,10 +532,17 @@ cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float
 
 template <class T> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
+  constexpr int BPS = sizeof(T) == 8 ? 4 : 5;  // resident blocks per SM (launch bounds)
   T** f = (T**)c->f;
   k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab,
                                              march_beta_slots(c->mtab, c->ny), c->sc);
-  dim3 grid((c->nx + 31) / 32, (c->nz + BZ - 1) / BZ);
+  static int nsm = 0;
+  if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
+  const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + BZ - 1) / BZ);
+  // FP64: persistent blocks (back substitution overlapped with the next tile); FP32: one
+  // tile per block (measured faster: its shorter rows leave the overlapped loads exposed)
+  const long long cap = sizeof(T) == 8 ? (long long)nsm * BPS : ntiles;
+  const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
   k_rhs_march<T, BZ, D, RS><<<grid, 32 * BZ, 0, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3],
                                                      f[4], f[5], f[6], f[12], f[13], f[14], c->sc);
   return cudaGetLastError();

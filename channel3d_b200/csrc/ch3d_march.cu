@@ -448,11 +448,10 @@ __global__ void __launch_bounds__(128) k_proj_march(Geo<T> g, Metrics<T> m, cons
       }
     }
   }
-  if (!DIAG) {
+  if constexpr (!DIAG) {
     const double bs = block_sum128(s, red[0]);
     if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
-    return;
-  }
+  } else {
   for (int o = 16; o > 0; o >>= 1) {
     s += __shfl_xor_sync(0xffffffffu, s, o);
     s2 += __shfl_xor_sync(0xffffffffu, s2, o);
@@ -479,6 +478,7 @@ __global__ void __launch_bounds__(128) k_proj_march(Geo<T> g, Metrics<T> m, cons
     atomic_max_nonneg(&sc->vmax[0], r[4]);
     atomic_max_nonneg(&sc->vmax[1], r[5]);
     atomic_max_nonneg(&sc->vmax[2], r[6]);
+  }
   }
 }
 

@@ -42,7 +42,7 @@ GROUP_ARRAYS = {0: 13, 2: 4, 3: 6, 4: 2, 5: 9}
 GROUP_NAMES = {0: "rhs", 1: "y_solves", 2: "k_prsrc_xfft", 3: "k_zfft+k_ysolve2+k_zfft", 4: "k_xifft",
                5: "k_proj", 6: "scalar_kernels_per_step"}
 # the group-0 kernel of each scheme (RHS, fused with the y solves for pimp and order4)
-GROUP0_KERNEL = {"pimp": "k_rhs_march", "order4": "k_rhs4_uhat", "fimp": "k_rhs_fimp", "les": "k_rhs_les"}
+GROUP0_KERNEL = {"pimp": "k_rhs_march", "order4": "k_rhs_march", "fimp": "k_rhs_fimp", "les": "k_rhs_les"}
 # CUDA kernels launched per step by the step graph (ch3d_api.cu record_step):
 # step_begin 1 + per substep (reduce_partials + substep_setup 2, march table (pimp) or
 # helm_factors 1, rhs+uhat 1, prsrc_xfft 1, zfft + ysolve2 (+ FP64 low modes in mixed) + zfft 3|4,

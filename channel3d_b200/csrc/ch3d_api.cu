@@ -465,8 +465,7 @@ int record_step(ch3d_ctx* c) {
       CU(launch_ptri_xz(c));
       CU(launch_uhat(c));
     } else {
-      CU(launch_helm_factors(c));
-      CU(launch_rhs4_uhat(c));
+      CU(launch_rhs_march(c));  // 4th order: the same column march with the 4th-order stencils
     }
     CU(launch_prsrc_xfft(c, 0));
     CU(launch_poisson_spectral(c));
@@ -998,7 +997,9 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
     for (int ns = 1; ns <= c->iadvance; ++ns) {
       CU(mark(6));
       if (c->cfg.order == 4) CU(launch_visc4_partials(c));
-      CU(launch_substep_setup(c, ns)); if (!march_path(c)) CU(launch_helm_factors(c)); CU(done());
+      CU(launch_substep_setup(c, ns));
+      if (!march_path(c) && c->cfg.order != 4) CU(launch_helm_factors(c));
+      CU(done());
       if (march_path(c)) {
         CU(mark(0)); CU(launch_rhs_march(c)); CU(done());
         CU(mark(1)); CU(done());
@@ -1009,7 +1010,7 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
         CU(mark(0)); CU(launch_rhs_fimp(c)); CU(done());
         CU(mark(1)); CU(launch_ptri_xz(c)); CU(launch_uhat(c)); CU(done());
       } else {
-        CU(mark(0)); CU(launch_rhs4_uhat(c)); CU(done());
+        CU(mark(0)); CU(launch_rhs_march(c)); CU(done());
         CU(mark(1)); CU(done());
       }
       CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());

@@ -129,7 +129,6 @@ cudaError_t launch_fill_row0(ch3d_ctx* c, int q, double v);  // field q: every j
 cudaError_t launch_convert(ch3d_ctx* c, const void* src, void* dst, long long n, int to_f32);  // FP64 <-> FP32
 // 4th-order solver (ch3d_step4.cu)
 cudaError_t launch_rhs4(ch3d_ctx* c);                  // stage path: interpolation + RhsX/Y/Z
-cudaError_t launch_rhs4_uhat(ch3d_ctx* c);             // fused step path: interpolation + RHS + y solve -> u*
 cudaError_t launch_visc4_partials(ch3d_ctx* c);        // mean viscous stress partial sums -> part
 // fully implicit 2nd-order step (ch3d_step.cu, ch3d_fimp.cu)
 cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP -> RhsX/Y/Z

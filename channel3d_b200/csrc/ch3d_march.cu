@@ -99,16 +99,22 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // flight while row j is computed.  Slot (j+D+2), written after the barrier of
 // iteration j, must differ from the slots of rows j-1, j, j+1 that other
 // threads still read: RS >= D + 4.
-template <class T, int BZ, int D, int RS>
-__global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * BZ))  // FP32: 5 blocks per SM
+//
+// O4: the 4th-order right-hand sides (clcRhsXYZ, src/CFD_4th/m_TScheme.f90:
+// 189-377) with a 3-cell x/z halo; their x- and z-interpolated velocities
+// (:209-227) are formed from the staged rows instead of being stored.
+template <class T, bool O4, int BZ, int D, int RS>
+__global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 640) : 512) / (32 * BZ))
     k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ ux, const T* __restrict__ uy,
                 const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
                 T* __restrict__ hz, T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
                 const DevScalars* __restrict__ sc) {
-  constexpr int BX = 32, NT = BX * BZ, SX = BX + 2, PL = SX * (BZ + 2);
+  constexpr int H = O4 ? 3 : 1;  // x/z halo
+  constexpr int BX = 32, NT = BX * BZ, SX = BX + 2 * H, PL = SX * (BZ + 2 * H);
   constexpr int NS = (PL + NT - 1) / NT;  // staging slots per thread and array
   static_assert(RS >= D + 4, "ring too small for the prefetch distance");
-  __shared__ __align__(16) T ring[4][RS][PL];  // ux uy uz p
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T (*ring)[RS][PL] = reinterpret_cast<T (*)[RS][PL]>(smem_raw);  // [4][RS][PL]: ux uy uz p
   if (sc->status) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long plane = (long long)nx * ny;
@@ -140,7 +146,8 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
       if (r < 0) {
         const T u = ring[0][slot(0)][s], w = ring[2][slot(0)][s], v1 = ring[1][slot(1)][s];
         ring[0][sl][s] = g.bc.lo == -1 ? (T)(g.bc.ux_lo * 2.0) - u : u - (T)(g.bc.ux_lo * g.bc.dyp1);
-        ring[1][sl][s] = (T)(g.bc.uy_lo * 2.0) - v1;  // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc)
+        // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc); never set (zero) in the 4th-order solver
+        ring[1][sl][s] = O4 ? (T)0 : (T)(g.bc.uy_lo * 2.0) - v1;
         ring[2][sl][s] = g.bc.lo == -1 ? (T)(g.bc.uz_lo * 2.0) - w : w - (T)(g.bc.uz_lo * g.bc.dyp1);
         ring[3][sl][s] = ring[3][slot(0)][s];
       } else {
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
   const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
   const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
   const T dpm = (T)sc->dpmdxns;
-  const int c0 = (tz + 1) * SX + tx + 1;
+  const int c0 = (tz + H) * SX + tx + H;
   const int ntx = (nx + BX - 1) / BX, ntiles = ntx * ((nz + BZ - 1) / BZ);
 
   // Persistent blocks walk tiles of 32 x BZ columns.  The back substitution of
@@ -175,7 +182,7 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
     const int s = tid + q * NT;
-    int ig = (i0 - 1 + s % SX) % nx, kg = (k0 - 1 + s / SX) % nz;
+    int ig = (i0 - H + s % SX) % nx, kg = (k0 - H + s / SX) % nz;
     if (ig < 0) ig += nx;
     if (kg < 0) kg += nz;
     so[q] = s < PL ? ig + plane * kg : 0;
@@ -217,6 +224,9 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
     T hxn = (T)0, hyn = (T)0, hzn = (T)0;
     if (hread && j + 2 < ny) { hxn = hx[idx + 2 * nx]; hyn = hy[idx + 2 * nx]; hzn = hz[idx + 2 * nx]; }
     if (act) {
+      T rx, ry, rz, ux_c, uy_c, uz_c, ux_jp, uy_jp, uz_jp;
+      const T* tr = tab + (size_t)j * MT_W;
+      if constexpr (!O4) {
       const T* X0 = &ring[0][slot(j - 1)][c0];
       const T* X1 = &ring[0][slot(j)][c0];
       const T* X2 = &ring[0][slot(j + 1)][c0];
@@ -228,19 +238,17 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
       const T* Z2 = &ring[2][slot(j + 1)][c0];
       const T* P0 = &ring[3][slot(j - 1)][c0];
       const T* P1 = &ring[3][slot(j)][c0];
-      const T* tr = tab + (size_t)j * MT_W;
 
-      const T ux_c = X1[0], ux_ip = X1[1], ux_im = X1[-1], ux_jp = X2[0], ux_jm = X0[0];
+      ux_c = X1[0]; const T ux_ip = X1[1], ux_im = X1[-1]; ux_jp = X2[0]; const T ux_jm = X0[0];
       const T ux_kp = X1[SX], ux_km = X1[-SX], ux_ip_jm = X0[1], ux_ip_km = X1[1 - SX];
-      const T uy_c = Y1[0], uy_ip = Y1[1], uy_im = Y1[-1], uy_jp = Y2[0], uy_jm = Y0[0];
+      uy_c = Y1[0]; uy_jp = Y2[0]; const T uy_ip = Y1[1], uy_im = Y1[-1], uy_jm = Y0[0];
       const T uy_im_jp = Y2[-1], uy_kp = Y1[SX], uy_km = Y1[-SX], uy_jp_km = Y2[-SX];
-      const T uz_c = Z1[0], uz_ip = Z1[1], uz_im = Z1[-1], uz_jp = Z2[0], uz_jm = Z0[0];
+      uz_c = Z1[0]; uz_jp = Z2[0]; const T uz_ip = Z1[1], uz_im = Z1[-1], uz_jm = Z0[0];
       const T uz_kp = Z1[SX], uz_km = Z1[-SX], uz_im_kp = Z1[SX - 1], uz_jm_kp = Z0[SX];
       const T p_c = P1[0], p_im = P1[-1], p_jm = P0[0], p_km = P1[-SX];
 
       const T IY1 = __ldg(tr + MT_IY1), IY2 = one - IY1;
       const T IY3 = __ldg(tr + MT_IY3), IY4 = one - IY3;
-      T rx, ry, rz;
       {  // RhsX (clcRhsX_PIMP, m_TSchemePIMP_inc.f90:7-75)
         const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
         const T sucaj = half * __ldg(tr + MT_RDYP);
@@ -285,6 +293,96 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 ? 640 : 512) / (32 * 
         T convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g.g3;
         rz = pmGamma * convEd3 + pmTheta * hzo - pmAlpha * gradp3 + two * pmBeta * d22q3;
         hz[idx] = convEd3;
+      }
+      } else {
+        // 4th order: row r, x offset dx, z offset dz of staged array a
+        auto V = [&](int a, int r, int dx, int dz) -> T { return ring[a][slot(r)][c0 + dx + dz * SX]; };
+        const C4<T> q(g);
+        // interpolated velocities (k_interp4 pattern): x for ux (i'-1..i'+2), uy, uz (i'-2..i'+1);
+        // z for ux, uy (k'-2..k'+1), uz (k'-1..k'+2)
+        auto uxhx = [&](int r, int o, int dz) {
+          return q.in1 * V(0, r, o - 1, dz) + q.in2 * V(0, r, o, dz) + q.in3 * V(0, r, o + 1, dz) + q.in4 * V(0, r, o + 2, dz);
+        };
+        auto hxa = [&](int a, int r, int o, int dz) {
+          return q.in1 * V(a, r, o - 2, dz) + q.in2 * V(a, r, o - 1, dz) + q.in3 * V(a, r, o, dz) + q.in4 * V(a, r, o + 1, dz);
+        };
+        auto hza = [&](int a, int r, int dx, int o) {
+          return q.in1 * V(a, r, dx, o - 2) + q.in2 * V(a, r, dx, o - 1) + q.in3 * V(a, r, dx, o) + q.in4 * V(a, r, dx, o + 1);
+        };
+        auto uzhz = [&](int r, int o) {
+          return q.in1 * V(2, r, 0, o - 1) + q.in2 * V(2, r, 0, o) + q.in3 * V(2, r, 0, o + 1) + q.in4 * V(2, r, 0, o + 2);
+        };
+        const bool top = j + 1 == ny;  // uyhx, uyhz vanish on the jc = nyp row (:223-226)
+        const T IY1 = __ldg(tr + MT_IY1), IY2 = one - IY1;
+        const T IY3 = __ldg(tr + MT_IY3), IY4 = one - IY3;
+        const T sucaj = __ldg(tr + MT_RDYP);
+        ux_c = V(0, j, 0, 0); ux_jp = V(0, j + 1, 0, 0);
+        uy_c = V(1, j, 0, 0); uy_jp = V(1, j + 1, 0, 0);
+        uz_c = V(2, j, 0, 0); uz_jp = V(2, j + 1, 0, 0);
+        {  // RhsX (:235-268)
+          const T ux_jm = V(0, j - 1, 0, 0);
+          const T uxhyc = IY1 * ux_jm + IY2 * ux_c;
+          const T uxhyp = IY3 * ux_c + IY4 * ux_jp;
+          const T a1 = uxhx(j, -2, 0), a2 = uxhx(j, -1, 0), a3 = uxhx(j, 0, 0), a4 = uxhx(j, 1, 0);
+          const T h11 = q.dx1 * a1 * a1 + q.dx2 * a2 * a2 + q.dx3 * a3 * a3 + q.dx4 * a4 * a4;
+          const T h12 = ((top ? (T)0 : hxa(1, j + 1, 0, 0)) * uxhyp - hxa(1, j, 0, 0) * uxhyc) * sucaj;
+          const T h13 = q.dz1 * hza(0, j, 0, -1) * hxa(2, j, 0, -1) + q.dz2 * hza(0, j, 0, 0) * hxa(2, j, 0, 0) +
+                        q.dz3 * hza(0, j, 0, 1) * hxa(2, j, 0, 1) + q.dz4 * hza(0, j, 0, 2) * hxa(2, j, 0, 2);
+          const T d11 = q.dxx1 * V(0, j, -2, 0) + q.dxx2 * V(0, j, -1, 0) + q.dxx3 * ux_c + q.dxx4 * V(0, j, 1, 0) +
+                        q.dxx5 * V(0, j, 2, 0);
+          const T d22 = __ldg(tr + MT_AP2C) * ux_jp + __ldg(tr + MT_AC2C) * ux_c + __ldg(tr + MT_AM2C) * ux_jm;
+          const T d33 = q.dzz1 * V(0, j, 0, -2) + q.dzz2 * V(0, j, 0, -1) + q.dzz3 * ux_c + q.dzz4 * V(0, j, 0, 1) +
+                        q.dzz5 * V(0, j, 0, 2);
+          const T conv = -h11 - h12 - h13 + xnu * (d11 + d33) + g.g1;
+          const T gradp = q.dx1 * V(3, j, -2, 0) + q.dx2 * V(3, j, -1, 0) + q.dx3 * V(3, j, 0, 0) + q.dx4 * V(3, j, 1, 0);
+          rx = pmGamma * conv + pmTheta * hxo - pmAlpha * gradp + two * pmBeta * d22;
+          hx[idx] = conv;
+        }
+        {  // RhsY (:270-305)
+          const T sucac = __ldg(tr + MT_RDYC), qsucac = quarter * sucac;
+          const T uxhym = IY1 * V(0, j - 1, -1, 0) + IY2 * V(0, j, -1, 0);
+          const T uxhyc = IY1 * V(0, j - 1, 0, 0) + IY2 * V(0, j, 0, 0);
+          const T uxhyp = IY1 * V(0, j - 1, 1, 0) + IY2 * V(0, j, 1, 0);
+          const T uxhyu = IY1 * V(0, j - 1, 2, 0) + IY2 * V(0, j, 2, 0);
+          const T uzhym = IY1 * V(2, j - 1, 0, -1) + IY2 * V(2, j, 0, -1);
+          const T uzhyc = IY1 * V(2, j - 1, 0, 0) + IY2 * V(2, j, 0, 0);
+          const T uzhyp = IY1 * V(2, j - 1, 0, 1) + IY2 * V(2, j, 0, 1);
+          const T uzhyu = IY1 * V(2, j - 1, 0, 2) + IY2 * V(2, j, 0, 2);
+          const T h21 = q.dx1 * hxa(1, j, -1, 0) * uxhym + q.dx2 * hxa(1, j, 0, 0) * uxhyc +
+                        q.dx3 * hxa(1, j, 1, 0) * uxhyp + q.dx4 * hxa(1, j, 2, 0) * uxhyu;
+          const T uy_jm = V(1, j - 1, 0, 0);
+          const T h22 = ((uy_jp + uy_c) * (uy_jp + uy_c) - (uy_c + uy_jm) * (uy_c + uy_jm)) * qsucac;
+          const T h23 = q.dz1 * hza(1, j, 0, -1) * uzhym + q.dz2 * hza(1, j, 0, 0) * uzhyc +
+                        q.dz3 * hza(1, j, 0, 1) * uzhyp + q.dz4 * hza(1, j, 0, 2) * uzhyu;
+          const T d11 = q.dxx1 * V(1, j, -2, 0) + q.dxx2 * V(1, j, -1, 0) + q.dxx3 * uy_c + q.dxx4 * V(1, j, 1, 0) +
+                        q.dxx5 * V(1, j, 2, 0);
+          const T d22 = __ldg(tr + MT_AP2P) * uy_jp + __ldg(tr + MT_AC2P) * uy_c + __ldg(tr + MT_AM2P) * uy_jm;
+          const T d33 = q.dzz1 * V(1, j, 0, -2) + q.dzz2 * V(1, j, 0, -1) + q.dzz3 * uy_c + q.dzz4 * V(1, j, 0, 1) +
+                        q.dzz5 * V(1, j, 0, 2);
+          const T conv = -h21 - h22 - h23 + xnu * (d11 + d33) + g.g2;
+          const T gradp = (V(3, j, 0, 0) - V(3, j - 1, 0, 0)) * sucac;
+          ry = pmGamma * conv + pmTheta * hyo - pmAlpha * gradp + two * pmBeta * d22;
+          hy[idx] = conv;
+        }
+        {  // RhsZ (:307-343)
+          const T uz_jm = V(2, j - 1, 0, 0);
+          const T uzhyc = IY1 * uz_jm + IY2 * uz_c;
+          const T uzhyp = IY3 * uz_c + IY4 * uz_jp;
+          const T h31 = q.dx1 * hxa(2, j, -1, 0) * hza(0, j, -1, 0) + q.dx2 * hxa(2, j, 0, 0) * hza(0, j, 0, 0) +
+                        q.dx3 * hxa(2, j, 1, 0) * hza(0, j, 1, 0) + q.dx4 * hxa(2, j, 2, 0) * hza(0, j, 2, 0);
+          const T h32 = ((top ? (T)0 : hza(1, j + 1, 0, 0)) * uzhyp - hza(1, j, 0, 0) * uzhyc) * sucaj;
+          const T b1 = uzhz(j, -2), b2 = uzhz(j, -1), b3 = uzhz(j, 0), b4 = uzhz(j, 1);
+          const T h33 = q.dz1 * b1 * b1 + q.dz2 * b2 * b2 + q.dz3 * b3 * b3 + q.dz4 * b4 * b4;
+          const T d11 = q.dxx1 * V(2, j, -2, 0) + q.dxx2 * V(2, j, -1, 0) + q.dxx3 * uz_c + q.dxx4 * V(2, j, 1, 0) +
+                        q.dxx5 * V(2, j, 2, 0);
+          const T d22 = __ldg(tr + MT_AP2C) * uz_jp + __ldg(tr + MT_AC2C) * uz_c + __ldg(tr + MT_AM2C) * uz_jm;
+          const T d33 = q.dzz1 * V(2, j, 0, -2) + q.dzz2 * V(2, j, 0, -1) + q.dzz3 * uz_c + q.dzz4 * V(2, j, 0, 1) +
+                        q.dzz5 * V(2, j, 0, 2);
+          const T conv = -h31 - h32 - h33 + xnu * (d11 + d33) + g.g3;
+          const T gradp = q.dz1 * V(3, j, 0, -2) + q.dz2 * V(3, j, 0, -1) + q.dz3 * V(3, j, 0, 0) + q.dz4 * V(3, j, 0, 1);
+          rz = pmGamma * conv + pmTheta * hzo - pmAlpha * gradp + two * pmBeta * d22;
+          hz[idx] = conv;
+        }
       }
       rx += dpm;                     // mean pressure gradient (clcRhsX_PIMP :61-74)
       if (j == 0) ry = (T)0;         // duy_ym: uy_ym is constant (Update_uy_ym_CH)
@@ -530,23 +628,34 @@ template <class T> static cudaError_t bulk_march_t(ch3d_ctx* c) {
 }
 cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float>(c) : bulk_march_t<double>(c); }
 
-template <class T> static cudaError_t rhs_march_t(ch3d_ctx* c) {
+template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
-  constexpr int BPS = sizeof(T) == 8 ? 4 : 5;  // resident blocks per SM (launch bounds)
+  constexpr int BPS = sizeof(T) == 8 ? 4 : 5;  // resident blocks per SM of the 2nd-order kernel
+  constexpr int H = O4 ? 3 : 1, PL = (32 + 2 * H) * (BZ + 2 * H);
+  const size_t smem = (size_t)4 * RS * PL * sizeof(T);
   T** f = (T**)c->f;
   k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab,
                                              march_beta_slots(c->mtab, c->ny), c->sc);
   static int nsm = 0;
   if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
+  auto kern = k_rhs_march<T, O4, BZ, D, RS>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
   const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + BZ - 1) / BZ);
-  // FP64: persistent blocks (back substitution overlapped with the next tile); FP32: one
-  // tile per block (measured faster: its shorter rows leave the overlapped loads exposed)
-  const long long cap = sizeof(T) == 8 ? (long long)nsm * BPS : ntiles;
+  // 2nd-order FP64: persistent blocks (back substitution overlapped with the next tile); otherwise
+  // one tile per block (measured faster for FP32: its shorter rows leave the overlapped loads exposed)
+  const long long cap = sizeof(T) == 8 && !O4 ? (long long)nsm * BPS : ntiles;
   const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
-  k_rhs_march<T, BZ, D, RS><<<grid, 32 * BZ, 0, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3],
-                                                     f[4], f[5], f[6], f[12], f[13], f[14], c->sc);
+  kern<<<grid, 32 * BZ, smem, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3], f[4], f[5],
+                                           f[6], f[12], f[13], f[14], c->sc);
   return cudaGetLastError();
 }
-cudaError_t launch_rhs_march(ch3d_ctx* c) { return c->fp32 ? rhs_march_t<float>(c) : rhs_march_t<double>(c); }
+cudaError_t launch_rhs_march(ch3d_ctx* c) {
+  if (c->cfg.order == 4) return c->fp32 ? rhs_march_t<float, true>(c) : rhs_march_t<double, true>(c);
+  return c->fp32 ? rhs_march_t<float, false>(c) : rhs_march_t<double, false>(c);
+}
 
 }  // namespace ch3d

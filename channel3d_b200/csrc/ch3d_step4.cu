@@ -1,7 +1,8 @@
 // ch3d_step4.cu -- sm_100a kernels specific to the 4th-order solver
-// (src/CFD_4th/m_TScheme.f90): the interpolated velocities, the fused
-// 4th-order RHS + y Crank-Nicolson solve, and the constant-flux forcing from
-// the mean viscous stress.  The pressure Poisson pipeline, projection and
+// (src/CFD_4th/m_TScheme.f90): the interpolated velocities and the RHS of the
+// stage entry points, and the constant-flux forcing from the mean viscous
+// stress.  The step runs the RHS and y solves as the column march of
+// ch3d_march.cu (4th-order branch).  The pressure Poisson pipeline, projection and
 // diagnostics are the 2nd-order kernels with their 4th-order branches.
 #include "ch3d_ctx.h"
 #include "ch3d_dev.cuh"
@@ -148,88 +149,6 @@ __global__ void __launch_bounds__(256) k_rhs4(Geo<T> g, Metrics<T> m, Interp4 ih
   rz[idx] = rhs4_comp<T, 2>(g, m, ih, ux, uy, uz, pr, hz, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
 }
 
-// Fused 4th-order RHS + y Crank-Nicolson solve (clcRhsXYZ + clcU1/2/3Hat,
-// src/CFD_4th/m_TScheme.f90:189-549).  Block: one velocity component, TI
-// consecutive i at one k, all j; the RHS of every row goes to shared memory,
-// then the partitioned tridiagonal solve (chunk sweeps, interface system,
-// reconstruction).  RhsX gets -pmAlpha*dpmdxns through sc->dpmdxns.
-template <class T, int C, int TI>
-__device__ __forceinline__ void rhs4_uhat_body(const Geo<T>& g, const Metrics<T>& m, const Interp4& ih,
-                                               const double* __restrict__ fac, int P, const T* __restrict__ ux,
-                                               const T* __restrict__ uy, const T* __restrict__ uz,
-                                               const T* __restrict__ pr, T* __restrict__ h, T* __restrict__ us,
-                                               int i0, int k, const DevScalars* __restrict__ sc, T* F, T* IF,
-                                               T* FS) {
-  const int nx = g.nx, ny = g.ny, Q = P - 1;
-  const int QQ = 2 * (Q > 0 ? Q : 1);
-  {  // this component's Helmholtz factors, staged in shared memory
-    const double* FG = fac + (C == 1 ? helm_set_stride(ny, P) : 0);
-    for (int t = threadIdx.x; t < helm_set_stride(ny, P); t += blockDim.x) FS[t] = (T)FG[t];
-  }
-  const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
-  const T add = C == 0 ? (T)sc->dpmdxns : (T)0;
-  const int tid = threadIdx.x;
-  for (int t = tid; t < ny * TI; t += blockDim.x) {
-    const int j = t / TI, ii = t % TI, i = i0 + ii;
-    T r = (T)0;
-    if (i < nx) r = rhs4_comp<T, C>(g, m, ih, ux, uy, uz, pr, h, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
-    if (C == 0) r += add;
-    if (C == 1 && j == 0) r = (T)0;  // duy_ym = 0 (Update_uy_ym, src/CFD_4th/m_FlowCase.f90:162-172)
-    F[t] = r;
-  }
-  __syncthreads();
-  for (int t = tid; t < TI * P; t += blockDim.x) {
-    const int ii = t % TI, p = t / TI;
-    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
-    T d = F[s * TI + ii] * (T)FS[s];
-    F[s * TI + ii] = d;
-    for (int j = s + 1; j <= e; ++j) {
-      d = (F[j * TI + ii] - (T)FS[ny + j] * d) * (T)FS[j];
-      F[j * TI + ii] = d;
-    }
-    for (int j = e - 1; j >= s; --j) {
-      d = F[j * TI + ii] - (T)FS[2 * ny + j] * d;
-      F[j * TI + ii] = d;
-    }
-  }
-  __syncthreads();
-  for (int t = tid; t < TI; t += blockDim.x) helm_interfaces<T>(FS + 5 * ny, F + t, TI, ny, P, IF + (size_t)t * QQ);
-  __syncthreads();
-  const T* u = C == 0 ? ux : (C == 1 ? uy : uz);
-  for (int t = tid; t < TI * P; t += blockDim.x) {
-    const int ii = t % TI, p = t / TI, i = i0 + ii;
-    if (i >= nx) continue;
-    const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
-    const T* G = IF + (size_t)ii * QQ;
-    const T uL = p > 0 ? G[2 * (p - 1)] : (T)0;
-    const T wR = p < P - 1 ? G[2 * p + 1] : (T)0;
-    long long idx = i + (long long)nx * (s + (long long)ny * k);
-    for (int j = s; j <= e; ++j, idx += nx) {
-      const T x = F[j * TI + ii] + (T)FS[3 * ny + j] * uL + (T)FS[4 * ny + j] * wR;
-      us[idx] = __ldg(u + idx) + x;
-    }
-  }
-}
-
-template <class T, int TI>
-__global__ void __launch_bounds__(256, 4) k_rhs4_uhat(Geo<T> g, Metrics<T> m, Interp4 ih, const double* __restrict__ fac,
-                                                      int P, const T* __restrict__ ux, const T* __restrict__ uy,
-                                                      const T* __restrict__ uz, const T* __restrict__ pr,
-                                                      T* __restrict__ hx, T* __restrict__ hy, T* __restrict__ hz,
-                                                      T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
-                                                      const DevScalars* __restrict__ sc) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  if (sc->status) return;
-  const int comp = blockIdx.x % 3;
-  const int i0 = (blockIdx.x / 3) * TI, k = blockIdx.y;
-  T* F = (T*)smem_raw;
-  T* IF = F + (size_t)g.ny * TI;
-  T* FS = IF + (size_t)TI * 2 * (P > 1 ? P - 1 : 1);
-  if (comp == 0) rhs4_uhat_body<T, 0, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hx, uxs, i0, k, sc, F, IF, FS);
-  else if (comp == 1) rhs4_uhat_body<T, 1, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hy, uys, i0, k, sc, F, IF, FS);
-  else rhs4_uhat_body<T, 2, TI>(g, m, ih, fac, P, ux, uy, uz, pr, hz, uzs, i0, k, sc, F, IF, FS);
-}
-
 // Block partial sums of (d11q1 + d33q1 + d22q1) * dyp over ux: the mean
 // viscous stress of the constant-flux forcing (src/CFD_4th/m_TScheme.f90:255-262,364-377).
 template <class T>
@@ -280,27 +199,6 @@ template <class T> static cudaError_t interp4_t(ch3d_ctx* c) {
   return cudaGetLastError();
 }
 
-template <class T> static cudaError_t rhs4_uhat_t(ch3d_ctx* c) {
-  constexpr int TI = 16;
-  cudaError_t e = interp4_t<T>(c);
-  if (e != cudaSuccess) return e;
-  T** f = (T**)c->f;
-  const int P = c->Pv, Q = P - 1;
-  size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) +
-                (size_t)helm_set_stride(c->ny, P) * sizeof(T) + 16;
-  static bool attr_set[2] = {false, false};
-  auto kern = k_rhs4_uhat<T, TI>;
-  if (!attr_set[sizeof(T) == 4]) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set[sizeof(T) == 4] = true;
-  }
-  dim3 grid(3 * ((c->nx + TI - 1) / TI), c->nz, 1);
-  int nthr = TI * P < 64 ? 64 : (TI * P > 256 ? 256 : TI * P);
-  kern<<<grid, nthr, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), interp_of<T>(c), c->hfac, P, f[0], f[1], f[2],
-                                        f[3], f[4], f[5], f[6], f[12], f[13], f[14], c->sc);
-  return cudaGetLastError();
-}
-cudaError_t launch_rhs4_uhat(ch3d_ctx* c) { return c->fp32 ? rhs4_uhat_t<float>(c) : rhs4_uhat_t<double>(c); }
 
 template <class T> static cudaError_t rhs4_t(ch3d_ctx* c) {
   cudaError_t e = interp4_t<T>(c);

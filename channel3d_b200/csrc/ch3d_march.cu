@@ -206,15 +206,17 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
   }
 
   // previous tile: row rb = ny-2-j of its back substitution at forward row j, its g
-  // loaded one row ahead
-  T n0 = (T)0, n1 = (T)0, n2 = (T)0;
+  // loaded two rows ahead
+  T n0 = (T)0, n1 = (T)0, n2 = (T)0, m0 = (T)0, m1 = (T)0, m2 = (T)0;
   if (pact && ny >= 2) { n0 = uxs[pidx - nx]; n1 = uys[pidx - nx]; n2 = uzs[pidx - nx]; }
+  if (pact && ny >= 3) { m0 = uxs[pidx - 2 * nx]; m1 = uys[pidx - 2 * nx]; m2 = uzs[pidx - 2 * nx]; }
   for (int j = 0; j < ny; ++j) {
     const int rb = ny - 2 - j;
     const bool bsub = pact && rb >= 0;
     const long long ob = pidx - (long long)(j + 1) * nx;
     const T b0 = n0, b1 = n1, b2 = n2;
-    if (pact && rb >= 1) { n0 = uxs[ob - nx]; n1 = uys[ob - nx]; n2 = uzs[ob - nx]; }
+    n0 = m0; n1 = m1; n2 = m2;
+    if (pact && rb >= 2) { m0 = uxs[ob - 2 * nx]; m1 = uys[ob - 2 * nx]; m2 = uzs[ob - 2 * nx]; }
     cp_async_wait<D>();  // this thread's copies of rows <= j+1 are done
     if (j + 1 == ny) ghost_row(ny);
     if (j == 0) ghost_row(-1);
@@ -645,9 +647,9 @@ template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
     attr = true;
   }
   const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + BZ - 1) / BZ);
-  // 2nd-order FP64: persistent blocks (back substitution overlapped with the next tile); otherwise
-  // one tile per block (measured faster for FP32: its shorter rows leave the overlapped loads exposed)
-  const long long cap = sizeof(T) == 8 && !O4 ? (long long)nsm * BPS : ntiles;
+  // 2nd order: persistent blocks (back substitution overlapped with the next tile's march);
+  // 4th order: one tile per block
+  const long long cap = !O4 ? (long long)nsm * BPS : ntiles;
   const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
   kern<<<grid, 32 * BZ, smem, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3], f[4], f[5],
                                            f[6], f[12], f[13], f[14], c->sc);

@@ -60,3 +60,26 @@ def test_step_parity_plans(built, shape, nsteps):
         assert e < 1e-10, (shape, k, e)
     assert di["divmax2"] < 1e-12
     s.close()
+
+
+def test_step_parity_persistent_march(built):
+    """More column tiles (8 x 81 = 648) than resident march blocks (4 FP64,
+    5 FP32 per SM on 148 SMs: 592 / 740), so the persistent FP64 blocks overlap
+    each tile's back substitution with the next tile's forward march; 3 steps
+    against the oracle."""
+    from channel3d_b200 import ChannelSolver, initfield, mesh_y
+    from oracle import oracle as O
+    cfg = small_channel(256, 24, 324)
+    yp = mesh_y(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp, seed=5)
+    o = O.Oracle(cfg)
+    o.set_state(ux, uy, uz, p)
+    s = ChannelSolver(cfg, yp=yp)
+    s.upload(ux, uy, uz, p)
+    s.step(3)
+    o.step(3)
+    go, gs = o.get_state(), s.download(hist=True)
+    for k in ("ux", "uy", "uz", "p"):
+        e = rel_l2(gs[k], go[k])
+        assert e < 1e-10, (k, e)
+    s.close()

@@ -67,6 +67,19 @@ __device__ __forceinline__ T at_jp(const T* __restrict__ a, const Geo<T>& g, int
   return g.bc.hi == -1 ? (T)(w * 2.0) - v : (T)(w * g.bc.dypN) + v;
 }
 
+// asynchronous 4-, 8- or 16-byte copy global -> shared (cp.async, completion by
+// commit groups; 16-byte copies bypass L1)
+template <class E> __device__ __forceinline__ void cp_async_el(E* smem, const E* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (sizeof(E) == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+  else if constexpr (sizeof(E) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // 4th-order stencil constants (src/CFD_4th/m_MeshAndMetries.f90:86-91)
 template <class T> struct C4 {
   T dx1, dx2, dx3, dx4, dz1, dz2, dz3, dz4;

@@ -84,17 +84,6 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
   if (threadIdx.x == 0) beta_slot[q] = bits;
 }
 
-// asynchronous 4- or 8-byte copy global -> shared (cp.async, completion by groups)
-template <class T> __device__ __forceinline__ void cp_async_el(T* smem, const T* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // Ring of RS row slots (row r in slot (r + 1) % RS); rows j+2 .. j+D+1 are in
 // flight while row j is computed.  Slot (j+D+2), written after the barrier of
 // iteration j, must differ from the slots of rows j-1, j, j+1 that other

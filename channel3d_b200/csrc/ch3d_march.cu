@@ -30,17 +30,24 @@ enum {
   MT_IY1, MT_IY3, MT_RDYP, MT_RDYC, MT_AP2C, MT_AC2C, MT_AM2C, MT_AP2P, MT_AC2P, MT_AM2P,
   MT_A0, MT_RM0, MT_CP0, MT_A1, MT_RM1, MT_CP1, MT_W
 };
+// Second table for the twisted march (lower half eliminated upwards, upper half
+// downwards): the downward factors c, 1/m', a/m' of both sets, with
+// m'_{ny-1} = b, m'_j = b_j - c_j aq_{j+1}; rows of MD_W values.
+enum { MD_C0, MD_RQ0, MD_AQ0, MD_C1, MD_RQ1, MD_AQ1, MD_W = 8 };
 
-// Layout of the march table buffer: one table per RK substep (ns = 1..3,
-// ny * MT_W values of precision T each), then per substep the pmBeta its
-// factors were computed for (FP64 bit patterns; all ones = not yet computed).
+// Layout of the march table buffer (values of precision T at the start of a
+// buffer sized for FP64): the row tables of the RK substeps ns = 1..3 (ny * MT_W
+// values each), their downward tables (ny * MD_W each), then per substep the
+// pmBeta its factors were computed for (FP64 bit patterns; all ones = not yet
+// computed).
 constexpr int kMarchTables = 3;
 size_t march_table_bytes(int ny) {
-  return (size_t)kMarchTables * ny * MT_W * sizeof(double) + kMarchTables * sizeof(unsigned long long);
+  return (size_t)kMarchTables * ny * (MT_W + MD_W) * sizeof(double) + kMarchTables * sizeof(unsigned long long);
 }
 static unsigned long long* march_beta_slots(void* mtab, int ny) {
-  return (unsigned long long*)((char*)mtab + (size_t)kMarchTables * ny * MT_W * sizeof(double));
+  return (unsigned long long*)((char*)mtab + (size_t)kMarchTables * ny * (MT_W + MD_W) * sizeof(double));
 }
+template <class T> static T* march_down_tables(void* mtab, int ny) { return (T*)mtab + (size_t)kMarchTables * ny * MT_W; }
 cudaError_t march_table_reset(ch3d_ctx* c) {
   return cudaMemsetAsync(march_beta_slots(c->mtab, c->ny), 0xff, kMarchTables * sizeof(unsigned long long),
                          c->stream);
@@ -49,7 +56,7 @@ cudaError_t march_table_reset(ch3d_ctx* c) {
 // Table of substep sc->ns; skipped when it already holds the factors of this
 // pmBeta (constant dt: computed once per substep of the run).
 template <class T>
-__global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__ tabs,
+__global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__ tabs, T* __restrict__ dtabs,
                               unsigned long long* __restrict__ beta_slot, const DevScalars* __restrict__ sc) {
   if (sc->status) return;
   const int q = sc->ns - 1;
@@ -72,6 +79,22 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
       cpp = cp;
     }
   }
+  if (threadIdx.x == 64 || threadIdx.x == 96) {  // downward elimination, sequential from the top
+    const int set = threadIdx.x == 64 ? 0 : 1;
+    const double pmBeta = sc->pmBeta;
+    T* col = dtabs + (size_t)q * ny * MD_W + (set ? MD_C1 : MD_C0);
+    double aqn = 0.0;
+    for (int j = ny - 1; j >= 0; --j) {
+      double a, b, c;
+      helm_abc(hc, set, pmBeta, j, a, b, c);
+      const double rq = 1.0 / (j == ny - 1 ? b : b - c * aqn);
+      const double aq = a * rq;
+      col[(size_t)j * MD_W + 0] = (T)c;
+      col[(size_t)j * MD_W + 1] = (T)rq;
+      col[(size_t)j * MD_W + 2] = (T)aq;
+      aqn = aq;
+    }
+  }
   for (int j = threadIdx.x; j < ny; j += blockDim.x) {
     const int jc = j + 1;
     T* row = tab + (size_t)j * MT_W;
@@ -92,9 +115,16 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
 // O4: the 4th-order right-hand sides (clcRhsXYZ, src/CFD_4th/m_TScheme.f90:
 // 189-377) with a 3-cell x/z halo; their x- and z-interpolated velocities
 // (:209-227) are formed from the staged rows instead of being stored.
-template <class T, bool O4, int BZ, int D, int RS>
-__global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 640) : 512) / (32 * BZ))
-    k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ ux, const T* __restrict__ uy,
+//
+// TW (twisted, for grids with too few column tiles to fill the GPU): the block
+// has two thread groups per tile; the lower marches rows 0..m-1 upwards with the
+// upward elimination, the upper rows ny-1..m downwards with the downward one,
+// each with its own row ring; they meet at rows m-1, m (a 2x2 solve) and
+// substitute outwards.  Same right-hand sides, half the march length.
+template <class T, bool O4, bool TW, int BZ, int D, int RS>
+__global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
+                                  (sizeof(T) == 4 || O4 ? (O4 ? 384 : 640) : 512) / (32 * BZ * (TW ? 2 : 1)))
+    k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ dtab, const T* __restrict__ ux, const T* __restrict__ uy,
                 const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
                 T* __restrict__ hz, T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
                 const DevScalars* __restrict__ sc) {
@@ -103,13 +133,28 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
   constexpr int NS = (PL + NT - 1) / NT;  // staging slots per thread and array
   static_assert(RS >= D + 4, "ring too small for the prefetch distance");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T (*ring)[RS][PL] = reinterpret_cast<T (*)[RS][PL]>(smem_raw);  // [4][RS][PL]: ux uy uz p
+  const int hf = TW ? (int)threadIdx.x / NT : 0;  // thread group: 0 lower (or the only one), 1 upper
+  T (*ring)[RS][PL] = reinterpret_cast<T (*)[RS][PL]>(smem_raw + (size_t)hf * 4 * RS * PL * sizeof(T));
   if (sc->status) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long plane = (long long)nx * ny;
-  tab += (size_t)(sc->ns - 1) * ny * MT_W;  // this substep's table
-  const int tid = threadIdx.x, tx = tid & 31, tz = tid >> 5;
+  tab += (size_t)(sc->ns - 1) * ny * MT_W;  // this substep's tables
+  dtab += (size_t)(sc->ns - 1) * ny * MD_W;
+  const int tid = TW ? (int)threadIdx.x - hf * NT : (int)threadIdx.x, tx = tid & 31, tz = tid >> 5;
+  const int mh = TW ? ny / 2 : ny;          // rows of the lower group (all rows without TW)
+  const int nrow = TW && hf ? ny - mh : mh;  // rows this group marches
+  const int dj = hf ? -1 : 1;                // march direction
+  auto in_group = [&](int r) { return TW ? (hf ? r >= mh - 1 && r < ny : r >= 0 && r <= mh) : r >= 0 && r < ny; };
   auto slot = [](int r) { return (r + 1) % RS; };  // r >= -1
+  // the groups march different numbers of rows (ny odd): each syncs on its own named barrier
+  auto group_sync = [&]() {
+    if constexpr (TW) {
+      if (hf) asm volatile("bar.sync 2, %0;" ::"n"(NT) : "memory");
+      else asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+    } else {
+      __syncthreads();
+    }
+  };
   long long so[NS];  // staging slot offsets of the current tile
   auto issue_row = [&](int r) {  // r < ny
     const long long ro = (long long)r * nx;
@@ -176,30 +221,35 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
     if (kg < 0) kg += nz;
     so[q] = s < PL ? ig + plane * kg : 0;
   }
-  // prologue: rows 0 .. D+1 in flight, one copy group per row
+  // prologue: the first D+2 rows of the march in flight, one copy group per row
 #pragma unroll
   for (int r = 0; r <= D + 1; ++r) {
-    if (r < ny) issue_row(r);
+    const int row = hf ? ny - 1 - r : r;
+    if (in_group(row)) issue_row(row);
     cp_async_commit();
   }
-  long long idx = act ? i + plane * k : 0;
+  const int jstart = hf ? ny - 1 : 0;
+  long long idx = act ? i + plane * k + (long long)jstart * nx : 0;
   T d0 = (T)0, d1 = (T)0, d2 = (T)0;       // eliminated right-hand sides of the previous row
   T g0 = (T)0, g1 = (T)0, g2 = (T)0;       // g of the last row (= u* of row ny-1)
   T hxo = (T)0, hyo = (T)0, hzo = (T)0;    // Hist of row j
   T hx1 = (T)0, hy1 = (T)0, hz1 = (T)0;    // Hist of row j+1
   // pmTheta = 0 (first RK3 substep): the old Hist does not enter, so it is not read
   const bool hread = act && pmTheta != (T)0;
+  const long long hstep = (long long)dj * nx;
   if (hread) {
     hxo = hx[idx]; hyo = hy[idx]; hzo = hz[idx];
-    if (ny > 1) { hx1 = hx[idx + nx]; hy1 = hy[idx + nx]; hz1 = hz[idx + nx]; }
+    if (nrow > 1) { hx1 = hx[idx + hstep]; hy1 = hy[idx + hstep]; hz1 = hz[idx + hstep]; }
   }
+  T lu0 = (T)0, lu1 = (T)0, lu2 = (T)0;  // u at the group's last row (TW meeting)
 
   // previous tile: row rb = ny-2-j of its back substitution at forward row j, its g
   // loaded two rows ahead
   T n0 = (T)0, n1 = (T)0, n2 = (T)0, m0 = (T)0, m1 = (T)0, m2 = (T)0;
   if (pact && ny >= 2) { n0 = uxs[pidx - nx]; n1 = uys[pidx - nx]; n2 = uzs[pidx - nx]; }
   if (pact && ny >= 3) { m0 = uxs[pidx - 2 * nx]; m1 = uys[pidx - 2 * nx]; m2 = uzs[pidx - 2 * nx]; }
-  for (int j = 0; j < ny; ++j) {
+  for (int sj = 0; sj < nrow; ++sj) {
+    const int j = jstart + dj * sj;
     const int rb = ny - 2 - j;
     const bool bsub = pact && rb >= 0;
     const long long ob = pidx - (long long)(j + 1) * nx;
@@ -209,13 +259,13 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
     cp_async_wait<D>();  // this thread's copies of rows <= j+1 are done
     if (j + 1 == ny) ghost_row(ny);
     if (j == 0) ghost_row(-1);
-    __syncthreads();
-    if (j + D + 2 < ny) issue_row(j + D + 2);
+    group_sync();
+    if (in_group(j + dj * (D + 2))) issue_row(j + dj * (D + 2));
     cp_async_commit();
     T hxn = (T)0, hyn = (T)0, hzn = (T)0;
-    if (hread && j + 2 < ny) { hxn = hx[idx + 2 * nx]; hyn = hy[idx + 2 * nx]; hzn = hz[idx + 2 * nx]; }
+    if (hread && sj + 2 < nrow) { hxn = hx[idx + 2 * hstep]; hyn = hy[idx + 2 * hstep]; hzn = hz[idx + 2 * hstep]; }
     if (act) {
-      T rx, ry, rz, ux_c, uy_c, uz_c, ux_jp, uy_jp, uz_jp;
+      T rx, ry, rz, ux_c, uy_c, uz_c, ux_jp, uy_jp, uz_jp, ux_jm, uy_jm, uz_jm;
       const T* tr = tab + (size_t)j * MT_W;
       if constexpr (!O4) {
       const T* X0 = &ring[0][slot(j - 1)][c0];
@@ -230,11 +280,11 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
       const T* P0 = &ring[3][slot(j - 1)][c0];
       const T* P1 = &ring[3][slot(j)][c0];
 
-      ux_c = X1[0]; const T ux_ip = X1[1], ux_im = X1[-1]; ux_jp = X2[0]; const T ux_jm = X0[0];
+      ux_c = X1[0]; const T ux_ip = X1[1], ux_im = X1[-1]; ux_jp = X2[0]; ux_jm = X0[0];
       const T ux_kp = X1[SX], ux_km = X1[-SX], ux_ip_jm = X0[1], ux_ip_km = X1[1 - SX];
-      uy_c = Y1[0]; uy_jp = Y2[0]; const T uy_ip = Y1[1], uy_im = Y1[-1], uy_jm = Y0[0];
+      uy_c = Y1[0]; uy_jp = Y2[0]; uy_jm = Y0[0]; const T uy_ip = Y1[1], uy_im = Y1[-1];
       const T uy_im_jp = Y2[-1], uy_kp = Y1[SX], uy_km = Y1[-SX], uy_jp_km = Y2[-SX];
-      uz_c = Z1[0]; uz_jp = Z2[0]; const T uz_ip = Z1[1], uz_im = Z1[-1], uz_jm = Z0[0];
+      uz_c = Z1[0]; uz_jp = Z2[0]; uz_jm = Z0[0]; const T uz_ip = Z1[1], uz_im = Z1[-1];
       const T uz_kp = Z1[SX], uz_km = Z1[-SX], uz_im_kp = Z1[SX - 1], uz_jm_kp = Z0[SX];
       const T p_c = P1[0], p_im = P1[-1], p_jm = P0[0], p_km = P1[-SX];
 
@@ -307,11 +357,10 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
         const T IY1 = __ldg(tr + MT_IY1), IY2 = one - IY1;
         const T IY3 = __ldg(tr + MT_IY3), IY4 = one - IY3;
         const T sucaj = __ldg(tr + MT_RDYP);
-        ux_c = V(0, j, 0, 0); ux_jp = V(0, j + 1, 0, 0);
-        uy_c = V(1, j, 0, 0); uy_jp = V(1, j + 1, 0, 0);
-        uz_c = V(2, j, 0, 0); uz_jp = V(2, j + 1, 0, 0);
+        ux_c = V(0, j, 0, 0); ux_jp = V(0, j + 1, 0, 0); ux_jm = V(0, j - 1, 0, 0);
+        uy_c = V(1, j, 0, 0); uy_jp = V(1, j + 1, 0, 0); uy_jm = V(1, j - 1, 0, 0);
+        uz_c = V(2, j, 0, 0); uz_jp = V(2, j + 1, 0, 0); uz_jm = V(2, j - 1, 0, 0);
         {  // RhsX (:235-268)
-          const T ux_jm = V(0, j - 1, 0, 0);
           const T uxhyc = IY1 * ux_jm + IY2 * ux_c;
           const T uxhyp = IY3 * ux_c + IY4 * ux_jp;
           const T a1 = uxhx(j, -2, 0), a2 = uxhx(j, -1, 0), a3 = uxhx(j, 0, 0), a4 = uxhx(j, 1, 0);
@@ -341,7 +390,6 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
           const T uzhyu = IY1 * V(2, j - 1, 0, 2) + IY2 * V(2, j, 0, 2);
           const T h21 = q.dx1 * hxa(1, j, -1, 0) * uxhym + q.dx2 * hxa(1, j, 0, 0) * uxhyc +
                         q.dx3 * hxa(1, j, 1, 0) * uxhyp + q.dx4 * hxa(1, j, 2, 0) * uxhyu;
-          const T uy_jm = V(1, j - 1, 0, 0);
           const T h22 = ((uy_jp + uy_c) * (uy_jp + uy_c) - (uy_c + uy_jm) * (uy_c + uy_jm)) * qsucac;
           const T h23 = q.dz1 * hza(1, j, 0, -1) * uzhym + q.dz2 * hza(1, j, 0, 0) * uzhyc +
                         q.dz3 * hza(1, j, 0, 1) * uzhyp + q.dz4 * hza(1, j, 0, 2) * uzhyu;
@@ -356,7 +404,6 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
           hy[idx] = conv;
         }
         {  // RhsZ (:307-343)
-          const T uz_jm = V(2, j - 1, 0, 0);
           const T uzhyc = IY1 * uz_jm + IY2 * uz_c;
           const T uzhyp = IY3 * uz_c + IY4 * uz_jp;
           const T h31 = q.dx1 * hxa(2, j, -1, 0) * hza(0, j, -1, 0) + q.dx2 * hxa(2, j, 0, 0) * hza(0, j, 0, 0) +
@@ -377,13 +424,24 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
       }
       rx += dpm;                     // mean pressure gradient (clcRhsX_PIMP :61-74)
       if (j == 0) ry = (T)0;         // duy_ym: uy_ym is constant (Update_uy_ym_CH)
-      d0 = (rx - __ldg(tr + MT_A0) * d0) * __ldg(tr + MT_RM0);
-      d1 = (ry - __ldg(tr + MT_A1) * d1) * __ldg(tr + MT_RM1);
-      d2 = (rz - __ldg(tr + MT_A0) * d2) * __ldg(tr + MT_RM0);
-      g0 = ux_c + d0 + __ldg(tr + MT_CP0) * ux_jp;
-      g1 = uy_c + d1 + __ldg(tr + MT_CP1) * uy_jp;
-      g2 = uz_c + d2 + __ldg(tr + MT_CP0) * uz_jp;
+      if (!TW || hf == 0) {  // upward elimination; g = u + d + cp u_{j+1}
+        d0 = (rx - __ldg(tr + MT_A0) * d0) * __ldg(tr + MT_RM0);
+        d1 = (ry - __ldg(tr + MT_A1) * d1) * __ldg(tr + MT_RM1);
+        d2 = (rz - __ldg(tr + MT_A0) * d2) * __ldg(tr + MT_RM0);
+        g0 = ux_c + d0 + __ldg(tr + MT_CP0) * ux_jp;
+        g1 = uy_c + d1 + __ldg(tr + MT_CP1) * uy_jp;
+        g2 = uz_c + d2 + __ldg(tr + MT_CP0) * uz_jp;
+      } else {               // downward elimination; g = u + e + aq u_{j-1}
+        const T* td = dtab + (size_t)j * MD_W;
+        d0 = (rx - __ldg(td + MD_C0) * d0) * __ldg(td + MD_RQ0);
+        d1 = (ry - __ldg(td + MD_C1) * d1) * __ldg(td + MD_RQ1);
+        d2 = (rz - __ldg(td + MD_C0) * d2) * __ldg(td + MD_RQ0);
+        g0 = ux_c + d0 + __ldg(td + MD_AQ0) * ux_jm;
+        g1 = uy_c + d1 + __ldg(td + MD_AQ1) * uy_jm;
+        g2 = uz_c + d2 + __ldg(td + MD_AQ0) * uz_jm;
+      }
       uxs[idx] = g0; uys[idx] = g1; uzs[idx] = g2;
+      lu0 = ux_c; lu1 = uy_c; lu2 = uz_c;
     }
     if (bsub) {  // u*_rb = g_rb - cp_rb u*_{rb+1}
       const T* tb = tab + (size_t)rb * MT_W;
@@ -391,12 +449,67 @@ __global__ void __launch_bounds__(32 * BZ, (sizeof(T) == 4 || O4 ? (O4 ? 384 : 6
       p0 = b0 - cb0 * p0; p1 = b1 - cb1 * p1; p2 = b2 - cb0 * p2;
       uxs[ob] = p0; uys[ob] = p1; uzs[ob] = p2;
     }
-    idx += nx;
+    idx += hstep;
     hxo = hx1; hyo = hy1; hzo = hz1;
     hx1 = hxn; hy1 = hyn; hz1 = hzn;
   }
   cp_async_wait<0>();
-  __syncthreads();  // the ring is refilled by the next tile's prologue
+  __syncthreads();  // the ring is refilled by the next tile's prologue (or reused below)
+  if constexpr (TW) {
+    // meeting of the groups at rows m-1 (lower: x = d - cp x_m) and m (upper: x = e - aq x_{m-1})
+    T* xch = reinterpret_cast<T*>(smem_raw);  // [2][NT][6]
+    if (act) {
+      T* o = xch + ((size_t)hf * NT + tid) * 6;
+      o[0] = d0; o[1] = d1; o[2] = d2; o[3] = lu0; o[4] = lu1; o[5] = lu2;
+    }
+    __syncthreads();
+    if (!act) return;
+    const T* lo = xch + (size_t)tid * 6;
+    const T* up = xch + ((size_t)NT + tid) * 6;
+    const T* tl = tab + (size_t)(mh - 1) * MT_W;
+    const T* tu = dtab + (size_t)mh * MD_W;
+    T xl[3], xu[3];
+    const T cpl[3] = {__ldg(tl + MT_CP0), __ldg(tl + MT_CP1), __ldg(tl + MT_CP0)};
+    const T aqu[3] = {__ldg(tu + MD_AQ0), __ldg(tu + MD_AQ1), __ldg(tu + MD_AQ0)};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      xl[q] = (lo[q] - cpl[q] * up[q]) / ((T)1 - cpl[q] * aqu[q]);
+      xu[q] = up[q] - aqu[q] * xl[q];
+    }
+    // this group's boundary row, then outwards: u*_j = g_j - f_j u*_{j -+ 1}
+    const int jb = hf ? mh : mh - 1;
+    const T* uu = hf ? up : lo;
+    const T* xx = hf ? xu : xl;
+    long long o = i + plane * k + (long long)jb * nx;
+    T c0v = uu[3] + xx[0], c1v = uu[4] + xx[1], c2v = uu[5] + xx[2];
+    uxs[o] = c0v; uys[o] = c1v; uzs[o] = c2v;
+    const T* ft = hf ? dtab : tab;  // substitution factors: aq (upper group) or cp (lower)
+    const int fw = hf ? MD_W : MT_W, fo0 = hf ? MD_AQ0 : MT_CP0, fo1 = hf ? MD_AQ1 : MT_CP1;
+    const int nout = hf ? ny - 1 - jb : jb;  // rows still to substitute
+    constexpr int B = 8;
+    for (int r0 = 0; r0 < nout; r0 += B) {
+      T a0[B], a1[B], a2[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        if (r0 + b < nout) {
+          const long long ob = o - (long long)dj * (r0 + b + 1) * nx;
+          a0[b] = uxs[ob]; a1[b] = uys[ob]; a2[b] = uzs[ob];
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        if (r0 + b < nout) {
+          const int jr = jb - dj * (r0 + b + 1);
+          const T* tb = ft + (size_t)jr * fw;
+          const T f0 = __ldg(tb + fo0), f1 = __ldg(tb + fo1);
+          c0v = a0[b] - f0 * c0v; c1v = a1[b] - f1 * c1v; c2v = a2[b] - f0 * c2v;
+          const long long ob = o - (long long)dj * (r0 + b + 1) * nx;
+          uxs[ob] = c0v; uys[ob] = c1v; uzs[ob] = c2v;
+        }
+      }
+    }
+    return;
+  }
   pact = act; pidx = idx - nx; p0 = g0; p1 = g1; p2 = g2;
   }  // tiles
   if (!pact) return;
@@ -626,22 +739,32 @@ template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   const size_t smem = (size_t)4 * RS * PL * sizeof(T);
   T** f = (T**)c->f;
   k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab,
+                                             march_down_tables<T>(c->mtab, c->ny),
                                              march_beta_slots(c->mtab, c->ny), c->sc);
-  static int nsm = 0;
-  if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
-  auto kern = k_rhs_march<T, O4, BZ, D, RS>;
-  static bool attr = false;
-  if (!attr) {
+  auto kern = k_rhs_march<T, O4, false, BZ, D, RS>;
+  auto kern_tw = k_rhs_march<T, O4, true, BZ, D, RS>;
+  static int nsm = 0, occ_tw = 0;
+  if (!nsm) {
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
+    cudaFuncSetAttribute(kern_tw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tw, kern_tw, 64 * BZ, 2 * smem) != cudaSuccess)
+      occ_tw = 0;
   }
   const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + BZ - 1) / BZ);
-  // 2nd order: persistent blocks (back substitution overlapped with the next tile's march);
-  // 4th order: one tile per block
-  const long long cap = !O4 ? (long long)nsm * BPS : ntiles;
-  const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
-  kern<<<grid, 32 * BZ, smem, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, f[0], f[1], f[2], f[3], f[4], f[5],
-                                           f[6], f[12], f[13], f[14], c->sc);
+  auto args = [&](auto k, unsigned grid, int threads, size_t sm) {
+    k<<<grid, threads, sm, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, march_down_tables<T>(c->mtab, c->ny), f[0],
+                                        f[1], f[2], f[3], f[4], f[5], f[6], f[12], f[13], f[14], c->sc);
+  };
+  if (c->ny >= 2 && ntiles <= (long long)nsm * occ_tw) {
+    // few column tiles: all fit at once as two-group (twisted) blocks, half the march length
+    args(kern_tw, (unsigned)ntiles, 64 * BZ, 2 * smem);
+  } else {
+    // 2nd order: persistent blocks (back substitution overlapped with the next tile's march);
+    // 4th order: one tile per block
+    const long long cap = !O4 ? (long long)nsm * BPS : ntiles;
+    args(kern, (unsigned)(ntiles < cap ? ntiles : cap), 32 * BZ, smem);
+  }
   return cudaGetLastError();
 }
 cudaError_t launch_rhs_march(ch3d_ctx* c) {

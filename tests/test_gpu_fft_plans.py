@@ -62,6 +62,42 @@ def test_step_parity_plans(built, shape, nsteps):
     s.close()
 
 
+# the largest x length with every z plan, odd and smallest-odd ny
+ODD_NY_SHAPES = [(768, 9, 576), (768, 8, 384), (768, 5, 256)]
+
+
+@pytest.mark.parametrize("shape", ODD_NY_SHAPES)
+def test_poisson_plans_odd_ny_fp64(built, shape):
+    a, b = _poisson_pair(small_channel(*shape))
+    assert rel_l2(a, b) < 1e-12, (shape, rel_l2(a, b))
+
+
+@pytest.mark.parametrize("shape", ODD_NY_SHAPES)
+def test_poisson_plans_odd_ny_mixed(built, shape):
+    a, b = _poisson_pair(small_channel(*shape, precision="mixed"))
+    assert rel_l2(a, b) < 2e-5, (shape, rel_l2(a, b))
+
+
+def test_step_parity_plans_odd_ny(built):
+    from channel3d_b200 import ChannelSolver, initfield, mesh_y
+    from oracle import oracle as O
+    cfg = small_channel(768, 17, 576)
+    yp = mesh_y(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp, seed=9)
+    o = O.Oracle(cfg)
+    o.set_state(ux, uy, uz, p)
+    s = ChannelSolver(cfg, yp=yp)
+    s.upload(ux, uy, uz, p)
+    di = s.step(2)
+    o.step(2)
+    go, gs = o.get_state(), s.download()
+    for k in ("ux", "uy", "uz", "p"):
+        e = rel_l2(gs[k], go[k])
+        assert e < 1e-10, (k, e)
+    assert di["divmax2"] < 1e-12
+    s.close()
+
+
 def test_step_parity_persistent_march(built):
     """More column tiles (8 x 81 = 648) than resident march blocks (4 FP64,
     5 FP32 per SM on 148 SMs: 592 / 740), so the persistent FP64 blocks overlap

@@ -6,8 +6,8 @@
 //   zfft_r        z transform of the spectrum, in place
 //   xifft_r       inverse x C2R transform * normfft -> phi (m_Poisson.f90:1194-1200)
 // The x kernels give each line to P <= 32 threads of one warp and loop over
-// lines without block barriers; the z kernel gives a block L consecutive kx
-// lines (coalesced L x 16-byte segments per kz) of P threads each.
+// lines without block barriers; the z kernel gives a block LZ = 8 consecutive kx
+// lines (coalesced 8 x 16-byte segments per kz) of P threads each.
 #include "ch3d_ctx.h"
 #include "ch3d_dev.cuh"
 #include "rfft.cuh"
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_xifft_r(Geo<T> g, const typ
 }
 
 template <class T, class PL, int LZ>
-__global__ void __launch_bounds__(LZ * PL::P) k_zfft_r(Geo<T> g, typename CplxOf<T>::type* __restrict__ spec,
+__global__ void __launch_bounds__(LZ * PL::P, sizeof(T) == 8 ? 2 : 1) k_zfft_r(Geo<T> g, typename CplxOf<T>::type* __restrict__ spec,
                                                        const typename CplxOf<T>::type* __restrict__ tw, int inverse,
                                                        const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
@@ -262,7 +262,10 @@ bool launch_xifft_r(ch3d_ctx* c, cudaError_t* err) { return c->fp32 ? xifft_r_t<
 
 template <class T> static bool zfft_r_t(ch3d_ctx* c, int inverse, cudaError_t* err) {
   typedef typename CplxOf<T>::type CT;
-  constexpr int LZ = sizeof(T) == 8 ? 4 : 8;  // kx lines per block (measured best per precision)
+  // kx lines per block: 128-byte FP64 (64-byte FP32) segments per kz; FP64 held to two
+  // blocks per SM (80 registers).  Measured at 768x384x576: 4 lines 2.79 ms per spectral
+  // group, 8 lines 2.57, 16 lines 2.91
+  constexpr int LZ = 8;
   return with_zplan(c->nz, [&](auto plan) {
     typedef decltype(plan) PL;
     auto kern = k_zfft_r<T, PL, LZ>;

@@ -296,6 +296,10 @@ def run_ours(args, ws, rank, local):
     names[0] = GROUP0_KERNEL[key]
     if key == "pimp":
         names[5] = "k_proj_march"
+    gsub = "gsub" in s.path_flags()
+    if gsub:  # the march stops at g; the divergence and projection marches substitute u*
+        names[2] = "k_div_bsub+k_prsrc_xfft"
+        names[5] = "k_proj_bsub"
     per_group = {}
     for g, arrs in GROUP_ARRAYS.items():
         b = arrs * cfg.npoints * word
@@ -307,11 +311,14 @@ def run_ours(args, ws, rank, local):
     peak, peak_kind = load_peaks()
     dom_b = GROUP_ARRAYS[dom] * cfg.npoints * word
     achieved = dom_b / (kt[dom] * 1e-3) / 1e9
-    tpp, tsrc = profile_traffic(names[dom], args.precision)
+    # the march that stops at g moves less than the one that substitutes: its own profile line
+    tpp, tsrc = profile_traffic(names[dom] + ("/g" if gsub and dom == 0 else ""), args.precision)
     traffic = tpp * cfg.npoints if tpp is not None else None
     step_alg = ALG_ARRAYS_PER_SUBSTEP[key] * 3 * word * cfg.npoints
     step_achieved = step_alg / (ms_per_step * 1e-3) / 1e9
     launches = 1 + 3 * LAUNCHES_PER_SUBSTEP[args.precision] + 4
+    if gsub:
+        launches += 3  # divergence march + x FFT in place of the fused divergence/x FFT kernel
     if key == "order4":
         launches += 3 * 2        # mean viscous stress partials, interpolated velocities
     elif key == "fimp":

@@ -98,6 +98,7 @@ SIGNATURES = {
     "ch3d_stats_fetch": (ctypes.c_int, [_VP, _DP, _IP, _DP, ctypes.c_int]),
     "ch3d_memory_bytes": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_longlong)]),
     "ch3d_last_step_ms": (ctypes.c_int, [_VP, _DP]),
+    "ch3d_path_flags": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
     "ch3d_kernel_times": (ctypes.c_int, [_VP, ctypes.c_int, _DP, ctypes.c_int]),
     "ch3d_mlp_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_void_p, ctypes.c_void_p]),

@@ -467,14 +467,19 @@ int record_step(ch3d_ctx* c) {
     } else {
       CU(launch_rhs_march(c));  // 4th order: the same column march with the 4th-order stencils
     }
-    CU(launch_prsrc_xfft(c, 0));
+    if (c->gsub) {
+      CU(launch_div_bsub(c));
+      CU(launch_prsrc_xfft(c, 3));
+    } else {
+      CU(launch_prsrc_xfft(c, 0));
+    }
     CU(launch_poisson_spectral(c));
     CU(launch_xifft(c));
     if (ns == c->iadvance && march_diag_fusable(c)) {  // CheckDivergence etc. ride on the last projection
       CU(launch_diag_reset(c));
-      CU(launch_proj_diag(c));
+      CU(c->gsub ? launch_proj_bsub(c, true) : launch_proj_diag(c));
     } else {
-      CU(launch_proj(c, 0));
+      CU(c->gsub ? launch_proj_bsub(c, false) : launch_proj(c, 0));
     }
   }
   if (!march_diag_fusable(c)) CU(launch_diag(c));
@@ -641,6 +646,8 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     dim3 g((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz);
     c->npart = (int)(g.x * g.y * g.z);
     c->march = march_path(c);
+    // large 2nd-order grids: the march stops at g, the divergence and projection substitute
+    c->gsub = c->march && !march_twisted(c) && xplan_exists(c->nx / 2);
     c->npart_m = march_npart(c);
     if (c->npart_m > c->npart) c->npart = c->npart_m;
     if (diag_npart(c) > c->npart) c->npart = diag_npart(c);
@@ -1013,13 +1020,18 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
         CU(mark(0)); CU(launch_rhs_march(c)); CU(done());
         CU(mark(1)); CU(done());
       }
-      CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());
+      if (c->gsub) {
+        CU(mark(2)); CU(launch_div_bsub(c)); CU(launch_prsrc_xfft(c, 3)); CU(done());
+      } else {
+        CU(mark(2)); CU(launch_prsrc_xfft(c, 0)); CU(done());
+      }
       CU(mark(3)); CU(launch_poisson_spectral(c)); CU(done());
       CU(mark(4)); CU(launch_xifft(c)); CU(done());
       if (ns == c->iadvance && march_diag_fusable(c)) {
-        CU(mark(5)); CU(launch_diag_reset(c)); CU(launch_proj_diag(c)); CU(done());
+        CU(mark(5)); CU(launch_diag_reset(c));
+        CU(c->gsub ? launch_proj_bsub(c, true) : launch_proj_diag(c)); CU(done());
       } else {
-        CU(mark(5)); CU(launch_proj(c, 0)); CU(done());
+        CU(mark(5)); CU(c->gsub ? launch_proj_bsub(c, false) : launch_proj(c, 0)); CU(done());
       }
     }
     CU(mark(6)); if (!march_diag_fusable(c)) CU(launch_diag(c)); CU(launch_step_end(c)); CU(done());
@@ -1064,6 +1076,15 @@ int ch3d_poisson_noalloc(int nxc, int nyc, int nzc, double xlx, double zlz, cons
 int ch3d_last_step_ms(ch3d_ctx* c, double* ms) {
   if (!c || !ms) return fail(CH3D_ERR_INVALID, "NULL argument");
   *ms = c->last_ms;
+  return CH3D_OK;
+}
+
+int ch3d_path_flags(ch3d_ctx* c, int* flags) {
+  if (!c || !flags) return fail(CH3D_ERR_INVALID, "NULL argument");
+  CU(cudaSetDevice(c->device));
+  const bool march = march_path(c) || c->cfg.order == 4;
+  *flags = (march ? CH3D_PATH_MARCH : 0) | (march && march_twisted(c) ? CH3D_PATH_TWISTED : 0) |
+           (c->gsub ? CH3D_PATH_GSUB : 0);
   return CH3D_OK;
 }
 

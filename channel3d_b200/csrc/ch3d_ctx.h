@@ -52,6 +52,7 @@ struct ch3d_ctx {
   double* yRM64 = nullptr;   // mixed path: FP64 factors of the low modes (kx < TSy, |kz| <= KL)
   double* yCP64 = nullptr;
   double* ylow = nullptr;    // mixed path: FP64 forward-sweep scratch of the low modes
+  bool gsub = false;         // the march stops at g; divergence and projection substitute u*
   int KL = 8;
   int TSy = 8;               // kx extent of the FP64 low modes
   int Pv = 32;               // chunks of the partitioned velocity Helmholtz solves
@@ -98,11 +99,16 @@ cudaError_t launch_rhs_march(ch3d_ctx* c);             // u -> u*, Hist, with it
 size_t march_table_bytes(int ny);
 cudaError_t march_table_reset(ch3d_ctx* c);           // forget the cached factors
 cudaError_t launch_proj_march(ch3d_ctx* c, int mode, bool diag);  // projection + pressure update + bulk partials
+bool march_twisted(const ch3d_ctx* c);                 // the march runs as two-group (twisted) blocks
+cudaError_t launch_div_bsub(ch3d_ctx* c);               // div(u*) from g into phi's array (gsub)
+cudaError_t launch_proj_bsub(ch3d_ctx* c, bool diag);   // projection + pressure update from g (gsub)
+bool xplan_exists(int m);                               // the register x FFT has a plan for m = nx/2
 bool march_diag_fusable(const ch3d_ctx* c);            // the step diagnostics can ride on the last projection
 cudaError_t launch_bulk_march(ch3d_ctx* c);            // bulk partials of an uploaded field
 int march_npart(const ch3d_ctx* c);
 cudaError_t launch_helm_factors(ch3d_ctx* c);
-cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlpha, 1: div(u), 2: source in phi
+cudaError_t launch_prsrc_xfft(ch3d_ctx* c, int mode);  // mode 0: div(u*)/pmAlpha, 1: div(u), 2: source in phi,
+                                                       // 3: div(u*) in phi's array, /pmAlpha (register FFT only)
 cudaError_t launch_poisson_spectral(ch3d_ctx* c);      // z fwd, y solve, z inv
 cudaError_t launch_xifft(ch3d_ctx* c);
 // register-resident FFT kernels for the lengths with a plan (ch3d_rfft.cu);

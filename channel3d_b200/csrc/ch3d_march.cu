@@ -121,7 +121,11 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
 // upward elimination, the upper rows ny-1..m downwards with the downward one,
 // each with its own row ring; they meet at rows m-1, m (a 2x2 solve) and
 // substitute outwards.  Same right-hand sides, half the march length.
-template <class T, bool O4, bool TW, int BZ, int D, int RS>
+//
+// BS = false: the march stops at g; k_div_bsub and k_proj_bsub substitute
+// u* = g - cp u*_{j+1} themselves while they walk each column downwards, so u*
+// is never stored and g is never read back here (6 arrays less traffic).
+template <class T, bool O4, bool TW, bool BS, int BZ, int D, int RS>
 __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
                                   (sizeof(T) == 4 || O4 ? (O4 ? 384 : 640) : 512) / (32 * BZ * (TW ? 2 : 1)))
     k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ dtab, const T* __restrict__ ux, const T* __restrict__ uy,
@@ -510,7 +514,7 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
     }
     return;
   }
-  pact = act; pidx = idx - nx; p0 = g0; p1 = g1; p2 = g2;
+  pact = BS && act; pidx = idx - nx; p0 = g0; p1 = g1; p2 = g2;
   }  // tiles
   if (!pact) return;
 
@@ -701,6 +705,212 @@ __global__ void __launch_bounds__(128) k_bulk_march(Geo<T> g, Metrics<T> m, cons
   if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = bs;
 }
 
+// ---------------------------------------------------------------------------
+// Marches that substitute the march's g themselves (BS = false above): one
+// thread per (i, k) column, 32 x 4 columns per block, walking j downwards with
+// u*_j = g_j - cp_j u*_{j+1} (cp of the substep's row table; u*_{ny-1} = g_{ny-1}
+// since cp_{ny-1} = 0) for its own column and, where a stencil needs them, for
+// the columns at i+1 (ux) and k+1 (uz), with the same expressions as the
+// threads that own them.  All loads of a batch of PB rows are issued before its
+// recurrence steps.
+// ---------------------------------------------------------------------------
+
+// clcPrSrcOther (src/CFD_2nd/m_TScheme.f90:213-241): div(u*) per cell into dv
+// (scaled by 1/pmAlpha and transformed by the x kernel, mode 3), its maximum
+// |div| into divmax1 (CheckDivergence before the projection).
+template <class T>
+__global__ void __launch_bounds__(128) k_div_bsub(Geo<T> g, Metrics<T> m, const T* __restrict__ tab,
+                                                  const T* __restrict__ gx, const T* __restrict__ gy,
+                                                  const T* __restrict__ gz, T* __restrict__ dv,
+                                                  DevScalars* __restrict__ sc) {
+  __shared__ double red[4];
+  if (sc->status) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long plane = (long long)nx * ny;
+  tab += (size_t)(sc->ns - 1) * ny * MT_W;
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31), k = blockIdx.y * 4 + (threadIdx.x >> 5);
+  double dmax = 0.0;
+  if (i < nx && k < nz) {
+    const long long col = i + plane * k;
+    const long long dxp = i + 1 == nx ? 1 - nx : 1;                            // offset to i+1
+    const long long dzp = k + 1 == nz ? -(long long)(nz - 1) * plane : plane;  // offset to k+1
+    const T rdx = g.rdx, rdz = g.rdz;
+    T ax = (T)0, axp = (T)0, ay = (T)0, az = (T)0, azp = (T)0;  // u* of row j+1
+    T ayn = (T)g.bc.uy_hi;  // uy at j+1: the wall value above the top row
+    // rows ny-1-b, ny-1-b-PB, ... pass through register slot b; a slot is refilled
+    // with the row PB below as soon as it is consumed
+    constexpr int PB = 4;
+    T vx[PB], vxp[PB], vy[PB], vz[PB], vzp[PB], c0[PB], c1[PB], sy[PB];
+    auto load = [&](int b, int j) {
+      const long long idx = col + (long long)j * nx;
+      vx[b] = gx[idx]; vxp[b] = gx[idx + dxp]; vy[b] = gy[idx];
+      vz[b] = gz[idx]; vzp[b] = gz[idx + dzp];
+      c0[b] = __ldg(tab + (size_t)j * MT_W + MT_CP0);
+      c1[b] = __ldg(tab + (size_t)j * MT_W + MT_CP1);
+      sy[b] = m.rdyp[j + 1];
+    };
+#pragma unroll
+    for (int b = 0; b < PB; ++b) load(b, ny - 1 - b >= 0 ? ny - 1 - b : 0);
+    for (int jb = ny - 1; jb >= 0; jb -= PB) {
+#pragma unroll
+      for (int b = 0; b < PB; ++b) {
+        const int j = jb - b;
+        if (j < 0) break;
+        ax = vx[b] - c0[b] * ax;
+        axp = vxp[b] - c0[b] * axp;
+        ay = vy[b] - c1[b] * ay;
+        az = vz[b] - c0[b] * az;
+        azp = vzp[b] - c0[b] * azp;
+        const T r = (axp - ax) * rdx + (ayn - ay) * sy[b] + (azp - az) * rdz;
+        if (j >= PB) load(b, j - PB);
+        dv[col + (long long)j * nx] = r;
+        dmax = fmax(dmax, fabs((double)r));
+        ayn = ay;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dmax;
+  __syncthreads();
+  if (threadIdx.x == 0) atomic_max_nonneg(&sc->divmax1, fmax(fmax(red[0], red[1]), fmax(red[2], red[3])));
+}
+
+// FluidVelUpdate + PressureUpdate_PIMP (m_TScheme.f90:281-306, m_TSchemePIMP_inc.f90:
+// 852-873) from g, as k_proj_march in mode 0; DIAG: the step diagnostics of the
+// last substep (CheckDivergence, CalcVmax, CalcMaxCFL, CalcUxAver).  Partial sums
+// go to the slots of the chunked projection grid (npz row chunks), the unused
+// chunk slots of each block set to zero.
+template <class T, bool DIAG>
+__global__ void __launch_bounds__(128) k_proj_bsub(Geo<T> g, Metrics<T> m, const T* __restrict__ tab,
+                                                   const T* __restrict__ gx, const T* __restrict__ gy,
+                                                   const T* __restrict__ gz, T* __restrict__ ux, T* __restrict__ uy,
+                                                   T* __restrict__ uz, T* __restrict__ pr, const T* __restrict__ phi,
+                                                   double* __restrict__ part, double* __restrict__ part2, int npz,
+                                                   DevScalars* __restrict__ sc) {
+  __shared__ double red[7][4];
+  if (sc->status) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long plane = (long long)nx * ny;
+  tab += (size_t)(sc->ns - 1) * ny * MT_W;
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31), k = blockIdx.y * 4 + (threadIdx.x >> 5);
+  double s = 0.0, s2 = 0.0, dvm = 0.0, v0 = 0.0, v1 = 0.0, v2 = 0.0, cf = 0.0;
+  if (i < nx && k < nz) {
+    const long long col = i + plane * k;
+    const long long dxm = i == 0 ? nx - 1 : -1;                                // offset to i-1
+    const long long dzm = k == 0 ? (long long)(nz - 1) * plane : -plane;       // offset to k-1
+    const long long dxp = i + 1 == nx ? 1 - nx : 1;                            // offset to i+1
+    const long long dzp = k + 1 == nz ? -(long long)(nz - 1) * plane : plane;  // offset to k+1
+    const T pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
+    const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha;
+    const double rdx = g.rdx, rdz = g.rdz;
+    T ax = (T)0, ay = (T)0, az = (T)0, axp = (T)0, azp = (T)0;  // u* of row j+1
+    T pc = __ldg(phi + col + (long long)(ny - 1) * nx);         // phi(j)
+    T pp = pc;                                                   // phi(j+1), clamped at the top row
+    T uyp = (T)g.bc.uy_hi;                                       // new uy at j+1 (DIAG)
+    // rows pass through PB register slots, each refilled with the row PB below once consumed
+    constexpr int PB = DIAG ? 2 : 4;
+    T vx[PB], vy[PB], vz[PB], vp[PB], vpm[PB], vpx[PB], vpz[PB], c0[PB], c1[PB];
+    T mr[PB], mp[PB], mc[PB], mm[PB], ms[PB];
+    T qx[PB], qz[PB], qpx[PB], qpz[PB], qrp[PB], qdy[PB];  // DIAG neighbours, metrics
+    auto load = [&](int b, int j) {
+      const long long idx = col + (long long)j * nx;
+      const int jm = j > 0 ? j - 1 : 0;
+      vx[b] = gx[idx]; vy[b] = gy[idx]; vz[b] = gz[idx]; vp[b] = pr[idx];
+      vpm[b] = __ldg(phi + col + (long long)jm * nx);
+      vpx[b] = __ldg(phi + idx + dxm);
+      vpz[b] = __ldg(phi + idx + dzm);
+      c0[b] = __ldg(tab + (size_t)j * MT_W + MT_CP0);
+      c1[b] = __ldg(tab + (size_t)j * MT_W + MT_CP1);
+      mr[b] = m.rdyc[j + 1]; mp[b] = m.ap2Pr[j + 1]; mc[b] = m.ac2Pr[j + 1]; mm[b] = m.am2Pr[j + 1];
+      ms[b] = m.s1coe[j + 1];
+      if (DIAG) {
+        qx[b] = gx[idx + dxp]; qpx[b] = __ldg(phi + idx + dxp);
+        qz[b] = gz[idx + dzp]; qpz[b] = __ldg(phi + idx + dzp);
+        qrp[b] = m.rdyp[j + 1]; qdy[b] = m.dyp[j + 1];
+      }
+    };
+#pragma unroll
+    for (int b = 0; b < PB; ++b) load(b, ny - 1 - b >= 0 ? ny - 1 - b : 0);
+    for (int jb = ny - 1; jb >= 0; jb -= PB) {
+#pragma unroll
+      for (int b = 0; b < PB; ++b) {
+        const int j = jb - b;
+        if (j < 0) break;
+        const long long idx = col + (long long)j * nx;
+        ax = vx[b] - c0[b] * ax;
+        ay = vy[b] - c1[b] * ay;
+        az = vz[b] - c0[b] * az;
+        const T pm = vpm[b];
+        const T sucacEta2 = mr[b] * pmAlpha;
+        const T uxn = ax - (pc - vpx[b]) * rdxEta2;
+        const T uyn = ay - (pc - pm) * sucacEta2;
+        const T uzn = az - (pc - vpz[b]) * rdzEta2;
+        ux[idx] = uxn; uy[idx] = uyn; uz[idx] = uzn;
+        const T pmBetap = -pmBeta * mp[b];
+        const T pmBetac = -pmBeta * mc[b] + (T)1;
+        const T pmBetam = -pmBeta * mm[b];
+        pr[idx] = vp[b] + pmBetap * pp + pmBetac * pc + pmBetam * pm;
+        s += (double)uxn * (double)ms[b];
+        if (DIAG) {
+          // the new velocity at i+1, k+1 and j+1, as the threads that own them compute it
+          axp = qx[b] - c0[b] * axp;
+          azp = qz[b] - c0[b] * azp;
+          const T uxp = axp - (qpx[b] - pc) * rdxEta2;
+          const T uzp = azp - (qpz[b] - pc) * rdzEta2;
+          const double a = uxn, bb = uyn, c = uzn, aip = uxp, bjp = uyp, ckp = uzp, rdyp = qrp[b];
+          double d = fabs((aip - a) * rdx + (bjp - bb) * rdyp + (ckp - c) * rdz);
+          if (!(d == d)) d = INFINITY;  // NaN folded into +inf: a NaN field trips the limits
+          dvm = fmax(dvm, d);
+          v0 = fmax(v0, a == a ? fabs(a) : INFINITY);
+          v1 = fmax(v1, bb == bb ? fabs(bb) : INFINITY);
+          v2 = fmax(v2, c == c ? fabs(c) : INFINITY);
+          cf = fmax(cf, fabs(a + aip) * rdx + fabs(bb + bjp) * rdyp + fabs(c + ckp) * rdz);
+          s2 += a * (double)qdy[b];
+          uyp = uyn;
+        }
+        pp = pc; pc = pm;
+        if (j >= PB) load(b, j - PB);
+      }
+    }
+  }
+  const int bid = blockIdx.x + gridDim.x * blockIdx.y, nb = gridDim.x * gridDim.y;
+  for (int z = 1 + threadIdx.x; z < npz; z += blockDim.x) {  // the chunk slots this grid leaves empty
+    part[bid + (long long)nb * z] = 0.0;
+    if (DIAG) part2[bid + (long long)nb * z] = 0.0;
+  }
+  if constexpr (!DIAG) {
+    const double bs = block_sum128(s, red[0]);
+    if (threadIdx.x == 0) part[bid] = bs;
+  } else {
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      dvm = fmax(dvm, __shfl_xor_sync(0xffffffffu, dvm, o));
+      v0 = fmax(v0, __shfl_xor_sync(0xffffffffu, v0, o));
+      v1 = fmax(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+      v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+      cf = fmax(cf, __shfl_xor_sync(0xffffffffu, cf, o));
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      red[0][w] = s; red[1][w] = s2; red[2][w] = cf; red[3][w] = dvm; red[4][w] = v0; red[5][w] = v1; red[6][w] = v2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double r[7];
+      for (int q = 0; q < 2; ++q) r[q] = (red[q][0] + red[q][1]) + (red[q][2] + red[q][3]);
+      for (int q = 2; q < 7; ++q) r[q] = fmax(fmax(red[q][0], red[q][1]), fmax(red[q][2], red[q][3]));
+      part[bid] = r[0];
+      part2[bid] = r[1];
+      atomic_max_nonneg(&sc->uddx, r[2] * 0.5);
+      atomic_max_nonneg(&sc->divmax2, r[3]);
+      atomic_max_nonneg(&sc->vmax[0], r[4]);
+      atomic_max_nonneg(&sc->vmax[1], r[5]);
+      atomic_max_nonneg(&sc->vmax[2], r[6]);
+    }
+  }
+}
+
 static dim3 march_proj_grid(const ch3d_ctx* c) { return dim3((c->nx + 31) / 32, (c->nz + 3) / 4, (c->ny + MJ - 1) / MJ); }
 int march_npart(const ch3d_ctx* c) {
   const dim3 g = march_proj_grid(c);
@@ -732,38 +942,99 @@ template <class T> static cudaError_t bulk_march_t(ch3d_ctx* c) {
 }
 cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float>(c) : bulk_march_t<double>(c); }
 
+template <class T> static cudaError_t div_bsub_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  const dim3 grid((c->nx + 31) / 32, (c->nz + 3) / 4);
+  k_div_bsub<T><<<grid, 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), (const T*)c->mtab, f[12], f[13], f[14],
+                                             f[10], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_div_bsub(ch3d_ctx* c) { return c->fp32 ? div_bsub_t<float>(c) : div_bsub_t<double>(c); }
+
+template <class T> static cudaError_t proj_bsub_t(ch3d_ctx* c, bool diag) {
+  T** f = (T**)c->f;
+  const dim3 grid((c->nx + 31) / 32, (c->nz + 3) / 4);
+  const int npz = (int)march_proj_grid(c).z;
+  if (diag)
+    k_proj_bsub<T, true><<<grid, 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), (const T*)c->mtab, f[12],
+                                                      f[13], f[14], f[0], f[1], f[2], f[3], f[10], c->part, c->part2,
+                                                      npz, c->sc);
+  else
+    k_proj_bsub<T, false><<<grid, 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), (const T*)c->mtab, f[12],
+                                                       f[13], f[14], f[0], f[1], f[2], f[3], f[10], c->part, c->part2,
+                                                       npz, c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_proj_bsub(ch3d_ctx* c, bool diag) {
+  return c->fp32 ? proj_bsub_t<float>(c, diag) : proj_bsub_t<double>(c, diag);
+}
+
+// The march runs twisted when all column tiles fit on the GPU at once as
+// two-group blocks.
+template <class T, bool O4> struct MarchShape {
+  static constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
+  static constexpr int BPS = sizeof(T) == 8 ? 4 : 5;  // resident blocks per SM of the 2nd-order kernel
+  static constexpr int H = O4 ? 3 : 1, PL = (32 + 2 * H) * (BZ + 2 * H);
+  static constexpr size_t smem = (size_t)4 * RS * PL * sizeof(T);
+};
+template <class T, bool O4> static bool march_twisted_t(const ch3d_ctx* c) {
+  typedef MarchShape<T, O4> S;
+  static int nsm = 0, occ_tw = 0;
+  if (!nsm) {
+    auto kern_tw = k_rhs_march<T, O4, true, true, S::BZ, S::D, S::RS>;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
+    cudaFuncSetAttribute(kern_tw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * S::smem));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tw, kern_tw, 64 * S::BZ, 2 * S::smem) != cudaSuccess)
+      occ_tw = 0;
+  }
+  const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + S::BZ - 1) / S::BZ);
+  return c->ny >= 2 && ntiles <= (long long)nsm * occ_tw;
+}
+bool march_twisted(const ch3d_ctx* c) {
+  if (c->cfg.order == 4) return c->fp32 ? march_twisted_t<float, true>(c) : march_twisted_t<double, true>(c);
+  return c->fp32 ? march_twisted_t<float, false>(c) : march_twisted_t<double, false>(c);
+}
+
 template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
-  constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
-  constexpr int BPS = sizeof(T) == 8 ? 4 : 5;  // resident blocks per SM of the 2nd-order kernel
-  constexpr int H = O4 ? 3 : 1, PL = (32 + 2 * H) * (BZ + 2 * H);
-  const size_t smem = (size_t)4 * RS * PL * sizeof(T);
+  typedef MarchShape<T, O4> S;
+  constexpr int BZ = S::BZ, D = S::D, RS = S::RS;
+  const size_t smem = S::smem;
   T** f = (T**)c->f;
   k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab,
                                              march_down_tables<T>(c->mtab, c->ny),
                                              march_beta_slots(c->mtab, c->ny), c->sc);
-  auto kern = k_rhs_march<T, O4, false, BZ, D, RS>;
-  auto kern_tw = k_rhs_march<T, O4, true, BZ, D, RS>;
-  static int nsm = 0, occ_tw = 0;
+  auto kern = k_rhs_march<T, O4, false, true, BZ, D, RS>;
+  auto kern_tw = k_rhs_march<T, O4, true, true, BZ, D, RS>;
+  const bool tw = march_twisted_t<T, O4>(c);  // also sets the twisted kernel's shared-memory limit
+  static int nsm = 0;
   if (!nsm) {
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(kern_tw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem));
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tw, kern_tw, 64 * BZ, 2 * smem) != cudaSuccess)
-      occ_tw = 0;
+    if constexpr (!O4)
+      cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, BZ, D, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
   }
   const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + BZ - 1) / BZ);
   auto args = [&](auto k, unsigned grid, int threads, size_t sm) {
     k<<<grid, threads, sm, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, march_down_tables<T>(c->mtab, c->ny), f[0],
                                         f[1], f[2], f[3], f[4], f[5], f[6], f[12], f[13], f[14], c->sc);
   };
-  if (c->ny >= 2 && ntiles <= (long long)nsm * occ_tw) {
+  if (tw) {
     // few column tiles: all fit at once as two-group (twisted) blocks, half the march length
     args(kern_tw, (unsigned)ntiles, 64 * BZ, 2 * smem);
   } else {
-    // 2nd order: persistent blocks (back substitution overlapped with the next tile's march);
-    // 4th order: one tile per block
-    const long long cap = !O4 ? (long long)nsm * BPS : ntiles;
-    args(kern, (unsigned)(ntiles < cap ? ntiles : cap), 32 * BZ, smem);
+    // 2nd order: persistent blocks (back substitution, if any, overlapped with the next
+    // tile's march); 4th order: one tile per block
+    const long long cap = !O4 ? (long long)nsm * S::BPS : ntiles;
+    const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
+    bool done = false;
+    if constexpr (!O4) {
+      if (c->gsub) {  // stops at g: the divergence and projection marches substitute
+        args(k_rhs_march<T, O4, false, false, BZ, D, RS>, grid, 32 * BZ, smem);
+        done = true;
+      }
+    }
+    if (!done) args(kern, grid, 32 * BZ, smem);
   }
   return cudaGetLastError();
 }

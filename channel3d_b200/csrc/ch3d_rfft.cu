@@ -44,7 +44,8 @@ __global__ void __launch_bounds__(32 * kXWarps, sizeof(T) == 4 ? 6 : 4) k_prsrc_
   const int t = lane % P, slot = warp * LPW + lane / P;
   CT* L = sm[slot];
   const int nlines = ny * nz;
-  const T sudtal = mode == 0 ? (T)(1.0 / sc->pmAlpha) : (T)1;
+  // mode 3: the divergence of u* already formed (k_div_bsub) in the first array
+  const T sudtal = mode == 0 || mode == 3 ? (T)(1.0 / sc->pmAlpha) : (T)1;
   const T rdx = g.rdx, rdz = g.rdz;
   double dmax = 0.0;
   // warp groups of LPW lines, grid-stride; every thread of a warp runs the same iterations
@@ -65,8 +66,10 @@ __global__ void __launch_bounds__(32 * kXWarps, sizeof(T) == 4 ? 6 : 4) k_prsrc_
         const int n = t + P * q;
         const int i0 = 2 * n, i2 = i0 + 2 == nx ? 0 : i0 + 2;
         T r0, r1;
-        if (mode == 2) {  // standalone Poisson: the source is in the first array
-          r0 = __ldg(ux + base + i0); r1 = __ldg(ux + base + i0 + 1);
+        if (mode == 2 || mode == 3) {  // the source (or divergence) is in the first array
+          typedef typename CplxOf<T>::type T2;  // (i0, i0+1) as one aligned vector load
+          const T2 s01 = __ldg(reinterpret_cast<const T2*>(ux + base + i0));
+          r0 = s01.x; r1 = s01.y;
         } else if (g.order == 4) {
           const C4<T> c4(g);
           r0 = div4_cell(g, c4, sucaj, ux, uy, uz, i0, j, k);
@@ -117,6 +120,7 @@ __global__ void __launch_bounds__(32 * kXWarps, sizeof(T) == 4 ? 6 : 4) k_prsrc_
     }
     __syncwarp();
   }
+  if (mode == 3) return;  // its maximum was taken where the divergence was formed
   for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
   if (lane == 0) wred[warp] = dmax;
   __syncthreads();
@@ -174,9 +178,9 @@ __global__ void __launch_bounds__(32 * kXWarps, 4) k_xifft_r(Geo<T> g, const typ
 }
 
 template <class T, class PL, int LZ>
-__global__ void __launch_bounds__(LZ * PL::P, sizeof(T) == 8 ? 2 : 1) k_zfft_r(Geo<T> g, typename CplxOf<T>::type* __restrict__ spec,
-                                                       const typename CplxOf<T>::type* __restrict__ tw, int inverse,
-                                                       const DevScalars* __restrict__ sc) {
+__device__ __forceinline__ void zfft_r_body(Geo<T> g, typename CplxOf<T>::type* __restrict__ spec,
+                                            const typename CplxOf<T>::type* __restrict__ tw, int inverse,
+                                            const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
   constexpr int P = PL::P, E = PL::E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -199,6 +203,21 @@ __global__ void __launch_bounds__(LZ * PL::P, sizeof(T) == 8 ? 2 : 1) k_zfft_r(G
 #pragma unroll
     for (int q = 0; q < E; ++q) col[zs * (t + P * q)] = inverse ? cconj(v[q]) : v[q];
   }
+}
+// FP64 held to two blocks per SM (80 registers); FP32 left to the compiler's own
+// register choice (76 at 576 points, two blocks per SM; a minimum of one block
+// raised it to 94 and cost 15%)
+template <class T, class PL, int LZ>
+__global__ void __launch_bounds__(LZ * PL::P, 2) k_zfft_r(Geo<T> g, typename CplxOf<T>::type* __restrict__ spec,
+                                                          const typename CplxOf<T>::type* __restrict__ tw,
+                                                          int inverse, const DevScalars* __restrict__ sc) {
+  zfft_r_body<T, PL, LZ>(g, spec, tw, inverse, sc);
+}
+template <class T, class PL, int LZ>
+__global__ void __launch_bounds__(LZ * PL::P) k_zfft_rf(Geo<T> g, typename CplxOf<T>::type* __restrict__ spec,
+                                                        const typename CplxOf<T>::type* __restrict__ tw, int inverse,
+                                                        const DevScalars* __restrict__ sc) {
+  zfft_r_body<T, PL, LZ>(g, spec, tw, inverse, sc);
 }
 
 // ---------------------------------------------------------------------------
@@ -223,6 +242,10 @@ template <class F> static bool with_zplan(int nz, F f) {
   }
 }
 
+bool xplan_exists(int m) {
+  return with_xplan(m, [](auto) {});
+}
+
 static int x_grid(const ch3d_ctx* c, int lpw) {
   const long long groups = ((long long)c->ny * c->nz + lpw - 1) / lpw;
   const long long blocks = (groups + kXWarps - 1) / kXWarps;
@@ -233,7 +256,7 @@ static int x_grid(const ch3d_ctx* c, int lpw) {
 template <class T> static bool prsrc_r_t(ch3d_ctx* c, int mode, cudaError_t* err) {
   typedef typename CplxOf<T>::type CT;
   T** f = (T**)c->f;
-  T* a = mode == 2 ? f[10] : (mode == 1 ? f[0] : f[12]);
+  T* a = mode >= 2 ? f[10] : (mode == 1 ? f[0] : f[12]);
   T* b = mode == 1 ? f[1] : f[13];
   T* cz = mode == 1 ? f[2] : f[14];
   return with_xplan(c->nx / 2, [&](auto plan) {
@@ -262,13 +285,14 @@ bool launch_xifft_r(ch3d_ctx* c, cudaError_t* err) { return c->fp32 ? xifft_r_t<
 
 template <class T> static bool zfft_r_t(ch3d_ctx* c, int inverse, cudaError_t* err) {
   typedef typename CplxOf<T>::type CT;
-  // kx lines per block: 128-byte FP64 (64-byte FP32) segments per kz; FP64 held to two
-  // blocks per SM (80 registers).  Measured at 768x384x576: 4 lines 2.79 ms per spectral
-  // group, 8 lines 2.57, 16 lines 2.91
+  // kx lines per block: 128-byte FP64 (64-byte FP32) segments per kz.  Measured at
+  // 768x384x576 FP64: 4 lines 2.79 ms per spectral group, 8 lines 2.57, 16 lines 2.91
   constexpr int LZ = 8;
   return with_zplan(c->nz, [&](auto plan) {
     typedef decltype(plan) PL;
-    auto kern = k_zfft_r<T, PL, LZ>;
+    void (*kern)(Geo<T>, CT*, const CT*, int, const DevScalars*);
+    if constexpr (sizeof(T) == 8) kern = k_zfft_r<T, PL, LZ>;
+    else kern = k_zfft_rf<T, PL, LZ>;
     const size_t smem = (size_t)PL::N * LZ * sizeof(CT);
     static bool attr = false;
     if (!attr) {

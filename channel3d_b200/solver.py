@@ -147,3 +147,10 @@ class ChannelSolver:
         v = ctypes.c_double()
         _lib.check(self.lib.ch3d_last_step_ms(self.ctx, ctypes.byref(v)), self.lib)
         return v.value
+
+    def path_flags(self):
+        """Kernel layout of the step: a set of "march", "twisted", "gsub"
+        (CH3D_PATH_* of include/ch3d.h)."""
+        v = ctypes.c_int()
+        _lib.check(self.lib.ch3d_path_flags(self.ctx, ctypes.byref(v)), self.lib)
+        return {n for bit, n in ((1, "march"), (2, "twisted"), (4, "gsub")) if v.value & bit}

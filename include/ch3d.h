@@ -257,6 +257,14 @@ CH3D_API int ch3d_poisson_noalloc(int nxc, int nyc, int nzc, double xlx, double 
    context's stream (milliseconds). */
 CH3D_API int ch3d_last_step_ms(ch3d_ctx* ctx, double* ms);
 
+/* Kernel layout the context chose for its step (no counterpart in the
+   reference; for profiling and benchmark labels): *flags receives the OR of */
+#define CH3D_PATH_MARCH 1    /* RHS and y Helmholtz solves as one column march */
+#define CH3D_PATH_TWISTED 2  /* the march runs from both walls (few column tiles) */
+#define CH3D_PATH_GSUB 4     /* the march stops at the eliminated values g; the
+                                divergence and projection kernels substitute u* */
+CH3D_API int ch3d_path_flags(ch3d_ctx* ctx, int* flags);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,7 +8,10 @@ against the oracle within the 1e-10 relative bound:
   z, and the smallest ny the layout takes;
 - one tile per plain block (more tiles than twisted blocks fit on the GPU, fewer
   than the resident persistent blocks), with a ragged last z tile;
-- the 4th-order march both ways (128 column tiles twisted, 384 plain)."""
+- the 4th-order march both ways (128 column tiles twisted, 384 plain);
+- the march that stops at g on grids with more tiles than twisted blocks fit
+  (2nd order): the divergence and projection marches substitute u* from g
+  themselves, and the last projection carries the step diagnostics."""
 import numpy as np
 import pytest
 
@@ -69,3 +72,33 @@ def test_march_4th(built, shape):
     go, gs, di = _run(cfg, 3)
     _check(go, gs)
     assert di["divmax2"] < 1e-12
+
+
+def test_gsub_step_info(built):
+    """The diagnostics the last projection computes from g (divergence, velocity
+    maxima, CFL, bulk mean) and the divergence before it, against the oracle's
+    step, on a grid above the twisted threshold (8 x 41 = 328 tiles)."""
+    go, gs, di = _run(small_channel(256, 16, 162), 3)
+    _check(go, gs)
+    from oracle import oracle as O
+    from channel3d_b200 import initfield, mesh_y
+    cfg = small_channel(256, 16, 162)
+    yp = mesh_y(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp, seed=11)
+    p = 0.01 * np.random.default_rng(11).standard_normal(cfg.shape)
+    o = O.Oracle(cfg)
+    o.set_state(ux, uy, uz, p)
+    do = o.step(3)
+    for k in ("divmax1", "cflmp", "uxm", "PrGradAver"):
+        assert abs(di[k] - do[k]) <= 1e-9 * max(1.0, abs(do[k])), (k, di[k], do[k])
+    for q in range(3):
+        assert abs(di["vmax"][q] - do["vmax"][q]) <= 1e-10 * abs(do["vmax"][q]), (q, di["vmax"], do["vmax"])
+    assert di["divmax2"] < 1e-12
+
+
+def test_gsub_mixed(built):
+    """Mixed path with the march stopping at g (8 x 81 = 648 tiles)."""
+    go, gs, di = _run(small_channel(256, 24, 324, precision="mixed"), 3)
+    for k in ("ux", "uy", "uz"):
+        assert rel_l2(gs[k], go[k]) < 1e-4, (k, rel_l2(gs[k], go[k]))
+    assert di["divmax2"] < 1e-4

@@ -27,8 +27,10 @@ typedef RPlan<64, 16, 4, 4, 4> PlanN64;
 typedef RPlan<576, 48, 4, 4, 3, 12> PlanN576;
 typedef RPlan<128, 16, 8, 2, 8> PlanZ128;
 
-template <class T, class PL>
-__global__ void __launch_bounds__(32 * kXWarps, sizeof(T) == 4 ? 6 : 4) k_prsrc_xfft_r(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+// SRC: modes 2 and 3, the source (or divergence) already formed in the first
+// array; compiled separately so it is not held to the divergence modes' registers.
+template <class T, class PL, bool SRC>
+__global__ void __launch_bounds__(32 * kXWarps, SRC ? 6 : (sizeof(T) == 4 ? 6 : 4)) k_prsrc_xfft_r(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
                                                               const T* __restrict__ uy, const T* __restrict__ uz,
                                                               typename CplxOf<T>::type* __restrict__ spec,
                                                               const typename CplxOf<T>::type* __restrict__ tw,
@@ -66,7 +68,7 @@ __global__ void __launch_bounds__(32 * kXWarps, sizeof(T) == 4 ? 6 : 4) k_prsrc_
         const int n = t + P * q;
         const int i0 = 2 * n, i2 = i0 + 2 == nx ? 0 : i0 + 2;
         T r0, r1;
-        if (mode == 2 || mode == 3) {  // the source (or divergence) is in the first array
+        if constexpr (SRC) {  // the source (or divergence) is in the first array
           typedef typename CplxOf<T>::type T2;  // (i0, i0+1) as one aligned vector load
           const T2 s01 = __ldg(reinterpret_cast<const T2*>(ux + base + i0));
           r0 = s01.x; r1 = s01.y;
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(32 * kXWarps, sizeof(T) == 4 ? 6 : 4) k_prsrc_
           r0 = (u01.y - u01.x) * rdx + (v01p.x - v01.x) * sucaj + (w01p.x - w01.x) * rdz;
           r1 = (u2 - u01.y) * rdx + (v01p.y - v01.y) * sucaj + (w01p.y - w01.y) * rdz;
         }
-        if (mode == 0 && g.implicit == 2) {  // clcPrSrc_FIMP: pressure += -xnu/2 div (m_TScheme.f90:271)
+        if (!SRC && mode == 0 && g.implicit == 2) {  // clcPrSrc_FIMP: pressure += -xnu/2 div (m_TScheme.f90:271)
           const T xnuhm = -(T)0.5 * g.xnu;
           pr[base + i0] = pr[base + i0] + xnuhm * r0;
           pr[base + i0 + 1] = pr[base + i0 + 1] + xnuhm * r1;
@@ -261,9 +263,14 @@ template <class T> static bool prsrc_r_t(ch3d_ctx* c, int mode, cudaError_t* err
   T* cz = mode == 1 ? f[2] : f[14];
   return with_xplan(c->nx / 2, [&](auto plan) {
     typedef decltype(plan) PL;
-    k_prsrc_xfft_r<T, PL><<<x_grid(c, 32 / PL::P), 32 * kXWarps, 0, c->stream>>>(
-        make_geo<T>(c), metrics_of<T>(c), a, b, cz, (CT*)c->spec, (const CT*)c->twx, (const CT*)c->twr, mode, c->sc,
-        f[3]);
+    if (mode >= 2)
+      k_prsrc_xfft_r<T, PL, true><<<x_grid(c, 32 / PL::P), 32 * kXWarps, 0, c->stream>>>(
+          make_geo<T>(c), metrics_of<T>(c), a, b, cz, (CT*)c->spec, (const CT*)c->twx, (const CT*)c->twr, mode, c->sc,
+          f[3]);
+    else
+      k_prsrc_xfft_r<T, PL, false><<<x_grid(c, 32 / PL::P), 32 * kXWarps, 0, c->stream>>>(
+          make_geo<T>(c), metrics_of<T>(c), a, b, cz, (CT*)c->spec, (const CT*)c->twx, (const CT*)c->twr, mode, c->sc,
+          f[3]);
     *err = cudaGetLastError();
   });
 }

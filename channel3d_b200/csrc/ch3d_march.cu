@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(128) k_div_bsub(Geo<T> g, Metrics<T> m, const 
     T ayn = (T)g.bc.uy_hi;  // uy at j+1: the wall value above the top row
     // rows ny-1-b, ny-1-b-PB, ... pass through register slot b; a slot is refilled
     // with the row PB below as soon as it is consumed
-    constexpr int PB = 4;
+    constexpr int PB = 8;
     T vx[PB], vxp[PB], vy[PB], vz[PB], vzp[PB], c0[PB], c1[PB], sy[PB];
     auto load = [&](int b, int j) {
       const long long idx = col + (long long)j * nx;

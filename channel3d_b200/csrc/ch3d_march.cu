@@ -717,8 +717,10 @@ __global__ void __launch_bounds__(128) k_bulk_march(Geo<T> g, Metrics<T> m, cons
 
 // clcPrSrcOther (src/CFD_2nd/m_TScheme.f90:213-241): div(u*) per cell into dv
 // (scaled by 1/pmAlpha and transformed by the x kernel, mode 3), its maximum
-// |div| into divmax1 (CheckDivergence before the projection).
-template <class T>
+// |div| into divmax1 (CheckDivergence before the projection).  PB rows of loads
+// in flight: 8 (168 registers, three blocks per SM) where the grid runs many
+// waves anyway, 4 (100 registers) where the column blocks fit in one wave at five.
+template <class T, int PB>
 __global__ void __launch_bounds__(128) k_div_bsub(Geo<T> g, Metrics<T> m, const T* __restrict__ tab,
                                                   const T* __restrict__ gx, const T* __restrict__ gy,
                                                   const T* __restrict__ gz, T* __restrict__ dv,
@@ -739,7 +741,6 @@ __global__ void __launch_bounds__(128) k_div_bsub(Geo<T> g, Metrics<T> m, const 
     T ayn = (T)g.bc.uy_hi;  // uy at j+1: the wall value above the top row
     // rows ny-1-b, ny-1-b-PB, ... pass through register slot b; a slot is refilled
     // with the row PB below as soon as it is consumed
-    constexpr int PB = 8;
     T vx[PB], vxp[PB], vy[PB], vz[PB], vzp[PB], c0[PB], c1[PB], sy[PB];
     auto load = [&](int b, int j) {
       const long long idx = col + (long long)j * nx;
@@ -945,8 +946,16 @@ cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float
 template <class T> static cudaError_t div_bsub_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
   const dim3 grid((c->nx + 31) / 32, (c->nz + 3) / 4);
-  k_div_bsub<T><<<grid, 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), (const T*)c->mtab, f[12], f[13], f[14],
-                                             f[10], c->sc);
+  static int nsm = 0;
+  if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
+  // 256x192x256 (512 blocks): 74 us with 4 rows, 93 with 8; 768x384x576 (3456 blocks):
+  // 0.84 ms with 8 rows against 0.88 with 4
+  if ((long long)grid.x * grid.y > 6LL * nsm)
+    k_div_bsub<T, 8><<<grid, 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), (const T*)c->mtab, f[12], f[13],
+                                                   f[14], f[10], c->sc);
+  else
+    k_div_bsub<T, 4><<<grid, 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), (const T*)c->mtab, f[12], f[13],
+                                                   f[14], f[10], c->sc);
   return cudaGetLastError();
 }
 cudaError_t launch_div_bsub(ch3d_ctx* c) { return c->fp32 ? div_bsub_t<float>(c) : div_bsub_t<double>(c); }

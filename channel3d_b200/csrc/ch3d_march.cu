@@ -107,6 +107,12 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
   if (threadIdx.x == 0) beta_slot[q] = bits;
 }
 
+// Shared memory of one thread group of the march: RS row slots of the four
+// staged fields (PL points each) and of the row table (MT_W values).
+template <class T> constexpr size_t march_group_smem(int RS, int PL) {
+  return (size_t)4 * RS * PL * sizeof(T) + (size_t)RS * MT_W * sizeof(T);
+}
+
 // Ring of RS row slots (row r in slot (r + 1) % RS); rows j+2 .. j+D+1 are in
 // flight while row j is computed.  Slot (j+D+2), written after the barrier of
 // iteration j, must differ from the slots of rows j-1, j, j+1 that other
@@ -127,7 +133,9 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
 // is never stored and g is never read back here (6 arrays less traffic).
 template <class T, bool O4, bool TW, bool BS, int BZ, int D, int RS>
 __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
-                                  (sizeof(T) == 4 || O4 ? (O4 ? 384 : 640) : 512) / (32 * BZ * (TW ? 2 : 1)))
+                                  (!BS && sizeof(T) == 4 && !O4)  // FP32 march stopping at g: 80 registers
+                                      ? 6
+                                      : (sizeof(T) == 4 || O4 ? (O4 ? 384 : 640) : 512) / (32 * BZ * (TW ? 2 : 1)))
     k_rhs_march(Geo<T> g, const T* __restrict__ tab, const T* __restrict__ dtab, const T* __restrict__ ux, const T* __restrict__ uy,
                 const T* __restrict__ uz, const T* __restrict__ pr, T* __restrict__ hx, T* __restrict__ hy,
                 T* __restrict__ hz, T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
@@ -138,7 +146,10 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
   static_assert(RS >= D + 4, "ring too small for the prefetch distance");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int hf = TW ? (int)threadIdx.x / NT : 0;  // thread group: 0 lower (or the only one), 1 upper
-  T (*ring)[RS][PL] = reinterpret_cast<T (*)[RS][PL]>(smem_raw + (size_t)hf * 4 * RS * PL * sizeof(T));
+  // per thread group: the field rows [4][RS][PL], then the table rows [RS][MT_W]
+  unsigned char* const grp_smem = smem_raw + (size_t)hf * march_group_smem<T>(RS, PL);
+  T (*ring)[RS][PL] = reinterpret_cast<T (*)[RS][PL]>(grp_smem);
+  T (*trs)[MT_W] = reinterpret_cast<T (*)[MT_W]>(grp_smem + (size_t)4 * RS * PL * sizeof(T));
   if (sc->status) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long plane = (long long)nx * ny;
@@ -173,6 +184,10 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
         cp_async_el(&ring[3][sl][s], pr + so[q] + ro);
       }
     }
+    // the row's table entries (MT_W values, 16-byte copies) in the same copy group
+    constexpr int TV = MT_W * (int)sizeof(T) / 16;
+    if (tid < TV)
+      cp_async_el(reinterpret_cast<float4*>(&trs[sl][0]) + tid, reinterpret_cast<const float4*>(tab + (size_t)r * MT_W) + tid);
   };
   // wall ghost rows from the thread's own staged slots next to them (at_jm / at_jp of ch3d_dev.cuh)
   auto ghost_row = [&](int r) {
@@ -270,7 +285,7 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
     if (hread && sj + 2 < nrow) { hxn = hx[idx + 2 * hstep]; hyn = hy[idx + 2 * hstep]; hzn = hz[idx + 2 * hstep]; }
     if (act) {
       T rx, ry, rz, ux_c, uy_c, uz_c, ux_jp, uy_jp, uz_jp, ux_jm, uy_jm, uz_jm;
-      const T* tr = tab + (size_t)j * MT_W;
+      const T* tr = trs[slot(j)];  // row j of the table, staged with the row
       if constexpr (!O4) {
       const T* X0 = &ring[0][slot(j - 1)][c0];
       const T* X1 = &ring[0][slot(j)][c0];
@@ -292,16 +307,16 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
       const T uz_kp = Z1[SX], uz_km = Z1[-SX], uz_im_kp = Z1[SX - 1], uz_jm_kp = Z0[SX];
       const T p_c = P1[0], p_im = P1[-1], p_jm = P0[0], p_km = P1[-SX];
 
-      const T IY1 = __ldg(tr + MT_IY1), IY2 = one - IY1;
-      const T IY3 = __ldg(tr + MT_IY3), IY4 = one - IY3;
+      const T IY1 = tr[MT_IY1], IY2 = one - IY1;
+      const T IY3 = tr[MT_IY3], IY4 = one - IY3;
       {  // RhsX (clcRhsX_PIMP, m_TSchemePIMP_inc.f90:7-75)
         const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
-        const T sucaj = half * __ldg(tr + MT_RDYP);
+        const T sucaj = half * tr[MT_RDYP];
         T h11 = ((ux_ip + ux_c) * (ux_ip + ux_c) - (ux_c + ux_im) * (ux_c + ux_im)) * qdx1;
         T h12 = ((uy_jp + uy_im_jp) * (IY3 * ux_c + IY4 * ux_jp) - (uy_c + uy_im) * (IY1 * ux_jm + IY2 * ux_c)) * sucaj;
         T h13 = ((uz_kp + uz_im_kp) * (ux_kp + ux_c) - (uz_c + uz_im) * (ux_c + ux_km)) * qdx3;
         T d11q1 = (ux_ip - two * ux_c + ux_im) * rdx2;
-        T d22q1 = __ldg(tr + MT_AP2C) * ux_jp + __ldg(tr + MT_AC2C) * ux_c + __ldg(tr + MT_AM2C) * ux_jm;
+        T d22q1 = tr[MT_AP2C] * ux_jp + tr[MT_AC2C] * ux_c + tr[MT_AM2C] * ux_jm;
         T d33q1 = g.ap3c * ux_kp + g.ac3c * ux_c + g.am3c * ux_km;
         T dcq13 = d11q1 + d33q1;
         T gradp1 = (p_c - p_im) * rdx;
@@ -311,12 +326,12 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
       }
       {  // RhsY (clcRhsY_PIMP, :161-209)
         const T hdx1 = half * rdx, hdx3 = half * rdz;
-        const T sucac = __ldg(tr + MT_RDYC), qsucac = quarter * sucac;
+        const T sucac = tr[MT_RDYC], qsucac = quarter * sucac;
         T h21 = ((IY1 * ux_ip_jm + IY2 * ux_ip) * (uy_ip + uy_c) - (IY1 * ux_jm + IY2 * ux_c) * (uy_c + uy_im)) * hdx1;
         T h22 = ((uy_jp + uy_c) * (uy_jp + uy_c) - (uy_c + uy_jm) * (uy_c + uy_jm)) * qsucac;
         T h23 = ((IY1 * uz_jm_kp + IY2 * uz_kp) * (uy_kp + uy_c) - (IY1 * uz_jm + IY2 * uz_c) * (uy_c + uy_km)) * hdx3;
         T d11q2 = g.ap1c * uy_ip + g.ac1c * uy_c + g.am1c * uy_im;
-        T d22q2 = __ldg(tr + MT_AP2P) * uy_jp + __ldg(tr + MT_AC2P) * uy_c + __ldg(tr + MT_AM2P) * uy_jm;
+        T d22q2 = tr[MT_AP2P] * uy_jp + tr[MT_AC2P] * uy_c + tr[MT_AM2P] * uy_jm;
         T d33q2 = g.ap3c * uy_kp + g.ac3c * uy_c + g.am3c * uy_km;
         T dcq13 = d11q2 + d33q2;
         T gradp2 = (p_c - p_jm) * sucac;
@@ -326,12 +341,12 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
       }
       {  // RhsZ (clcRhsZ_PIMP, :277-325)
         const T qdx1 = quarter * rdx, qdx3 = quarter * rdz;
-        const T sucaj = half * __ldg(tr + MT_RDYP);
+        const T sucaj = half * tr[MT_RDYP];
         T h31 = ((ux_ip + ux_ip_km) * (uz_ip + uz_c) - (ux_c + ux_km) * (uz_c + uz_im)) * qdx1;
         T h32 = ((uy_jp + uy_jp_km) * (IY3 * uz_c + IY4 * uz_jp) - (uy_c + uy_km) * (IY1 * uz_jm + IY2 * uz_c)) * sucaj;
         T h33 = ((uz_kp + uz_c) * (uz_kp + uz_c) - (uz_c + uz_km) * (uz_c + uz_km)) * qdx3;
         T d11q3 = g.ap1c * uz_ip + g.ac1c * uz_c + g.am1c * uz_im;
-        T d22q3 = __ldg(tr + MT_AP2C) * uz_jp + __ldg(tr + MT_AC2C) * uz_c + __ldg(tr + MT_AM2C) * uz_jm;
+        T d22q3 = tr[MT_AP2C] * uz_jp + tr[MT_AC2C] * uz_c + tr[MT_AM2C] * uz_jm;
         T d33q3 = (uz_kp - two * uz_c + uz_km) * rdz2;
         T dcq13 = d11q3 + d33q3;
         T gradp3 = (p_c - p_km) * rdz;
@@ -358,9 +373,9 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
           return q.in1 * V(2, r, 0, o - 1) + q.in2 * V(2, r, 0, o) + q.in3 * V(2, r, 0, o + 1) + q.in4 * V(2, r, 0, o + 2);
         };
         const bool top = j + 1 == ny;  // uyhx, uyhz vanish on the jc = nyp row (:223-226)
-        const T IY1 = __ldg(tr + MT_IY1), IY2 = one - IY1;
-        const T IY3 = __ldg(tr + MT_IY3), IY4 = one - IY3;
-        const T sucaj = __ldg(tr + MT_RDYP);
+        const T IY1 = tr[MT_IY1], IY2 = one - IY1;
+        const T IY3 = tr[MT_IY3], IY4 = one - IY3;
+        const T sucaj = tr[MT_RDYP];
         ux_c = V(0, j, 0, 0); ux_jp = V(0, j + 1, 0, 0); ux_jm = V(0, j - 1, 0, 0);
         uy_c = V(1, j, 0, 0); uy_jp = V(1, j + 1, 0, 0); uy_jm = V(1, j - 1, 0, 0);
         uz_c = V(2, j, 0, 0); uz_jp = V(2, j + 1, 0, 0); uz_jm = V(2, j - 1, 0, 0);
@@ -374,7 +389,7 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
                         q.dz3 * hza(0, j, 0, 1) * hxa(2, j, 0, 1) + q.dz4 * hza(0, j, 0, 2) * hxa(2, j, 0, 2);
           const T d11 = q.dxx1 * V(0, j, -2, 0) + q.dxx2 * V(0, j, -1, 0) + q.dxx3 * ux_c + q.dxx4 * V(0, j, 1, 0) +
                         q.dxx5 * V(0, j, 2, 0);
-          const T d22 = __ldg(tr + MT_AP2C) * ux_jp + __ldg(tr + MT_AC2C) * ux_c + __ldg(tr + MT_AM2C) * ux_jm;
+          const T d22 = tr[MT_AP2C] * ux_jp + tr[MT_AC2C] * ux_c + tr[MT_AM2C] * ux_jm;
           const T d33 = q.dzz1 * V(0, j, 0, -2) + q.dzz2 * V(0, j, 0, -1) + q.dzz3 * ux_c + q.dzz4 * V(0, j, 0, 1) +
                         q.dzz5 * V(0, j, 0, 2);
           const T conv = -h11 - h12 - h13 + xnu * (d11 + d33) + g.g1;
@@ -383,7 +398,7 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
           hx[idx] = conv;
         }
         {  // RhsY (:270-305)
-          const T sucac = __ldg(tr + MT_RDYC), qsucac = quarter * sucac;
+          const T sucac = tr[MT_RDYC], qsucac = quarter * sucac;
           const T uxhym = IY1 * V(0, j - 1, -1, 0) + IY2 * V(0, j, -1, 0);
           const T uxhyc = IY1 * V(0, j - 1, 0, 0) + IY2 * V(0, j, 0, 0);
           const T uxhyp = IY1 * V(0, j - 1, 1, 0) + IY2 * V(0, j, 1, 0);
@@ -399,7 +414,7 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
                         q.dz3 * hza(1, j, 0, 1) * uzhyp + q.dz4 * hza(1, j, 0, 2) * uzhyu;
           const T d11 = q.dxx1 * V(1, j, -2, 0) + q.dxx2 * V(1, j, -1, 0) + q.dxx3 * uy_c + q.dxx4 * V(1, j, 1, 0) +
                         q.dxx5 * V(1, j, 2, 0);
-          const T d22 = __ldg(tr + MT_AP2P) * uy_jp + __ldg(tr + MT_AC2P) * uy_c + __ldg(tr + MT_AM2P) * uy_jm;
+          const T d22 = tr[MT_AP2P] * uy_jp + tr[MT_AC2P] * uy_c + tr[MT_AM2P] * uy_jm;
           const T d33 = q.dzz1 * V(1, j, 0, -2) + q.dzz2 * V(1, j, 0, -1) + q.dzz3 * uy_c + q.dzz4 * V(1, j, 0, 1) +
                         q.dzz5 * V(1, j, 0, 2);
           const T conv = -h21 - h22 - h23 + xnu * (d11 + d33) + g.g2;
@@ -417,7 +432,7 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
           const T h33 = q.dz1 * b1 * b1 + q.dz2 * b2 * b2 + q.dz3 * b3 * b3 + q.dz4 * b4 * b4;
           const T d11 = q.dxx1 * V(2, j, -2, 0) + q.dxx2 * V(2, j, -1, 0) + q.dxx3 * uz_c + q.dxx4 * V(2, j, 1, 0) +
                         q.dxx5 * V(2, j, 2, 0);
-          const T d22 = __ldg(tr + MT_AP2C) * uz_jp + __ldg(tr + MT_AC2C) * uz_c + __ldg(tr + MT_AM2C) * uz_jm;
+          const T d22 = tr[MT_AP2C] * uz_jp + tr[MT_AC2C] * uz_c + tr[MT_AM2C] * uz_jm;
           const T d33 = q.dzz1 * V(2, j, 0, -2) + q.dzz2 * V(2, j, 0, -1) + q.dzz3 * uz_c + q.dzz4 * V(2, j, 0, 1) +
                         q.dzz5 * V(2, j, 0, 2);
           const T conv = -h31 - h32 - h33 + xnu * (d11 + d33) + g.g3;
@@ -429,12 +444,12 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
       rx += dpm;                     // mean pressure gradient (clcRhsX_PIMP :61-74)
       if (j == 0) ry = (T)0;         // duy_ym: uy_ym is constant (Update_uy_ym_CH)
       if (!TW || hf == 0) {  // upward elimination; g = u + d + cp u_{j+1}
-        d0 = (rx - __ldg(tr + MT_A0) * d0) * __ldg(tr + MT_RM0);
-        d1 = (ry - __ldg(tr + MT_A1) * d1) * __ldg(tr + MT_RM1);
-        d2 = (rz - __ldg(tr + MT_A0) * d2) * __ldg(tr + MT_RM0);
-        g0 = ux_c + d0 + __ldg(tr + MT_CP0) * ux_jp;
-        g1 = uy_c + d1 + __ldg(tr + MT_CP1) * uy_jp;
-        g2 = uz_c + d2 + __ldg(tr + MT_CP0) * uz_jp;
+        d0 = (rx - tr[MT_A0] * d0) * tr[MT_RM0];
+        d1 = (ry - tr[MT_A1] * d1) * tr[MT_RM1];
+        d2 = (rz - tr[MT_A0] * d2) * tr[MT_RM0];
+        g0 = ux_c + d0 + tr[MT_CP0] * ux_jp;
+        g1 = uy_c + d1 + tr[MT_CP1] * uy_jp;
+        g2 = uz_c + d2 + tr[MT_CP0] * uz_jp;
       } else {               // downward elimination; g = u + e + aq u_{j-1}
         const T* td = dtab + (size_t)j * MD_W;
         d0 = (rx - __ldg(td + MD_C0) * d0) * __ldg(td + MD_RQ0);
@@ -982,9 +997,10 @@ cudaError_t launch_proj_bsub(ch3d_ctx* c, bool diag) {
 // two-group blocks.
 template <class T, bool O4> struct MarchShape {
   static constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
-  static constexpr int BPS = sizeof(T) == 8 ? 4 : 5;  // resident blocks per SM of the 2nd-order kernel
+  // resident blocks per SM of the 2nd-order kernel (FP32: 6 when it stops at g, 5 otherwise)
+  static constexpr int bps(bool stops_at_g) { return sizeof(T) == 8 ? 4 : (stops_at_g ? 6 : 5); }
   static constexpr int H = O4 ? 3 : 1, PL = (32 + 2 * H) * (BZ + 2 * H);
-  static constexpr size_t smem = (size_t)4 * RS * PL * sizeof(T);
+  static constexpr size_t smem = march_group_smem<T>(RS, PL);
 };
 template <class T, bool O4> static bool march_twisted_t(const ch3d_ctx* c) {
   typedef MarchShape<T, O4> S;
@@ -1034,7 +1050,7 @@ template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   } else {
     // 2nd order: persistent blocks (back substitution, if any, overlapped with the next
     // tile's march); 4th order: one tile per block
-    const long long cap = !O4 ? (long long)nsm * S::BPS : ntiles;
+    const long long cap = !O4 ? (long long)nsm * S::bps(c->gsub) : ntiles;
     const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
     bool done = false;
     if constexpr (!O4) {

@@ -733,10 +733,13 @@ template <> struct Vec2Of<float> { typedef float2 type; };
 // array, layout [j][low column]), the backward sweep overwrites it with the
 // solution.  Rows are processed in batches of YB: the batch's loads are all
 // issued before its dependent recurrence, so YB rows of every column are in
-// flight at once.
-constexpr int YB = 8;
+// flight at once.  YB is 16 in the FP64 kernel and 8 in the mixed one (whose
+// FP64 low-mode sweeps share the FP32 sweeps' register budget); at 768x384x576
+// the spectral group takes 2.51 ms FP64 with 16 rows against 2.61 with 8, mixed
+// 1.65 with 8 against 1.73 with 16; refilling each row's slot as soon as it is
+// consumed instead of whole batches was slower in both.
 
-template <class R, class CT, class LD, class ST, class STD, class LDD>
+template <class R, class CT, int YB, class LD, class ST, class STD, class LDD>
 __device__ __forceinline__ void thomas_column(int ny, bool pin, const R* __restrict__ rm, const R* __restrict__ cp,
                                               size_t fst, const double* __restrict__ am, LD load, ST store,
                                               STD store_d, LDD load_d) {
@@ -810,7 +813,7 @@ __global__ void __launch_bounds__(128) k_ythomas(Geo<T> g, Metrics<double> m, co
   const R* cp = CPf + (size_t)kzh * ny * st + kx;
   auto load = [&](int j) { return col[st * j]; };
   auto store = [&](int j, R x, R y) { col[st * j] = mk((T)x, (T)y); };
-  thomas_column<R, CT>(ny, kx == 0 && kz == 0, rm, cp, st, m.am2Pr, load, store, store, load);
+  thomas_column<R, CT, 16>(ny, kx == 0 && kz == 0, rm, cp, st, m.am2Pr, load, store, store, load);
 }
 
 // Mixed path: FP32 sweeps with FP32 factors, except the low modes kx < KX,
@@ -841,13 +844,13 @@ __global__ void __launch_bounds__(128) k_ythomas_mixed(Geo<T> g, Metrics<double>
     auto store = [&](int j, double x, double y) { col[st * j] = mk((T)x, (T)y); };
     auto store_d = [&](int j, double x, double y) { w[nlow * j] = make_double2(x, y); };
     auto load_d = [&](int j) { return w[nlow * j]; };
-    thomas_column<double, double2>(ny, pin, RM64 + (size_t)kzh * ny * KX + kx, CP64 + (size_t)kzh * ny * KX + kx,
+    thomas_column<double, double2, 8>(ny, pin, RM64 + (size_t)kzh * ny * KX + kx, CP64 + (size_t)kzh * ny * KX + kx,
                                    (size_t)KX, m.am2Pr, [&](int j) { const CT v = load(j); return make_double2(v.x, v.y); },
                                    store, store_d, load_d);
     return;
   }
   auto store = [&](int j, float x, float y) { col[st * j] = mk((T)x, (T)y); };
-  thomas_column<float, CT>(ny, pin, RM32 + (size_t)kzh * ny * st + kx, CP32 + (size_t)kzh * ny * st + kx, st, m.am2Pr,
+  thomas_column<float, CT, 8>(ny, pin, RM32 + (size_t)kzh * ny * st + kx, CP32 + (size_t)kzh * ny * st + kx, st, m.am2Pr,
                            load, store, store, load);
 }
 

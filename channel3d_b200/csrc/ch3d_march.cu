@@ -4,19 +4,22 @@
 // followed by clcU1/2/3Hat_PIMP (:392-430, 542-589, 702-740), u -> u*.
 //
 // One thread owns one (i, k) column and all three velocity components.  A
-// block of 32 x BZ columns marches j upwards through a ring of four staged
-// rows in shared memory (ux, uy, uz, p of the block's columns plus a one-cell
-// halo in x and z; rows -1 and ny are the wall ghosts of SetBC_and_UpdateHalo,
-// src/CFD_2nd/m_BC_and_Halo.f90:241-282).  At row j the thread evaluates the
-// three right-hand sides from rows j-1, j, j+1 of the ring, updates Hist, and
-// eliminates row j of the three tridiagonal systems (Thomas; the factors are
-// the same for every column and come from a per-row table).  Instead of the
-// eliminated right-hand side d_j it stores
+// block of 32 x BZ columns marches j upwards through a ring of staged rows in
+// shared memory (ux, uy, uz, p of the block's columns plus a one-cell halo in
+// x and z, and the row's table entries; rows -1 and ny are the wall ghosts of
+// SetBC_and_UpdateHalo, src/CFD_2nd/m_BC_and_Halo.f90:241-282).  At row j the
+// thread evaluates the three right-hand sides from rows j-1, j, j+1 of the
+// ring, updates Hist, and eliminates row j of the three tridiagonal systems
+// (Thomas; the factors are the same for every column and come from a per-row
+// table).  Instead of the eliminated right-hand side d_j it stores
 //     g_j = u_j + d_j + cp_j u_{j+1}
 // in the u* array; the back substitution x_j = d_j - cp_j x_{j+1} of
 // u*_j = u_j + x_j then reads only g:  u*_j = g_j - cp_j u*_{j+1}.
-// Global traffic per cell: ux uy uz p, Hist x3 read + written, g x3 written
-// and read back, u* x3 written (19 values).
+// On grids with few column tiles the march runs from both walls (twisted); on
+// large grids it stops at g and the divergence and projection marches of this
+// file substitute u* themselves (13 values of global traffic per cell: ux uy
+// uz p, Hist x3 read + written, g x3 written).  Where the march substitutes
+// itself, g is read back and u* written as well (19 values).
 #include "ch3d_ctx.h"
 #include "ch3d_dev.cuh"
 

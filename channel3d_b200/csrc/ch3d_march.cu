@@ -110,6 +110,11 @@ __global__ void k_march_table(HelmCoef hc, Metrics<T> m, int ny, T* __restrict__
   if (threadIdx.x == 0) beta_slot[q] = bits;
 }
 
+// Staging geometry: x halo H rounded up to whole copy vectors of VW points, and
+// points per staged row of a 32 x BZ tile.
+constexpr int march_hx(int H, int VW) { return (H + VW - 1) / VW * VW; }
+constexpr int march_pl(int H, int VW, int BZ) { return (32 + 2 * march_hx(H, VW)) * (BZ + 2 * H); }
+
 // Shared memory of one thread group of the march: RS row slots of the four
 // staged fields (PL points each) and of the row table (MT_W values).
 template <class T> constexpr size_t march_group_smem(int RS, int PL) {
@@ -134,7 +139,10 @@ template <class T> constexpr size_t march_group_smem(int RS, int PL) {
 // BS = false: the march stops at g; k_div_bsub and k_proj_bsub substitute
 // u* = g - cp u*_{j+1} themselves while they walk each column downwards, so u*
 // is never stored and g is never read back here (6 arrays less traffic).
-template <class T, bool O4, bool TW, bool BS, int BZ, int D, int RS>
+//
+// VW: rows staged in copy vectors of VW elements (4: 16-byte copies of FP32
+// rows, the x halo rounded up to 4 points; needs nx % 4 == 0), 1: element-wise.
+template <class T, bool O4, bool TW, bool BS, int VW, int BZ, int D, int RS>
 __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
                                   (!BS && sizeof(T) == 4 && !O4)  // FP32 march stopping at g: 80 registers
                                       ? 6
@@ -144,8 +152,11 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
                 T* __restrict__ hz, T* __restrict__ uxs, T* __restrict__ uys, T* __restrict__ uzs,
                 const DevScalars* __restrict__ sc) {
   constexpr int H = O4 ? 3 : 1;  // x/z halo
-  constexpr int BX = 32, NT = BX * BZ, SX = BX + 2 * H, PL = SX * (BZ + 2 * H);
-  constexpr int NS = (PL + NT - 1) / NT;  // staging slots per thread and array
+  constexpr int HX = march_hx(H, VW);  // staged x halo
+  constexpr int BX = 32, NT = BX * BZ, SX = BX + 2 * HX, PL = march_pl(H, VW, BZ);
+  constexpr int NS = (PL / VW + NT - 1) / NT;  // staging vectors per thread and array
+  static_assert(VW == 1 || (VW == 4 && sizeof(T) == 4), "16-byte vectors of FP32 rows only");
+  typedef typename std::conditional<VW == 4, float4, T>::type VT;
   static_assert(RS >= D + 4, "ring too small for the prefetch distance");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int hf = TW ? (int)threadIdx.x / NT : 0;  // thread group: 0 lower (or the only one), 1 upper
@@ -179,12 +190,12 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
     const int sl = slot(r);
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
-      const int s = tid + q * NT;
+      const int s = (tid + q * NT) * VW;
       if (s < PL) {
-        cp_async_el(&ring[0][sl][s], ux + so[q] + ro);
-        cp_async_el(&ring[1][sl][s], uy + so[q] + ro);
-        cp_async_el(&ring[2][sl][s], uz + so[q] + ro);
-        cp_async_el(&ring[3][sl][s], pr + so[q] + ro);
+        cp_async_el(reinterpret_cast<VT*>(&ring[0][sl][s]), reinterpret_cast<const VT*>(ux + so[q] + ro));
+        cp_async_el(reinterpret_cast<VT*>(&ring[1][sl][s]), reinterpret_cast<const VT*>(uy + so[q] + ro));
+        cp_async_el(reinterpret_cast<VT*>(&ring[2][sl][s]), reinterpret_cast<const VT*>(uz + so[q] + ro));
+        cp_async_el(reinterpret_cast<VT*>(&ring[3][sl][s]), reinterpret_cast<const VT*>(pr + so[q] + ro));
       }
     }
     // the row's table entries (MT_W values, 16-byte copies) in the same copy group
@@ -196,8 +207,8 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
   auto ghost_row = [&](int r) {
     const int sl = slot(r);
 #pragma unroll
-    for (int q = 0; q < NS; ++q) {
-      const int s = tid + q * NT;
+    for (int qv = 0; qv < NS * VW; ++qv) {  // the elements of this thread's staging vectors
+      const int s = (tid + (qv / VW) * NT) * VW + qv % VW;
       if (s >= PL) continue;
       if (r < 0) {
         const T u = ring[0][slot(0)][s], w = ring[2][slot(0)][s], v1 = ring[1][slot(1)][s];
@@ -221,7 +232,7 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
   const T rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2, xnu = g.xnu;
   const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
   const T dpm = (T)sc->dpmdxns;
-  const int c0 = (tz + H) * SX + tx + H;
+  const int c0 = (tz + H) * SX + tx + HX;
   const int ntx = (nx + BX - 1) / BX, ntiles = ntx * ((nz + BZ - 1) / BZ);
 
   // Persistent blocks walk tiles of 32 x BZ columns.  The back substitution of
@@ -237,8 +248,8 @@ __global__ void __launch_bounds__(32 * BZ * (TW ? 2 : 1),
   // staging slots: s = tid + q NT -> halo-tile position (s % SX, s / SX), periodic in x and z
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
-    const int s = tid + q * NT;
-    int ig = (i0 - H + s % SX) % nx, kg = (k0 - H + s / SX) % nz;
+    const int s = (tid + q * NT) * VW;  // a vector never wraps: nx and i0 - HX are multiples of VW
+    int ig = (i0 - HX + s % SX) % nx, kg = (k0 - H + s / SX) % nz;
     if (ig < 0) ig += nx;
     if (kg < 0) kg += nz;
     so[q] = s < PL ? ig + plane * kg : 0;
@@ -1002,14 +1013,16 @@ template <class T, bool O4> struct MarchShape {
   static constexpr int BZ = 4, D = sizeof(T) == 8 ? 2 : 4, RS = D + 4;
   // resident blocks per SM of the 2nd-order kernel (FP32: 6 when it stops at g, 5 otherwise)
   static constexpr int bps(bool stops_at_g) { return sizeof(T) == 8 ? 4 : (stops_at_g ? 6 : 5); }
-  static constexpr int H = O4 ? 3 : 1, PL = (32 + 2 * H) * (BZ + 2 * H);
+  static constexpr int H = O4 ? 3 : 1, PL = march_pl(H, 1, BZ);
   static constexpr size_t smem = march_group_smem<T>(RS, PL);
+  // FP32 march that stops at g, staged in 16-byte vectors
+  static constexpr size_t smem_v4 = march_group_smem<T>(RS, march_pl(H, 4, BZ));
 };
 template <class T, bool O4> static bool march_twisted_t(const ch3d_ctx* c) {
   typedef MarchShape<T, O4> S;
   static int nsm = 0, occ_tw = 0;
   if (!nsm) {
-    auto kern_tw = k_rhs_march<T, O4, true, true, S::BZ, S::D, S::RS>;
+    auto kern_tw = k_rhs_march<T, O4, true, true, 1, S::BZ, S::D, S::RS>;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
     cudaFuncSetAttribute(kern_tw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * S::smem));
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tw, kern_tw, 64 * S::BZ, 2 * S::smem) != cudaSuccess)
@@ -1031,16 +1044,20 @@ template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   k_march_table<T><<<1, 128, 0, c->stream>>>(helm_coef(c), metrics_of<T>(c), c->ny, (T*)c->mtab,
                                              march_down_tables<T>(c->mtab, c->ny),
                                              march_beta_slots(c->mtab, c->ny), c->sc);
-  auto kern = k_rhs_march<T, O4, false, true, BZ, D, RS>;
-  auto kern_tw = k_rhs_march<T, O4, true, true, BZ, D, RS>;
+  auto kern = k_rhs_march<T, O4, false, true, 1, BZ, D, RS>;
+  auto kern_tw = k_rhs_march<T, O4, true, true, 1, BZ, D, RS>;
   const bool tw = march_twisted_t<T, O4>(c);  // also sets the twisted kernel's shared-memory limit
   static int nsm = 0;
   if (!nsm) {
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if constexpr (!O4)
-      cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, BZ, D, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if constexpr (!O4) {
+      cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, 1, BZ, D, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
+      if constexpr (sizeof(T) == 4)
+        cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, 4, BZ, D, RS>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_v4);
+    }
   }
   const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + BZ - 1) / BZ);
   auto args = [&](auto k, unsigned grid, int threads, size_t sm) {
@@ -1058,7 +1075,14 @@ template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
     bool done = false;
     if constexpr (!O4) {
       if (c->gsub) {  // stops at g: the divergence and projection marches substitute
-        args(k_rhs_march<T, O4, false, false, BZ, D, RS>, grid, 32 * BZ, smem);
+        bool v4 = false;
+        if constexpr (sizeof(T) == 4) {
+          if (c->nx % 4 == 0) {  // FP32 rows in 16-byte vectors
+            args(k_rhs_march<T, O4, false, false, 4, BZ, D, RS>, grid, 32 * BZ, S::smem_v4);
+            v4 = true;
+          }
+        }
+        if (!v4) args(k_rhs_march<T, O4, false, false, 1, BZ, D, RS>, grid, 32 * BZ, smem);
         done = true;
       }
     }

@@ -13,6 +13,16 @@
 
 namespace ch3d {
 
+// One-time set-up at a launch site (a function attribute, a cached device
+// property) for each device a process drives: true the first time the site
+// asks for `device` (cudaFuncSetAttribute applies to the current device only).
+inline bool first_on_device(unsigned& mask, int device) {
+  const unsigned bit = 1u << (device & 31);
+  if (mask & bit) return false;
+  mask |= bit;
+  return true;
+}
+
 template <class T> struct CplxOf;
 template <> struct CplxOf<double> { typedef double2 type; };
 template <> struct CplxOf<float> { typedef float2 type; };

@@ -975,7 +975,8 @@ cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float
 template <class T> static cudaError_t div_bsub_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
   const dim3 grid((c->nx + 31) / 32, (c->nz + 3) / 4);
-  static int nsm = 0;
+  static int nsm_dev[32] = {};  // SM count per device
+  int& nsm = nsm_dev[c->device & 31];
   if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
   // 256x192x256 (512 blocks): 74 us with 4 rows, 93 with 8; 768x384x576 (3456 blocks):
   // 0.84 ms with 8 rows against 0.88 with 4
@@ -1020,7 +1021,9 @@ template <class T, bool O4> struct MarchShape {
 };
 template <class T, bool O4> static bool march_twisted_t(const ch3d_ctx* c) {
   typedef MarchShape<T, O4> S;
-  static int nsm = 0, occ_tw = 0;
+  static int nsm_dev[32] = {}, occ_dev[32] = {};  // per device: SM count, twisted blocks per SM
+  int& nsm = nsm_dev[c->device & 31];
+  int& occ_tw = occ_dev[c->device & 31];
   if (!nsm) {
     auto kern_tw = k_rhs_march<T, O4, true, true, 1, S::BZ, S::D, S::RS>;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
@@ -1047,7 +1050,8 @@ template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   auto kern = k_rhs_march<T, O4, false, true, 1, BZ, D, RS>;
   auto kern_tw = k_rhs_march<T, O4, true, true, 1, BZ, D, RS>;
   const bool tw = march_twisted_t<T, O4>(c);  // also sets the twisted kernel's shared-memory limit
-  static int nsm = 0;
+  static int nsm_dev[32] = {};  // per device: SM count (and the kernels' attributes set)
+  int& nsm = nsm_dev[c->device & 31];
   if (!nsm) {
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

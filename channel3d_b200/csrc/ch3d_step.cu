@@ -1186,11 +1186,10 @@ template <class T> static cudaError_t uhat_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
   const int P = c->Pv, Q = P - 1;
   size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) + 16;
-  static bool attr_set[2] = {false, false};
+  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
   auto kern = k_uhat_pimp<T, TI>;
-  if (!attr_set[sizeof(T) == 4]) {
+  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set[sizeof(T) == 4] = true;
   }
   dim3 grid((c->nx + TI - 1) / TI, c->nz, 3);
   int nthr = TI * P < 64 ? 64 : (TI * P > 256 ? 256 : TI * P);
@@ -1221,10 +1220,9 @@ template <class T> static cudaError_t prsrc_t(ch3d_ctx* c, int mode) {
   const int LPB = lines_per_block<T>(M);
   const int nlines = c->ny * c->nz;
   size_t smem = (size_t)2 * LPB * M * sizeof(CT);
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[sizeof(T) == 4]) {
+  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
+  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
     cudaFuncSetAttribute(k_prsrc_xfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set[sizeof(T) == 4] = true;
   }
   const int nthr = 256;
   T* a = mode == 2 ? f[10] : (mode == 1 ? f[0] : f[12]);
@@ -1249,10 +1247,9 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   TKX = t;
   size_t smemz = (size_t)2 * TKX * nz * sizeof(CT);
   const int nthrz = 256;
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[sizeof(T) == 4]) {
+  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
+  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
     cudaFuncSetAttribute(k_zfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set[sizeof(T) == 4] = true;
   }
   dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
   if (!zr) {
@@ -1305,10 +1302,9 @@ template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {
   const int LPB = lines_per_block<T>(M);
   const int nlines = c->ny * c->nz;
   size_t smem = (size_t)2 * LPB * M * sizeof(CT);
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[sizeof(T) == 4]) {
+  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
+  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
     cudaFuncSetAttribute(k_xifft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set[sizeof(T) == 4] = true;
   }
   const int nthr = 256;
   k_xifft<T><<<(nlines + LPB - 1) / LPB, nthr, smem, c->stream>>>(make_geo<T>(c), (const CT*)c->spec, f[10], c->planx,

@@ -392,13 +392,25 @@ CH3D_MLP_API size_t ch3d_mlp_workspace_bytes(int batch) {
          256;
 }
 
+// One-time attribute set-up per device a process drives (cudaFuncSetAttribute
+// applies to the current device only): true the first time for that device.
+static bool first_on_current_device(unsigned& mask) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  const unsigned bit = 1u << (dev & 31);
+  if (mask & bit) return false;
+  mask |= bit;
+  return true;
+}
+
 CH3D_MLP_API int ch3d_mlp_forward(const float* X, int batch, const float* params, float* Y, int* status,
                                   void* stream) {
   if (!X || !params || !Y || !status || batch <= 0) return 1;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) != cudaSuccess) return 2;
-    attr = true;
+  static unsigned attr = 0u;  // devices set up
+  if (first_on_current_device(attr) &&
+      cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) != cudaSuccess) {
+    attr = 0u;  // set up again on the next call
+    return 2;
   }
   k_mlp_fwd<<<(batch + TILE - 1) / TILE, TILE, SMEM_FWD, (cudaStream_t)stream>>>(X, batch, params, Y, nullptr, nullptr,
                                                                                 status);
@@ -408,12 +420,12 @@ CH3D_MLP_API int ch3d_mlp_forward(const float* X, int batch, const float* params
 CH3D_MLP_API int ch3d_mlp_grad(const float* X, const float* T, int batch, const float* params, void* work,
                                float* grad, float* loss, int* status, void* stream) {
   if (!X || !T || !params || !work || !grad || !loss || !status || batch <= 0) return 1;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) != cudaSuccess ||
-        cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BWD) != cudaSuccess)
-      return 2;
-    attr = true;
+  static unsigned attr = 0u;  // devices set up
+  if (first_on_current_device(attr) &&
+      (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) != cudaSuccess ||
+       cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BWD) != cudaSuccess)) {
+    attr = 0u;  // set up again on the next call
+    return 2;
   }
   cudaStream_t st = (cudaStream_t)stream;
   const int nb = (batch + TILE - 1) / TILE;

@@ -149,3 +149,27 @@ def test_two_rank_reference_arm_on_cpu():
     import json
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
+
+
+def test_max_over_ranks_gloo(tmp_path):
+    """The replica timing of bench.py (one process per GPU): dist_init, the
+    barriers around the timed region and the max over ranks of the device
+    time, here with 2 gloo ranks on the CPU; every rank must see the slowest
+    rank's time."""
+    script = tmp_path / "ranks.py"
+    script.write_text(
+        "import sys\n"
+        "sys.path.insert(0, %r)\n"
+        "import bench\n"
+        "ws, rank, local = bench.dist_init()\n"
+        "bench.barrier(ws)\n"
+        "v = bench.allmax(ws, 10.0 + 5.0 * rank)\n"
+        "bench.barrier(ws)\n"
+        "print('RANK%%d %%d %%.1f' %% (rank, ws, v))\n" % ROOT)
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", CUDA_VISIBLE_DEVICES="")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", "29541", str(script)]
+    out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    got = sorted(l for l in out.stdout.splitlines() if l.startswith("RANK"))
+    assert got == ["RANK0 2 15.0", "RANK1 2 15.0"], (got, out.stderr[-1000:])

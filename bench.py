@@ -298,7 +298,8 @@ def run_ours(args, ws, rank, local):
     names[0] = GROUP0_KERNEL[key]
     if key == "pimp":
         names[5] = "k_proj_march"
-    gsub = "gsub" in s.path_flags()
+    path = sorted(s.path_flags())
+    gsub = "gsub" in path
     if gsub:  # the march stops at g; the divergence and projection marches substitute u*
         names[2] = "k_div_bsub+k_prsrc_xfft"
         names[5] = "k_proj_bsub"
@@ -375,7 +376,8 @@ def run_ours(args, ws, rank, local):
             "data": "synthetic (seeded laminar + 10% uniform noise, projected divergence-free)",
             "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": solver_name(cfg),
                        "precision": args.precision, "parallelism": "replicas" if ws > 1 else "single",
-                       "l2": "inputs larger than L2 (%.1f GB of fields)" % (s.memory_bytes() / 1e9)},
+                       "l2": "inputs larger than L2 (%.1f GB of fields)" % (s.memory_bytes() / 1e9),
+                       "kernel_path": path},
             "steps_per_s": 1e3 / ms_per_step,
             "gpu_launches": int(args.steps * launches),
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,

@@ -10,9 +10,14 @@ exchange on one GPU per field, so N GPUs run N independent replicas ("replicas
 only", weak scaling); the only collectives are the timing barrier and the
 max-over-ranks reduction.
 
+An FP64 run also times the same workload in mixed precision in the same
+process and reports it in the line's "mixed" object (the metric compares the
+two precisions), with its own clocks and the speed-up at equal clock.
+
 --impl reference times the reference algorithm's CPU implementation (the C++
-restatement in oracle/, all host threads) on a bounded sample of the same
-workload and prints the same JSON line with "impl": "reference".
+restatement in oracle/, all host threads) on a z-slab of the workload (the
+same slab as the CPU-baseline leg of the GPU line, --cpu-nz planes) and prints
+the same JSON line with "impl": "reference" and the slab's own time per step.
 """
 import argparse
 import json
@@ -63,8 +68,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
-    ap.add_argument("--cpu-nz", type=int, default=48, help="z planes of the CPU-baseline sample")
-    ap.add_argument("--cpu-nz-ref", type=int, default=12, help="z planes of the --impl reference sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision timing of an FP64 run")
+    ap.add_argument("--cpu-nz", type=int, default=48,
+                    help="z planes of the CPU sample (the CPU-baseline leg and --impl reference)")
+    ap.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the CPU-baseline leg")
     return ap.parse_args()
 
 
@@ -168,8 +175,10 @@ def cpu_sample_cfg(cfg, nz_sample):
     return cfg.copy(nzc=nz_sample, zlz=cfg.zlz * nz_sample / cfg.nzc)
 
 
-def cpu_reference(cfg, args, ws, rank, steps=1):
-    """Times the CPU restatement (oracle/) on `steps` full steps of cfg."""
+def cpu_reference(cfg, args, steps=3, warmup=1):
+    """Times the CPU restatement (oracle/, OpenMP over all host threads) on
+    `steps` RK3 steps of cfg after `warmup` untimed ones (page-in,
+    first-touch).  Returns (Gpt-steps/s, threads, seconds, steps)."""
     from oracle import oracle as O
     from channel3d_b200 import initfield
     if args.cpu_threads:
@@ -180,12 +189,12 @@ def cpu_reference(cfg, args, ws, rank, steps=1):
     ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp)
     o.set_state(ux, uy, uz, p)
     del ux, uy, uz, p
-    o.step(1)  # untimed warm-up step (page-in, first-touch)
+    o.step(max(1, warmup))
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
     o.close()
-    return cfg.npoints * steps / dt / 1e9, threads, dt
+    return cfg.npoints * steps / dt / 1e9, threads, dt, steps
 
 
 def solver_name(cfg):
@@ -207,38 +216,26 @@ def scheme_key(cfg):
 def run_reference(args, ws, rank):
     """The reference's algorithm on the host cores: the C++ restatement of the
     step (oracle/, OpenMP over all host threads), each timed step one RK3 step
-    of a z-slab sample of the workload."""
+    of the same z-slab sample of the workload the CPU-baseline leg of the GPU
+    line uses; ms_per_step is the slab's own time per step."""
     from channel3d_b200 import workloads
     cfg, _ = workloads.get(args.workload, precision="fp64")
     if rank != 0:
         return
-    sample = cpu_sample_cfg(cfg, args.cpu_nz_ref)
-    from oracle import oracle as O
-    from channel3d_b200 import initfield
-    if args.cpu_threads:
-        O.set_threads(args.cpu_threads)
-    thr = O.num_threads()
-    o = O.Oracle(sample)
-    ux, uy, uz, p = initfield.laminar_noise(sample, yp=o.mesh()[0])
-    o.set_state(ux, uy, uz, p)
-    del ux, uy, uz, p
-    o.step(max(1, args.warmup))
-    t0 = time.perf_counter()
-    o.step(args.steps)
-    dt = time.perf_counter() - t0
-    o.close()
-    v = sample.npoints * args.steps / dt / 1e9
+    sample = cpu_sample_cfg(cfg, args.cpu_nz)
+    v, thr, dt, nst = cpu_reference(sample, args, steps=args.steps, warmup=args.warmup)
+    slab = "%s (%dx%dx%d z-slab)" % (args.workload, sample.nxc, sample.nyc, sample.nzc)
     line = {
         "impl": "reference", "metric": "Gpt-steps/s", "value": v, "unit": "Gpt-steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cfg.npoints / (v * 1e9) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / nst * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded laminar + 10% uniform noise)",
-        "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": solver_name(cfg),
-                   "precision": "fp64"},
+        "config": {"workload": slab, "grid": [sample.nxc, sample.nyc, sample.nzc], "solver": solver_name(cfg),
+                   "precision": "fp64", "full_grid": [cfg.nxc, cfg.nyc, cfg.nzc]},
         "cpu_baseline": {"value": v, "unit": "Gpt-steps/s", "cores": thr, "kind": "port",
                          "sample": "%d RK3 steps (after %d untimed) of a %dx%dx%d z-slab of the %s workload "
                                    "(%.1f s); C++ restatement of the reference step (oracle/), OpenMP, %d threads"
-                                   % (args.steps, max(1, args.warmup), sample.nxc, sample.nyc, sample.nzc,
+                                   % (nst, max(1, args.warmup), sample.nxc, sample.nyc, sample.nzc,
                                       args.workload, dt, thr)},
         "e2e": {"value": v, "unit": "Gpt-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -261,17 +258,36 @@ def profile_traffic(kernel, precision):
     return None, None
 
 
-def run_ours(args, ws, rank, local):
+def launches_per_step(cfg, key, precision, gsub):
+    """Kernel launches of one graph-replayed step (ch3d_api.cu record_step)."""
+    launches = 1 + 3 * LAUNCHES_PER_SUBSTEP[precision] + 4
+    if key == "pimp" and cfg.nxc % 32 == 0 and cfg.nzc % 4 == 0:
+        launches -= 1  # the last projection carries the step diagnostics (no diag kernel)
+    if gsub:
+        launches += 3  # divergence march + x FFT in place of the fused divergence/x FFT kernel
+    if key == "order4":
+        launches += 3 * 2        # mean viscous stress partials, interpolated velocities
+    elif key == "fimp":
+        launches += 3 * 4        # RHS and y solve unfused, x/z periodic sweeps + their factors
+    elif key == "les":
+        launches += 3 * 1 + 1 + (1 if cfg.LES_type == 10 else 0)  # RHS/y solve unfused, eddy viscosity (+ wall shear)
+    return launches
+
+
+def measure(args, ws, rank, local, precision, want_e2e):
+    """One precision of the workload: device-timed steps (CUDA events on the
+    context's stream, max over ranks), kernel-group times, the roofline of the
+    dominant group and, optionally, the end-to-end time through the C ABI."""
     import torch
     from channel3d_b200 import ChannelSolver, initfield, workloads
-    cfg, _ = workloads.get(args.workload, precision=args.precision)
+    cfg, _ = workloads.get(args.workload, precision=precision)
     cfg = cfg.copy(device=local)
     torch.cuda.set_device(local)
     s = ChannelSolver(cfg)
     ux, uy, uz, p = initfield.laminar_noise(cfg, yp=s.yp)
     s.upload(ux, uy, uz, p)
     s.project()
-    s.step(max(args.warmup, 3) if args.warmup >= 3 else 3)
+    s.step(max(args.warmup, 3))
 
     clk = ClockSampler(local)
     barrier(ws)
@@ -292,7 +308,7 @@ def run_ours(args, ws, rank, local):
     # context's stream over two more (ungraphed) steps; groups 0-5 per substep
     # launch, the scalar kernels per step
     kt = s.kernel_times(2)
-    word = 4 if args.precision == "mixed" else 8
+    word = 4 if precision == "mixed" else 8
     key = scheme_key(cfg)
     names = dict(GROUP_NAMES)
     names[0] = GROUP0_KERNEL[key]
@@ -315,25 +331,15 @@ def run_ours(args, ws, rank, local):
     dom_b = GROUP_ARRAYS[dom] * cfg.npoints * word
     achieved = dom_b / (kt[dom] * 1e-3) / 1e9
     # the march that stops at g moves less than the one that substitutes: its own profile line
-    tpp, tsrc = profile_traffic(names[dom] + ("/g" if gsub and dom == 0 else ""), args.precision)
+    tpp, tsrc = profile_traffic(names[dom] + ("/g" if gsub and dom == 0 else ""), precision)
     traffic = tpp * cfg.npoints if tpp is not None else None
     step_alg = ALG_ARRAYS_PER_SUBSTEP[key] * 3 * word * cfg.npoints
     step_achieved = step_alg / (ms_per_step * 1e-3) / 1e9
-    launches = 1 + 3 * LAUNCHES_PER_SUBSTEP[args.precision] + 4
-    if key == "pimp" and cfg.nxc % 32 == 0 and cfg.nzc % 4 == 0:
-        launches -= 1  # the last projection carries the step diagnostics (no diag kernel)
-    if gsub:
-        launches += 3  # divergence march + x FFT in place of the fused divergence/x FFT kernel
-    if key == "order4":
-        launches += 3 * 2        # mean viscous stress partials, interpolated velocities
-    elif key == "fimp":
-        launches += 3 * 4        # RHS and y solve unfused, x/z periodic sweeps + their factors
-    elif key == "les":
-        launches += 3 * 1 + 1 + (1 if cfg.LES_type == 10 else 0)  # RHS/y solve unfused, eddy viscosity (+ wall shear)
+    launches = launches_per_step(cfg, key, precision, gsub)
 
     # end-to-end through the public API: pinned host arrays -> upload -> K steps -> download
     e2e = None
-    if not args.no_e2e:
+    if want_e2e:
         pin = [torch.empty(cfg.npoints, dtype=torch.float64).pin_memory().numpy().reshape(cfg.shape)
                for _ in range(4)]
         for dst, src in zip(pin, (ux, uy, uz, p)):
@@ -344,7 +350,7 @@ def run_ours(args, ws, rank, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s.upload(*pin)
-        inf2 = s.step(args.steps)
+        s.step(args.steps)
         from channel3d_b200 import _lib
         _lib.check(s.lib.ch3d_download_state(s.ctx, _lib.LAYOUT_INTERIOR, *(_lib.dptr(o) for o in outs), None))
         torch.cuda.synchronize()
@@ -355,49 +361,82 @@ def run_ours(args, ws, rank, local):
                "h2d_bytes_per_step": bytes_io / args.steps, "d2h_bytes_per_step": bytes_io / args.steps,
                "what": "ch3d_upload_state (4 FP64 arrays from pinned host memory) + ch3d_step(K) + "
                        "ch3d_download_state (4 arrays), wall clock, max over ranks"}
+    r = {
+        "cfg": cfg, "value": value, "ms_per_step": ms_per_step, "info": info, "wall_s": wall, "clocks": clocks,
+        "path": path, "launches": launches, "kernels": per_group, "memory_bytes": s.memory_bytes(), "e2e": e2e,
+        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind + " (hbm_gbs, burst copy)",
+                     "alg_bytes_per_launch": dom_b,
+                     "traffic_source": ("profiles/%s: ncu dram__bytes_read.sum + dram__bytes_write.sum per grid "
+                                        "point of a smaller capture, scaled to this launch" % tsrc) if tsrc else None},
+        "step_roofline": {"alg_bytes_per_cell_step": ALG_ARRAYS_PER_SUBSTEP[key] * 3 * word,
+                          "achieved": step_achieved, "peak": peak, "frac": step_achieved / peak},
+    }
+    s.close()
+    return r
+
+
+def run_ours(args, ws, rank, local):
+    main = measure(args, ws, rank, local, args.precision, not args.no_e2e)
+    cfg = main["cfg"]
+    # the other precision of the same workload, in the same process (FP64 against mixed)
+    other = None
+    if not args.no_mixed and args.precision == "fp64" and scheme_key(cfg) in ("pimp", "order4", "fimp"):
+        other = measure(args, ws, rank, local, "mixed", not args.no_e2e)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
             sample = cpu_sample_cfg(cfg.copy(precision="fp64", device=0), args.cpu_nz)
-            v, thr, dt = cpu_reference(sample, args, ws, rank, steps=1)
+            v, thr, dt, nst = cpu_reference(sample, args, steps=args.cpu_steps)
             cpu = {"value": v, "unit": "Gpt-steps/s", "cores": thr, "kind": "port",
-                   "sample": "1 RK3 step (after 1 untimed) of a %dx%dx%d z-slab of %s (%.1f s); C++ restatement "
+                   "sample": "%d RK3 steps (after 1 untimed) of a %dx%dx%d z-slab of %s (%.1f s); C++ restatement "
                              "of the reference step (oracle/), OpenMP, %d threads"
-                             % (sample.nxc, sample.nyc, sample.nzc, args.workload, dt, thr)}
+                             % (nst, sample.nxc, sample.nyc, sample.nzc, args.workload, dt, thr)}
         except Exception as ex:  # keep the GPU line even if host memory is short
             cpu = {"value": None, "unit": "Gpt-steps/s", "cores": None, "kind": "port", "sample": "failed: %s" % ex}
 
     if rank == 0:
         line = {
-            "metric": "Gpt-steps/s", "value": value, "unit": "Gpt-steps/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "metric": "Gpt-steps/s", "value": main["value"], "unit": "Gpt-steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded laminar + 10% uniform noise, projected divergence-free)",
             "config": {"workload": args.workload, "grid": [cfg.nxc, cfg.nyc, cfg.nzc], "solver": solver_name(cfg),
                        "precision": args.precision, "parallelism": "replicas" if ws > 1 else "single",
-                       "l2": "inputs larger than L2 (%.1f GB of fields)" % (s.memory_bytes() / 1e9),
-                       "kernel_path": path},
-            "steps_per_s": 1e3 / ms_per_step,
-            "gpu_launches": int(args.steps * launches),
-            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": peak_kind + " (hbm_gbs, burst copy)",
-                         "alg_bytes_per_launch": dom_b,
-                         "traffic_source": ("profiles/%s: ncu dram__bytes_read.sum + dram__bytes_write.sum per grid "
-                                            "point of a smaller capture, scaled to this launch" % tsrc) if tsrc else None},
-            "step_roofline": {"alg_bytes_per_cell_step": ALG_ARRAYS_PER_SUBSTEP[key] * 3 * word,
-                              "achieved": step_achieved, "peak": peak, "frac": step_achieved / peak},
-            "kernels": per_group,
-            "memory_bytes": s.memory_bytes(),
-            "clocks": clocks,
-            "e2e": e2e,
+                       "l2": "inputs larger than L2 (%.1f GB of fields)" % (main["memory_bytes"] / 1e9),
+                       "kernel_path": main["path"]},
+            "steps_per_s": 1e3 / main["ms_per_step"],
+            "gpu_launches": int(args.steps * main["launches"]),
+            "roofline": main["roofline"],
+            "step_roofline": main["step_roofline"],
+            "kernels": main["kernels"],
+            "memory_bytes": main["memory_bytes"],
+            "clocks": main["clocks"],
+            "e2e": main["e2e"],
             "cpu_baseline": cpu,
-            "last_info": info,
-            "wall_s": wall,
+            "last_info": main["info"],
+            "wall_s": main["wall_s"],
         }
+        if other is not None:
+            c64, c32 = main["clocks"].get("sm_mhz"), other["clocks"].get("sm_mhz")
+            line["mixed"] = {
+                "value": other["value"], "unit": "Gpt-steps/s", "ms_per_step": other["ms_per_step"],
+                "steps": args.steps, "dtype": "f32+f64", "steps_per_s": 1e3 / other["ms_per_step"],
+                "gpu_launches": int(args.steps * other["launches"]), "kernel_path": other["path"],
+                "roofline": other["roofline"], "step_roofline": other["step_roofline"],
+                "kernels": other["kernels"], "memory_bytes": other["memory_bytes"], "clocks": other["clocks"],
+                "e2e": other["e2e"], "last_info": other["info"],
+                "speedup_vs_fp64": main["ms_per_step"] / other["ms_per_step"],
+                "speedup_vs_fp64_at_equal_clock": (main["ms_per_step"] * c64) / (other["ms_per_step"] * c32)
+                if c64 and c32 else None,
+                "what": "the same workload in mixed precision (FP32 fields, stencils, ADI and FFTs; FP64 low-mode "
+                        "Poisson y solves, bulk constraint and reductions), timed like the FP64 line in the same "
+                        "process; speedup_vs_fp64_at_equal_clock compares time x median sampled SM clock",
+            }
         print(json.dumps(line), flush=True)
-    s.close()
 
 
 def main():

@@ -39,25 +39,22 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="channel256x192x256_re13750")
-    ap.add_argument("--steps", type=int, default=0)
-    ap.add_argument("--ivstats", type=int, default=20)
-    ap.add_argument("--stat-from", type=int, default=0)
-    a = ap.parse_args()
-    cfg64, steps = workloads.get(a.workload, precision="fp64")
-    steps = a.steps or steps
+def compare(workload="channel256x192x256_re13750", steps=0, ivstats=20, stat_from=0, device=0):
+    """Runs the workload in FP64 and in mixed precision from the same projected
+    seeded start and returns the comparison (a dict, see the module text)."""
+    cfg64, nsteps = workloads.get(workload, precision="fp64")
+    cfg64 = cfg64.copy(device=device)
+    steps = steps or nsteps
     s = ChannelSolver(cfg64)
     s.upload(*initfield.laminar_noise(cfg64, yp=s.yp))
     s.project()
     st = s.download()
     s.close()
     state = (st["ux"], st["uy"], st["uz"], st["p"])
-    p64, i64, ms64 = run(cfg64, state, steps, a.ivstats, a.stat_from)
-    p32, i32, ms32 = run(cfg64.copy(precision="mixed"), state, steps, a.ivstats, a.stat_from)
-    out = {
-        "workload": a.workload, "steps": steps, "ivstats": a.ivstats,
+    p64, i64, ms64 = run(cfg64, state, steps, ivstats, stat_from)
+    p32, i32, ms32 = run(cfg64.copy(precision="mixed"), state, steps, ivstats, stat_from)
+    return {
+        "workload": workload, "steps": steps, "ivstats": ivstats, "stat_from": stat_from,
         "rel_err_U": rel(p32["U"], p64["U"]), "rel_err_urms": rel(p32["urms"], p64["urms"]),
         "rel_err_vrms": rel(p32["vrms"], p64["vrms"]), "rel_err_wrms": rel(p32["wrms"], p64["wrms"]),
         "Re_tau_fp64": p64["Re_tau"], "Re_tau_mixed": p32["Re_tau"],
@@ -65,6 +62,16 @@ def main():
         "divmax_fp64": i64["divmax2"], "divmax_mixed": i32["divmax2"],
         "ms_per_step_fp64": ms64, "ms_per_step_mixed": ms32, "speedup": ms64 / ms32,
     }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="channel256x192x256_re13750")
+    ap.add_argument("--steps", type=int, default=0)
+    ap.add_argument("--ivstats", type=int, default=20)
+    ap.add_argument("--stat-from", type=int, default=0)
+    a = ap.parse_args()
+    out = compare(a.workload, a.steps, a.ivstats, a.stat_from)
     print(json.dumps(out))
 
 

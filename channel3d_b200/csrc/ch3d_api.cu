@@ -232,6 +232,8 @@ int check_config(const ch3d_config* g) {
       return fail(CH3D_ERR_INVALID, "unrecognized FilterType");
   }
   if (g->precision != CH3D_PREC_FP64 && g->precision != CH3D_PREC_MIXED) return fail(CH3D_ERR_INVALID, "bad precision");
+  if (g->device < 0 || g->device >= kMaxDevices)
+    return fail(CH3D_ERR_INVALID, "device %d out of range (0..%d)", g->device, kMaxDevices - 1);
   if (g->IsUxConst && !(g->ybulk2 > g->ybulk1)) return fail(CH3D_ERR_INVALID, "ybulk1 OR ybulk2 wrong");
   if (!(g->dtMax > 0)) return fail(CH3D_ERR_INVALID, "dtMax must be positive");
   return CH3D_OK;
@@ -312,48 +314,54 @@ double host_get(const ch3d_ctx* c, int layout, const double* a, int i, int j, in
   return a[gidx4(c, i, j, k)];
 }
 
-// Host-side ghost fill of a downloaded field, per SetBC_and_UpdateHalo /
-// SetBC_and_UpdateHalo_pr (src/CFD_2nd/m_BC_and_Halo.f90:232-344,410-456)
-// for periodic x,z.  comp: 0 ux, 1 uy, 2 uz, 3 p.
+// Host-side ghost fill of a downloaded field: the boundary rules and the
+// periodic halo copies (myupdate_halo, src/CFD_2nd/m_Decomp2d.f90:1588-1743:
+// x planes over the whole y and z extent first, then z planes over the whole
+// x and y extent) of SetBC_and_UpdateHalo and SetBC_and_UpdateHalo_pr, with
+// each tree's halo widths: 2nd order (src/CFD_2nd/m_BC_and_Halo.f90:20-29,
+// 232-344, 410-456) one plane on each side in x and z; 4th order
+// (src/CFD_4th/m_BC_and_Halo.f90:24-46, 51-96, 136-150) two on each side for
+// the velocity, two below and one above for the pressure.  Cells those routines
+// never write (x = nxc+2 and z = nzc+2 of the 2nd-order arrays, the y plane
+// nyc+2 of ux, uz, p, uy(:,0,:) of the 4th-order tree) keep the host's values.
+// Periodic x and z.  comp: 0 ux, 1 uy, 2 uz, 3 p.
 void host_fill_ghosts(const ch3d_ctx* c, int layout, double* a, int comp) {
   const int nxc = c->nx, nyc = c->ny, nzc = c->nz, nyp = nyc + 1;
   const ch3d_config& g = c->cfg;
-  auto at = [&](int i, int j, int k) -> double& {
-    return layout == CH3D_LAYOUT_GHOST2 ? a[gidx2(c, i, j, k)] : a[gidx4(c, i, j, k)];
-  };
-  const int jtop = layout == CH3D_LAYOUT_GHOST2 ? nyc + 2 : nyc + 1;
+  const bool g2 = layout == CH3D_LAYOUT_GHOST2;
+  auto at = [&](int i, int j, int k) -> double& { return g2 ? a[gidx2(c, i, j, k)] : a[gidx4(c, i, j, k)]; };
   for (int k = 1; k <= nzc; ++k)
     for (int i = 1; i <= nxc; ++i) {
       if (comp == 3) { at(i, nyp, k) = at(i, nyc, k); at(i, 0, k) = at(i, 1, k); continue; }
       if (comp == 1) {
         at(i, nyp, k) = g.uyBcValue[3];
-        if (jtop >= nyp + 1) at(i, nyp + 1, k) = g.uyBcValue[3] * 2.0 - at(i, nyc, k);
-        // uy(ic,0,kc) is never set by the 4th-order solver (zero)
-        at(i, 0, k) = g.order == 4 ? 0.0 : g.uyBcValue[2] * 2.0 - at(i, 2, k);
+        if (g.order == 2) {
+          at(i, nyp + 1, k) = g.uyBcValue[3] * 2.0 - at(i, nyc, k);
+          at(i, 0, k) = g.uyBcValue[2] * 2.0 - at(i, 2, k);  // uy_ym = uyBcValue(ym_dir)
+        }
         continue;
       }
-      double wl = comp == 0 ? g.uxBcValue[2] : g.uzBcValue[2];
-      double wh = comp == 0 ? g.uxBcValue[3] : g.uzBcValue[3];
+      const double wl = comp == 0 ? g.uxBcValue[2] : g.uzBcValue[2];
+      const double wh = comp == 0 ? g.uxBcValue[3] : g.uzBcValue[3];
       if (g.BcOption[3] == -1) at(i, nyp, k) = wh * 2.0 - at(i, nyc, k);
       else at(i, nyp, k) = wh * c->dyp[nyp] + at(i, nyc, k);
       if (g.BcOption[2] == -1) at(i, 0, k) = wl * 2.0 - at(i, 1, k);
       else at(i, 0, k) = at(i, 1, k) - wl * c->dyp[1];
     }
-  const int hx = layout == CH3D_LAYOUT_GHOST2 ? 1 : 2;  // halo depth kept by the layout
-  const int jlo = 0, jhi = jtop;
-  for (int k = 1; k <= nzc; ++k)
-    for (int j = jlo; j <= jhi; ++j)
-      for (int h = 1; h <= hx; ++h) {
-        at(1 - h, j, k) = at(nxc - h + 1, j, k);
-        at(nxc + h, j, k) = at(h, j, k);
-      }
-  const int ilo = 1 - hx, ihi = nxc + hx;
-  for (int h = 1; h <= hx; ++h)
-    for (int j = jlo; j <= jhi; ++j)
-      for (int i = ilo; i <= ihi; ++i) {
-        at(i, j, 1 - h) = at(i, j, nzc - h + 1);
-        at(i, j, nzc + h) = at(i, j, h);
-      }
+  // halo widths below / above in x and z, and the allocated bounds
+  const int hm = g2 ? 1 : 2, hp = g2 ? 1 : (comp == 3 ? 1 : 2);
+  const int xmm = g2 ? 0 : -1, xpm = nxc + 2, ypm = g2 ? nyc + 2 : nyc + 1, zmm = g2 ? 0 : -1, zpm = nzc + 2;
+  for (int k = zmm; k <= zpm; ++k)
+    for (int j = 0; j <= ypm; ++j) {
+      for (int h = 1; h <= hm; ++h) at(1 - h, j, k) = at(nxc - h + 1, j, k);
+      for (int h = 1; h <= hp; ++h) at(nxc + h, j, k) = at(h, j, k);
+    }
+  for (int h = 1; h <= hm; ++h)
+    for (int j = 0; j <= ypm; ++j)
+      for (int i = xmm; i <= xpm; ++i) at(i, j, 1 - h) = at(i, j, nzc - h + 1);
+  for (int h = 1; h <= hp; ++h)
+    for (int j = 0; j <= ypm; ++j)
+      for (int i = xmm; i <= xpm; ++i) at(i, j, nzc + h) = at(i, j, h);
 }
 
 template <class T>
@@ -1068,6 +1076,11 @@ int ch3d_poisson_noalloc(int nxc, int nyc, int nzc, double xlx, double zlz, cons
   if (need > (size_t)CH3D_NOALLOC_SCRATCH_BYTES)
     return fail(CH3D_ERR_INVALID, "grid %d x %d x %d needs %zu bytes of scratch, more than the %u bytes of "
                 "CH3D_NOALLOC_SCRATCH_BYTES", nxc, nyc, nzc, need, (unsigned)CH3D_NOALLOC_SCRATCH_BYTES);
+  const size_t smem = noalloc_smem(nxc, nyc, nzc);
+  if (smem > noalloc_smem_limit())
+    return fail(CH3D_ERR_UNSUPPORTED, "grid %d x %d x %d: a transform or y-solve block of the allocation-free solve "
+                "needs %zu bytes of shared memory, more than its %zu-byte limit", nxc, nyc, nzc, smem,
+                noalloc_smem_limit());
   cudaError_t e = poisson_noalloc(nxc, nyc, nzc, xlx, zlz, yp, bc_ym, bc_yp, d_src, d_phi, (cudaStream_t)stream, px, pz);
   if (e != cudaSuccess) return fail(CH3D_ERR_CUDA, "ch3d_poisson_noalloc: %s", cudaGetErrorString(e));
   return CH3D_OK;

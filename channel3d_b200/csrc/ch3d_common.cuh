@@ -11,16 +11,60 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
+
 namespace ch3d {
 
-// One-time set-up at a launch site (a function attribute, a cached device
-// property) for each device a process drives: true the first time the site
-// asks for `device` (cudaFuncSetAttribute applies to the current device only).
-inline bool first_on_device(unsigned& mask, int device) {
-  const unsigned bit = 1u << (device & 31);
-  if (mask & bit) return false;
-  mask |= bit;
-  return true;
+// Devices a process may drive through this library (device ordinals 0..63).
+constexpr int kMaxDevices = 64;
+
+// One-time set-up at a launch site (function attributes, cached device
+// properties) for each device a process drives; cudaFuncSetAttribute applies
+// to the current device only, so each site keeps one flag per device.
+struct PerDevice {
+  std::atomic<unsigned long long> done{0ull};
+};
+
+inline std::recursive_mutex& setup_mutex() {
+  static std::recursive_mutex m;
+  return m;
+}
+
+// Runs setup() (returning cudaError_t) the first time `site` meets `device`,
+// under a process-wide mutex; the device is marked only when setup succeeds,
+// so a second host thread never launches before the attributes are in place
+// and a failed set-up is retried on the next call.  The caller has `device`
+// current.  Ordinals outside [0, kMaxDevices) give cudaErrorInvalidDevice.
+template <class F> cudaError_t once_per_device(PerDevice& site, int device, F&& setup) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  const unsigned long long bit = 1ull << device;
+  if (site.done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  std::lock_guard<std::recursive_mutex> lk(setup_mutex());
+  if (site.done.load(std::memory_order_relaxed) & bit) return cudaSuccess;
+  const cudaError_t e = setup();
+  if (e == cudaSuccess) site.done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
+
+// SM count of a device, queried once (148, the B200's, if the query fails).
+inline int sm_count(int device) {
+  static PerDevice site;
+  static int nsm[kMaxDevices] = {};
+  const cudaError_t e = once_per_device(site, device, [&] {
+    int v = 0;
+    const cudaError_t r = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    if (r == cudaSuccess) nsm[device] = v;
+    return r;
+  });
+  return e == cudaSuccess ? nsm[device] : 148;
+}
+
+// Shared-memory limit of one kernel, set once per device.
+template <class K> cudaError_t smem_limit_once(PerDevice& site, int device, K kern, size_t bytes) {
+  return once_per_device(site, device, [&] {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  });
 }
 
 template <class T> struct CplxOf;

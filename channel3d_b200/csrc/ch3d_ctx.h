@@ -119,6 +119,8 @@ bool launch_xifft_r(ch3d_ctx* c, cudaError_t* err);
 cudaError_t launch_ysolve_factors(ch3d_ctx* c);
 // allocation-free Poisson solve (static device scratch, ch3d_step.cu)
 size_t noalloc_bytes(int nx, int ny, int nz);
+size_t noalloc_smem(int nx, int ny, int nz);
+size_t noalloc_smem_limit();
 cudaError_t noalloc_scratch_address(int dev, void** out);
 cudaError_t poisson_noalloc(int nx, int ny, int nz, double xlx, double zlz, const double* yp, int bclo, int bchi,
                             const double* d_src, double* d_phi, cudaStream_t st, const FFTPlanDev& planx,

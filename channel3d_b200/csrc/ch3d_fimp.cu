@@ -111,10 +111,8 @@ template <class T> static cudaError_t ptri_t(ch3d_ctx* c) {
   if (LB < 1) LB = 1;
   const long long nlines = (long long)c->ny * c->nz;
   const size_t smem = (size_t)LB * (c->nx + 1) * sizeof(T);
-  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
-  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
-    cudaFuncSetAttribute(k_ptri_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  }
+  static PerDevice attr;  // per precision (template instance)
+  if ((e = smem_limit_once(attr, c->device, k_ptri_x<T>, 200 * 1024)) != cudaSuccess) return e;
   k_ptri_x<T><<<dim3((unsigned)((nlines + LB - 1) / LB), 3), 128, smem, c->stream>>>(c->nx, nlines, LB, c->pfac, f[7],
                                                                                       f[8], f[9], c->sc);
   e = cudaGetLastError();

@@ -975,9 +975,7 @@ cudaError_t launch_bulk_march(ch3d_ctx* c) { return c->fp32 ? bulk_march_t<float
 template <class T> static cudaError_t div_bsub_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
   const dim3 grid((c->nx + 31) / 32, (c->nz + 3) / 4);
-  static int nsm_dev[32] = {};  // SM count per device
-  int& nsm = nsm_dev[c->device & 31];
-  if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
+  const int nsm = sm_count(c->device);
   // 256x192x256 (512 blocks): 74 us with 4 rows, 93 with 8; 768x384x576 (3456 blocks):
   // 0.84 ms with 8 rows against 0.88 with 4
   if ((long long)grid.x * grid.y > 6LL * nsm)
@@ -1021,18 +1019,21 @@ template <class T, bool O4> struct MarchShape {
 };
 template <class T, bool O4> static bool march_twisted_t(const ch3d_ctx* c) {
   typedef MarchShape<T, O4> S;
-  static int nsm_dev[32] = {}, occ_dev[32] = {};  // per device: SM count, twisted blocks per SM
-  int& nsm = nsm_dev[c->device & 31];
-  int& occ_tw = occ_dev[c->device & 31];
-  if (!nsm) {
-    auto kern_tw = k_rhs_march<T, O4, true, true, 1, S::BZ, S::D, S::RS>;
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
-    cudaFuncSetAttribute(kern_tw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * S::smem));
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tw, kern_tw, 64 * S::BZ, 2 * S::smem) != cudaSuccess)
-      occ_tw = 0;
-  }
+  static PerDevice site;                  // per instance: the twisted kernel's limit and occupancy
+  static int occ_dev[kMaxDevices] = {};   // twisted blocks per SM, written once per device under the set-up lock
+  auto kern_tw = k_rhs_march<T, O4, true, true, 1, S::BZ, S::D, S::RS>;
+  const cudaError_t e = once_per_device(site, c->device, [&] {
+    cudaError_t r = cudaFuncSetAttribute(kern_tw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * S::smem));
+    if (r != cudaSuccess) return r;
+    int occ = 0;
+    if ((r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern_tw, 64 * S::BZ, 2 * S::smem)) != cudaSuccess)
+      return r;
+    occ_dev[c->device] = occ;
+    return cudaSuccess;
+  });
+  if (e != cudaSuccess) return false;  // the one-directional march has no such requirement
   const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + S::BZ - 1) / S::BZ);
-  return c->ny >= 2 && ntiles <= (long long)nsm * occ_tw;
+  return c->ny >= 2 && ntiles <= (long long)sm_count(c->device) * occ_dev[c->device];
 }
 bool march_twisted(const ch3d_ctx* c) {
   if (c->cfg.order == 4) return c->fp32 ? march_twisted_t<float, true>(c) : march_twisted_t<double, true>(c);
@@ -1050,19 +1051,20 @@ template <class T, bool O4> static cudaError_t rhs_march_t(ch3d_ctx* c) {
   auto kern = k_rhs_march<T, O4, false, true, 1, BZ, D, RS>;
   auto kern_tw = k_rhs_march<T, O4, true, true, 1, BZ, D, RS>;
   const bool tw = march_twisted_t<T, O4>(c);  // also sets the twisted kernel's shared-memory limit
-  static int nsm_dev[32] = {};  // per device: SM count (and the kernels' attributes set)
-  int& nsm = nsm_dev[c->device & 31];
-  if (!nsm) {
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) nsm = 148;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static PerDevice site;  // per instance: the one-directional kernels' limits
+  cudaError_t e = once_per_device(site, c->device, [&] {
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t r = cudaFuncSetAttribute(kern, a, (int)smem);
     if constexpr (!O4) {
-      cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, 1, BZ, D, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+      if (r == cudaSuccess) r = cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, 1, BZ, D, RS>, a, (int)smem);
       if constexpr (sizeof(T) == 4)
-        cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, 4, BZ, D, RS>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_v4);
+        if (r == cudaSuccess)
+          r = cudaFuncSetAttribute(k_rhs_march<T, O4, false, false, 4, BZ, D, RS>, a, (int)S::smem_v4);
     }
-  }
+    return r;
+  });
+  if (e != cudaSuccess) return e;
+  const int nsm = sm_count(c->device);
   const long long ntiles = (long long)((c->nx + 31) / 32) * ((c->nz + BZ - 1) / BZ);
   auto args = [&](auto k, unsigned grid, int threads, size_t sm) {
     k<<<grid, threads, sm, c->stream>>>(make_geo<T>(c), (const T*)c->mtab, march_down_tables<T>(c->mtab, c->ny), f[0],

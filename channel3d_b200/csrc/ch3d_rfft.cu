@@ -301,9 +301,8 @@ template <class T> static bool zfft_r_t(ch3d_ctx* c, int inverse, cudaError_t* e
     if constexpr (sizeof(T) == 8) kern = k_zfft_r<T, PL, LZ>;
     else kern = k_zfft_rf<T, PL, LZ>;
     const size_t smem = (size_t)PL::N * LZ * sizeof(CT);
-    static unsigned attr = 0u;  // devices set up
-    if (first_on_device(attr, c->device))
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static PerDevice attr;  // per kernel instance
+    if ((*err = smem_limit_once(attr, c->device, kern, smem)) != cudaSuccess) return;
     dim3 grid((c->nxh + LZ - 1) / LZ, c->ny);
     kern<<<grid, LZ * PL::P, smem, c->stream>>>(make_geo<T>(c), (CT*)c->spec, (const CT*)c->twz, inverse, c->sc);
     *err = cudaGetLastError();

@@ -1186,11 +1186,10 @@ template <class T> static cudaError_t uhat_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
   const int P = c->Pv, Q = P - 1;
   size_t smem = (size_t)c->ny * TI * sizeof(T) + (size_t)TI * 2 * (Q > 0 ? Q : 1) * sizeof(T) + 16;
-  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
+  static PerDevice attr;  // per precision (template instance)
   auto kern = k_uhat_pimp<T, TI>;
-  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  }
+  cudaError_t e = smem_limit_once(attr, c->device, kern, 200 * 1024);
+  if (e != cudaSuccess) return e;
   dim3 grid((c->nx + TI - 1) / TI, c->nz, 3);
   int nthr = TI * P < 64 ? 64 : (TI * P > 256 ? 256 : TI * P);
   kern<<<grid, nthr, smem, c->stream>>>(make_geo<T>(c), c->hfac, P, f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13],
@@ -1220,10 +1219,8 @@ template <class T> static cudaError_t prsrc_t(ch3d_ctx* c, int mode) {
   const int LPB = lines_per_block<T>(M);
   const int nlines = c->ny * c->nz;
   size_t smem = (size_t)2 * LPB * M * sizeof(CT);
-  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
-  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
-    cudaFuncSetAttribute(k_prsrc_xfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  }
+  static PerDevice attr;  // per precision (template instance)
+  if ((e = smem_limit_once(attr, c->device, k_prsrc_xfft<T>, 200 * 1024)) != cudaSuccess) return e;
   const int nthr = 256;
   T* a = mode == 2 ? f[10] : (mode == 1 ? f[0] : f[12]);
   T* b = mode == 1 ? f[1] : f[13];
@@ -1247,10 +1244,8 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   TKX = t;
   size_t smemz = (size_t)2 * TKX * nz * sizeof(CT);
   const int nthrz = 256;
-  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
-  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
-    cudaFuncSetAttribute(k_zfft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  }
+  static PerDevice attr;  // per precision (template instance)
+  if ((e = smem_limit_once(attr, c->device, k_zfft<T>, 200 * 1024)) != cudaSuccess) return e;
   dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
   if (!zr) {
     k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 0, c->sc);
@@ -1302,10 +1297,8 @@ template <class T> static cudaError_t xifft_t(ch3d_ctx* c) {
   const int LPB = lines_per_block<T>(M);
   const int nlines = c->ny * c->nz;
   size_t smem = (size_t)2 * LPB * M * sizeof(CT);
-  static unsigned attr_set[2] = {0u, 0u};  // devices set up, per precision
-  if (first_on_device(attr_set[sizeof(T) == 4], c->device)) {
-    cudaFuncSetAttribute(k_xifft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  }
+  static PerDevice attr;  // per precision (template instance)
+  if ((e = smem_limit_once(attr, c->device, k_xifft<T>, 200 * 1024)) != cudaSuccess) return e;
   const int nthr = 256;
   k_xifft<T><<<(nlines + LPB - 1) / LPB, nthr, smem, c->stream>>>(make_geo<T>(c), (const CT*)c->spec, f[10], c->planx,
                                                                  (const CT*)c->twx, (const CT*)c->twr, LPB,
@@ -1559,24 +1552,69 @@ cudaError_t launch_stats(ch3d_ctx* c) { return c->fp32 ? stats_t<float>(c) : sta
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CH3D_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[128] = {nullptr};
+// per device: the scratch array's device address and the kernels' shared-memory limits set
+PerDevice g_noalloc_site;
+void* g_noalloc_addr[kMaxDevices] = {nullptr};
+constexpr int kNoallocSmemLimit = 200 * 1024;
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 }  // namespace
 
+// Once per device (that device current): looks up the array's device address
+// and sets the dynamic shared-memory limit of the four kernels the solve runs.
 cudaError_t noalloc_scratch_address(int dev, void** out) {
-  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  cudaError_t e = once_per_device(g_noalloc_site, dev, [&] {
     void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
+    cudaError_t r = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (r != cudaSuccess) return r;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((r = cudaFuncSetAttribute(k_prsrc_xfft<double>, a, kNoallocSmemLimit)) != cudaSuccess) return r;
+    if ((r = cudaFuncSetAttribute(k_zfft<double>, a, kNoallocSmemLimit)) != cudaSuccess) return r;
+    if ((r = cudaFuncSetAttribute(k_ysolve<double>, a, kNoallocSmemLimit)) != cudaSuccess) return r;
+    if ((r = cudaFuncSetAttribute(k_xifft<double>, a, kNoallocSmemLimit)) != cudaSuccess) return r;
     g_noalloc_addr[dev] = p;
-  }
-  *out = g_noalloc_addr[dev];
-  return cudaSuccess;
+    return cudaSuccess;
+  });
+  if (e == cudaSuccess) *out = g_noalloc_addr[dev];
+  return e;
 }
+
+// Launch shapes of the allocation-free solve: x-transform lines per block,
+// z-transform kx lines per block, y-solve threads per system, and the dynamic
+// shared memory of the x, z and y kernels.
+struct NoallocShape {
+  int LPB, TKX, P, TS;
+  size_t smx, smz, smy;
+};
+static NoallocShape noalloc_shape(int nx, int ny, int nz) {
+  NoallocShape s;
+  const int M = nx / 2;
+  s.LPB = lines_per_block<double>(M);
+  int TKX = kFFTSmem / (2 * nz * (int)sizeof(double2));
+  int tk = 1;
+  while (tk * 2 <= TKX && tk * 2 <= 16) tk *= 2;
+  s.TKX = tk;
+  int P = 16;
+  while (P > 1 && ny < 2 * P) P >>= 1;
+  s.P = P;
+  s.TS = 8;
+  const int Q = P - 1;
+  s.smx = (size_t)2 * s.LPB * M * sizeof(double2);
+  s.smz = (size_t)2 * s.TKX * nz * sizeof(double2);
+  s.smy = (size_t)ny * s.TS * (sizeof(double2) + 2 * sizeof(double)) +
+          (size_t)s.TS * (Q > 0 ? Q : 1) * (2 * sizeof(double2) + 5 * sizeof(double)) + 16;
+  return s;
+}
+
+// Largest dynamic shared memory (bytes) one kernel of the solve of an
+// nx x ny x nz grid asks for; the solve runs only where it is within
+// noalloc_smem_limit().
+size_t noalloc_smem(int nx, int ny, int nz) {
+  const NoallocShape s = noalloc_shape(nx, ny, nz);
+  size_t m = s.smx > s.smz ? s.smx : s.smz;
+  return m > s.smy ? m : s.smy;
+}
+size_t noalloc_smem_limit() { return (size_t)kNoallocSmemLimit; }
 
 // Bytes of scratch the solve of an nx x ny x nz grid needs.
 size_t noalloc_bytes(int nx, int ny, int nz) {
@@ -1662,34 +1700,18 @@ cudaError_t poisson_noalloc(int nx, int ny, int nz, double xlx, double zlz, cons
   const double2* twz = tw + 2 * M + 1;
 
   // forward x transform of the source (mode 2: the source is read as is)
-  const int LPB = lines_per_block<double>(M);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_prsrc_xfft<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_zfft<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_ysolve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_xifft<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  const NoallocShape sh = noalloc_shape(nx, ny, nz);
+  const int LPB = sh.LPB, TKX = sh.TKX, P = sh.P, TS = sh.TS;
   const int nlines = ny * nz;
-  k_prsrc_xfft<double><<<(nlines + LPB - 1) / LPB, 256, (size_t)2 * LPB * M * sizeof(double2), st>>>(
-      g, m, d_src, d_src, d_src, spec, planx, twx, twr, LPB, 2, sc, nullptr);
-  int TKX = kFFTSmem / (2 * nz * (int)sizeof(double2));
-  int tk = 1;
-  while (tk * 2 <= TKX && tk * 2 <= 16) tk *= 2;
-  TKX = tk;
+  k_prsrc_xfft<double><<<(nlines + LPB - 1) / LPB, 256, sh.smx, st>>>(g, m, d_src, d_src, d_src, spec, planx, twx,
+                                                                      twr, LPB, 2, sc, nullptr);
   dim3 gz((nxh + TKX - 1) / TKX, ny);
-  const size_t smz = (size_t)2 * TKX * nz * sizeof(double2);
-  k_zfft<double><<<gz, 256, smz, st>>>(g, spec, planz, twz, TKX, 0, sc);
-  int P = 16;
-  while (P > 1 && ny < 2 * P) P >>= 1;
-  const int TS = 8, Q = P - 1;
-  const size_t smy = (size_t)ny * TS * (sizeof(double2) + 2 * sizeof(double)) +
-                     (size_t)TS * (Q > 0 ? Q : 1) * (2 * sizeof(double2) + 5 * sizeof(double)) + 16;
-  k_ysolve<double><<<dim3((nxh + TS - 1) / TS, nz), TS * P < 64 ? 64 : TS * P, smy, st>>>(g, m, wave, spec, TS, P, sc);
-  k_zfft<double><<<gz, 256, smz, st>>>(g, spec, planz, twz, TKX, 1, sc);
-  k_xifft<double><<<(nlines + LPB - 1) / LPB, 256, (size_t)2 * LPB * M * sizeof(double2), st>>>(
-      g, spec, d_phi, planx, twx, twr, LPB, 1.0 / ((double)nx * (double)nz), sc);
+  k_zfft<double><<<gz, 256, sh.smz, st>>>(g, spec, planz, twz, TKX, 0, sc);
+  k_ysolve<double><<<dim3((nxh + TS - 1) / TS, nz), TS * P < 64 ? 64 : TS * P, sh.smy, st>>>(g, m, wave, spec, TS, P,
+                                                                                              sc);
+  k_zfft<double><<<gz, 256, sh.smz, st>>>(g, spec, planz, twz, TKX, 1, sc);
+  k_xifft<double><<<(nlines + LPB - 1) / LPB, 256, sh.smx, st>>>(g, spec, d_phi, planx, twx, twr, LPB,
+                                                                 1.0 / ((double)nx * (double)nz), sc);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   // the host tables above are pageable and local to this call

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/ch3d_mlp.h"
+#include "ch3d_common.cuh"
 
 namespace ch3d_mlp {
 
@@ -384,6 +385,14 @@ constexpr size_t SMEM_BWD = 1024 + TILE * NH * 2 + TILE * TILE * 2 + NH * TILE *
 
 using namespace ch3d_mlp;
 
+// One-time attribute set-up per device a process drives (cudaFuncSetAttribute
+// applies to the current device only), under the library's set-up lock.
+template <class F> static bool setup_on_current_device(ch3d::PerDevice& site, F&& setup) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  return ch3d::once_per_device(site, dev, setup) == cudaSuccess;
+}
+
 extern "C" {
 
 CH3D_MLP_API size_t ch3d_mlp_workspace_bytes(int batch) {
@@ -392,26 +401,14 @@ CH3D_MLP_API size_t ch3d_mlp_workspace_bytes(int batch) {
          256;
 }
 
-// One-time attribute set-up per device a process drives (cudaFuncSetAttribute
-// applies to the current device only): true the first time for that device.
-static bool first_on_current_device(unsigned& mask) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
-  const unsigned bit = 1u << (dev & 31);
-  if (mask & bit) return false;
-  mask |= bit;
-  return true;
-}
-
 CH3D_MLP_API int ch3d_mlp_forward(const float* X, int batch, const float* params, float* Y, int* status,
                                   void* stream) {
   if (!X || !params || !Y || !status || batch <= 0) return 1;
-  static unsigned attr = 0u;  // devices set up
-  if (first_on_current_device(attr) &&
-      cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) != cudaSuccess) {
-    attr = 0u;  // set up again on the next call
+  static ch3d::PerDevice attr;
+  if (!setup_on_current_device(attr, [] {
+        return cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD);
+      }))
     return 2;
-  }
   k_mlp_fwd<<<(batch + TILE - 1) / TILE, TILE, SMEM_FWD, (cudaStream_t)stream>>>(X, batch, params, Y, nullptr, nullptr,
                                                                                 status);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
@@ -420,13 +417,14 @@ CH3D_MLP_API int ch3d_mlp_forward(const float* X, int batch, const float* params
 CH3D_MLP_API int ch3d_mlp_grad(const float* X, const float* T, int batch, const float* params, void* work,
                                float* grad, float* loss, int* status, void* stream) {
   if (!X || !T || !params || !work || !grad || !loss || !status || batch <= 0) return 1;
-  static unsigned attr = 0u;  // devices set up
-  if (first_on_current_device(attr) &&
-      (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) != cudaSuccess ||
-       cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BWD) != cudaSuccess)) {
-    attr = 0u;  // set up again on the next call
+  static ch3d::PerDevice attr;
+  if (!setup_on_current_device(attr, [] {
+        cudaError_t r = cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD);
+        if (r == cudaSuccess)
+          r = cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BWD);
+        return r;
+      }))
     return 2;
-  }
   cudaStream_t st = (cudaStream_t)stream;
   const int nb = (batch + TILE - 1) / TILE;
   unsigned char* w = (unsigned char*)work;

@@ -47,21 +47,42 @@ class ChannelSolver:
         assert a.size == self.cfg.npoints, "array size does not match the grid"
         return a
 
-    def upload(self, ux, uy, uz, p, hist=None):
-        ux, uy, uz, p = (self._arr(a) for a in (ux, uy, uz, p))
+    def layout_shape(self, layout):
+        """C-order shape of a host array of the given layout: interior
+        (nzc, nyc, nxc); GHOST2 the 2nd-order bounds (0:nxc+2, 0:nyc+2,
+        0:nzc+2); GHOST4 the 4th-order bounds (-1:nxc+2, 0:nyc+1, -1:nzc+2)."""
+        nx, ny, nz = self.cfg.nxc, self.cfg.nyc, self.cfg.nzc
+        if layout == _lib.LAYOUT_GHOST2:
+            return (nz + 3, ny + 3, nx + 3)
+        if layout == _lib.LAYOUT_GHOST4:
+            return (nz + 4, ny + 2, nx + 4)
+        return (nz, ny, nx)
+
+    def upload(self, ux, uy, uz, p, hist=None, layout=_lib.LAYOUT_INTERIOR):
+        n = int(np.prod(self.layout_shape(layout)))
+        fields = [np.ascontiguousarray(a, dtype=np.float64) for a in (ux, uy, uz, p)]
+        assert all(a.size == n for a in fields), "array size does not match the layout"
         h = None
         if hist is not None:
             h = np.ascontiguousarray(np.stack([self._arr(a) for a in hist]))
-        _lib.check(self.lib.ch3d_upload_state(self.ctx, _lib.LAYOUT_INTERIOR, _lib.dptr(ux), _lib.dptr(uy),
-                                              _lib.dptr(uz), _lib.dptr(p), _lib.dptr(h)), self.lib)
+        _lib.check(self.lib.ch3d_upload_state(self.ctx, int(layout), *(_lib.dptr(a) for a in fields), _lib.dptr(h)),
+                   self.lib)
 
-    def download(self, hist=False):
-        shp = self.cfg.shape
-        ux, uy, uz, p = (np.empty(shp) for _ in range(4))
-        h = np.empty((3,) + shp) if hist else None
-        _lib.check(self.lib.ch3d_download_state(self.ctx, _lib.LAYOUT_INTERIOR, _lib.dptr(ux), _lib.dptr(uy),
-                                                _lib.dptr(uz), _lib.dptr(p), _lib.dptr(h)), self.lib)
-        out = {"ux": ux, "uy": uy, "uz": uz, "p": p}
+    def download(self, hist=False, layout=_lib.LAYOUT_INTERIOR, out=None):
+        """Current state as {"ux", "uy", "uz", "p"[, "hist"]}.  With a ghosted
+        layout the ghost cells follow the reference's boundary and halo rules;
+        `out` may give the host arrays (their cells outside the rules keep
+        their values), else they start at zero."""
+        shp = self.layout_shape(layout)
+        if out is None:
+            out = {k: np.zeros(shp) for k in ("ux", "uy", "uz", "p")}
+        for k in ("ux", "uy", "uz", "p"):
+            a = out[k]
+            assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"] and a.size == int(np.prod(shp))
+        h = np.empty((3,) + self.cfg.shape) if hist else None
+        _lib.check(self.lib.ch3d_download_state(self.ctx, int(layout), *(_lib.dptr(out[k]) for k in ("ux", "uy", "uz",
+                                                                                                      "p")),
+                                                _lib.dptr(h)), self.lib)
         if hist:
             out["hist"] = h
         return out

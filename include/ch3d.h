@@ -3,7 +3,7 @@
  *
  * The Fortran host of the reference keeps its .prm input, its module call
  * sites and its restart/statistics layout, and binds these entry points
- * through ISO_C_BINDING (see INTEGRATION.md).  Every function returns an int
+ * through ISO_C_BINDING.  Every function returns an int
  * status (CH3D_OK = 0); the message of the last failure of a thread is
  * available from ch3d_last_error().  Arrays crossing this boundary are plain
  * host pointers to real(8) data in Fortran (column-major) order.
@@ -16,8 +16,12 @@
  *                          2nd-order solver (src/CFD_2nd/m_Variables.f90:59-61).
  *   CH3D_LAYOUT_GHOST4     (-1:nxc+2,0:nyc+1,-1:nzc+2), the `mb1` bounds of the
  *                          4th-order solver (src/CFD_4th/m_Variables.f90:47-49).
- * On download, ghost cells are filled by the boundary/halo rules of
- * SetBC_and_UpdateHalo (src/CFD_2nd/m_BC_and_Halo.f90:232-344).
+ * Upload reads the interior of a ghosted array.  On download, ghost cells
+ * are filled by the boundary rules and periodic halo copies of
+ * SetBC_and_UpdateHalo / SetBC_and_UpdateHalo_pr with each tree's halo
+ * widths (src/CFD_2nd/m_BC_and_Halo.f90:20-29,232-344,410-456;
+ * src/CFD_4th/m_BC_and_Halo.f90:24-46,51-96,136-150); cells those routines
+ * never write keep the values the host array had.
  *
  * Threading: one context = one CUDA stream on one device; a context is not
  * thread-safe, distinct contexts are independent.  Device memory is owned by

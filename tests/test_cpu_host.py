@@ -13,6 +13,13 @@ from helpers import small_channel
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+def _free_port():
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
 def test_library_exports_every_declared_symbol(built):
     from channel3d_b200 import _lib
     lib = _lib.load_library()
@@ -53,6 +60,29 @@ def test_invalid_configs_fail_cleanly(built):
     c = small_channel(16, 12, 8).to_c()
     h = ctypes.c_void_p()
     assert lib.ch3d_create(ctypes.byref(c), _lib.dptr(bad), ctypes.byref(h)) == _lib.CH3D_ERR_INVALID
+    c = small_channel(16, 12, 8, device=64).to_c()  # beyond the per-device set-up tables
+    assert lib.ch3d_create(ctypes.byref(c), _lib.dptr(yp), ctypes.byref(h)) == _lib.CH3D_ERR_INVALID
+    assert b"device 64" in lib.ch3d_last_error()
+
+
+def test_noalloc_argument_checks(built):
+    """ch3d_poisson_noalloc rejects, before touching the GPU, grids whose
+    spectrum exceeds its static scratch array and narrow tall grids whose
+    y-solve block would need more shared memory than its kernels may use."""
+    import ctypes
+    from channel3d_b200 import _lib
+    lib = _lib.load_library()
+    fake = ctypes.c_void_p(256)  # never dereferenced: the checks fail first
+    yp = np.linspace(0.0, 2.0, 257)
+    assert lib.ch3d_poisson_noalloc(512, 256, 512, 6.28, 3.14, _lib.dptr(yp), -1, -1, fake, fake,
+                                    None) == _lib.CH3D_ERR_INVALID
+    assert b"CH3D_NOALLOC_SCRATCH_BYTES" in lib.ch3d_last_error()
+    yp = np.linspace(0.0, 2.0, 801)
+    assert lib.ch3d_poisson_noalloc(4, 800, 2, 6.28, 3.14, _lib.dptr(yp), -1, -1, fake, fake,
+                                    None) == _lib.CH3D_ERR_UNSUPPORTED
+    assert b"shared memory" in lib.ch3d_last_error()
+    assert lib.ch3d_poisson_noalloc(4, 800, 2, 6.28, 3.14, _lib.dptr(yp), -1, 0, fake, fake,
+                                    None) == _lib.CH3D_ERR_UNSUPPORTED
 
 
 PRM = """
@@ -108,10 +138,14 @@ def test_prm_reader(tmp_path):
     assert abs(cfg.xnu - 3.5714e-4) < 1e-12
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/Input"), reason="reference decks not mounted")
+REF_DECKS = os.environ.get("CH3D_REFERENCE_INPUT", "")
+
+
+@pytest.mark.skipif(not REF_DECKS or not os.path.isdir(REF_DECKS),
+                    reason="set CH3D_REFERENCE_INPUT to the reference's Input/ folder to read its decks")
 def test_prm_reader_reads_reference_decks():
     from channel3d_b200 import ChannelConfig
-    cfg = ChannelConfig.from_prm("/root/reference/Input/TurbulentChannel_2nd.prm")
+    cfg = ChannelConfig.from_prm(os.path.join(REF_DECKS, "TurbulentChannel_2nd.prm"))
     assert (cfg.nxc, cfg.nyc, cfg.nzc) == (256, 150, 256)
     assert cfg.IsImplicit == 1 and cfg.BcOption == [0, 0, -1, -1, 0, 0]
     assert cfg.nycSection == [75, 75] and cfg.StretType == [1, 1]
@@ -140,7 +174,7 @@ def test_two_rank_reference_arm_on_cpu():
     the JSON line, rank 1 exits without work."""
     env = dict(os.environ, MASTER_ADDR="127.0.0.1", CUDA_VISIBLE_DEVICES="")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
-           "--master-addr", "127.0.0.1", "--master-port", "29533", os.path.join(ROOT, "bench.py"),
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), os.path.join(ROOT, "bench.py"),
            "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--workload", "channel48_les"]
     out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
@@ -168,8 +202,9 @@ def test_max_over_ranks_gloo(tmp_path):
         "print('RANK%%d %%d %%.1f' %% (rank, ws, v))\n" % ROOT)
     env = dict(os.environ, MASTER_ADDR="127.0.0.1", CUDA_VISIBLE_DEVICES="")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
-           "--master-addr", "127.0.0.1", "--master-port", "29541", str(script)]
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), str(script)]
     out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr[-2000:]
-    got = sorted(l for l in out.stdout.splitlines() if l.startswith("RANK"))
+    # the two ranks share the pipe, so their lines may interleave
+    got = sorted(re.findall(r"RANK\d \d+ [\d.]+", out.stdout))
     assert got == ["RANK0 2 15.0", "RANK1 2 15.0"], (got, out.stderr[-1000:])

@@ -665,7 +665,8 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
         cudaMalloc(&c->red2, CH3D_NRED * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->sc, sizeof(DevScalars)) != cudaSuccess)
       return cleanup(fail(CH3D_ERR_NOMEM, "partials"));
-    const size_t nstat = (size_t)35 * (c->ny + 1) + 1;  // SumStat(35, nyp) | PrGradsum
+    // SumStat(35, nyp) | PrGradsum [| SumGrad(98, nyp) of the 4th-order statistics]
+    const size_t nstat = (size_t)35 * (c->ny + 1) + 1 + (cfg->order == 4 ? (size_t)98 * (c->ny + 1) : 0);
     const int kch = (c->nz + 7) / 8, nch = (c->nz + kch - 1) / kch;
     if (cudaMalloc(&c->stat, nstat * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->statpart, (size_t)35 * (c->ny + 1) * nch * sizeof(double)) != cudaSuccess)
@@ -915,13 +916,15 @@ int ch3d_set_dt(ch3d_ctx* c, double dt) {
   return CH3D_OK;
 }
 
+static size_t stat_doubles(const ch3d_ctx* c) {
+  return (size_t)35 * (c->ny + 1) + 1 + (c->cfg.order == 4 ? (size_t)98 * (c->ny + 1) : 0);
+}
+
 int ch3d_stats_accumulate(ch3d_ctx* c) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
-  if (c->cfg.order != 2)
-    return fail(CH3D_ERR_UNSUPPORTED, "statistics are built for the 2nd-order solver (clcStat_CH)");
   CU(cudaSetDevice(c->device));
   if (!c->scalars_ready) { int rc = init_scalars(c); if (rc) return rc; }
-  CU(launch_stats(c));
+  CU(c->cfg.order == 4 ? launch_stats4(c) : launch_stats(c));
   CU(cudaStreamSynchronize(c->stream));
   c->nfstime += 1;
   return CH3D_OK;
@@ -938,10 +941,21 @@ int ch3d_stats_fetch(ch3d_ctx* c, double* sumstat, int* nfstime, double* prgrads
   if (prgradsum) *prgradsum = h[n];
   if (nfstime) *nfstime = c->nfstime;
   if (reset) {
-    CU(cudaMemsetAsync(c->stat, 0, (n + 1) * sizeof(double), c->stream));
+    CU(cudaMemsetAsync(c->stat, 0, stat_doubles(c) * sizeof(double), c->stream));
     CU(cudaStreamSynchronize(c->stream));
     c->nfstime = 0;
   }
+  return CH3D_OK;
+}
+
+int ch3d_stats_fetch_grad(ch3d_ctx* c, double* sumgrad) {
+  if (!c || !sumgrad) return fail(CH3D_ERR_INVALID, "NULL argument");
+  if (c->cfg.order != 4)
+    return fail(CH3D_ERR_UNSUPPORTED, "the gradient moments belong to the 4th-order statistics");
+  CU(cudaSetDevice(c->device));
+  const size_t off = (size_t)35 * (c->ny + 1) + 1, n = (size_t)98 * (c->ny + 1);
+  CU(cudaMemcpyAsync(sumgrad, c->stat + off, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
   return CH3D_OK;
 }
 

@@ -71,7 +71,7 @@ struct ch3d_ctx {
   int npart = 0;
   bool march = false;        // 2nd-order PIMP without LES: march kernels, npart_m partial sums in part
   int npart_m = 0;
-  double* stat = nullptr;    // SumStat(35, nyp) accumulator (FP64)
+  double* stat = nullptr;    // SumStat(35, nyp) | PrGradsum [| SumGrad(98, nyp), 4th order] (FP64)
   double* statpart = nullptr;
   int nfstime = 0;
   double prgradsum = 0;
@@ -132,6 +132,7 @@ cudaError_t launch_bulk_partials(ch3d_ctx* c);
 cudaError_t launch_diag(ch3d_ctx* c);
 int diag_npart(const ch3d_ctx* c);                     // partial sums k_diag writes to part2
 cudaError_t launch_stats(ch3d_ctx* c);
+cudaError_t launch_stats4(ch3d_ctx* c);
 cudaError_t launch_divmax(ch3d_ctx* c, unsigned long long* slot);
 cudaError_t launch_fill_row0(ch3d_ctx* c, int q, double v);  // field q: every j = 0 value := v
 cudaError_t launch_convert(ch3d_ctx* c, const void* src, void* dst, long long n, int to_f32);  // FP64 <-> FP32

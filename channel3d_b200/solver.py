@@ -159,6 +159,12 @@ class ChannelSolver:
                    self.lib)
         return s.reshape(self.cfg.nyc + 1, 35), n.value, pg.value
 
+    def stats_fetch_grad(self):
+        """4th order: SumGrad(98, nyp) as (nyp, 98) (the vGrad moment sums)."""
+        g = np.empty((self.cfg.nyc + 1) * 98)
+        _lib.check(self.lib.ch3d_stats_fetch_grad(self.ctx, _lib.dptr(g)), self.lib)
+        return g.reshape(self.cfg.nyc + 1, 98)
+
     def kernel_times(self, nsteps=1):
         out = np.zeros(7)
         _lib.check(self.lib.ch3d_kernel_times(self.ctx, int(nsteps), _lib.dptr(out), 7), self.lib)

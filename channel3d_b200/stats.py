@@ -1,25 +1,41 @@
-"""Channel statistics of clcStat_CH (src/CFD_2nd/m_FlowType_Channel.f90:175-362):
-35 plane-averaged moments per y row (rows 1..nyp), accumulated on the device,
-the stats<itime> file writer, and derived profiles (mean U(y), rms, Re_tau)."""
+"""Channel statistics: the moments of clcStat_CH (2nd order,
+src/CFD_2nd/m_FlowType_Channel.f90:175-362) and of clcStat (4th order,
+src/CFD_4th/m_FlowCase.f90:330-998), 35 plane-averaged moments per y row (rows
+1..nyp) plus, for the 4th order, 98 gradient moments; accumulated on the
+device.  The stats<itime> and vGrad<itime> file writers, and derived profiles
+(mean U(y), rms, Re_tau)."""
 import numpy as np
 
 NSTAT = 35
+NGRAD = 98
 
 
-def write_stats(path, sumstat, nfstime, prgradsum, itime, ivstats, is_ux_const=True):
-    """stats%10.10d in the reference's text layout (:333-360)."""
+def write_stats(path, sumstat, nfstime, prgradsum, itime, ivstats, is_ux_const=True, order=2):
+    """stats%10.10d in the reference's text layout (2nd order :333-360; the 4th
+    order writes the magnitude of the mean pressure gradient,
+    src/CFD_4th/m_FlowCase.f90:958-980)."""
     inf = 1.0 / nfstime
     with open(path, "w") as f:
         f.write("  The time step range for this fluid statistics is %7d:%7d:%7d\n"
                 % (itime - (nfstime - 1) * ivstats, ivstats, itime))
         f.write("  \n")
         if is_ux_const:
+            pg = abs(prgradsum) if order == 4 else prgradsum
             f.write("  Constant velocity in x-dir by adding a pressure gradient.\n")
-            f.write("    time averaged pressure gradient is: %24.15E\n" % (prgradsum * inf))
+            f.write("    time averaged pressure gradient is: %24.15E\n" % (pg * inf))
         else:
             f.write("  Variable velocity in x-dir while adding a constant body force.\n")
         f.write("  \n")
         for row in np.asarray(sumstat).reshape(-1, NSTAT):
+            f.write("".join("%24.15E" % (v * inf) for v in row) + "\n")
+
+
+def write_vgrad(path, sumgrad, nfstime):
+    """vGrad%10.10d of the 4th order (src/CFD_4th/m_FlowCase.f90:983-997): per
+    row jc = 1..nyp the 98 gradient moments / nfstime."""
+    inf = 1.0 / nfstime
+    with open(path, "w") as f:
+        for row in np.asarray(sumgrad).reshape(-1, NGRAD):
             f.write("".join("%24.15E" % (v * inf) for v in row) + "\n")
 
 

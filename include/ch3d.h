@@ -184,12 +184,19 @@ CH3D_API int ch3d_project(ch3d_ctx* ctx, double* divmax_before, double* divmax_a
 /* Sets dt (iCFL = 2 runs only use dtMax). */
 CH3D_API int ch3d_set_dt(ch3d_ctx* ctx, double dt);
 
-/* Statistics: clcStat_CH moment sums (src/CFD_2nd/m_FlowType_Channel.f90:175-330),
-   accumulated on the device in FP64; fetch returns SumStat(35,nyp) in
-   Fortran order, nfstime and PrGradsum, and optionally resets them. */
+/* Statistics: the moment sums of clcStat_CH (2nd order,
+   src/CFD_2nd/m_FlowType_Channel.f90:175-330) or clcStat (4th order,
+   src/CFD_4th/m_FlowCase.f90:330-640), accumulated on the device in FP64;
+   fetch returns SumStat(35,nyp) in Fortran order, nfstime and PrGradsum,
+   and optionally resets them (the gradient moments of the 4th order too). */
 CH3D_API int ch3d_stats_accumulate(ch3d_ctx* ctx);
 CH3D_API int ch3d_stats_fetch(ch3d_ctx* ctx, double* sumstat, int* nfstime,
                      double* prgradsum, int reset);
+
+/* 4th order: the gradient moments SumGrad(98,nyp) of clcStat
+   (HighOrderGradStat, src/CFD_4th/m_FlowCase.f90:485-589, the vGrad file's
+   sums), Fortran order.  Fetch them before a resetting ch3d_stats_fetch. */
+CH3D_API int ch3d_stats_fetch_grad(ch3d_ctx* ctx, double* sumgrad);
 
 /* LES: computes nut from the current velocity as the step does once per
    step, Clc_SGS_Vis (src/CFD_2nd/m_LESModels.f90:47-62) followed by the wall

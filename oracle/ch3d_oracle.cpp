@@ -231,6 +231,7 @@ struct Oracle {
 
   // statistics (m_FlowType_Channel)
   std::vector<double> SumStat;  // (35, nyp)
+  std::vector<double> SumGrad;  // (98, nyp), 4th order (src/CFD_4th/m_FlowCase.f90:24-26)
   int nfstime = 0;
   double PrGradsum = 0;
 
@@ -1902,6 +1903,133 @@ struct Oracle {
     nfstime += 1;
   }
 
+  // ---- src/CFD_4th/m_FlowCase.f90:330-640 (clcStat moments: SumStat(35,nyp) and, with
+  //      HighOrderGradStat defined at :17, SumGrad(98,nyp)); the spectra branch
+  //      (:642-) is separate.  pressure(nxc+2,:,:) and pressure(:,:,nzc+2) are never
+  //      written by SetBC_and_UpdateHalo_pr (halo xph = zph = 1,
+  //      src/CFD_4th/m_BC_and_Halo.f90:42-45), so dpdxx and dpdzz read the zero the
+  //      array was allocated with (src/CFD_4th/m_Variables.f90:85) there. ----
+  void clcStat4() {
+    const double rdxt = rdx / 12.0, rdzt = rdz / 12.0;
+    const double inxz = one / ((double)nxc * (double)nzc);
+    if (SumGrad.empty()) SumGrad.assign((size_t)98 * nyp, 0.0);
+    for (int jc = 1; jc <= nyc; ++jc) {
+      const int jp = jc + 1, jm = jc - 1;
+      const double InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+      const double cac = rdyc(jc), cacU = rdyc(jp), caj = rdyp(jc);
+      double S[35] = {0}, G[98] = {0};
+      for (int kc = 1; kc <= nzc; ++kc) {
+        const int ks = kc - 2, km = kc - 1, kp = kc + 1, ku = kc + 2;
+        for (int ic = 1; ic <= nxc; ++ic) {
+          const int is = ic - 2, im = ic - 1, ip = ic + 1, iu = ic + 2;
+          const F3 &U = ux, &V = uy, &W = uz, &pr = pressure;
+          double uxloc = U(ic, jc, kc) + uCRF, uyloc = V(ic, jc, kc), uzloc = W(ic, jc, kc), prloc = pr(ic, jc, kc);
+          double uxCell = InterpCoe1 * U(im, jc, kc) + InterpCoe2 * U(ic, jc, kc) + InterpCoe3 * U(ip, jc, kc) + InterpCoe4 * U(iu, jc, kc) + uCRF;
+          double uyCell = (uyloc + V(ic, jp, kc)) * half;
+          double uy_xc = InterpCoe1 * V(is, jc, kc) + InterpCoe2 * V(im, jc, kc) + InterpCoe3 * V(ic, jc, kc) + InterpCoe4 * V(ip, jc, kc);
+          double uy_xp = InterpCoe1 * V(is, jp, kc) + InterpCoe2 * V(im, jp, kc) + InterpCoe3 * V(ic, jp, kc) + InterpCoe4 * V(ip, jp, kc);
+          double uzCell = InterpCoe1 * W(ic, jc, km) + InterpCoe2 * W(ic, jc, kc) + InterpCoe3 * W(ic, jc, kp) + InterpCoe4 * W(ic, jc, ku);
+          double prloc2 = InterpY1 * (InterpCoe1 * pr(is, jm, kc) + InterpCoe2 * pr(im, jm, kc) +
+                                      InterpCoe3 * pr(ic, jm, kc) + InterpCoe4 * pr(ip, jm, kc)) +
+                          InterpY2 * (InterpCoe1 * pr(is, jc, kc) + InterpCoe2 * pr(im, jc, kc) +
+                                      InterpCoe3 * pr(ic, jc, kc) + InterpCoe4 * pr(ip, jc, kc));
+          double dudx = dxCoe1 * U(im, jc, kc) + dxCoe2 * U(ic, jc, kc) + dxCoe3 * U(ip, jc, kc) + dxCoe4 * U(iu, jc, kc);
+          double dudy = (U(ic, jc, kc) - U(ic, jm, kc)) * cac;
+          double dudz = dzCoe1 * U(ic, jc, ks) + dzCoe2 * U(ic, jc, km) + dzCoe3 * U(ic, jc, kc) + dzCoe4 * U(ic, jc, kp);
+          double dvdx = dxCoe1 * V(is, jc, kc) + dxCoe2 * V(im, jc, kc) + dxCoe3 * V(ic, jc, kc) + dxCoe4 * V(ip, jc, kc);
+          double dvdy = (V(ic, jp, kc) - uyloc) * caj;
+          double dvdz = dzCoe1 * V(ic, jc, ks) + dzCoe2 * V(ic, jc, km) + dzCoe3 * V(ic, jc, kc) + dzCoe4 * V(ic, jc, kp);
+          double dwdx = dxCoe1 * W(is, jc, kc) + dxCoe2 * W(im, jc, kc) + dxCoe3 * W(ic, jc, kc) + dxCoe4 * W(ip, jc, kc);
+          double dwdy = (uzloc - W(ic, jm, kc)) * cac;
+          double dwdz = dzCoe1 * W(ic, jc, km) + dzCoe2 * W(ic, jc, kc) + dzCoe3 * W(ic, jc, kp) + dzCoe4 * W(ic, jc, ku);
+          double dudxx = dxxCoe1 * U(is, jc, kc) + dxxCoe2 * U(im, jc, kc) + dxxCoe3 * U(ic, jc, kc) + dxxCoe4 * U(ip, jc, kc) + dxxCoe5 * U(iu, jc, kc);
+          double dudyy = ap2c(jc) * U(ic, jp, kc) + ac2c(jc) * U(ic, jc, kc) + am2c(jc) * U(ic, jm, kc);
+          double dudzz = dzzCoe1 * U(ic, jc, ks) + dzzCoe2 * U(ic, jc, km) + dzzCoe3 * U(ic, jc, kc) + dzzCoe4 * U(ic, jc, kp) + dzzCoe5 * U(ic, jc, ku);
+          double dvdxx = dxxCoe1 * V(is, jc, kc) + dxxCoe2 * V(im, jc, kc) + dxxCoe3 * V(ic, jc, kc) + dxxCoe4 * V(ip, jc, kc) + dxxCoe5 * V(iu, jc, kc);
+          double dvdyy = ap2p(jc) * V(ic, jp, kc) + ac2p(jc) * V(ic, jc, kc) + am2p(jc) * V(ic, jm, kc);
+          double dvdzz = dzzCoe1 * V(ic, jc, ks) + dzzCoe2 * V(ic, jc, km) + dzzCoe3 * V(ic, jc, kc) + dzzCoe4 * V(ic, jc, kp) + dzzCoe5 * V(ic, jc, ku);
+          double dwdxx = dxxCoe1 * W(is, jc, kc) + dxxCoe2 * W(im, jc, kc) + dxxCoe3 * W(ic, jc, kc) + dxxCoe4 * W(ip, jc, kc) + dxxCoe5 * W(iu, jc, kc);
+          double dwdyy = ap2c(jc) * W(ic, jp, kc) + ac2c(jc) * W(ic, jc, kc) + am2c(jc) * W(ic, jm, kc);
+          double dwdzz = dzzCoe1 * W(ic, jc, ks) + dzzCoe2 * W(ic, jc, km) + dzzCoe3 * W(ic, jc, kc) + dzzCoe4 * W(ic, jc, kp) + dzzCoe5 * W(ic, jc, ku);
+          double vor_x = dwdy - dvdz, vor_y = dudz - dwdx, vor_z = dvdx - dudy;
+          double dudxC = (-U(iu, jc, kc) + 8.0 * U(ip, jc, kc) - 8.0 * U(im, jc, kc) + U(is, jc, kc)) * rdxt;
+          double dvdxU = dxCoe1 * V(is, jp, kc) + dxCoe2 * V(im, jp, kc) + dxCoe3 * V(ic, jp, kc) + dxCoe4 * V(ip, jp, kc);
+          double dudyU = (U(ic, jp, kc) - U(ic, jc, kc)) * cacU;
+          double dudzC = (InterpY1 * (-U(ic, jm, ku) + 8.0 * U(ic, jm, kp) - 8.0 * U(ic, jm, km) + U(ic, jm, ks)) +
+                          InterpY2 * (-U(ic, jc, ku) + 8.0 * U(ic, jc, kp) - 8.0 * U(ic, jc, km) + U(ic, jc, ks))) * rdzt;
+          double dvdzC = ((-V(is, jc, ku) + 8.0 * V(is, jc, kp) - 8.0 * V(is, jc, km) + V(is, jc, ks)) * InterpCoe1 +
+                          (-V(im, jc, ku) + 8.0 * V(im, jc, kp) - 8.0 * V(im, jc, km) + V(im, jc, ks)) * InterpCoe2 +
+                          (-V(ic, jc, ku) + 8.0 * V(ic, jc, kp) - 8.0 * V(ic, jc, km) + V(ic, jc, ks)) * InterpCoe3 +
+                          (-V(ip, jc, ku) + 8.0 * V(ip, jc, kp) - 8.0 * V(ip, jc, km) + V(ip, jc, ks)) * InterpCoe4) * rdzt;
+          S[0] += uxloc; S[1] += uyloc; S[2] += uzloc; S[3] += prloc;
+          S[4] += uxloc * uxloc; S[5] += uyloc * uyloc; S[6] += uzloc * uzloc; S[7] += prloc * prloc;
+          S[8] += uxCell * uyCell; S[9] += uyCell * uzCell; S[10] += uxCell * uzCell;
+          S[11] += uxCell * prloc; S[12] += uyCell * prloc; S[13] += uzCell * prloc;
+          S[14] += uxCell * uxCell * uyCell; S[15] += uyloc * uyloc * uyloc; S[16] += uzCell * uzCell * uyCell;
+          S[17] += uxCell * uyCell * uyCell; S[18] += uxloc * uxloc * uxloc; S[19] += uzloc * uzloc * uzloc;
+          S[20] += uxloc * uxloc * uxloc * uxloc; S[21] += uyloc * uyloc * uyloc * uyloc; S[22] += uzloc * uzloc * uzloc * uzloc;
+          S[23] += prloc * dudx; S[24] += prloc * dvdy; S[25] += prloc * dwdz;
+          S[26] += prloc2 * (dudy + dvdx);
+          S[27] += uxloc * (dudxx + dudyy + dudzz); S[28] += uyloc * (dvdxx + dvdyy + dvdzz); S[29] += uzloc * (dwdxx + dwdyy + dwdzz);
+          S[30] += (dudxC * (dvdxU + dvdx) + (dudyU + dudy) * (uy_xp - uy_xc) * caj) * half;
+          S[31] += dudzC * dvdzC;
+          S[32] += vor_x * vor_x; S[33] += vor_y * vor_y; S[34] += vor_z * vor_z;
+          // pressure gradients (:485-490)
+          double dpdx = dxCoe1 * pr(is, jc, kc) + dxCoe2 * pr(im, jc, kc) + dxCoe3 * pr(ic, jc, kc) + dxCoe4 * pr(ip, jc, kc);
+          double dpdy = (pr(ic, jc, kc) - pr(ic, jm, kc)) * cac;
+          double dpdz = dzCoe1 * pr(ic, jc, ks) + dzCoe2 * pr(ic, jc, km) + dzCoe3 * pr(ic, jc, kc) + dzCoe4 * pr(ic, jc, kp);
+          double dpdxx = dxxCoe1 * pr(is, jc, kc) + dxxCoe2 * pr(im, jc, kc) + dxxCoe3 * pr(ic, jc, kc) + dxxCoe4 * pr(ip, jc, kc) + dxxCoe5 * pr(iu, jc, kc);
+          double dpdyy = ap2c(jc) * pr(ic, jp, kc) + ac2c(jc) * pr(ic, jc, kc) + am2c(jc) * pr(ic, jm, kc);
+          double dpdzz = dzzCoe1 * pr(ic, jc, ks) + dzzCoe2 * pr(ic, jc, km) + dzzCoe3 * pr(ic, jc, kc) + dzzCoe4 * pr(ic, jc, kp) + dzzCoe5 * pr(ic, jc, ku);
+          G[0] += prloc * prloc * prloc;
+          G[1] += prloc * prloc * prloc * prloc;
+          // SumVec2(3..98): the first four powers of each gradient, in the order of :496-589
+          const double q[24] = {dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz, dpdx, dpdy, dpdz,
+                                dudxx, dudyy, dudzz, dvdxx, dvdyy, dvdzz, dwdxx, dwdyy, dwdzz, dpdxx, dpdyy, dpdzz};
+          for (int t = 0; t < 24; ++t) {
+            const double a = q[t];
+            G[2 + 4 * t] += a;
+            G[3 + 4 * t] += a * a;
+            G[4 + 4 * t] += a * a * a;
+            G[5 + 4 * t] += a * a * a * a;
+          }
+        }
+      }
+      for (int t = 0; t < 35; ++t) SumStat[(size_t)t + 35 * (size_t)(jc - 1)] += S[t] * inxz;
+      for (int t = 0; t < 98; ++t) SumGrad[(size_t)t + 98 * (size_t)(jc - 1)] += G[t] * inxz;
+    }
+    {  // nyp only (:594-631)
+      const int jc = nyp, jm = jc - 1;
+      const double cac = rdyc(jc), InterpY1 = YinterpCoe(jc), InterpY2 = one - InterpY1;
+      double S26 = 0, S32 = 0, S34 = 0, G[8] = {0};
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          const int is = ic - 2, im = ic - 1, ip = ic + 1;
+          const F3& pr = pressure;
+          double prloc2 = InterpY1 * (InterpCoe1 * pr(is, jm, kc) + InterpCoe2 * pr(im, jm, kc) + InterpCoe3 * pr(ic, jm, kc) + InterpCoe4 * pr(ip, jm, kc)) +
+                          InterpY2 * (InterpCoe1 * pr(is, jc, kc) + InterpCoe2 * pr(im, jc, kc) + InterpCoe3 * pr(ic, jc, kc) + InterpCoe4 * pr(ip, jc, kc));
+          double dudy = (ux(ic, jc, kc) - ux(ic, jm, kc)) * cac;
+          double dwdy = (uz(ic, jc, kc) - uz(ic, jm, kc)) * cac;
+          double vor_x = dwdy, vor_z = -dudy;
+          S26 += prloc2 * (dudy + zero);
+          S32 += vor_x * vor_x;
+          S34 += vor_z * vor_z;
+          G[0] += dudy; G[1] += dudy * dudy; G[2] += dudy * dudy * dudy; G[3] += dudy * dudy * dudy * dudy;
+          G[4] += dwdy; G[5] += dwdy * dwdy; G[6] += dwdy * dwdy * dwdy; G[7] += dwdy * dwdy * dwdy * dwdy;
+        }
+      const size_t r = (size_t)(jc - 1);
+      SumStat[26 + 35 * r] += S26 * inxz;
+      SumStat[32 + 35 * r] += S32 * inxz;
+      SumStat[34 + 35 * r] += S34 * inxz;
+      for (int t = 0; t < 4; ++t) {
+        SumGrad[6 + t + 98 * r] += G[t] * inxz;      // SumVec2(7..10): dudy
+        SumGrad[30 + t + 98 * r] += G[4 + t] * inxz; // SumVec2(31..34): dwdy
+      }
+    }
+    PrGradsum = PrGradsum + PrGradAver;
+    nfstime += 1;
+  }
+
   F3* field(int id) {
     switch (id) {
       case 0: return &ux; case 1: return &uy; case 2: return &uz; case 3: return &pressure;
@@ -2065,7 +2193,19 @@ void orc_hc2r(int n, double* x) {
   hc2r(pl, x, a, b);
 }
 
-void orc_stats_accumulate(void* h) { ((Oracle*)h)->clcStat_CH(); }
+void orc_stats_accumulate(void* h) {
+  Oracle* o = (Oracle*)h;
+  if (o->o4) o->clcStat4();
+  else o->clcStat_CH();
+}
+
+// SumGrad(98,nyp) of the 4th-order statistics (zeros before the first accumulation);
+// returns nfstime.
+int orc_stats_get_grad(void* h, double* sumgrad) {
+  Oracle* o = (Oracle*)h;
+  for (size_t q = 0; q < (size_t)98 * o->nyp; ++q) sumgrad[q] = o->SumGrad.empty() ? 0.0 : o->SumGrad[q];
+  return o->nfstime;
+}
 
 // SumStat (35 x nyp, Fortran order), nfstime and PrGradsum.
 int orc_stats_get(void* h, double* sumstat, double* prgradsum) {

@@ -85,6 +85,8 @@ def lib():
         L.orc_stats_accumulate.argtypes = [ctypes.c_void_p]
         L.orc_stats_get.restype = ctypes.c_int
         L.orc_stats_get.argtypes = [ctypes.c_void_p, _DP, _DP]
+        L.orc_stats_get_grad.restype = ctypes.c_int
+        L.orc_stats_get_grad.argtypes = [ctypes.c_void_p, _DP]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_sgs.restype = ctypes.c_double
         L.orc_sgs.argtypes = [ctypes.c_void_p]
@@ -232,6 +234,12 @@ class Oracle:
         pg = ctypes.c_double()
         n = self.L.orc_stats_get(self.h, _p(s), ctypes.byref(pg))
         return s.reshape(self.cfg.nyc + 1, 35), n, pg.value
+
+    def stats_get_grad(self):
+        """4th order: SumGrad(98, nyp) as (nyp, 98), and nfstime."""
+        g = np.empty(98 * (self.cfg.nyc + 1))
+        n = self.L.orc_stats_get_grad(self.h, _p(g))
+        return g.reshape(self.cfg.nyc + 1, 98), n
 
 
 def r2hc(x):

@@ -169,6 +169,32 @@ def test_restart_roundtrip_and_size_check(tmp_path):
         restart.read_restart(path, cfg)
 
 
+def test_stats_writers(tmp_path):
+    """The stats file of both trees and the 4th order's vGrad file: one line per
+    row jc = 1..nyp, 35 / 98 values of 24 characters, averaged over nfstime;
+    the 4th-order header writes the magnitude of the mean pressure gradient
+    (src/CFD_4th/m_FlowCase.f90:958-997)."""
+    from channel3d_b200 import stats
+    nyp = 7
+    s = np.arange(35 * nyp, dtype=float).reshape(nyp, 35)
+    g = -np.arange(98 * nyp, dtype=float).reshape(nyp, 98)
+    for order in (2, 4):
+        p = tmp_path / ("stats%d" % order)
+        stats.write_stats(str(p), s * 4, 4, -0.8, itime=400, ivstats=100, order=order)
+        lines = p.read_text().splitlines()
+        assert lines[0] == "  The time step range for this fluid statistics is     100:    100:    400"
+        pg = float(lines[3].split()[-1])
+        assert pg == (0.2 if order == 4 else -0.2)
+        rows = lines[5:]
+        assert len(rows) == nyp and all(len(r) == 35 * 24 for r in rows)
+        assert np.allclose(np.array([[float(r[24 * q:24 * q + 24]) for q in range(35)] for r in rows]), s)
+    p = tmp_path / "vGrad"
+    stats.write_vgrad(str(p), g * 2, 2)
+    rows = p.read_text().splitlines()
+    assert len(rows) == nyp and all(len(r) == 98 * 24 for r in rows)
+    assert np.allclose(np.array([[float(r[24 * q:24 * q + 24]) for q in range(98)] for r in rows]), g)
+
+
 def test_two_rank_reference_arm_on_cpu():
     """bench.py --impl reference under torchrun with 2 gloo ranks: rank 0 prints
     the JSON line, rank 1 exits without work."""

@@ -141,8 +141,8 @@ class Oracle:
     def __init__(self, cfg):
         self.L = lib()
         self.cfg = cfg
-        self.P = params_from(cfg)
-        self.h = self.L.orc_create(ctypes.byref(self.P))
+        self.params = params_from(cfg)
+        self.h = self.L.orc_create(ctypes.byref(self.params))
         if not self.h:
             raise ValueError("oracle rejected the configuration")
         self.shape = (cfg.nzc, cfg.nyc, cfg.nxc)

@@ -57,7 +57,7 @@ def test_ghosted_layout_matches_oracle_arrays(built, name):
     yp, st = _start(cfg)
     o = O.Oracle(cfg)
     o.set_state(*st)
-    ids = {"ux": o.UX, "uy": o.UY, "uz": o.UZ, "p": o.P}
+    ids = {"ux": O.Oracle.UX, "uy": O.Oracle.UY, "uz": O.Oracle.UZ, "p": O.Oracle.P}  # array ids of orc_get_array
     with ChannelSolver(cfg, yp=yp) as s:
         shp = s.layout_shape(layout)
         # the host passes its ghosted arrays as they are (the oracle's, here)

@@ -629,6 +629,21 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     if (march_table_reset(c) != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "march table"));
   }
   {
+    // mixed path: low modes kept in FP64: kx < TSy, |kz| <= KL (KL < nz/2 so the two kz ranges are disjoint)
+    c->KL = 8;
+    if (c->KL > c->nz / 2 - 1) c->KL = c->nz / 2 - 1;
+    if (c->KL < 0) c->KL = 0;
+    c->ychunk = ychunk_usable(c);
+  }
+  if (c->ychunk) {
+    // partitioned y solve: factors on the fly from cp at the chunk boundaries
+    const size_t nb = ychunk_bound_doubles(c);
+    if (cudaMalloc(&c->yB, nb * sizeof(double)) != cudaSuccess)
+      return cleanup(fail(CH3D_ERR_NOMEM, "Poisson chunk factors"));
+    c->bytes += (long long)nb * sizeof(double);
+    e = launch_ysolve_factors(c);
+    if (e != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "Poisson factors: %s", cudaGetErrorString(e)));
+  } else {
     // Poisson y-solve (Thomas) factors per (kx, |kz|), computed once
     const size_t nrow = (size_t)(c->nz / 2 + 1) * c->ny * c->nxh;
     const size_t fw = c->fp32 ? sizeof(float) : sizeof(double);
@@ -636,10 +651,6 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
       return cleanup(fail(CH3D_ERR_NOMEM, "Poisson factors"));
     c->bytes += (long long)(2 * nrow) * fw;
     if (c->fp32) {
-      // low modes kept in FP64: kx < TSy, |kz| <= KL (KL < nz/2 so the two kz ranges are disjoint)
-      c->KL = 8;
-      if (c->KL > c->nz / 2 - 1) c->KL = c->nz / 2 - 1;
-      if (c->KL < 0) c->KL = 0;
       const size_t lr = (size_t)(c->KL + 1) * c->ny * c->TSy;
       const size_t ls = (size_t)(2 * c->KL + 1) * c->TSy * c->ny * 2;  // FP64 complex sweep scratch
       if (cudaMalloc(&c->yRM64, lr * sizeof(double)) != cudaSuccess ||
@@ -694,7 +705,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   if (c->les_delta) cudaFree(c->les_delta);
   void* mbufs[] = {c->mlp_params, c->mlp_x, c->mlp_y, c->mlp_fb, c->mlp_status, c->sgs_tau, c->sgs_f};
   for (void* b : mbufs) if (b) cudaFree(b);
-  void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yB, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1098,6 +1109,25 @@ int ch3d_poisson_noalloc(int nxc, int nyc, int nzc, double xlx, double zlz, cons
   cudaError_t e = poisson_noalloc(nxc, nyc, nzc, xlx, zlz, yp, bc_ym, bc_yp, d_src, d_phi, (cudaStream_t)stream, px, pz);
   if (e != cudaSuccess) return fail(CH3D_ERR_CUDA, "ch3d_poisson_noalloc: %s", cudaGetErrorString(e));
   return CH3D_OK;
+}
+
+int ch3d_interp_state(ch3d_ctx* dst, const ch3d_ctx* src) {
+  if (!dst || !src || dst == src) return fail(CH3D_ERR_INVALID, "need two distinct contexts");
+  if (dst->device != src->device) return fail(CH3D_ERR_INVALID, "both contexts must be on one device");
+  if (dst->fp32 != src->fp32) return fail(CH3D_ERR_INVALID, "both contexts must have the same precision");
+  if (std::fabs(dst->cfg.yly - src->cfg.yly) > 1e-12 * std::fabs(src->cfg.yly))
+    return fail(CH3D_ERR_INVALID, "yly differs (%g, %g): the resampling keeps the channel height", src->cfg.yly,
+                dst->cfg.yly);
+  CU(cudaSetDevice(dst->device));
+  const cudaError_t e = launch_interp_state(dst, src);
+  if (e == cudaErrorInvalidValue) return fail(CH3D_ERR_INVALID, "a new y point lies outside the old grid");
+  if (e != cudaSuccess) return fail(CH3D_ERR_CUDA, "ch3d_interp_state: %s", cudaGetErrorString(e));
+  // as a restart read of the resampled field: Hist zero, the wall row of uy, fresh scalars
+  const size_t word = dst->fp32 ? sizeof(float) : sizeof(double);
+  for (int q = 4; q < 7; ++q) CU(cudaMemsetAsync(dst->f[q], 0, (size_t)dst->N * word, dst->stream));
+  CU(launch_fill_row0(dst, 1, dst->cfg.uyBcValue[2]));
+  CU(cudaStreamSynchronize(dst->stream));
+  return init_scalars(dst);
 }
 
 int ch3d_last_step_ms(ch3d_ctx* c, double* ms) {

@@ -159,6 +159,11 @@ class ChannelSolver:
                    self.lib)
         return s.reshape(self.cfg.nyc + 1, 35), n.value, pg.value
 
+    def interp_from(self, src):
+        """Resamples another solver's state onto this grid (the reference's
+        interpolateField tool, Interp_uvwp) and makes it this solver's state."""
+        _lib.check(self.lib.ch3d_interp_state(self.ctx, src.ctx), self.lib)
+
     def stats_fetch_grad(self):
         """4th order: SumGrad(98, nyp) as (nyp, 98) (the vGrad moment sums)."""
         g = np.empty((self.cfg.nyc + 1) * 98)

@@ -264,6 +264,18 @@ CH3D_API int ch3d_poisson_noalloc(int nxc, int nyc, int nzc, double xlx, double 
                                   const double* yp, int bc_ym, int bc_yp,
                                   const double* d_src, double* d_phi, void* stream);
 
+/* Resamples the state of `src` onto the grid of `dst` and makes it dst's
+   state, as the reference's interpolateField tool does between restart files
+   (Interp_init / Interp_uvwp, Tool/interpolateField/src/m_Interp.f90:20-361):
+   ux, uy, uz and p interpolated trilinearly at their own staggered positions
+   of the new grid from the old field and its ghost cells
+   (Tool/interpolateField/src/m_BC_and_Halo.f90:21-340), x and z in
+   coordinates normalised by the domain lengths, y physical (the two grids
+   share yly); ux rescaled to dst's ubulk when dst holds the flow rate
+   (IsUxConst, :225-236).  dst's Hist is zero afterwards (an RK3 restart).
+   Both contexts on one device, same precision. */
+CH3D_API int ch3d_interp_state(ch3d_ctx* dst, const ch3d_ctx* src);
+
 /* Time of the last ch3d_step call's kernels, measured with CUDA events on the
    context's stream (milliseconds). */
 CH3D_API int ch3d_last_step_ms(ch3d_ctx* ctx, double* ms);

@@ -2157,6 +2157,133 @@ long long orc_set_array(void* h, int id, const double* in) {
 
 void orc_set_dt(void* h, double dt) { ((Oracle*)h)->dt = dt; }
 
+// ---- Tool/interpolateField/src/m_Interp.f90:20-179 (Interp_init, one rank) and
+//      :184-361 (Interp_uvwp): trilinear resampling of the state of `src` onto the
+//      grid of `dst` (same yly; x and z in coordinates normalised by the domain
+//      length, Tool/interpolateField/src/m_MeshAndMetries.f90:40-59), with the
+//      tool's ghost rules on the old grid (Tool/interpolateField/src/m_BC_and_Halo.f90:
+//      21-340, periodic x and z), ux rescaled to ubulk when IsUxConst.  The result
+//      becomes dst's state (as a restart read, orc_set_state; Hist zero). ----
+void orc_interp(void* hdst, void* hsrc) {
+  Oracle* N = (Oracle*)hdst;
+  Oracle* O = (Oracle*)hsrc;
+  const int nxo = O->nxc, nyo = O->nyc, nzo = O->nzc, nxn = N->nxc, nyn = N->nyc, nzn = N->nzc;
+  const int nypo = nyo + 1;
+  // normalised x/z point and centre coordinates
+  auto pts = [](int n, std::vector<double>& xp, std::vector<double>& xc) {
+    xp.assign(n + 2, 0.0); xc.assign(n + 2, 0.0);
+    for (int j = 1; j <= n + 1; ++j) xp[j] = (double)(j - 1) / (double)n;
+    xp[1] = 0.0; xp[n + 1] = 1.0;
+    for (int j = 1; j <= n; ++j) xc[j] = 0.5 * (xp[j] + xp[j + 1]);
+    xc[0] = 2.0 * xp[1] - xc[1];
+    xc[n + 1] = 2.0 * xp[n + 1] - xc[n];
+  };
+  std::vector<double> xpO, xcO, xpN, xcN, zpO, zcO, zpN, zcN;
+  pts(nxo, xpO, xcO); pts(nxn, xpN, xcN); pts(nzo, zpO, zcO); pts(nzn, zpN, zcN);
+  std::vector<double> ypO(nypo + 1), ycO(nypo + 1), ypN(nyn + 2), ycN(nyn + 2);
+  for (int j = 1; j <= nypo; ++j) ypO[j] = O->yp(j);
+  for (int j = 1; j <= nyn + 1; ++j) ypN[j] = N->yp(j);
+  for (int j = 1; j <= nyo; ++j) ycO[j] = 0.5 * (ypO[j] + ypO[j + 1]);
+  ycO[0] = 2.0 * ypO[1] - ycO[1]; ycO[nypo] = 2.0 * ypO[nypo] - ycO[nyo];
+  for (int j = 1; j <= nyn; ++j) ycN[j] = 0.5 * (ypN[j] + ypN[j + 1]);
+  // index and ratio tables (Interp_init :130-179)
+  auto xtab = [](int nn, int no, const std::vector<double>& pN, const std::vector<double>& pO, bool centred,
+                 std::vector<int>& ind, std::vector<double>& rat) {
+    ind.assign(nn + 1, 0); rat.assign(nn + 1, 0.0);
+    const double rd = (double)no;
+    for (int i = 1; i <= nn; ++i) {
+      int ic = (int)std::floor(pN[i] * rd) + 1;
+      ic = std::min(ic, no); ic = std::max(ic, 1);
+      if (centred && pN[i] < pO[ic]) ic = ic - 1;
+      ind[i] = ic; rat[i] = (pO[ic + 1] - pN[i]) * rd;
+    }
+  };
+  std::vector<int> ixp, ixc, izp, izc, iyp(nyn + 1), iyc(nyn + 1);
+  std::vector<double> rxp, rxc, rzp, rzc, ryp(nyn + 1), ryc(nyn + 1);
+  xtab(nxn, nxo, xpN, xpO, false, ixp, rxp); xtab(nxn, nxo, xcN, xcO, true, ixc, rxc);
+  xtab(nzn, nzo, zpN, zpO, false, izp, rzp); xtab(nzn, nzo, zcN, zcO, true, izc, rzc);
+  auto ysearch = [&](double y) {  // largest jc in 0..nypo with ypO(jc) <= y (bisection of :148-156)
+    int js = 0, je = nypo + 1, jc;
+    for (;;) {
+      jc = (js + je) / 2;
+      if (je - js == 1) break;
+      if (y < ypO[jc]) je = jc; else js = jc;
+    }
+    return jc;
+  };
+  for (int j = 1; j <= nyn; ++j) {
+    int jc = ysearch(ypN[j]);
+    iyp[j] = jc; ryp[j] = (ypO[jc + 1] - ypN[j]) / (ypO[jc + 1] - ypO[jc]);
+    jc = ysearch(ycN[j]);
+    if (ycN[j] < ycO[jc]) jc = jc - 1;
+    iyc[j] = jc; ryc[j] = (ycO[jc + 1] - ycN[j]) / (ycO[jc + 1] - ycO[jc]);
+  }
+  // the old state with the tool's ghosts, bounds (0:nxc+1, 0:nyc+1, 0:nzc+1)
+  const int* Bc = O->P.BcOption;
+  auto ghosted = [&](const F3& a, int comp) {
+    F3 g;
+    g.init(0, nxo + 1, 0, nyo + 1, 0, nzo + 1);
+    for (int k = 1; k <= nzo; ++k) for (int j = 1; j <= nyo; ++j) for (int i = 1; i <= nxo; ++i) g(i, j, k) = a(i, j, k);
+    for (int k = 1; k <= nzo; ++k)
+      for (int i = 1; i <= nxo; ++i) {
+        if (comp == 3) { g(i, nypo, k) = g(i, nyo, k); g(i, 0, k) = g(i, 1, k); continue; }
+        if (comp == 1) {
+          g(i, nypo, k) = Bc[3] == -1 ? O->P.uyBcValue[3] : 0.0;
+          g(i, 1, k) = Bc[2] == -1 ? O->P.uyBcValue[2] : 0.0;
+          continue;
+        }
+        const double* w = comp == 0 ? O->P.uxBcValue : O->P.uzBcValue;
+        g(i, nypo, k) = Bc[3] == -1 ? w[3] * 2.0 - g(i, nyo, k) : g(i, nyo, k);
+        g(i, 0, k) = Bc[2] == -1 ? w[2] * 2.0 - g(i, 1, k) : g(i, 1, k);
+      }
+    for (int k = 1; k <= nzo; ++k) for (int j = 0; j <= nypo; ++j) { g(0, j, k) = g(nxo, j, k); g(nxo + 1, j, k) = g(1, j, k); }
+    for (int j = 0; j <= nypo; ++j) for (int i = 0; i <= nxo + 1; ++i) { g(i, j, 0) = g(i, j, nzo); g(i, j, nzo + 1) = g(i, j, 1); }
+    return g;
+  };
+  const size_t Nn = (size_t)nxn * nyn * nzn;
+  std::vector<double> out[4];
+  for (int comp = 0; comp < 4; ++comp) {
+    const F3& src = comp == 0 ? O->ux : comp == 1 ? O->uy : comp == 2 ? O->uz : O->pressure;
+    const F3 A = ghosted(src, comp);
+    const std::vector<int>& IX = comp == 0 ? ixp : ixc;
+    const std::vector<double>& RX = comp == 0 ? rxp : rxc;
+    const std::vector<int>& IY = comp == 1 ? iyp : iyc;
+    const std::vector<double>& RY = comp == 1 ? ryp : ryc;
+    const std::vector<int>& IZ = comp == 2 ? izp : izc;
+    const std::vector<double>& RZ = comp == 2 ? rzp : rzc;
+    out[comp].assign(Nn, 0.0);
+    for (int kc = 1; kc <= nzn; ++kc) {
+      const int idz1 = IZ[kc], idz2 = idz1 + 1;
+      const double prz1 = RZ[kc], prz2 = one - prz1;
+      for (int jc = 1; jc <= nyn; ++jc) {
+        const int idy1 = IY[jc], idy2 = idy1 + 1;
+        const double pry1 = RY[jc], pry2 = one - pry1;
+        for (int ic = 1; ic <= nxn; ++ic) {
+          const int idx1 = IX[ic], idx2 = idx1 + 1;
+          const double prx1 = RX[ic], prx2 = one - prx1;
+          out[comp][(size_t)(ic - 1) + (size_t)nxn * ((size_t)(jc - 1) + (size_t)nyn * (kc - 1))] =
+              A(idx1, idy1, idz1) * prx1 * pry1 * prz1 + A(idx2, idy1, idz1) * prx2 * pry1 * prz1 +
+              A(idx1, idy2, idz1) * prx1 * pry2 * prz1 + A(idx2, idy2, idz1) * prx2 * pry2 * prz1 +
+              A(idx1, idy1, idz2) * prx1 * pry1 * prz2 + A(idx2, idy1, idz2) * prx2 * pry1 * prz2 +
+              A(idx1, idy2, idz2) * prx1 * pry2 * prz2 + A(idx2, idy2, idz2) * prx2 * pry2 * prz2;
+        }
+      }
+    }
+  }
+  if (N->P.IsUxConst) {  // :225-236
+    double MeanValue = zero;
+    for (int kc = 1; kc <= nzn; ++kc)
+      for (int jc = 1; jc <= nyn; ++jc)
+        for (int ic = 1; ic <= nxn; ++ic)
+          MeanValue = MeanValue + out[0][(size_t)(ic - 1) + (size_t)nxn * ((size_t)(jc - 1) + (size_t)nyn * (kc - 1))] *
+                                      (ypN[jc + 1] - ypN[jc]);
+    MeanValue = MeanValue / (double)nxn / (double)nzn / N->P.yly;
+    const double s = N->P.ubulk / MeanValue;
+    for (double& v : out[0]) v = s * v;
+  }
+  orc_set_state(hdst, out[0].data(), out[1].data(), out[2].data(), out[3].data(), nullptr);
+}
+
 void orc_stage(void* h, int st, int ns) { ((Oracle*)h)->stage(st, ns); }
 
 int orc_step(void* h, int nsteps, orc_info* info) {

@@ -92,6 +92,7 @@ def lib():
         L.orc_sgs.argtypes = [ctypes.c_void_p]
         L.orc_set_sgs_tau.argtypes = [ctypes.c_void_p, _DP]
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
+        L.orc_interp.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -195,6 +196,11 @@ class Oracle:
             return np.ascontiguousarray(g[2:nz + 2, 1:ny + 1, 2:nx + 2])
         g = a.reshape(nz + 3, ny + 3, nx + 3)   # (0:nxc+2, 0:nyc+2, 0:nzc+2)
         return np.ascontiguousarray(g[1:nz + 1, 1:ny + 1, 1:nx + 1])
+
+    def interp_from(self, src):
+        """Resamples src's state onto this grid (the interpolateField tool's
+        Interp_uvwp); it becomes this oracle's state."""
+        self.L.orc_interp(self.h, src.h)
 
     def stage(self, st, ns):
         self.L.orc_stage(self.h, st, ns)

@@ -339,3 +339,37 @@ def test_les_step_is_divergence_free(built):
         o.set_state(ux, uy, uz, p)
         d = o.step(3)
         assert d["divmax2"] < 1e-13 and d["rc"] == 0, model
+
+
+def test_oracle_interp_known_answers():
+    """The oracle's restatement of the interpolateField tool
+    (Tool/interpolateField/src/m_Interp.f90:20-361): onto the same grid it
+    returns the field unchanged; a field linear in y is reproduced exactly at
+    the cell centres of another stretching away from the walls; ux is held at
+    ubulk when the flow rate is constant."""
+    from channel3d_b200 import initfield, mesh_y
+    from oracle import oracle as O
+    cfg = small_channel(32, 24, 16)
+    st = initfield.laminar_noise(cfg, yp=mesh_y(cfg))
+    a = O.Oracle(cfg)
+    a.set_state(*st)
+    b = O.Oracle(cfg.copy(IsUxConst=False))
+    b.interp_from(a)
+    g, r = b.get_state(), a.get_state()
+    for k in ("ux", "uy", "uz", "p"):
+        assert np.array_equal(g[k], r[k]), k
+    new = small_channel(32, 20, 16, StretType=[2, 2], SectioncStret=[1.0, 1.0])
+    yc = 0.5 * (mesh_y(cfg)[1:] + mesh_y(cfg)[:-1])
+    f = np.broadcast_to((0.3 * yc + 0.1)[None, :, None], cfg.shape).copy()
+    a.set_state(f, np.zeros(cfg.shape), f, f)
+    c = O.Oracle(new.copy(IsUxConst=False))
+    c.interp_from(a)
+    ycn = 0.5 * (mesh_y(new)[1:] + mesh_y(new)[:-1])
+    got = c.get_state()
+    for k in ("uz", "p"):
+        assert np.abs(got[k][:, 2:-2, :] - (0.3 * ycn[2:-2] + 0.1)[None, :, None]).max() < 1e-14, k
+    d = O.Oracle(new.copy(ubulk=0.8))
+    d.interp_from(a)
+    ux = d.get_state()["ux"]
+    dy = np.diff(mesh_y(new))
+    assert abs((ux * dy[None, :, None]).sum() / (new.nxc * new.nzc * new.yly) - 0.8) < 1e-12

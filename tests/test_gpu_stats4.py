@@ -51,12 +51,12 @@ def test_statistics_parity_4th(built, shape):
     ga = s.stats_fetch_grad()
     gb, _ = o.stats_get_grad()
     scale = np.empty(98)
-    prms = np.sqrt(np.maximum(b[:, 7], 0.0)).max()  # <p^2> of SumStat
+    prms = np.sqrt(np.maximum(b[:, 7] / nb, 0.0)).max()  # <p^2> of SumStat (sums of nb samples)
     scale[0], scale[1] = prms ** 3, prms ** 4
     for t in range(24):  # SumVec2(3 + 4t .. 6 + 4t): the powers 1..4 of gradient t
-        rms = np.sqrt(np.maximum(gb[:, 3 + 4 * t], 0.0)).max()
+        rms = np.sqrt(np.maximum(gb[:, 3 + 4 * t] / nb, 0.0)).max()
         scale[2 + 4 * t: 6 + 4 * t] = [rms, rms ** 2, rms ** 3, rms ** 4]
-    err = np.abs(ga - gb).max(axis=0) / np.maximum(scale, 1e-300)
+    err = np.abs(ga - gb).max(axis=0) / nb / np.maximum(scale, 1e-300)
     assert err.max() < 1e-10, (int(err.argmax()) + 1, err.max())
     # the moments the nyp row carries (SumVec2 7..10 and 31..34) are non-zero there
     assert np.all(gb[-1, 6:10] != 0) and np.all(gb[-1, 30:34] != 0)

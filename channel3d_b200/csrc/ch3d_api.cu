@@ -633,17 +633,6 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     c->KL = 8;
     if (c->KL > c->nz / 2 - 1) c->KL = c->nz / 2 - 1;
     if (c->KL < 0) c->KL = 0;
-    c->ychunk = ychunk_usable(c);
-  }
-  if (c->ychunk) {
-    // partitioned y solve: factors on the fly from cp at the chunk boundaries
-    const size_t nb = ychunk_bound_doubles(c);
-    if (cudaMalloc(&c->yB, nb * sizeof(double)) != cudaSuccess)
-      return cleanup(fail(CH3D_ERR_NOMEM, "Poisson chunk factors"));
-    c->bytes += (long long)nb * sizeof(double);
-    e = launch_ysolve_factors(c);
-    if (e != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "Poisson factors: %s", cudaGetErrorString(e)));
-  } else {
     // Poisson y-solve (Thomas) factors per (kx, |kz|), computed once
     const size_t nrow = (size_t)(c->nz / 2 + 1) * c->ny * c->nxh;
     const size_t fw = c->fp32 ? sizeof(float) : sizeof(double);
@@ -705,7 +694,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   if (c->les_delta) cudaFree(c->les_delta);
   void* mbufs[] = {c->mlp_params, c->mlp_x, c->mlp_y, c->mlp_fb, c->mlp_status, c->sgs_tau, c->sgs_f};
   for (void* b : mbufs) if (b) cudaFree(b);
-  void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yB, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);

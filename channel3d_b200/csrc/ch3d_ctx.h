@@ -52,8 +52,6 @@ struct ch3d_ctx {
   double* yRM64 = nullptr;   // mixed path: FP64 factors of the low modes (kx < TSy, |kz| <= KL)
   double* yCP64 = nullptr;
   double* ylow = nullptr;    // mixed path: FP64 forward-sweep scratch of the low modes
-  bool ychunk = false;       // the y solve runs partitioned in shared memory (ch3d_ysolve.cu);
-  double* yB = nullptr;      // then only cp at the chunk boundaries is tabulated (FP64)
   bool gsub = false;         // the march stops at g; divergence and projection substitute u*
   int KL = 8;
   int TSy = 8;               // kx extent of the FP64 low modes
@@ -119,10 +117,6 @@ bool launch_prsrc_xfft_r(ch3d_ctx* c, int mode, cudaError_t* err);
 bool launch_zfft_r(ch3d_ctx* c, int inverse, cudaError_t* err);
 bool launch_xifft_r(ch3d_ctx* c, cudaError_t* err);
 cudaError_t launch_ysolve_factors(ch3d_ctx* c);
-bool ychunk_usable(const ch3d_ctx* c);                 // partitioned y solve applies to this grid
-size_t ychunk_bound_doubles(const ch3d_ctx* c);
-cudaError_t launch_ychunk_bounds(ch3d_ctx* c);         // cp at the chunk boundaries, once per run
-cudaError_t launch_ychunk(ch3d_ctx* c);                // partitioned y solve of the spectrum, in place
 cudaError_t launch_interp_state(ch3d_ctx* dst, const ch3d_ctx* src);  // Interp_uvwp onto dst's grid
 // allocation-free Poisson solve (static device scratch, ch3d_step.cu)
 size_t noalloc_bytes(int nx, int ny, int nz);

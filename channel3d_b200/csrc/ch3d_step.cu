@@ -1253,9 +1253,7 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
     if (e != cudaSuccess) return e;
   }
   const unsigned gy = (unsigned)(((long long)c->nxh * c->nz + 127) / 128);
-  if (c->ychunk) {
-    if ((e = launch_ychunk(c)) != cudaSuccess) return e;  // partitioned, the columns in shared memory
-  } else if (!c->fp32) {
+  if (!c->fp32) {
     k_ythomas<T, double><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
                                                     (const double*)c->yCP, (CT*)c->spec, c->sc);
   } else {
@@ -1271,7 +1269,6 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   return cudaGetLastError();
 }
 template <class T> static cudaError_t yfactors_t(ch3d_ctx* c) {
-  if (c->ychunk) return launch_ychunk_bounds(c);
   const dim3 g((c->nxh + 127) / 128, c->nz / 2 + 1);
   if (!c->fp32) {
     k_ythomas_factors<double><<<g, 128, 0, c->stream>>>(c->m64full, c->wave, c->nx, c->ny, (double*)c->yRM,

@@ -183,10 +183,12 @@ def box_filtered_profiles(fields, cfg, box):
 
 def evaluate(dns_cfg, les_cfg, dns_warm, dns_steps, n_snapshots, per_snapshot, les_steps, les_avg_from,
              box=(4, 2, 4), train_iters=3000, batch=65536, lr=1e-3, n_profile_snapshots=10, seed=0, log=print,
-             turbulent_start=0.0, warm_dt=None):
+             turbulent_start=0.0, warm_dt=None, les_start="seeded"):
     """The learned-closure experiment end to end on one GPU: DNS with
     box-filtered snapshots, training, and LES runs with the learned closure
-    and with the Smagorinsky / van Driest model from the same seeded start.
+    and with the Smagorinsky / van Driest model from the same start: the
+    seeded start, or (les_start="dns") the last DNS field resampled onto the
+    LES grid (ch3d_interp_state, the reference's interpolateField).
     Returns a report dict (profiles, errors against the filtered DNS,
     a-priori stress errors, LES cost per step)."""
     import time
@@ -225,6 +227,13 @@ def evaluate(dns_cfg, les_cfg, dns_warm, dns_steps, n_snapshots, per_snapshot, l
         s.step(every)
         prof.append(box_filtered_profiles(s.download(), dns_cfg, box))
     ref = {k: np.mean([p[k] for p in prof], axis=0) for k in prof[0]}
+    dns_start = None
+    if les_start == "dns":  # the DNS field on the LES grid
+        r = ChannelSolver(les_cfg.copy(LES_type=10))
+        r.interp_from(s)
+        st = r.download()
+        dns_start = (st["ux"], st["uy"], st["uz"], st["p"])
+        r.close()
     s.close()
     # train / hold-out split by snapshot
     nho = max(1, n_snapshots // 10) * per_snapshot
@@ -244,8 +253,12 @@ def evaluate(dns_cfg, les_cfg, dns_warm, dns_steps, n_snapshots, per_snapshot, l
     for name, lt in (("mlp", 11), ("smagorinsky_vd", 10)):
         cfg = les_cfg.copy(LES_type=lt)
         ls = ChannelSolver(cfg)
-        start = (initfield.large_scale(cfg, amplitude=turbulent_start, yp=ls.yp, seed=seed) if turbulent_start > 0
-                 else initfield.laminar_noise(cfg, yp=ls.yp, seed=seed))
+        if dns_start is not None:
+            start = dns_start
+        elif turbulent_start > 0:
+            start = initfield.large_scale(cfg, amplitude=turbulent_start, yp=ls.yp, seed=seed)
+        else:
+            start = initfield.laminar_noise(cfg, yp=ls.yp, seed=seed)
         ls.upload(*start)
         ls.project()
         if lt == 11:
@@ -291,12 +304,23 @@ def main():
     ap.add_argument("--turbulent-start", type=float, default=0.0,
                     help="amplitude of a large-scale start (0: the seeded white-noise start)")
     ap.add_argument("--warm-dt", type=float, default=None, help="time step of the mixed-precision warm-up")
+    ap.add_argument("--dns-grid", default="256x192x256",
+                    help="DNS cells nx x ny x nz of the 2pi x 2 x pi Re_b 13750 channel; 192x192x192 with --box 4,4,4 "
+                         "gives filter boxes that are exactly the cells of the 48^3 LES grid")
+    ap.add_argument("--box", default="4,2,4", help="filter box fx,fy,fz in DNS cells")
+    ap.add_argument("--les-start", default="seeded", choices=["seeded", "dns"],
+                    help="start of the LES runs: the seeded field, or the last DNS field resampled onto the LES grid")
     args = ap.parse_args()
+    nx, ny, nz = (int(v) for v in args.dns_grid.lower().split("x"))
     dns, _ = workloads.get("channel256x192x256_re13750")
+    dns = dns.copy(nxc=nx, nyc=ny, nzc=nz, nycSection=[ny // 2, ny - ny // 2])
     les, _ = workloads.get("channel48_les", LES_type=10, Cs=0.1)
+    box = tuple(int(v) for v in args.box.split(","))
     rep = evaluate(dns, les, args.dns_warm, args.dns_steps, args.snapshots, args.per_snapshot, args.les_steps,
-                   args.les_avg_from, train_iters=args.train_iters, turbulent_start=args.turbulent_start,
-                   warm_dt=args.warm_dt)
+                   args.les_avg_from, box=box, train_iters=args.train_iters, turbulent_start=args.turbulent_start,
+                   warm_dt=args.warm_dt, les_start=args.les_start)
+    rep["dns_grid"] = [nx, ny, nz]
+    rep["les_start"] = args.les_start
     json.dump(rep, open(args.out, "w"))
 
 

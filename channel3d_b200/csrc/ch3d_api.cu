@@ -692,7 +692,8 @@ int ch3d_destroy(ch3d_ctx* c) {
   for (int q = 0; q < 6; ++q) if (c->ih[q]) cudaFree(c->ih[q]);
   if (c->pfac) cudaFree(c->pfac);
   if (c->les_delta) cudaFree(c->les_delta);
-  void* mbufs[] = {c->mlp_params, c->mlp_x, c->mlp_y, c->mlp_fb, c->mlp_status, c->sgs_tau, c->sgs_f};
+  void* mbufs[] = {c->mlp_params, c->mlp_x, c->mlp_y, c->mlp_fb, c->mlp_status, c->sgs_tau, c->sgs_f, c->spec2,
+                   c->specacc};
   for (void* b : mbufs) if (b) cudaFree(b);
   void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
@@ -945,6 +946,49 @@ int ch3d_stats_fetch(ch3d_ctx* c, double* sumstat, int* nfstime, double* prgrads
     CU(cudaStreamSynchronize(c->stream));
     c->nfstime = 0;
   }
+  return CH3D_OK;
+}
+
+static size_t spectra_doubles(const ch3d_ctx* c) { return (size_t)18 * c->ny * (c->nxh + c->nz / 2 + 1); }
+
+int ch3d_spectra_accumulate(ch3d_ctx* c, int jfor1, int jfor2) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (c->cfg.order != 4)
+    return fail(CH3D_ERR_UNSUPPORTED, "the 1-D spectra belong to the 4th-order statistics");
+  if (jfor1 < 1 || jfor1 > c->ny / 2 || jfor2 < 1 || jfor2 > c->ny / 2)
+    return fail(CH3D_ERR_INVALID, "jForLCS (%d, %d) must lie in 1..nyc/2", jfor1, jfor2);
+  CU(cudaSetDevice(c->device));
+  if (!c->specacc) {
+    const size_t word = c->fp32 ? sizeof(float) : sizeof(double);
+    if (cudaMalloc(&c->spec2, (size_t)c->NS * 2 * word) != cudaSuccess ||
+        cudaMalloc(&c->specacc, spectra_doubles(c) * sizeof(double)) != cudaSuccess)
+      return fail(CH3D_ERR_NOMEM, "spectra buffers");
+    c->bytes += (long long)c->NS * 2 * word + (long long)spectra_doubles(c) * sizeof(double);
+    CU(cudaMemsetAsync(c->specacc, 0, spectra_doubles(c) * sizeof(double), c->stream));
+  }
+  CU(launch_spectra(c, jfor1, jfor2));
+  CU(cudaStreamSynchronize(c->stream));
+  c->nspectime += 1;
+  return CH3D_OK;
+}
+
+int ch3d_spectra_fetch(ch3d_ctx* c, double* specx, double* specz, int* nspectime, int reset) {
+  if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
+  if (c->cfg.order != 4)
+    return fail(CH3D_ERR_UNSUPPORTED, "the 1-D spectra belong to the 4th-order statistics");
+  CU(cudaSetDevice(c->device));
+  const size_t nxs = (size_t)18 * c->ny * c->nxh, nzs = (size_t)18 * c->ny * (c->nz / 2 + 1);
+  if (!c->specacc) {
+    if (specx) std::memset(specx, 0, nxs * sizeof(double));
+    if (specz) std::memset(specz, 0, nzs * sizeof(double));
+  } else {
+    if (specx) CU(cudaMemcpyAsync(specx, c->specacc, nxs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (specz) CU(cudaMemcpyAsync(specz, c->specacc + nxs, nzs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (reset) CU(cudaMemsetAsync(c->specacc, 0, spectra_doubles(c) * sizeof(double), c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+  }
+  if (nspectime) *nspectime = c->nspectime;
+  if (reset) c->nspectime = 0;
   return CH3D_OK;
 }
 

@@ -71,6 +71,9 @@ struct ch3d_ctx {
   int npart = 0;
   bool march = false;        // 2nd-order PIMP without LES: march kernels, npart_m partial sums in part
   int npart_m = 0;
+  void* spec2 = nullptr;     // second half spectrum of the 1-D spectra (allocated at their first sample)
+  double* specacc = nullptr; // EnergySpecX (nxh, ny, 18) | EnergySpecZ (nz/2+1, ny, 18) sums (FP64)
+  int nspectime = 0;
   double* stat = nullptr;    // SumStat(35, nyp) | PrGradsum [| SumGrad(98, nyp), 4th order] (FP64)
   double* statpart = nullptr;
   int nfstime = 0;
@@ -118,6 +121,8 @@ bool launch_zfft_r(ch3d_ctx* c, int inverse, cudaError_t* err);
 bool launch_xifft_r(ch3d_ctx* c, cudaError_t* err);
 cudaError_t launch_ysolve_factors(ch3d_ctx* c);
 cudaError_t launch_interp_state(ch3d_ctx* dst, const ch3d_ctx* src);  // Interp_uvwp onto dst's grid
+cudaError_t launch_zfft_forward(ch3d_ctx* c);          // forward z transform of the spectrum alone
+cudaError_t launch_spectra(ch3d_ctx* c, int jfor1, int jfor2);  // one sample of the 4th-order 1-D spectra
 // allocation-free Poisson solve (static device scratch, ch3d_step.cu)
 size_t noalloc_bytes(int nx, int ny, int nz);
 size_t noalloc_smem(int nx, int ny, int nz);

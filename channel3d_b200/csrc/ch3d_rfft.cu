@@ -27,7 +27,7 @@ typedef RPlan<64, 16, 4, 4, 4> PlanN64;
 typedef RPlan<576, 48, 4, 4, 3, 12> PlanN576;
 typedef RPlan<128, 16, 8, 2, 8> PlanZ128;
 
-// SRC: modes 2 and 3, the source (or divergence) already formed in the first
+// SRC: modes 2, 3 and 4, the source (or divergence, or field) already formed in the first
 // array; compiled separately so it is not held to the divergence modes' registers.
 template <class T, class PL, bool SRC>
 __global__ void __launch_bounds__(32 * kXWarps, SRC ? 6 : (sizeof(T) == 4 ? 6 : 4)) k_prsrc_xfft_r(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
@@ -46,7 +46,8 @@ __global__ void __launch_bounds__(32 * kXWarps, SRC ? 6 : (sizeof(T) == 4 ? 6 : 
   const int t = lane % P, slot = warp * LPW + lane / P;
   CT* L = sm[slot];
   const int nlines = ny * nz;
-  // mode 3: the divergence of u* already formed (k_div_bsub) in the first array
+  // mode 3: the divergence of u* already formed (k_div_bsub) in the first array; mode 4:
+  // any real field in the first array, transformed as it is (no scaling, no maximum)
   const T sudtal = mode == 0 || mode == 3 ? (T)(1.0 / sc->pmAlpha) : (T)1;
   const T rdx = g.rdx, rdz = g.rdz;
   double dmax = 0.0;
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(32 * kXWarps, SRC ? 6 : (sizeof(T) == 4 ? 6 : 
     }
     __syncwarp();
   }
-  if (mode == 3) return;  // its maximum was taken where the divergence was formed
+  if (mode >= 3) return;  // mode 3: its maximum was taken where the divergence was formed; 4: a plain transform
   for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
   if (lane == 0) wred[warp] = dmax;
   __syncthreads();

@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(256) k_prsrc_xfft(Geo<T> g, Metrics<T> m, cons
       r0 = div4_cell(g, c4, sucaj, ux, uy, uz, i0, j, k);
       r1 = div4_cell(g, c4, sucaj, ux, uy, uz, i1, j, k);
     }
-    if (mode == 2) { r0 = u0; r1 = u1; }  // standalone Poisson: ux carries the source
+    if (mode == 2 || mode == 4) { r0 = u0; r1 = u1; }  // ux carries the source (standalone Poisson) or the field
     if (mode == 0 && g.implicit == 2) {     // clcPrSrc_FIMP: pressure += -xnu/2 div (m_TScheme.f90:271)
       const T xnuhm = -(T)0.5 * g.xnu;
       pr[base + i0] = pr[base + i0] + xnuhm * r0;
@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(256) k_prsrc_xfft(Geo<T> g, Metrics<T> m, cons
     if (threadIdx.x < 32) {
       double v = threadIdx.x < (blockDim.x + 31) / 32 ? wred[threadIdx.x] : 0.0;
       for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if (threadIdx.x == 0) atomic_max_nonneg(&sc->divmax1, v);
+      if (threadIdx.x == 0 && mode != 4) atomic_max_nonneg(&sc->divmax1, v);
     }
     __syncthreads();
   }
@@ -1222,7 +1222,7 @@ template <class T> static cudaError_t prsrc_t(ch3d_ctx* c, int mode) {
   static PerDevice attr;  // per precision (template instance)
   if ((e = smem_limit_once(attr, c->device, k_prsrc_xfft<T>, 200 * 1024)) != cudaSuccess) return e;
   const int nthr = 256;
-  T* a = mode == 2 ? f[10] : (mode == 1 ? f[0] : f[12]);
+  T* a = mode == 2 || mode == 4 ? f[10] : (mode == 1 ? f[0] : f[12]);
   T* b = mode == 1 ? f[1] : f[13];
   T* cz = mode == 1 ? f[2] : f[14];
   k_prsrc_xfft<T><<<(nlines + LPB - 1) / LPB, nthr, smem, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), a, b, cz,
@@ -1268,6 +1268,25 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);
   return cudaGetLastError();
 }
+// Forward z transform of the spectrum alone (the first step of the spectral solve).
+template <class T> static cudaError_t zfft_fwd_t(ch3d_ctx* c) {
+  typedef typename CplxOf<T>::type CT;
+  cudaError_t e;
+  if (launch_zfft_r(c, 0, &e)) return e;
+  const int nz = c->nz;
+  int TKX = kFFTSmem / (2 * nz * (int)sizeof(CT));
+  int t = 1;
+  while (t * 2 <= TKX && t * 2 <= 16) t *= 2;
+  TKX = t;
+  static PerDevice attr;  // per precision (template instance)
+  if ((e = smem_limit_once(attr, c->device, k_zfft<T>, 200 * 1024)) != cudaSuccess) return e;
+  dim3 gz((c->nxh + TKX - 1) / TKX, c->ny);
+  k_zfft<T><<<gz, 256, (size_t)2 * TKX * nz * sizeof(CT), c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz,
+                                                                      (const CT*)c->twz, TKX, 0, c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_zfft_forward(ch3d_ctx* c) { return c->fp32 ? zfft_fwd_t<float>(c) : zfft_fwd_t<double>(c); }
+
 template <class T> static cudaError_t yfactors_t(ch3d_ctx* c) {
   const dim3 g((c->nxh + 127) / 128, c->nz / 2 + 1);
   if (!c->fp32) {

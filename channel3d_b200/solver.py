@@ -164,6 +164,21 @@ class ChannelSolver:
         interpolateField tool, Interp_uvwp) and makes it this solver's state."""
         _lib.check(self.lib.ch3d_interp_state(self.ctx, src.ctx), self.lib)
 
+    def spectra_accumulate(self, jfor=(1, 1)):
+        """4th order: one sample of the 1-D spectra (clcSpectra1D) with the
+        coherence spectra against rows jForLCS(1:2) (1-based)."""
+        _lib.check(self.lib.ch3d_spectra_accumulate(self.ctx, int(jfor[0]), int(jfor[1])), self.lib)
+
+    def spectra_fetch(self, reset=False):
+        """(EnergySpecX as (18, nyc, nxc/2+1), EnergySpecZ as (18, nyc, nzc/2+1), nSpectime)."""
+        c = self.cfg
+        sx = np.empty((18, c.nyc, c.nxc // 2 + 1))
+        sz = np.empty((18, c.nyc, c.nzc // 2 + 1))
+        n = ctypes.c_int()
+        _lib.check(self.lib.ch3d_spectra_fetch(self.ctx, _lib.dptr(sx), _lib.dptr(sz), ctypes.byref(n), int(reset)),
+                   self.lib)
+        return sx, sz, n.value
+
     def stats_fetch_grad(self):
         """4th order: SumGrad(98, nyp) as (nyp, 98) (the vGrad moment sums)."""
         g = np.empty((self.cfg.nyc + 1) * 98)

@@ -51,3 +51,13 @@ def profiles(sumstat, nfstime, prgradsum, xnu, h=1.0):
     dpdx = prgradsum / nfstime
     utau = np.sqrt(max(h * dpdx, 0.0))
     return {"U": U, "urms": urms, "vrms": vrms, "wrms": wrms, "dpdx": dpdx, "Re_tau": utau * h / xnu}
+
+
+def write_spectra(path_x, path_z, specx, specz, nspectime):
+    """SpecX%10.10d and SpecZ%10.10d of the 4th order (src/CFD_4th/m_FlowCase.f90:1000-1045):
+    EnergySpecX(nxc/2+1, nyc, 18) and EnergySpecZ(nzc/2+1, nyc, 18) / nSpectime as raw
+    native-endian FP64 in Fortran order (the C order of the (18, nyc, n) arrays)."""
+    inf = 1.0 / nspectime
+    for path, a in ((path_x, specx), (path_z, specz)):
+        (np.ascontiguousarray(a, dtype=np.float64) * inf).tofile(path)
+

@@ -2030,6 +2030,156 @@ struct Oracle {
     nfstime += 1;
   }
 
+  // ---- src/CFD_4th/m_FlowCase.f90:642-880 (clcStat, the 1-D spectra branch with
+  //      clcSpectra1D: 18 x- and z-spectra per row: UU, VV, WW, PP energy spectra,
+  //      UV and UV2 cospectra, and for UU, VV, WW, PP the linear coherence spectra
+  //      R1, I1, R2 against the rows jForLCS(1:2)), with clcEnergySpectraX/Z and
+  //      clcCospectraX/Z (:1152-1266), clcLTS_x/z (:1271-1632) and transform_uy
+  //      (:2303-2332); R2HC transforms of every x and z line (FFTW_R2HC). ----
+  std::vector<double> EnergySpecX, EnergySpecZ;  // (nxhp, nyc, 18), (nzhp, nyc, 18)
+  int nSpectime = 0;
+  void clcSpectra1D(int jFor1, int jFor2) {
+    const int nxh = nxc / 2, nxhp = nxh + 1, nzh = nzc / 2, nzhp = nzh + 1;
+    if (EnergySpecX.empty()) {
+      EnergySpecX.assign((size_t)nxhp * nyc * 18, 0.0);
+      EnergySpecZ.assign((size_t)nzhp * nyc * 18, 0.0);
+    }
+    const size_t N3 = (size_t)nxc * nyc * nzc;
+    auto I3 = [&](int ic, int jc, int kc) { return (size_t)(ic - 1) + (size_t)nxc * ((size_t)(jc - 1) + (size_t)nyc * (kc - 1)); };
+    // the quantity arrays (interior, Fortran order)
+    std::vector<double> qux(N3), quy(N3), quz(N3), qpr(N3), quxc(N3), quyc(N3);
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          const size_t q = I3(ic, jc, kc);
+          qux[q] = ux(ic, jc, kc) + uCRF;
+          quxc[q] = InterpCoe1 * ux(ic - 1, jc, kc) + InterpCoe2 * ux(ic, jc, kc) + InterpCoe3 * ux(ic + 1, jc, kc) +
+                    InterpCoe4 * ux(ic + 2, jc, kc) + uCRF;
+          quyc[q] = half * (uy(ic, jc, kc) + uy(ic, jc + 1, kc));
+          int jp = jc + 1;  // transform_uy, channel (FT_CH)
+          if (jc > nyc / 2) jp = jc;
+          quy[q] = uy(ic, jp, kc);
+          quz[q] = uz(ic, jc, kc);
+          qpr[q] = pressure(ic, jc, kc);
+        }
+    // R2HC of every x line and of every z line
+    std::vector<cplx> ba, bb;
+    auto hcx = [&](const std::vector<double>& a) {
+      std::vector<double> h(a);
+      for (int kc = 1; kc <= nzc; ++kc) for (int jc = 1; jc <= nyc; ++jc) r2hc(planx, &h[I3(1, jc, kc)], ba, bb);
+      return h;
+    };
+    auto hcz = [&](const std::vector<double>& a) {
+      std::vector<double> h(a), line(nzc);
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int kc = 1; kc <= nzc; ++kc) line[kc - 1] = a[I3(ic, jc, kc)];
+          r2hc(planz, line.data(), ba, bb);
+          for (int kc = 1; kc <= nzc; ++kc) h[I3(ic, jc, kc)] = line[kc - 1];
+        }
+      return h;
+    };
+    const double normX = one / ((double)nxc * (double)nxc * (double)nzc);
+    const double normZ = one / ((double)nxc * (double)nzc * (double)nzc);
+    auto SX = [&](int ic, int jc, int m) -> double& { return EnergySpecX[(size_t)(ic - 1) + (size_t)nxhp * ((size_t)(jc - 1) + (size_t)nyc * m)]; };
+    auto SZ = [&](int kc, int jc, int m) -> double& { return EnergySpecZ[(size_t)(kc - 1) + (size_t)nzhp * ((size_t)(jc - 1) + (size_t)nyc * m)]; };
+    // clcEnergySpectraX / clcCospectraX (a == b for the energy spectra)
+    auto cospX = [&](const std::vector<double>& a, const std::vector<double>& b, int m) {
+      for (int jc = 1; jc <= nyc; ++jc) {
+        std::vector<double> E(nxhp + 1, 0.0);
+        for (int kc = 1; kc <= nzc; ++kc) {
+          E[1] = E[1] + a[I3(1, jc, kc)] * b[I3(1, jc, kc)];
+          E[nxhp] = E[nxhp] + a[I3(nxhp, jc, kc)] * b[I3(nxhp, jc, kc)];
+          for (int ic = 2; ic <= nxh; ++ic) {
+            const int icC = nxc + 2 - ic;
+            E[ic] = E[ic] + (a[I3(ic, jc, kc)] * b[I3(ic, jc, kc)] + a[I3(icC, jc, kc)] * b[I3(icC, jc, kc)]) * two;
+          }
+        }
+        for (int ic = 1; ic <= nxhp; ++ic) SX(ic, jc, m) = SX(ic, jc, m) + E[ic] * normX;
+      }
+    };
+    auto cospZ = [&](const std::vector<double>& a, const std::vector<double>& b, int m) {
+      for (int jc = 1; jc <= nyc; ++jc) {
+        std::vector<double> E(nzhp + 1, 0.0);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          E[1] = E[1] + a[I3(ic, jc, 1)] * b[I3(ic, jc, 1)];
+          E[nzhp] = E[nzhp] + a[I3(ic, jc, nzhp)] * b[I3(ic, jc, nzhp)];
+          for (int kc = 2; kc <= nzh; ++kc) {
+            const int kcC = nzc + 2 - kc;
+            E[kc] = E[kc] + (a[I3(ic, jc, kc)] * b[I3(ic, jc, kc)] + a[I3(ic, jc, kcC)] * b[I3(ic, jc, kcC)]) * two;
+          }
+        }
+        for (int kc = 1; kc <= nzhp; ++kc) SZ(kc, jc, m) = SZ(kc, jc, m) + E[kc] * normZ;
+      }
+    };
+    // clcLTS_x / clcLTS_z: products with the reference row (jForLCS, mirrored in the upper half)
+    auto jref = [&](int jc, int jf) { return jc <= nyc / 2 ? jf : nyc + 1 - jf; };
+    auto ltsX = [&](const std::vector<double>& h, int n1, int n2, int n3) {
+      for (int jc = 1; jc <= nyc; ++jc) {
+        std::vector<double> R1(nxhp + 1, 0.0), Im(nxhp + 1, 0.0), R2(nxhp + 1, 0.0);
+        const int j1 = jref(jc, jFor1), j2 = jref(jc, jFor2);
+        for (int kc = 1; kc <= nzc; ++kc) {
+          R1[1] = R1[1] + h[I3(1, jc, kc)] * h[I3(1, j1, kc)];
+          R1[nxhp] = R1[nxhp] + h[I3(nxhp, jc, kc)] * h[I3(nxhp, j1, kc)];
+          R2[1] = R2[1] + h[I3(1, jc, kc)] * h[I3(1, j2, kc)];
+          R2[nxhp] = R2[nxhp] + h[I3(nxhp, jc, kc)] * h[I3(nxhp, j2, kc)];
+          for (int ic = 2; ic <= nxh; ++ic) {
+            const int icC = nxc + 2 - ic;
+            R1[ic] = R1[ic] + (h[I3(ic, jc, kc)] * h[I3(ic, j1, kc)] + h[I3(icC, jc, kc)] * h[I3(icC, j1, kc)]);
+            Im[ic] = Im[ic] + (h[I3(icC, jc, kc)] * h[I3(ic, j1, kc)] - h[I3(ic, jc, kc)] * h[I3(icC, j1, kc)]);
+            R2[ic] = R2[ic] + (h[I3(ic, jc, kc)] * h[I3(ic, j2, kc)] + h[I3(icC, jc, kc)] * h[I3(icC, j2, kc)]);
+          }
+        }
+        for (int ic = 1; ic <= nxhp; ++ic) {
+          SX(ic, jc, n1) = SX(ic, jc, n1) + R1[ic] * normX;
+          SX(ic, jc, n2) = SX(ic, jc, n2) + Im[ic] * normX;
+          SX(ic, jc, n3) = SX(ic, jc, n3) + R2[ic] * normX;
+        }
+      }
+    };
+    auto ltsZ = [&](const std::vector<double>& h, int n1, int n2, int n3) {
+      for (int jc = 1; jc <= nyc; ++jc) {
+        std::vector<double> R1(nzhp + 1, 0.0), Im(nzhp + 1, 0.0), R2(nzhp + 1, 0.0);
+        const int j1 = jref(jc, jFor1), j2 = jref(jc, jFor2);
+        for (int ic = 1; ic <= nxc; ++ic) {
+          R1[1] = R1[1] + h[I3(ic, jc, 1)] * h[I3(ic, j1, 1)];
+          R1[nzhp] = R1[nzhp] + h[I3(ic, jc, nzhp)] * h[I3(ic, j1, nzhp)];
+          R2[1] = R2[1] + h[I3(ic, jc, 1)] * h[I3(ic, j2, 1)];
+          R2[nzhp] = R2[nzhp] + h[I3(ic, jc, nzhp)] * h[I3(ic, j2, nzhp)];
+          for (int kc = 2; kc <= nzh; ++kc) {
+            const int kcC = nzc + 2 - kc;
+            R1[kc] = R1[kc] + (h[I3(ic, jc, kc)] * h[I3(ic, j1, kc)] + h[I3(ic, jc, kcC)] * h[I3(ic, j1, kcC)]);
+            Im[kc] = Im[kc] + (h[I3(ic, jc, kcC)] * h[I3(ic, j1, kc)] - h[I3(ic, jc, kc)] * h[I3(ic, j1, kcC)]);
+            R2[kc] = R2[kc] + (h[I3(ic, jc, kc)] * h[I3(ic, j2, kc)] + h[I3(ic, jc, kcC)] * h[I3(ic, j2, kcC)]);
+          }
+        }
+        for (int kc = 1; kc <= nzhp; ++kc) {
+          SZ(kc, jc, n1) = SZ(kc, jc, n1) + R1[kc] * normZ;
+          SZ(kc, jc, n2) = SZ(kc, jc, n2) + Im[kc] * normZ;
+          SZ(kc, jc, n3) = SZ(kc, jc, n3) + R2[kc] * normZ;
+        }
+      }
+    };
+    // the order of :662-720 (x) and :786-849 (z); indices iSpec1D* - 1 (:43-60)
+    {
+      const std::vector<double> a = hcx(qux), b = hcx(quyc), f = hcx(quxc);
+      cospX(a, a, 0); ltsX(a, 6, 7, 8); cospX(a, b, 5); cospX(f, b, 4);
+      const std::vector<double> v = hcx(quy), w = hcx(quz), pp = hcx(qpr);
+      cospX(v, v, 1); ltsX(v, 9, 10, 11);
+      cospX(w, w, 2); ltsX(w, 12, 13, 14);
+      cospX(pp, pp, 3); ltsX(pp, 15, 16, 17);
+    }
+    {
+      const std::vector<double> a = hcz(qux), b = hcz(quyc), f = hcz(quxc);
+      cospZ(a, a, 0); ltsZ(a, 6, 7, 8); cospZ(a, b, 5); cospZ(f, b, 4);
+      const std::vector<double> v = hcz(quy), w = hcz(quz), pp = hcz(qpr);
+      cospZ(v, v, 1); ltsZ(v, 9, 10, 11);
+      cospZ(w, w, 2); ltsZ(w, 12, 13, 14);
+      cospZ(pp, pp, 3); ltsZ(pp, 15, 16, 17);
+    }
+    nSpectime += 1;
+  }
+
   F3* field(int id) {
     switch (id) {
       case 0: return &ux; case 1: return &uy; case 2: return &uz; case 3: return &pressure;
@@ -2324,6 +2474,18 @@ void orc_stats_accumulate(void* h) {
   Oracle* o = (Oracle*)h;
   if (o->o4) o->clcStat4();
   else o->clcStat_CH();
+}
+
+// 1-D spectra of the 4th-order statistics (clcSpectra1D) at the current state.
+void orc_spectra_accumulate(void* h, int jFor1, int jFor2) { ((Oracle*)h)->clcSpectra1D(jFor1, jFor2); }
+
+// EnergySpecX(nxhp,nyc,18) and EnergySpecZ(nzhp,nyc,18) sums; returns nSpectime.
+int orc_spectra_get(void* h, double* specx, double* specz) {
+  Oracle* o = (Oracle*)h;
+  const size_t nx = (size_t)(o->nxc / 2 + 1) * o->nyc * 18, nz = (size_t)(o->nzc / 2 + 1) * o->nyc * 18;
+  for (size_t q = 0; q < nx; ++q) specx[q] = o->EnergySpecX.empty() ? 0.0 : o->EnergySpecX[q];
+  for (size_t q = 0; q < nz; ++q) specz[q] = o->EnergySpecZ.empty() ? 0.0 : o->EnergySpecZ[q];
+  return o->nSpectime;
 }
 
 // SumGrad(98,nyp) of the 4th-order statistics (zeros before the first accumulation);

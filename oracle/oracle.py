@@ -93,6 +93,9 @@ def lib():
         L.orc_set_sgs_tau.argtypes = [ctypes.c_void_p, _DP]
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         L.orc_interp.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_spectra_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_spectra_get.restype = ctypes.c_int
+        L.orc_spectra_get.argtypes = [ctypes.c_void_p, _DP, _DP]
         _lib = L
     return _lib
 
@@ -240,6 +243,19 @@ class Oracle:
         pg = ctypes.c_double()
         n = self.L.orc_stats_get(self.h, _p(s), ctypes.byref(pg))
         return s.reshape(self.cfg.nyc + 1, 35), n, pg.value
+
+    def spectra_accumulate(self, jfor=(1, 1)):
+        """4th order: one sample of the 1-D spectra (clcSpectra1D) with the
+        linear coherence spectra against rows jForLCS(1:2) (1-based)."""
+        self.L.orc_spectra_accumulate(self.h, int(jfor[0]), int(jfor[1]))
+
+    def spectra_get(self):
+        """(EnergySpecX as (18, nyc, nxc/2+1), EnergySpecZ as (18, nyc, nzc/2+1), nSpectime)."""
+        c = self.cfg
+        sx = np.empty((18, c.nyc, c.nxc // 2 + 1))
+        sz = np.empty((18, c.nyc, c.nzc // 2 + 1))
+        n = self.L.orc_spectra_get(self.h, _p(sx), _p(sz))
+        return sx, sz, n
 
     def stats_get_grad(self):
         """4th order: SumGrad(98, nyp) as (nyp, 98), and nfstime."""

@@ -234,3 +234,16 @@ def test_max_over_ranks_gloo(tmp_path):
     # the two ranks share the pipe, so their lines may interleave
     got = sorted(re.findall(r"RANK\d \d+ [\d.]+", out.stdout))
     assert got == ["RANK0 2 15.0", "RANK1 2 15.0"], (got, out.stderr[-1000:])
+
+
+def test_spectra_writer(tmp_path):
+    """SpecX / SpecZ: the sums / nSpectime as raw FP64 in Fortran order of
+    (nxc/2+1, nyc, 18), i.e. 18 blocks of nyc rows (src/CFD_4th/m_FlowCase.f90:1000-1045)."""
+    from channel3d_b200 import stats
+    sx = np.arange(18 * 5 * 9, dtype=float).reshape(18, 5, 9)
+    sz = -np.arange(18 * 5 * 4, dtype=float).reshape(18, 5, 4)
+    stats.write_spectra(str(tmp_path / "SpecX"), str(tmp_path / "SpecZ"), sx * 3, sz * 3, 3)
+    bx = np.fromfile(str(tmp_path / "SpecX"), dtype=np.float64)
+    bz = np.fromfile(str(tmp_path / "SpecZ"), dtype=np.float64)
+    assert bx.size == sx.size and np.allclose(bx.reshape(9, 5, 18, order="F"), np.moveaxis(sx, [0, 1, 2], [2, 1, 0]))
+    assert np.allclose(bz, sz.ravel())

@@ -949,12 +949,15 @@ int ch3d_stats_fetch(ch3d_ctx* c, double* sumstat, int* nfstime, double* prgrads
   return CH3D_OK;
 }
 
-static size_t spectra_doubles(const ch3d_ctx* c) { return (size_t)18 * c->ny * (c->nxh + c->nz / 2 + 1); }
+// EnergySpecX (nxh, ny, 18) | EnergySpecZ (nz/2+1, ny, 18) | EnergySpec2D (nxh, ny/2, nz/2+1, 9)
+static size_t spectra_doubles(const ch3d_ctx* c) {
+  return (size_t)18 * c->ny * (c->nxh + c->nz / 2 + 1) + (size_t)9 * c->nxh * (c->ny / 2) * (c->nz / 2 + 1);
+}
 
 int ch3d_spectra_accumulate(ch3d_ctx* c, int jfor1, int jfor2) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
   if (c->cfg.order != 4)
-    return fail(CH3D_ERR_UNSUPPORTED, "the 1-D spectra belong to the 4th-order statistics");
+    return fail(CH3D_ERR_UNSUPPORTED, "the spectra belong to the 4th-order statistics");
   if (jfor1 < 1 || jfor1 > c->ny / 2 || jfor2 < 1 || jfor2 > c->ny / 2)
     return fail(CH3D_ERR_INVALID, "jForLCS (%d, %d) must lie in 1..nyc/2", jfor1, jfor2);
   CU(cudaSetDevice(c->device));
@@ -972,18 +975,22 @@ int ch3d_spectra_accumulate(ch3d_ctx* c, int jfor1, int jfor2) {
   return CH3D_OK;
 }
 
-int ch3d_spectra_fetch(ch3d_ctx* c, double* specx, double* specz, int* nspectime, int reset) {
+int ch3d_spectra_fetch(ch3d_ctx* c, double* specx, double* specz, double* spec2d, int* nspectime, int reset) {
   if (!c) return fail(CH3D_ERR_INVALID, "ctx is NULL");
   if (c->cfg.order != 4)
-    return fail(CH3D_ERR_UNSUPPORTED, "the 1-D spectra belong to the 4th-order statistics");
+    return fail(CH3D_ERR_UNSUPPORTED, "the spectra belong to the 4th-order statistics");
   CU(cudaSetDevice(c->device));
   const size_t nxs = (size_t)18 * c->ny * c->nxh, nzs = (size_t)18 * c->ny * (c->nz / 2 + 1);
+  const size_t n2s = (size_t)9 * c->nxh * (c->ny / 2) * (c->nz / 2 + 1);
   if (!c->specacc) {
     if (specx) std::memset(specx, 0, nxs * sizeof(double));
     if (specz) std::memset(specz, 0, nzs * sizeof(double));
+    if (spec2d) std::memset(spec2d, 0, n2s * sizeof(double));
   } else {
     if (specx) CU(cudaMemcpyAsync(specx, c->specacc, nxs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (specz) CU(cudaMemcpyAsync(specz, c->specacc + nxs, nzs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (spec2d)
+      CU(cudaMemcpyAsync(spec2d, c->specacc + nxs + nzs, n2s * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (reset) CU(cudaMemsetAsync(c->specacc, 0, spectra_doubles(c) * sizeof(double), c->stream));
     CU(cudaStreamSynchronize(c->stream));
   }

@@ -1,5 +1,6 @@
-// ch3d_spectra.cu -- one-dimensional spectra of the 4th-order statistics
-// (clcStat's clcSpectra1D branch, src/CFD_4th/m_FlowCase.f90:642-880):
+// ch3d_spectra.cu -- spectra of the 4th-order statistics: clcStat's
+// clcSpectra1D branch (src/CFD_4th/m_FlowCase.f90:642-880) and its 2-D
+// spectra (clcSpectra2D, :881-935):
 // per row jc and per direction 18 spectra: the energy spectra of ux, of uy
 // at the faces transform_uy picks (:2303-2332), of uz and of p; the cospectra
 // of the cell-centred ux and uy (UV) and of ux and the cell-centred uy (UV2);
@@ -15,7 +16,8 @@
 // reference, follow from Parseval's theorem along x:
 //   sum_x Z_A(x, kz) conj Z_B(x, kz) = (1/nx) sum over all kx of Y_A conj Y_B,
 // where the half spectrum supplies kx > nx/2 as Y(nx - kx, kz) =
-// conj Y(kx, nz - kz).  Accumulation in FP64.
+// conj Y(kx, nz - kz).  The 2-D spectra are the same products of Y (k_spec2d).
+// Accumulation in FP64.
 #include "ch3d_ctx.h"
 #include "ch3d_dev.cuh"
 
@@ -105,6 +107,33 @@ __global__ void __launch_bounds__(128) k_specz(const CT* __restrict__ A, const C
   }
 }
 
+// 2-D spectra (clcSpecAndLCSR2DFrom1D / clcCosSpectra2D, :1896-2298): the
+// reference transforms the real and imaginary parts of the x spectrum along z
+// separately (R2HC) and sums Re(R_A conj R_B) + Re(I_A conj I_B), which is
+// Re(T(kx, kz) + T(kx, -kz)) / 2 of T = Y_A conj Y_B for 0 < kz < nz/2 and
+// Re T(kx, kz) at kz = 0, nz/2.  Rows folded about the centre:
+// out(kx, jc, kz) += norm (F(jc) + sgn F(ny-1-jc)), jc < ny/2, the layout
+// EnergySpec2D(nxc/2+1, nyc/2, nzc/2+1).  jref >= 0: B is row jref (below the
+// centre) or ny-1-jref (above) of the same spectrum.
+template <class CT>
+__global__ void k_spec2d(const CT* __restrict__ A, const CT* __restrict__ B, int nx, int ny, int nz, int jref, int sgn,
+                         double norm, double* __restrict__ out) {
+  const int nxh = nx / 2 + 1, nzh1 = nz / 2 + 1, nyh = ny / 2;
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y, jc = blockIdx.z;
+  if (kx >= nxh) return;
+  const int kzm = kz == 0 ? 0 : nz - kz;
+  const bool edge = kz == 0 || 2 * kz == nz;
+  auto F = [&](int j) {
+    const int jb = jref < 0 ? j : (j < nyh ? jref : ny - 1 - jref);
+    const CT a = A[kx + (size_t)nxh * (j + (size_t)ny * kz)], b = B[kx + (size_t)nxh * (jb + (size_t)ny * kz)];
+    double re = (double)a.x * b.x + (double)a.y * b.y;
+    if (edge) return re;
+    const CT c = A[kx + (size_t)nxh * (j + (size_t)ny * kzm)], d = B[kx + (size_t)nxh * (jb + (size_t)ny * kzm)];
+    return 0.5 * (re + (double)c.x * d.x + (double)c.y * d.y);
+  };
+  out[kx + (size_t)nxh * (jc + (size_t)nyh * kz)] += norm * (F(jc) + (double)sgn * F(ny - 1 - jc));
+}
+
 template <class T> static cudaError_t spectra_t(ch3d_ctx* c, int jf1, int jf2) {
   typedef typename CplxOf<T>::type CT;
   T** f = (T**)c->f;
@@ -112,6 +141,8 @@ template <class T> static cudaError_t spectra_t(ch3d_ctx* c, int jf1, int jf2) {
   const double normX = 1.0 / ((double)nx * (double)nx * (double)nz), normZ = 1.0 / ((double)nx * (double)nz * (double)nz);
   double* SX = c->specacc;                          // [m][j][kx]
   double* SZ = c->specacc + (size_t)18 * ny * nxh;  // [m][j][kz]
+  double* S2 = SZ + (size_t)18 * ny * nzh1;          // [m][kz][jc][kx], jc < ny/2
+  const double norm2 = 0.5 / ((double)nx * (double)nz * (double)nx * (double)nz);
   const size_t sbytes = (size_t)c->NS * sizeof(CT);
   cudaError_t e;
   auto field = [&](int which) {
@@ -135,6 +166,11 @@ template <class T> static cudaError_t spectra_t(ch3d_ctx* c, int jf1, int jf2) {
   auto sz = [&](const void* A, const void* B, int m, int jref, int part, int dbl) {
     k_specz<CT><<<dim3(nzh1, ny), 128, 0, c->stream>>>((const CT*)A, (const CT*)B, nx, ny, nz, jref, part, dbl, normZ,
                                                       SZ + (size_t)m * ny * nzh1);
+    return cudaGetLastError();
+  };
+  auto s2 = [&](const void* A, const void* B, int m, int jref, int sgn) {
+    k_spec2d<CT><<<dim3((nxh + 127) / 128, nzh1, ny / 2), 128, 0, c->stream>>>(
+        (const CT*)A, (const CT*)B, nx, ny, nz, jref, sgn, norm2, S2 + (size_t)m * nxh * (ny / 2) * nzh1);
     return cudaGetLastError();
   };
   // energy spectrum m and the coherence spectra (n, n+1, n+2) of the spectrum in c->spec, in both directions
@@ -161,10 +197,13 @@ template <class T> static cudaError_t spectra_t(ch3d_ctx* c, int jf1, int jf2) {
   CK(zfwd(c->spec));
   CK(zfwd(c->spec2));
   CK(energy_lcs(0, 6, false));
+  CK(s2(c->spec, c->spec, 0, -1, 1));
+  CK(s2(c->spec, c->spec, 5, jf1, 1));
   CK(sz(c->spec, c->spec2, 5, -1, 0, 1));
   CK(field(4));
   CK(zfwd(c->spec));
   CK(sz(c->spec, c->spec2, 4, -1, 0, 1));
+  CK(s2(c->spec, c->spec2, 4, -1, -1));  // UV: antisymmetric about the centre
   // VV, WW, PP
   const int which[3] = {1, 2, 3};
   for (int q = 0; q < 3; ++q) {
@@ -172,6 +211,8 @@ template <class T> static cudaError_t spectra_t(ch3d_ctx* c, int jf1, int jf2) {
     CK(energy_lcs(1 + q, 9 + 3 * q, true));
     CK(zfwd(c->spec));
     CK(energy_lcs(1 + q, 9 + 3 * q, false));
+    CK(s2(c->spec, c->spec, 1 + q, -1, 1));
+    CK(s2(c->spec, c->spec, 6 + q, jf1, 1));
   }
 #undef CK
   return cudaSuccess;

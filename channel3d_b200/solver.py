@@ -169,15 +169,17 @@ class ChannelSolver:
         coherence spectra against rows jForLCS(1:2) (1-based)."""
         _lib.check(self.lib.ch3d_spectra_accumulate(self.ctx, int(jfor[0]), int(jfor[1])), self.lib)
 
-    def spectra_fetch(self, reset=False):
-        """(EnergySpecX as (18, nyc, nxc/2+1), EnergySpecZ as (18, nyc, nzc/2+1), nSpectime)."""
+    def spectra_fetch(self, reset=False, two_d=False):
+        """(EnergySpecX as (18, nyc, nxc/2+1), EnergySpecZ as (18, nyc, nzc/2+1), nSpectime),
+        with two_d also EnergySpec2D as (9, nzc/2+1, nyc/2, nxc/2+1) before nSpectime."""
         c = self.cfg
         sx = np.empty((18, c.nyc, c.nxc // 2 + 1))
         sz = np.empty((18, c.nyc, c.nzc // 2 + 1))
+        s2 = np.empty((9, c.nzc // 2 + 1, c.nyc // 2, c.nxc // 2 + 1)) if two_d else None
         n = ctypes.c_int()
-        _lib.check(self.lib.ch3d_spectra_fetch(self.ctx, _lib.dptr(sx), _lib.dptr(sz), ctypes.byref(n), int(reset)),
-                   self.lib)
-        return sx, sz, n.value
+        _lib.check(self.lib.ch3d_spectra_fetch(self.ctx, _lib.dptr(sx), _lib.dptr(sz), _lib.dptr(s2), ctypes.byref(n),
+                                               int(reset)), self.lib)
+        return (sx, sz, s2, n.value) if two_d else (sx, sz, n.value)
 
     def stats_fetch_grad(self):
         """4th order: SumGrad(98, nyp) as (nyp, 98) (the vGrad moment sums)."""

@@ -61,3 +61,18 @@ def write_spectra(path_x, path_z, specx, specz, nspectime):
     for path, a in ((path_x, specx), (path_z, specz)):
         (np.ascontiguousarray(a, dtype=np.float64) * inf).tofile(path)
 
+
+def write_spectra2d(path, spec2d, nspectime):
+    """Spec2D%10.10d of the 4th order (src/CFD_4th/m_FlowCase.f90:1047-1140): the
+    EnergySpec2D(nxc/2+1, nyc/2, nzc/2+1, 9) sums / nSpectime weighted by Ratio2D
+    (4 inside, 2 on the kx = 0, nxc/2 and kz = 0, nzc/2 edges, 1 at the corners: the
+    wavenumbers the half spectra stand for), as native-endian FP32 (SAVE_SINGLE_Spec2D)
+    in Fortran order (the C order of the (9, nzc/2+1, nyc/2, nxc/2+1) array)."""
+    a = np.asarray(spec2d, dtype=np.float64)
+    nzh1, nxh = a.shape[1], a.shape[3]
+    r = np.full((nzh1, nxh), 4.0)
+    r[:, 0] = r[:, -1] = 2.0
+    r[0, :] = r[-1, :] = 2.0
+    r[0, 0] = r[0, -1] = r[-1, 0] = r[-1, -1] = 1.0
+    (a * (r[None, :, None, :] / nspectime)).astype(np.float32).tofile(path)
+

@@ -193,20 +193,25 @@ CH3D_API int ch3d_stats_accumulate(ch3d_ctx* ctx);
 CH3D_API int ch3d_stats_fetch(ch3d_ctx* ctx, double* sumstat, int* nfstime,
                      double* prgradsum, int reset);
 
-/* 4th order: one sample of the 1-D spectra of clcStat's clcSpectra1D branch
-   (src/CFD_4th/m_FlowCase.f90:642-880) from the current state, accumulated
-   on the device in FP64: per row jc, in x (nxc/2+1 wavenumbers) and in z
-   (nzc/2+1), 18 spectra in the order of the reference's iSpec1D* indices
-   (:43-60): UU VV WW PP UV UV2, then for UU, VV, WW, PP the linear coherence
-   spectra R1 I1 R2 against rows jForLCS(1) and jForLCS(2) (1..nyc/2, mirrored
-   above the centre).  The first call allocates a second half spectrum and the
-   sums. */
+/* 4th order: one sample of the spectra of clcStat (src/CFD_4th/m_FlowCase.f90:
+   642-935) from the current state, accumulated on the device in FP64.  1-D
+   (clcSpectra1D): per row jc, in x (nxc/2+1 wavenumbers) and in z (nzc/2+1),
+   18 spectra in the order of the iSpec1D* indices (:43-60): UU VV WW PP UV
+   UV2, then for UU, VV, WW, PP the linear coherence spectra R1 I1 R2 against
+   rows jForLCS(1) and jForLCS(2) (1..nyc/2, mirrored above the centre).  2-D
+   (clcSpectra2D): per (kx, jc <= nyc/2, kz) the 9 spectra of the iSpec2D*
+   indices (:62-72): UU VV WW PP UV and the coherence spectra R of UU, VV,
+   WW, PP against row jForLCS(1), the two halves of the channel folded
+   together.  The first call allocates a second half spectrum and the sums. */
 CH3D_API int ch3d_spectra_accumulate(ch3d_ctx* ctx, int jForLCS1, int jForLCS2);
 
-/* The sums EnergySpecX(nxc/2+1, nyc, 18) and EnergySpecZ(nzc/2+1, nyc, 18) in
-   Fortran order (the SpecX / SpecZ files hold them divided by nSpectime), and
-   nSpectime; any pointer may be NULL; reset zeroes them. */
-CH3D_API int ch3d_spectra_fetch(ch3d_ctx* ctx, double* specx, double* specz, int* nSpectime, int reset);
+/* The sums EnergySpecX(nxc/2+1, nyc, 18), EnergySpecZ(nzc/2+1, nyc, 18) and
+   EnergySpec2D(nxc/2+1, nyc/2, nzc/2+1, 9) in Fortran order (the SpecX /
+   SpecZ files hold the 1-D sums divided by nSpectime; Spec2D the 2-D sums
+   divided by nSpectime and weighted by Ratio2D, :1050-1100), and nSpectime;
+   any pointer may be NULL; reset zeroes them. */
+CH3D_API int ch3d_spectra_fetch(ch3d_ctx* ctx, double* specx, double* specz, double* spec2d, int* nSpectime,
+                                int reset);
 
 /* 4th order: the gradient moments SumGrad(98,nyp) of clcStat
    (HighOrderGradStat, src/CFD_4th/m_FlowCase.f90:485-589, the vGrad file's

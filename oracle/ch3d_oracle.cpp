@@ -2037,12 +2037,14 @@ struct Oracle {
   //      clcCospectraX/Z (:1152-1266), clcLTS_x/z (:1271-1632) and transform_uy
   //      (:2303-2332); R2HC transforms of every x and z line (FFTW_R2HC). ----
   std::vector<double> EnergySpecX, EnergySpecZ;  // (nxhp, nyc, 18), (nzhp, nyc, 18)
+  std::vector<double> EnergySpec2D;              // (nxhp, nyc/2, nzhp, 9)
   int nSpectime = 0;
   void clcSpectra1D(int jFor1, int jFor2) {
     const int nxh = nxc / 2, nxhp = nxh + 1, nzh = nzc / 2, nzhp = nzh + 1;
     if (EnergySpecX.empty()) {
       EnergySpecX.assign((size_t)nxhp * nyc * 18, 0.0);
       EnergySpecZ.assign((size_t)nzhp * nyc * 18, 0.0);
+      EnergySpec2D.assign((size_t)nxhp * (nyc / 2) * nzhp * 9, 0.0);
     }
     const size_t N3 = (size_t)nxc * nyc * nzc;
     auto I3 = [&](int ic, int jc, int kc) { return (size_t)(ic - 1) + (size_t)nxc * ((size_t)(jc - 1) + (size_t)nyc * (kc - 1)); };
@@ -2176,6 +2178,67 @@ struct Oracle {
       cospZ(v, v, 1); ltsZ(v, 9, 10, 11);
       cospZ(w, w, 2); ltsZ(w, 12, 13, 14);
       cospZ(pp, pp, 3); ltsZ(pp, 15, 16, 17);
+    }
+    // ---- 2-D spectra (clcSpecAndLCSR2DFrom1D :1896-2138, clcCosSpectra2D :2143-2298):
+    //      the real part (ic = 1..nxhp) and the imaginary part (ic = 2..nxh, from
+    //      nxc+2-ic) of every x spectrum transformed along z (R2HC); the two
+    //      halves of the channel folded together (UV antisymmetric). ----
+    {
+      const int nyh = nyc / 2;
+      const double norm2 = one / ((double)nxc * (double)nzc) / ((double)nxc * (double)nzc) * half;
+      auto S2 = [&](int ic, int jc, int kc, int m) -> double& {
+        return EnergySpec2D[(size_t)(ic - 1) + (size_t)nxhp * ((size_t)(jc - 1) + (size_t)nyh * ((size_t)(kc - 1) + (size_t)nzhp * m))];
+      };
+      // z transforms of the real and imaginary parts: (nxhp, nyc, nzc) each
+      auto parts = [&](const std::vector<double>& h, std::vector<double>& R, std::vector<double>& I) {
+        R.assign((size_t)nxhp * nyc * nzc, 0.0);
+        I.assign((size_t)nxhp * nyc * nzc, 0.0);
+        auto P3 = [&](int ic, int jc, int kc) { return (size_t)(ic - 1) + (size_t)nxhp * ((size_t)(jc - 1) + (size_t)nyc * (kc - 1)); };
+        std::vector<double> lr(nzc), li(nzc);
+        for (int jc = 1; jc <= nyc; ++jc)
+          for (int ic = 1; ic <= nxhp; ++ic) {
+            for (int kc = 1; kc <= nzc; ++kc) {
+              lr[kc - 1] = h[I3(ic, jc, kc)];
+              li[kc - 1] = (ic == 1 || ic == nxhp) ? zero : h[I3(nxc + 2 - ic, jc, kc)];
+            }
+            r2hc(planz, lr.data(), ba, bb);
+            r2hc(planz, li.data(), ba, bb);
+            for (int kc = 1; kc <= nzc; ++kc) { R[P3(ic, jc, kc)] = lr[kc - 1]; I[P3(ic, jc, kc)] = li[kc - 1]; }
+          }
+      };
+      auto P3 = [&](int ic, int jc, int kc) { return (size_t)(ic - 1) + (size_t)nxhp * ((size_t)(jc - 1) + (size_t)nyc * (kc - 1)); };
+      // sum over the real and imaginary parts of the z-spectrum products of rows j (A) and jb (B)
+      auto prod = [&](const std::vector<double>& RA, const std::vector<double>& IA, const std::vector<double>& RB,
+                      const std::vector<double>& IB, int ic, int j, int jb, int kc) {
+        if (kc == 1 || kc == nzhp)
+          return RA[P3(ic, j, kc)] * RB[P3(ic, jb, kc)] + IA[P3(ic, j, kc)] * IB[P3(ic, jb, kc)];
+        const int kct = nzc + 2 - kc;
+        return RA[P3(ic, j, kc)] * RB[P3(ic, jb, kc)] + RA[P3(ic, j, kct)] * RB[P3(ic, jb, kct)] +
+               IA[P3(ic, j, kc)] * IB[P3(ic, jb, kc)] + IA[P3(ic, j, kct)] * IB[P3(ic, jb, kct)];
+      };
+      auto acc2 = [&](const std::vector<double>& RA, const std::vector<double>& IA, const std::vector<double>& RB,
+                      const std::vector<double>& IB, int m, bool lcs, double rCoe) {
+        for (int jc = 1; jc <= nyh; ++jc) {
+          const int jcs = nyc + 1 - jc;
+          const int ja = lcs ? jFor1 : jc, jb = lcs ? nyc + 1 - jFor1 : jcs;
+          for (int kc = 1; kc <= nzhp; ++kc)
+            for (int ic = 1; ic <= nxhp; ++ic)
+              S2(ic, jc, kc, m) = S2(ic, jc, kc, m) +
+                                  norm2 * (prod(RA, IA, RB, IB, ic, jc, ja, kc) + rCoe * prod(RA, IA, RB, IB, ic, jcs, jb, kc));
+        }
+      };
+      std::vector<double> R1, I1, R2, I2;
+      parts(hcx(qux), R1, I1);
+      acc2(R1, I1, R1, I1, 0, false, one); acc2(R1, I1, R1, I1, 5, true, one);
+      parts(hcx(quxc), R1, I1);
+      parts(hcx(quyc), R2, I2);
+      acc2(R1, I1, R2, I2, 4, false, -one);
+      const std::vector<double>* qs[3] = {&quy, &quz, &qpr};
+      for (int q = 0; q < 3; ++q) {
+        parts(hcx(*qs[q]), R1, I1);
+        acc2(R1, I1, R1, I1, 1 + q, false, one);
+        acc2(R1, I1, R1, I1, 6 + q, true, one);
+      }
     }
     nSpectime += 1;
   }
@@ -2485,6 +2548,14 @@ int orc_spectra_get(void* h, double* specx, double* specz) {
   const size_t nx = (size_t)(o->nxc / 2 + 1) * o->nyc * 18, nz = (size_t)(o->nzc / 2 + 1) * o->nyc * 18;
   for (size_t q = 0; q < nx; ++q) specx[q] = o->EnergySpecX.empty() ? 0.0 : o->EnergySpecX[q];
   for (size_t q = 0; q < nz; ++q) specz[q] = o->EnergySpecZ.empty() ? 0.0 : o->EnergySpecZ[q];
+  return o->nSpectime;
+}
+
+// EnergySpec2D(nxhp, nyc/2, nzhp, 9) sums; returns nSpectime.
+int orc_spectra_get2d(void* h, double* spec2d) {
+  Oracle* o = (Oracle*)h;
+  const size_t n = (size_t)(o->nxc / 2 + 1) * (o->nyc / 2) * (o->nzc / 2 + 1) * 9;
+  for (size_t q = 0; q < n; ++q) spec2d[q] = o->EnergySpec2D.empty() ? 0.0 : o->EnergySpec2D[q];
   return o->nSpectime;
 }
 

@@ -96,6 +96,8 @@ def lib():
         L.orc_spectra_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.orc_spectra_get.restype = ctypes.c_int
         L.orc_spectra_get.argtypes = [ctypes.c_void_p, _DP, _DP]
+        L.orc_spectra_get2d.restype = ctypes.c_int
+        L.orc_spectra_get2d.argtypes = [ctypes.c_void_p, _DP]
         _lib = L
     return _lib
 
@@ -256,6 +258,13 @@ class Oracle:
         sz = np.empty((18, c.nyc, c.nzc // 2 + 1))
         n = self.L.orc_spectra_get(self.h, _p(sx), _p(sz))
         return sx, sz, n
+
+    def spectra_get2d(self):
+        """EnergySpec2D as (9, nzc/2+1, nyc/2, nxc/2+1), and nSpectime."""
+        c = self.cfg
+        s2 = np.empty((9, c.nzc // 2 + 1, c.nyc // 2, c.nxc // 2 + 1))
+        n = self.L.orc_spectra_get2d(self.h, _p(s2))
+        return s2, n
 
     def stats_get_grad(self):
         """4th order: SumGrad(98, nyp) as (nyp, 98), and nfstime."""

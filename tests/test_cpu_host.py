@@ -247,3 +247,8 @@ def test_spectra_writer(tmp_path):
     bz = np.fromfile(str(tmp_path / "SpecZ"), dtype=np.float64)
     assert bx.size == sx.size and np.allclose(bx.reshape(9, 5, 18, order="F"), np.moveaxis(sx, [0, 1, 2], [2, 1, 0]))
     assert np.allclose(bz, sz.ravel())
+    s2 = np.ones((9, 3, 5, 4))
+    stats.write_spectra2d(str(tmp_path / "Spec2D"), s2 * 2, 2)
+    b2 = np.fromfile(str(tmp_path / "Spec2D"), dtype=np.float32).reshape(9, 3, 5, 4)
+    assert b2[0, 1, 2, 1] == 4 and b2[0, 0, 2, 1] == 2 and b2[0, 1, 2, 3] == 2 and b2[0, 2, 0, 0] == 1
+

@@ -1,12 +1,15 @@
-"""One-dimensional spectra of the 4th-order statistics on the device
+"""Spectra of the 4th-order statistics on the device
 (ch3d_spectra_accumulate: clcStat's clcSpectra1D branch,
 src/CFD_4th/m_FlowCase.f90:642-880, with clcEnergySpectraX/Z,
-clcCospectraX/Z and clcLTS_x/z) against the oracle, which transforms every
-x and z line with R2HC as the reference does; the device reaches the z
-spectra through the 2-D spectrum and Parseval's theorem along x.
+clcCospectraX/Z and clcLTS_x/z, and its clcSpectra2D branch with
+clcSpecAndLCSR2DFrom1D and clcCosSpectra2D, :1896-2298) against the oracle,
+which transforms every x and z line with R2HC as the reference does; the
+device reaches the z and 2-D spectra through the 2-D spectrum and Parseval's
+theorem along x.
 
-Tolerance: each of the 2 x 18 spectra within 1e-10 of its largest magnitude
-(FP64), 1e-4 for the mixed path's energy spectra."""
+Tolerance: each of the 2 x 18 one-dimensional and 9 two-dimensional spectra
+within 1e-10 of its largest magnitude (FP64), 1e-4 for the mixed path's
+energy spectra."""
 import numpy as np
 import pytest
 
@@ -42,13 +45,17 @@ def test_spectra_parity_4th(built, shape):
         o.step(2)
         s.spectra_accumulate(jfor)
         o.spectra_accumulate(jfor)
-    ax, az, na = s.spectra_fetch()
+    ax, az, a2, na = s.spectra_fetch(two_d=True)
     bx, bz, nb = o.spectra_get()
+    b2, _ = o.spectra_get2d()
     assert na == nb == 2
     for m in range(18):
         for a, b, d in ((ax, bx, "x"), (az, bz, "z")):
             e = np.abs(a[m] - b[m]).max() / max(np.abs(b[m]).max(), 1e-300)
             assert e < 1e-10, (d, m, e)
+    for m in range(9):  # the 2-D spectra (clcSpectra2D)
+        e = np.abs(a2[m] - b2[m]).max() / max(np.abs(b2[m]).max(), 1e-300)
+        assert e < 1e-10, ("2d", m, e)
     s.spectra_fetch(reset=True)
     ax, az, n = s.spectra_fetch()
     assert n == 0 and not ax.any() and not az.any()

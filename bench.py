@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision timing of an FP64 run")
+    ap.add_argument("--les-type", type=int, default=0,
+                    help="LES closure of an LES workload: 2 WALE, 3 MTS, 10 Smagorinsky / van Driest, 11 the learned "
+                         "closure (the network's seeded initial weights, inputs never out of range)")
     ap.add_argument("--cpu-nz", type=int, default=48,
                     help="z planes of the CPU sample (the CPU-baseline leg and --impl reference)")
     ap.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the CPU-baseline leg")
@@ -282,8 +285,15 @@ def measure(args, ws, rank, local, precision, want_e2e):
     from channel3d_b200 import ChannelSolver, initfield, workloads
     cfg, _ = workloads.get(args.workload, precision=precision)
     cfg = cfg.copy(device=local)
+    if args.les_type:
+        cfg = cfg.copy(LES_type=args.les_type, Cs=0.1)
     torch.cuda.set_device(local)
     s = ChannelSolver(cfg)
+    if args.les_type == 11:  # the learned closure: seeded weights, a standardisation that accepts every input
+        from channel3d_b200.mlp import MLPClosure
+        norm = np.zeros(52, dtype=np.float32)
+        norm[10:20], norm[20:30], norm[30:40], norm[46:52] = 1.0, -1e30, 1e30, 1.0
+        s.sgs_mlp_set(MLPClosure(seed=0, device=local).params(), norm)
     ux, uy, uz, p = initfield.laminar_noise(cfg, yp=s.yp)
     s.upload(ux, uy, uz, p)
     s.project()
@@ -382,7 +392,8 @@ def run_ours(args, ws, rank, local):
     cfg = main["cfg"]
     # the other precision of the same workload, in the same process (FP64 against mixed)
     other = None
-    if not args.no_mixed and args.precision == "fp64" and scheme_key(cfg) in ("pimp", "order4", "fimp"):
+    if not args.no_mixed and args.precision == "fp64" and scheme_key(cfg) in ("pimp", "order4", "fimp") \
+            and not args.les_type:
         other = measure(args, ws, rank, local, "mixed", not args.no_e2e)
 
     cpu = None

@@ -55,9 +55,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");  // visible to the tensor-core commit
 }
 // bounded wait for the phase with the given parity; false on expiry
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned limit = WAIT_LIMIT) {
   const uint32_t a = su32(bar);
-  for (unsigned it = 0; it < WAIT_LIMIT; ++it) {
+  for (unsigned it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -381,6 +381,17 @@ __global__ void k_adam(float* __restrict__ P, const float* __restrict__ g, float
 constexpr size_t SMEM_FWD = 1024 + TILE * NINP * 2 + TILE * NH * 2 + NH * NINP * 2 + 2 * NH * NH * 2 + NOUTP * NH * 2;
 constexpr size_t SMEM_BWD = 1024 + TILE * NH * 2 + TILE * TILE * 2 + NH * TILE * 2 + NH * NH * 2 + 4 * 64 * 4;
 
+// The expiry path of the bounded waits: one thread waits on an mbarrier that
+// nothing arrives at (no MMA issued, no tensor memory held) and, when the
+// wait gives up after `limit` polls, records the expiry in *status as the
+// MLP kernels do.
+__global__ void k_mlp_wait_check(unsigned limit, int* __restrict__ status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  if (!mbar_wait(&bar, 0, limit)) atomicExch(status, 1);
+}
+
 }  // namespace ch3d_mlp
 
 using namespace ch3d_mlp;
@@ -399,6 +410,12 @@ CH3D_MLP_API size_t ch3d_mlp_workspace_bytes(int batch) {
   const size_t nb = (size_t)(batch + TILE - 1) / TILE;
   return (size_t)3 * batch * NH * 4 + (size_t)3 * batch * NH * 2 + (size_t)batch * NOUT * 4 + nb * NPARAM * 4 + nb * 4 +
          256;
+}
+
+CH3D_MLP_API int ch3d_mlp_wait_check(unsigned limit, int* status, void* stream) {
+  if (!status || limit == 0) return 1;
+  k_mlp_wait_check<<<1, 32, 0, (cudaStream_t)stream>>>(limit, status);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 CH3D_MLP_API int ch3d_mlp_forward(const float* X, int batch, const float* params, float* Y, int* status,

@@ -47,6 +47,13 @@ CH3D_MLP_API int ch3d_mlp_grad(const float* X, const float* T, int batch, const 
 CH3D_MLP_API int ch3d_mlp_adam(float* params, const float* grad, float* m, float* v, float lr, float beta1,
                                float beta2, float eps, int step, void* stream);
 
+/* Failure detection of the tensor-core kernels without a fault: runs their
+   bounded mbarrier wait, `limit` polls long, on a barrier nothing completes
+   (no MMA in flight, no tensor memory held) and sets *status to 1 when the
+   wait gives up, as a kernel whose tensor-core work never completes does;
+   the context stays usable. */
+CH3D_MLP_API int ch3d_mlp_wait_check(unsigned limit, int* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -259,15 +259,13 @@ int alloc_fields(ch3d_ctx* c) {
   }
   if (c->cfg.LES_type == CH3D_LES_MLP) {
     CU(cudaMalloc(&c->mlp_params, CH3D_MLP_NPARAM * sizeof(float)));
-    CU(cudaMalloc(&c->mlp_x, (size_t)c->N * 10 * sizeof(float)));
-    CU(cudaMalloc(&c->mlp_y, (size_t)c->N * 6 * sizeof(float)));
-    CU(cudaMalloc(&c->mlp_fb, (size_t)c->N));
     CU(cudaMalloc(&c->mlp_status, sizeof(int)));
     CU(cudaMemsetAsync(c->mlp_status, 0, sizeof(int), c->stream));
     CU(cudaMalloc(&c->sgs_tau, (size_t)c->N * 6 * sizeof(double)));
     CU(cudaMalloc(&c->sgs_f, (size_t)c->N * 3 * sizeof(double)));
     CU(cudaMemsetAsync(c->sgs_f, 0, (size_t)c->N * 3 * sizeof(double), c->stream));
-    c->bytes += (long long)c->N * (16 * 4 + 1 + 9 * 8);
+    CU(launch_fill_nut(c));  // the closure's total viscosity stays xnu
+    c->bytes += (long long)c->N * 9 * 8;
   }
   if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
     const size_t nb = ptri_factor_doubles(c->nx, c->nz) * sizeof(double);
@@ -692,7 +690,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   for (int q = 0; q < 6; ++q) if (c->ih[q]) cudaFree(c->ih[q]);
   if (c->pfac) cudaFree(c->pfac);
   if (c->les_delta) cudaFree(c->les_delta);
-  void* mbufs[] = {c->mlp_params, c->mlp_x, c->mlp_y, c->mlp_fb, c->mlp_status, c->sgs_tau, c->sgs_f, c->spec2,
+  void* mbufs[] = {c->mlp_params, c->mlp_status, c->sgs_tau, c->sgs_f, c->spec2,
                    c->specacc};
   for (void* b : mbufs) if (b) cudaFree(b);
   void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,

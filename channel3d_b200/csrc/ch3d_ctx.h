@@ -41,9 +41,6 @@ struct ch3d_ctx {
   float* mlp_params = nullptr;   // CH3D_MLP_NPARAM FP32
   float mlp_norm[CH3D_SGS_NORM_FLOATS] = {0};
   bool mlp_ready = false;
-  float* mlp_x = nullptr;        // N x 10 inputs
-  float* mlp_y = nullptr;        // N x 6 outputs
-  unsigned char* mlp_fb = nullptr;  // N fallback flags
   int* mlp_status = nullptr;
   double* sgs_tau = nullptr;     // 6 N stresses at the cell centres
   double* sgs_f = nullptr;       // 3 N stress-divergence forces at the velocity points
@@ -150,6 +147,7 @@ cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP -> Rh
 cudaError_t launch_ptri_xz(ch3d_ctx* c);               // periodic x and z sweeps of RhsX/Y/Z, in place
 size_t ptri_factor_doubles(int nx, int nz);
 // LES (ch3d_les.cu), FP64
+cudaError_t launch_fill_nut(ch3d_ctx* c);              // nut = xnu (learned closure)
 cudaError_t launch_sgs_nut(ch3d_ctx* c);               // Clc_SGS_Vis -> nut
 cudaError_t launch_rhs_les(ch3d_ctx* c);               // clcRhsX/Y/Z_PIMP_LES -> RhsX/Y/Z
 cudaError_t launch_uhat_les(ch3d_ctx* c);              // clcU1/2/3Hat_PIMP_LES -> u*

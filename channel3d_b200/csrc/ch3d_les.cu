@@ -11,6 +11,7 @@
 #include "../../include/ch3d_mlp.h"
 #include "ch3d_ctx.h"
 #include "ch3d_dev.cuh"
+#include "mlp_tc.cuh"
 
 namespace ch3d {
 
@@ -379,59 +380,70 @@ __device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metri
   G[8] = (at(uz, n, n.zp) - at(uz, n, 0)) * rdz;
 }
 
-// inputs X [N x 10] (FP32, standardised; gradients in wall units g nu / u_tau^2,
-// then y+), the fallback stress of every point into tau [6][N] and the
-// out-of-range flag
-__global__ void __launch_bounds__(256) k_sgs_features(Geo<double> g, Metrics<double> m, LesPar lp, MlpNorm nm,
-                                                      const double* __restrict__ ux, const double* __restrict__ uy,
-                                                      const double* __restrict__ uz, float* __restrict__ X,
-                                                      double* __restrict__ tau, unsigned char* __restrict__ fb,
-                                                      const DevScalars* __restrict__ sc) {
-  if (sc->status) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i >= g.nx || j >= g.ny) return;
-  const Nbr n = make_nbr(g, i, j, k);
-  const int jc = j + 1;
-  double G[9];
-  cell_gradients(g, m, ux, uy, uz, n, jc, G);
-  const double ut = sc->utau > 1e-30 ? sc->utau : 1e-30;
-  const double gs = (double)g.xnu / (ut * ut);
-  const double yplus = lp.dwall[jc] * ut / (double)g.xnu;
-  bool out = false;
-  for (int q = 0; q < 10; ++q) {
-    const double v = q < 9 ? G[q] * gs : yplus;
-    const float xs = (float)((v - nm.in_mean[q]) / nm.in_std[q]);
-    X[n.c * 10 + q] = xs;
-    out = out || !(xs >= nm.in_lo[q] && xs <= nm.in_hi[q]);
-  }
-  fb[n.c] = out ? 1 : 0;
-  // Smagorinsky / van Driest stress: tau_ij = -2 nu_t S_ij
-  const double S11 = G[0], S22 = G[4], S33 = G[8];
-  const double S12 = 0.5 * (G[1] + G[3]), S13 = 0.5 * (G[2] + G[6]), S23 = 0.5 * (G[5] + G[7]);
-  const double Smag = sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23)));
-  const double D = 1.0 - exp(-yplus / 26.0);
-  const double l = lp.Cs * D * lp.delta[jc];
-  const double nt = l * l * Smag;
+// The learned closure's stresses, one tile of 128 consecutive cells per CTA:
+// each thread forms its cell's network inputs (the nine cell-centre velocity
+// gradients in wall units g nu / u_tau^2, then y+; standardised in FP64 and
+// rounded to FP32) and the Smagorinsky / van Driest fallback stress
+// -2 nu_t S_ij, the CTA runs the network on the tensor cores (mlp_tc.cuh),
+// and each thread writes tau [6][N]: the network's output de-standardised
+// and scaled by u_tau^2, or the fallback where an input left the training
+// range.  When a wait on the tensor cores expires the kernel records it in
+// *mstatus and writes the fallback stresses.
+__global__ void __launch_bounds__(ch3d_mlp::TILE, 4)
+    k_sgs_mlp(Geo<double> g, Metrics<double> m, LesPar lp, MlpNorm nm, const double* __restrict__ ux,
+              const double* __restrict__ uy, const double* __restrict__ uz, const float* __restrict__ P,
+              double* __restrict__ tau, int* __restrict__ mstatus, const DevScalars* __restrict__ sc) {
+  using namespace ch3d_mlp;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  if (sc->status) return;  // uniform: every thread reads the same word
   const long long N = g.N;
-  tau[0 * N + n.c] = -2.0 * nt * S11;
-  tau[1 * N + n.c] = -2.0 * nt * S12;
-  tau[2 * N + n.c] = -2.0 * nt * S13;
-  tau[3 * N + n.c] = -2.0 * nt * S22;
-  tau[4 * N + n.c] = -2.0 * nt * S23;
-  tau[5 * N + n.c] = -2.0 * nt * S33;
-}
-
-// network outputs -> tau (kept: the fallback stress where the input left the range)
-__global__ void __launch_bounds__(256) k_sgs_tau(long long N, MlpNorm nm, const float* __restrict__ Y,
-                                                 const unsigned char* __restrict__ fb, double* __restrict__ tau,
-                                                 const DevScalars* __restrict__ sc) {
-  if (sc->status) return;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= N || fb[c]) return;
+  const long long c = (long long)blockIdx.x * TILE + threadIdx.x;
+  const bool valid = c < N;
+  float x[NIN];
+  double fb[6] = {0, 0, 0, 0, 0, 0};
+  bool out = true;
+  const double ut = sc->utau > 1e-30 ? sc->utau : 1e-30;
+  if (valid) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const Nbr n = make_nbr(g, i, j, k);
+    const int jc = j + 1;
+    double G[9];
+    cell_gradients(g, m, ux, uy, uz, n, jc, G);
+    const double gs = (double)g.xnu / (ut * ut);
+    const double yplus = lp.dwall[jc] * ut / (double)g.xnu;
+    out = false;
+#pragma unroll
+    for (int q = 0; q < NIN; ++q) {
+      const double v = q < 9 ? G[q] * gs : yplus;
+      const float xs = (float)((v - nm.in_mean[q]) / nm.in_std[q]);
+      x[q] = xs;
+      out = out || !(xs >= nm.in_lo[q] && xs <= nm.in_hi[q]);
+    }
+    const double S11 = G[0], S22 = G[4], S33 = G[8];
+    const double S12 = 0.5 * (G[1] + G[3]), S13 = 0.5 * (G[2] + G[6]), S23 = 0.5 * (G[5] + G[7]);
+    const double Smag = sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23)));
+    const double D = 1.0 - exp(-yplus / 26.0);
+    const double l = lp.Cs * D * lp.delta[jc];
+    const double nt = l * l * Smag;
+    fb[0] = -2.0 * nt * S11;
+    fb[1] = -2.0 * nt * S12;
+    fb[2] = -2.0 * nt * S13;
+    fb[3] = -2.0 * nt * S22;
+    fb[4] = -2.0 * nt * S23;
+    fb[5] = -2.0 * nt * S33;
+  } else {
+#pragma unroll
+    for (int q = 0; q < NIN; ++q) x[q] = 0.f;
+  }
+  fwd_prologue(smem, P, x);
+  float y[NOUT];
+  const bool ok = fwd_layers(smem, y, nullptr, nullptr, c, valid, N);
+  if (!ok && threadIdx.x == 0) atomicExch(mstatus, 1);
+  if (!valid) return;
   const double u2 = sc->utau * sc->utau;
-  for (int q = 0; q < 6; ++q) tau[q * N + c] = ((double)Y[c * 6 + q] * nm.out_std[q] + nm.out_mean[q]) * u2;
+#pragma unroll
+  for (int q = 0; q < NOUT; ++q)
+    tau[q * N + c] = (out || !ok) ? fb[q] : ((double)y[q] * nm.out_std[q] + nm.out_mean[q]) * u2;
 }
 
 // f_i = -d tau_ij / dx_j at the staggered points of u_i.  Off-diagonal
@@ -561,21 +573,35 @@ cudaError_t launch_sgs_nut(ch3d_ctx* c) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  k_sgs_nut<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, f[0], f[1], f[2], f[11], c->sc);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || lp.model != CH3D_LES_MLP) return e;
+  // the learned closure keeps nut = xnu (filled when the context was created)
+  if (lp.model != CH3D_LES_MLP) {
+    k_sgs_nut<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, f[0], f[1], f[2], f[11], c->sc);
+    return cudaGetLastError();
+  }
   MlpNorm nm;
   static_assert(sizeof(MlpNorm) == CH3D_SGS_NORM_FLOATS * sizeof(float), "norm layout");
   memcpy(&nm, c->mlp_norm, sizeof(nm));
-  k_sgs_features<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, nm, f[0], f[1], f[2], c->mlp_x, c->sgs_tau,
-                                                             c->mlp_fb, c->sc);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if (ch3d_mlp_forward(c->mlp_x, (int)c->N, c->mlp_params, c->mlp_y, c->mlp_status, c->stream) != 0)
-    return cudaErrorLaunchFailure;
-  k_sgs_tau<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>(c->N, nm, c->mlp_y, c->mlp_fb, c->sgs_tau, c->sc);
+  static PerDevice attr;
+  cudaError_t e = once_per_device(attr, c->device, [] {
+    return cudaFuncSetAttribute(k_sgs_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ch3d_mlp::FwdSmem::BYTES);
+  });
+  if (e != cudaSuccess) return e;
+  k_sgs_mlp<<<(unsigned)((c->N + ch3d_mlp::TILE - 1) / ch3d_mlp::TILE), ch3d_mlp::TILE, ch3d_mlp::FwdSmem::BYTES,
+              c->stream>>>(g, c->m64, lp, nm, f[0], f[1], f[2], c->mlp_params, c->sgs_tau, c->mlp_status, c->sc);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_sgs_force<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, c->sgs_tau, c->sgs_f, c->sgs_f + c->N,
                                                           c->sgs_f + 2 * c->N, c->sc);
+  return cudaGetLastError();
+}
+
+// nut = xnu everywhere (the learned closure's total viscosity)
+__global__ void k_fill_nut(double* __restrict__ nut, long long N, double xnu) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < N) nut[q] = xnu;
+}
+
+cudaError_t launch_fill_nut(ch3d_ctx* c) {
+  k_fill_nut<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>((double*)c->f[11], c->N, (double)c->cfg.xnu);
   return cudaGetLastError();
 }
 

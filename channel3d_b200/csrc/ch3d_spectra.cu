@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(128) k_specz(const CT* __restrict__ A, const C
 template <class CT>
 __global__ void k_spec2d(const CT* __restrict__ A, const CT* __restrict__ B, int nx, int ny, int nz, int jref, int sgn,
                          double norm, double* __restrict__ out) {
-  const int nxh = nx / 2 + 1, nzh1 = nz / 2 + 1, nyh = ny / 2;
+  const int nxh = nx / 2 + 1, nyh = ny / 2;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y, jc = blockIdx.z;
   if (kx >= nxh) return;
   const int kzm = kz == 0 ? 0 : nz - kz;

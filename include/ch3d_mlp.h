@@ -1,6 +1,7 @@
 /* ch3d_mlp.h -- the learned subgrid-stress closure of the LES step: a
-   10 -> 64 -> 64 -> 64 -> 6 multilayer perceptron (GELU activations, BF16
-   tensor-core operands, FP32 accumulation) trained and evaluated on the GPU.
+   10 -> 64 -> 64 -> 64 -> 6 multilayer perceptron (GELU activations in their
+   tanh form, BF16 tensor-core operands, FP32 accumulation) trained and
+   evaluated on the GPU.
    No counterpart in the reference (its LES models are the eddy-viscosity
    closures of src/CFD_2nd/m_LESModels.f90); the LES step calls it in place
    of Clc_SGS_Vis when LES_type = CH3D_LES_MLP.

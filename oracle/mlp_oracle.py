@@ -1,14 +1,14 @@
 """CPU restatement of the learned SGS closure's network (channel3d_b200/csrc/mlp_tc.cu).
 
 TEST INFRASTRUCTURE ONLY: the checker of the tensor-core forward and
-backward kernels.  A 10 -> 64 -> 64 -> 64 -> 6 MLP with exact (erf) GELU;
+backward kernels.  A 10 -> 64 -> 64 -> 64 -> 6 MLP with the tanh form of
+GELU (Hendrycks & Gimpel 2016);
 every GEMM operand is rounded to BF16 (round to nearest even) where the
 device rounds it, products are accumulated in FP64, biases, pre-activations
 and the loss stay unrounded.  The model has no counterpart in the reference,
 so this restatement is pinned by finite differences (tests/test_mlp_oracle.py).
 """
 import numpy as np
-from scipy.special import erf
 
 NIN, NH, NOUT = 10, 64, 6
 SHAPES = [("W1", (NH, NIN)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("W3", (NH, NH)), ("b3", (NH,)),
@@ -55,12 +55,17 @@ def init_params(seed=0):
     return pack(d).astype(np.float32)
 
 
+C_GELU = np.sqrt(2.0 / np.pi)
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(C_GELU * (z + 0.044715 * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(C_GELU * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * C_GELU * (1.0 + 3.0 * 0.044715 * z * z)
 
 
 def forward(P, X):

@@ -461,8 +461,7 @@ int record_step(ch3d_ctx* c) {
     CU(launch_substep_setup(c, ns));
     if (march_path(c)) {  // RHS + y solves as one column march, its own Thomas factors
       CU(launch_rhs_march(c));
-    } else if (c->cfg.LES_type > 0) {
-      CU(launch_helm_factors(c));
+    } else if (c->cfg.LES_type > 0) {  // the LES y solves form their own coefficients
       CU(launch_rhs_les(c));
       CU(launch_uhat_les(c));
     } else if (fimp) {
@@ -1076,7 +1075,7 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
       CU(mark(6));
       if (c->cfg.order == 4) CU(launch_visc4_partials(c));
       CU(launch_substep_setup(c, ns));
-      if (!march_path(c) && c->cfg.order != 4) CU(launch_helm_factors(c));
+      if (!march_path(c) && c->cfg.order != 4 && c->cfg.LES_type == 0) CU(launch_helm_factors(c));
       CU(done());
       if (march_path(c)) {
         CU(mark(0)); CU(launch_rhs_march(c)); CU(done());

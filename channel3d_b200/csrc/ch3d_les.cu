@@ -283,6 +283,30 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
 // (InverseTridiagonal, src/CFD_2nd/m_Tools.f90:224-251) with the column's own
 // coefficients; the u* buffer holds the elimination factors until the back
 // substitution overwrites them.  blockIdx.y = component.
+// coefficients (a, b, c) of row j of the variable-viscosity Crank-Nicolson
+// system of component comp in column (i, k)
+__device__ __forceinline__ void uhat_les_coef(const Geo<double>& g, const HelmCoef& hc, const double* __restrict__ nut,
+                                              double pmBetaT, int comp, int i, int j, int k, double& a, double& b,
+                                              double& c) {
+  const Nbr n = make_nbr(g, i, j, k);
+  const int jc = j + 1;
+  double rt1, rt2;
+  if (comp == 1) {
+    if (j == 0) { a = 0.0; b = 1.0; c = 0.0; return; }
+    rt1 = pmBetaT * nut_at(nut, g, n, 0, -1) * hc.am2p[jc];
+    rt2 = pmBetaT * nut_at(nut, g, n, 0, 0) * hc.ap2p[jc];
+  } else {
+    const long long o = comp == 0 ? n.xm : n.zm;
+    const double visc = comp == 0 ? 0.25 * (nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, 0, -1) + nut_at(nut, g, n, o, -1))
+                                  : 0.25 * (nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, o, -1) + nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, 0, -1));
+    const double visd = comp == 0 ? 0.25 * (nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, 0, 1) + nut_at(nut, g, n, o, 1))
+                                  : 0.25 * (nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, o, 1) + nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, 0, 1));
+    rt1 = pmBetaT * visc * hc.am2cForCN[jc];
+    rt2 = pmBetaT * visd * hc.ap2cForCN[jc];
+  }
+  a = -rt1; b = rt1 + rt2 + 1.0; c = -rt2;
+}
+
 __global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, const double* __restrict__ nut,
                                                   const double* __restrict__ ux, const double* __restrict__ uy,
                                                   const double* __restrict__ uz, double* __restrict__ rx,
@@ -300,25 +324,7 @@ __global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, co
   const double pmBetaT = sc->pmBetaT;
   const int ny = g.ny;
   const long long nxl = g.nx;
-  auto coef = [&](int j, double& a, double& b, double& c) {
-    const Nbr n = make_nbr(g, i, j, k);
-    const int jc = j + 1;
-    double rt1, rt2;
-    if (comp == 1) {
-      if (j == 0) { a = 0.0; b = 1.0; c = 0.0; return; }
-      rt1 = pmBetaT * nut_at(nut, g, n, 0, -1) * hc.am2p[jc];
-      rt2 = pmBetaT * nut_at(nut, g, n, 0, 0) * hc.ap2p[jc];
-    } else {
-      const long long o = comp == 0 ? n.xm : n.zm;
-      const double visc = comp == 0 ? 0.25 * (nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, 0, -1) + nut_at(nut, g, n, o, -1))
-                                    : 0.25 * (nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, o, -1) + nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, 0, -1));
-      const double visd = comp == 0 ? 0.25 * (nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, 0, 1) + nut_at(nut, g, n, o, 1))
-                                    : 0.25 * (nut_at(nut, g, n, o, 0) + nut_at(nut, g, n, o, 1) + nut_at(nut, g, n, 0, 0) + nut_at(nut, g, n, 0, 1));
-      rt1 = pmBetaT * visc * hc.am2cForCN[jc];
-      rt2 = pmBetaT * visd * hc.ap2cForCN[jc];
-    }
-    a = -rt1; b = rt1 + rt2 + 1.0; c = -rt2;
-  };
+  auto coef = [&](int j, double& a, double& b, double& c) { uhat_les_coef(g, hc, nut, pmBetaT, comp, i, j, k, a, b, c); };
   const long long base = i + nxl * ny * k;
   double a, b, c;
   coef(0, a, b, c);
@@ -345,6 +351,86 @@ __global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, co
     fn = r[base + nxl * j] - arr * fn;
   }
   us[base] = u[base] + fn;
+}
+
+// The same solves for small grids, 32 columns per block of 8 warps: the
+// warps form every row's coefficients and right-hand side in parallel
+// (their loads independent of the recurrence) into shared memory, warp 0
+// runs the forward elimination and the back substitution there, and all
+// warps write u* = u + x and the forward-swept right-hand side (what the
+// one-thread-per-column kernel leaves in the RHS array).  Shared memory:
+// 4 x 32 x ny doubles.
+constexpr int kUhatTileCols = 32;
+constexpr size_t kUhatTileSmemMax = 200 * 1024;  // ny <= 200
+__global__ void __launch_bounds__(256) k_uhat_les_tile(Geo<double> g, HelmCoef hc, const double* __restrict__ nut,
+                                                       const double* __restrict__ ux, const double* __restrict__ uy,
+                                                       const double* __restrict__ uz, double* __restrict__ rx,
+                                                       double* __restrict__ ry, double* __restrict__ rz,
+                                                       double* __restrict__ uxs, double* __restrict__ uys,
+                                                       double* __restrict__ uzs, const DevScalars* __restrict__ sc) {
+  extern __shared__ double tl[];
+  if (sc->status) return;  // uniform over the block
+  const int ny = g.ny, ncol = g.nx * g.nz;
+  double* A = tl;                                // a(j), then arr(j)
+  double* B = A + kUhatTileCols * ny;            // b(j), then the solution x(j)
+  double* C = B + kUhatTileCols * ny;            // c(j)
+  double* F = C + kUhatTileCols * ny;            // right-hand side, then its forward-swept values
+  const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+  const int col = blockIdx.x * kUhatTileCols + lane;
+  const bool valid = col < ncol;
+  const int comp = blockIdx.y;
+  const int i = valid ? col % g.nx : 0, k = valid ? col / g.nx : 0;
+  const double* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
+  double* r = comp == 0 ? rx : (comp == 1 ? ry : rz);
+  double* us = comp == 0 ? uxs : (comp == 1 ? uys : uzs);
+  const double pmBetaT = sc->pmBetaT;
+  const long long nxl = g.nx;
+  const long long base = i + nxl * ny * k;
+  if (valid) {
+    for (int j = wy; j < ny; j += 8) {
+      double a, b, c;
+      uhat_les_coef(g, hc, nut, pmBetaT, comp, i, j, k, a, b, c);
+      const int e = j * kUhatTileCols + lane;
+      A[e] = a;
+      B[e] = b;
+      C[e] = c;
+      // row 1 of the uy system is the wall condition duy_ym = 0 (constant wall velocity)
+      F[e] = (comp == 1 && j == 0) ? 0.0 : r[base + nxl * j];
+    }
+  }
+  __syncthreads();
+  if (wy == 0 && valid) {
+    double vecm = B[lane];
+    double f = F[lane] / vecm;
+    F[lane] = f;
+    double cprev = C[lane];
+    for (int j = 1; j < ny; ++j) {
+      const int e = j * kUhatTileCols + lane;
+      const double a = A[e];
+      const double arr = cprev / vecm;
+      A[e] = arr;
+      vecm = B[e] - a * arr;
+      f = (F[e] - a * f) / vecm;
+      F[e] = f;
+      cprev = C[e];
+    }
+    double fn = f;
+    for (int j = ny - 2; j >= 0; --j) {
+      const int e1 = (j + 1) * kUhatTileCols + lane;
+      B[e1] = fn;
+      fn = F[j * kUhatTileCols + lane] - A[e1] * fn;
+    }
+    B[lane] = fn;
+  }
+  __syncthreads();
+  if (valid) {
+    for (int j = wy; j < ny; j += 8) {
+      const int e = j * kUhatTileCols + lane;
+      const long long q = base + nxl * j;
+      us[q] = u[q] + B[e];
+      r[q] = F[e];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -389,7 +475,7 @@ __device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metri
 // and scaled by u_tau^2, or the fallback where an input left the training
 // range.  When a wait on the tensor cores expires the kernel records it in
 // *mstatus and writes the fallback stresses.
-__global__ void __launch_bounds__(ch3d_mlp::TILE, 4)
+__global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
     k_sgs_mlp(Geo<double> g, Metrics<double> m, LesPar lp, MlpNorm nm, const double* __restrict__ ux,
               const double* __restrict__ uy, const double* __restrict__ uz, const float* __restrict__ P,
               double* __restrict__ tau, int* __restrict__ mstatus, const DevScalars* __restrict__ sc) {
@@ -583,7 +669,11 @@ cudaError_t launch_sgs_nut(ch3d_ctx* c) {
   memcpy(&nm, c->mlp_norm, sizeof(nm));
   static PerDevice attr;
   cudaError_t e = once_per_device(attr, c->device, [] {
-    return cudaFuncSetAttribute(k_sgs_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ch3d_mlp::FwdSmem::BYTES);
+    cudaError_t r =
+        cudaFuncSetAttribute(k_sgs_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ch3d_mlp::FwdSmem::BYTES);
+    if (r == cudaSuccess)  // all of the SM's on-chip memory as shared memory: six CTAs per SM
+      r = cudaFuncSetAttribute(k_sgs_mlp, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return r;
   });
   if (e != cudaSuccess) return e;
   k_sgs_mlp<<<(unsigned)((c->N + ch3d_mlp::TILE - 1) / ch3d_mlp::TILE), ch3d_mlp::TILE, ch3d_mlp::FwdSmem::BYTES,
@@ -635,6 +725,18 @@ cudaError_t launch_uhat_les(ch3d_ctx* c) {
   hc.ap2p = M + 7 * L; hc.ac2p = M + 8 * L; hc.am2p = M + 9 * L;
   hc.ap2cForCN = M + 14 * L; hc.am2cForCN = M + 15 * L;
   const int ncol = c->nx * c->nz;
+  // the tiled kernel while its shared memory (4 x 32 x ny doubles) fits
+  const size_t tsm = (size_t)4 * kUhatTileCols * c->ny * sizeof(double);
+  if (tsm <= kUhatTileSmemMax) {
+    static PerDevice attr;
+    cudaError_t e = once_per_device(attr, c->device, [] {
+      return cudaFuncSetAttribute(k_uhat_les_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUhatTileSmemMax);
+    });
+    if (e != cudaSuccess) return e;
+    k_uhat_les_tile<<<dim3((ncol + kUhatTileCols - 1) / kUhatTileCols, 3), 256, tsm, c->stream>>>(
+        make_geo<double>(c), hc, f[11], f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13], f[14], c->sc);
+    return cudaGetLastError();
+  }
   k_uhat_les<<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(make_geo<double>(c), hc, f[11], f[0], f[1], f[2], f[7],
                                                                  f[8], f[9], f[12], f[13], f[14], c->sc);
   return cudaGetLastError();

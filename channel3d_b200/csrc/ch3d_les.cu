@@ -446,6 +446,12 @@ struct MlpNorm {
   float in_mean[10], in_std[10], in_lo[10], in_hi[10];  // lo/hi: training range of the standardised inputs
   float out_mean[6], out_std[6];
 };
+// the same on the device: input means and reciprocal standard deviations in FP64
+struct MlpNormD {
+  double in_mean[10], in_rstd[10];
+  float in_lo[10], in_hi[10];
+  float out_mean[6], out_std[6];
+};
 
 // cell-centre gradients (the WALE stencils, m_LESModels.f90:98-111)
 __device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metrics<double>& m, const double* ux,
@@ -476,21 +482,22 @@ __device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metri
 // range.  When a wait on the tensor cores expires the kernel records it in
 // *mstatus and writes the fallback stresses.
 __global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
-    k_sgs_mlp(Geo<double> g, Metrics<double> m, LesPar lp, MlpNorm nm, const double* __restrict__ ux,
+    k_sgs_mlp(Geo<double> g, Metrics<double> m, LesPar lp, MlpNormD nm, const double* __restrict__ ux,
               const double* __restrict__ uy, const double* __restrict__ uz, const float* __restrict__ P,
               double* __restrict__ tau, int* __restrict__ mstatus, const DevScalars* __restrict__ sc) {
   using namespace ch3d_mlp;
   extern __shared__ __align__(1024) unsigned char smem[];
   if (sc->status) return;  // uniform: every thread reads the same word
-  const long long N = g.N;
-  const long long c = (long long)blockIdx.x * TILE + threadIdx.x;
+  const long long N = g.N;  // below 2^31 (checked by the launch)
+  const int c = blockIdx.x * TILE + threadIdx.x;
   const bool valid = c < N;
   float x[NIN];
   double fb[6] = {0, 0, 0, 0, 0, 0};
   bool out = true;
   const double ut = sc->utau > 1e-30 ? sc->utau : 1e-30;
   if (valid) {
-    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const unsigned cu = (unsigned)c, row = cu / (unsigned)g.nx;
+    const int i = (int)(cu - row * (unsigned)g.nx), k = (int)(row / (unsigned)g.ny), j = (int)(row - (unsigned)k * g.ny);
     const Nbr n = make_nbr(g, i, j, k);
     const int jc = j + 1;
     double G[9];
@@ -501,7 +508,7 @@ __global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
 #pragma unroll
     for (int q = 0; q < NIN; ++q) {
       const double v = q < 9 ? G[q] * gs : yplus;
-      const float xs = (float)((v - nm.in_mean[q]) / nm.in_std[q]);
+      const float xs = (float)((v - nm.in_mean[q]) * nm.in_rstd[q]);
       x[q] = xs;
       out = out || !(xs >= nm.in_lo[q] && xs <= nm.in_hi[q]);
     }
@@ -529,7 +536,7 @@ __global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
   const double u2 = sc->utau * sc->utau;
 #pragma unroll
   for (int q = 0; q < NOUT; ++q)
-    tau[q * N + c] = (out || !ok) ? fb[q] : ((double)y[q] * nm.out_std[q] + nm.out_mean[q]) * u2;
+    tau[(long long)q * N + c] = (out || !ok) ? fb[q] : ((double)y[q] * nm.out_std[q] + nm.out_mean[q]) * u2;
 }
 
 // f_i = -d tau_ij / dx_j at the staggered points of u_i.  Off-diagonal
@@ -664,9 +671,18 @@ cudaError_t launch_sgs_nut(ch3d_ctx* c) {
     k_sgs_nut<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, f[0], f[1], f[2], f[11], c->sc);
     return cudaGetLastError();
   }
-  MlpNorm nm;
+  MlpNorm nh;
   static_assert(sizeof(MlpNorm) == CH3D_SGS_NORM_FLOATS * sizeof(float), "norm layout");
-  memcpy(&nm, c->mlp_norm, sizeof(nm));
+  memcpy(&nh, c->mlp_norm, sizeof(nh));
+  MlpNormD nm;
+  for (int q = 0; q < 10; ++q) {
+    nm.in_mean[q] = nh.in_mean[q];
+    nm.in_rstd[q] = 1.0 / (double)nh.in_std[q];
+    nm.in_lo[q] = nh.in_lo[q];
+    nm.in_hi[q] = nh.in_hi[q];
+  }
+  for (int q = 0; q < 6; ++q) { nm.out_mean[q] = nh.out_mean[q]; nm.out_std[q] = nh.out_std[q]; }
+  if (c->N >= (1LL << 31)) return cudaErrorInvalidValue;  // 32-bit cell indices in k_sgs_mlp
   static PerDevice attr;
   cudaError_t e = once_per_device(attr, c->device, [] {
     cudaError_t r =

@@ -15,7 +15,7 @@ namespace ch3d_mlp {
 // forward: X [B x 10] FP32 -> Y [B x 6] FP32.  Training mode also stores the
 // pre-activations Z1..Z3 (FP32) and activations H1..H3 (BF16), [B x 64] each.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TILE, 4) k_mlp_fwd(const float* __restrict__ X, int B,
+__global__ void __launch_bounds__(TILE, 6) k_mlp_fwd(const float* __restrict__ X, int B,
                                                      const float* __restrict__ P, float* __restrict__ Y,
                                                      float* __restrict__ Z, __nv_bfloat16* __restrict__ H,
                                                      int* __restrict__ status) {
@@ -216,7 +216,9 @@ CH3D_MLP_API int ch3d_mlp_forward(const float* X, int batch, const float* params
   if (!X || !params || !Y || !status || batch <= 0) return 1;
   static ch3d::PerDevice attr;
   if (!setup_on_current_device(attr, [] {
-        return cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD);
+        cudaError_t r = cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD);
+        if (r == cudaSuccess) r = cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        return r;
       }))
     return 2;
   k_mlp_fwd<<<(batch + TILE - 1) / TILE, TILE, SMEM_FWD, (cudaStream_t)stream>>>(X, batch, params, Y, nullptr, nullptr,

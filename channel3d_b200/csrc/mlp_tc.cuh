@@ -158,13 +158,26 @@ __device__ __forceinline__ void gemm_issue(uint32_t d_tmem, const unsigned char*
 
 // GELU in its tanh form (Hendrycks & Gimpel 2016): 0.5 x (1 + tanh u),
 // u = sqrt(2/pi) (x + 0.044715 x^3).  With r = 1 / (1 + exp(2u)),
-// 1 + tanh u = 2 (1 - r), so gelu = x - x r; the fast exponential and
-// division intrinsics give r to about 1e-7 (r -> 0 as exp(2u) overflows to
+// 1 + tanh u = 2 (1 - r), so gelu = x - x r.  exp(2u) = 2^(2u log2 e) with
+// the factor log2 e folded into the cubic's coefficients, evaluated with the
+// hardware's approximate base-2 exponential and reciprocal (relative errors
+// near 2^-22): r to about 1e-7 (r -> 0 as the exponential overflows to
 // infinity, r -> 1 as it underflows).  Derivative:
 // (1 - r) + 2 x r (1 - r) u'(x), u' = sqrt(2/pi) (1 + 3 * 0.044715 x^2).
+__device__ __forceinline__ float ex2_approx(float a) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float a) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+  return y;
+}
 __device__ __forceinline__ float gelu_r(float x) {
-  const float two_u = x * (1.5957691216057308f + 0.071354816272600f * x * x);  // 2 sqrt(2/pi) (x + 0.044715 x^3)
-  return __fdividef(1.0f, 1.0f + __expf(two_u));
+  // 2u log2 e = x (2 sqrt(2/pi) log2 e + 2 sqrt(2/pi) 0.044715 log2 e x^2)
+  const float t = x * fmaf(0.1029432395800235f, x * x, 2.302208198144325f);
+  return rcp_approx(1.0f + ex2_approx(t));
 }
 __device__ __forceinline__ float gelu(float x) { return x - x * gelu_r(x); }
 __device__ __forceinline__ float gelu_d(float x) {
@@ -219,11 +232,13 @@ struct Smem {
   int err;
 };
 
-// shared memory of the forward pass: header, X tile, activation tile, the
-// four weight operands and the biases
+// shared memory of the forward pass: header, activation tile (its first
+// 4 KB hold the X tile until the first layer's MMA has read it: the
+// activations are written only after that MMA completed), the four weight
+// operands and the biases; 37.8 KB, so that six CTAs fit an SM
 struct FwdSmem {
-  static constexpr size_t XA = 1024;
-  static constexpr size_t HA = XA + TILE * NINP * 2;
+  static constexpr size_t XA = 128;
+  static constexpr size_t HA = XA;
   static constexpr size_t W1 = HA + TILE * NH * 2;
   static constexpr size_t W2 = W1 + NH * NINP * 2;
   static constexpr size_t W3 = W2 + NH * NH * 2;
@@ -298,9 +313,12 @@ __device__ __forceinline__ bool fwd_layers(unsigned char* smem, float* y, float*
       for (int c0 = 0; c0 < NH; c0 += 16) {
         float acc[16], h[16];
         tmem_ld<16>(lane_addr + c0, acc);
+        float bq[16];
+#pragma unroll
+        for (int q = 0; q < 16; q += 4) *reinterpret_cast<float4*>(bq + q) = *reinterpret_cast<const float4*>(bs + l * NH + c0 + q);
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-          const float z = acc[q] + bs[l * NH + c0 + q];
+          const float z = acc[q] + bq[q];
           h[q] = gelu(z);
           if (Z != nullptr && valid) {
             Z[(long long)l * B * NH + pt * NH + c0 + q] = z;

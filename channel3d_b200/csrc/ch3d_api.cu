@@ -597,6 +597,14 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
   if (e != cudaSuccess) { int r = fail(CH3D_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); delete c; return r; }
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
     return cleanup(fail(CH3D_ERR_CUDA, "event create failed"));
+  if (c->fp32) {
+    int lo = 0, hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+      return cleanup(fail(CH3D_ERR_CUDA, "side stream create failed"));
+  }
   rc = c->fp32 ? alloc_fields<float>(c) : alloc_fields<double>(c);
   if (rc) return cleanup(rc);
   {
@@ -697,6 +705,9 @@ int ch3d_destroy(ch3d_ctx* c) {
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return CH3D_OK;

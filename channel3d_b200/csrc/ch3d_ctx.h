@@ -17,6 +17,10 @@ struct ch3d_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // mixed path: a high-priority side stream for the FP64 low-mode Poisson y solves,
+  // forked from and joined to `stream` around the FP32 solves
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   double last_ms = 0;
 
   // Runge-Kutta constants (src/CFD_2nd/m_Parameters.f90:291-306)

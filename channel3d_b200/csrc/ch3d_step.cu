@@ -795,11 +795,13 @@ __device__ __forceinline__ void thomas_column(int ny, bool pin, const R* __restr
   }
 }
 
-// FP64 path: every column in FP64 (sel 0).
-template <class T, class R>
+// All columns in the precision of the field (FP64 path), or in the mixed
+// path the FP32 columns: the low modes kx < KX, |kz| <= KL are skipped
+// (KX = 0: none) and solved by k_ythomas_low.
+template <class T, class R, int YB>
 __global__ void __launch_bounds__(128) k_ythomas(Geo<T> g, Metrics<double> m, const R* __restrict__ RMf,
                                                  const R* __restrict__ CPf, typename CplxOf<T>::type* __restrict__ spec,
-                                                 const DevScalars* __restrict__ sc) {
+                                                 int KL, int KX, const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
   if (sc->status) return;
   const int nxh = g.nxh, ny = g.ny, nz = g.nz;
@@ -807,51 +809,45 @@ __global__ void __launch_bounds__(128) k_ythomas(Geo<T> g, Metrics<double> m, co
   if (t >= (long long)nxh * nz) return;
   const int kx = (int)(t % nxh), kz = (int)(t / nxh);
   const int kzh = kz <= nz - kz ? kz : nz - kz;
+  if (kx < KX && kzh <= KL) return;
   const size_t st = (size_t)nxh;
   CT* col = spec + kx + st * ny * kz;
   const R* rm = RMf + (size_t)kzh * ny * st + kx;
   const R* cp = CPf + (size_t)kzh * ny * st + kx;
   auto load = [&](int j) { return col[st * j]; };
   auto store = [&](int j, R x, R y) { col[st * j] = mk((T)x, (T)y); };
-  thomas_column<R, CT, 16>(ny, kx == 0 && kz == 0, rm, cp, st, m.am2Pr, load, store, store, load);
+  thomas_column<R, CT, YB>(ny, kx == 0 && kz == 0, rm, cp, st, m.am2Pr, load, store, store, load);
 }
 
-// Mixed path: FP32 sweeps with FP32 factors, except the low modes kx < KX,
-// |kz| <= KL, solved in FP64 with FP64 factors and the FP64 scratch.
+// Mixed path: the low modes kx < KX, |kz| <= KL (column zi = kz for kz <= KL,
+// KL + nz - kz above) in FP64 with FP64 factors, their forward sweep kept in
+// the FP64 scratch [j][low column].
 template <class T>
-__global__ void __launch_bounds__(128) k_ythomas_mixed(Geo<T> g, Metrics<double> m, const float* __restrict__ RM32,
-                                                       const float* __restrict__ CP32,
-                                                       const double* __restrict__ RM64,
-                                                       const double* __restrict__ CP64,
-                                                       typename CplxOf<T>::type* __restrict__ spec,
-                                                       double2* __restrict__ scr, int KL, int KX,
-                                                       const DevScalars* __restrict__ sc) {
+__global__ void __launch_bounds__(128) k_ythomas_low(Geo<T> g, Metrics<double> m, const double* __restrict__ RM64,
+                                                     const double* __restrict__ CP64,
+                                                     typename CplxOf<T>::type* __restrict__ spec,
+                                                     double2* __restrict__ scr, int KL, int KX,
+                                                     const DevScalars* __restrict__ sc) {
   typedef typename CplxOf<T>::type CT;
   if (sc->status) return;
   const int nxh = g.nxh, ny = g.ny, nz = g.nz;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)nxh * nz) return;
-  const int kx = (int)(t % nxh), kz = (int)(t / nxh);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (2 * KL + 1) * KX) return;
+  const int zi = q / KX, kx = q - zi * KX;
+  const int kz = zi <= KL ? zi : nz - (zi - KL);
+  if (kx >= nxh || (zi > KL && kz <= KL)) return;
   const int kzh = kz <= nz - kz ? kz : nz - kz;
   const size_t st = (size_t)nxh;
   CT* col = spec + kx + st * ny * kz;
-  const bool pin = (kx == 0 && kz == 0);
-  auto load = [&](int j) { return col[st * j]; };
-  if (kx < KX && kzh <= KL) {
-    const int zi = kz <= KL ? kz : KL + (nz - kz);  // 0..2KL
-    const size_t nlow = (size_t)(2 * KL + 1) * KX;
-    double2* w = scr + (size_t)zi * KX + kx;         // [j][low column]
-    auto store = [&](int j, double x, double y) { col[st * j] = mk((T)x, (T)y); };
-    auto store_d = [&](int j, double x, double y) { w[nlow * j] = make_double2(x, y); };
-    auto load_d = [&](int j) { return w[nlow * j]; };
-    thomas_column<double, double2, 8>(ny, pin, RM64 + (size_t)kzh * ny * KX + kx, CP64 + (size_t)kzh * ny * KX + kx,
-                                   (size_t)KX, m.am2Pr, [&](int j) { const CT v = load(j); return make_double2(v.x, v.y); },
-                                   store, store_d, load_d);
-    return;
-  }
-  auto store = [&](int j, float x, float y) { col[st * j] = mk((T)x, (T)y); };
-  thomas_column<float, CT, 8>(ny, pin, RM32 + (size_t)kzh * ny * st + kx, CP32 + (size_t)kzh * ny * st + kx, st, m.am2Pr,
-                           load, store, store, load);
+  const size_t nlow = (size_t)(2 * KL + 1) * KX;
+  double2* w = scr + (size_t)zi * KX + kx;  // [j][low column]
+  auto load = [&](int j) { const CT v = col[st * j]; return make_double2(v.x, v.y); };
+  auto store = [&](int j, double x, double y) { col[st * j] = mk((T)x, (T)y); };
+  auto store_d = [&](int j, double x, double y) { w[nlow * j] = make_double2(x, y); };
+  auto load_d = [&](int j) { return w[nlow * j]; };
+  thomas_column<double, double2, 16>(ny, kx == 0 && kz == 0, RM64 + (size_t)kzh * ny * KX + kx,
+                                     CP64 + (size_t)kzh * ny * KX + kx, (size_t)KX, m.am2Pr, load, store, store_d,
+                                     load_d);
 }
 
 // ---------------------------------------------------------------------------
@@ -1254,15 +1250,25 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
   }
   const unsigned gy = (unsigned)(((long long)c->nxh * c->nz + 127) / 128);
   if (!c->fp32) {
-    k_ythomas<T, double><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
-                                                    (const double*)c->yCP, (CT*)c->spec, c->sc);
+    k_ythomas<T, double, 16><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
+                                                        (const double*)c->yCP, (CT*)c->spec, 0, 0, c->sc);
   } else {
-    // mixed: FP32 systems and factors, except the low modes near kx = kz = 0 in FP64
-    k_ythomas_mixed<T><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const float*)c->yRM,
-                                                  (const float*)c->yCP, c->yRM64, c->yCP64, (CT*)c->spec,
-                                                  (double2*)c->ylow, c->KL, c->TSy, c->sc);
+    // mixed: FP32 systems and factors; the low modes near kx = kz = 0 in FP64 on the
+    // high-priority side stream, overlapping the FP32 sweeps (a fork and a join in
+    // the captured step graph)
+    const int nlow = (2 * c->KL + 1) * c->TSy;
+    if ((e = cudaEventRecord(c->ev_fork, c->stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(c->side, c->ev_fork, 0)) != cudaSuccess) return e;
+    k_ythomas_low<T><<<(nlow + 127) / 128, 128, 0, c->side>>>(make_geo<T>(c), c->m64full, c->yRM64, c->yCP64,
+                                                              (CT*)c->spec, (double2*)c->ylow, c->KL, c->TSy, c->sc);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(c->ev_join, c->side)) != cudaSuccess) return e;
+    k_ythomas<T, float, 16><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const float*)c->yRM,
+                                                       (const float*)c->yCP, (CT*)c->spec, c->KL, c->TSy, c->sc);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
   }
-  e = cudaGetLastError();
+  e = e != cudaSuccess ? e : cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (launch_zfft_r(c, 1, &e)) return e;
   k_zfft<T><<<gz, nthrz, smemz, c->stream>>>(make_geo<T>(c), (CT*)c->spec, c->planz, (const CT*)c->twz, TKX, 1, c->sc);

@@ -353,16 +353,17 @@ __global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, co
   us[base] = u[base] + fn;
 }
 
-// The same solves for small grids, 32 columns per block of 8 warps: the
-// warps form every row's coefficients and right-hand side in parallel
-// (their loads independent of the recurrence) into shared memory, warp 0
-// runs the forward elimination and the back substitution there, and all
-// warps write u* = u + x and the forward-swept right-hand side (what the
-// one-thread-per-column kernel leaves in the RHS array).  Shared memory:
-// 4 x 32 x ny doubles.
-constexpr int kUhatTileCols = 32;
-constexpr size_t kUhatTileSmemMax = 200 * 1024;  // ny <= 200
-__global__ void __launch_bounds__(256) k_uhat_les_tile(Geo<double> g, HelmCoef hc, const double* __restrict__ nut,
+// The same solves for small grids, 16 columns per block of 128 threads (8
+// row groups of 16): the threads form every row's coefficients and
+// right-hand side in parallel (their loads independent of the recurrence)
+// into shared memory, the first 16 threads run the forward elimination and
+// the back substitution there, and all threads write u* = u + x and the
+// forward-swept right-hand side (what the one-thread-per-column kernel
+// leaves in the RHS array).  Shared memory: 4 x 16 x ny doubles; at 48^3 the
+// 432 blocks are one wave on 148 SMs (32-column blocks: 1.5 waves, 21 us).
+constexpr int kUhatTileCols = 16;
+constexpr size_t kUhatTileSmemMax = 100 * 1024;  // ny <= 200
+__global__ void __launch_bounds__(128) k_uhat_les_tile(Geo<double> g, HelmCoef hc, const double* __restrict__ nut,
                                                        const double* __restrict__ ux, const double* __restrict__ uy,
                                                        const double* __restrict__ uz, double* __restrict__ rx,
                                                        double* __restrict__ ry, double* __restrict__ rz,
@@ -375,7 +376,7 @@ __global__ void __launch_bounds__(256) k_uhat_les_tile(Geo<double> g, HelmCoef h
   double* B = A + kUhatTileCols * ny;            // b(j), then the solution x(j)
   double* C = B + kUhatTileCols * ny;            // c(j)
   double* F = C + kUhatTileCols * ny;            // right-hand side, then its forward-swept values
-  const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+  const int lane = threadIdx.x % kUhatTileCols, wy = threadIdx.x / kUhatTileCols;  // wy: row group 0..7
   const int col = blockIdx.x * kUhatTileCols + lane;
   const bool valid = col < ncol;
   const int comp = blockIdx.y;
@@ -741,7 +742,7 @@ cudaError_t launch_uhat_les(ch3d_ctx* c) {
   hc.ap2p = M + 7 * L; hc.ac2p = M + 8 * L; hc.am2p = M + 9 * L;
   hc.ap2cForCN = M + 14 * L; hc.am2cForCN = M + 15 * L;
   const int ncol = c->nx * c->nz;
-  // the tiled kernel while its shared memory (4 x 32 x ny doubles) fits
+  // the tiled kernel while its shared memory (4 x 16 x ny doubles) fits
   const size_t tsm = (size_t)4 * kUhatTileCols * c->ny * sizeof(double);
   if (tsm <= kUhatTileSmemMax) {
     static PerDevice attr;
@@ -749,7 +750,7 @@ cudaError_t launch_uhat_les(ch3d_ctx* c) {
       return cudaFuncSetAttribute(k_uhat_les_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUhatTileSmemMax);
     });
     if (e != cudaSuccess) return e;
-    k_uhat_les_tile<<<dim3((ncol + kUhatTileCols - 1) / kUhatTileCols, 3), 256, tsm, c->stream>>>(
+    k_uhat_les_tile<<<dim3((ncol + kUhatTileCols - 1) / kUhatTileCols, 3), 128, tsm, c->stream>>>(
         make_geo<double>(c), hc, f[11], f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13], f[14], c->sc);
     return cudaGetLastError();
   }

@@ -624,7 +624,11 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
   else c->m32 = Metrics<float>();
   if (!c->fp32) c->m64 = metrics_ptrs<double>((const double*)c->met, c->ny);
   c->TSy = 8;  // kx extent of the FP64 low modes of the mixed path
-  c->Pv = 32;
+  // chunks of the partitioned Helmholtz solves: the power of two nearest below
+  // sqrt(ny) (2..32), balancing the chunk sweeps (2 ny / P rows) against the
+  // serial interface solve (P - 1 steps)
+  c->Pv = 2;
+  while (c->Pv < 32 && 4 * c->Pv * c->Pv <= c->ny) c->Pv <<= 1;
   while (c->Pv > 1 && c->ny < 2 * c->Pv) c->Pv >>= 1;
   {
     size_t nf = (size_t)2 * (5 * c->ny + 6 * (c->Pv > 1 ? c->Pv - 1 : 1));

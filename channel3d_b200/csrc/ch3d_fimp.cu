@@ -43,62 +43,95 @@ __global__ void k_ptri_factors(int nx, int nz, double rdx2, double rdz2, double*
   abc[3] = c * v2[1] + a * v2[n - 1] + b;
 }
 
-// One periodic line f(1..n) at stride s (in place).
-template <class T>
-__device__ __forceinline__ void ptri_line(const double* __restrict__ F, int n, T* f, int s) {
+// One periodic line f(1..n) at stride s (in place), with the factor block F
+// (ppj | vecn1 | vecn2 | a b c den) in shared memory.  The two recurrences
+// load YB values ahead of their dependent chain (the values do not depend on
+// it), the closing pass is element-wise; the arithmetic is that of
+// InversePTriFixedCoe, term for term.
+template <class T, int YB>
+__device__ __forceinline__ void ptri_line(const double* __restrict__ F, int n, T* f, long long s) {
   const double *ppj = F, *v1 = F + (n + 1), *v2 = F + 2 * (n + 1), *abc = F + 3 * (n + 1);
   const T a = (T)abc[0], b = (T)abc[1], c = (T)abc[2], den = (T)abc[3];
-  // forward elimination, rows 1..n-1
+  // forward elimination, rows 1..n-1 (0-based index q = row - 1)
   T prev = f[0] / b;
   f[0] = prev;
-  for (int j = 2; j <= n - 1; ++j) {
-    prev = (f[(j - 1) * s] - a * prev) * (T)ppj[j];
-    f[(j - 1) * s] = prev;
+  for (int q0 = 1; q0 < n - 1; q0 += YB) {
+    T v[YB], w[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u)
+      if (q0 + u < n - 1) { v[u] = f[(q0 + u) * s]; w[u] = (T)ppj[q0 + u + 1]; }
+#pragma unroll
+    for (int u = 0; u < YB; ++u)
+      if (q0 + u < n - 1) { prev = (v[u] - a * prev) * w[u]; f[(q0 + u) * s] = prev; }
   }
   // backward pass: arrmn(j) = f(j) + vecn1(j) arrmn(j+1), stored in place
   T arr = (T)0;
-  for (int j = n - 1; j >= 1; --j) {
-    arr = f[(j - 1) * s] + (T)v1[j] * arr;
-    f[(j - 1) * s] = arr;
+  for (int q0 = n - 2; q0 >= 0; q0 -= YB) {
+    T v[YB], w[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u)
+      if (q0 - u >= 0) { v[u] = f[(q0 - u) * s]; w[u] = (T)v1[q0 - u + 1]; }
+#pragma unroll
+    for (int u = 0; u < YB; ++u)
+      if (q0 - u >= 0) { arr = v[u] + w[u] * arr; f[(q0 - u) * s] = arr; }
   }
   const T fn = (f[(n - 1) * s] - c * f[0] - a * f[(n - 2) * s]) / den;
   f[(n - 1) * s] = fn;
-  for (int j = n - 1; j >= 1; --j) f[(j - 1) * s] = fn * (T)v2[j] + f[(j - 1) * s];
+  for (int q0 = 0; q0 < n - 1; q0 += YB) {
+#pragma unroll
+    for (int u = 0; u < YB; ++u)
+      if (q0 + u < n - 1) f[(q0 + u) * s] = fn * (T)v2[q0 + u + 1] + f[(q0 + u) * s];
+  }
 }
 
-// x sweep: LB consecutive x lines (contiguous in memory) per block staged in
-// shared memory with a padded stride; one thread per line.  blockIdx.y = component.
+// copy the factor block of one direction into shared memory
+__device__ __forceinline__ void ptri_stage_factors(double* dst, const double* __restrict__ src, int n) {
+  for (int t = threadIdx.x; t < ptri_stride(n); t += blockDim.x) dst[t] = src[t];
+}
+
+// x sweep: LB consecutive x lines (contiguous in memory) per block, staged
+// in shared memory with a padded stride (after the factor block) by all 128
+// threads; one thread per line solves.  blockIdx.y = component.
 template <class T>
 __global__ void __launch_bounds__(128) k_ptri_x(int nx, long long nlines, int LB, const double* __restrict__ pf,
-                                                T* __restrict__ r0, T* __restrict__ r1, T* __restrict__ r2,
-                                                const DevScalars* __restrict__ sc) {
+                                               T* __restrict__ r0, T* __restrict__ r1, T* __restrict__ r2,
+                                               const DevScalars* __restrict__ sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (sc->status) return;
-  T* S = (T*)smem_raw;
+  double* Fs = (double*)smem_raw;
+  T* S = (T*)(Fs + ptri_stride(nx));
   const int ld = nx + 1;
   T* r = blockIdx.y == 0 ? r0 : (blockIdx.y == 1 ? r1 : r2);
   const long long l0 = (long long)blockIdx.x * LB;
   const int nl = (int)min((long long)LB, nlines - l0);
   T* g = r + l0 * nx;
+  ptri_stage_factors(Fs, pf, nx);
+#pragma unroll 8
   for (int t = threadIdx.x; t < nl * nx; t += blockDim.x) S[(t / nx) * ld + (t % nx)] = g[t];
   __syncthreads();
-  for (int l = threadIdx.x; l < nl; l += blockDim.x) ptri_line<T>(pf, nx, S + l * ld, 1);
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) ptri_line<T, 8>(Fs, nx, S + l * ld, 1);
   __syncthreads();
+#pragma unroll 8
   for (int t = threadIdx.x; t < nl * nx; t += blockDim.x) g[t] = S[(t / nx) * ld + (t % nx)];
 }
 
 // z sweep: one thread per (i, j) column, in place in global memory (a warp
-// covers 32 consecutive i, so every access is coalesced).  blockIdx.z = component.
+// covers 32 consecutive i, so every access is coalesced); 16 rows of loads in
+// flight ahead of each recurrence.  blockIdx.z = component.
 template <class T>
 __global__ void __launch_bounds__(128) k_ptri_z(int nx, int ny, int nz, const double* __restrict__ pf,
                                                 T* __restrict__ r0, T* __restrict__ r1, T* __restrict__ r2,
                                                 const DevScalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   if (sc->status) return;
+  double* Fs = (double*)smem_raw;
+  ptri_stage_factors(Fs, pf + ptri_stride(nx), nz);
+  __syncthreads();
   const int i = blockIdx.x * 32 + (threadIdx.x & 31);
   const int j = blockIdx.y * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (i >= nx || j >= ny) return;
   T* r = blockIdx.z == 0 ? r0 : (blockIdx.z == 1 ? r1 : r2);
-  ptri_line<T>(pf + ptri_stride(nx), nz, r + i + (long long)nx * j, nx * ny);
+  ptri_line<T, 16>(Fs, nz, r + i + (long long)nx * j, (long long)nx * ny);
 }
 
 template <class T> static cudaError_t ptri_t(ch3d_ctx* c) {
@@ -106,19 +139,23 @@ template <class T> static cudaError_t ptri_t(ch3d_ctx* c) {
   k_ptri_factors<<<2, 32, 0, c->stream>>>(c->nx, c->nz, c->rdx2, c->rdz2, c->pfac, c->sc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  // x: one thread per line, at most 64 KB of lines per block
   int LB = (int)((64 * 1024) / ((size_t)(c->nx + 1) * sizeof(T)));
   if (LB > 128) LB = 128;
   if (LB < 1) LB = 1;
   const long long nlines = (long long)c->ny * c->nz;
-  const size_t smem = (size_t)LB * (c->nx + 1) * sizeof(T);
+  const size_t smem = (size_t)ptri_stride(c->nx) * sizeof(double) + (size_t)LB * (c->nx + 1) * sizeof(T);
   static PerDevice attr;  // per precision (template instance)
   if ((e = smem_limit_once(attr, c->device, k_ptri_x<T>, 200 * 1024)) != cudaSuccess) return e;
   k_ptri_x<T><<<dim3((unsigned)((nlines + LB - 1) / LB), 3), 128, smem, c->stream>>>(c->nx, nlines, LB, c->pfac, f[7],
                                                                                       f[8], f[9], c->sc);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_ptri_z<T><<<dim3((c->nx + 31) / 32, (c->ny + 3) / 4, 3), 128, 0, c->stream>>>(c->nx, c->ny, c->nz, c->pfac, f[7],
-                                                                                 f[8], f[9], c->sc);
+  const size_t smz = (size_t)ptri_stride(c->nz) * sizeof(double);
+  static PerDevice attrz;  // per precision (template instance)
+  if ((e = smem_limit_once(attrz, c->device, k_ptri_z<T>, 200 * 1024)) != cudaSuccess) return e;
+  k_ptri_z<T><<<dim3((c->nx + 31) / 32, (c->ny + 3) / 4, 3), 128, smz, c->stream>>>(c->nx, c->ny, c->nz, c->pfac,
+                                                                                   f[7], f[8], f[9], c->sc);
   return cudaGetLastError();
 }
 cudaError_t launch_ptri_xz(ch3d_ctx* c) { return c->fp32 ? ptri_t<float>(c) : ptri_t<double>(c); }

@@ -322,7 +322,9 @@ __global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const 
 }
 
 // clcRhsX/Y/Z_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:6-177), one thread per
-// cell, RhsX with the mean pressure gradient (:57-66) included.
+// cell and component (blockIdx.z = component * nz + k: a thread holds one
+// component's stencil, so more threads fit an SM than with all three),
+// RhsX with the mean pressure gradient (:57-66) included.
 template <class T>
 __global__ void __launch_bounds__(256) k_rhs_fimp(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
                                                   const T* __restrict__ uy, const T* __restrict__ uz,
@@ -332,13 +334,16 @@ __global__ void __launch_bounds__(256) k_rhs_fimp(Geo<T> g, Metrics<T> m, const 
   if (sc->status) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+  const int comp = blockIdx.z / g.nz, k = blockIdx.z - comp * g.nz;
   if (i >= g.nx || j >= g.ny) return;
   const T pmGamma = (T)sc->pmGamma, pmTheta = (T)sc->pmTheta, pmAlpha = (T)sc->pmAlpha, pmBeta = (T)sc->pmBeta;
   const long long idx = i + (long long)g.nx * (j + (long long)g.ny * k);
-  rx[idx] = rhs_comp<T, 0>(g, m, ux, uy, uz, pr, hx, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta) + (T)sc->dpmdxns;
-  ry[idx] = rhs_comp<T, 1>(g, m, ux, uy, uz, pr, hy, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
-  rz[idx] = rhs_comp<T, 2>(g, m, ux, uy, uz, pr, hz, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
+  if (comp == 0)
+    rx[idx] = rhs_comp<T, 0>(g, m, ux, uy, uz, pr, hx, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta) + (T)sc->dpmdxns;
+  else if (comp == 1)
+    ry[idx] = rhs_comp<T, 1>(g, m, ux, uy, uz, pr, hy, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
+  else
+    rz[idx] = rhs_comp<T, 2>(g, m, ux, uy, uz, pr, hz, i, j, k, pmGamma, pmTheta, pmAlpha, pmBeta);
 }
 
 // Precomputes the chunk factors, spikes and interface block-Thomas factors of
@@ -411,14 +416,21 @@ __global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, const double* __res
   // the 4th-order and FIMP RhsX already carry the forcing (k_rhs4, k_rhs_fimp)
   const T add = (comp == 0 && g.order != 4 && g.implicit != 2) ? (T)sc->dpmdxns : (T)0;
   const int tid = threadIdx.x;
+  // the block's right-hand sides, coalesced rows of TI values, before the sweeps
+  for (int t = tid; t < ny * TI; t += blockDim.x) {
+    const int j = t / TI, ii = t % TI, i = i0 + ii;
+    T f = (T)0;
+    if (i < nx) f = rhs[i + (long long)nx * (j + (long long)ny * k)] + add;
+    if (comp == 1 && j == 0) f = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
+    F[t] = f;
+  }
+  __syncthreads();
   for (int t = tid; t < TI * P; t += blockDim.x) {
-    const int ii = t % TI, p = t / TI, i = i0 + ii;
+    const int ii = t % TI, p = t / TI;
     const int s = chunk_lo(p, ny, P), e = chunk_hi(p, ny, P);
     T d = (T)0;
     for (int j = s; j <= e; ++j) {
-      T f = (T)0;
-      if (i < nx) f = rhs[i + (long long)nx * (j + (long long)ny * k)] + add;
-      if (comp == 1 && j == 0) f = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
+      const T f = F[j * TI + ii];
       d = (j == s) ? f * (T)RM[j] : (f - (T)AA[j] * d) * (T)RM[j];
       F[j * TI + ii] = d;
     }
@@ -1166,7 +1178,8 @@ template <class T> static cudaError_t rhs_t(ch3d_ctx* c) {
 cudaError_t launch_rhs(ch3d_ctx* c) { return c->fp32 ? rhs_t<float>(c) : rhs_t<double>(c); }
 template <class T> static cudaError_t rhs_fimp_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
-  k_rhs_fimp<T><<<cell_grid(c), cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], f[3],
+  const dim3 grid((c->nx + 31) / 32, (c->ny + 7) / 8, 3 * c->nz);  // z: component * nz + k
+  k_rhs_fimp<T><<<grid, cell_block(), 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], f[1], f[2], f[3],
                                                               f[4], f[5], f[6], f[7], f[8], f[9], c->sc);
   return cudaGetLastError();
 }

@@ -105,14 +105,17 @@ __global__ void __launch_bounds__(128) k_ptri_x(int nx, long long nlines, int LB
   const long long l0 = (long long)blockIdx.x * LB;
   const int nl = (int)min((long long)LB, nlines - l0);
   T* g = r + l0 * nx;
+  // the lines by asynchronous copies, all in flight at once
+  for (int l = 0; l < nl; ++l)
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) cp_async_el(S + l * ld + x, g + (long long)l * nx + x);
+  cp_async_commit();
   ptri_stage_factors(Fs, pf, nx);
-#pragma unroll 8
-  for (int t = threadIdx.x; t < nl * nx; t += blockDim.x) S[(t / nx) * ld + (t % nx)] = g[t];
+  cp_async_wait<0>();
   __syncthreads();
   for (int l = threadIdx.x; l < nl; l += blockDim.x) ptri_line<T, 8>(Fs, nx, S + l * ld, 1);
   __syncthreads();
-#pragma unroll 8
-  for (int t = threadIdx.x; t < nl * nx; t += blockDim.x) g[t] = S[(t / nx) * ld + (t % nx)];
+  for (int l = 0; l < nl; ++l)
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) g[(long long)l * nx + x] = S[l * ld + x];
 }
 
 // z sweep: one thread per (i, j) column, in place in global memory (a warp

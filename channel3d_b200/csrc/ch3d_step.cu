@@ -416,11 +416,18 @@ __global__ void __launch_bounds__(256) k_uhat_pimp(Geo<T> g, const double* __res
   // the 4th-order and FIMP RhsX already carry the forcing (k_rhs4, k_rhs_fimp)
   const T add = (comp == 0 && g.order != 4 && g.implicit != 2) ? (T)sc->dpmdxns : (T)0;
   const int tid = threadIdx.x;
-  // the block's right-hand sides, coalesced rows of TI values, before the sweeps
+  // the block's right-hand sides (coalesced rows of TI values) by asynchronous
+  // copies, all in flight at once
+  for (int t = tid; t < ny * TI; t += blockDim.x) {
+    const int j = t / TI, ii = t % TI, i = i0 + ii;
+    if (i < nx) cp_async_el(F + t, rhs + i + (long long)nx * (j + (long long)ny * k));
+  }
+  cp_async_commit();
+  cp_async_wait<0>();  // this thread's copies (the slots it reads next)
   for (int t = tid; t < ny * TI; t += blockDim.x) {
     const int j = t / TI, ii = t % TI, i = i0 + ii;
     T f = (T)0;
-    if (i < nx) f = rhs[i + (long long)nx * (j + (long long)ny * k)] + add;
+    if (i < nx) f = F[t] + add;
     if (comp == 1 && j == 0) f = (T)0;  // duy_ym: uy_ym is constant (Update_uy_ym_CH)
     F[t] = f;
   }

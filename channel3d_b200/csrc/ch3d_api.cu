@@ -668,6 +668,7 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     c->npart_m = march_npart(c);
     if (c->npart_m > c->npart) c->npart = c->npart_m;
     if (diag_npart(c) > c->npart) c->npart = diag_npart(c);
+    if (visc4_npart(c) > c->npart) c->npart = visc4_npart(c);
     if (cudaMalloc(&c->part, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->part2, (size_t)c->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->red1, CH3D_NRED * sizeof(double)) != cudaSuccess ||

@@ -1159,7 +1159,10 @@ __global__ void __launch_bounds__(256) k_reduce_partials(const double* __restric
 }
 
 cudaError_t launch_substep_setup(ch3d_ctx* c, int ns) {
-  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part, c->march ? c->npart_m : c->npart, c->red1);
+  // the partials of the bulk sums (march projection or k_bulk_partial), or of the
+  // 4th-order viscous sum (k_visc4_partial)
+  const int np = c->cfg.order == 4 ? visc4_npart(c) : (c->march ? c->npart_m : c->npart);
+  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(c->part, np, c->red1);
   const double norm_bulk = 1.0 / ((double)c->nx * (double)c->nz) / (c->cfg.ybulk2 - c->cfg.ybulk1);
   k_substep_setup<<<1, 256, 0, c->stream>>>(c->sc, c->red1, CH3D_NRED, ns, c->gam[ns - 1], c->the[ns - 1],
                                             c->alp[ns - 1], c->cfg.xnu, c->cfg.IsUxConst, c->cfg.ubulk, norm_bulk,

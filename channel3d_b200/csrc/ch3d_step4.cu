@@ -152,33 +152,49 @@ __global__ void __launch_bounds__(256) k_rhs4(Geo<T> g, Metrics<T> m, Interp4 ih
 // Block partial sums of (d11q1 + d33q1 + d22q1) * dyp over ux: the mean
 // viscous stress of the constant-flux forcing (src/CFD_4th/m_TScheme.f90:255-262,364-377).
 template <class T>
-__global__ void __launch_bounds__(256) k_visc4_partial(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
-                                                       double* __restrict__ part) {
-  __shared__ double red[256];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  const int tl = threadIdx.x + blockDim.x * threadIdx.y;
+__global__ void __launch_bounds__(128) k_visc4_partial(Geo<T> g, Metrics<T> m, const T* __restrict__ ux,
+                                                       double* __restrict__ part, int rows) {
+  __shared__ double red[4];
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31), k = blockIdx.y * 4 + (threadIdx.x >> 5);
+  const int j0 = blockIdx.z * rows, j1 = min(j0 + rows, g.ny);
   double s = 0.0;
-  if (i < g.nx && j < g.ny) {
-    const Nbr n = make_nbr(g, i, j, k);
+  if (i < g.nx && k < g.nz) {
     const C4<T> c(g);
-    const int jc = j + 1;
-    const T ux_c = at(ux, n, 0);
-    const T d11 = c.dxx1 * at(ux, n, n.xm2) + c.dxx2 * at(ux, n, n.xm) + c.dxx3 * ux_c + c.dxx4 * at(ux, n, n.xp) +
-                  c.dxx5 * at(ux, n, n.xp2);
-    const T d22 = m.ap2c[jc] * at_jp(ux, g, 0, n, 0) + m.ac2c[jc] * ux_c + m.am2c[jc] * at_jm(ux, g, 0, n, 0);
-    const T d33 = c.dzz1 * at(ux, n, n.zm2) + c.dzz2 * at(ux, n, n.zm) + c.dzz3 * ux_c + c.dzz4 * at(ux, n, n.zp) +
-                  c.dzz5 * at(ux, n, n.zp2);
-    s = ((double)(d11 + d33) + (double)d22) * (double)m.dyp[jc];
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const Nbr n = make_nbr(g, i, j, k);
+      const int jc = j + 1;
+      const T ux_c = at(ux, n, 0);
+      const T d11 = c.dxx1 * at(ux, n, n.xm2) + c.dxx2 * at(ux, n, n.xm) + c.dxx3 * ux_c + c.dxx4 * at(ux, n, n.xp) +
+                    c.dxx5 * at(ux, n, n.xp2);
+      const T d22 = m.ap2c[jc] * at_jp(ux, g, 0, n, 0) + m.ac2c[jc] * ux_c + m.am2c[jc] * at_jm(ux, g, 0, n, 0);
+      const T d33 = c.dzz1 * at(ux, n, n.zm2) + c.dzz2 * at(ux, n, n.zm) + c.dzz3 * ux_c + c.dzz4 * at(ux, n, n.zp) +
+                    c.dzz5 * at(ux, n, n.zp2);
+      s += ((double)(d11 + d33) + (double)d22) * (double)m.dyp[jc];
+    }
   }
-  red[tl] = s;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
-  for (int w = blockDim.x * blockDim.y / 2; w > 0; w >>= 1) {
-    if (tl < w) red[tl] += red[tl + w];
-    __syncthreads();
-  }
-  if (tl == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = red[0];
+  if (threadIdx.x == 0)
+    part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = (red[0] + red[1]) + (red[2] + red[3]);
+}
+
+// rows per k_visc4_partial block: whole columns when the x-z plane alone gives
+// about eight blocks per SM, shorter chunks on small grids
+static int visc4_rows(const ch3d_ctx* c) {
+  const long long cols = (long long)((c->nx + 31) / 32) * ((c->nz + 3) / 4);
+  const long long chunks = (148LL * 8 + cols - 1) / cols;
+  const int rows = (int)((c->ny + chunks - 1) / chunks);
+  return rows < 8 ? 8 : rows;
+}
+static dim3 visc4_grid(const ch3d_ctx* c) {
+  const int rows = visc4_rows(c);
+  return dim3((c->nx + 31) / 32, (c->nz + 3) / 4, (c->ny + rows - 1) / rows);
+}
+int visc4_npart(const ch3d_ctx* c) {
+  const dim3 g = visc4_grid(c);
+  return (int)(g.x * g.y * g.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -213,8 +229,8 @@ cudaError_t launch_rhs4(ch3d_ctx* c) { return c->fp32 ? rhs4_t<float>(c) : rhs4_
 
 template <class T> static cudaError_t visc4_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
-  k_visc4_partial<T><<<dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz), dim3(32, 8), 0, c->stream>>>(
-      make_geo<T>(c), metrics_of<T>(c), f[0], c->part);
+  k_visc4_partial<T><<<visc4_grid(c), 128, 0, c->stream>>>(make_geo<T>(c), metrics_of<T>(c), f[0], c->part,
+                                                           visc4_rows(c));
   return cudaGetLastError();
 }
 cudaError_t launch_visc4_partials(ch3d_ctx* c) { return c->fp32 ? visc4_t<float>(c) : visc4_t<double>(c); }

@@ -97,6 +97,7 @@ SIGNATURES = {
                                                  ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     "ch3d_stats_fetch": (ctypes.c_int, [_VP, _DP, _IP, _DP, ctypes.c_int]),
     "ch3d_stats_fetch_grad": (ctypes.c_int, [_VP, _DP]),
+    "ch3d_dissipation": (ctypes.c_int, [_VP, _DP]),
     "ch3d_interp_state": (ctypes.c_int, [_VP, _VP]),
     "ch3d_spectra_accumulate": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "ch3d_spectra_fetch": (ctypes.c_int, [_VP, _DP, _DP, _DP, _IP, ctypes.c_int]),

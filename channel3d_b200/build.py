@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libch3d.so")
-SOURCES = ["ch3d_step.cu", "ch3d_step4.cu", "ch3d_fimp.cu", "ch3d_march.cu", "ch3d_rfft.cu", "ch3d_interp.cu", "ch3d_spectra.cu", "ch3d_les.cu", "mlp_tc.cu", "ch3d_api.cu"]
+SOURCES = ["ch3d_step.cu", "ch3d_step4.cu", "ch3d_fimp.cu", "ch3d_march.cu", "ch3d_rfft.cu", "ch3d_interp.cu", "ch3d_spectra.cu", "ch3d_tg.cu", "ch3d_les.cu", "mlp_tc.cu", "ch3d_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1023,6 +1023,22 @@ int ch3d_stats_fetch_grad(ch3d_ctx* c, double* sumgrad) {
   return CH3D_OK;
 }
 
+int ch3d_dissipation(ch3d_ctx* c, double* eps) {
+  if (!c || !eps) return fail(CH3D_ERR_INVALID, "NULL argument");
+  if (c->cfg.order != 2) return fail(CH3D_ERR_UNSUPPORTED, "clcStat_TG belongs to the 2nd-order solver");
+  CU(cudaSetDevice(c->device));
+  int np = 0;
+  CU(launch_dissipation(c, &np));
+  CU(launch_reduce_partials(c, c->part2, np, c->red2));
+  std::vector<double> r(CH3D_NRED);
+  CU(cudaMemcpyAsync(r.data(), c->red2, CH3D_NRED * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  double s = 0.0;
+  for (double v : r) s += v;
+  *eps = c->cfg.xnu * s / ((double)c->nx * (double)c->ny * (double)c->nz);
+  return CH3D_OK;
+}
+
 int ch3d_sgs_mlp_set(ch3d_ctx* c, const float* params, const float* norm) {
   if (!c || !params || !norm) return fail(CH3D_ERR_INVALID, "NULL argument");
   if (c->cfg.LES_type != CH3D_LES_MLP) return fail(CH3D_ERR_INVALID, "LES_type is not CH3D_LES_MLP");

@@ -147,6 +147,8 @@ cudaError_t launch_convert(ch3d_ctx* c, const void* src, void* dst, long long n,
 cudaError_t launch_rhs4(ch3d_ctx* c);                  // stage path: interpolation + RhsX/Y/Z
 cudaError_t launch_visc4_partials(ch3d_ctx* c);        // mean viscous stress partial sums -> part
 int visc4_npart(const ch3d_ctx* c);                   // their count
+cudaError_t launch_dissipation(ch3d_ctx* c, int* npart);  // CalcDissipationRate partials -> part2
+cudaError_t launch_reduce_partials(ch3d_ctx* c, const double* in, int n, double* out);  // CH3D_NRED sums
 // fully implicit 2nd-order step (ch3d_step.cu, ch3d_fimp.cu)
 cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP -> RhsX/Y/Z
 cudaError_t launch_ptri_xz(ch3d_ctx* c);               // periodic x and z sweeps of RhsX/Y/Z, in place

@@ -1158,6 +1158,11 @@ __global__ void __launch_bounds__(256) k_reduce_partials(const double* __restric
   if (threadIdx.x == 0) out[blockIdx.x] = red[0];
 }
 
+cudaError_t launch_reduce_partials(ch3d_ctx* c, const double* in, int n, double* out) {
+  k_reduce_partials<<<CH3D_NRED, 256, 0, c->stream>>>(in, n, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_substep_setup(ch3d_ctx* c, int ns) {
   // the partials of the bulk sums (march projection or k_bulk_partial), or of the
   // 4th-order viscous sum (k_visc4_partial)

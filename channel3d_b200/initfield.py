@@ -75,3 +75,28 @@ def large_scale(cfg, amplitude=0.3, seed=SEED, yp=None, ubulk=1.0, kmax=4):
     uy[:, 0, :] = 0.0
     uz = out[2]
     return ux, uy, uz, np.zeros((nz, ny, nx))
+
+
+def taylor_green(cfg, yp=None, vel=1.0, length=1.0):
+    """InitVelocity_TG (src/CFD_2nd/m_FlowType_TGVortex.f90:20-47) on the
+    staggered mesh: ux(i,j,k) = V sin(x_i / L) cos(yc_j / L) cos(zc_k / L),
+    uy = -V cos(xc_i / L) sin(yp_j / L) cos(zc_k / L), uz = 0, p = 0, with
+    x_i = (i - 1) dx, xc = x + dx / 2 (the same in z), yp the y nodes and yc
+    the cell centres.  The field is mirror-symmetric about y = 0 and y = pi L
+    (uy odd, ux and uz even), so a box of height pi L with free-slip walls
+    holds half a period of the triply periodic vortex."""
+    if yp is None:
+        yp = mesh_y(cfg)
+    yp = np.asarray(yp)
+    yc = cell_centres(yp)
+    nx, nz = cfg.nxc, cfg.nzc
+    dx, dz = cfg.xlx / nx, cfg.zlz / nz
+    xp = np.arange(nx) * dx
+    zp = np.arange(nz) * dz
+    xc, zc = xp + 0.5 * dx, zp + 0.5 * dz
+    ux = vel * np.sin(xp / length)[None, None, :] * np.cos(yc / length)[None, :, None] * np.cos(zc / length)[:, None, None]
+    uy = -vel * np.cos(xc / length)[None, None, :] * np.sin(yp[:-1] / length)[None, :, None] * np.cos(zc / length)[:, None, None]
+    uz = np.zeros(cfg.shape)
+    p = np.zeros(cfg.shape)
+    return np.ascontiguousarray(ux), np.ascontiguousarray(uy), uz, p
+

@@ -187,6 +187,13 @@ class ChannelSolver:
         _lib.check(self.lib.ch3d_stats_fetch_grad(self.ctx, _lib.dptr(g)), self.lib)
         return g.reshape(self.cfg.nyc + 1, 98)
 
+    def dissipation(self):
+        """clcStat_TG (src/CFD_2nd/m_FlowType_TGVortex.f90:87-113): xnu times the
+        mean over the cells of CalcDissipationRate, 2 S_ij S_ij, of the current field."""
+        v = np.zeros(1)
+        _lib.check(self.lib.ch3d_dissipation(self.ctx, _lib.dptr(v)), self.lib)
+        return float(v[0])
+
     def kernel_times(self, nsteps=1):
         out = np.zeros(7)
         _lib.check(self.lib.ch3d_kernel_times(self.ctx, int(nsteps), _lib.dptr(out), 7), self.lib)

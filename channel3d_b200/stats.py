@@ -76,3 +76,12 @@ def write_spectra2d(path, spec2d, nspectime):
     r[0, 0] = r[0, -1] = r[-1, 0] = r[-1, -1] = 1.0
     (a * (r[None, :, None, :] / nspectime)).astype(np.float32).tofile(path)
 
+
+def write_tg_dissipation(path, rows):
+    """The TG_dissp file of clcStat_TG (src/CFD_2nd/m_FlowType_TGVortex.f90:
+    69-80, 105-109): one line per sample, SimTime and xnu <2 S_ij S_ij> in the
+    format (2ES24.15)."""
+    with open(path, "w") as f:
+        for t, eps in rows:
+            f.write("%24.15E%24.15E\n" % (t, eps))
+

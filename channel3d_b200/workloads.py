@@ -35,6 +35,18 @@ WORKLOADS = {
 }
 
 
+def taylor_green(n=64, xnu=6.25e-4, dt=0.01, **kw):
+    """The Taylor-Green vortex of Input/TaylorGreenVortex.prm (FlowType 3, V = L = 1,
+    xnu 6.25e-4, dt 0.01 fixed) in a 2pi x pi x 2pi box with free-slip walls at
+    y = 0 and pi (half a period of the triply periodic vortex, whose symmetry
+    the walls keep), n x n/2 x n uniform cells (dy = dx, so the staggered
+    initial field is discretely divergence-free); no forcing."""
+    return ChannelConfig(FlowType=3, nxc=n, nyc=n // 2, nzc=n, xlx=2 * np.pi, yly=np.pi, zlz=2 * np.pi, xnu=xnu,
+                         dtMax=dt, iCFL=2, IsImplicit=1, BcOption=[0, 0, -2, -2, 0, 0], IsUxConst=False, ubulk=0.0,
+                         ybulk1=0.0, ybulk2=np.pi, nSection=1, SectionLength=[1.0], nycSection=[n // 2],
+                         StretType=[0], StretOption=[0], SectioncStret=[0.0], RunName="TGVortex", **kw)
+
+
 def get(name, **kw):
     factory, steps = WORKLOADS[name]
     return factory(**kw), steps

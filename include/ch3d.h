@@ -218,6 +218,14 @@ CH3D_API int ch3d_spectra_fetch(ch3d_ctx* ctx, double* specx, double* specz, dou
    sums), Fortran order.  Fetch them before a resetting ch3d_stats_fetch. */
 CH3D_API int ch3d_stats_fetch_grad(ch3d_ctx* ctx, double* sumgrad);
 
+/* The Taylor-Green vortex statistic of the 2nd-order solver: clcStat_TG
+   (src/CFD_2nd/m_FlowType_TGVortex.f90:87-113), *eps = xnu times the mean
+   over the cells of CalcDissipationRate (src/CFD_2nd/m_Tools.f90:497-540,
+   2 S_ij S_ij with the reference's stencils), of the current velocity: the
+   value the reference writes to TG_dissp beside SimTime.  Synchronous;
+   CH3D_ERR_UNSUPPORTED for a 4th-order context. */
+CH3D_API int ch3d_dissipation(ch3d_ctx* ctx, double* eps);
+
 /* LES: computes nut from the current velocity as the step does once per
    step, Clc_SGS_Vis (src/CFD_2nd/m_LESModels.f90:47-62) followed by the wall
    and periodic ghost rules of SetBC_and_UpdateHalo_SGS (:375-428).

@@ -974,8 +974,10 @@ struct Oracle {
     }
   }
 
-  // ---- src/CFD_2nd/m_LESModels.f90:328-370 (ClcVelStrainRate): |S| = sqrt(2 Sij Sij) ----
-  double StrainRate(int ic, int jc, int kc) {
+  // ---- src/CFD_2nd/m_LESModels.f90:328-370 (ClcVelStrainRate): |S| = sqrt(2 Sij Sij);
+  // the same sum without the root is CalcDissipationRate (src/CFD_2nd/m_Tools.f90:497-540) ----
+  double StrainRate(int ic, int jc, int kc) { return std::sqrt(StrainRate2(ic, jc, kc)); }
+  double StrainRate2(int ic, int jc, int kc) {
     int ip = ic + 1, im = ic - 1, jp = jc + 1, jm = jc - 1, kp = kc + 1, km = kc - 1;
     double caj = rdyp(jc), cac1 = rdyc(jc), cac2 = rdyc(jp), cac12 = cac1 - cac2;
     const double oneEighth = 0.125;
@@ -990,7 +992,17 @@ struct Oracle {
     double st6 = oneEighth * ((uy(ic, jp, kp) + uy(ic, jc, kp) - uy(ic, jp, km) - uy(ic, jc, km)) * rdz +
                               (uz(ic, jp, kp) + uz(ic, jp, kc)) * cac2 + (uz(ic, jc, kp) + uz(ic, jc, kc)) * cac12 -
                               (uz(ic, jm, kp) + uz(ic, jm, kc)) * cac1);
-    return std::sqrt(two * (st1 * st1 + st2 * st2 + st3 * st3) + four * (st4 * st4 + st5 * st5 + st6 * st6));
+    return two * (st1 * st1 + st2 * st2 + st3 * st3) + four * (st4 * st4 + st5 * st5 + st6 * st6);
+  }
+
+  // ---- src/CFD_2nd/m_FlowType_TGVortex.f90:87-113 (clcStat_TG): xnu * sum(dissp) / (nxc nyc nzc) ----
+  double TGDissipation() {
+    SetBC_and_UpdateHalo();
+    double sumr = 0.0;
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) sumr += StrainRate2(ic, jc, kc);
+    return P.xnu * sumr / ((double)nxc * (double)nyc * (double)nzc);
   }
 
   // ---- src/CFD_2nd/m_LESModels.f90:145-258 (Clc_SGS_MTS), filter from InitFilterCoe :35-41 ----
@@ -2532,6 +2544,8 @@ void orc_hc2r(int n, double* x) {
   std::vector<cplx> a, b;
   hc2r(pl, x, a, b);
 }
+
+double orc_dissipation(void* h) { return ((Oracle*)h)->TGDissipation(); }
 
 void orc_stats_accumulate(void* h) {
   Oracle* o = (Oracle*)h;

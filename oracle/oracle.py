@@ -98,6 +98,8 @@ def lib():
         L.orc_spectra_get.argtypes = [ctypes.c_void_p, _DP, _DP]
         L.orc_spectra_get2d.restype = ctypes.c_int
         L.orc_spectra_get2d.argtypes = [ctypes.c_void_p, _DP]
+        L.orc_dissipation.argtypes = [ctypes.c_void_p]
+        L.orc_dissipation.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -265,6 +267,10 @@ class Oracle:
         s2 = np.empty((9, c.nzc // 2 + 1, c.nyc // 2, c.nxc // 2 + 1))
         n = self.L.orc_spectra_get2d(self.h, _p(s2))
         return s2, n
+
+    def dissipation(self):
+        """clcStat_TG's value: xnu * mean over the cells of CalcDissipationRate."""
+        return float(lib().orc_dissipation(self.h))
 
     def stats_get_grad(self):
         """4th order: SumGrad(98, nyp) as (nyp, 98), and nfstime."""

@@ -252,3 +252,27 @@ def test_spectra_writer(tmp_path):
     b2 = np.fromfile(str(tmp_path / "Spec2D"), dtype=np.float32).reshape(9, 3, 5, 4)
     assert b2[0, 1, 2, 1] == 4 and b2[0, 0, 2, 1] == 2 and b2[0, 1, 2, 3] == 2 and b2[0, 2, 0, 0] == 1
 
+
+def test_taylor_green_field_and_writer(tmp_path):
+    """InitVelocity_TG on the staggered mesh: the analytic values, uy zero on
+    the y = 0 plane, discretely divergence-free when dy = dx; and the
+    TG_dissp lines in the reference's (2ES24.15) format."""
+    from channel3d_b200 import initfield, stats, workloads
+    cfg = workloads.taylor_green(16)
+    yp = np.linspace(0.0, np.pi, cfg.nyc + 1)
+    ux, uy, uz, p = initfield.taylor_green(cfg, yp=yp)
+    h = cfg.xlx / cfg.nxc
+    i, j, k = 3, 5, 7
+    yc = 0.5 * (yp[j] + yp[j + 1])
+    assert abs(ux[k, j, i] - np.sin(i * h) * np.cos(yc) * np.cos((k + 0.5) * h)) < 1e-15
+    assert abs(uy[k, j, i] + np.cos((i + 0.5) * h) * np.sin(yp[j]) * np.cos((k + 0.5) * h)) < 1e-15
+    assert not uy[:, 0, :].any() and not uz.any() and not p.any()
+    uyp = np.concatenate([uy[:, 1:, :], np.zeros_like(uy[:, :1, :])], axis=1)
+    div = (np.roll(ux, -1, axis=2) - ux) / h + (uyp - uy) / np.diff(yp)[None, :, None]
+    assert np.abs(div).max() < 1e-13
+    path = tmp_path / "TG_dissp0000001000"
+    stats.write_tg_dissipation(path, [(0.0, 4.6426766105924085e-4), (0.01, 4.64e-4)])
+    lines = path.read_text().splitlines()
+    assert lines[0] == "   0.000000000000000E+00   4.642676610592409E-04"
+    assert len(lines[1]) == 48
+

@@ -373,3 +373,20 @@ def test_oracle_interp_known_answers():
     ux = d.get_state()["ux"]
     dy = np.diff(mesh_y(new))
     assert abs((ux * dy[None, :, None]).sum() / (new.nxc * new.nzc * new.yly) - 0.8) < 1e-12
+
+
+def test_oracle_tg_dissipation_known_answer():
+    """CalcDissipationRate of the Taylor-Green field (clcStat_TG) on a uniform
+    mesh of spacing h: xnu (s^2/2 + c^2/4), s = sin(h/2)/(h/2),
+    c = sin(h) cos(h/2)/h, for two resolutions."""
+    from channel3d_b200 import initfield, workloads
+    from oracle import oracle as O
+    for n in (16, 32):
+        cfg = workloads.taylor_green(n)
+        h = cfg.xlx / n
+        s, c = np.sin(h / 2) / (h / 2), np.sin(h) * np.cos(h / 2) / h
+        o = O.Oracle(cfg)
+        o.set_state(*initfield.taylor_green(cfg, yp=o.mesh()[0]))
+        eps = o.dissipation()
+        assert abs(eps / (cfg.xnu * (s * s / 2 + c * c / 4)) - 1.0) < 1e-13, (n, eps)
+

@@ -259,6 +259,7 @@ int alloc_fields(ch3d_ctx* c) {
   }
   if (c->cfg.LES_type == CH3D_LES_MLP) {
     CU(cudaMalloc(&c->mlp_params, CH3D_MLP_NPARAM * sizeof(float)));
+    CU(cudaMalloc(&c->mlp_packed, 32 * 1024));  // the network's parameter image (21.3 KB)
     CU(cudaMalloc(&c->mlp_status, sizeof(int)));
     CU(cudaMemsetAsync(c->mlp_status, 0, sizeof(int), c->stream));
     CU(cudaMalloc(&c->sgs_tau, (size_t)c->N * 6 * sizeof(double)));
@@ -702,7 +703,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   for (int q = 0; q < 6; ++q) if (c->ih[q]) cudaFree(c->ih[q]);
   if (c->pfac) cudaFree(c->pfac);
   if (c->les_delta) cudaFree(c->les_delta);
-  void* mbufs[] = {c->mlp_params, c->mlp_status, c->sgs_tau, c->sgs_f, c->spec2,
+  void* mbufs[] = {c->mlp_params, c->mlp_packed, c->mlp_status, c->sgs_tau, c->sgs_f, c->spec2,
                    c->specacc};
   for (void* b : mbufs) if (b) cudaFree(b);
   void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
@@ -1048,6 +1049,8 @@ int ch3d_sgs_mlp_set(ch3d_ctx* c, const float* params, const float* norm) {
     if (!(norm[46 + q] > 0)) return fail(CH3D_ERR_INVALID, "output standard deviation %d not positive", q);
   CU(cudaSetDevice(c->device));
   CU(cudaMemcpy(c->mlp_params, params, CH3D_MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  CU(launch_mlp_pack(c));
+  CU(cudaStreamSynchronize(c->stream));
   std::memcpy(c->mlp_norm, norm, sizeof(c->mlp_norm));
   c->mlp_ready = true;
   if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }  // the norm is a kernel argument

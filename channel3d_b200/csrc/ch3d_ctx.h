@@ -43,6 +43,7 @@ struct ch3d_ctx {
   double* les_delta = nullptr;  // LES: DeltaCell (ny+2) | wall distance of the cell centres (ny+2)
   // learned closure (LES_type CH3D_LES_MLP)
   float* mlp_params = nullptr;   // CH3D_MLP_NPARAM FP32
+  unsigned char* mlp_packed = nullptr;  // their BF16 operand image (k_mlp_pack)
   float mlp_norm[CH3D_SGS_NORM_FLOATS] = {0};
   bool mlp_ready = false;
   int* mlp_status = nullptr;
@@ -154,6 +155,7 @@ cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP -> Rh
 cudaError_t launch_ptri_xz(ch3d_ctx* c);               // periodic x and z sweeps of RhsX/Y/Z, in place
 size_t ptri_factor_doubles(int nx, int nz);
 // LES (ch3d_les.cu), FP64
+cudaError_t launch_mlp_pack(ch3d_ctx* c);              // parameter image of the closure's network
 cudaError_t launch_fill_nut(ch3d_ctx* c);              // nut = xnu (learned closure)
 cudaError_t launch_sgs_nut(ch3d_ctx* c);               // Clc_SGS_Vis -> nut
 cudaError_t launch_rhs_les(ch3d_ctx* c);               // clcRhsX/Y/Z_PIMP_LES -> RhsX/Y/Z

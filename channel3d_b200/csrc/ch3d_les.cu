@@ -484,11 +484,12 @@ __device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metri
 // *mstatus and writes the fallback stresses.
 __global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
     k_sgs_mlp(Geo<double> g, Metrics<double> m, LesPar lp, MlpNormD nm, const double* __restrict__ ux,
-              const double* __restrict__ uy, const double* __restrict__ uz, const float* __restrict__ P,
+              const double* __restrict__ uy, const double* __restrict__ uz, const unsigned char* __restrict__ img,
               double* __restrict__ tau, int* __restrict__ mstatus, const DevScalars* __restrict__ sc) {
   using namespace ch3d_mlp;
   extern __shared__ __align__(1024) unsigned char smem[];
   if (sc->status) return;  // uniform: every thread reads the same word
+  fwd_prologue_packed(smem, img);  // the parameter image arrives while the inputs are formed
   const long long N = g.N;  // below 2^31 (checked by the launch)
   const int c = blockIdx.x * TILE + threadIdx.x;
   const bool valid = c < N;
@@ -529,9 +530,10 @@ __global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
 #pragma unroll
     for (int q = 0; q < NIN; ++q) x[q] = 0.f;
   }
-  fwd_prologue(smem, P, x);
   float y[NOUT];
-  const bool ok = fwd_layers(smem, y, nullptr, nullptr, c, valid, N);
+  bool ok = false;
+  if (fwd_inputs(smem, x)) ok = fwd_layers(smem, y, nullptr, nullptr, c, valid, N);
+  else fwd_abort(smem);
   if (!ok && threadIdx.x == 0) atomicExch(mstatus, 1);
   if (!valid) return;
   const double u2 = sc->utau * sc->utau;
@@ -694,10 +696,21 @@ cudaError_t launch_sgs_nut(ch3d_ctx* c) {
   });
   if (e != cudaSuccess) return e;
   k_sgs_mlp<<<(unsigned)((c->N + ch3d_mlp::TILE - 1) / ch3d_mlp::TILE), ch3d_mlp::TILE, ch3d_mlp::FwdSmem::BYTES,
-              c->stream>>>(g, c->m64, lp, nm, f[0], f[1], f[2], c->mlp_params, c->sgs_tau, c->mlp_status, c->sc);
+              c->stream>>>(g, c->m64, lp, nm, f[0], f[1], f[2], c->mlp_packed, c->sgs_tau, c->mlp_status, c->sc);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_sgs_force<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, c->sgs_tau, c->sgs_f, c->sgs_f + c->N,
                                                           c->sgs_f + 2 * c->N, c->sc);
+  return cudaGetLastError();
+}
+
+// the network's parameter image (BF16 operands and FP32 biases as the
+// forward pass holds them in shared memory), once per parameter set
+__global__ void __launch_bounds__(128) k_mlp_pack(const float* __restrict__ P, unsigned char* __restrict__ img) {
+  ch3d_mlp::pack_params(img, P);
+}
+
+cudaError_t launch_mlp_pack(ch3d_ctx* c) {
+  k_mlp_pack<<<1, 128, 0, c->stream>>>(c->mlp_params, c->mlp_packed);
   return cudaGetLastError();
 }
 

@@ -227,7 +227,8 @@ __device__ __forceinline__ void stage_wt(unsigned char* t, const float* __restri
 }
 
 struct Smem {
-  uint64_t bar;
+  uint64_t bar;   // tensor-core completion
+  uint64_t wbar;  // arrival of the packed parameters (fwd_prologue_packed)
   uint32_t tmem;
   int err;
 };
@@ -247,6 +248,26 @@ struct FwdSmem {
   static constexpr size_t BYTES = BIAS + (3 * NH + 16) * 4;
 };
 
+// bytes of the parameter image: the four weight operands and the biases, as
+// they lie in the forward pass's shared memory from FwdSmem::W1 on
+constexpr size_t kPackedBytes = FwdSmem::BYTES - FwdSmem::W1;
+static_assert(FwdSmem::W1 % 16 == 0 && kPackedBytes % 16 == 0, "bulk copy alignment");
+
+// Write the parameter image of P into `img` (global or shared memory; all
+// threads of the block take part): W1..W4 as BF16 K-major operands, the
+// biases as FP32, at their offsets from FwdSmem::W1.
+__device__ __forceinline__ void pack_params(unsigned char* img, const float* __restrict__ P) {
+  stage_w(img + (FwdSmem::W1 - FwdSmem::W1), P + OW1, NH, NIN, NH, NINP);
+  stage_w(img + (FwdSmem::W2 - FwdSmem::W1), P + OW2, NH, NH, NH, NH);
+  stage_w(img + (FwdSmem::W3 - FwdSmem::W1), P + OW3, NH, NH, NH, NH);
+  stage_w(img + (FwdSmem::W4 - FwdSmem::W1), P + OW4, NOUT, NH, NOUTP, NH);
+  float* bs = (float*)(img + (FwdSmem::BIAS - FwdSmem::W1));
+  for (int e = threadIdx.x; e < 3 * NH + 16; e += blockDim.x) {
+    const int l = e / NH, c = e - l * NH;
+    bs[e] = l < 3 ? __ldg(P + (l == 0 ? OB1 : l == 1 ? OB2 : OB3) + c) : (c < NOUT ? __ldg(P + OB4 + c) : 0.f);
+  }
+}
+
 // Stage the parameters (weights as BF16 operands, biases as FP32) and the
 // point's standardised inputs x[0..9] (row tid of the X tile), set up the
 // mbarrier and the tensor memory (64 columns).  Ends with the barrier that
@@ -256,15 +277,7 @@ __device__ __forceinline__ void fwd_prologue(unsigned char* smem, const float* _
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) { mbar_init(&S->bar, 1); S->err = 0; }
   if (warp == 0) { tmem_alloc(&S->tmem, 64); tmem_relinquish(); }
-  stage_w(smem + FwdSmem::W1, P + OW1, NH, NIN, NH, NINP);
-  stage_w(smem + FwdSmem::W2, P + OW2, NH, NH, NH, NH);
-  stage_w(smem + FwdSmem::W3, P + OW3, NH, NH, NH, NH);
-  stage_w(smem + FwdSmem::W4, P + OW4, NOUT, NH, NOUTP, NH);
-  float* bs = (float*)(smem + FwdSmem::BIAS);
-  for (int e = tid; e < 3 * NH + 16; e += blockDim.x) {
-    const int l = e / NH, c = e - l * NH;
-    bs[e] = l < 3 ? __ldg(P + (l == 0 ? OB1 : l == 1 ? OB2 : OB3) + c) : (c < NOUT ? __ldg(P + OB4 + c) : 0.f);
-  }
+  pack_params(smem + FwdSmem::W1, P);
   float xp[16];
 #pragma unroll
   for (int k = 0; k < 16; ++k) xp[k] = k < NIN ? x[k] : 0.f;
@@ -274,6 +287,56 @@ __device__ __forceinline__ void fwd_prologue(unsigned char* smem, const float* _
   fence_before();
   __syncthreads();
   fence_after();
+}
+
+// The same with the parameter image `img` (kPackedBytes, 16-byte aligned,
+// written by pack_params) brought in by one bulk asynchronous copy issued at
+// entry: the copy runs while the caller forms the inputs; fwd_inputs then
+// stages them and waits for the copy (bounded).
+__device__ __forceinline__ void fwd_prologue_packed(unsigned char* smem, const unsigned char* __restrict__ img) {
+  Smem* S = (Smem*)smem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (tid == 0) {
+    mbar_init(&S->bar, 1);
+    mbar_init(&S->wbar, 1);
+    S->err = 0;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(&S->wbar)),
+                 "r"((uint32_t)kPackedBytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            su32(smem + FwdSmem::W1)),
+        "l"(img), "r"((uint32_t)kPackedBytes), "r"(su32(&S->wbar))
+        : "memory");
+  }
+  if (warp == 0) { tmem_alloc(&S->tmem, 64); tmem_relinquish(); }
+}
+// Stage the point's inputs x[0..9] (row tid of the X tile) and wait for the
+// parameter image.  Returns false (uniformly) when the wait expired; the
+// caller then skips the network, the copy having been waited for as long as
+// the limit allows.
+__device__ __forceinline__ bool fwd_inputs(unsigned char* smem, const float* x) {
+  Smem* S = (Smem*)smem;
+  const int tid = threadIdx.x;
+  float xp[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) xp[k] = k < NIN ? x[k] : 0.f;
+  st_bf16x8(smem + FwdSmem::XA, tid, 0, TILE, xp);
+  st_bf16x8(smem + FwdSmem::XA, tid, 8, TILE, xp + 8);
+  fence_async_smem();
+  fence_before();
+  __syncthreads();  // the barriers' initialisation, the X tile, the tensor memory
+  fence_after();
+  return __syncthreads_or(mbar_wait(&S->wbar, 0) ? 0 : 1) == 0;
+}
+
+// After an expired wait in fwd_inputs: wait once more (bounded) for the copy
+// in flight, then release the tensor memory.
+__device__ __forceinline__ void fwd_abort(unsigned char* smem) {
+  Smem* S = (Smem*)smem;
+  mbar_wait(&S->wbar, 0);
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(S->tmem, 64);
 }
 
 // The four layers on the staged tile: y[0..5] = network output of this

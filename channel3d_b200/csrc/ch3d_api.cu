@@ -225,8 +225,8 @@ int check_config(const ch3d_config* g) {
     if (g->LES_type != CH3D_LES_WALE && g->LES_type != CH3D_LES_MTS && g->LES_type != CH3D_LES_SMAG_VD &&
         g->LES_type != CH3D_LES_MLP)
       return fail(CH3D_ERR_UNSUPPORTED, "LES_type=%d not built", g->LES_type);
-    if (g->order != 2 || g->IsImplicit != 1 || g->precision != CH3D_PREC_FP64)
-      return fail(CH3D_ERR_UNSUPPORTED, "LES is built for the 2nd-order partially implicit FP64 step (the reference "
+    if (g->order != 2 || g->IsImplicit != 1)
+      return fail(CH3D_ERR_UNSUPPORTED, "LES is built for the 2nd-order partially implicit step (the reference "
                   "has no FIMP+LES either)");
     if (g->LES_type == CH3D_LES_MTS && g->FilterType != 0 && g->FilterType != 1)
       return fail(CH3D_ERR_INVALID, "unrecognized FilterType");

@@ -16,7 +16,8 @@
 namespace ch3d {
 
 // nut at a y row that may be the wall ghost (j = -1 or ny)
-__device__ __forceinline__ double nut_at(const double* __restrict__ nut, const Geo<double>& g, const Nbr& n,
+template <class T>
+__device__ __forceinline__ double nut_at(const T* __restrict__ nut, const Geo<T>& g, const Nbr& n,
                                          long long o, int dj) {
   if (dj < 0 && n.jlo) {
     const double v = __ldg(nut + n.c + o);
@@ -30,8 +31,9 @@ __device__ __forceinline__ double nut_at(const double* __restrict__ nut, const G
 }
 
 // |S| = sqrt(2 Sij Sij) of ClcVelStrainRate (src/CFD_2nd/m_LESModels.f90:328-370)
-__device__ __forceinline__ double strain_rate(const Geo<double>& g, const Metrics<double>& m, const double* ux,
-                                              const double* uy, const double* uz, const Nbr& n, int jc) {
+template <class T>
+__device__ __forceinline__ double strain_rate(const Geo<T>& g, const Metrics<double>& m, const T* ux,
+                                              const T* uy, const T* uz, const Nbr& n, int jc) {
   const double rdx = g.rdx, rdz = g.rdz;
   const double caj = m.rdyp[jc], cac1 = m.rdyc[jc], cac2 = m.rdyc[jc + 1], cac12 = cac1 - cac2;
   const double e = 0.125;
@@ -60,7 +62,8 @@ struct LesPar {
 };
 
 // x-z mean wall shear -> u_tau (Smagorinsky / van Driest); one block
-__global__ void __launch_bounds__(1024) k_wall_utau(Geo<double> g, const double* __restrict__ ux, double d1, double dN,
+template <class T>
+__global__ void __launch_bounds__(1024) k_wall_utau(Geo<T> g, const T* __restrict__ ux, double d1, double dN,
                                                     DevScalars* __restrict__ sc) {
   __shared__ double r1[1024], r2[1024];
   if (sc->status) return;
@@ -84,9 +87,10 @@ __global__ void __launch_bounds__(1024) k_wall_utau(Geo<double> g, const double*
   }
 }
 
-__global__ void __launch_bounds__(256) k_sgs_nut(Geo<double> g, Metrics<double> m, LesPar lp,
-                                                 const double* __restrict__ ux, const double* __restrict__ uy,
-                                                 const double* __restrict__ uz, double* __restrict__ nut,
+template <class T>
+__global__ void __launch_bounds__(256) k_sgs_nut(Geo<T> g, Metrics<double> m, LesPar lp,
+                                                 const T* __restrict__ ux, const T* __restrict__ uy,
+                                                 const T* __restrict__ uz, T* __restrict__ nut,
                                                  const DevScalars* __restrict__ sc) {
   if (sc->status) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -128,7 +132,7 @@ __global__ void __launch_bounds__(256) k_sgs_nut(Geo<double> g, Metrics<double> 
   } else if (lp.model == CH3D_LES_MTS) {  // Clc_SGS_MTS (m_LESModels.f90:145-258)
     const double* F = lp.Fc;
     // test-filtered fluctuation u - F(u) of a staggered component at offset o of row dj
-    auto filt = [&](const double* u, int comp, long long o, int dj) {
+    auto filt = [&](const T* u, int comp, long long o, int dj) {
       auto val = [&](long long oo) { return dj > 0 ? at_jp(u, g, comp, n, o + oo) : at(u, n, o + oo); };
       return F[0] * val(n.xm + n.zm) + F[1] * val(n.zm) + F[2] * val(n.xp + n.zm) +
              F[3] * val(n.xm) + (F[4] - 1.0) * val(0) + F[5] * val(n.xp) +
@@ -170,16 +174,17 @@ __global__ void __launch_bounds__(256) k_sgs_nut(Geo<double> g, Metrics<double> 
     const double l = lp.Cs * D * lp.delta[jc];
     v = l * l * strain_rate(g, m, ux, uy, uz, n, jc) + xnu;
   }
-  nut[n.c] = v;
+  nut[n.c] = (T)v;
 }
 
 // clcRhsX/Y/Z_PIMP_LES at one cell; RhsX includes dpmdxns (:140-153).
-__global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> m, const double* __restrict__ ux,
-                                                 const double* __restrict__ uy, const double* __restrict__ uz,
-                                                 const double* __restrict__ pr, const double* __restrict__ nut,
-                                                 double* __restrict__ hx, double* __restrict__ hy,
-                                                 double* __restrict__ hz, double* __restrict__ rx,
-                                                 double* __restrict__ ry, double* __restrict__ rz,
+template <class T>
+__global__ void __launch_bounds__(256) k_rhs_les(Geo<T> g, Metrics<double> m, const T* __restrict__ ux,
+                                                 const T* __restrict__ uy, const T* __restrict__ uz,
+                                                 const T* __restrict__ pr, const T* __restrict__ nut,
+                                                 T* __restrict__ hx, T* __restrict__ hy,
+                                                 T* __restrict__ hz, T* __restrict__ rx,
+                                                 T* __restrict__ ry, T* __restrict__ rz,
                                                  const double* __restrict__ fsgs, const DevScalars* __restrict__ sc) {
   if (sc->status) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -219,8 +224,8 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
     const double gradp1 = (at(pr, n, 0) - at(pr, n, n.xm)) * rdx;
     const double conv = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + g.g1 + f1;
     const double ho = hx[n.c];
-    hx[n.c] = conv;
-    rx[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp1 + 2.0 * pmBetaT * d22q1 + sc->dpmdxns;
+    hx[n.c] = (T)conv;
+    rx[n.c] = (T)(pmGamma * conv + pmTheta * ho - pmAlpha * gradp1 + 2.0 * pmBetaT * d22q1 + sc->dpmdxns);
   }
   {  // RhsY (:214-272)
     const double sucac = m.rdyc[jc], qsucac = 0.25 * sucac;
@@ -246,8 +251,8 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
     const double gradp2 = (at(pr, n, 0) - at_jm(pr, g, 3, n, 0)) * sucac;
     const double conv = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + g.g2 + f2;
     const double ho = hy[n.c];
-    hy[n.c] = conv;
-    ry[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp2 + 2.0 * pmBetaT * sgs2;
+    hy[n.c] = (T)conv;
+    ry[n.c] = (T)(pmGamma * conv + pmTheta * ho - pmAlpha * gradp2 + 2.0 * pmBetaT * sgs2);
   }
   {  // RhsZ (:330-387)
     const double sucaj = 0.25 * m.rdyp[jc];
@@ -274,8 +279,8 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
     const double gradp3 = (at(pr, n, 0) - at(pr, n, n.zm)) * rdz;
     const double conv = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + g.g3 + f3;
     const double ho = hz[n.c];
-    hz[n.c] = conv;
-    rz[n.c] = pmGamma * conv + pmTheta * ho - pmAlpha * gradp3 + 2.0 * pmBetaT * d22q3;
+    hz[n.c] = (T)conv;
+    rz[n.c] = (T)(pmGamma * conv + pmTheta * ho - pmAlpha * gradp3 + 2.0 * pmBetaT * d22q3);
   }
 }
 
@@ -285,7 +290,8 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<double> g, Metrics<double> 
 // substitution overwrites them.  blockIdx.y = component.
 // coefficients (a, b, c) of row j of the variable-viscosity Crank-Nicolson
 // system of component comp in column (i, k)
-__device__ __forceinline__ void uhat_les_coef(const Geo<double>& g, const HelmCoef& hc, const double* __restrict__ nut,
+template <class T>
+__device__ __forceinline__ void uhat_les_coef(const Geo<T>& g, const HelmCoef& hc, const T* __restrict__ nut,
                                               double pmBetaT, int comp, int i, int j, int k, double& a, double& b,
                                               double& c) {
   const Nbr n = make_nbr(g, i, j, k);
@@ -307,20 +313,21 @@ __device__ __forceinline__ void uhat_les_coef(const Geo<double>& g, const HelmCo
   a = -rt1; b = rt1 + rt2 + 1.0; c = -rt2;
 }
 
-__global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, const double* __restrict__ nut,
-                                                  const double* __restrict__ ux, const double* __restrict__ uy,
-                                                  const double* __restrict__ uz, double* __restrict__ rx,
-                                                  double* __restrict__ ry, double* __restrict__ rz,
-                                                  double* __restrict__ uxs, double* __restrict__ uys,
-                                                  double* __restrict__ uzs, const DevScalars* __restrict__ sc) {
+template <class T>
+__global__ void __launch_bounds__(128) k_uhat_les(Geo<T> g, HelmCoef hc, const T* __restrict__ nut,
+                                                  const T* __restrict__ ux, const T* __restrict__ uy,
+                                                  const T* __restrict__ uz, T* __restrict__ rx,
+                                                  T* __restrict__ ry, T* __restrict__ rz,
+                                                  T* __restrict__ uxs, T* __restrict__ uys,
+                                                  T* __restrict__ uzs, const DevScalars* __restrict__ sc) {
   if (sc->status) return;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= g.nx * g.nz) return;
   const int comp = blockIdx.y;
   const int i = col % g.nx, k = col / g.nx;
-  const double* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
-  double* r = comp == 0 ? rx : (comp == 1 ? ry : rz);  // the RHS column is consumed in place
-  double* us = comp == 0 ? uxs : (comp == 1 ? uys : uzs);
+  const T* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
+  T* r = comp == 0 ? rx : (comp == 1 ? ry : rz);  // the RHS column is consumed in place
+  T* us = comp == 0 ? uxs : (comp == 1 ? uys : uzs);
   const double pmBetaT = sc->pmBetaT;
   const int ny = g.ny;
   const long long nxl = g.nx;
@@ -363,12 +370,13 @@ __global__ void __launch_bounds__(128) k_uhat_les(Geo<double> g, HelmCoef hc, co
 // 432 blocks are one wave on 148 SMs (32-column blocks: 1.5 waves, 21 us).
 constexpr int kUhatTileCols = 16;
 constexpr size_t kUhatTileSmemMax = 100 * 1024;  // ny <= 200
-__global__ void __launch_bounds__(128) k_uhat_les_tile(Geo<double> g, HelmCoef hc, const double* __restrict__ nut,
-                                                       const double* __restrict__ ux, const double* __restrict__ uy,
-                                                       const double* __restrict__ uz, double* __restrict__ rx,
-                                                       double* __restrict__ ry, double* __restrict__ rz,
-                                                       double* __restrict__ uxs, double* __restrict__ uys,
-                                                       double* __restrict__ uzs, const DevScalars* __restrict__ sc) {
+template <class T>
+__global__ void __launch_bounds__(128) k_uhat_les_tile(Geo<T> g, HelmCoef hc, const T* __restrict__ nut,
+                                                       const T* __restrict__ ux, const T* __restrict__ uy,
+                                                       const T* __restrict__ uz, T* __restrict__ rx,
+                                                       T* __restrict__ ry, T* __restrict__ rz,
+                                                       T* __restrict__ uxs, T* __restrict__ uys,
+                                                       T* __restrict__ uzs, const DevScalars* __restrict__ sc) {
   extern __shared__ double tl[];
   if (sc->status) return;  // uniform over the block
   const int ny = g.ny, ncol = g.nx * g.nz;
@@ -381,9 +389,9 @@ __global__ void __launch_bounds__(128) k_uhat_les_tile(Geo<double> g, HelmCoef h
   const bool valid = col < ncol;
   const int comp = blockIdx.y;
   const int i = valid ? col % g.nx : 0, k = valid ? col / g.nx : 0;
-  const double* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
-  double* r = comp == 0 ? rx : (comp == 1 ? ry : rz);
-  double* us = comp == 0 ? uxs : (comp == 1 ? uys : uzs);
+  const T* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
+  T* r = comp == 0 ? rx : (comp == 1 ? ry : rz);
+  T* us = comp == 0 ? uxs : (comp == 1 ? uys : uzs);
   const double pmBetaT = sc->pmBetaT;
   const long long nxl = g.nx;
   const long long base = i + nxl * ny * k;
@@ -455,8 +463,9 @@ struct MlpNormD {
 };
 
 // cell-centre gradients (the WALE stencils, m_LESModels.f90:98-111)
-__device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metrics<double>& m, const double* ux,
-                                               const double* uy, const double* uz, const Nbr& n, int jc,
+template <class T>
+__device__ __forceinline__ void cell_gradients(const Geo<T>& g, const Metrics<double>& m, const T* ux,
+                                               const T* uy, const T* uz, const Nbr& n, int jc,
                                                double* G /* 9: dudx dudy dudz dvdx dvdy dvdz dwdx dwdy dwdz */) {
   const double rdx = g.rdx, rdz = g.rdz;
   const double caj = m.rdyp[jc], cac1 = m.rdyc[jc], cac2 = m.rdyc[jc + 1], cac12 = cac1 - cac2;
@@ -482,9 +491,10 @@ __device__ __forceinline__ void cell_gradients(const Geo<double>& g, const Metri
 // and scaled by u_tau^2, or the fallback where an input left the training
 // range.  When a wait on the tensor cores expires the kernel records it in
 // *mstatus and writes the fallback stresses.
+template <class T>
 __global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
-    k_sgs_mlp(Geo<double> g, Metrics<double> m, LesPar lp, MlpNormD nm, const double* __restrict__ ux,
-              const double* __restrict__ uy, const double* __restrict__ uz, const unsigned char* __restrict__ img,
+    k_sgs_mlp(Geo<T> g, Metrics<double> m, LesPar lp, MlpNormD nm, const T* __restrict__ ux,
+              const T* __restrict__ uy, const T* __restrict__ uz, const unsigned char* __restrict__ img,
               double* __restrict__ tau, int* __restrict__ mstatus, const DevScalars* __restrict__ sc) {
   using namespace ch3d_mlp;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -545,7 +555,8 @@ __global__ void __launch_bounds__(ch3d_mlp::TILE, 6)
 // f_i = -d tau_ij / dx_j at the staggered points of u_i.  Off-diagonal
 // stresses are averaged from the four surrounding cell centres onto the cell
 // edges; they vanish on the walls.
-__global__ void __launch_bounds__(256) k_sgs_force(Geo<double> g, Metrics<double> m, const double* __restrict__ tau,
+template <class T>
+__global__ void __launch_bounds__(256) k_sgs_force(Geo<T> g, Metrics<double> m, const double* __restrict__ tau,
                                                    double* __restrict__ fx, double* __restrict__ fy,
                                                    double* __restrict__ fz, const DevScalars* __restrict__ sc) {
   if (sc->status) return;
@@ -659,19 +670,19 @@ static LesPar les_par(const ch3d_ctx* c) {
 
 static dim3 les_grid(const ch3d_ctx* c) { return dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz); }
 
-cudaError_t launch_sgs_nut(ch3d_ctx* c) {
-  double** f = (double**)c->f;
-  const Geo<double> g = make_geo<double>(c);
+template <class T> static cudaError_t sgs_nut_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  const Geo<T> g = make_geo<T>(c);
   const LesPar lp = les_par(c);
   if (lp.model == CH3D_LES_SMAG_VD || lp.model == CH3D_LES_MLP) {
     const double d1 = c->yc[1] - c->yp[1], dN = c->yp[c->ny + 1] - c->yc[c->ny];
-    k_wall_utau<<<1, 1024, 0, c->stream>>>(g, f[0], d1, dN, c->sc);
+    k_wall_utau<T><<<1, 1024, 0, c->stream>>>(g, f[0], d1, dN, c->sc);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   // the learned closure keeps nut = xnu (filled when the context was created)
   if (lp.model != CH3D_LES_MLP) {
-    k_sgs_nut<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, f[0], f[1], f[2], f[11], c->sc);
+    k_sgs_nut<T><<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, lp, f[0], f[1], f[2], f[11], c->sc);
     return cudaGetLastError();
   }
   MlpNorm nh;
@@ -686,22 +697,23 @@ cudaError_t launch_sgs_nut(ch3d_ctx* c) {
   }
   for (int q = 0; q < 6; ++q) { nm.out_mean[q] = nh.out_mean[q]; nm.out_std[q] = nh.out_std[q]; }
   if (c->N >= (1LL << 31)) return cudaErrorInvalidValue;  // 32-bit cell indices in k_sgs_mlp
-  static PerDevice attr;
+  static PerDevice attr;  // per precision (template instance)
   cudaError_t e = once_per_device(attr, c->device, [] {
     cudaError_t r =
-        cudaFuncSetAttribute(k_sgs_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ch3d_mlp::FwdSmem::BYTES);
+        cudaFuncSetAttribute(k_sgs_mlp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ch3d_mlp::FwdSmem::BYTES);
     if (r == cudaSuccess)  // all of the SM's on-chip memory as shared memory: six CTAs per SM
-      r = cudaFuncSetAttribute(k_sgs_mlp, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      r = cudaFuncSetAttribute(k_sgs_mlp<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     return r;
   });
   if (e != cudaSuccess) return e;
-  k_sgs_mlp<<<(unsigned)((c->N + ch3d_mlp::TILE - 1) / ch3d_mlp::TILE), ch3d_mlp::TILE, ch3d_mlp::FwdSmem::BYTES,
-              c->stream>>>(g, c->m64, lp, nm, f[0], f[1], f[2], c->mlp_packed, c->sgs_tau, c->mlp_status, c->sc);
+  k_sgs_mlp<T><<<(unsigned)((c->N + ch3d_mlp::TILE - 1) / ch3d_mlp::TILE), ch3d_mlp::TILE, ch3d_mlp::FwdSmem::BYTES,
+                 c->stream>>>(g, c->m64, lp, nm, f[0], f[1], f[2], c->mlp_packed, c->sgs_tau, c->mlp_status, c->sc);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_sgs_force<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, c->sgs_tau, c->sgs_f, c->sgs_f + c->N,
-                                                          c->sgs_f + 2 * c->N, c->sc);
+  k_sgs_force<T><<<les_grid(c), dim3(32, 8), 0, c->stream>>>(g, c->m64, c->sgs_tau, c->sgs_f, c->sgs_f + c->N,
+                                                             c->sgs_f + 2 * c->N, c->sc);
   return cudaGetLastError();
 }
+cudaError_t launch_sgs_nut(ch3d_ctx* c) { return c->fp32 ? sgs_nut_t<float>(c) : sgs_nut_t<double>(c); }
 
 // the network's parameter image (BF16 operands and FP32 biases as the
 // forward pass holds them in shared memory), once per parameter set
@@ -715,13 +727,15 @@ cudaError_t launch_mlp_pack(ch3d_ctx* c) {
 }
 
 // nut = xnu everywhere (the learned closure's total viscosity)
-__global__ void k_fill_nut(double* __restrict__ nut, long long N, double xnu) {
+template <class T> __global__ void k_fill_nut(T* __restrict__ nut, long long N, double xnu) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < N) nut[q] = xnu;
+  if (q < N) nut[q] = (T)xnu;
 }
 
 cudaError_t launch_fill_nut(ch3d_ctx* c) {
-  k_fill_nut<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>((double*)c->f[11], c->N, (double)c->cfg.xnu);
+  const unsigned grid = (unsigned)((c->N + 255) / 256);
+  if (c->fp32) k_fill_nut<float><<<grid, 256, 0, c->stream>>>((float*)c->f[11], c->N, c->cfg.xnu);
+  else k_fill_nut<double><<<grid, 256, 0, c->stream>>>((double*)c->f[11], c->N, c->cfg.xnu);
   return cudaGetLastError();
 }
 
@@ -739,16 +753,17 @@ cudaError_t launch_sgs_samples(ch3d_ctx* c, int fx, int fy, int fz, float* X, fl
   return cudaGetLastError();
 }
 
-cudaError_t launch_rhs_les(ch3d_ctx* c) {
-  double** f = (double**)c->f;
-  k_rhs_les<<<les_grid(c), dim3(32, 8), 0, c->stream>>>(make_geo<double>(c), c->m64, f[0], f[1], f[2], f[3], f[11],
-                                                         f[4], f[5], f[6], f[7], f[8], f[9],
-                                                         c->cfg.LES_type == CH3D_LES_MLP ? c->sgs_f : nullptr, c->sc);
+template <class T> static cudaError_t rhs_les_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  k_rhs_les<T><<<les_grid(c), dim3(32, 8), 0, c->stream>>>(make_geo<T>(c), c->m64, f[0], f[1], f[2], f[3], f[11], f[4],
+                                                            f[5], f[6], f[7], f[8], f[9],
+                                                            c->cfg.LES_type == CH3D_LES_MLP ? c->sgs_f : nullptr, c->sc);
   return cudaGetLastError();
 }
+cudaError_t launch_rhs_les(ch3d_ctx* c) { return c->fp32 ? rhs_les_t<float>(c) : rhs_les_t<double>(c); }
 
-cudaError_t launch_uhat_les(ch3d_ctx* c) {
-  double** f = (double**)c->f;
+template <class T> static cudaError_t uhat_les_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
   HelmCoef hc;
   const double* M = c->met64;
   const int L = c->ny + 3;
@@ -758,18 +773,19 @@ cudaError_t launch_uhat_les(ch3d_ctx* c) {
   // the tiled kernel while its shared memory (4 x 16 x ny doubles) fits
   const size_t tsm = (size_t)4 * kUhatTileCols * c->ny * sizeof(double);
   if (tsm <= kUhatTileSmemMax) {
-    static PerDevice attr;
+    static PerDevice attr;  // per precision (template instance)
     cudaError_t e = once_per_device(attr, c->device, [] {
-      return cudaFuncSetAttribute(k_uhat_les_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUhatTileSmemMax);
+      return cudaFuncSetAttribute(k_uhat_les_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUhatTileSmemMax);
     });
     if (e != cudaSuccess) return e;
-    k_uhat_les_tile<<<dim3((ncol + kUhatTileCols - 1) / kUhatTileCols, 3), 128, tsm, c->stream>>>(
-        make_geo<double>(c), hc, f[11], f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13], f[14], c->sc);
+    k_uhat_les_tile<T><<<dim3((ncol + kUhatTileCols - 1) / kUhatTileCols, 3), 128, tsm, c->stream>>>(
+        make_geo<T>(c), hc, f[11], f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13], f[14], c->sc);
     return cudaGetLastError();
   }
-  k_uhat_les<<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(make_geo<double>(c), hc, f[11], f[0], f[1], f[2], f[7],
-                                                                 f[8], f[9], f[12], f[13], f[14], c->sc);
+  k_uhat_les<T><<<dim3((ncol + 127) / 128, 3), 128, 0, c->stream>>>(make_geo<T>(c), hc, f[11], f[0], f[1], f[2], f[7],
+                                                                    f[8], f[9], f[12], f[13], f[14], c->sc);
   return cudaGetLastError();
 }
+cudaError_t launch_uhat_les(ch3d_ctx* c) { return c->fp32 ? uhat_les_t<float>(c) : uhat_les_t<double>(c); }
 
 }  // namespace ch3d

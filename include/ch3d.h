@@ -55,7 +55,10 @@ extern "C" {
 
 #define CH3D_PREC_FP64 0
 #define CH3D_PREC_MIXED 1       /* FP32 fields, FP64 low-mode Poisson, bulk
-                                   constraint and statistics */
+                                   constraint and statistics; LES: the eddy
+                                   viscosity, the closure's inputs and the
+                                   variable-viscosity solves in FP64
+                                   arithmetic on the FP32 fields */
 
 /* LES closures; the reference's LES_type values (src/CFD_2nd/m_Parameters.f90:256-259)
    plus the closures added on top (no counterpart in the reference). */

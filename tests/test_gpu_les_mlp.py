@@ -129,3 +129,28 @@ def test_training_samples_match_numpy_box_filter(built):
                            (dw * ut / cfg.xnu).reshape(-1, 1)], axis=1)
     assert rel_max(X, Xref) < 1e-5, rel_max(X, Xref)
     assert rel_max(T, Tref) < 1e-4, rel_max(T, Tref)
+
+
+def test_learned_closure_mixed_precision(built):
+    """The learned closure in the mixed path: its stresses from the FP32 fields
+    within 1e-3 (L2) of those of the FP64 path on the same state, and 20 steps
+    stay finite and divergence-free to FP32 round-off."""
+    import sgs_numpy as SN
+    from channel3d_b200 import ChannelSolver
+    from oracle import mlp_oracle as M
+    cfg = _cfg()
+    o, s, yp, ux = _pair(cfg)
+    X = SN.features(SN.gradients(o, cfg, yp), cfg, yp, SN.utau(ux, cfg, yp))
+    P, norm = M.init_params(3) * 0.5, _norm(-8, 8, X.mean(axis=0), X.std(axis=0) + 1e-3)
+    s.sgs_mlp_set(P, norm)
+    s.sgs_viscosity()
+    t64 = _tau(s)
+    st = s.download()
+    m = ChannelSolver(cfg.copy(precision="mixed"), yp=yp)
+    m.upload(st["ux"], st["uy"], st["uz"], st["p"])
+    m.sgs_mlp_set(P, norm)
+    m.sgs_viscosity()
+    assert rel_l2(_tau(m), t64) < 1e-3, rel_l2(_tau(m), t64)
+    info = m.step(20)
+    assert info["status"] == 0 and info["divmax2"] < 1e-4
+    m.close()

@@ -98,13 +98,24 @@ template <class T> struct C4 {
 // 4th-order divergence at one cell: clcPrSrc (src/CFD_4th/m_TScheme.f90:114-143)
 // and CheckDivergence (src/CFD_4th/m_Tools.f90:54-81).
 template <class T>
-__device__ __forceinline__ T div4_cell(const Geo<T>& g, const C4<T>& c, T rdyp, const T* __restrict__ ux,
-                                       const T* __restrict__ uy, const T* __restrict__ uz, int i, int j, int k) {
-  const Nbr n = make_nbr(g, i, j, k);
+__device__ __forceinline__ T div4_at(const Geo<T>& g, const C4<T>& c, T rdyp, const T* __restrict__ ux,
+                                     const T* __restrict__ uy, const T* __restrict__ uz, const Nbr& n) {
   const T dudx = c.dx1 * at(ux, n, n.xm) + c.dx2 * at(ux, n, 0) + c.dx3 * at(ux, n, n.xp) + c.dx4 * at(ux, n, n.xp2);
   const T dvdy = (at_jp(uy, g, 1, n, 0) - at(uy, n, 0)) * rdyp;
   const T dwdz = c.dz1 * at(uz, n, n.zm) + c.dz2 * at(uz, n, 0) + c.dz3 * at(uz, n, n.zp) + c.dz4 * at(uz, n, n.zp2);
   return dudx + dvdy + dwdz;
+}
+template <class T>
+__device__ __forceinline__ T div4_cell(const Geo<T>& g, const C4<T>& c, T rdyp, const T* __restrict__ ux,
+                                       const T* __restrict__ uy, const T* __restrict__ uz, int i, int j, int k) {
+  return div4_at(g, c, rdyp, ux, uy, uz, make_nbr(g, i, j, k));
+}
+// move a neighbourhood one row up the same column (the x and z offsets do not
+// depend on j)
+template <class T> __device__ __forceinline__ void nbr_next_row(Nbr& n, const Geo<T>& g, int j) {
+  n.c += g.nx;
+  n.jlo = (j == 0);
+  n.jhi = (j == g.ny - 1);
 }
 
 // ---------------------------------------------------------------------------

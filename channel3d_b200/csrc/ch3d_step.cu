@@ -1048,8 +1048,11 @@ __global__ void __launch_bounds__(128) k_diag(Geo<T> g, Metrics<T> m, const T* _
     const long long dzp = k + 1 == nz ? -(long long)(nz - 1) * plane : plane;
     const double rdx = g.rdx, rdz = g.rdz;
     double b = uy[col + (long long)j0 * nx];
+    const C4<T> c4(g);
+    Nbr n4 = make_nbr(g, i, j0, k);  // the 4th-order divergence's neighbourhood, moved up row by row
 #pragma unroll 4
     for (int j = j0; j < j1; ++j) {
+      if (j > j0) nbr_next_row(n4, g, j);
       const long long idx = col + (long long)j * nx;
       const int jc = j + 1;
       const double a = ux[idx], c = uz[idx];
@@ -1057,7 +1060,7 @@ __global__ void __launch_bounds__(128) k_diag(Geo<T> g, Metrics<T> m, const T* _
       const double bjp = j + 1 < ny ? (double)uy[idx + nx] : (double)(T)g.bc.uy_hi;
       const double rdyp = m.rdyp[jc];
       double d = fabs((aip - a) * rdx + (bjp - b) * rdyp + (ckp - c) * rdz);
-      if (g.order == 4) d = fabs((double)div4_cell(g, C4<T>(g), m.rdyp[jc], ux, uy, uz, i, j, k));
+      if (g.order == 4) d = fabs((double)div4_at(g, c4, m.rdyp[jc], ux, uy, uz, n4));
       // fmax(NaN, x) = x on the device, so NaN is folded into +inf first: a NaN
       // field still trips the limit checks of the step
       if (!(d == d)) d = INFINITY;

@@ -160,9 +160,10 @@ __global__ void __launch_bounds__(128) k_visc4_partial(Geo<T> g, Metrics<T> m, c
   double s = 0.0;
   if (i < g.nx && k < g.nz) {
     const C4<T> c(g);
+    Nbr n = make_nbr(g, i, j0, k);
 #pragma unroll 4
     for (int j = j0; j < j1; ++j) {
-      const Nbr n = make_nbr(g, i, j, k);
+      if (j > j0) nbr_next_row(n, g, j);
       const int jc = j + 1;
       const T ux_c = at(ux, n, 0);
       const T d11 = c.dxx1 * at(ux, n, n.xm2) + c.dxx2 * at(ux, n, n.xm) + c.dxx3 * ux_c + c.dxx4 * at(ux, n, n.xp) +

@@ -31,7 +31,7 @@ def test_short_a_posteriori_run(built):
     filter (the cells of the 48^3 LES grid, whose tanh mesh the DNS mesh
     nests), training, and 48^3 LES runs with the learned closure and with the
     Smagorinsky / van Driest model from the DNS field resampled onto the LES
-    grid, both judged against the box-filtered DNS profiles.  Asserted: the
+    grid, both compared with the box-filtered DNS profiles.  Asserted: the
     network beats Smagorinsky a priori on held-out snapshots, both LES runs
     stay finite and keep the mean profile within 10% of the filtered DNS, and
     the learned closure's cost per step is reported."""

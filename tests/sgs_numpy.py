@@ -1,5 +1,5 @@
 """Numpy restatement of the learned closure's per-point quantities (test
-checker for channel3d_b200/csrc/ch3d_les.cu k_sgs_features and
+checker for channel3d_b200/csrc/ch3d_les.cu k_sgs_mlp (its inputs) and
 k_sgs_train_samples): cell-centre velocity gradients with the WALE stencils
 of src/CFD_2nd/m_LESModels.f90:98-111, the Smagorinsky / van Driest
 fallback stress, y+ and the box-filtered training samples."""

@@ -304,7 +304,7 @@ __device__ __forceinline__ void fwd_prologue_packed(unsigned char* smem, const u
                  "r"((uint32_t)kPackedBytes)
                  : "memory");
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+        "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
             su32(smem + FwdSmem::W1)),
         "l"(img), "r"((uint32_t)kPackedBytes), "r"(su32(&S->wbar))
         : "memory");

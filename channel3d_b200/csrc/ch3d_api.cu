@@ -214,13 +214,20 @@ int check_config(const ch3d_config* g) {
   if (g->nxc < 4 || g->nyc < 4 || g->nzc < 2) return fail(CH3D_ERR_INVALID, "grid too small: %d %d %d", g->nxc, g->nyc, g->nzc);
   if (g->nxc % 2) return fail(CH3D_ERR_INVALID, "nxc must be even (real-to-complex x transform)");
   if (g->ischeme != 3) return fail(CH3D_ERR_UNSUPPORTED, "only RK3 (ischeme=3) is built");
-  if (g->IsImplicit != 1 && !(g->order == 2 && g->IsImplicit == 2))
-    return fail(CH3D_ERR_UNSUPPORTED, "IsImplicit=%d not built (PIMP=1, and FIMP=2 for order 2, are)", g->IsImplicit);
+  if (g->IsImplicit != 1 && !(g->order == 2 && (g->IsImplicit == 2 || g->IsImplicit == 0)))
+    return fail(CH3D_ERR_UNSUPPORTED, "IsImplicit=%d not built (PIMP=1; FIMP=2 and FEXP=0 for order 2)", g->IsImplicit);
+  if (g->IsImplicit == 0 && g->precision != CH3D_PREC_FP64)
+    return fail(CH3D_ERR_UNSUPPORTED, "the explicit scheme (IsImplicit=0) is built in FP64");
   if (g->BcOption[0] != 0 || g->BcOption[1] != 0 || g->BcOption[4] != 0 || g->BcOption[5] != 0)
     return fail(CH3D_ERR_UNSUPPORTED, "x and z must be periodic (BcOption 1,2,5,6 = 0)");
+  if ((g->BcOption[2] == 0) != (g->BcOption[3] == 0)) return fail(CH3D_ERR_INVALID, "Periodic Bc Wrong");
   for (int s = 2; s < 4; ++s)
-    if (g->BcOption[s] != -1 && g->BcOption[s] != -2)
-      return fail(CH3D_ERR_UNSUPPORTED, "y boundaries must be no-slip (-1) or free-slip (-2)");
+    if (g->BcOption[s] != -1 && g->BcOption[s] != -2 && g->BcOption[s] != 0)
+      return fail(CH3D_ERR_UNSUPPORTED, "y boundaries must be no-slip (-1), free-slip (-2) or periodic (0)");
+  // periodic y: the triply periodic steps (clcU*Hat_FIMP_000, clcU*Hat_PIMP_0 or FEXP, clcPPE_z1_periodic)
+  if (g->BcOption[2] == 0 && (g->order != 2 || g->LES_type != 0 || g->precision != CH3D_PREC_FP64))
+    return fail(CH3D_ERR_UNSUPPORTED, "periodic y is built for the 2nd-order step (IsImplicit 0, 1 or 2), FP64, "
+                "without LES");
   if (g->LES_type != 0) {
     if (g->LES_type != CH3D_LES_WALE && g->LES_type != CH3D_LES_MTS && g->LES_type != CH3D_LES_SMAG_VD &&
         g->LES_type != CH3D_LES_MLP)
@@ -268,8 +275,8 @@ int alloc_fields(ch3d_ctx* c) {
     CU(launch_fill_nut(c));  // the closure's total viscosity stays xnu
     c->bytes += (long long)c->N * 9 * 8;
   }
-  if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
-    const size_t nb = ptri_factor_doubles(c->nx, c->nz) * sizeof(double);
+  if ((c->cfg.order == 2 && c->cfg.IsImplicit == 2) || y_periodic(c)) {
+    const size_t nb = ptri_factor_doubles(c->nx, c->ny, c->nz) * sizeof(double);
     CU(cudaMalloc(&c->pfac, nb));
     CU(cudaMemsetAsync(c->pfac, 0, nb, c->stream));
     c->bytes += (long long)nb;
@@ -323,7 +330,8 @@ double host_get(const ch3d_ctx* c, int layout, const double* a, int i, int j, in
 // the velocity, two below and one above for the pressure.  Cells those routines
 // never write (x = nxc+2 and z = nzc+2 of the 2nd-order arrays, the y plane
 // nyc+2 of ux, uz, p, uy(:,0,:) of the 4th-order tree) keep the host's values.
-// Periodic x and z.  comp: 0 ux, 1 uy, 2 uz, 3 p.
+// Periodic x and z; y periodic (BcOption(3:4) = 0) copies the halo rows
+// j = 0 and nyp first.  comp: 0 ux, 1 uy, 2 uz, 3 p.
 void host_fill_ghosts(const ch3d_ctx* c, int layout, double* a, int comp) {
   const int nxc = c->nx, nyc = c->ny, nzc = c->nz, nyp = nyc + 1;
   const ch3d_config& g = c->cfg;
@@ -331,6 +339,11 @@ void host_fill_ghosts(const ch3d_ctx* c, int layout, double* a, int comp) {
   auto at = [&](int i, int j, int k) -> double& { return g2 ? a[gidx2(c, i, j, k)] : a[gidx4(c, i, j, k)]; };
   for (int k = 1; k <= nzc; ++k)
     for (int i = 1; i <= nxc; ++i) {
+      if (y_periodic(c)) {  // y halo rows (one each side, Init_Halo, m_BC_and_Halo.f90:25-29)
+        at(i, 0, k) = at(i, nyc, k);
+        at(i, nyp, k) = at(i, 1, k);
+        continue;
+      }
       if (comp == 3) { at(i, nyp, k) = at(i, nyc, k); at(i, 0, k) = at(i, 1, k); continue; }
       if (comp == 1) {
         at(i, nyp, k) = g.uyBcValue[3];
@@ -369,7 +382,7 @@ int upload_field(ch3d_ctx* c, int q, int layout, const double* a, int comp) {
     // FP64 interior arrays are the device layout: one copy (DMA from pinned memory), then the uy wall row
     if (a) CU(cudaMemcpyAsync(c->f[q], a, (size_t)c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     else CU(cudaMemsetAsync(c->f[q], 0, (size_t)c->N * sizeof(double), c->stream));
-    if (comp == 1) CU(launch_fill_row0(c, q, c->cfg.uyBcValue[2]));  // uy(ic,1,kc) = uy_ym
+    if (comp == 1 && !y_periodic(c)) CU(launch_fill_row0(c, q, c->cfg.uyBcValue[2]));  // uy(ic,1,kc) = uy_ym
     CU(cudaStreamSynchronize(c->stream));
     return CH3D_OK;
   }
@@ -386,7 +399,7 @@ int upload_field(ch3d_ctx* c, int q, int layout, const double* a, int comp) {
         CU(launch_convert(c, c->spec, (T*)c->f[q] + off, n, 1));
       }
     }
-    if (comp == 1) CU(launch_fill_row0(c, q, c->cfg.uyBcValue[2]));  // uy(ic,1,kc) = uy_ym
+    if (comp == 1 && !y_periodic(c)) CU(launch_fill_row0(c, q, c->cfg.uyBcValue[2]));  // uy(ic,1,kc) = uy_ym
     CU(cudaStreamSynchronize(c->stream));
     return CH3D_OK;
   }
@@ -396,7 +409,7 @@ int upload_field(ch3d_ctx* c, int q, int layout, const double* a, int comp) {
     for (int j = 1; j <= c->ny; ++j)
       for (int i = 1; i <= c->nx; ++i, ++n) {
         double v = a ? host_get(c, layout, a, i, j, k) : 0.0;
-        if (comp == 1 && j == 1) v = c->cfg.uyBcValue[2];  // uy(ic,1,kc) = uy_ym
+        if (comp == 1 && j == 1 && !y_periodic(c)) v = c->cfg.uyBcValue[2];  // uy(ic,1,kc) = uy_ym
         h[n] = (T)v;
       }
   CU(cudaMemcpyAsync(c->f[q], h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
@@ -450,7 +463,7 @@ int init_scalars(ch3d_ctx* c) {
 // The 2nd-order partially implicit step without LES runs its right-hand
 // sides and y solves as one column-march kernel (ch3d_march.cu).
 static bool march_path(const ch3d_ctx* c) {
-  return c->cfg.LES_type == 0 && c->cfg.order == 2 && c->cfg.IsImplicit != 2;
+  return c->cfg.LES_type == 0 && c->cfg.order == 2 && c->cfg.IsImplicit == 1 && !y_periodic(c);
 }
 
 int record_step(ch3d_ctx* c) {
@@ -466,10 +479,16 @@ int record_step(ch3d_ctx* c) {
       CU(launch_rhs_les(c));
       CU(launch_uhat_les(c));
     } else if (fimp) {
-      CU(launch_helm_factors(c));
+      if (!y_periodic(c)) CU(launch_helm_factors(c));
       CU(launch_rhs_fimp(c));
       CU(launch_ptri_xz(c));
-      CU(launch_uhat(c));
+      CU(y_periodic(c) ? launch_ptri_y(c) : launch_uhat(c));  // FIMP_000 or FIMP_010
+    } else if (c->cfg.IsImplicit == 0) {  // FEXP: explicit right-hand sides, u* = u + Rhs
+      CU(launch_rhs_fimp(c));
+      CU(launch_uhat_fexp(c));
+    } else if (y_periodic(c)) {  // PIMP_0: the periodic y sweep alone
+      CU(launch_rhs(c));
+      CU(launch_ptri_y(c));
     } else {
       CU(launch_rhs_march(c));  // 4th order: the same column march with the 4th-order stencils
     }
@@ -657,6 +676,11 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
           cudaMalloc(&c->ylow, ls * sizeof(double)) != cudaSuccess)
         return cleanup(fail(CH3D_ERR_NOMEM, "Poisson low-mode factors"));
     }
+    if (y_periodic(c)) {
+      if (cudaMalloc(&c->yA2, nrow * sizeof(double)) != cudaSuccess)
+        return cleanup(fail(CH3D_ERR_NOMEM, "Poisson factors"));
+      c->bytes += (long long)nrow * sizeof(double);
+    }
     e = launch_ysolve_factors(c);
     if (e != cudaSuccess) return cleanup(fail(CH3D_ERR_CUDA, "Poisson factors: %s", cudaGetErrorString(e)));
   }
@@ -706,7 +730,7 @@ int ch3d_destroy(ch3d_ctx* c) {
   void* mbufs[] = {c->mlp_params, c->mlp_packed, c->mlp_status, c->sgs_tau, c->sgs_f, c->spec2,
                    c->specacc};
   for (void* b : mbufs) if (b) cudaFree(b);
-  void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
+  void* bufs[] = {c->hfac, c->mtab, c->yRM, c->yCP, c->ylow, c->yA2, c->yRM64, c->yCP64, c->spec, c->met, c->met64, c->wave, c->twx, c->twr, c->twz, c->sc, c->part, c->part2,
                   c->red1, c->red2, c->stat, c->statpart};
   for (void* b : bufs) if (b) cudaFree(b);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -821,11 +845,13 @@ int ch3d_stage(ch3d_ctx* c, int stage, int ns) {
       break;
     case 1:
       if (c->cfg.LES_type > 0) CU(launch_rhs_les(c));
-      else CU(c->cfg.order == 4 ? launch_rhs4(c) : (c->cfg.IsImplicit == 2 ? launch_rhs_fimp(c) : launch_rhs(c)));
+      else CU(c->cfg.order == 4 ? launch_rhs4(c) : (c->cfg.IsImplicit != 1 ? launch_rhs_fimp(c) : launch_rhs(c)));
       break;
     case 2:
       if (c->cfg.LES_type > 0) { CU(launch_uhat_les(c)); break; }
+      if (c->cfg.IsImplicit == 0) { CU(launch_uhat_fexp(c)); break; }
       if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) CU(launch_ptri_xz(c));
+      if (y_periodic(c)) { CU(launch_ptri_y(c)); break; }
       CU(launch_helm_factors(c));
       CU(launch_uhat(c));
       break;
@@ -1110,7 +1136,8 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
       CU(mark(6));
       if (c->cfg.order == 4) CU(launch_visc4_partials(c));
       CU(launch_substep_setup(c, ns));
-      if (!march_path(c) && c->cfg.order != 4 && c->cfg.LES_type == 0) CU(launch_helm_factors(c));
+      if (!march_path(c) && c->cfg.order != 4 && c->cfg.LES_type == 0 && !y_periodic(c) && c->cfg.IsImplicit != 0)
+        CU(launch_helm_factors(c));
       CU(done());
       if (march_path(c)) {
         CU(mark(0)); CU(launch_rhs_march(c)); CU(done());
@@ -1120,7 +1147,13 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
         CU(mark(1)); CU(launch_uhat_les(c)); CU(done());
       } else if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
         CU(mark(0)); CU(launch_rhs_fimp(c)); CU(done());
-        CU(mark(1)); CU(launch_ptri_xz(c)); CU(launch_uhat(c)); CU(done());
+        CU(mark(1)); CU(launch_ptri_xz(c)); CU(y_periodic(c) ? launch_ptri_y(c) : launch_uhat(c)); CU(done());
+      } else if (c->cfg.IsImplicit == 0) {
+        CU(mark(0)); CU(launch_rhs_fimp(c)); CU(done());
+        CU(mark(1)); CU(launch_uhat_fexp(c)); CU(done());
+      } else if (y_periodic(c)) {
+        CU(mark(0)); CU(launch_rhs(c)); CU(done());
+        CU(mark(1)); CU(launch_ptri_y(c)); CU(done());
       } else {
         CU(mark(0)); CU(launch_rhs_march(c)); CU(done());
         CU(mark(1)); CU(done());
@@ -1187,6 +1220,8 @@ int ch3d_interp_state(ch3d_ctx* dst, const ch3d_ctx* src) {
   if (!dst || !src || dst == src) return fail(CH3D_ERR_INVALID, "need two distinct contexts");
   if (dst->device != src->device) return fail(CH3D_ERR_INVALID, "both contexts must be on one device");
   if (dst->fp32 != src->fp32) return fail(CH3D_ERR_INVALID, "both contexts must have the same precision");
+  if (y_periodic(dst) || y_periodic(src))
+    return fail(CH3D_ERR_UNSUPPORTED, "the resampling is built for walls in y (periodic x and z)");
   if (std::fabs(dst->cfg.yly - src->cfg.yly) > 1e-12 * std::fabs(src->cfg.yly))
     return fail(CH3D_ERR_INVALID, "yly differs (%g, %g): the resampling keeps the channel height", src->cfg.yly,
                 dst->cfg.yly);

@@ -107,7 +107,7 @@ template <class T> struct Metrics {
 
 // Boundary description for y (x and z are periodic).
 struct YBc {
-  int lo, hi;                     // BcOption(3), BcOption(4): -1 no-slip, -2 free-slip
+  int lo, hi;                     // BcOption(3), BcOption(4): -1 no-slip, -2 free-slip, 0 periodic
   double ux_lo, ux_hi, uz_lo, uz_hi, uy_lo, uy_hi;
   double dyp1, dypN;              // dyp(1), dyp(nyp)
 };
@@ -128,13 +128,15 @@ __device__ __forceinline__ int wrapm(int i, int n) { return i == 0 ? n - 1 : i -
 __device__ __forceinline__ int wrapp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
 
 // Field value with y ghost cells from the boundary rules
-// (SetBC_and_UpdateHalo, src/CFD_2nd/m_BC_and_Halo.f90:241-282).
+// (SetBC_and_UpdateHalo, src/CFD_2nd/m_BC_and_Halo.f90:241-282), or the
+// periodic halo rows when y is periodic (BcOption(3:4) = 0).
 // comp: 0 ux, 1 uy, 2 uz, 3 pressure.  j may be -1 .. ny.
 template <class T>
 __device__ __forceinline__ T fld(const T* __restrict__ a, const Geo<T>& g, int comp, int i, int j, int k) {
   const int nx = g.nx, ny = g.ny;
   if (j >= 0 && j < ny) return __ldg(a + i + (long long)nx * (j + (long long)ny * k));
   if (j < 0) {
+    if (g.bc.lo == 0) return __ldg(a + i + (long long)nx * ((ny - 1) + (long long)ny * k));
     if (comp == 1) {  // uy(ic,0,kc) = uy_ym*2 - uy(ic,2,kc); never set (zero) in the 4th-order solver
       if (g.order == 4) return (T)0;
       return (T)(g.bc.uy_lo * 2.0) - __ldg(a + i + (long long)nx * (1 + (long long)ny * k));
@@ -146,6 +148,7 @@ __device__ __forceinline__ T fld(const T* __restrict__ a, const Geo<T>& g, int c
     return v - (T)(w * g.bc.dyp1);
   }
   // j == ny  (reference index nyp)
+  if (g.bc.hi == 0) return __ldg(a + i + (long long)nx * ((long long)ny * k));
   if (comp == 1) return (T)g.bc.uy_hi;  // uy(ic,nyp,kc) = uyBcValue(yp)
   T v = __ldg(a + i + (long long)nx * ((ny - 1) + (long long)ny * k));
   if (comp == 3) return v;

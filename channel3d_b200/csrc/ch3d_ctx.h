@@ -39,7 +39,7 @@ struct ch3d_ctx {
   void* ih[6] = {nullptr};   // 4th order: uxhx uyhx uzhx uxhz uyhz uzhz (precision T)
   double* hfac = nullptr;    // Helmholtz chunk/interface factors of the current substep
   void* mtab = nullptr;      // column-march row table of the current substep (precision T)
-  double* pfac = nullptr;    // FIMP: periodic x/z sweep factors of the current substep
+  double* pfac = nullptr;    // FIMP or periodic y: periodic x/z/y sweep factors of the current substep
   double* les_delta = nullptr;  // LES: DeltaCell (ny+2) | wall distance of the cell centres (ny+2)
   // learned closure (LES_type CH3D_LES_MLP)
   float* mlp_params = nullptr;   // CH3D_MLP_NPARAM FP32
@@ -54,6 +54,7 @@ struct ch3d_ctx {
   double* yRM64 = nullptr;   // mixed path: FP64 factors of the low modes (kx < TSy, |kz| <= KL)
   double* yCP64 = nullptr;
   double* ylow = nullptr;    // mixed path: FP64 forward-sweep scratch of the low modes
+  double* yA2 = nullptr;     // periodic y: the Poisson cyclic solve's closure vector per mode
   bool gsub = false;         // the march stops at g; divergence and projection substitute u*
   int KL = 8;
   int TSy = 8;               // kx extent of the FP64 low modes
@@ -93,6 +94,9 @@ struct ch3d_ctx {
 };
 
 namespace ch3d {
+
+// y periodic (BcOption(3:4) = 0): the triply periodic steps (FIMP_000, PIMP_0)
+inline bool y_periodic(const ch3d_ctx* c) { return c->cfg.BcOption[2] == 0; }
 // launchers (ch3d_step.cu)
 cudaError_t launch_substep_setup(ch3d_ctx* c, int ns);
 cudaError_t launch_step_begin(ch3d_ctx* c);
@@ -150,10 +154,12 @@ cudaError_t launch_visc4_partials(ch3d_ctx* c);        // mean viscous stress pa
 int visc4_npart(const ch3d_ctx* c);                   // their count
 cudaError_t launch_dissipation(ch3d_ctx* c, int* npart);  // CalcDissipationRate partials -> part2
 cudaError_t launch_reduce_partials(ch3d_ctx* c, const double* in, int n, double* out);  // CH3D_NRED sums
-// fully implicit 2nd-order step (ch3d_step.cu, ch3d_fimp.cu)
-cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP -> RhsX/Y/Z
+// fully implicit and explicit 2nd-order steps (ch3d_step.cu, ch3d_fimp.cu)
+cudaError_t launch_rhs_fimp(ch3d_ctx* c);              // clcRhsX/Y/Z_FIMP (or _FEXP) -> RhsX/Y/Z
+cudaError_t launch_uhat_fexp(ch3d_ctx* c);             // clcU1/2/3Hat_FEXP: u* = u + RhsX/Y/Z
 cudaError_t launch_ptri_xz(ch3d_ctx* c);               // periodic x and z sweeps of RhsX/Y/Z, in place
-size_t ptri_factor_doubles(int nx, int nz);
+cudaError_t launch_ptri_y(ch3d_ctx* c);                // periodic y sweep (y periodic, FIMP or PIMP): u* = u + solution
+size_t ptri_factor_doubles(int nx, int ny, int nz);
 // LES (ch3d_les.cu), FP64
 cudaError_t launch_mlp_pack(ch3d_ctx* c);              // parameter image of the closure's network
 cudaError_t launch_fill_nut(ch3d_ctx* c);              // nut = xnu (learned closure)

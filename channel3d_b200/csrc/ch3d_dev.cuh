@@ -10,7 +10,8 @@ namespace ch3d {
 // Neighbour addressing of one cell: a base index plus signed offsets that
 // already contain the periodic wrap in x and z; y neighbours past the walls
 // are replaced by the ghost rules of SetBC_and_UpdateHalo
-// (src/CFD_2nd/m_BC_and_Halo.f90:241-282).
+// (src/CFD_2nd/m_BC_and_Halo.f90:241-282), or by the periodic halo rows when
+// y is periodic (BcOption(3:4) = 0).
 struct Nbr {
   long long c;        // cell index
   int xp, xm;         // offsets to i+1, i-1
@@ -48,6 +49,7 @@ template <class T> __device__ __forceinline__ T at(const T* __restrict__ a, cons
 template <class T>
 __device__ __forceinline__ T at_jm(const T* __restrict__ a, const Geo<T>& g, int comp, const Nbr& n, long long o) {
   if (!n.jlo) return __ldg(a + n.c + o - n.yp);
+  if (g.bc.lo == 0) return __ldg(a + n.c + o + (long long)(g.ny - 1) * n.yp);  // periodic: row ny-1
   if (comp == 1) {  // uy(ic,0,kc) = 2 uy_ym - uy(ic,2,kc); zero in the 4th-order solver
     if (g.order == 4) return (T)0;
     return (T)(g.bc.uy_lo * 2.0) - __ldg(a + n.c + o + n.yp);
@@ -60,6 +62,7 @@ __device__ __forceinline__ T at_jm(const T* __restrict__ a, const Geo<T>& g, int
 template <class T>
 __device__ __forceinline__ T at_jp(const T* __restrict__ a, const Geo<T>& g, int comp, const Nbr& n, long long o) {
   if (!n.jhi) return __ldg(a + n.c + o + n.yp);
+  if (g.bc.hi == 0) return __ldg(a + n.c + o - (long long)(g.ny - 1) * n.yp);  // periodic: row 0
   if (comp == 1) return (T)g.bc.uy_hi;  // uy(ic,nyp,kc) = uyBcValue(yp)
   const T v = __ldg(a + n.c + o);
   if (comp == 3) return v;

@@ -1,8 +1,9 @@
 // ch3d_fimp.cu -- sm_100a kernels of the fully implicit (FIMP) 2nd-order
-// step for the channel: the periodic x and z Crank-Nicolson sweeps of
-// clcU1/2/3Hat_FIMP_010 (src/CFD_2nd/m_TSchemeFIMP_inc.f90:263-347, 636-729,
-// 1035-1128).  The y sweep that follows is the PIMP Helmholtz solve
-// (same coefficients), the RHS is rhs_comp with its FIMP branch.
+// step: the periodic x and z Crank-Nicolson sweeps of clcU1/2/3Hat_FIMP_010
+// (src/CFD_2nd/m_TSchemeFIMP_inc.f90:263-347, 636-729, 1035-1128), whose y
+// sweep between walls is the PIMP Helmholtz solve (same coefficients), and
+// the periodic y sweep of clcU1/2/3Hat_FIMP_000 (:187-258, 559-631, 950-1030)
+// when y is periodic too.  The RHS is rhs_comp with its FIMP branch.
 //
 // The periodic constant-coefficient solver is InversePTriFixedCoe
 // (src/CFD_2nd/m_Tools.f90:167-219): elimination of the first n-1 unknowns
@@ -18,14 +19,15 @@ namespace ch3d {
 // index 1..n) then a, b, c, denominator.
 __host__ __device__ inline int ptri_stride(int n) { return 3 * (n + 1) + 4; }
 
-// blockIdx.x: 0 = x (n = nx, rdx2), 1 = z (n = nz, rdz2)
-__global__ void k_ptri_factors(int nx, int nz, double rdx2, double rdz2, double* __restrict__ pf,
-                               const DevScalars* __restrict__ sc) {
+// direction d0 + blockIdx.x: 0 = x (n = nx, rdx2), 1 = z (n = nz, rdz2),
+// 2 = y (n = ny, rdy2; periodic y only)
+__global__ void k_ptri_factors(int d0, int nx, int ny, int nz, double rdx2, double rdy2, double rdz2,
+                               double* __restrict__ pf, const DevScalars* __restrict__ sc) {
   if (sc->status || threadIdx.x != 0) return;
-  const int d = blockIdx.x;
-  const int n = d == 0 ? nx : nz;
-  const double r2 = d == 0 ? rdx2 : rdz2;
-  double* F = pf + (d == 0 ? 0 : ptri_stride(nx));
+  const int d = d0 + blockIdx.x;
+  const int n = d == 0 ? nx : (d == 1 ? nz : ny);
+  const double r2 = d == 0 ? rdx2 : (d == 1 ? rdz2 : rdy2);
+  double* F = pf + (d == 0 ? 0 : (d == 1 ? ptri_stride(nx) : ptri_stride(nx) + ptri_stride(nz)));
   double *ppj = F, *v1 = F + (n + 1), *v2 = F + 2 * (n + 1), *abc = F + 3 * (n + 1);
   const double pmBeta = sc->pmBeta;
   const double a = -pmBeta * r2, c = -pmBeta * r2, b = pmBeta * r2 * 2.0 + 1.0;
@@ -137,9 +139,44 @@ __global__ void __launch_bounds__(128) k_ptri_z(int nx, int ny, int nz, const do
   ptri_line<T, 16>(Fs, nz, r + i + (long long)nx * j, (long long)nx * ny);
 }
 
+// periodic y sweep (the last sweep of clcU1/2/3Hat_FIMP_000, or the one sweep
+// of clcU1/2/3Hat_PIMP_0, src/CFD_2nd/m_TSchemePIMP_inc.f90:435-461, 594-621,
+// 745-771): one thread per (i, k) column, in place on the right-hand side (a
+// warp covers 32 consecutive i, so every access is coalesced), then
+// u* = u + the solution.  The partially implicit RhsX gets the mean pressure
+// gradient first (clcRhsX_PIMP adds it; the FIMP RhsX carries it already).
+// blockIdx.z = component.
+template <class T>
+__global__ void __launch_bounds__(128) k_ptri_y(int nx, int ny, int nz, int pimp, const double* __restrict__ pf,
+                                                const T* __restrict__ u0, const T* __restrict__ u1,
+                                                const T* __restrict__ u2, T* __restrict__ r0, T* __restrict__ r1,
+                                                T* __restrict__ r2, T* __restrict__ s0, T* __restrict__ s1,
+                                                T* __restrict__ s2, const DevScalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (sc->status) return;
+  double* Fs = (double*)smem_raw;
+  ptri_stage_factors(Fs, pf + ptri_stride(nx) + ptri_stride(nz), ny);
+  __syncthreads();
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int k = blockIdx.y * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (i >= nx || k >= nz) return;
+  const int comp = blockIdx.z;
+  const T* u = comp == 0 ? u0 : (comp == 1 ? u1 : u2);
+  T* r = comp == 0 ? r0 : (comp == 1 ? r1 : r2);
+  T* us = comp == 0 ? s0 : (comp == 1 ? s1 : s2);
+  const long long col = i + (long long)nx * ny * k;
+  if (pimp && comp == 0) {
+    const T add = (T)sc->dpmdxns;
+    for (int j = 0; j < ny; ++j) r[col + (long long)nx * j] = r[col + (long long)nx * j] + add;
+  }
+  ptri_line<T, 16>(Fs, ny, r + col, (long long)nx);
+  for (int j = 0; j < ny; ++j) us[col + (long long)nx * j] = u[col + (long long)nx * j] + r[col + (long long)nx * j];
+}
+
 template <class T> static cudaError_t ptri_t(ch3d_ctx* c) {
   T** f = (T**)c->f;
-  k_ptri_factors<<<2, 32, 0, c->stream>>>(c->nx, c->nz, c->rdx2, c->rdz2, c->pfac, c->sc);
+  k_ptri_factors<<<y_periodic(c) ? 3 : 2, 32, 0, c->stream>>>(0, c->nx, c->ny, c->nz, c->rdx2, c->rdy2, c->rdz2,
+                                                              c->pfac, c->sc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   // x: one thread per line, at most 64 KB of lines per block
@@ -163,6 +200,26 @@ template <class T> static cudaError_t ptri_t(ch3d_ctx* c) {
 }
 cudaError_t launch_ptri_xz(ch3d_ctx* c) { return c->fp32 ? ptri_t<float>(c) : ptri_t<double>(c); }
 
-size_t ptri_factor_doubles(int nx, int nz) { return (size_t)ptri_stride(nx) + ptri_stride(nz); }
+template <class T> static cudaError_t ptri_y_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  const int pimp = c->cfg.IsImplicit == 1;
+  cudaError_t e;
+  if (pimp) {  // the y factor block alone (FIMP: made by launch_ptri_xz with the x and z blocks)
+    k_ptri_factors<<<1, 32, 0, c->stream>>>(2, c->nx, c->ny, c->nz, c->rdx2, c->rdy2, c->rdz2, c->pfac, c->sc);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  const size_t smy = (size_t)ptri_stride(c->ny) * sizeof(double);
+  static PerDevice attr;  // per precision (template instance)
+  if ((e = smem_limit_once(attr, c->device, k_ptri_y<T>, 200 * 1024)) != cudaSuccess) return e;
+  k_ptri_y<T><<<dim3((c->nx + 31) / 32, (c->nz + 3) / 4, 3), 128, smy, c->stream>>>(
+      c->nx, c->ny, c->nz, pimp, c->pfac, f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13], f[14], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_ptri_y(ch3d_ctx* c) { return c->fp32 ? ptri_y_t<float>(c) : ptri_y_t<double>(c); }
+
+// x, z and y factor blocks (the y block is filled only when y is periodic)
+size_t ptri_factor_doubles(int nx, int ny, int nz) {
+  return (size_t)ptri_stride(nx) + ptri_stride(nz) + ptri_stride(ny);
+}
 
 }  // namespace ch3d

@@ -83,7 +83,10 @@ __global__ void __launch_bounds__(32 * kXWarps, SRC ? 6 : (sizeof(T) == 4 ? 6 : 
           const T2 u01 = __ldg(reinterpret_cast<const T2*>(ux + base + i0));
           const T u2 = __ldg(ux + base + i2);
           const T2 v01 = __ldg(reinterpret_cast<const T2*>(uy + base + i0));
-          const T2 v01p = top ? mk((T)g.bc.uy_hi, (T)g.bc.uy_hi) : __ldg(reinterpret_cast<const T2*>(uy + base + nx + i0));
+          // uy at j+1: the next row, above the top row the wall value or, periodic in y, row 0
+          const T2 v01p = !top ? __ldg(reinterpret_cast<const T2*>(uy + base + nx + i0))
+                          : (g.bc.hi == 0 ? __ldg(reinterpret_cast<const T2*>(uy + base - (long long)(ny - 1) * nx + i0))
+                                          : mk((T)g.bc.uy_hi, (T)g.bc.uy_hi));
           const T2 w01 = __ldg(reinterpret_cast<const T2*>(uz + base + i0));
           const T2 w01p = __ldg(reinterpret_cast<const T2*>(uz + basep + i0));
           r0 = (u01.y - u01.x) * rdx + (v01p.x - v01.x) * sucaj + (w01p.x - w01.x) * rdz;

@@ -201,7 +201,7 @@ __device__ __forceinline__ void rhs_point(const Geo<T>& g, const Metrics<T>& m, 
   }
 }
 
-// One component of clcRhsX/Y/Z_PIMP (or _FIMP) at one cell (C = 0, 1, 2),
+// One component of clcRhsX/Y/Z_PIMP (or _FIMP, _FEXP) at one cell (C = 0, 1, 2),
 // with its Hist update.
 template <class T, int C>
 __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, const T* __restrict__ ux,
@@ -234,6 +234,11 @@ __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, cons
     T d33q1 = g.ap3c * ux_kp + g.ac3c * ux_c + g.am3c * ux_km;
     T dcq13 = d11q1 + d33q1;
     T gradp1 = (p_c - p_im) * rdx;
+    if (g.implicit == 0) {  // clcRhsX_FEXP (src/CFD_2nd/m_TSchemeFEXP_inc.f90:33-55)
+      T convEd1 = -h11 - h12 - h13 + xnu * (d11q1 + d22q1 + d33q1) + g.g1;
+      h[n.c] = convEd1;
+      return pmGamma * convEd1 + pmTheta * h_o - pmAlpha * gradp1;
+    }
     if (g.implicit == 2) {  // clcRhsX_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:45-55)
       T convEd1 = -h11 - h12 - h13 + g.g1;
       h[n.c] = convEd1;
@@ -262,6 +267,11 @@ __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, cons
     T d33q2 = g.ap3c * uy_kp + g.ac3c * uy_c + g.am3c * uy_km;
     T dcq13 = d11q2 + d33q2;
     T gradp2 = (p_c - p_jm) * sucac;
+    if (g.implicit == 0) {  // clcRhsY_FEXP (src/CFD_2nd/m_TSchemeFEXP_inc.f90:183-204)
+      T convEd2 = -h21 - h22 - h23 + xnu * (d11q2 + d22q2 + d33q2) + g.g2;
+      h[n.c] = convEd2;
+      return pmGamma * convEd2 + pmTheta * h_o - pmAlpha * gradp2;
+    }
     if (g.implicit == 2) {  // clcRhsY_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:104-115)
       T convEd2 = -h21 - h22 - h23 + g.g2;
       h[n.c] = convEd2;
@@ -291,6 +301,11 @@ __device__ __forceinline__ T rhs_comp(const Geo<T>& g, const Metrics<T>& m, cons
     T d33q3 = (uz_kp - two * uz_c + uz_km) * rdz2;
     T dcq13 = d11q3 + d33q3;
     T gradp3 = (p_c - p_km) * rdz;
+    if (g.implicit == 0) {  // clcRhsZ_FEXP (src/CFD_2nd/m_TSchemeFEXP_inc.f90:299-320)
+      T convEd3 = -h31 - h32 - h33 + xnu * (d11q3 + d22q3 + d33q3) + g.g3;
+      h[n.c] = convEd3;
+      return pmGamma * convEd3 + pmTheta * h_o - pmAlpha * gradp3;
+    }
     if (g.implicit == 2) {  // clcRhsZ_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:161-172)
       T convEd3 = -h31 - h32 - h33 + g.g3;
       h[n.c] = convEd3;
@@ -321,7 +336,8 @@ __global__ void __launch_bounds__(256) k_rhs_pimp(Geo<T> g, Metrics<T> m, const 
   rx[idx] = a; ry[idx] = b; rz[idx] = c;
 }
 
-// clcRhsX/Y/Z_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:6-177), one thread per
+// clcRhsX/Y/Z_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:6-177), or _FEXP
+// (src/CFD_2nd/m_TSchemeFEXP_inc.f90:6-324) when g.implicit = 0, one thread per
 // cell and component (blockIdx.z = component * nz + k: a thread holds one
 // component's stencil, so more threads fit an SM than with all three),
 // RhsX with the mean pressure gradient (:57-66) included.
@@ -870,6 +886,150 @@ __global__ void __launch_bounds__(128) k_ythomas_low(Geo<T> g, Metrics<double> m
 }
 
 // ---------------------------------------------------------------------------
+// Periodic y (clcPPE_z1_periodic, src/CFD_2nd/m_Poisson.f90:954-1073): the
+// systems [am2Pr, ac2Pr + wx(kx) + wz(kz), ap2Pr] are cyclic, solved by
+// InversePeriodicTridiagonal (src/CFD_2nd/m_Tools.f90:109-162), with row 1
+// of the (0,0) system replaced by phi = 0 (:1012-1029).  Its coefficient
+// recurrences depend on the mode only and are computed once per run, one
+// thread per (kx, |kz|), FP64, layout ((kzh * ny) + j) * nxh + kx:
+//   PP_0 = b_1 (row 1 divides), PP_j = 1 / (b + a arrmn1_{j-1}) (ppj),
+//   A1_j = arrmn1_j, A1_{n-1} = the closing denominator,
+//   A2_j = arrmn2_j after the backward pass.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_ycyclic_factors(Metrics<double> m, const double* __restrict__ wave, int nx,
+                                                         int ny, int nxh, double* __restrict__ PP,
+                                                         double* __restrict__ A1, double* __restrict__ A2) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x, kzh = blockIdx.y;
+  if (kx >= nxh) return;
+  const double lam = wave[kx] + wave[nx + kzh];
+  const bool pin = (kx == 0 && kzh == 0);
+  const size_t st = (size_t)nxh, o = (size_t)kzh * ny * st + kx;
+  auto coef = [&](int j, double& a, double& b, double& c) {
+    a = m.am2Pr[j + 1]; c = m.ap2Pr[j + 1]; b = m.ac2Pr[j + 1] + lam;
+    if (pin && j == 0) { a = 0.0; b = 1.0; c = 0.0; }
+  };
+  double a, b, c;
+  coef(0, a, b, c);
+  double v1 = -c / b, v2 = -a / b;
+  PP[o] = b; A1[o] = v1; A2[o] = v2;
+  for (int j = 1; j <= ny - 2; ++j) {
+    coef(j, a, b, c);
+    const double ppj = 1.0 / (b + a * v1);
+    v1 = -c * ppj;
+    v2 = -a * v2 * ppj;
+    PP[o + st * j] = ppj; A1[o + st * j] = v1; A2[o + st * j] = v2;
+  }
+  // backward pass: arrmn2_n = 1, arrmn2_j += arrmn1_j arrmn2_{j+1}
+  double w = 1.0;
+  A2[o + st * (ny - 1)] = w;
+  for (int j = ny - 2; j >= 0; --j) {
+    w = A2[o + st * j] + A1[o + st * j] * w;
+    A2[o + st * j] = w;
+  }
+  coef(ny - 1, a, b, c);
+  A1[o + st * (ny - 1)] = c * A2[o] + a * A2[o + st * (ny - 2)] + b;
+}
+
+// One thread per (kx, kz) column of the (kx, j, kz) spectrum (kx fastest, so
+// a warp reads 32 consecutive kx of one row), FP64, in place: forward
+// elimination, the backward pass of the right-hand side (arrmn3), the closure
+// of row n, and the back substitution f_j = f_n arrmn2_j + arrmn3_j.  Each
+// pass loads YB rows (and their factors) before its dependent recurrence, so
+// YB loads of every column are in flight at once.
+template <class T, int YB>
+__global__ void __launch_bounds__(128) k_ycyclic(Geo<T> g, Metrics<double> m, const double* __restrict__ PP,
+                                                 const double* __restrict__ A1, const double* __restrict__ A2,
+                                                 typename CplxOf<T>::type* __restrict__ spec,
+                                                 const DevScalars* __restrict__ sc) {
+  typedef typename CplxOf<T>::type CT;
+  if (sc->status) return;
+  const int nxh = g.nxh, ny = g.ny, nz = g.nz;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nxh * nz) return;
+  const int kx = (int)(t % nxh), kz = (int)(t / nxh);
+  const int kzh = kz <= nz - kz ? kz : nz - kz;
+  const size_t st = (size_t)nxh;
+  CT* col = spec + kx + st * ny * kz;
+  const size_t o = (size_t)kzh * ny * st + kx;
+  const bool pin = (kx == 0 && kz == 0);
+  // forward elimination, rows 1..n-1 (0-based 0..ny-2); row 1 divides by b_1
+  double dx = 0.0, dy = 0.0;
+  for (int j0 = 0; j0 <= ny - 2; j0 += YB) {
+    double fx[YB], fy[YB], pp[YB], am[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j <= ny - 2) {
+        const CT f = col[st * j];
+        fx[u] = (double)f.x; fy[u] = (double)f.y;
+        pp[u] = PP[o + st * j];
+        am[u] = m.am2Pr[j + 1];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j <= ny - 2) {
+        if (j == 0) {
+          dx = pin ? 0.0 : fx[u] / pp[u];
+          dy = pin ? 0.0 : fy[u] / pp[u];
+        } else {
+          dx = (fx[u] - am[u] * dx) * pp[u];
+          dy = (fy[u] - am[u] * dy) * pp[u];
+        }
+        col[st * j] = mk((T)dx, (T)dy);
+      }
+    }
+  }
+  // backward pass: arrmn3_n = 0, arrmn3_j = f_j + arrmn1_j arrmn3_{j+1}
+  double ex = 0.0, ey = 0.0, lx = 0.0, ly = 0.0;
+  for (int j1 = ny - 2; j1 >= 0; j1 -= YB) {
+    double vx[YB], vy[YB], a1[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j1 - u;
+      if (j >= 0) {
+        const CT f = col[st * j];
+        vx[u] = (double)f.x; vy[u] = (double)f.y;
+        a1[u] = A1[o + st * j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j1 - u;
+      if (j >= 0) {
+        ex = vx[u] + a1[u] * ex;
+        ey = vy[u] + a1[u] * ey;
+        col[st * j] = mk((T)ex, (T)ey);
+        if (j == ny - 2) { lx = ex; ly = ey; }
+      }
+    }
+  }
+  // closure of row n, then f_j = f_n arrmn2_j + arrmn3_j
+  const double an = m.am2Pr[ny], cn = m.ap2Pr[ny], den = A1[o + st * (ny - 1)];
+  const CT fl = col[st * (ny - 1)];
+  const double fnx = ((double)fl.x - cn * ex - an * lx) / den, fny = ((double)fl.y - cn * ey - an * ly) / den;
+  col[st * (ny - 1)] = mk((T)fnx, (T)fny);
+  for (int j0 = 0; j0 <= ny - 2; j0 += YB) {
+    double vx[YB], vy[YB], a2[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j <= ny - 2) {
+        const CT f = col[st * j];
+        vx[u] = (double)f.x; vy[u] = (double)f.y;
+        a2[u] = A2[o + st * j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j <= ny - 2) col[st * j] = mk((T)(fnx * a2[u] + vx[u]), (T)(fny * a2[u] + vy[u]));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // inverse x transform (complex-to-real, unnormalised as FFTW's HC2R) * normfft
 // (src/CFD_2nd/m_Poisson.f90:1194-1200) -> phi.
 // ---------------------------------------------------------------------------
@@ -960,7 +1120,8 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
     const T pmAlpha = mode == 0 ? (T)sc->pmAlpha : (T)1;
     const T phic = phi[idx];
     const T phim_x = phi[im + (long long)nx * (j + (long long)ny * k)];
-    const T phim_y = phi[i + (long long)nx * ((j > 0 ? j - 1 : 0) + (long long)ny * k)];
+    const int jm = j > 0 ? j - 1 : (g.bc.lo == 0 ? ny - 1 : 0);  // phi(ic,0,kc): Neumann or periodic halo
+    const T phim_y = phi[i + (long long)nx * (jm + (long long)ny * k)];
     const T phim_z = phi[i + (long long)nx * (j + (long long)ny * km)];
     const T rdxEta2 = g.rdx * pmAlpha, rdzEta2 = g.rdz * pmAlpha, sucacEta2 = m.rdyc[jc] * pmAlpha;
     T uxn = uxs[idx] - (phic - phim_x) * rdxEta2;
@@ -991,10 +1152,13 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
       const T pmBetam = -pmBetaT * metr1 * visc;
       const T pmBetac = -(pmBetap + pmBetam) + (T)1;
       pr[idx] = pr[idx] + pmBetap * phip_y + pmBetac * phic + pmBetam * phim_y;
-    } else if (mode == 0 && g.implicit == 2) {
-      pr[idx] = pr[idx] + phic;  // PressureUpdate_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386)
+    } else if (mode == 0 && (g.implicit == 2 || g.implicit == 0)) {
+      // PressureUpdate_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386), _FEXP
+      // (src/CFD_2nd/m_TSchemeFEXP_inc.f90:513-528)
+      pr[idx] = pr[idx] + phic;
     } else if (mode == 0) {
-      const T phip_y = phi[i + (long long)nx * ((j < ny - 1 ? j + 1 : ny - 1) + (long long)ny * k)];
+      const int jp = j < ny - 1 ? j + 1 : (g.bc.hi == 0 ? 0 : ny - 1);  // phi(ic,nyp,kc): Neumann or periodic halo
+      const T phip_y = phi[i + (long long)nx * (jp + (long long)ny * k)];
       const T pmBeta = (T)sc->pmBeta;
       const T pmBetap = -pmBeta * m.ap2Pr[jc];
       const T pmBetac = -pmBeta * m.ac2Pr[jc] + (T)1;
@@ -1057,7 +1221,8 @@ __global__ void __launch_bounds__(128) k_diag(Geo<T> g, Metrics<T> m, const T* _
       const int jc = j + 1;
       const double a = ux[idx], c = uz[idx];
       const double aip = ux[idx + dxp], ckp = uz[idx + dzp];
-      const double bjp = j + 1 < ny ? (double)uy[idx + nx] : (double)(T)g.bc.uy_hi;
+      const double bjp = j + 1 < ny ? (double)uy[idx + nx]
+                                    : (g.bc.hi == 0 ? (double)uy[col] : (double)(T)g.bc.uy_hi);  // periodic: row 0
       const double rdyp = m.rdyp[jc];
       double d = fabs((aip - a) * rdx + (bjp - b) * rdyp + (ckp - c) * rdz);
       if (g.order == 4) d = fabs((double)div4_at(g, c4, m.rdyp[jc], ux, uy, uz, n4));
@@ -1203,6 +1368,38 @@ template <class T> static cudaError_t rhs_fimp_t(ch3d_ctx* c) {
 }
 cudaError_t launch_rhs_fimp(ch3d_ctx* c) { return c->fp32 ? rhs_fimp_t<float>(c) : rhs_fimp_t<double>(c); }
 
+// clcU1/2/3Hat_FEXP (src/CFD_2nd/m_TSchemeFEXP_inc.f90:391-488): u* = u + Rhs,
+// every cell; between walls the uy row on the lower wall then takes uy_ym,
+// as SetBC_and_UpdateHaloForPrSrc (src/CFD_2nd/m_BC_and_Halo.f90:349-405)
+// sets it before the divergence.  blockIdx.y = component.
+template <class T>
+__global__ void __launch_bounds__(256) k_uhat_fexp(Geo<T> g, const T* __restrict__ ux, const T* __restrict__ uy,
+                                                   const T* __restrict__ uz, const T* __restrict__ rx,
+                                                   const T* __restrict__ ry, const T* __restrict__ rz,
+                                                   T* __restrict__ sx, T* __restrict__ sy, T* __restrict__ sz,
+                                                   const DevScalars* __restrict__ sc) {
+  if (sc->status) return;
+  const int comp = blockIdx.y;
+  const T* u = comp == 0 ? ux : (comp == 1 ? uy : uz);
+  const T* r = comp == 0 ? rx : (comp == 1 ? ry : rz);
+  T* us = comp == 0 ? sx : (comp == 1 ? sy : sz);
+  const long long plane = (long long)g.nx * g.ny;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < g.N; q += (long long)gridDim.x * blockDim.x) {
+    T v = u[q] + r[q];
+    if (comp == 1 && g.bc.lo != 0 && q % plane < g.nx) v = (T)g.bc.uy_lo;
+    us[q] = v;
+  }
+}
+template <class T> static cudaError_t uhat_fexp_t(ch3d_ctx* c) {
+  T** f = (T**)c->f;
+  const long long nb = (c->N + 255) / 256;
+  const unsigned gx = (unsigned)(nb < 148LL * 16 ? nb : 148LL * 16);
+  k_uhat_fexp<T><<<dim3(gx, 3), 256, 0, c->stream>>>(make_geo<T>(c), f[0], f[1], f[2], f[7], f[8], f[9], f[12], f[13],
+                                                     f[14], c->sc);
+  return cudaGetLastError();
+}
+cudaError_t launch_uhat_fexp(ch3d_ctx* c) { return c->fp32 ? uhat_fexp_t<float>(c) : uhat_fexp_t<double>(c); }
+
 cudaError_t launch_helm_factors(ch3d_ctx* c) {
   k_helm_factors<<<2, 64, 0, c->stream>>>(helm_coef(c), c->ny, c->Pv, c->hfac, c->sc);
   return cudaGetLastError();
@@ -1280,7 +1477,10 @@ template <class T> static cudaError_t spectral_t(ch3d_ctx* c) {
     if (e != cudaSuccess) return e;
   }
   const unsigned gy = (unsigned)(((long long)c->nxh * c->nz + 127) / 128);
-  if (!c->fp32) {
+  if (y_periodic(c)) {  // periodic y (FP64 only): the cyclic systems
+    k_ycyclic<T, 16><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
+                                                (const double*)c->yCP, c->yA2, (CT*)c->spec, c->sc);
+  } else if (!c->fp32) {
     k_ythomas<T, double, 16><<<gy, 128, 0, c->stream>>>(make_geo<T>(c), c->m64full, (const double*)c->yRM,
                                                         (const double*)c->yCP, (CT*)c->spec, 0, 0, c->sc);
   } else {
@@ -1326,7 +1526,10 @@ cudaError_t launch_zfft_forward(ch3d_ctx* c) { return c->fp32 ? zfft_fwd_t<float
 
 template <class T> static cudaError_t yfactors_t(ch3d_ctx* c) {
   const dim3 g((c->nxh + 127) / 128, c->nz / 2 + 1);
-  if (!c->fp32) {
+  if (y_periodic(c)) {  // periodic y (FP64 only)
+    k_ycyclic_factors<<<g, 128, 0, c->stream>>>(c->m64full, c->wave, c->nx, c->ny, c->nxh, (double*)c->yRM,
+                                                (double*)c->yCP, c->yA2);
+  } else if (!c->fp32) {
     k_ythomas_factors<double><<<g, 128, 0, c->stream>>>(c->m64full, c->wave, c->nx, c->ny, (double*)c->yRM,
                                                         (double*)c->yCP, c->nxh, c->nxh);
   } else {

@@ -84,7 +84,8 @@ def taylor_green(cfg, yp=None, vel=1.0, length=1.0):
     x_i = (i - 1) dx, xc = x + dx / 2 (the same in z), yp the y nodes and yc
     the cell centres.  The field is mirror-symmetric about y = 0 and y = pi L
     (uy odd, ux and uz even), so a box of height pi L with free-slip walls
-    holds half a period of the triply periodic vortex."""
+    holds half a period of the triply periodic vortex; a box of height 2 pi L
+    with periodic y holds the whole period."""
     if yp is None:
         yp = mesh_y(cfg)
     yp = np.asarray(yp)

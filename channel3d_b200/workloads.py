@@ -47,6 +47,18 @@ def taylor_green(n=64, xnu=6.25e-4, dt=0.01, **kw):
                          StretType=[0], StretOption=[0], SectioncStret=[0.0], RunName="TGVortex", **kw)
 
 
+def taylor_green_periodic(n=64, xnu=6.25e-4, dt=0.01, **kw):
+    """The Taylor-Green vortex of Input/TaylorGreenVortex.prm (FlowType 3, V = L = 1,
+    xnu 6.25e-4, dt 0.01 fixed) in its triply periodic 2pi x 2pi x 2pi box
+    (BcOption 0 0 0 0 0 0), n^3 uniform cells, with the fully implicit step
+    (IsImplicit 2: clcU*Hat_FIMP_000 and clcPPE_z1_periodic; the reference's
+    input runs the explicit scheme, IsImplicit 0, which is not built); no forcing."""
+    return ChannelConfig(FlowType=3, nxc=n, nyc=n, nzc=n, xlx=2 * np.pi, yly=2 * np.pi, zlz=2 * np.pi, xnu=xnu,
+                         dtMax=dt, iCFL=2, IsImplicit=2, BcOption=[0, 0, 0, 0, 0, 0], IsUxConst=False, ubulk=0.0,
+                         ybulk1=0.0, ybulk2=2 * np.pi, nSection=1, SectionLength=[1.0], nycSection=[n],
+                         StretType=[0], StretOption=[0], SectioncStret=[0.0], RunName="TGVortex", **kw)
+
+
 def get(name, **kw):
     factory, steps = WORKLOADS[name]
     return factory(**kw), steps

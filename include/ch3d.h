@@ -86,8 +86,11 @@ typedef struct ch3d_config {
   double CFLc;
   int ischeme;            /* 1 AB2, 2 RK2, 3 RK3 */
   int IsImplicit;         /* 1 PIMP (y Crank-Nicolson), 2 FIMP (x,z,y ADI) */
-  int FlowType;           /* 1 channel, 2 half channel */
-  int BcOption[6];        /* x-,x+,y-,y+,z-,z+ : 0 periodic, -1 no-slip, -2 free-slip */
+  int FlowType;           /* 1 channel, 2 half channel, 3 Taylor-Green vortex */
+  int BcOption[6];        /* x-,x+,y-,y+,z-,z+ : 0 periodic, -1 no-slip, -2 free-slip;
+                             x and z periodic; y periodic on both sides only with
+                             IsImplicit = 2 in FP64 (clcU*Hat_FIMP_000,
+                             src/CFD_2nd/m_TScheme.f90:151-157) */
   double uxBcValue[6], uyBcValue[6], uzBcValue[6];
   double gravity[3];
   int IsUxConst;

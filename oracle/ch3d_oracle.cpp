@@ -18,7 +18,8 @@
 // (i fastest), ghosted arrays with the bounds of `myallocate`
 // (src/CFD_2nd/m_Decomp2d.f90:1517-1583) for a single rank (y1start=1,
 // y1end=n).  Only periodic x and z are supported (the channel configuration);
-// y may be no-slip or free-slip.
+// y may be no-slip, free-slip, or periodic (clcU*Hat_FIMP_000 or
+// clcU*Hat_PIMP_0, clcPPE_z1_periodic).
 //
 // The FFT that the reference takes from FFTW 3.3.9 (r2r kinds R2HC/HC2R,
 // src/CFD_2nd/m_Poisson.f90:267-307) is restated from its definition
@@ -661,10 +662,37 @@ struct Oracle {
     for (int j = n - 2; j >= 0; --j) fj[j] = fj[j] - arr[j + 1] * fj[j + 1];
   }
 
-  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75 (clcRhsX_PIMP); with fimp the
+  // ---- src/CFD_2nd/m_Tools.f90:109-162 (InversePeriodicTridiagonal), one cyclic
+  //      system (aj: sub, bj: diagonal, cj: super; aj[0] and cj[n-1] wrap) ----
+  static void InversePeriodicTridiagonal1(const double* aj, const double* bj, const double* cj, double* fj, int n,
+                                          double* a1, double* a2, double* a3) {
+    a1[0] = -cj[0] / bj[0];
+    a2[0] = -aj[0] / bj[0];
+    fj[0] = fj[0] / bj[0];
+    for (int j = 1; j <= n - 2; ++j) {
+      double ppj = one / (bj[j] + aj[j] * a1[j - 1]);
+      a1[j] = -cj[j] * ppj;
+      a2[j] = -aj[j] * a2[j - 1] * ppj;
+      fj[j] = (fj[j] - aj[j] * fj[j - 1]) * ppj;
+    }
+    a2[n - 1] = one;
+    a3[n - 1] = zero;
+    for (int j = n - 2; j >= 0; --j) {
+      a2[j] = a2[j] + a1[j] * a2[j + 1];
+      a3[j] = fj[j] + a1[j] * a3[j + 1];
+    }
+    fj[n - 1] = (fj[n - 1] - cj[n - 1] * a3[0] - aj[n - 1] * a3[n - 2]) /
+                (cj[n - 1] * a2[0] + aj[n - 1] * a2[n - 2] + bj[n - 1]);
+    for (int j = n - 2; j >= 0; --j) fj[j] = fj[n - 1] * a2[j] + a3[j];
+  }
+
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:7-75 (clcRhsX_PIMP); scheme 2: the
   //      same loop is clcRhsX_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:6-67): no
-  //      explicit viscous term in convEd1, 2*pmBeta*(d11+d22+d33) instead ----
-  void clcRhsX_PIMP(F3& RhsX, F3& Hist, bool fimp = false) {
+  //      explicit viscous term in convEd1, 2*pmBeta*(d11+d22+d33) instead;
+  //      scheme 0: clcRhsX_FEXP (src/CFD_2nd/m_TSchemeFEXP_inc.f90:6-75), the
+  //      whole viscous term in convEd1 and no pmBeta term ----
+  void clcRhsX_PIMP(F3& RhsX, F3& Hist, int scheme = 1) {
+    const bool fimp = scheme == 2, fexp = scheme == 0;
     double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
     std::vector<double> part(nzc + 1, 0.0);
     const double g1 = P.gravity[0], xnu = P.xnu;
@@ -696,6 +724,10 @@ struct Oracle {
           double convEd1, dcn;
           if (fimp) { convEd1 = -h11 - h12 - h13 + g1; dcn = d11q1 + d22q1 + d33q1; }
           else { convEd1 = -h11 - h12 - h13 + xnu * dcq13 + g1; dcn = d22q1; }
+          if (fexp) {  // clcRhsX_FEXP: the whole viscous term explicit
+            convEd1 = -h11 - h12 - h13 + xnu * (d11q1 + d22q1 + d33q1) + g1;
+            RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1;
+          } else
           RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1 + two * pmBeta * dcn;
           Hist(ic, jc, kc) = convEd1;
         }
@@ -717,7 +749,8 @@ struct Oracle {
 
   // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:161-209 (clcRhsY_PIMP); fimp:
   //      clcRhsY_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:72-119) ----
-  void clcRhsY_PIMP(F3& RhsY, F3& Hist, bool fimp = false) {
+  void clcRhsY_PIMP(F3& RhsY, F3& Hist, int scheme = 1) {
+    const bool fimp = scheme == 2, fexp = scheme == 0;
     double hdx1 = half * rdx, hdx3 = half * rdz;
     const double g2 = P.gravity[1], xnu = P.xnu;
 #pragma omp parallel for schedule(static)
@@ -743,6 +776,10 @@ struct Oracle {
           double convEd2, dcn;
           if (fimp) { convEd2 = -h21 - h22 - h23 + g2; dcn = d11q2 + d22q2 + d33q2; }
           else { convEd2 = -h21 - h22 - h23 + xnu * dcq13 + g2; dcn = d22q2; }
+          if (fexp) {  // clcRhsY_FEXP: the whole viscous term explicit
+            convEd2 = -h21 - h22 - h23 + xnu * (d11q2 + d22q2 + d33q2) + g2;
+            RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2;
+          } else
           RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2 + two * pmBeta * dcn;
           Hist(ic, jc, kc) = convEd2;
         }
@@ -753,7 +790,8 @@ struct Oracle {
   // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:277-325 (clcRhsZ_PIMP); RhsZ is the
   //      ghosted RealHalo in the reference, only its interior is written; fimp:
   //      clcRhsZ_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:124-177) ----
-  void clcRhsZ_PIMP(F3& RhsZ, F3& Hist, bool fimp = false) {
+  void clcRhsZ_PIMP(F3& RhsZ, F3& Hist, int scheme = 1) {
+    const bool fimp = scheme == 2, fexp = scheme == 0;
     double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
     const double g3 = P.gravity[2], xnu = P.xnu;
 #pragma omp parallel for schedule(static)
@@ -780,6 +818,10 @@ struct Oracle {
           double convEd3, dcn;
           if (fimp) { convEd3 = -h31 - h32 - h33 + g3; dcn = d11q3 + d22q3 + d33q3; }
           else { convEd3 = -h31 - h32 - h33 + xnu * dcq13 + g3; dcn = d22q3; }
+          if (fexp) {  // clcRhsZ_FEXP: the whole viscous term explicit
+            convEd3 = -h31 - h32 - h33 + xnu * (d11q3 + d22q3 + d33q3) + g3;
+            RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3;
+          } else
           RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3 + two * pmBeta * dcn;
           Hist(ic, jc, kc) = convEd3;
         }
@@ -889,6 +931,25 @@ struct Oracle {
     }
   }
 
+  // ---- src/CFD_2nd/m_TSchemeFIMP_inc.f90:241-257 (the y sweep of clcU1Hat_FIMP_000;
+  //      :614-630 and :1013-1029 for uy and uz) and src/CFD_2nd/m_TSchemePIMP_inc.f90:
+  //      435-461, 594-621, 745-771 (clcU1/2/3Hat_PIMP_0): periodic y, constant
+  //      coefficients, u = u + the solution ----
+  void clcUHat_y_periodic(F3& u, F3& Rhs) {
+    const double mjc = -pmBeta * rdy2, pjc = -pmBeta * rdy2, cjc = pmBeta * rdy2 * two + one;
+#pragma omp parallel
+    {
+      std::vector<double> a, b, c, d, line(nyc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int jc = 1; jc <= nyc; ++jc) line[jc - 1] = Rhs(ic, jc, kc);
+          InversePTriFixedCoe1(mjc, cjc, pjc, line.data(), nyc, 1, a, b, c, d);
+          for (int jc = 1; jc <= nyc; ++jc) u(ic, jc, kc) = u(ic, jc, kc) + line[jc - 1];
+        }
+    }
+  }
+
   // ---- src/CFD_2nd/m_TScheme.f90:245-276 (clcPrSrc_FIMP): clcPrSrcOther plus
   //      pressure += -xnu/2 * div ----
   double clcPrSrc_FIMP(F3& prsrc) {
@@ -917,7 +978,16 @@ struct Oracle {
     return m;
   }
 
-  // ---- src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386 (PressureUpdate_FIMP) ----
+  // ---- src/CFD_2nd/m_TSchemeFEXP_inc.f90:391-488 (clcU1/2/3Hat_FEXP): u = u + Rhs ----
+  void clcUHat_FEXP(F3& u, F3& Rhs) {
+#pragma omp parallel for schedule(static)
+    for (int kc = 1; kc <= nzc; ++kc)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) u(ic, jc, kc) = u(ic, jc, kc) + Rhs(ic, jc, kc);
+  }
+
+  // ---- src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386 (PressureUpdate_FIMP), and
+  //      src/CFD_2nd/m_TSchemeFEXP_inc.f90:513-528 (PressureUpdate_FEXP, the same) ----
   void PressureUpdate_FIMP(const F3& phi) {
 #pragma omp parallel for schedule(static)
     for (int kc = 1; kc <= nzc; ++kc)
@@ -1357,7 +1427,8 @@ struct Oracle {
   }
 
   // ---- src/CFD_2nd/m_Poisson.f90:1078-1201 (clcPPE_z1: z R2HC, x R2HC, per-slot
-  //      y tridiagonal with the (1,1,1) pin, x HC2R, z HC2R, * normfft) ----
+  //      y tridiagonal with the (1,1,1) pin, x HC2R, z HC2R, * normfft); with y
+  //      periodic :954-1073 (clcPPE_z1_periodic: the same with cyclic y systems) ----
   void clcPPE(F3& prsrc, F3& prphiHalo) {
     // forward z transform of every (i,j) line
 #pragma omp parallel
@@ -1383,7 +1454,7 @@ struct Oracle {
     // y tridiagonal per (ic,kc) slot
 #pragma omp parallel
     {
-      std::vector<double> a(nyc), b(nyc), c(nyc), f(nyc), arr(nyc);
+      std::vector<double> a(nyc), b(nyc), c(nyc), f(nyc), arr(nyc), a2(nyc), a3(nyc);
 #pragma omp for schedule(static)
       for (int kc = 1; kc <= nzc; ++kc)
         for (int ic = 1; ic <= nxc; ++ic) {
@@ -1394,7 +1465,10 @@ struct Oracle {
             f[jc - 1] = prsrc(ic, jc, kc);
           }
           if (ic == 1 && kc == 1) { c[0] = zero; b[0] = one; a[0] = zero; f[0] = zero; }
-          InverseTridiagonal1(a.data(), b.data(), c.data(), f.data(), nyc, arr.data());
+          if (yper())  // clcPPE_z1_periodic (src/CFD_2nd/m_Poisson.f90:996-1052)
+            InversePeriodicTridiagonal1(a.data(), b.data(), c.data(), f.data(), nyc, arr.data(), a2.data(), a3.data());
+          else
+            InverseTridiagonal1(a.data(), b.data(), c.data(), f.data(), nyc, arr.data());
           for (int jc = 1; jc <= nyc; ++jc) prsrc(ic, jc, kc) = f[jc - 1];
         }
     }
@@ -1761,7 +1835,7 @@ struct Oracle {
   // 5: FluidVelUpdate; 6: PressureUpdate + SetBC_and_UpdateHalo(u) + ..._pr(p)
   void stage(int st, int ns) {
     if (o4) { stage4(st, ns); return; }
-    const bool fimp = P.IsImplicit == 2;
+    const bool fimp = P.IsImplicit == 2, fexp = P.IsImplicit == 0;
     const bool les = P.LES_type > 0;
     switch (st) {
       case 0: PMcoeUpdate(ns); Update_uy_ym(); break;
@@ -1772,9 +1846,9 @@ struct Oracle {
           clcRhsZ_PIMP_LES(RealHalo, HistZ);
           break;
         }
-        clcRhsX_PIMP(RealArr1, HistX, fimp);
-        clcRhsY_PIMP(RealArr2, HistY, fimp);
-        clcRhsZ_PIMP(RealHalo, HistZ, fimp);
+        clcRhsX_PIMP(RealArr1, HistX, P.IsImplicit);
+        clcRhsY_PIMP(RealArr2, HistY, P.IsImplicit);
+        clcRhsZ_PIMP(RealHalo, HistZ, P.IsImplicit);
         break;
       case 2:
         if (les) {
@@ -1783,7 +1857,14 @@ struct Oracle {
           clcUHat_PIMP_LES(2, uz, RealHalo);
           break;
         }
+        if (fexp) { clcUHat_FEXP(ux, RealArr1); clcUHat_FEXP(uy, RealArr2); clcUHat_FEXP(uz, RealHalo); break; }
         if (fimp) { clcUHat_FIMP_xz(RealArr1); clcUHat_FIMP_xz(RealArr2); clcUHat_FIMP_xz(RealHalo); }
+        if (yper()) {  // clcU1/2/3Hat_FIMP_000 (after the x and z sweeps) or clcU1/2/3Hat_PIMP_0
+          clcUHat_y_periodic(ux, RealArr1);
+          clcUHat_y_periodic(uy, RealArr2);
+          clcUHat_y_periodic(uz, RealHalo);
+          break;
+        }
         clcUHat_PIMP_c(ux, RealArr1);
         clcU2Hat_PIMP(RealArr2);
         clcUHat_PIMP_c(uz, RealHalo);
@@ -1799,7 +1880,7 @@ struct Oracle {
       case 5: FluidVelUpdate(RealHalo); break;
       case 6:
         if (les) PressureUpdate_PIMP_LES(RealHalo);
-        else if (fimp) PressureUpdate_FIMP(RealHalo);
+        else if (fimp || fexp) PressureUpdate_FIMP(RealHalo);  // PressureUpdate_FEXP is the same update
         else PressureUpdate_PIMP(RealHalo);
         SetBC_and_UpdateHalo();
         SetBC_and_UpdateHalo_pr(pressure);

@@ -47,8 +47,14 @@ def test_invalid_configs_fail_cleanly(built):
     from channel3d_b200 import _lib
     lib = _lib.load_library()
     yp = np.linspace(0, 2, 13)
-    for change, code in ((dict(nxc=15), _lib.CH3D_ERR_INVALID), (dict(IsImplicit=0), _lib.CH3D_ERR_UNSUPPORTED),
+    for change, code in ((dict(nxc=15), _lib.CH3D_ERR_INVALID), (dict(IsImplicit=3), _lib.CH3D_ERR_UNSUPPORTED),
+                         (dict(IsImplicit=0, precision="mixed"), _lib.CH3D_ERR_UNSUPPORTED),
+                         (dict(IsImplicit=0, order=4), _lib.CH3D_ERR_UNSUPPORTED),
                          (dict(BcOption=[-1, -1, -1, -1, 0, 0]), _lib.CH3D_ERR_UNSUPPORTED),
+                         # periodic y: both sides ("Periodic Bc Wrong"), and only the FP64 2nd-order step without LES
+                         (dict(BcOption=[0, 0, 0, -1, 0, 0], IsImplicit=2), _lib.CH3D_ERR_INVALID),
+                         (dict(BcOption=[0, 0, 0, 0, 0, 0], LES_type=2), _lib.CH3D_ERR_UNSUPPORTED),
+                         (dict(BcOption=[0, 0, 0, 0, 0, 0], IsImplicit=2, precision="mixed"), _lib.CH3D_ERR_UNSUPPORTED),
                          (dict(dtMax=-1.0), _lib.CH3D_ERR_INVALID)):
         cfg = small_channel(16, 12, 8).copy(**change)
         c = cfg.to_c()
@@ -149,6 +155,18 @@ def test_prm_reader_reads_reference_decks():
     assert (cfg.nxc, cfg.nyc, cfg.nzc) == (256, 150, 256)
     assert cfg.IsImplicit == 1 and cfg.BcOption == [0, 0, -1, -1, 0, 0]
     assert cfg.nycSection == [75, 75] and cfg.StretType == [1, 1]
+    # the Taylor-Green deck (explicit, triply periodic) passes the library's
+    # argument checks: ch3d_create gets as far as the device
+    import ctypes
+    from channel3d_b200 import _lib, mesh_y
+    tg = ChannelConfig.from_prm(os.path.join(REF_DECKS, "TaylorGreenVortex.prm"))
+    assert tg.IsImplicit == 0 and tg.BcOption == [0, 0, 0, 0, 0, 0] and tg.FlowType == 3
+    lib = _lib.load_library()
+    c, h = tg.to_c(), ctypes.c_void_p()
+    rc = lib.ch3d_create(ctypes.byref(c), _lib.dptr(mesh_y(tg)), ctypes.byref(h))
+    assert rc in (_lib.CH3D_OK, _lib.CH3D_ERR_CUDA), (rc, lib.ch3d_last_error())
+    if h.value:
+        lib.ch3d_destroy(h)
 
 
 def test_restart_roundtrip_and_size_check(tmp_path):

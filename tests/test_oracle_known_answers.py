@@ -390,3 +390,45 @@ def test_oracle_tg_dissipation_known_answer():
         eps = o.dissipation()
         assert abs(eps / (cfg.xnu * (s * s / 2 + c * c / 4)) - 1.0) < 1e-13, (n, eps)
 
+
+
+def test_poisson_residual_periodic_y():
+    """clcPPE_z1_periodic (src/CFD_2nd/m_Poisson.f90:954-1073): with y periodic
+    the operator is the 3-point Laplacian in all three directions; for a source
+    of zero mean the pinned (0,0) system also satisfies its first row, so the
+    residual vanishes everywhere."""
+    from channel3d_b200 import workloads
+    from oracle import oracle as O
+    cfg = workloads.taylor_green_periodic(16).copy(nxc=24, nyc=20, nzc=12, nycSection=[20])
+    o = O.Oracle(cfg)
+    src = np.random.default_rng(4).standard_normal(cfg.shape)
+    src -= src.mean()
+    phi = o.poisson(src)
+    r2 = [(cfg.nxc / cfg.xlx) ** 2, (cfg.nyc / cfg.yly) ** 2, (cfg.nzc / cfg.zlz) ** 2]
+    L = sum((np.roll(phi, 1, a) - 2 * phi + np.roll(phi, -1, a)) * r2[2 - a] for a in range(3))
+    assert np.abs(L - src).max() < 1e-10 * np.abs(src).max()
+    assert abs(phi[:, 0, :].mean()) < 1e-12 * np.abs(phi).max()
+
+
+@pytest.mark.parametrize("implicit", [1, 2])
+def test_oracle_periodic_box_mirrors_free_slip_half_box(implicit):
+    """The Taylor-Green field is mirror-symmetric about y = 0 and pi, the planes
+    where the free-slip walls of the half-period box sit: 20 steps of the
+    triply periodic box (clcU*Hat_PIMP_0 or clcU*Hat_FIMP_000,
+    clcPPE_z1_periodic) equal, on its lower half, those of the 2pi x pi x 2pi
+    box with free-slip walls (clcU*Hat_PIMP or clcU*Hat_FIMP_010), to rounding."""
+    from channel3d_b200 import initfield, workloads
+    from oracle import oracle as O
+    n = 16
+    out = []
+    for cfg in (workloads.taylor_green_periodic(n, dt=0.02).copy(IsImplicit=implicit),
+                workloads.taylor_green(n, dt=0.02).copy(IsImplicit=implicit)):
+        o = O.Oracle(cfg)
+        o.set_state(*initfield.taylor_green(cfg, yp=o.mesh()[0]))
+        info = o.step(20)
+        assert info["divmax2"] < 1e-13
+        out.append((o.get_state(), o.dissipation()))
+    (a, ea), (b, eb) = out
+    for k in ("ux", "uy", "uz", "p"):
+        assert np.abs(a[k][:, :n // 2, :] - b[k]).max() < 1e-13 * max(1.0, np.abs(b[k]).max()), k
+    assert abs(ea / eb - 1.0) < 1e-12

@@ -232,9 +232,9 @@ int check_config(const ch3d_config* g) {
     if (g->LES_type != CH3D_LES_WALE && g->LES_type != CH3D_LES_MTS && g->LES_type != CH3D_LES_SMAG_VD &&
         g->LES_type != CH3D_LES_MLP)
       return fail(CH3D_ERR_UNSUPPORTED, "LES_type=%d not built", g->LES_type);
-    if (g->order != 2 || g->IsImplicit != 1)
-      return fail(CH3D_ERR_UNSUPPORTED, "LES is built for the 2nd-order partially implicit step (the reference "
-                  "has no FIMP+LES either)");
+    if (g->order != 2 || g->IsImplicit == 2)
+      return fail(CH3D_ERR_UNSUPPORTED, "LES is built for the 2nd-order partially implicit and explicit steps (the "
+                  "reference has no FIMP+LES either)");
     if (g->LES_type == CH3D_LES_MTS && g->FilterType != 0 && g->FilterType != 1)
       return fail(CH3D_ERR_INVALID, "unrecognized FilterType");
   }
@@ -475,9 +475,9 @@ int record_step(ch3d_ctx* c) {
     CU(launch_substep_setup(c, ns));
     if (march_path(c)) {  // RHS + y solves as one column march, its own Thomas factors
       CU(launch_rhs_march(c));
-    } else if (c->cfg.LES_type > 0) {  // the LES y solves form their own coefficients
+    } else if (c->cfg.LES_type > 0) {  // the LES y solves form their own coefficients (FEXP: none)
       CU(launch_rhs_les(c));
-      CU(launch_uhat_les(c));
+      CU(c->cfg.IsImplicit == 0 ? launch_uhat_fexp(c) : launch_uhat_les(c));
     } else if (fimp) {
       if (!y_periodic(c)) CU(launch_helm_factors(c));
       CU(launch_rhs_fimp(c));
@@ -848,8 +848,8 @@ int ch3d_stage(ch3d_ctx* c, int stage, int ns) {
       else CU(c->cfg.order == 4 ? launch_rhs4(c) : (c->cfg.IsImplicit != 1 ? launch_rhs_fimp(c) : launch_rhs(c)));
       break;
     case 2:
-      if (c->cfg.LES_type > 0) { CU(launch_uhat_les(c)); break; }
       if (c->cfg.IsImplicit == 0) { CU(launch_uhat_fexp(c)); break; }
+      if (c->cfg.LES_type > 0) { CU(launch_uhat_les(c)); break; }
       if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) CU(launch_ptri_xz(c));
       if (y_periodic(c)) { CU(launch_ptri_y(c)); break; }
       CU(launch_helm_factors(c));
@@ -1144,7 +1144,7 @@ int ch3d_kernel_times(ch3d_ctx* c, int nsteps, double* out, int nout) {
         CU(mark(1)); CU(done());
       } else if (c->cfg.LES_type > 0) {
         CU(mark(0)); CU(launch_rhs_les(c)); CU(done());
-        CU(mark(1)); CU(launch_uhat_les(c)); CU(done());
+        CU(mark(1)); CU(c->cfg.IsImplicit == 0 ? launch_uhat_fexp(c) : launch_uhat_les(c)); CU(done());
       } else if (c->cfg.order == 2 && c->cfg.IsImplicit == 2) {
         CU(mark(0)); CU(launch_rhs_fimp(c)); CU(done());
         CU(mark(1)); CU(launch_ptri_xz(c)); CU(y_periodic(c) ? launch_ptri_y(c) : launch_uhat(c)); CU(done());

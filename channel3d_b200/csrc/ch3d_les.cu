@@ -198,6 +198,9 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<T> g, Metrics<double> m, co
   const double pmGamma = sc->pmGamma, pmTheta = sc->pmTheta, pmAlpha = sc->pmAlpha, pmBetaT = sc->pmBetaT;
   const double rdx = g.rdx, rdz = g.rdz, rdx2 = g.rdx2, rdz2 = g.rdz2;
   const double qdx1 = 0.25 * rdx, qdx3 = 0.25 * rdz;
+  // the explicit scheme (clcRhsX/Y/Z_FEXP_LES, src/CFD_2nd/m_TSchemeFEXP_inc.f90:80-155,
+  // 213-271, 329-386): the same terms, the y viscous term inside convEd, no pmBetaT term
+  const bool fexp = g.implicit == 0;
   auto N = [&](long long o, int dj) { return nut_at(nut, g, n, o, dj); };
   {  // RhsX (m_TSchemePIMP_inc.f90:80-156)
     const double sucaj = 0.25 * m.rdyp[jc];
@@ -220,12 +223,13 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<T> g, Metrics<double> m, co
     const double sgs3 = rdx * rdz * (visd * (at(uz, n, n.zp) - at(uz, n, n.xm + n.zp)) - visc * (at(uz, n, 0) - at(uz, n, n.xm)));
     const double d22q1 = m.ap2c[jc] * visb * (u_jp - u_c) - m.am2c[jc] * visa * (u_c - u_jm);
     const double d33q1 = g.ap3c * visd * (u_kp - u_c) - g.am3c * visc * (u_c - u_km);
-    const double dcq13 = sgs1 + d33q1;
+    const double dcq13 = fexp ? sgs1 + d22q1 + d33q1 : sgs1 + d33q1;  // FEXP: the y term explicit too
     const double gradp1 = (at(pr, n, 0) - at(pr, n, n.xm)) * rdx;
     const double conv = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + g.g1 + f1;
     const double ho = hx[n.c];
     hx[n.c] = (T)conv;
-    rx[n.c] = (T)(pmGamma * conv + pmTheta * ho - pmAlpha * gradp1 + 2.0 * pmBetaT * d22q1 + sc->dpmdxns);
+    const double r = pmGamma * conv + pmTheta * ho - pmAlpha * gradp1;
+    rx[n.c] = (T)((fexp ? r : r + 2.0 * pmBetaT * d22q1) + sc->dpmdxns);
   }
   {  // RhsY (:214-272)
     const double sucac = m.rdyc[jc], qsucac = 0.25 * sucac;
@@ -247,12 +251,13 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<T> g, Metrics<double> m, co
     const double sgs3 = rdz * sucac * (visd * (at(uz, n, n.zp) - at_jm(uz, g, 2, n, n.zp)) - visc * (at(uz, n, 0) - at_jm(uz, g, 2, n, 0)));
     const double d11q2 = g.ap1c * visb * (v_ip - v_c) - g.am1c * visa * (v_c - v_im);
     const double d33q2 = g.ap3c * visd * (v_kp - v_c) - g.am3c * visc * (v_c - v_km);
-    const double dcq13 = d11q2 + d33q2;
+    const double dcq13 = fexp ? d11q2 + sgs2 + d33q2 : d11q2 + d33q2;
     const double gradp2 = (at(pr, n, 0) - at_jm(pr, g, 3, n, 0)) * sucac;
     const double conv = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + g.g2 + f2;
     const double ho = hy[n.c];
     hy[n.c] = (T)conv;
-    ry[n.c] = (T)(pmGamma * conv + pmTheta * ho - pmAlpha * gradp2 + 2.0 * pmBetaT * sgs2);
+    const double r = pmGamma * conv + pmTheta * ho - pmAlpha * gradp2;
+    ry[n.c] = (T)(fexp ? r : r + 2.0 * pmBetaT * sgs2);
   }
   {  // RhsZ (:330-387)
     const double sucaj = 0.25 * m.rdyp[jc];
@@ -275,12 +280,13 @@ __global__ void __launch_bounds__(256) k_rhs_les(Geo<T> g, Metrics<double> m, co
     const double sgs3 = rdz2 * (n_c * (w_kp - w_c) - n_km * (w_c - w_km));
     const double d11q3 = g.ap1c * visb * (w_ip - w_c) - g.am1c * visa * (w_c - w_im);
     const double d22q3 = m.ap2c[jc] * visd * (w_jp - w_c) - m.am2c[jc] * visc * (w_c - w_jm);
-    const double dcq13 = d11q3 + sgs3;
+    const double dcq13 = fexp ? d11q3 + d22q3 + sgs3 : d11q3 + sgs3;
     const double gradp3 = (at(pr, n, 0) - at(pr, n, n.zm)) * rdz;
     const double conv = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + g.g3 + f3;
     const double ho = hz[n.c];
     hz[n.c] = (T)conv;
-    rz[n.c] = (T)(pmGamma * conv + pmTheta * ho - pmAlpha * gradp3 + 2.0 * pmBetaT * d22q3);
+    const double r = pmGamma * conv + pmTheta * ho - pmAlpha * gradp3;
+    rz[n.c] = (T)(fexp ? r : r + 2.0 * pmBetaT * d22q3);
   }
 }
 

@@ -1140,7 +1140,7 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
     ux[idx] = uxn;
     uy[idx] = uyn;
     uz[idx] = uzn;
-    if (mode == 0 && g.les) {  // PressureUpdate_PIMP_LES (src/CFD_2nd/m_TSchemePIMP_inc.f90:878-904)
+    if (mode == 0 && g.les && g.implicit == 1) {  // PressureUpdate_PIMP_LES (src/CFD_2nd/m_TSchemePIMP_inc.f90:878-904)
       const T phip_y = phi[i + (long long)nx * ((j < ny - 1 ? j + 1 : ny - 1) + (long long)ny * k)];
       const T nc = nut[idx];
       const T njp = j < ny - 1 ? nut[idx + nx] : (g.bc.hi == -1 ? (T)2 * g.xnu - nc : nc);
@@ -1153,8 +1153,8 @@ __global__ void __launch_bounds__(256) k_proj(Geo<T> g, Metrics<T> m, const T* u
       const T pmBetac = -(pmBetap + pmBetam) + (T)1;
       pr[idx] = pr[idx] + pmBetap * phip_y + pmBetac * phic + pmBetam * phim_y;
     } else if (mode == 0 && (g.implicit == 2 || g.implicit == 0)) {
-      // PressureUpdate_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386), _FEXP
-      // (src/CFD_2nd/m_TSchemeFEXP_inc.f90:513-528)
+      // PressureUpdate_FIMP (src/CFD_2nd/m_TSchemeFIMP_inc.f90:1371-1386), _FEXP and
+      // _FEXP_LES (src/CFD_2nd/m_TSchemeFEXP_inc.f90:513-548)
       pr[idx] = pr[idx] + phic;
     } else if (mode == 0) {
       const int jp = j < ny - 1 ? j + 1 : (g.bc.hi == 0 ? 0 : ny - 1);  // phi(ic,nyp,kc): Neumann or periodic halo

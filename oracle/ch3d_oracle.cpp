@@ -1215,8 +1215,10 @@ struct Oracle {
     return sgs_f[q * N + (size_t)(ic - 1) + (size_t)nxc * ((size_t)(jc - 1) + (size_t)nyc * (kc - 1))];
   }
 
-  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:80-156 (clcRhsX_PIMP_LES) ----
-  void clcRhsX_PIMP_LES(F3& RhsX, F3& Hist) {
+  // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:80-156 (clcRhsX_PIMP_LES); fexp:
+  //      src/CFD_2nd/m_TSchemeFEXP_inc.f90:80-155 (clcRhsX_FEXP_LES), the y
+  //      viscous term inside convEd1 and no pmBetaT term ----
+  void clcRhsX_PIMP_LES(F3& RhsX, F3& Hist, bool fexp = false) {
     double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
     std::vector<double> part(nzc + 1, 0.0);
 #pragma omp parallel for schedule(static)
@@ -1245,11 +1247,12 @@ struct Oracle {
           double d11q1 = sgs1;
           double d22q1 = ap2c(jc) * visb * (ux(ic, jp, kc) - ux(ic, jc, kc)) - am2c(jc) * visa * (ux(ic, jc, kc) - ux(ic, jm, kc));
           double d33q1 = ap3c(kc) * visd * (ux(ic, jc, kp) - ux(ic, jc, kc)) - am3c(kc) * visc * (ux(ic, jc, kc) - ux(ic, jc, km));
-          double dcq13 = d11q1 + d33q1;
+          double dcq13 = fexp ? d11q1 + d22q1 + d33q1 : d11q1 + d33q1;
           double gradp1 = (pressure(ic, jc, kc) - pressure(im, jc, kc)) * rdx;
           s1tot = s1tot + ux(ic, jc, kc) * s1totCoe;
           double convEd1 = -h11 - h12 - h13 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[0] + sgsf(0, ic, jc, kc);
-          RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1 + two * pmBetaT * d22q1;
+          RhsX(ic, jc, kc) = pmGamma * convEd1 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp1;
+          if (!fexp) RhsX(ic, jc, kc) = RhsX(ic, jc, kc) + two * pmBetaT * d22q1;
           Hist(ic, jc, kc) = convEd1;
         }
       }
@@ -1269,7 +1272,7 @@ struct Oracle {
   }
 
   // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:214-272 (clcRhsY_PIMP_LES) ----
-  void clcRhsY_PIMP_LES(F3& RhsY, F3& Hist) {
+  void clcRhsY_PIMP_LES(F3& RhsY, F3& Hist, bool fexp = false) {
     double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
 #pragma omp parallel for schedule(static)
     for (int kc = 1; kc <= nzc; ++kc) {
@@ -1295,10 +1298,11 @@ struct Oracle {
           double d11q2 = ap1c(ic) * visb * (uy(ip, jc, kc) - uy(ic, jc, kc)) - am1c(ic) * visa * (uy(ic, jc, kc) - uy(im, jc, kc));
           double d22q2 = sgs2;
           double d33q2 = ap3c(kc) * visd * (uy(ic, jc, kp) - uy(ic, jc, kc)) - am3c(kc) * visc * (uy(ic, jc, kc) - uy(ic, jc, km));
-          double dcq13 = d11q2 + d33q2;
+          double dcq13 = fexp ? d11q2 + d22q2 + d33q2 : d11q2 + d33q2;
           double gradp2 = (pressure(ic, jc, kc) - pressure(ic, jm, kc)) * sucac;
           double convEd2 = -h21 - h22 - h23 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[1] + sgsf(1, ic, jc, kc);
-          RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2 + two * pmBetaT * d22q2;
+          RhsY(ic, jc, kc) = pmGamma * convEd2 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp2;
+          if (!fexp) RhsY(ic, jc, kc) = RhsY(ic, jc, kc) + two * pmBetaT * d22q2;
           Hist(ic, jc, kc) = convEd2;
         }
       }
@@ -1306,7 +1310,7 @@ struct Oracle {
   }
 
   // ---- src/CFD_2nd/m_TSchemePIMP_inc.f90:330-387 (clcRhsZ_PIMP_LES) ----
-  void clcRhsZ_PIMP_LES(F3& RhsZ, F3& Hist) {
+  void clcRhsZ_PIMP_LES(F3& RhsZ, F3& Hist, bool fexp = false) {
     double qdx1 = quarter * rdx, qdx3 = quarter * rdz;
 #pragma omp parallel for schedule(static)
     for (int kc = 1; kc <= nzc; ++kc) {
@@ -1332,10 +1336,11 @@ struct Oracle {
           double d11q3 = ap1c(ic) * visb * (uz(ip, jc, kc) - uz(ic, jc, kc)) - am1c(ic) * visa * (uz(ic, jc, kc) - uz(im, jc, kc));
           double d22q3 = ap2c(jc) * visd * (uz(ic, jp, kc) - uz(ic, jc, kc)) - am2c(jc) * visc * (uz(ic, jc, kc) - uz(ic, jm, kc));
           double d33q3 = sgs3;
-          double dcq13 = d11q3 + d33q3;
+          double dcq13 = fexp ? d11q3 + d22q3 + d33q3 : d11q3 + d33q3;
           double gradp3 = (pressure(ic, jc, kc) - pressure(ic, jc, km)) * rdz;
           double convEd3 = -h31 - h32 - h33 + sgs1 + sgs2 + sgs3 + dcq13 + P.gravity[2] + sgsf(2, ic, jc, kc);
-          RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3 + two * pmBetaT * d22q3;
+          RhsZ(ic, jc, kc) = pmGamma * convEd3 + pmTheta * Hist(ic, jc, kc) - pmAlpha * gradp3;
+          if (!fexp) RhsZ(ic, jc, kc) = RhsZ(ic, jc, kc) + two * pmBetaT * d22q3;
           Hist(ic, jc, kc) = convEd3;
         }
       }
@@ -1841,9 +1846,9 @@ struct Oracle {
       case 0: PMcoeUpdate(ns); Update_uy_ym(); break;
       case 1:
         if (les) {
-          clcRhsX_PIMP_LES(RealArr1, HistX);
-          clcRhsY_PIMP_LES(RealArr2, HistY);
-          clcRhsZ_PIMP_LES(RealHalo, HistZ);
+          clcRhsX_PIMP_LES(RealArr1, HistX, fexp);
+          clcRhsY_PIMP_LES(RealArr2, HistY, fexp);
+          clcRhsZ_PIMP_LES(RealHalo, HistZ, fexp);
           break;
         }
         clcRhsX_PIMP(RealArr1, HistX, P.IsImplicit);
@@ -1851,13 +1856,13 @@ struct Oracle {
         clcRhsZ_PIMP(RealHalo, HistZ, P.IsImplicit);
         break;
       case 2:
+        if (fexp) { clcUHat_FEXP(ux, RealArr1); clcUHat_FEXP(uy, RealArr2); clcUHat_FEXP(uz, RealHalo); break; }
         if (les) {
           clcUHat_PIMP_LES(0, ux, RealArr1);
           clcUHat_PIMP_LES(1, uy, RealArr2);
           clcUHat_PIMP_LES(2, uz, RealHalo);
           break;
         }
-        if (fexp) { clcUHat_FEXP(ux, RealArr1); clcUHat_FEXP(uy, RealArr2); clcUHat_FEXP(uz, RealHalo); break; }
         if (fimp) { clcUHat_FIMP_xz(RealArr1); clcUHat_FIMP_xz(RealArr2); clcUHat_FIMP_xz(RealHalo); }
         if (yper()) {  // clcU1/2/3Hat_FIMP_000 (after the x and z sweeps) or clcU1/2/3Hat_PIMP_0
           clcUHat_y_periodic(ux, RealArr1);
@@ -1879,7 +1884,7 @@ struct Oracle {
         break;
       case 5: FluidVelUpdate(RealHalo); break;
       case 6:
-        if (les) PressureUpdate_PIMP_LES(RealHalo);
+        if (les && !fexp) PressureUpdate_PIMP_LES(RealHalo);
         else if (fimp || fexp) PressureUpdate_FIMP(RealHalo);  // PressureUpdate_FEXP is the same update
         else PressureUpdate_PIMP(RealHalo);
         SetBC_and_UpdateHalo();

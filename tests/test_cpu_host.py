@@ -50,6 +50,7 @@ def test_invalid_configs_fail_cleanly(built):
     for change, code in ((dict(nxc=15), _lib.CH3D_ERR_INVALID), (dict(IsImplicit=3), _lib.CH3D_ERR_UNSUPPORTED),
                          (dict(IsImplicit=0, precision="mixed"), _lib.CH3D_ERR_UNSUPPORTED),
                          (dict(IsImplicit=0, order=4), _lib.CH3D_ERR_UNSUPPORTED),
+                         (dict(IsImplicit=2, LES_type=2), _lib.CH3D_ERR_UNSUPPORTED),  # no FIMP+LES
                          (dict(BcOption=[-1, -1, -1, -1, 0, 0]), _lib.CH3D_ERR_UNSUPPORTED),
                          # periodic y: both sides ("Periodic Bc Wrong"), and only the FP64 2nd-order step without LES
                          (dict(BcOption=[0, 0, 0, -1, 0, 0], IsImplicit=2), _lib.CH3D_ERR_INVALID),

@@ -1,7 +1,8 @@
 """The explicit 2nd-order step (IsImplicit 0: clcRhsX/Y/Z_FEXP with the whole
 viscous term explicit, clcU1/2/3Hat_FEXP u* = u + Rhs, clcPrSrcOther and
 PressureUpdate_FEXP p += phi; src/CFD_2nd/m_TSchemeFEXP_inc.f90) in the channel
-between no-slip walls and in the half channel with a free-slip top, on the
+between no-slip walls, in the half channel with a free-slip top and with the
+LES eddy viscosities (the _FEXP_LES right-hand sides), on the
 device against the CPU oracle, FP64, through the C ABI; and the reference's
 own Taylor-Green input (Input/TaylorGreenVortex.prm: explicit, triply
 periodic, xnu 6.25e-4, dt 0.01) at 64^3.
@@ -107,3 +108,49 @@ def test_reference_tg_input_fexp(built):
     for k in ("ux", "uy", "uz", "p"):
         assert rel_l2(gs[k], go[k]) < 1e-10, (k, rel_l2(gs[k], go[k]))
     assert abs(eps / o.dissipation() - 1.0) < 1e-12
+
+
+def _les(model, nx=32, ny=24, nz=16):
+    from channel3d_b200 import workloads
+    cfg, _ = workloads.get("channel48_les")
+    return cfg.copy(nxc=nx, nyc=ny, nzc=nz, nycSection=[ny // 2, ny - ny // 2], LES_type=model, Cs=0.1,
+                    IsImplicit=0, dtMax=2e-4)
+
+
+@pytest.mark.parametrize("model", (2, 3, 10))
+def test_les_fexp_parity(built, model):
+    """clcRhsX/Y/Z_FEXP_LES (src/CFD_2nd/m_TSchemeFEXP_inc.f90:80-386) with the
+    WALE, mixed-time-scale and Smagorinsky / van Driest eddy viscosities: stage
+    by stage at 32 x 24 x 16, then 20 whole steps, against the oracle."""
+    o, s = _pair(_les(model))
+    s.sgs_viscosity()
+    o.sgs()
+    for ns in (1, 2, 3):
+        o.stage(0, ns); s.stage(0, ns)
+        o.stage(1, ns); s.stage(1, ns)
+        for wo, wg in ((o.ARR1, s.RHSX), (o.ARR2, s.RHSY), (o.HALO, s.RHSZ), (o.HISTX, s.HISTX),
+                       (o.HISTY, s.HISTY), (o.HISTZ, s.HISTZ)):
+            a, b = s.get_array(wg), o.get_interior(wo)
+            assert rel_max(a, b) < 5e-12, (ns, wg, rel_max(a, b))
+        o.stage(2, ns); s.stage(2, ns)
+        o.stage(3, ns); s.stage(3, ns)
+        go = o.get_state()
+        for k, w in (("ux", 12), ("uy", 13), ("uz", 14)):
+            assert rel_max(s.get_array(w), go[k]) < 1e-12, (ns, "uhat", k)
+        o.stage(4, ns); s.stage(4, ns)
+        assert rel_l2(s.get_array(s.PRPHI), o.get_interior(o.HALO)) < 5e-11, (ns, "phi")
+        o.stage(5, ns); s.stage(5, ns)
+        o.stage(6, ns); s.stage(6, ns)
+        go, gs = o.get_state(), s.download()
+        for k in ("ux", "uy", "uz", "p"):
+            tol = 5e-11 if k == "p" else 1e-11
+            assert rel_max(gs[k], go[k]) < tol, (ns, "final", k, rel_max(gs[k], go[k]))
+    s.close()
+    o, s = _pair(_les(model))
+    di = s.step(20)
+    o.step(20)
+    go, gs = o.get_state(), s.download()
+    s.close()
+    for k in ("ux", "uy", "uz", "p"):
+        assert rel_l2(gs[k], go[k]) < 1e-10, (k, rel_l2(gs[k], go[k]))
+    assert di["divmax2"] < 1e-12

@@ -281,6 +281,30 @@ def test_fimp_step_is_divergence_free_and_laminar_steady(built):
     assert abs(d["uxm"] - 1.0) < 0.01 * abs(d0["uxm"] - 1.0)
 
 
+def test_fexp_step_is_divergence_free_and_laminar_steady(built):
+    """The explicit scheme (clcRhsX/Y/Z_FEXP, clcU1/2/3Hat_FEXP,
+    PressureUpdate_FEXP): divergence-free steps from a noisy field; a laminar
+    profile stays a function of y alone with uy = uz = 0, and the bulk
+    controller drives <u> to ubulk."""
+    from channel3d_b200 import initfield
+    from oracle import oracle as O
+    cfg = _cfg_fimp(32, 24, 16).copy(IsImplicit=0, dtMax=2e-4)
+    o = O.Oracle(cfg)
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0])
+    o.set_state(ux, uy, uz, p)
+    d = o.step(3)
+    assert d["divmax2"] < 1e-13 and d["rc"] == 0
+    assert np.all(o.get_state()["uy"][:, 0, :] == 0.0)  # the wall row keeps uy_ym
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=o.mesh()[0], amplitude=0.0)
+    o.set_state(ux, uy, uz, p)
+    d0 = o.step(1)
+    d = o.step(5)
+    s = o.get_state()
+    assert np.abs(s["uy"]).max() < 1e-14 and np.abs(s["uz"]).max() < 1e-14
+    assert np.abs(s["ux"] - s["ux"][:1, :, :1]).max() < 1e-13
+    assert abs(d["uxm"] - 1.0) < 0.01 * abs(d0["uxm"] - 1.0)
+
+
 def _cfg_les(model, nx=24, ny=16, nz=12):
     from channel3d_b200 import workloads
     cfg, _ = workloads.get("channel48_les")

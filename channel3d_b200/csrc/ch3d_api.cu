@@ -213,7 +213,7 @@ int check_config(const ch3d_config* g) {
     return fail(CH3D_ERR_UNSUPPORTED, "the 4th-order solver is built for the channel (FlowType=1, no-slip walls)");
   if (g->nxc < 4 || g->nyc < 4 || g->nzc < 2) return fail(CH3D_ERR_INVALID, "grid too small: %d %d %d", g->nxc, g->nyc, g->nzc);
   if (g->nxc % 2) return fail(CH3D_ERR_INVALID, "nxc must be even (real-to-complex x transform)");
-  if (g->ischeme != 3) return fail(CH3D_ERR_UNSUPPORTED, "only RK3 (ischeme=3) is built");
+  if (g->ischeme < 1 || g->ischeme > 3) return fail(CH3D_ERR_INVALID, "Time scheme WRONG!!! ischeme=%d", g->ischeme);
   if (g->IsImplicit != 1 && !(g->order == 2 && (g->IsImplicit == 2 || g->IsImplicit == 0)))
     return fail(CH3D_ERR_UNSUPPORTED, "IsImplicit=%d not built (PIMP=1; FIMP=2 and FEXP=0 for order 2)", g->IsImplicit);
   if (g->IsImplicit == 0 && g->precision != CH3D_PREC_FP64)
@@ -602,10 +602,20 @@ int ch3d_create(const ch3d_config* cfg, const double* yp, ch3d_ctx** out) {
     delete c;
     return fail(CH3D_ERR_UNSUPPORTED, "nxc/2 and nzc must be products of 2 and 3 (got %d, %d)", cfg->nxc / 2, cfg->nzc);
   }
-  // RK3 constants (src/CFD_2nd/m_Parameters.f90:299-306)
-  c->iadvance = 3;
-  c->gam[0] = 8.0 / 15.0; c->gam[1] = 5.0 / 12.0; c->gam[2] = 3.0 / 4.0;
-  c->the[0] = 0.0; c->the[1] = -17.0 / 60.0; c->the[2] = -5.0 / 12.0;
+  // time-scheme constants (src/CFD_2nd/m_Parameters.f90:135-150; the same in
+  // src/CFD_4th/m_Parameters.f90:158-173): AB2 one substep, RK2 two, RK3 three
+  if (cfg->ischeme == 1) {
+    c->iadvance = 1;
+    c->gam[0] = 1.5; c->the[0] = -0.5;
+  } else if (cfg->ischeme == 2) {
+    c->iadvance = 2;
+    c->gam[0] = 0.5; c->gam[1] = 1.0;
+    c->the[0] = 0.0; c->the[1] = -0.5;
+  } else {
+    c->iadvance = 3;
+    c->gam[0] = 8.0 / 15.0; c->gam[1] = 5.0 / 12.0; c->gam[2] = 3.0 / 4.0;
+    c->the[0] = 0.0; c->the[1] = -17.0 / 60.0; c->the[2] = -5.0 / 12.0;
+  }
   for (int s = 0; s < 3; ++s) c->alp[s] = c->gam[s] + c->the[s];
   c->yp.assign(c->ny + 3, 0.0);
   for (int j = 1; j <= c->ny + 1; ++j) c->yp[j] = yp[j - 1];

@@ -426,7 +426,7 @@ struct Oracle {
     P = *p;
     o4 = (P.order == 4);
     nxc = P.nxc; nyc = P.nyc; nzc = P.nzc; nxp = nxc + 1; nyp = nyc + 1; nzp = nzc + 1;
-    // src/CFD_2nd/m_Parameters.f90:288-306
+    // src/CFD_2nd/m_Parameters.f90:135-150 (ReadAndInitParameters: the time-scheme constants)
     if (P.ischeme == 1) {
       iadvance = 1;
       pmGammaConst[0] = 1.5; pmGammaConst[1] = 0; pmGammaConst[2] = 0;

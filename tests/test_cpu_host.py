@@ -51,6 +51,7 @@ def test_invalid_configs_fail_cleanly(built):
                          (dict(IsImplicit=0, precision="mixed"), _lib.CH3D_ERR_UNSUPPORTED),
                          (dict(IsImplicit=0, order=4), _lib.CH3D_ERR_UNSUPPORTED),
                          (dict(IsImplicit=2, LES_type=2), _lib.CH3D_ERR_UNSUPPORTED),  # no FIMP+LES
+                         (dict(ischeme=4), _lib.CH3D_ERR_INVALID),  # "Time scheme WRONG" 
                          (dict(BcOption=[-1, -1, -1, -1, 0, 0]), _lib.CH3D_ERR_UNSUPPORTED),
                          # periodic y: both sides ("Periodic Bc Wrong"), and only the FP64 2nd-order step without LES
                          (dict(BcOption=[0, 0, 0, -1, 0, 0], IsImplicit=2), _lib.CH3D_ERR_INVALID),

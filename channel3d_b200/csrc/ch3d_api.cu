@@ -216,8 +216,6 @@ int check_config(const ch3d_config* g) {
   if (g->ischeme < 1 || g->ischeme > 3) return fail(CH3D_ERR_INVALID, "Time scheme WRONG!!! ischeme=%d", g->ischeme);
   if (g->IsImplicit != 1 && !(g->order == 2 && (g->IsImplicit == 2 || g->IsImplicit == 0)))
     return fail(CH3D_ERR_UNSUPPORTED, "IsImplicit=%d not built (PIMP=1; FIMP=2 and FEXP=0 for order 2)", g->IsImplicit);
-  if (g->IsImplicit == 0 && g->precision != CH3D_PREC_FP64)
-    return fail(CH3D_ERR_UNSUPPORTED, "the explicit scheme (IsImplicit=0) is built in FP64");
   if (g->BcOption[0] != 0 || g->BcOption[1] != 0 || g->BcOption[4] != 0 || g->BcOption[5] != 0)
     return fail(CH3D_ERR_UNSUPPORTED, "x and z must be periodic (BcOption 1,2,5,6 = 0)");
   if ((g->BcOption[2] == 0) != (g->BcOption[3] == 0)) return fail(CH3D_ERR_INVALID, "Periodic Bc Wrong");

@@ -48,7 +48,8 @@ def test_invalid_configs_fail_cleanly(built):
     lib = _lib.load_library()
     yp = np.linspace(0, 2, 13)
     for change, code in ((dict(nxc=15), _lib.CH3D_ERR_INVALID), (dict(IsImplicit=3), _lib.CH3D_ERR_UNSUPPORTED),
-                         (dict(IsImplicit=0, precision="mixed"), _lib.CH3D_ERR_UNSUPPORTED),
+                         (dict(IsImplicit=0, precision="mixed", BcOption=[0, 0, 0, 0, 0, 0]),
+                          _lib.CH3D_ERR_UNSUPPORTED),  # periodic y is FP64 only
                          (dict(IsImplicit=0, order=4), _lib.CH3D_ERR_UNSUPPORTED),
                          (dict(IsImplicit=2, LES_type=2), _lib.CH3D_ERR_UNSUPPORTED),  # no FIMP+LES
                          (dict(ischeme=4), _lib.CH3D_ERR_INVALID),  # "Time scheme WRONG" 

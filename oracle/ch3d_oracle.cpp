@@ -149,6 +149,37 @@ void hc2r(const FFTPlan& pl, double* x, std::vector<cplx>& bufa, std::vector<cpl
   for (int j = 0; j < n; ++j) x[j] = bufb[j].real();
 }
 
+// cos(pi m / (2n)), m = 0..4n-1: the angles of both cosine transforms of length n
+std::vector<double> dct_table(int n) {
+  std::vector<double> t((size_t)4 * n);
+  for (int m = 0; m < 4 * n; ++m)
+    t[m] = (double)std::cos(3.141592653589793238462643383279502884L * (long double)m / (long double)(2 * n));
+  return t;
+}
+
+// FFTW_REDFT10 (DCT-II) on a contiguous line (in place), unnormalised:
+// Y_k = 2 sum_{j=0}^{n-1} X_j cos(pi (j + 1/2) k / n), the reference's forward
+// transform in a direction between walls (src/CFD_2nd/m_Poisson.f90:267-307).
+void redft10(int n, double* x, const std::vector<double>& tab, std::vector<double>& buf) {
+  buf.assign(x, x + n);
+  for (int k = 0; k < n; ++k) {
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s += buf[j] * tab[(size_t)(((long long)(2 * j + 1) * k) % (4 * n))];
+    x[k] = 2.0 * s;
+  }
+}
+
+// FFTW_REDFT01 (DCT-III), the inverse of REDFT10 up to the factor 2n:
+// Y_k = X_0 + 2 sum_{j=1}^{n-1} X_j cos(pi j (k + 1/2) / n).
+void redft01(int n, double* x, const std::vector<double>& tab, std::vector<double>& buf) {
+  buf.assign(x, x + n);
+  for (int k = 0; k < n; ++k) {
+    double s = 0.0;
+    for (int j = 1; j < n; ++j) s += buf[j] * tab[(size_t)(((long long)j * (2 * k + 1)) % (4 * n))];
+    x[k] = buf[0] + 2.0 * s;
+  }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -381,6 +412,7 @@ struct Oracle {
   }
 
   // ---- src/CFD_2nd/m_Poisson.f90:28-66 (modified wavenumbers, normfft) ----
+  std::vector<double> zcos;  // cosine table of the z transforms between walls
   void InitPoissonSolver() {
     WaveNumX.init(1, nxc); WaveNumZ.init(1, nzc);
     normfft = one;
@@ -389,14 +421,17 @@ struct Oracle {
       WaveNumX(i) = two * rdx2 * (std::cos(wa1) - one);
     }
     normfft = normfft * one * (double)nxc;
+    // z between walls: cosine transform, WaveCoe = pi, norm = 2 (:53-64)
+    const double wcz = zper() ? 2.0 * PI : PI, nrmz = zper() ? one : two;
     for (int k = 1; k <= nzc; ++k) {
-      double wa3 = 2.0 * PI * (double)(k - 1) / (double)nzc;
+      double wa3 = wcz * (double)(k - 1) / (double)nzc;
       WaveNumZ(k) = two * rdz2 * (std::cos(wa3) - one);
     }
-    normfft = normfft * one * (double)nzc;
+    normfft = normfft * nrmz * (double)nzc;
     normfft = one / normfft;
     planx.init(nxc);
     planz.init(nzc);
+    if (!zper()) zcos = dct_table(nzc);
   }
 
   // ---- src/CFD_4th/m_MeshAndMetries.f90:86-91 (4th-order FD constants) ----
@@ -525,8 +560,10 @@ struct Oracle {
         m(i, j, nzc + h) = m(i, j, h);
   }
   bool yper() const { return P.BcOption[2] == 0; }
+  bool zper() const { return P.BcOption[4] == 0; }
 
-  // ---- src/CFD_2nd/m_BC_and_Halo.f90:232-344 (SetBC_and_UpdateHalo), x/z periodic ----
+  // ---- src/CFD_2nd/m_BC_and_Halo.f90:232-344 (SetBC_and_UpdateHalo), x periodic,
+  //      z periodic or between walls ----
   void SetBC_and_UpdateHalo() {
     const int* Bc = P.BcOption;
     if (Bc[3] == -1) {
@@ -561,10 +598,30 @@ struct Oracle {
         uz(i, 0, k) = uz(i, 1, k) - P.uzBcValue[2] * dyp(1);
       }
     }
-    int yh = yper() ? 1 : 0;
-    halo(ux, 1, 1, yh, yh, 1, 1);
-    halo(uy, 1, 1, yh, yh, 1, 1);
-    halo(uz, 1, 1, yh, yh, 1, 1);
+    // z walls (:313-338): ghost planes k = 0 and nzp over i = 1..nxc, j = 0..nyp;
+    // uz's wall faces k = 1 and nzp hold the wall values
+    if (Bc[5] == -1 || Bc[5] == -2) {
+      const bool ns = Bc[5] == -1;
+      for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) {
+        ux(i, j, nzp) = ns ? P.uxBcValue[5] * two - ux(i, j, nzc) : ux(i, j, nzc) + P.uxBcValue[5] * dz;
+        uy(i, j, nzp) = ns ? P.uyBcValue[5] * two - uy(i, j, nzc) : uy(i, j, nzc) + P.uyBcValue[5] * dz;
+        uz(i, j, nzp) = P.uzBcValue[5];
+        uz(i, j, nzp + 1) = P.uzBcValue[5] * two - uz(i, j, nzc);
+      }
+    }
+    if (Bc[4] == -1 || Bc[4] == -2) {
+      const bool ns = Bc[4] == -1;
+      for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) {
+        ux(i, j, 0) = ns ? P.uxBcValue[4] * two - ux(i, j, 1) : ux(i, j, 1) - P.uxBcValue[4] * dz;
+        uy(i, j, 0) = ns ? P.uyBcValue[4] * two - uy(i, j, 1) : uy(i, j, 1) - P.uyBcValue[4] * dz;
+        uz(i, j, 1) = P.uzBcValue[4];
+        uz(i, j, 0) = P.uzBcValue[4] * two - uz(i, j, 2);
+      }
+    }
+    int yh = yper() ? 1 : 0, zh = zper() ? 1 : 0;  // no halo copies across walls
+    halo(ux, 1, 1, yh, yh, zh, zh);
+    halo(uy, 1, 1, yh, yh, zh, zh);
+    halo(uz, 1, 1, yh, yh, zh, zh);
   }
 
   // ---- src/CFD_2nd/m_BC_and_Halo.f90:349-405 (SetBC_and_UpdateHaloForPrSrc) ----
@@ -575,9 +632,13 @@ struct Oracle {
     if (Bc[2] == -1 || Bc[2] == -2)
       for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i)
         uy(i, 1, k) = uy_ym[(size_t)(i - 1) + (size_t)nxc * (k - 1)];
+    if (Bc[5] == -1 || Bc[5] == -2)
+      for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) uz(i, j, nzp) = P.uzBcValue[5];
+    if (Bc[4] == -1 || Bc[4] == -2)
+      for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) uz(i, j, 1) = P.uzBcValue[4];
     halo(ux, 0, 1, 0, 0, 0, 0);
     halo(uy, 0, 0, 0, yper() ? 1 : 0, 0, 0);
-    halo(uz, 0, 0, 0, 0, 0, 1);
+    halo(uz, 0, 0, 0, 0, 0, zper() ? 1 : 0);
   }
 
   // ---- src/CFD_2nd/m_BC_and_Halo.f90:410-456 (SetBC_and_UpdateHalo_pr) ----
@@ -585,8 +646,10 @@ struct Oracle {
     const int* Bc = P.BcOption;
     if (Bc[3] < 0) for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) pr(i, nyp, k) = pr(i, nyc, k);
     if (Bc[2] < 0) for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) pr(i, 0, k) = pr(i, 1, k);
-    int yh = yper() ? 1 : 0;
-    halo(pr, 1, 1, yh, yh, 1, 1);
+    if (Bc[5] < 0) for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) pr(i, j, nzp) = pr(i, j, nzc);
+    if (Bc[4] < 0) for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) pr(i, j, 0) = pr(i, j, 1);
+    int yh = yper() ? 1 : 0, zh = zper() ? 1 : 0;
+    halo(pr, 1, 1, yh, yh, zh, zh);
   }
 
   // ---- src/CFD_2nd/m_Tools.f90:21-46 (CalcMaxCFL) ----
@@ -927,6 +990,54 @@ struct Oracle {
           for (int kc = 1; kc <= nzc; ++kc) line[kc - 1] = Rhs(ic, jc, kc);
           InversePTriFixedCoe1(mkc, ckc, pkc, line.data(), nzc, 1, a, b, c, d);
           for (int kc = 1; kc <= nzc; ++kc) Rhs(ic, jc, kc) = line[kc - 1];
+        }
+    }
+  }
+
+  // ---- the periodic x sweep alone (src/CFD_2nd/m_TSchemeFIMP_inc.f90:375-393 of
+  //      clcU1Hat_FIMP_011, :758-776 and :1165-1183 of the uy and uz routines) ----
+  void clcUHat_FIMP_x(F3& Rhs) {
+    const double mic = -pmBeta * rdx2, pic = -pmBeta * rdx2, cic = pmBeta * rdx2 * two + one;
+#pragma omp parallel
+    {
+      std::vector<double> a, b, c, d, line(nxc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) {
+          for (int ic = 1; ic <= nxc; ++ic) line[ic - 1] = Rhs(ic, jc, kc);
+          InversePTriFixedCoe1(mic, cic, pic, line.data(), nxc, 1, a, b, c, d);
+          for (int ic = 1; ic <= nxc; ++ic) Rhs(ic, jc, kc) = line[ic - 1];
+        }
+    }
+  }
+
+  // ---- the z sweep between walls: ux and uy (src/CFD_2nd/m_TSchemeFIMP_inc.f90:
+  //      395-417, and :778-800 of clcU2Hat_FIMP_011) with the Crank-Nicolson wall
+  //      metrics am3cForCN / ap3cForCN; uz (:1185-1218 of clcU3Hat_FIMP_011) with
+  //      constant coefficients and its wall face k = 1 held (row 1 = identity, zero
+  //      right-hand side) ----
+  void clcUHat_FIMP_zwall(F3& Rhs, bool uzface) {
+    std::vector<double> tm(nzc), tc(nzc), tp(nzc);
+    for (int kc = 1; kc <= nzc; ++kc) {
+      if (uzface) {
+        tm[kc - 1] = -pmBeta * rdz2; tp[kc - 1] = -pmBeta * rdz2; tc[kc - 1] = pmBeta * rdz2 * two + one;
+      } else {
+        tp[kc - 1] = -pmBeta * ap3cForCN(kc);
+        tm[kc - 1] = -pmBeta * am3cForCN(kc);
+        tc[kc - 1] = -tp[kc - 1] - tm[kc - 1] + one;
+      }
+    }
+    if (uzface) { tp[0] = zero; tc[0] = one; tm[0] = zero; }
+#pragma omp parallel
+    {
+      std::vector<double> f(nzc), arr(nzc);
+#pragma omp for schedule(static)
+      for (int jc = 1; jc <= nyc; ++jc)
+        for (int ic = 1; ic <= nxc; ++ic) {
+          for (int kc = 1; kc <= nzc; ++kc) f[kc - 1] = Rhs(ic, jc, kc);
+          if (uzface) f[0] = zero;
+          InverseTridiagonal1(tm.data(), tc.data(), tp.data(), f.data(), nzc, arr.data());
+          for (int kc = 1; kc <= nzc; ++kc) Rhs(ic, jc, kc) = f[kc - 1];
         }
     }
   }
@@ -1433,18 +1544,20 @@ struct Oracle {
 
   // ---- src/CFD_2nd/m_Poisson.f90:1078-1201 (clcPPE_z1: z R2HC, x R2HC, per-slot
   //      y tridiagonal with the (1,1,1) pin, x HC2R, z HC2R, * normfft); with y
-  //      periodic :954-1073 (clcPPE_z1_periodic: the same with cyclic y systems) ----
+  //      periodic :954-1073 (clcPPE_z1_periodic: the same with cyclic y systems);
+  //      with z between walls the z transforms are REDFT10 / REDFT01 (:267-307) ----
   void clcPPE(F3& prsrc, F3& prphiHalo) {
     // forward z transform of every (i,j) line
 #pragma omp parallel
     {
-      std::vector<double> line(nzc);
+      std::vector<double> line(nzc), db;
       std::vector<cplx> ba, bb;
 #pragma omp for schedule(static)
       for (int jc = 1; jc <= nyc; ++jc)
         for (int ic = 1; ic <= nxc; ++ic) {
           for (int kc = 1; kc <= nzc; ++kc) line[kc - 1] = prsrc(ic, jc, kc);
-          r2hc(planz, line.data(), ba, bb);
+          if (zper()) r2hc(planz, line.data(), ba, bb);
+          else redft10(nzc, line.data(), zcos, db);  // z between walls: REDFT10
           for (int kc = 1; kc <= nzc; ++kc) prsrc(ic, jc, kc) = line[kc - 1];
         }
     }
@@ -1487,13 +1600,14 @@ struct Oracle {
     }
 #pragma omp parallel
     {
-      std::vector<double> line(nzc);
+      std::vector<double> line(nzc), db;
       std::vector<cplx> ba, bb;
 #pragma omp for schedule(static)
       for (int jc = 1; jc <= nyc; ++jc)
         for (int ic = 1; ic <= nxc; ++ic) {
           for (int kc = 1; kc <= nzc; ++kc) line[kc - 1] = prsrc(ic, jc, kc);
-          hc2r(planz, line.data(), ba, bb);
+          if (zper()) hc2r(planz, line.data(), ba, bb);
+          else redft01(nzc, line.data(), zcos, db);  // REDFT01
           for (int kc = 1; kc <= nzc; ++kc) prsrc(ic, jc, kc) = line[kc - 1];
         }
     }
@@ -1863,7 +1977,11 @@ struct Oracle {
           clcUHat_PIMP_LES(2, uz, RealHalo);
           break;
         }
-        if (fimp) { clcUHat_FIMP_xz(RealArr1); clcUHat_FIMP_xz(RealArr2); clcUHat_FIMP_xz(RealHalo); }
+        if (fimp && zper()) { clcUHat_FIMP_xz(RealArr1); clcUHat_FIMP_xz(RealArr2); clcUHat_FIMP_xz(RealHalo); }
+        if (fimp && !zper()) {  // clcU1/2/3Hat_FIMP_011
+          clcUHat_FIMP_x(RealArr1); clcUHat_FIMP_x(RealArr2); clcUHat_FIMP_x(RealHalo);
+          clcUHat_FIMP_zwall(RealArr1, false); clcUHat_FIMP_zwall(RealArr2, false); clcUHat_FIMP_zwall(RealHalo, true);
+        }
         if (yper()) {  // clcU1/2/3Hat_FIMP_000 (after the x and z sweeps) or clcU1/2/3Hat_PIMP_0
           clcUHat_y_periodic(ux, RealArr1);
           clcUHat_y_periodic(uy, RealArr2);
@@ -2629,6 +2747,15 @@ void orc_hc2r(int n, double* x) {
   FFTPlan pl; pl.init(n);
   std::vector<cplx> a, b;
   hc2r(pl, x, a, b);
+}
+// FFTW-convention cosine transforms (REDFT10, REDFT01) of one line, for known-answer tests.
+void orc_redft10(int n, double* x) {
+  std::vector<double> b;
+  redft10(n, x, dct_table(n), b);
+}
+void orc_redft01(int n, double* x) {
+  std::vector<double> b;
+  redft01(n, x, dct_table(n), b);
 }
 
 double orc_dissipation(void* h) { return ((Oracle*)h)->TGDissipation(); }

@@ -79,6 +79,8 @@ def lib():
         L.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(OrcInfo)]
         L.orc_poisson.argtypes = [ctypes.c_void_p, _DP, _DP]
         L.orc_r2hc.argtypes = [ctypes.c_int, _DP]
+        L.orc_redft10.argtypes = [ctypes.c_int, _DP]
+        L.orc_redft01.argtypes = [ctypes.c_int, _DP]
         L.orc_hc2r.argtypes = [ctypes.c_int, _DP]
         L.orc_get_mesh.argtypes = [ctypes.c_void_p, _DP, _DP, _DP, _DP]
         L.orc_set_dt.argtypes = [ctypes.c_void_p, ctypes.c_double]
@@ -288,6 +290,18 @@ def r2hc(x):
 def hc2r(x):
     y = np.array(x, dtype=np.float64)
     lib().orc_hc2r(y.size, _p(y))
+    return y
+
+
+def redft10(x):
+    y = np.array(x, dtype=np.float64)
+    lib().orc_redft10(y.size, _p(y))
+    return y
+
+
+def redft01(x):
+    y = np.array(x, dtype=np.float64)
+    lib().orc_redft01(y.size, _p(y))
     return y
 
 

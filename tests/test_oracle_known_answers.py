@@ -456,3 +456,95 @@ def test_oracle_periodic_box_mirrors_free_slip_half_box(implicit):
     for k in ("ux", "uy", "uz", "p"):
         assert np.abs(a[k][:, :n // 2, :] - b[k]).max() < 1e-13 * max(1.0, np.abs(b[k]).max()), k
     assert abs(ea / eb - 1.0) < 1e-12
+
+
+def test_redft_matches_definition():
+    """FFTW's REDFT10 / REDFT01 (the z transforms between walls,
+    src/CFD_2nd/m_Poisson.f90:267-307) against their definitions:
+    Y_k = 2 sum_j X_j cos(pi (j + 1/2) k / n) and
+    Y_k = X_0 + 2 sum_{j>=1} X_j cos(pi j (k + 1/2) / n); the pair is 2n times
+    the identity."""
+    from oracle import oracle as O
+    for n in (6, 8, 12, 18):
+        x = np.random.default_rng(n).standard_normal(n)
+        j = np.arange(n)
+        y10 = np.array([2 * np.sum(x * np.cos(np.pi * (j + 0.5) * k / n)) for k in range(n)])
+        y01 = np.array([x[0] + 2 * np.sum(x[1:] * np.cos(np.pi * j[1:] * (k + 0.5) / n)) for k in range(n)])
+        assert np.abs(O.redft10(x) - y10).max() < 1e-12 * np.abs(y10).max()
+        assert np.abs(O.redft01(x) - y01).max() < 1e-12 * np.abs(y01).max()
+        assert np.abs(O.redft01(O.redft10(x)) / (2 * n) - x).max() < 1e-13
+
+
+def _z_walls(cfg, bc):
+    return cfg.copy(BcOption=[0, 0, cfg.BcOption[2], cfg.BcOption[3], bc, bc])
+
+
+def test_poisson_residual_z_walls():
+    """clcPPE with walls in z: the operator is the periodic 3-point Laplacian in
+    x, [am2Pr, ac2Pr, ap2Pr] in y and the 3-point Laplacian with Neumann ghosts
+    (phi_0 = phi_1, phi_nzc+1 = phi_nzc) in z; the residual is a plane constant
+    at j = 1 only (the (0,0)-mode pin)."""
+    from oracle import oracle as O
+    cfg = _z_walls(small_channel(24, 20, 12), -1)
+    o = O.Oracle(cfg)
+    src = np.random.default_rng(5).standard_normal(cfg.shape)
+    phi = o.poisson(src)
+    L = _laplacian(cfg, o, phi)
+    rdz2 = (cfg.nzc / cfg.zlz) ** 2
+    # replace the periodic z second difference of _laplacian by the Neumann one
+    L -= (np.roll(phi, 1, 0) - 2 * phi + np.roll(phi, -1, 0)) * rdz2
+    zm = np.concatenate([phi[:1], phi[:-1]], axis=0)
+    zp = np.concatenate([phi[1:], phi[-1:]], axis=0)
+    L += (zm - 2 * phi + zp) * rdz2
+    r = L - src
+    rm = r.mean(axis=(0, 2))
+    assert np.abs(r - rm[None, :, None]).max() < 1e-9 * np.abs(src).max()
+    assert np.abs(rm[1:]).max() < 1e-9 * np.abs(src).max()
+
+
+@pytest.mark.parametrize("implicit", [0, 1, 2])
+def test_oracle_z_walls_box_mirrors_z_periodic_box(implicit):
+    """The Taylor-Green field is also mirror-symmetric about z = 0 and pi (ux and
+    uy even, uz odd): 20 steps of the 2pi x pi x pi box with free-slip walls in
+    y and z (the z walls of m_BC_and_Halo.f90:313-338, REDFT10/01 in the Poisson
+    solve, FIMP's clcU*Hat_FIMP_011 sweeps) equal, on its lower z half, those of
+    the 2pi x pi x 2pi box with periodic z, to rounding, for the explicit,
+    partially and fully implicit schemes."""
+    from channel3d_b200 import initfield, workloads
+    from oracle import oracle as O
+    n = 16
+    full = workloads.taylor_green(n, dt=0.02).copy(IsImplicit=implicit, **({"dtMax": 0.005} if implicit == 0 else {}))
+    half = _z_walls(full.copy(nzc=n // 2, zlz=np.pi), -2)
+    out = []
+    for cfg in (full, half):
+        o = O.Oracle(cfg)
+        o.set_state(*initfield.taylor_green(cfg, yp=o.mesh()[0]))
+        d = o.step(20)
+        assert d["divmax2"] < 1e-13
+        out.append(o.get_state())
+    a, b = out
+    assert np.abs(b["uz"]).max() > 1e-2  # the flow has left the plane initial field
+    for k in ("ux", "uy", "uz", "p"):
+        assert np.abs(a[k][: n // 2] - b[k]).max() < 1e-13 * max(1.0, np.abs(b[k]).max()), k
+
+
+@pytest.mark.parametrize("implicit", [0, 1, 2])
+def test_oracle_duct_laminar_invariants(implicit):
+    """A duct (no-slip walls in y and z, periodic x): a streamwise field ux(y, z)
+    keeps uy = uz = 0 and stays independent of x under every scheme, and steps
+    from a noisy field are divergence-free."""
+    from channel3d_b200 import initfield
+    from oracle import oracle as O
+    cfg = _z_walls(small_channel(16, 12, 10, IsImplicit=implicit, dtMax=2e-4), -1)
+    o = O.Oracle(cfg)
+    yp = o.mesh()[0]
+    ux, uy, uz, p = initfield.laminar_noise(cfg, yp=yp)
+    o.set_state(ux, uy, uz, p)
+    assert o.step(3)["divmax2"] < 1e-13
+    zc = (np.arange(cfg.nzc) + 0.5) / cfg.nzc
+    ux0 = initfield.laminar_noise(cfg, yp=yp, amplitude=0.0)[0] * (4 * zc * (1 - zc))[:, None, None]
+    o.set_state(ux0, np.zeros(cfg.shape), np.zeros(cfg.shape), np.zeros(cfg.shape))
+    o.step(5)
+    s = o.get_state()
+    assert np.abs(s["uy"]).max() < 1e-14 and np.abs(s["uz"]).max() < 1e-14
+    assert np.abs(s["ux"] - s["ux"][:, :, :1]).max() < 1e-13

@@ -412,16 +412,17 @@ struct Oracle {
   }
 
   // ---- src/CFD_2nd/m_Poisson.f90:28-66 (modified wavenumbers, normfft) ----
-  std::vector<double> zcos;  // cosine table of the z transforms between walls
+  std::vector<double> zcos, xcos;  // cosine tables of the z and x transforms between walls
   void InitPoissonSolver() {
     WaveNumX.init(1, nxc); WaveNumZ.init(1, nzc);
     normfft = one;
+    // x or z between walls: cosine transform, WaveCoe = pi, norm = 2 (:39-64)
+    const double wcx = xper() ? 2.0 * PI : PI, nrmx = xper() ? one : two;
     for (int i = 1; i <= nxc; ++i) {
-      double wa1 = 2.0 * PI * (double)(i - 1) / (double)nxc;
+      double wa1 = wcx * (double)(i - 1) / (double)nxc;
       WaveNumX(i) = two * rdx2 * (std::cos(wa1) - one);
     }
-    normfft = normfft * one * (double)nxc;
-    // z between walls: cosine transform, WaveCoe = pi, norm = 2 (:53-64)
+    normfft = normfft * nrmx * (double)nxc;
     const double wcz = zper() ? 2.0 * PI : PI, nrmz = zper() ? one : two;
     for (int k = 1; k <= nzc; ++k) {
       double wa3 = wcz * (double)(k - 1) / (double)nzc;
@@ -432,6 +433,7 @@ struct Oracle {
     planx.init(nxc);
     planz.init(nzc);
     if (!zper()) zcos = dct_table(nzc);
+    if (!xper()) xcos = dct_table(nxc);
   }
 
   // ---- src/CFD_4th/m_MeshAndMetries.f90:86-91 (4th-order FD constants) ----
@@ -561,9 +563,10 @@ struct Oracle {
   }
   bool yper() const { return P.BcOption[2] == 0; }
   bool zper() const { return P.BcOption[4] == 0; }
+  bool xper() const { return P.BcOption[0] == 0; }
 
-  // ---- src/CFD_2nd/m_BC_and_Halo.f90:232-344 (SetBC_and_UpdateHalo), x periodic,
-  //      z periodic or between walls ----
+  // ---- src/CFD_2nd/m_BC_and_Halo.f90:232-344 (SetBC_and_UpdateHalo), x and z
+  //      periodic or between walls ----
   void SetBC_and_UpdateHalo() {
     const int* Bc = P.BcOption;
     if (Bc[3] == -1) {
@@ -598,6 +601,26 @@ struct Oracle {
         uz(i, 0, k) = uz(i, 1, k) - P.uzBcValue[2] * dyp(1);
       }
     }
+    // x walls (:285-311): ghost planes i = 0 and nxp over j = 0..nyp, k = 1..nzc;
+    // ux's wall faces i = 1 and nxp hold the wall values
+    if (Bc[1] == -1 || Bc[1] == -2) {
+      const bool ns = Bc[1] == -1;
+      for (int k = 1; k <= nzc; ++k) for (int j = 0; j <= nyp; ++j) {
+        ux(nxp, j, k) = P.uxBcValue[1];
+        ux(nxp + 1, j, k) = P.uxBcValue[1] * two - ux(nxc, j, k);
+        uy(nxp, j, k) = ns ? P.uyBcValue[1] * two - uy(nxc, j, k) : uy(nxc, j, k) + P.uyBcValue[1] * dx;
+        uz(nxp, j, k) = ns ? P.uzBcValue[1] * two - uz(nxc, j, k) : uz(nxc, j, k) + P.uzBcValue[1] * dx;
+      }
+    }
+    if (Bc[0] == -1 || Bc[0] == -2) {
+      const bool ns = Bc[0] == -1;
+      for (int k = 1; k <= nzc; ++k) for (int j = 0; j <= nyp; ++j) {
+        ux(1, j, k) = P.uxBcValue[0];
+        ux(0, j, k) = P.uxBcValue[0] * two - ux(2, j, k);
+        uy(0, j, k) = ns ? P.uyBcValue[0] * two - uy(1, j, k) : uy(1, j, k) - P.uyBcValue[0] * dx;
+        uz(0, j, k) = ns ? P.uzBcValue[0] * two - uz(1, j, k) : uz(1, j, k) - P.uzBcValue[0] * dx;
+      }
+    }
     // z walls (:313-338): ghost planes k = 0 and nzp over i = 1..nxc, j = 0..nyp;
     // uz's wall faces k = 1 and nzp hold the wall values
     if (Bc[5] == -1 || Bc[5] == -2) {
@@ -618,10 +641,10 @@ struct Oracle {
         uz(i, j, 0) = P.uzBcValue[4] * two - uz(i, j, 2);
       }
     }
-    int yh = yper() ? 1 : 0, zh = zper() ? 1 : 0;  // no halo copies across walls
-    halo(ux, 1, 1, yh, yh, zh, zh);
-    halo(uy, 1, 1, yh, yh, zh, zh);
-    halo(uz, 1, 1, yh, yh, zh, zh);
+    int xh = xper() ? 1 : 0, yh = yper() ? 1 : 0, zh = zper() ? 1 : 0;  // no halo copies across walls
+    halo(ux, xh, xh, yh, yh, zh, zh);
+    halo(uy, xh, xh, yh, yh, zh, zh);
+    halo(uz, xh, xh, yh, yh, zh, zh);
   }
 
   // ---- src/CFD_2nd/m_BC_and_Halo.f90:349-405 (SetBC_and_UpdateHaloForPrSrc) ----
@@ -632,11 +655,15 @@ struct Oracle {
     if (Bc[2] == -1 || Bc[2] == -2)
       for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i)
         uy(i, 1, k) = uy_ym[(size_t)(i - 1) + (size_t)nxc * (k - 1)];
+    if (Bc[1] == -1 || Bc[1] == -2)
+      for (int k = 1; k <= nzc; ++k) for (int j = 0; j <= nyp; ++j) ux(nxp, j, k) = P.uxBcValue[1];
+    if (Bc[0] == -1 || Bc[0] == -2)
+      for (int k = 1; k <= nzc; ++k) for (int j = 0; j <= nyp; ++j) ux(1, j, k) = P.uxBcValue[0];
     if (Bc[5] == -1 || Bc[5] == -2)
       for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) uz(i, j, nzp) = P.uzBcValue[5];
     if (Bc[4] == -1 || Bc[4] == -2)
       for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) uz(i, j, 1) = P.uzBcValue[4];
-    halo(ux, 0, 1, 0, 0, 0, 0);
+    halo(ux, 0, xper() ? 1 : 0, 0, 0, 0, 0);
     halo(uy, 0, 0, 0, yper() ? 1 : 0, 0, 0);
     halo(uz, 0, 0, 0, 0, 0, zper() ? 1 : 0);
   }
@@ -646,10 +673,12 @@ struct Oracle {
     const int* Bc = P.BcOption;
     if (Bc[3] < 0) for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) pr(i, nyp, k) = pr(i, nyc, k);
     if (Bc[2] < 0) for (int k = 1; k <= nzc; ++k) for (int i = 1; i <= nxc; ++i) pr(i, 0, k) = pr(i, 1, k);
+    if (Bc[1] < 0) for (int k = 1; k <= nzc; ++k) for (int j = 0; j <= nyp; ++j) pr(nxp, j, k) = pr(nxc, j, k);
+    if (Bc[0] < 0) for (int k = 1; k <= nzc; ++k) for (int j = 0; j <= nyp; ++j) pr(0, j, k) = pr(1, j, k);
     if (Bc[5] < 0) for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) pr(i, j, nzp) = pr(i, j, nzc);
     if (Bc[4] < 0) for (int j = 0; j <= nyp; ++j) for (int i = 1; i <= nxc; ++i) pr(i, j, 0) = pr(i, j, 1);
-    int yh = yper() ? 1 : 0, zh = zper() ? 1 : 0;
-    halo(pr, 1, 1, yh, yh, zh, zh);
+    int xh = xper() ? 1 : 0, yh = yper() ? 1 : 0, zh = zper() ? 1 : 0;
+    halo(pr, xh, xh, yh, yh, zh, zh);
   }
 
   // ---- src/CFD_2nd/m_Tools.f90:21-46 (CalcMaxCFL) ----
@@ -1007,6 +1036,37 @@ struct Oracle {
           for (int ic = 1; ic <= nxc; ++ic) line[ic - 1] = Rhs(ic, jc, kc);
           InversePTriFixedCoe1(mic, cic, pic, line.data(), nxc, 1, a, b, c, d);
           for (int ic = 1; ic <= nxc; ++ic) Rhs(ic, jc, kc) = line[ic - 1];
+        }
+    }
+  }
+
+  // ---- the x sweep between walls (clcU1/2/3Hat_FIMP_111, src/CFD_2nd/
+  //      m_TSchemeFIMP_inc.f90:476-507, 868-890, 1286-1308): uy and uz with the
+  //      Crank-Nicolson wall metrics am1cForCN / ap1cForCN, ux with constant
+  //      coefficients and its wall face i = 1 held.  The reference accepts walls
+  //      in x only together with walls in z (m_TScheme.f90:111-113). ----
+  void clcUHat_FIMP_xwall(F3& Rhs, bool uxface) {
+    std::vector<double> tm(nxc), tc(nxc), tp(nxc);
+    for (int ic = 1; ic <= nxc; ++ic) {
+      if (uxface) {
+        tm[ic - 1] = -pmBeta * rdx2; tp[ic - 1] = -pmBeta * rdx2; tc[ic - 1] = pmBeta * rdx2 * two + one;
+      } else {
+        tp[ic - 1] = -pmBeta * ap1cForCN(ic);
+        tm[ic - 1] = -pmBeta * am1cForCN(ic);
+        tc[ic - 1] = -tp[ic - 1] - tm[ic - 1] + one;
+      }
+    }
+    if (uxface) { tp[0] = zero; tc[0] = one; tm[0] = zero; }
+#pragma omp parallel
+    {
+      std::vector<double> f(nxc), arr(nxc);
+#pragma omp for schedule(static)
+      for (int kc = 1; kc <= nzc; ++kc)
+        for (int jc = 1; jc <= nyc; ++jc) {
+          for (int ic = 1; ic <= nxc; ++ic) f[ic - 1] = Rhs(ic, jc, kc);
+          if (uxface) f[0] = zero;
+          InverseTridiagonal1(tm.data(), tc.data(), tp.data(), f.data(), nxc, arr.data());
+          for (int ic = 1; ic <= nxc; ++ic) Rhs(ic, jc, kc) = f[ic - 1];
         }
     }
   }
@@ -1565,9 +1625,13 @@ struct Oracle {
 #pragma omp parallel
     {
       std::vector<cplx> ba, bb;
+      std::vector<double> db;
 #pragma omp for schedule(static)
       for (int kc = 1; kc <= nzc; ++kc)
-        for (int jc = 1; jc <= nyc; ++jc) r2hc(planx, &prsrc(1, jc, kc), ba, bb);
+        for (int jc = 1; jc <= nyc; ++jc) {
+          if (xper()) r2hc(planx, &prsrc(1, jc, kc), ba, bb);
+          else redft10(nxc, &prsrc(1, jc, kc), xcos, db);  // x between walls: REDFT10
+        }
     }
     // y tridiagonal per (ic,kc) slot
 #pragma omp parallel
@@ -1594,9 +1658,13 @@ struct Oracle {
 #pragma omp parallel
     {
       std::vector<cplx> ba, bb;
+      std::vector<double> db;
 #pragma omp for schedule(static)
       for (int kc = 1; kc <= nzc; ++kc)
-        for (int jc = 1; jc <= nyc; ++jc) hc2r(planx, &prsrc(1, jc, kc), ba, bb);
+        for (int jc = 1; jc <= nyc; ++jc) {
+          if (xper()) hc2r(planx, &prsrc(1, jc, kc), ba, bb);
+          else redft01(nxc, &prsrc(1, jc, kc), xcos, db);  // REDFT01
+        }
     }
 #pragma omp parallel
     {
@@ -1978,8 +2046,9 @@ struct Oracle {
           break;
         }
         if (fimp && zper()) { clcUHat_FIMP_xz(RealArr1); clcUHat_FIMP_xz(RealArr2); clcUHat_FIMP_xz(RealHalo); }
-        if (fimp && !zper()) {  // clcU1/2/3Hat_FIMP_011
-          clcUHat_FIMP_x(RealArr1); clcUHat_FIMP_x(RealArr2); clcUHat_FIMP_x(RealHalo);
+        if (fimp && !zper()) {  // clcU1/2/3Hat_FIMP_011, or _111 with walls in x too
+          if (xper()) { clcUHat_FIMP_x(RealArr1); clcUHat_FIMP_x(RealArr2); clcUHat_FIMP_x(RealHalo); }
+          else { clcUHat_FIMP_xwall(RealArr1, true); clcUHat_FIMP_xwall(RealArr2, false); clcUHat_FIMP_xwall(RealHalo, false); }
           clcUHat_FIMP_zwall(RealArr1, false); clcUHat_FIMP_zwall(RealArr2, false); clcUHat_FIMP_zwall(RealHalo, true);
         }
         if (yper()) {  // clcU1/2/3Hat_FIMP_000 (after the x and z sweeps) or clcU1/2/3Hat_PIMP_0

@@ -548,3 +548,74 @@ def test_oracle_duct_laminar_invariants(implicit):
     s = o.get_state()
     assert np.abs(s["uy"]).max() < 1e-14 and np.abs(s["uz"]).max() < 1e-14
     assert np.abs(s["ux"] - s["ux"][:, :, :1]).max() < 1e-13
+
+
+@pytest.mark.parametrize("implicit", [0, 1, 2])
+def test_oracle_walled_box_mirrors_periodic_box(implicit):
+    """Walls in x as well (clcU*Hat_FIMP_111's x sweep, the x-wall ghost rules of
+    m_BC_and_Halo.f90:285-311, REDFT10/01 in x): the Taylor-Green field is
+    mirror-symmetric about x = 0 and pi too (ux odd, uy and uz even), so 20 steps
+    of the pi x pi x pi box with free-slip walls on all six faces equal, on the
+    corner x, z in [0, pi], those of the 2pi x pi x 2pi box periodic in x and z."""
+    from channel3d_b200 import initfield, workloads
+    from oracle import oracle as O
+    n = 16
+    full = workloads.taylor_green(n, dt=0.02).copy(IsImplicit=implicit, **({"dtMax": 0.005} if implicit == 0 else {}))
+    box = full.copy(nxc=n // 2, nzc=n // 2, xlx=np.pi, zlz=np.pi, BcOption=[-2, -2, -2, -2, -2, -2])
+    out = []
+    for cfg in (full, box):
+        o = O.Oracle(cfg)
+        o.set_state(*initfield.taylor_green(cfg, yp=o.mesh()[0]))
+        assert o.step(20)["divmax2"] < 1e-13
+        out.append(o.get_state())
+    a, b = out
+    for k in ("ux", "uy", "uz", "p"):
+        assert np.abs(a[k][: n // 2, :, : n // 2] - b[k]).max() < 1e-13 * max(1.0, np.abs(b[k]).max()), k
+
+
+def test_poisson_residual_x_and_z_walls():
+    """clcPPE with walls in x and z: Neumann 3-point Laplacians in x and z, the
+    walls' operator in y; the residual is a plane constant at j = 1 only."""
+    from oracle import oracle as O
+    cfg = small_channel(16, 20, 12).copy(BcOption=[-1, -1, -1, -1, -1, -1])
+    o = O.Oracle(cfg)
+    src = np.random.default_rng(6).standard_normal(cfg.shape)
+    phi = o.poisson(src)
+    L = _laplacian(cfg, o, phi)
+    r2 = {2: (cfg.nxc / cfg.xlx) ** 2, 0: (cfg.nzc / cfg.zlz) ** 2}
+    for ax, rr in r2.items():
+        n = phi.shape[ax]
+        L -= (np.roll(phi, 1, ax) - 2 * phi + np.roll(phi, -1, ax)) * rr
+        lo = np.take(phi, [0] + list(range(n - 1)), axis=ax)
+        hi = np.take(phi, list(range(1, n)) + [n - 1], axis=ax)
+        L += (lo - 2 * phi + hi) * rr
+    r = L - src
+    rm = r.mean(axis=(0, 2))
+    assert np.abs(r - rm[None, :, None]).max() < 1e-9 * np.abs(src).max()
+    assert np.abs(rm[1:]).max() < 1e-9 * np.abs(src).max()
+
+
+def test_oracle_lid_driven_cavity_symmetry():
+    """The lid-driven cavity of Input/LidDrivenCavity.prm (FlowType 5, no-slip
+    walls on all faces, the top wall moving with ux = 1, fully implicit,
+    xnu 1e-2) at 16^3: started from rest the flow is divergence-free and stays
+    mirror-symmetric about the mid-plane z = 1/2 (ux, uy, p even, uz odd)."""
+    from channel3d_b200 import ChannelConfig
+    from oracle import oracle as O
+    n = 16
+    cfg = ChannelConfig(FlowType=5, nxc=n, nyc=n, nzc=n, xlx=1.0, yly=1.0, zlz=1.0, xnu=1e-2, dtMax=1e-2, iCFL=2,
+                        IsImplicit=2, BcOption=[-1, -1, -1, -1, -1, -1], uxBcValue=[0, 0, 0, 1.0, 0, 0],
+                        IsUxConst=False, ubulk=0.0, ybulk1=0.0, ybulk2=1.0, nSection=1, SectionLength=[1.0],
+                        nycSection=[n], StretType=[0], StretOption=[0], SectioncStret=[0.0], RunName="LidCavity")
+    o = O.Oracle(cfg)
+    z = np.zeros(cfg.shape)
+    o.set_state(z, z, z, z)
+    d = o.step(20)
+    assert d["rc"] == 0 and d["divmax2"] < 1e-13
+    s = o.get_state()
+    assert np.abs(s["ux"]).max() > 0.1  # the lid has set the fluid moving
+    for k in ("ux", "uy", "p"):
+        assert np.abs(s[k] - s[k][::-1]).max() < 1e-13, k
+    # uz lives on the z faces k = 0..n-1 (face 0 the wall): face k mirrors face n - k
+    uz = s["uz"]
+    assert np.abs(uz[1:] + uz[:0:-1]).max() < 1e-13 and np.abs(uz[0]).max() == 0.0

@@ -170,6 +170,13 @@ def test_prm_reader_reads_reference_decks():
     assert rc in (_lib.CH3D_OK, _lib.CH3D_ERR_CUDA), (rc, lib.ch3d_last_error())
     if h.value:
         lib.ch3d_destroy(h)
+    # the lid-driven cavity deck (walls on all faces, FlowType 5): read as written,
+    # rejected by the library (walls in x and z are in the oracle only)
+    cav = ChannelConfig.from_prm(os.path.join(REF_DECKS, "LidDrivenCavity.prm"))
+    assert cav.FlowType == 5 and cav.BcOption == [-1] * 6 and cav.uxBcValue[3] == 1.0 and cav.IsImplicit == 2
+    c, h = cav.to_c(), ctypes.c_void_p()
+    assert lib.ch3d_create(ctypes.byref(c), _lib.dptr(mesh_y(cav)), ctypes.byref(h)) == _lib.CH3D_ERR_UNSUPPORTED
+    assert not h.value
 
 
 def test_restart_roundtrip_and_size_check(tmp_path):

@@ -619,3 +619,31 @@ def test_oracle_lid_driven_cavity_symmetry():
     # uz lives on the z faces k = 0..n-1 (face 0 the wall): face k mirrors face n - k
     uz = s["uz"]
     assert np.abs(uz[1:] + uz[:0:-1]).max() < 1e-13 and np.abs(uz[0]).max() == 0.0
+
+
+@pytest.mark.parametrize("bc", ["periodic_y", "walls_xz"])
+def test_boundary_variants_are_thread_count_independent(bc):
+    """The oracle is also the timed CPU baseline on all host threads: the
+    periodic-y (cyclic Poisson solve, FIMP_000) and walled (cosine transforms,
+    FIMP_111) variants give bit-identical states on 1 and 4 threads."""
+    from channel3d_b200 import initfield, workloads
+    from oracle import oracle as O
+    if bc == "periodic_y":
+        cfg = workloads.taylor_green_periodic(16).copy(nxc=16, nyc=12, nzc=8, nycSection=[12])
+    else:
+        cfg = small_channel(16, 12, 8, IsImplicit=2).copy(BcOption=[-1, -1, -1, -1, -1, -1], IsUxConst=False,
+                                                          uxBcValue=[0, 0, 0, 1.0, 0, 0])
+    o = O.Oracle(cfg)
+    st = initfield.laminar_noise(cfg, yp=o.mesh()[0])
+    out = []
+    nthr = O.num_threads()
+    try:
+        for n in (1, 4):
+            O.set_threads(n)
+            o.set_state(*st)
+            assert o.step(3)["divmax2"] < 1e-13
+            out.append(o.get_state())
+    finally:
+        O.set_threads(nthr)
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
